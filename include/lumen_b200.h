@@ -1,0 +1,218 @@
+/*
+ * lumen_b200 — C ABI of the B200 photon-transport engine (the photon loop behind lumen.simulate).
+ *
+ * The reference runs its photon loop through tallymap (src/lumen/run.py:93 `run`, :693 `trace`, :534 `rebuild`):
+ * one item per photon loops `step` (src/lumen/transport/step.py:516) until the photon ends, appends a deposit record
+ * per sensor crossing, and a second launch folds the records into per-sensor cells. This library replaces that seam:
+ * one call traces a batch of photons on the GPU and reduces their deposits straight into per-sensor FP64 tallies
+ * (arrival, arrival x time, per-photon second moment, time histograms, health fates, and optionally the Jacobian of
+ * the arrivals in the run's gradient parameters).
+ *
+ * Conventions: plain C types and pointers only; every entry point returns a LumenStatus (0 = OK), never throws; a
+ * scene handle is immutable after creation except for its parameter pools (lumen_b200_scene_set_pools), and one
+ * handle may serve concurrent calls on different streams. Pointers documented "device" are CUDA device memory owned
+ * by the caller; "host" pointers are read during the call only.
+ */
+#ifndef LUMEN_B200_H
+#define LUMEN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUMEN_B200_ABI_VERSION 1
+
+typedef enum LumenStatus {
+  LUMEN_OK = 0,
+  LUMEN_ERR_ARG = 1,          /* a bad argument: null pointer, size out of range, inconsistent scene arrays */
+  LUMEN_ERR_CUDA = 2,         /* a CUDA runtime call failed (the message says which) */
+  LUMEN_ERR_SCENE = 3,        /* the scene uses a feature this engine does not build (see lumen_b200_last_error) */
+  LUMEN_ERR_STEP_BUDGET = 4,  /* the device step budget of the call ran out before every photon ended */
+  LUMEN_ERR_NO_DEVICE = 5,    /* no CUDA device, or not an sm_100 device */
+  LUMEN_ERR_NOT_SUPPORTED = 6 /* a request outside this build (e.g. more gradient parameters than LUMEN_MAX_GRAD) */
+} LumenStatus;
+
+/* ---------------------------------------------------------------------------------------------- array layouts */
+/* Per volume v (0..n_vol-1; index n_vol is the outside), int record of LUMEN_VOL_I int32: */
+enum {
+  LUMEN_VI_KIND = 0,   /* the solid (kind) of the volume; -1 for the outside */
+  LUMEN_VI_PARENT = 1, /* the mother volume (n_vol for a top volume; -1 for the outside) */
+  LUMEN_VI_CLS = 2,    /* the surface lookup's class */
+  LUMEN_VI_SENSOR = 3, /* sensor index, -1 none */
+  LUMEN_VI_PRIO = 4,   /* the locate rule's order among siblings (lower first) */
+  LUMEN_VI_C0 = 5,     /* first candidate (daughter) in cand[] */
+  LUMEN_VI_CN = 6,     /* number of candidates */
+  LUMEN_VI_NODE0 = 7,  /* first BVH node of the volume's daughter BVH (world frame) */
+  LUMEN_VI_NODE1 = 8,  /* one past its last node (NODE0 == NODE1: no daughters) */
+  LUMEN_VOL_I = 10
+};
+/* Per volume, float record of LUMEN_VOL_F float32: R (3x3 row-major, world = R local + t), t (3), padded world box */
+enum { LUMEN_VF_R = 0, LUMEN_VF_T = 9, LUMEN_VF_LO = 12, LUMEN_VF_HI = 15, LUMEN_VOL_F = 18 };
+/* BVH node: float lo (3), hi (3); int skip (next node when not descending), count (items at a leaf), start */
+enum { LUMEN_NODE_F = 6, LUMEN_NODE_I = 4 };
+/* Kind (one distinct solid): int l0 (first leaf), nl (leaves), p0 (first program op), pl (program length) */
+enum { LUMEN_KIND_I = 4 };
+/* Leaf: float og (3) plane origin, oq (3) quadric origin, A (9, row-major), b (3), c, sa = max |A_ij| */
+enum { LUMEN_LF_OG = 0, LUMEN_LF_OQ = 3, LUMEN_LF_A = 6, LUMEN_LF_B = 15, LUMEN_LF_C = 18, LUMEN_LF_SA = 19,
+       LUMEN_LEAF_F = 20 };
+/* Leaf ints: typ (0: planes only, 1: quadric and planes), p0 (first plane), np (planes) */
+enum { LUMEN_LEAF_I = 4 };
+/* Plane: n (3), h — the leaf holds n . (x - og) <= h */
+enum { LUMEN_PLANE_F = 4 };
+/* Program op: op (0 push leaf arg, 1 union, 2 intersection, 3 subtraction), arg */
+enum { LUMEN_PROG_I = 2 };
+
+/* Surface table: row ints of LUMEN_ROW_I: model (0 reflect, 1 dielectric, 2 complex index), normal, glisur,
+   far_opaque, per_normal, then one table index per column (LUMEN_COL_*) read at the photon energy */
+enum { LUMEN_COL_R = 0, LUMEN_COL_T, LUMEN_COL_EFF, LUMEN_COL_PSPIKE, LUMEN_COL_PLOBE, LUMEN_COL_PBACK,
+       LUMEN_COL_SIGMA, LUMEN_COL_POLISH, LUMEN_COL_NR, LUMEN_COL_NK, LUMEN_N_COL };
+enum { LUMEN_RI_MODEL = 0, LUMEN_RI_NORMAL = 1, LUMEN_RI_GLISUR = 2, LUMEN_RI_FAR_OPAQUE = 3,
+       LUMEN_RI_PER_NORMAL = 4, LUMEN_RI_COL = 6, LUMEN_ROW_I = 16 };
+/* Medium ints: index table (-1 opaque), absorption-length table (-1 none), Rayleigh-length table (-1 none) */
+enum { LUMEN_MI_INDEX = 0, LUMEN_MI_ABS = 1, LUMEN_MI_RAY = 2, LUMEN_MED_I = 4 };
+/* Table t: tab[2t] = offset into a pool, tab[2t+1] = knots k >= 1; pool[off .. off+k) energies (eV, ascending),
+   pool[off+k .. off+2k) values; linear in photon energy between knots, held beyond (G4PhysicsVector::Value) */
+
+#define LUMEN_MAX_GRAD 8      /* gradient parameters per call */
+#define LUMEN_MAX_LEAVES 16   /* leaves per solid */
+#define LUMEN_MAX_PLANES 8    /* planes per leaf */
+#define LUMEN_MAX_KNOTS 64    /* knots of an index table (its group index is tabulated per call) */
+
+/* ------------------------------------------------------------------------------------------ the detector */
+typedef struct LumenSceneDesc {
+  /* geometry (the navigator's arrays, src/lumen/geometry/navigator_build.py:51, csg_build.py:30) */
+  int32_t n_vol, n_kind, n_leaf, n_plane, n_prog, n_node, n_item, n_cand;
+  const int32_t* vol_i;   /* host, (n_vol + 1) * LUMEN_VOL_I */
+  const float* vol_f;     /* host, n_vol * LUMEN_VOL_F */
+  const int32_t* cand;    /* host, n_cand: daughters per volume (and the outside's top volumes) */
+  const float* node_f;    /* host, n_node * LUMEN_NODE_F */
+  const int32_t* node_i;  /* host, n_node * LUMEN_NODE_I */
+  const int32_t* items;   /* host, n_item: BVH leaf items (volume ids) */
+  const int32_t* kind_i;  /* host, n_kind * LUMEN_KIND_I */
+  const float* leaf_f;    /* host, n_leaf * LUMEN_LEAF_F */
+  const int32_t* leaf_i;  /* host, n_leaf * LUMEN_LEAF_I */
+  const float* plane_f;   /* host, n_plane * LUMEN_PLANE_F */
+  const int32_t* prog_i;  /* host, n_prog * LUMEN_PROG_I */
+  float reach;            /* m: the diagonal of the box holding every volume (transport/step.py:98) */
+  /* optics (the surface lookup, src/lumen/build/lookup.py:394; media, src/lumen/media/bulk.py:88) */
+  int32_t n_cls, n_med, n_row, n_tab, n_pool, n_sensor;
+  const int32_t* cls_medium; /* host, n_cls */
+  const int32_t* row_of;     /* host, n_cls * n_cls: surface row of a (class left, class met) pair, -1 none */
+  const int32_t* med_i;      /* host, n_med * LUMEN_MED_I */
+  const int32_t* row_i;      /* host, n_row * LUMEN_ROW_I */
+  const int32_t* tab;        /* host, n_tab * 2 */
+  const float* pool;         /* host, n_pool: the table values every call reads unless set_pools replaces them */
+} LumenSceneDesc;
+
+typedef struct LumenScene LumenScene; /* opaque: the device copy of a LumenSceneDesc */
+
+/* ------------------------------------------------------------------------------------------- the photons */
+/* Explicit emission rows, structure of arrays on the device (src/lumen/record.py Photons: x, d, t, lam, w, pol).
+   pol may be null: every row unpolarised (E = 0). */
+typedef struct LumenRows {
+  const float *x, *y, *z;       /* device, n: start position (m) */
+  const float *dx, *dy, *dz;    /* device, n: unit direction */
+  const float *t, *lam, *w;     /* device, n: time (ns), wavelength (nm), the row's weight w0 */
+  const float* pol;             /* device, n * 6 (er xyz, ei xyz) or null */
+  const int32_t* event;         /* device, n: the event each row tallies into, or null (event 0) */
+} LumenRows;
+
+/* A procedural source drawn on the device from the photon's own key (src/lumen/sources/_base.py:312): photon i of
+   the call belongs to the event e with ev_first[e] <= first_id + i < ev_first[e + 1]. */
+enum { LUMEN_SRC_POINT = 0,   /* isotropic point (sources/point.py:73): ev_f = x y z, time */
+       LUMEN_SRC_TRACK = 1,   /* straight track emitting on a cone: ev_f = x y z (start), ux uy uz (unit), length, time */
+       LUMEN_SRC_SCINT = 2 }; /* isotropic scintillation point with a two-exponential profile: ev_f = x y z, time */
+enum { LUMEN_EV_F = 8 };
+typedef struct LumenSource {
+  int32_t kind;
+  int32_t n_events;
+  const float* ev_f;        /* device, n_events * LUMEN_EV_F */
+  const int64_t* ev_first;  /* device, n_events + 1: prefix sums of the events' photon counts */
+  const float* ev_w;        /* device, n_events: each photon's row weight w0 in that event */
+  float lam0, lam1;         /* nm: a fixed wavelength (lam1 <= lam0) or uniform in [lam0, lam1] */
+  float cone_cos;           /* LUMEN_SRC_TRACK: cosine of the cone half-angle */
+  float tau1, tau2, frac1;  /* LUMEN_SRC_SCINT: decay times (ns) and the first component's share */
+} LumenSource;
+
+/* ------------------------------------------------------------------------------------------ the controls */
+typedef struct LumenControls {
+  float max_distance;      /* m: a query's reach (<= 0: the scene's reach) */
+  float roulette;          /* epsilon > 0 (src/lumen/rules/choices.py:112) */
+  int32_t max_vertices;    /* the per-photon vertex guard (src/lumen/run.py:70) */
+  int32_t n_grad;          /* gradient parameters (0..LUMEN_MAX_GRAD) */
+  int32_t grad_tab[LUMEN_MAX_GRAD];  /* each parameter: the table whose values all move together (d/d value) */
+  int64_t step_budget;     /* device step budget of the call (<= 0: none) */
+} LumenControls;
+
+/* --------------------------------------------------------------------------------------------- the tallies */
+/* Device outputs, FP64, ADDED to (the caller zeroes them): per event e and sensor s, index e * n_sensor + s. */
+enum { LUMEN_H_LOST = 0, LUMEN_H_ABANDONED, LUMEN_H_ESCAPED, LUMEN_H_DISTANCE_CUT, LUMEN_H_ABSORBED_BULK,
+       LUMEN_H_ABSORBED_SURFACE, LUMEN_H_ROULETTED, LUMEN_H_REWEIGHTED, LUMEN_H_TRUNCATED, LUMEN_H_PUSHED,
+       LUMEN_H_START, LUMEN_N_HEALTH };
+enum { LUMEN_C_PHOTONS = 0, LUMEN_C_STEPS, LUMEN_C_DEPOSITS, LUMEN_C_TRUNCATED, LUMEN_C_MULTI, LUMEN_N_COUNT };
+typedef struct LumenTallies {
+  int32_t n_events;          /* events tallied (>= 1) */
+  int32_t n_bins;            /* time-histogram bins per sensor (0: none) */
+  float bin0, bin_w;         /* ns: first bin edge and width */
+  double* arrival;           /* device, n_events * n_sensor: sum of q w0 (src/lumen/readout/fill.py:216) */
+  double* arrival_t;         /* device, same: sum of q w0 time */
+  double* arrival2;          /* device, same: sum over photons of (the photon's sum of q w0)^2 */
+  double* hist;              /* device, n_events * n_sensor * n_bins, or null */
+  double* jac;               /* device, n_events * n_sensor * n_grad: d arrival / d parameter, or null */
+  double* health;            /* device, LUMEN_N_HEALTH: the fates summed over photons (times w0) */
+  unsigned long long* counts;/* device, LUMEN_N_COUNT */
+} LumenTallies;
+
+/* ------------------------------------------------------------------------------------------- entry points */
+/* Version of this ABI (LUMEN_B200_ABI_VERSION). */
+int32_t lumen_b200_abi_version(void);
+/* The last error message of this thread (static storage; "" after success). */
+const char* lumen_b200_last_error(void);
+
+/* Upload a detector to the current CUDA device; replaces the reference's Navigator.operands / pack.pack device put
+   (src/lumen/geometry/navigate.py:140, src/lumen/api.py:842). */
+int32_t lumen_b200_scene_create(const LumenSceneDesc* desc, LumenScene** out);
+/* Replace the live and reference parameter pools (host, n_pool floats each; ref may be null: the live pool): the
+   reference's packed params and reference (src/lumen/transport/step.py:129 `operands`). */
+int32_t lumen_b200_scene_set_pools(LumenScene* scene, const float* pool_live, const float* pool_ref);
+int32_t lumen_b200_scene_destroy(LumenScene* scene);
+
+/* Trace photons first_id .. first_id + n - 1 and add their tallies. Replaces runner.trace + runner.rebuild
+   (src/lumen/run.py:693, :534): photon i keyed fold_in(key, first_id + i) (src/lumen/run.py:309). Exactly one of
+   rows / source is non-null. stream: a cudaStream_t (null: the default stream). */
+int32_t lumen_b200_trace(const LumenScene* scene, const LumenRows* rows, const LumenSource* source,
+                         uint32_t key0, uint32_t key1, int64_t first_id, int64_t n, const LumenControls* controls,
+                         LumenTallies* out, void* stream);
+
+/* The adjoint: replay photons first_id .. first_id + n - 1 from their keys (no stored path) and add
+   grads[p] += sum over events e and sensors s of cotangent[e * n_sensor + s] * d arrival[e, s] / d parameter p.
+   Replaces the reverse pass of the reference's custom_jvp rule (src/lumen/api.py:748-787). cotangent, grads:
+   device; grads has controls->n_grad doubles. */
+int32_t lumen_b200_adjoint(const LumenScene* scene, const LumenRows* rows, const LumenSource* source,
+                           uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
+                           const LumenControls* controls, const double* cotangent, int32_t n_events,
+                           double* grads, void* stream);
+
+/* Per-photon trace record for parity checks: for each photon, out_i[5*i ..] = vertices, deposits, end code
+   (0 alive at the guard, 1 ended), first sensor hit (-1 none), last volume; out_f[4*i ..] = sum of q, final
+   weight, final time, sum of q * time. Same inputs as lumen_b200_trace; device outputs. */
+int32_t lumen_b200_trace_photons(const LumenScene* scene, const LumenRows* rows, const LumenSource* source,
+                                 uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
+                                 const LumenControls* controls, int32_t* out_i, float* out_f, void* stream);
+
+/* Navigator query on a fixed ray set (the geometry hot spot, src/lumen/geometry/navigate.py:663, as the step calls
+   it through TrackedGeometry.query, src/lumen/build/tracked.py:86): for ray i, out_i[8*i ..] = hit, vol_before,
+   vol_after, cls_before, cls_after, srf, zero, sensor; out_f[4*i ..] = t, normal xyz. vol[i] < 0: located first.
+   Device inputs: ray (n * 6: origin, direction), vol, srf (n each); t_max a scalar. */
+int32_t lumen_b200_query(const LumenScene* scene, const float* ray, const int32_t* vol, const int32_t* srf,
+                         float t_max, int64_t n, int32_t* out_i, float* out_f, void* stream);
+
+/* Volume holding each point (src/lumen/geometry/navigate.py:226 `locate`): device pts (n * 3) -> vol (n). */
+int32_t lumen_b200_locate(const LumenScene* scene, const float* pts, int64_t n, int32_t* vol, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUMEN_B200_H */

@@ -1,0 +1,151 @@
+"""ctypes mirror of the C ABI (include/lumen_b200.h) and the loader of the engine library.
+
+The engine is ``lumen_b200/liblumen_b200.so`` (built in-tree by ``lumen_b200.build``). ``engine()`` loads it and fails
+loudly when it is missing: there is no CPU fallback on the product path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liblumen_b200.so")
+
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+c_f64p = ctypes.POINTER(ctypes.c_double)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+MAX_GRAD = 8
+N_COL = 10
+N_HEALTH = 11
+N_COUNT = 5
+HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "absorbed_surface", "rouletted",
+          "reweighted", "truncated", "pushed", "start")  # fmt: skip
+COUNTS = ("photons", "steps", "deposits", "truncated", "multi")
+SRC_POINT, SRC_TRACK, SRC_SCINT = 0, 1, 2
+EV_F = 8
+
+
+class LumenSceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_vol", ctypes.c_int32), ("n_kind", ctypes.c_int32), ("n_leaf", ctypes.c_int32),
+        ("n_plane", ctypes.c_int32), ("n_prog", ctypes.c_int32), ("n_node", ctypes.c_int32),
+        ("n_item", ctypes.c_int32), ("n_cand", ctypes.c_int32),
+        ("vol_i", c_i32p), ("vol_f", c_f32p), ("cand", c_i32p), ("node_f", c_f32p), ("node_i", c_i32p),
+        ("items", c_i32p), ("kind_i", c_i32p), ("leaf_f", c_f32p), ("leaf_i", c_i32p), ("plane_f", c_f32p),
+        ("prog_i", c_i32p), ("reach", ctypes.c_float),
+        ("n_cls", ctypes.c_int32), ("n_med", ctypes.c_int32), ("n_row", ctypes.c_int32), ("n_tab", ctypes.c_int32),
+        ("n_pool", ctypes.c_int32), ("n_sensor", ctypes.c_int32),
+        ("cls_medium", c_i32p), ("row_of", c_i32p), ("med_i", c_i32p), ("row_i", c_i32p), ("tab", c_i32p),
+        ("pool", c_f32p),
+    ]  # fmt: skip
+
+
+class LumenRows(ctypes.Structure):
+    _fields_ = [("x", c_f32p), ("y", c_f32p), ("z", c_f32p), ("dx", c_f32p), ("dy", c_f32p), ("dz", c_f32p),
+                ("t", c_f32p), ("lam", c_f32p), ("w", c_f32p), ("pol", c_f32p), ("event", c_i32p)]  # fmt: skip
+
+
+class LumenSource(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("n_events", ctypes.c_int32), ("ev_f", c_f32p), ("ev_first", c_i64p),
+                ("ev_w", c_f32p), ("lam0", ctypes.c_float), ("lam1", ctypes.c_float), ("cone_cos", ctypes.c_float),
+                ("tau1", ctypes.c_float), ("tau2", ctypes.c_float), ("frac1", ctypes.c_float)]  # fmt: skip
+
+
+class LumenControls(ctypes.Structure):
+    _fields_ = [("max_distance", ctypes.c_float), ("roulette", ctypes.c_float), ("max_vertices", ctypes.c_int32),
+                ("n_grad", ctypes.c_int32), ("grad_tab", ctypes.c_int32 * MAX_GRAD),
+                ("step_budget", ctypes.c_int64)]  # fmt: skip
+
+
+class LumenTallies(ctypes.Structure):
+    _fields_ = [("n_events", ctypes.c_int32), ("n_bins", ctypes.c_int32), ("bin0", ctypes.c_float),
+                ("bin_w", ctypes.c_float), ("arrival", c_f64p), ("arrival_t", c_f64p), ("arrival2", c_f64p),
+                ("hist", c_f64p), ("jac", c_f64p), ("health", c_f64p), ("counts", c_u64p)]  # fmt: skip
+
+
+def iptr(a):
+    return a.ctypes.data_as(c_i32p) if a is not None and a.size else ctypes.cast(None, c_i32p)
+
+
+def fptr(a):
+    return a.ctypes.data_as(c_f32p) if a is not None and a.size else ctypes.cast(None, c_f32p)
+
+
+def dptr(a):
+    return a.ctypes.data_as(c_f64p) if a is not None and a.size else ctypes.cast(None, c_f64p)
+
+
+def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=(), step_budget=0):
+    c = LumenControls()
+    c.max_distance = float(max_distance)
+    c.roulette = float(roulette)
+    c.max_vertices = int(max_vertices)
+    if len(grad_tabs) > MAX_GRAD:
+        raise ValueError(f"at most {MAX_GRAD} gradient parameters")
+    c.n_grad = len(grad_tabs)
+    for i, t in enumerate(grad_tabs):
+        c.grad_tab[i] = int(t)
+    c.step_budget = int(step_budget)
+    return c
+
+
+ENTRY_POINTS = ("lumen_b200_abi_version", "lumen_b200_last_error", "lumen_b200_scene_create",
+                "lumen_b200_scene_set_pools", "lumen_b200_scene_destroy", "lumen_b200_trace", "lumen_b200_adjoint",
+                "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate")  # fmt: skip
+
+_lib = None
+
+
+def engine():
+    """Return the loaded engine library (ctypes); raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError(f"the CUDA engine {LIB} is not built: run `python -c 'import __graft_entry__ as g; "
+                               "g.build()'` (there is no CPU fallback)")  # fmt: skip
+        lib = ctypes.CDLL(LIB)
+        vp = ctypes.c_void_p
+        lib.lumen_b200_abi_version.restype = ctypes.c_int32
+        lib.lumen_b200_last_error.restype = ctypes.c_char_p
+        lib.lumen_b200_scene_create.argtypes = [ctypes.POINTER(LumenSceneDesc), ctypes.POINTER(vp)]
+        lib.lumen_b200_scene_set_pools.argtypes = [vp, c_f32p, c_f32p]
+        lib.lumen_b200_scene_destroy.argtypes = [vp]
+        lib.lumen_b200_trace.argtypes = [vp, ctypes.POINTER(LumenRows), ctypes.POINTER(LumenSource), ctypes.c_uint32,
+                                         ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
+                                         ctypes.POINTER(LumenControls), ctypes.POINTER(LumenTallies), vp]  # fmt: skip
+        lib.lumen_b200_adjoint.argtypes = [vp, ctypes.POINTER(LumenRows), ctypes.POINTER(LumenSource),
+                                           ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
+                                           ctypes.POINTER(LumenControls), c_f64p, ctypes.c_int32, c_f64p, vp]  # fmt: skip
+        lib.lumen_b200_trace_photons.argtypes = [vp, ctypes.POINTER(LumenRows), ctypes.POINTER(LumenSource),
+                                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
+                                                 ctypes.POINTER(LumenControls), c_i32p, c_f32p, vp]  # fmt: skip
+        lib.lumen_b200_query.argtypes = [vp, c_f32p, c_i32p, c_i32p, ctypes.c_float, ctypes.c_int64, c_i32p, c_f32p,
+                                         vp]  # fmt: skip
+        lib.lumen_b200_locate.argtypes = [vp, c_f32p, ctypes.c_int64, c_i32p, vp]
+        for name in ENTRY_POINTS[2:]:
+            getattr(lib, name).restype = ctypes.c_int32
+        _lib = lib
+    return _lib
+
+
+def check(status: int):
+    """Raise the engine's error for a non-zero status."""
+    if status != 0:
+        msg = engine().lumen_b200_last_error().decode(errors="replace")
+        raise RuntimeError(f"lumen_b200 status {status}: {msg}")
+
+
+def key_of_seed(seed: int):
+    """Return jax.random.PRNGKey(seed)'s key data for a 32-bit seed: (0, seed) (threefry_seed)."""
+    s = int(seed)
+    return (s >> 32) & 0xFFFFFFFF, s & 0xFFFFFFFF
+
+
+def np_f32(a):
+    return np.ascontiguousarray(a, np.float32)

@@ -1,0 +1,208 @@
+"""A built detector: geometry + optics flattened into the arrays of the C ABI, with its parameters by name.
+
+``Detector`` mirrors what the reference's ``lumen.load`` gives (src/lumen/api.py:70 ``Detector``, ``params()``,
+``sensor_table()``): the navigator arrays, the optics tables and the packed parameter values. The class rule follows
+the reference's surface lookup (src/lumen/build/lookup.py:394 Optics: a class per placed volume's optical role, a row
+per crossed class pair, a medium per class) and src/lumen/build/tracked.py:181 (sensor per volume).
+
+    det = build(top, materials, borders=[...], skins={...}, sensors={"pmt": "PMT"})
+    det.params()["media/Water/absorption"]      # a table (energies, values)
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from lumen_b200 import geometry as G
+from lumen_b200 import optics as O
+
+OUTSIDE = "OUT"
+
+
+@dataclass
+class SensorTable:
+    """The sensors in the order of ``Light.arrivals`` (src/lumen/api.py:498 SensorTable)."""
+
+    name: list
+    group: list
+    position: np.ndarray
+    axis: np.ndarray
+
+
+@dataclass
+class Detector:
+    """The flattened detector (see the module docstring)."""
+
+    arrays: dict
+    pool: np.ndarray
+    params_index: dict  # parameter name -> table index
+    sensors: SensorTable
+    names: list
+    classes: dict = field(default_factory=dict)
+    groups: dict = field(default_factory=dict)  # sensor group -> sensor indices
+
+    @property
+    def n_sensor(self) -> int:
+        return len(self.sensors.name)
+
+    def params(self) -> dict:
+        """Return {name: (energies, values)} of every parameter table (src/lumen/api.py:70 Detector.params)."""
+        out = {}
+        for k, t in self.params_index.items():
+            off, n = self.arrays["tab"][t]
+            out[k] = (self.pool[off:off + n].copy(), self.pool[off + n:off + 2 * n].copy())
+        return out
+
+    def pool_with(self, values: dict | None) -> np.ndarray:
+        """Return the pool with some parameters replaced: {name: constant or values array (same knots)}."""
+        p = self.pool.copy()
+        for k, v in (values or {}).items():
+            t = self.params_index[k]
+            off, n = self.arrays["tab"][t]
+            p[off + n:off + 2 * n] = np.broadcast_to(np.asarray(v, np.float32), (n,))
+        return p
+
+    def sensor_table(self) -> SensorTable:
+        return self.sensors
+
+    # ------------------------------------------------------------------------------------ the C ABI's descriptor
+    def desc(self):
+        """Return (LumenSceneDesc, keepalive) over this detector's arrays (host pointers)."""
+        from lumen_b200._abi import LumenSceneDesc, iptr, fptr
+
+        a = self.arrays
+        keep = {k: np.ascontiguousarray(v) for k, v in a.items() if isinstance(v, np.ndarray)}
+        keep["pool"] = np.ascontiguousarray(self.pool, np.float32)
+        d = LumenSceneDesc()
+        d.n_vol, d.n_kind, d.n_leaf = a["n_vol"], len(keep["kind_i"]), len(keep["leaf_i"])
+        d.n_plane, d.n_prog, d.n_node = len(keep["plane_f"]), len(keep["prog_i"]), len(keep["node_i"])
+        d.n_item, d.n_cand = len(keep["items"]), len(keep["cand"])
+        d.vol_i, d.vol_f, d.cand = iptr(keep["vol_i"]), fptr(keep["vol_f"]), iptr(keep["cand"])
+        d.node_f, d.node_i, d.items = fptr(keep["node_f"]), iptr(keep["node_i"]), iptr(keep["items"])
+        d.kind_i, d.leaf_f, d.leaf_i = iptr(keep["kind_i"]), fptr(keep["leaf_f"]), iptr(keep["leaf_i"])
+        d.plane_f, d.prog_i = fptr(keep["plane_f"]), iptr(keep["prog_i"])
+        d.reach = ctypes.c_float(a["reach"])
+        d.n_cls, d.n_med, d.n_row = a["n_cls"], len(keep["med_i"]), len(keep["row_i"])
+        d.n_tab, d.n_pool, d.n_sensor = len(keep["tab"]), len(keep["pool"]), self.n_sensor
+        d.cls_medium, d.row_of, d.med_i = iptr(keep["cls_medium"]), iptr(keep["row_of"]), iptr(keep["med_i"])
+        d.row_i, d.tab, d.pool = iptr(keep["row_i"]), iptr(keep["tab"]), fptr(keep["pool"])
+        return d, keep
+
+
+def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None) -> Detector:
+    """Return the Detector of the volume tree ``top`` (the detector volume, placed at the origin).
+
+    ``materials``: {name: Material}. ``borders``: [(pv from, pv to, OpticalSurface)] (Geant4 border surfaces, ordered);
+    ``skins``: {lv name: OpticalSurface}. ``sensors``: {group: lv name}: every placement of that logical volume is a
+    sensor, counted where a crossing's surface into it deposits (the ``border_into`` rule). Light that leaves ``top``
+    is absorbed there (the detector volume's boundary, as the reference's recipe ``detector_volume``).
+    """
+    skins = skins or {}
+    sensors = sensors or {}
+    placed = G.flatten(top)
+    names = [p.name for p in placed]
+    by_name = {p.name: i for i, p in enumerate(placed)}
+    # optical roles -> classes (the outside is class 0's neighbour: its own class)
+    roles = [set() for _ in placed]
+    for a, b, s in borders:
+        roles[by_name[a]].add((s.name, "from"))
+        roles[by_name[b]].add((s.name, "to"))
+    sensor_lv = {lv: g for g, lv in sensors.items()}
+    keys = []
+    for i, p in enumerate(placed):
+        keys.append((p.lv.name, p.lv.material, tuple(sorted(roles[i])), p.lv.name in skins, p.lv.name in sensor_lv))
+    cls_of_key, vol_cls, cls_lv, cls_mat = {}, [], [], []
+    for i, k in enumerate(keys):
+        if k not in cls_of_key:
+            cls_of_key[k] = len(cls_of_key)
+            cls_lv.append(placed[i].lv)
+            cls_mat.append(placed[i].lv.material)
+        vol_cls.append(cls_of_key[k])
+    out_cls = len(cls_of_key)
+    n_cls = out_cls + 1
+    # sensors: every placement of a sensor LV, in the walk's order
+    vol_sensor = np.full(len(placed), -1, np.int32)
+    s_name, s_group, s_pos, s_axis, groups = [], [], [], [], {}
+    for i, p in enumerate(placed):
+        g = sensor_lv.get(p.lv.name)
+        if g is not None:
+            vol_sensor[i] = len(s_name)
+            groups.setdefault(g, []).append(len(s_name))
+            s_name.append(p.name)
+            s_group.append(g)
+            s_pos.append(p.t)
+            s_axis.append(p.R[:, 2])
+    nav = G.navigator_arrays(placed, vol_cls, out_cls, vol_sensor, prio)
+    # media
+    pool = O.Pool()
+    med_names = sorted(set(cls_mat))
+    med_i = np.full((len(med_names), 4), -1, np.int32)
+    opaque = {}
+    for m, name in enumerate(med_names):
+        mat = materials[name]
+        opaque[name] = mat.rindex is None
+        if mat.rindex is not None:
+            med_i[m, 0] = pool.add(mat.rindex, f"media/{name}/index")
+        if mat.abslength is not None:
+            med_i[m, 1] = pool.add(mat.abslength, f"media/{name}/absorption")
+        ray = mat.rayleigh
+        if ray is None and name.split("0x")[0] == "Water" and mat.rindex is not None:
+            ray = O.water_rayleigh(O.table(mat.rindex))
+        if ray is not None and mat.rindex is not None:
+            med_i[m, 2] = pool.add(ray, f"media/{name}/rayleigh")
+    mi_of = {n: i for i, n in enumerate(med_names)}
+    cls_medium = np.asarray([mi_of[m] for m in cls_mat] + [mi_of[cls_mat[0]] if cls_mat else 0], np.int32)
+    # surface rows per crossed class pair
+    neutral = {c: pool.add(v) for c, v in O.NEUTRAL.items()}
+    rows, row_key, row_of = [], {}, np.full((n_cls, n_cls), -1, np.int32)
+    border_of = {}
+    for a, b, s in borders:
+        border_of[(vol_cls[by_name[a]], vol_cls[by_name[b]])] = s
+    for ca in range(n_cls):
+        for cb in range(n_cls):
+            if ca == cb:
+                continue
+            into_out = cb == out_cls
+            from_out = ca == out_cls
+            far_opq = into_out or opaque[cls_mat[cb]]
+            surf = border_of.get((ca, cb))
+            if surf is None and not from_out and cls_lv[ca].name in skins:
+                surf = skins[cls_lv[ca].name]
+            if surf is None and not into_out and cls_lv[cb].name in skins:
+                surf = skins[cls_lv[cb].name]
+            is_sensor = (not into_out) and cls_lv[cb].name in sensor_lv
+            if surf is None:
+                if into_out or from_out or opaque[cls_mat[cb]] or opaque[cls_mat[ca]]:
+                    surf = O.ABSORBER  # the detector volume's boundary; Geant4's NoRINDEX
+                else:
+                    surf = O.OpticalSurface("__fresnel__", "dielectric_dielectric", "polished")
+            key = (surf.name, is_sensor, far_opq, id(surf))
+            if key not in row_key:
+                row = O.surface_row(surf, is_sensor, far_opq)
+                row.sensor = is_sensor
+                row_key[key] = len(rows)
+                rows.append(row)
+            row_of[ca, cb] = row_key[key]
+    row_i = np.zeros((len(rows), 16), np.int32)
+    col_tab = {}  # one table per (surface, column): every row of a surface reads (and moves with) the same values
+    for r, row in enumerate(rows):
+        row_i[r, 0:4] = [row.model, row.normal, row.glisur, row.far_opaque]
+        for c, col in enumerate(O.COLUMNS):
+            if col not in row.cols or (col == "eff" and not row.sensor):
+                row_i[r, 6 + c] = neutral[col]
+                continue
+            k = (row.name, col)
+            if k not in col_tab:
+                col_tab[k] = pool.add(row.cols[col], None if row.name.startswith("__") else f"surfaces/{row.name}/{col}")
+            row_i[r, 6 + c] = col_tab[k]
+    params_index = dict(pool.names)
+    tab, data = pool.arrays()
+    arrays = dict(nav)
+    arrays.update(n_cls=n_cls, cls_medium=cls_medium, row_of=row_of.ravel().astype(np.int32), med_i=med_i,
+                  row_i=row_i, tab=tab)  # fmt: skip
+    st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
+    cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}
+    return Detector(arrays, data, params_index, st, names, cls_names, groups)

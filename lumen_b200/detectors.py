@@ -1,0 +1,148 @@
+"""The detectors of the benchmark and test workloads, built with ``lumen_b200.detector.build``.
+
+- ``toy_tank()``: lumen's tutorial detector (examples/data/example_tank.gdml and examples/example_tank.py:21-35 of the
+  reference): a 1 m cube of water (tabulated RINDEX and ABSLENGTH; Geant4's water Rayleigh table from RINDEX), 8 disc
+  PMTs (radius 50 mm, 20 mm thick) behind a dielectric_metal cathode border (REFLECTIVITY 0, EFFICIENCY 1); light that
+  leaves the water is absorbed.
+- ``cylinder_tank()``: a water cylinder (radius 5 m, height 10 m) with 2000 inward-facing hemispherical PMTs (radius
+  0.1 m) on a regular barrel and end-cap grid, black-sheet walls of reflectivity 0.1; water with absorption length
+  50 m, Rayleigh length 80 m and a flat index of 1.34.
+- ``lar_box()``: a 5 x 4 x 4 m liquid-argon box (index 1.38, Rayleigh 0.9 m, absorption 20 m) with a CSG cathode
+  (a plate with a cut-out window, a box subtraction) and a field cage (a box shell with a union of two rails: box
+  subtractions and unions) of reflectivity 0.9, and 120 flat discs (20 cm diameter) on one wall.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from lumen_b200 import detector as D
+from lumen_b200 import geometry as G
+from lumen_b200 import optics as O
+
+MM = 1e-3
+
+
+def toy_tank() -> D.Detector:
+    """Return the tutorial tank (values of examples/data/example_tank.gdml in the reference)."""
+    water = O.Material("Water", rindex=([1.5, 2.5, 3.5, 5.0], [1.332, 1.336, 1.345, 1.366]),
+                       abslength=([1.5, 2.5, 3.0, 3.5, 5.0], [5.0, 40.0, 60.0, 30.0, 2.0]))  # fmt: skip
+    cathode = O.Material("Photocathode")
+    pmt = G.Volume("PMT", G.Tube(rmax=50 * MM, dz=10 * MM), "Photocathode")
+    tank = G.Volume("TankLV", G.Box(0.5, 0.5, 0.5), "Water")
+    places = [((0, 0, -480), None), ((0, 0, 480), None), ((-480, 0, 0), ("y", 90)), ((480, 0, 0), ("y", 90)),
+              ((0, -480, 0), ("x", 90)), ((0, 480, 0), ("x", 90)), ((-250, 0, -480), None), ((250, 0, -480), None)]
+    for i, (p, r) in enumerate(places):
+        rot = None if r is None else G.gdml_rotation(**{r[0]: r[1]})
+        tank.place(pmt, np.asarray(p, float) * MM, rot, name=f"PMT_{i}", copy=i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    borders = [("TankLV", f"PMT_{i}", surf) for i in range(8)]
+    return D.build(tank, {"Water": water, "Photocathode": cathode}, borders=borders, sensors={"pmt": "PMT"})
+
+
+def _grid_tank(n_pmt, radius, half_h, r_pmt, inset):
+    """Return (positions, inward axes) of n_pmt PMTs on a regular barrel and end-cap grid."""
+    area = 2 * math.pi * radius * 2 * half_h + 2 * math.pi * radius**2
+    s = math.sqrt(area / n_pmt)
+    while True:
+        n_phi = max(int(round(2 * math.pi * radius / s)), 1)
+        n_z = max(int(round(2 * half_h / s)), 1)
+        pos, ax = [], []
+        rr = radius - inset
+        for iz in range(n_z):
+            z = -half_h + (iz + 0.5) * (2 * half_h / n_z)
+            for ip in range(n_phi):
+                ph = 2 * math.pi * (ip + 0.5) / n_phi
+                c, si = math.cos(ph), math.sin(ph)
+                pos.append((rr * c, rr * si, z))
+                ax.append((-c, -si, 0.0))
+        cap = []
+        m = int(math.ceil(radius / s)) + 1
+        for i in range(-m, m + 1):
+            for j in range(-m, m + 1):
+                x, y = (i + 0.5) * s, (j + 0.5) * s
+                if math.hypot(x, y) + r_pmt < radius - 2 * r_pmt:
+                    cap.append((x, y))
+        cap.sort(key=lambda p: (math.hypot(*p), p))
+        need = n_pmt - len(pos)
+        if 0 <= need <= 2 * len(cap):
+            top = cap[: (need + 1) // 2]
+            bot = cap[: need // 2]
+            for x, y in top:
+                pos.append((x, y, half_h - inset))
+                ax.append((0.0, 0.0, -1.0))
+            for x, y in bot:
+                pos.append((x, y, -half_h + inset))
+                ax.append((0.0, 0.0, 1.0))
+            return np.asarray(pos), np.asarray(ax)
+        s *= 0.99 if need > 2 * len(cap) else 1.01
+
+
+def _frame_z(axis):
+    """Return a rotation whose local z is ``axis``."""
+    z = np.asarray(axis, float)
+    z = z / np.linalg.norm(z)
+    a = np.array([1.0, 0, 0]) if abs(z[0]) < 0.9 else np.array([0, 1.0, 0])
+    x = np.cross(a, z)
+    x /= np.linalg.norm(x)
+    y = np.cross(z, x)
+    return np.stack([x, y, z], 1)
+
+
+def cylinder_tank(n_pmt=2000, radius=5.0, half_h=5.0, r_pmt=0.1, wall_r=0.1, wall_finish="polished",
+                  sigma_alpha=0.0, abs_len=50.0, ray_len=80.0, rindex=1.34) -> D.Detector:
+    """Return the synthetic water tank of the plain-forward workload (see the module docstring)."""
+    water = O.Material("Water", rindex=rindex, abslength=abs_len, rayleigh=ray_len)
+    pmt = G.Volume("PMT", G.Sphere(r_pmt, hemisphere=+1), "Photocathode")
+    tank = G.Volume("Tank", G.Tube(rmax=radius, dz=half_h), "Water")
+    # the hemisphere's flat face 1.5 mm inside the wall: the disc's rim clears the curved barrel wall
+    pos, ax = _grid_tank(n_pmt, radius, half_h, r_pmt, inset=1.5 * MM)
+    for i in range(len(pos)):
+        tank.place(pmt, pos[i], _frame_z(ax[i]), name=f"PMT_{i}", copy=i)
+    cath = O.OpticalSurface("Cathode", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    if wall_finish == "polished":
+        wall = O.OpticalSurface("BlackSheet", "dielectric_metal", "polished", reflectivity=wall_r)
+    else:
+        wall = O.OpticalSurface("BlackSheet", "dielectric_metal", "ground", reflectivity=wall_r,
+                                sigma_alpha=sigma_alpha, specularlobe=1.0 if sigma_alpha > 0 else 0.0)  # fmt: skip
+    borders = [("Tank", f"PMT_{i}", cath) for i in range(len(pos))]
+    return D.build(tank, {"Water": water, "Photocathode": O.Material("Photocathode")}, borders=borders,
+                   skins={"Tank": wall}, sensors={"pmt": "PMT"})  # fmt: skip
+
+
+def lar_box(n_x=12, n_y=10, cage_r=0.9, sigma_alpha=0.0, ray_len=0.9, abs_len=20.0, rindex=1.38) -> D.Detector:
+    """Return the synthetic liquid-argon box of the scintillation workload (see the module docstring)."""
+    lar = O.Material("LAr", rindex=rindex, abslength=abs_len, rayleigh=ray_len)
+    steel = O.Material("Steel")
+    box = G.Volume("LArBox", G.Box(2.5, 2.0, 2.0), "LAr")
+    # field cage: a box shell 2 cm thick inside the walls, minus the sensor wall's face, plus two rails (union)
+    shell = G.Boolean("subtraction", G.Box(2.45, 1.95, 1.95), G.Box(2.43, 1.93, 1.93))
+    open_face = G.Boolean("subtraction", shell, G.Box(0.02, 1.94, 1.94), pos=(-2.44, 0.0, 0.0))
+    cage_solid = G.Boolean("union", open_face, G.Box(2.0, 0.02, 0.02), pos=(0.0, 1.9, 0.0))
+    cage = G.Volume("FieldCage", cage_solid, "Steel")
+    # cathode: a plate at x = +0.5 m with a window cut out (a box subtraction)
+    plate = G.Boolean("subtraction", G.Box(0.01, 1.5, 1.5), G.Box(0.02, 0.3, 0.3))
+    cathode = G.Volume("Cathode", plate, "Steel")
+    box.place(cage, (0.0, 0.0, 0.0), name="FieldCage")
+    box.place(cathode, (0.5, 0.0, 0.0), name="Cathode")
+    disc = G.Volume("Sensor", G.Tube(rmax=0.1, dz=0.005), "Steel")
+    rot = _frame_z((1.0, 0.0, 0.0))
+    k = 0
+    for iy in range(n_x):
+        for iz in range(n_y):
+            y = -1.65 + 3.3 * (iy + 0.5) / n_x
+            z = -1.6 + 3.2 * (iz + 0.5) / n_y
+            box.place(disc, (-2.49, y, z), rot, name=f"Sensor_{k}", copy=k)
+            k += 1
+    if sigma_alpha > 0.0:
+        refl = O.OpticalSurface("CageSurface", "dielectric_metal", "ground", reflectivity=cage_r,
+                                sigma_alpha=sigma_alpha, specularlobe=1.0)  # fmt: skip
+    else:
+        refl = O.OpticalSurface("CageSurface", "dielectric_metal", "ground", reflectivity=cage_r)
+    sens = O.OpticalSurface("SensorSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    borders = [("LArBox", f"Sensor_{i}", sens) for i in range(k)]
+    # the box's own walls absorb (the detector volume's boundary)
+    return D.build(box, {"LAr": lar, "Steel": steel}, borders=borders,
+                   skins={"FieldCage": refl, "Cathode": refl}, sensors={"sensor": "Sensor"})  # fmt: skip

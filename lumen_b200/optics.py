@@ -1,0 +1,151 @@
+"""Optics on the host: materials, optical surfaces, the surface lookup's classes and rows, and the parameter pool.
+
+The reference compiles a detector's optics into a class per placed volume, a surface row per crossed class pair
+(``row_of[C, C]``), a medium per class and packed parameter tables (src/lumen/build/lookup.py:360-500 SurfaceTable,
+Optics, pack; src/lumen/build/pack.py:84). This module builds the same structure for the C ABI
+(include/lumen_b200.h): every value a run reads is a table, linear in photon energy between its knots and held beyond
+(src/lumen/media/laws.py:86), stored in one float32 pool that a call may replace (live and reference values).
+
+Surface types follow Geant4's chain as the reference restates it (src/lumen/surfaces/types.py:445-493):
+``dielectric_metal`` polished = a specular metal (R into the spike), ground unified = the reflection constants
+(spike, lobe, backscatter, Lambertian), ``dielectric_dielectric`` polished = the Fresnel interface, and the absorber
+(nothing continues). A sensor's surface reads EFFICIENCY as its detected share; on any other surface it is fixed at 0
+(types.py:557 no_detection).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HC = 1239.8419843320025  # h c in eV nm (src/lumen/units.py:20)
+HC_EV_M = HC * 1e-9
+# G4OpRayleigh::CalculateRayleighMeanFreePaths for a material named "Water" (src/lumen/rules/optics.py:98-103)
+WATER_COMPRESSIBILITY = 7.658e-23  # m3 / MeV
+WATER_TEMPERATURE = 283.15  # K
+K_BOLTZMANN = 8.617333e-11  # MeV / K
+
+# the columns of a surface row and their neutral values (src/lumen/surfaces/types.py:72 COLUMNS)
+COLUMNS = ("R", "T", "eff", "p_spike", "p_lobe", "p_back", "sigma_alpha", "polish", "nr", "nk")
+NEUTRAL = {"R": 0.0, "T": 0.0, "eff": 0.0, "p_spike": 0.0, "p_lobe": 0.0, "p_back": 0.0, "sigma_alpha": 0.1,
+           "polish": 0.0, "nr": 1.0, "nk": 0.0}  # fmt: skip
+MODEL_REFLECT, MODEL_DIELECTRIC, MODEL_COMPLEX = 0, 1, 2
+
+
+def table(v, energy=None):
+    """Return a table (energies eV ascending, values) from a constant or from (energies, values)."""
+    if energy is None:
+        if isinstance(v, tuple) and len(v) == 2:
+            e, y = np.asarray(v[0], float), np.asarray(v[1], float)
+        else:
+            return np.array([1.0]), np.array([float(v)])
+    else:
+        e, y = np.asarray(energy, float), np.asarray(v, float)
+    o = np.argsort(e)
+    return e[o], y[o]
+
+
+def water_rayleigh(rindex):
+    """Return Geant4's Rayleigh-length table of water on the RINDEX knots (src/lumen/rules/optics.py:208-254)."""
+    e, n = rindex
+    c1 = WATER_COMPRESSIBILITY * WATER_TEMPERATURE * K_BOLTZMANN / (6.0 * math.pi)
+    e32, n32 = np.float32(e), np.float32(n)
+    k = np.float32(2.0 * math.pi / HC_EV_M) * e32
+    n2 = n32 * n32
+    L = np.float32(1.0) / (np.float32(c1) * k**4 * ((n2 - 1.0) * (n2 + 2.0) / np.float32(3.0)) ** 2)
+    return e, np.asarray(L, float)
+
+
+@dataclass
+class Material:
+    """A medium: RINDEX (None: opaque), ABSLENGTH (m, None: no absorption), RAYLEIGH (m; None: Geant4's water
+    table for a material named Water, else no scattering). Tables are (energies eV, values) or constants."""  # noqa: D205
+
+    name: str
+    rindex: object = None
+    abslength: object = None
+    rayleigh: object = None
+
+
+@dataclass
+class OpticalSurface:
+    """A Geant4 optical surface (G4OpticalSurface + its property table)."""
+
+    name: str
+    type: str = "dielectric_metal"  # or "dielectric_dielectric"
+    finish: str = "polished"  # or "ground"
+    model: str = "unified"
+    sigma_alpha: float = 0.0
+    reflectivity: object = None
+    efficiency: object = None
+    transmittance: object = None
+    specularspike: object = None
+    specularlobe: object = None
+    backscatter: object = None
+
+
+ABSORBER = OpticalSurface("__absorber__", "dielectric_metal", "polished", reflectivity=0.0)
+
+
+@dataclass
+class Row:
+    """One surface row: model, flags and a value per column."""
+
+    model: int
+    normal: int = 0
+    glisur: int = 0
+    far_opaque: int = 0
+    cols: dict = field(default_factory=dict)  # column -> table
+    name: str = ""
+    sensor: bool = False
+
+
+def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
+    """Return the row of a Geant4 surface (types.py:445-493 types, :557 no_detection)."""
+    eff = surf.efficiency if (sensor and surf.efficiency is not None) else 0.0
+    if surf.type == "dielectric_dielectric":
+        if surf.finish != "polished":
+            raise NotImplementedError("dielectric_dielectric ground (GLISUR / unified facets) is not built")
+        cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
+                "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff}  # fmt: skip
+        return Row(MODEL_DIELECTRIC, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+    # dielectric_metal
+    R = 1.0 if surf.reflectivity is None else surf.reflectivity
+    cols = {"R": R, "eff": eff, "T": 0.0 if surf.transmittance is None else surf.transmittance}
+    if surf.finish == "polished" or surf.model == "glisur":
+        cols["p_spike"] = 1.0  # polished: the mirror (types.py:573 SPECULAR_METAL)
+        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+    ss = 0.0 if surf.specularspike is None else surf.specularspike
+    sl = 0.0 if surf.specularlobe is None else surf.specularlobe
+    bs = 0.0 if surf.backscatter is None else surf.backscatter
+    cols.update({"p_spike": ss, "p_lobe": sl, "p_back": bs, "sigma_alpha": surf.sigma_alpha})
+    lobe_on = not (isinstance(sl, (int, float)) and sl == 0.0)
+    normal = int(surf.sigma_alpha == 0.0)
+    if lobe_on and not normal:
+        raise NotImplementedError("the unified facet lobe (GLOSSY with sigma_alpha > 0) is not built")
+    return Row(MODEL_REFLECT, normal=normal, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+
+
+class Pool:
+    """The parameter pool: every table's knots and values in one float32 array (include/lumen_b200.h tables)."""
+
+    def __init__(self):
+        self.tabs = []  # (offset, k)
+        self.data = []
+        self.names = {}
+
+    def add(self, tab, name=None) -> int:
+        e, y = table(tab)
+        k = len(e)
+        self.tabs.append((len(self.data), k))
+        self.data.extend(np.float32(e).tolist())
+        self.data.extend(np.float32(y).tolist())
+        t = len(self.tabs) - 1
+        if name is not None:
+            self.names[name] = t
+        return t
+
+    def arrays(self):
+        return np.asarray(self.tabs, np.int32).reshape(-1, 2), np.asarray(self.data, np.float32)

@@ -1,0 +1,187 @@
+"""Photon sources: emission rows drawn on the device from each photon's own key.
+
+Mirrors ``lumen.sources`` (src/lumen/sources/point.py:37 ``Point``, _base.py:312 ``photon_uniforms``, :318
+``gaussian``): photon i of a run takes its uniforms from vertex 0 of ``fold_in(fold_in(key, SOURCE_STREAM), i)`` and a
+point source draws an isotropic direction as a normalised Gaussian triple; a source stands for ``n_photons`` physical
+photons shared by the run's samples (row weight n_photons / samples). Events: a source with several events (a batch)
+assigns photon ids to events by contiguous ranges of uneven sizes (``counts``), every photon tallied into its event.
+
+- ``Point(position, n_photons, lam | lam_range, time)``: isotropic points, one per event.
+- ``Tracks(start, direction, length, cone_angle, ...)``: straight tracks emitting on a cone of fixed half-angle about
+  their direction (a Cherenkov-like source; linear polarisation in the plane of track and photon, polar.py:89).
+- ``Scintillation(position, tau=(tau1, tau2), fraction)``: isotropic points with a two-exponential time profile.
+- ``FromArrays(x, d, t, lam, w, pol)``: explicit rows (src/lumen/sources/arrays.py:24).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from lumen_b200 import _abi as A
+
+
+def _events(v, n_ev, width):
+    a = np.asarray(v, np.float32)
+    return np.broadcast_to(a, (n_ev, width)) if a.ndim <= 1 else a
+
+
+@dataclass
+class Source:
+    """Base: ``arrays()`` gives the LumenSource layout (kind, per-event records, event ranges and row weights)."""
+
+    def events(self) -> int:
+        return 1
+
+    def counts(self, samples: int) -> np.ndarray:
+        """Return the photons of each event in a run of ``samples`` photons."""
+        return np.asarray([samples], np.int64)
+
+
+@dataclass
+class Point(Source):
+    """Isotropic points (src/lumen/sources/point.py:37): ``position`` (3,) or (E, 3) m, one event each."""
+
+    position: object
+    n_photons: object = 1.0
+    lam: float | None = None
+    lam_range: tuple | None = None
+    time: object = 0.0
+    counts_: object = None
+
+    def events(self):
+        p = np.asarray(self.position, np.float32)
+        return 1 if p.ndim == 1 else len(p)
+
+    def counts(self, samples):
+        if self.counts_ is not None:
+            return np.asarray(self.counts_, np.int64)
+        e = self.events()
+        base = np.full(e, samples // e, np.int64)
+        base[: samples - base.sum()] += 1
+        return base
+
+    def arrays(self, samples):
+        e = self.events()
+        pos = _events(self.position, e, 3)
+        ev_f = np.zeros((e, A.EV_F), np.float32)
+        ev_f[:, 0:3] = pos
+        ev_f[:, 3] = np.broadcast_to(np.asarray(self.time, np.float32), (e,))
+        cnt = self.counts(samples)
+        return _common(self, A.SRC_POINT, ev_f, cnt, self.n_photons)
+
+
+@dataclass
+class Tracks(Source):
+    """Straight tracks emitting on a cone about their direction, one event per track."""
+
+    start: object
+    direction: object
+    length: object
+    cone_angle: float = math.radians(42.0)
+    n_photons: object = 1.0
+    lam: float | None = None
+    lam_range: tuple | None = None
+    time: object = 0.0
+    counts_: object = None
+
+    def events(self):
+        return len(np.asarray(self.start, np.float32).reshape(-1, 3))
+
+    def counts(self, samples):
+        if self.counts_ is not None:
+            return np.asarray(self.counts_, np.int64)
+        e = self.events()
+        base = np.full(e, samples // e, np.int64)
+        base[: samples - base.sum()] += 1
+        return base
+
+    def arrays(self, samples):
+        e = self.events()
+        ev_f = np.zeros((e, A.EV_F), np.float32)
+        ev_f[:, 0:3] = _events(self.start, e, 3)
+        u = np.asarray(_events(self.direction, e, 3), np.float64)
+        ev_f[:, 3:6] = u / np.linalg.norm(u, axis=1, keepdims=True)
+        ev_f[:, 6] = np.broadcast_to(np.asarray(self.length, np.float32), (e,))
+        ev_f[:, 7] = np.broadcast_to(np.asarray(self.time, np.float32), (e,))
+        out = _common(self, A.SRC_TRACK, ev_f, self.counts(samples), self.n_photons)
+        out["cone_cos"] = float(np.float32(math.cos(self.cone_angle)))
+        return out
+
+
+@dataclass
+class Scintillation(Source):
+    """Isotropic scintillation points with a two-exponential time profile, one event per point."""
+
+    position: object
+    tau: tuple = (6.0, 1500.0)
+    fraction: float = 0.25
+    n_photons: object = 1.0
+    lam: float | None = None
+    lam_range: tuple | None = None
+    time: object = 0.0
+    counts_: object = None
+
+    def events(self):
+        return len(np.asarray(self.position, np.float32).reshape(-1, 3))
+
+    def counts(self, samples):
+        if self.counts_ is not None:
+            return np.asarray(self.counts_, np.int64)
+        e = self.events()
+        base = np.full(e, samples // e, np.int64)
+        base[: samples - base.sum()] += 1
+        return base
+
+    def arrays(self, samples):
+        e = self.events()
+        ev_f = np.zeros((e, A.EV_F), np.float32)
+        ev_f[:, 0:3] = _events(self.position, e, 3)
+        ev_f[:, 3] = np.broadcast_to(np.asarray(self.time, np.float32), (e,))
+        out = _common(self, A.SRC_SCINT, ev_f, self.counts(samples), self.n_photons)
+        out.update(tau1=float(self.tau[0]), tau2=float(self.tau[1]), frac1=float(self.fraction))
+        return out
+
+
+def _common(src, kind, ev_f, cnt, n_photons):
+    e = len(cnt)
+    first = np.zeros(e + 1, np.int64)
+    first[1:] = np.cumsum(cnt)
+    nph = np.broadcast_to(np.asarray(n_photons, np.float64), (e,))
+    ev_w = np.where(cnt > 0, nph / np.maximum(cnt, 1), 0.0).astype(np.float32)
+    if src.lam is not None:
+        lam0, lam1 = float(src.lam), 0.0
+    elif src.lam_range is not None:
+        lam0, lam1 = float(src.lam_range[0]), float(src.lam_range[1])
+    else:
+        raise ValueError("a source needs lam or lam_range")
+    return dict(kind=kind, ev_f=ev_f, ev_first=first, ev_w=ev_w, lam0=lam0, lam1=lam1, cone_cos=1.0, tau1=0.0,
+                tau2=0.0, frac1=0.0)  # fmt: skip
+
+
+@dataclass
+class FromArrays(Source):
+    """Explicit emission rows (src/lumen/sources/arrays.py:24): x (n, 3), d (n, 3), t, lam, w (n,), pol (n, 2, 3)."""
+
+    x: object
+    d: object
+    t: object = 0.0
+    lam: object = 400.0
+    w: object = 1.0
+    pol: object = None
+    event: object = None
+
+    def rows(self):
+        x = np.asarray(self.x, np.float32).reshape(-1, 3)
+        n = len(x)
+        d = np.asarray(self.d, np.float32).reshape(-1, 3)
+        return dict(x=x, d=d, t=np.broadcast_to(np.float32(self.t), (n,)).copy(),
+                    lam=np.broadcast_to(np.asarray(self.lam, np.float32), (n,)).copy(),
+                    w=np.broadcast_to(np.asarray(self.w, np.float32), (n,)).copy(),
+                    pol=None if self.pol is None else np.asarray(self.pol, np.float32).reshape(-1, 6),
+                    event=None if self.event is None else np.asarray(self.event, np.int32))  # fmt: skip
+
+    def events(self):
+        return 1 if self.event is None else int(np.max(self.event)) + 1

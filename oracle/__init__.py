@@ -1,0 +1,202 @@
+"""ORACLE (test infrastructure): ctypes access to the CPU restatement in ``oracle/liblumen_oracle.so``.
+
+Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline import this package, and only as the checker
+(or the timed CPU baseline). The product path (``lumen_b200``) never does.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from lumen_b200 import _abi as A
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liblumen_oracle.so")
+_lib = None
+
+
+def build():
+    """Compile the restatement (make)."""
+    subprocess.run(["make", "-C", HERE, "-s"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        vp = ctypes.c_void_p
+        P = ctypes.POINTER
+        L.lumen_oracle_trace.argtypes = [P(A.LumenSceneDesc), A.c_f32p, A.c_f32p, P(A.LumenRows), P(A.LumenSource),
+                                         ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
+                                         P(A.LumenControls), P(A.LumenTallies), A.c_i32p, A.c_f32p, ctypes.c_int32]
+        L.lumen_oracle_query.argtypes = [P(A.LumenSceneDesc), A.c_f32p, A.c_i32p, A.c_i32p, ctypes.c_float,
+                                         ctypes.c_int64, A.c_i32p, A.c_f32p]
+        L.lumen_oracle_locate.argtypes = [P(A.LumenSceneDesc), A.c_f32p, ctypes.c_int64, A.c_i32p]
+        L.lumen_oracle_uniforms.argtypes = [ctypes.c_uint32, ctypes.c_uint32, A.c_i64p, ctypes.c_int64,
+                                            ctypes.c_int32, ctypes.c_int32, A.c_f32p]
+        L.lumen_oracle_threefry.argtypes = [ctypes.c_uint32] * 4 + [P(ctypes.c_uint32)]
+        L.lumen_oracle_math.argtypes = [ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_fresnel.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_basis.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_source_rows.argtypes = [P(A.LumenSource), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
+                                               ctypes.c_int64, A.c_f32p, A.c_i32p]
+        del vp
+        _lib = L
+    return _lib
+
+
+def threefry(k0, k1, x0, x1):
+    out = (ctypes.c_uint32 * 2)()
+    lib().lumen_oracle_threefry(k0, k1, x0, x1, out)
+    return int(out[0]), int(out[1])
+
+
+def uniforms(key, ids, vertex, n):
+    ids = np.ascontiguousarray(ids, np.int64)
+    out = np.zeros((len(ids), n), np.float32)
+    lib().lumen_oracle_uniforms(key[0], key[1], ids.ctypes.data_as(A.c_i64p), len(ids), vertex, n, A.fptr(out))
+    return out
+
+
+MATH = {"exp": 0, "log": 1, "sin2pi": 2, "cos2pi": 3, "acos": 4, "cbrt": 5, "erfinv": 6, "sin": 7, "cos": 8,
+        "dipole_cos": 9, "gaussian": 10}  # fmt: skip
+
+
+def math(fn, x):
+    x = A.np_f32(x)
+    out = np.zeros_like(x)
+    A.check(0) if False else None
+    st = lib().lumen_oracle_math(MATH[fn], A.fptr(x), x.size, A.fptr(out))
+    assert st == 0
+    return out
+
+
+def fresnel(cos_i, n1, n2re, n2im):
+    b = np.broadcast_arrays(*(np.asarray(v, np.float32) for v in (cos_i, n1, n2re, n2im)))
+    inp = np.ascontiguousarray(np.stack([v.ravel() for v in b], 1), np.float32)
+    out = np.zeros((len(inp), 8), np.float32)
+    lib().lumen_oracle_fresnel(A.fptr(inp), len(inp), A.fptr(out))
+    return out
+
+
+def basis(n):
+    n = A.np_f32(n).reshape(-1, 3)
+    out = np.zeros((len(n), 6), np.float32)
+    lib().lumen_oracle_basis(A.fptr(n), len(n), A.fptr(out))
+    return out[:, :3], out[:, 3:]
+
+
+def locate(det, pts):
+    d, keep = det.desc()
+    pts = A.np_f32(pts).reshape(-1, 3)
+    vol = np.zeros(len(pts), np.int32)
+    st = lib().lumen_oracle_locate(ctypes.byref(d), A.fptr(pts), len(pts), A.iptr(vol))
+    assert st == 0, st
+    return vol
+
+
+def query(det, o, dvec, vol=None, srf=None, t_max=None):
+    """The navigator query per ray (the layout of lumen_b200_query): (out_i (n, 8), out_f (n, 4))."""
+    d, keep = det.desc()
+    o, dvec = A.np_f32(o).reshape(-1, 3), A.np_f32(dvec).reshape(-1, 3)
+    n = len(o)
+    ray = np.ascontiguousarray(np.concatenate([o, dvec], 1), np.float32)
+    vol = np.full(n, -1, np.int32) if vol is None else np.ascontiguousarray(vol, np.int32)
+    srf = np.full(n, -1, np.int32) if srf is None else np.ascontiguousarray(srf, np.int32)
+    out_i = np.zeros((n, 8), np.int32)
+    out_f = np.zeros((n, 4), np.float32)
+    tm = det.arrays["reach"] if t_max is None else t_max
+    st = lib().lumen_oracle_query(ctypes.byref(d), A.fptr(ray), A.iptr(vol), A.iptr(srf), ctypes.c_float(tm), n,
+                                  A.iptr(out_i), A.fptr(out_f))  # fmt: skip
+    assert st == 0, st
+    return out_i, out_f
+
+
+class Tallies:
+    """Host FP64 tallies in the LumenTallies layout."""
+
+    def __init__(self, n_sensor, n_events=1, n_bins=0, bin0=0.0, bin_w=1.0, n_grad=0):
+        S, E = max(n_sensor, 1), max(n_events, 1)
+        self.arrival = np.zeros((E, S))
+        self.arrival_t = np.zeros((E, S))
+        self.arrival2 = np.zeros((E, S))
+        self.hist = np.zeros((E, S, n_bins)) if n_bins else None
+        self.jac = np.zeros((E, S, n_grad)) if n_grad else None
+        self.health = np.zeros(A.N_HEALTH)
+        self.counts = np.zeros(A.N_COUNT, np.uint64)
+        t = A.LumenTallies()
+        t.n_events, t.n_bins, t.bin0, t.bin_w = E, n_bins, bin0, bin_w
+        t.arrival, t.arrival_t, t.arrival2 = A.dptr(self.arrival), A.dptr(self.arrival_t), A.dptr(self.arrival2)
+        t.hist = A.dptr(self.hist)
+        t.jac = A.dptr(self.jac)
+        t.health = A.dptr(self.health)
+        t.counts = self.counts.ctypes.data_as(A.c_u64p)
+        self.c = t
+
+
+def host_rows(rows: dict):
+    """Return (LumenRows over host arrays, keepalive) of a dict of row arrays (x (n,3), d (n,3), t, lam, w, pol?)."""
+    keep = {}
+    x, d = A.np_f32(rows["x"]).reshape(-1, 3), A.np_f32(rows["d"]).reshape(-1, 3)
+    for i, k in enumerate("xyz"):
+        keep[k] = np.ascontiguousarray(x[:, i])
+        keep["d" + k] = np.ascontiguousarray(d[:, i])
+    for k in ("t", "lam", "w"):
+        keep[k] = A.np_f32(rows[k])
+    r = A.LumenRows()
+    for k in ("x", "y", "z", "dx", "dy", "dz", "t", "lam", "w"):
+        setattr(r, k, A.fptr(keep[k]))
+    if rows.get("pol") is not None:
+        keep["pol"] = A.np_f32(rows["pol"]).reshape(-1, 6)
+        r.pol = A.fptr(keep["pol"])
+    if rows.get("event") is not None:
+        keep["event"] = np.ascontiguousarray(rows["event"], np.int32)
+        r.event = A.iptr(keep["event"])
+    return r, keep
+
+
+def host_source(src, samples):
+    """Return (LumenSource over host arrays, keepalive) of a lumen_b200.sources.Source's arrays."""
+    a = src.arrays(samples)
+    keep = {"ev_f": A.np_f32(a["ev_f"]), "ev_first": np.ascontiguousarray(a["ev_first"], np.int64),
+            "ev_w": A.np_f32(a["ev_w"])}  # fmt: skip
+    s = A.LumenSource()
+    s.kind, s.n_events = a["kind"], len(keep["ev_w"])
+    s.ev_f, s.ev_first, s.ev_w = A.fptr(keep["ev_f"]), keep["ev_first"].ctypes.data_as(A.c_i64p), A.fptr(keep["ev_w"])
+    s.lam0, s.lam1, s.cone_cos = a["lam0"], a["lam1"], a["cone_cos"]
+    s.tau1, s.tau2, s.frac1 = a["tau1"], a["tau2"], a["frac1"]
+    return s, keep
+
+
+def trace(det, key, n, *, rows=None, source=None, samples=None, first_id=0, pool_live=None, pool_ref=None,
+          controls=None, n_events=1, n_bins=0, bin0=0.0, bin_w=1.0, records=False, threads=0):
+    """Trace photons first_id .. first_id + n - 1 on the CPU; return (Tallies, (rec_i, rec_f) or None)."""
+    d, keep = det.desc()
+    c = controls or A.controls()
+    T = Tallies(det.n_sensor, n_events, n_bins, bin0, bin_w, c.n_grad)
+    rr, rkeep = host_rows(rows) if rows is not None else (None, None)
+    ss, skeep = host_source(source, samples or n) if source is not None else (None, None)
+    live = None if pool_live is None else A.np_f32(pool_live)
+    ref = None if pool_ref is None else A.np_f32(pool_ref)
+    rec_i = np.zeros((n, 5), np.int32) if records else None
+    rec_f = np.zeros((n, 4), np.float32) if records else None
+    st = lib().lumen_oracle_trace(ctypes.byref(d), A.fptr(live), A.fptr(ref),
+                                  ctypes.byref(rr) if rr is not None else None,
+                                  ctypes.byref(ss) if ss is not None else None, key[0], key[1], first_id, n,
+                                  ctypes.byref(c), ctypes.byref(T.c), A.iptr(rec_i), A.fptr(rec_f), threads)
+    assert st == 0, f"oracle status {st}"
+    return T, ((rec_i, rec_f) if records else None)
+
+
+def source_rows(source, key, n, first_id=0, samples=None):
+    ss, skeep = host_source(source, samples or n)
+    out_f = np.zeros((n, 15), np.float32)
+    ev = np.zeros(n, np.int32)
+    lib().lumen_oracle_source_rows(ctypes.byref(ss), key[0], key[1], first_id, n, A.fptr(out_f), A.iptr(ev))
+    return out_f, ev

@@ -1,0 +1,714 @@
+/*
+ * ORACLE (test infrastructure; only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline load it, and only as
+ * the checker or the timed CPU baseline, never as the product path).
+ *
+ * A scalar C++ restatement of lumen's photon loop (src/lumen/run.py:293-368 `_loop` / `item` / `body`) over one
+ * photon at a time: the step (src/lumen/transport/step.py:516 `step`, with `_recover` :245, `_step_context` :318,
+ * `_surface_event` :362, `_bulk` :397, `_after` :464, `_advance` :495), the deposit reduction the reference does in
+ * its records + rebuild launches (src/lumen/run.py:443-557, src/lumen/readout/fill.py:216: arrival, arrival_t,
+ * arrival2), and the sources (src/lumen/sources/point.py:73, _base.py:312-322). FP64 tallies; OpenMP over photons.
+ *
+ * Derivatives are forward-mode tangents of the live weight at the reference values, one per gradient parameter
+ * (a table whose values move together): the reference's reweighting estimator (src/lumen/transport/estimator.py)
+ * differentiated along the fixed path, deposits' tangents summed per sensor.
+ */
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "physics.h"
+#include "rng.h"
+
+#define O_SOURCE_STREAM 0xFFFFFFFFu
+#define O_POL_STREAM 0x9017u
+#define O_NORMAL_LO -0.99999994039535522461f /* nextafter(-1, 0) in float32: jax.random.normal's bound */
+#define O_SQRT2 1.41421356237309504880f
+#define O_MAXG LUMEN_MAX_GRAD
+
+typedef struct ORun {
+  OScene S;
+  const float* live;
+  const float* ref;
+  int shared; /* live == ref */
+  float max_distance, roulette, reach;
+  int max_vertices;
+  int P;
+  int gt[O_MAXG];
+} ORun;
+
+typedef struct OPhoton {
+  float x[3], d[3], t, lam, w, wr;
+  int alive, vertex;
+  float er[3], ei[3];
+  int vol, srf;
+  float sn[3];
+  int nz, cls;
+  float dw[O_MAXG];
+} OPhoton;
+
+typedef struct ODep {
+  int sensor;
+  float q, time, lam;
+  float fates[8]; /* lost, abandoned, escaped, distance_cut, absorbed_bulk, absorbed_surface, rouletted, reweighted */
+  float pushed;
+  float dq[O_MAXG];
+} ODep;
+
+static inline float o_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0.0f; }
+
+/* tangents of a medium's rates in the gradient parameters: d(1/L)/dL = -1/L^2 where L's table moves */
+static inline void o_dmed(const ORun* R, int mi, float lam, const OMed* m, float* dmu_abs, float* dmu_c) {
+  const int32_t* mr = R->S.D->med_i + (size_t)mi * LUMEN_MED_I;
+  float E = O_HC / lam;
+  for (int p = 0; p < R->P; ++p) {
+    dmu_abs[p] = 0.0f;
+    dmu_c[p] = 0.0f;
+    if (mr[LUMEN_MI_ABS] >= 0 && mr[LUMEN_MI_ABS] == R->gt[p]) {
+      float L = o_tab(R->S.D, R->live, mr[LUMEN_MI_ABS], E, 0);
+      dmu_abs[p] = L >= O_FLT_TINY ? -(m->mu_abs * m->mu_abs) : 0.0f;
+    }
+    if (mr[LUMEN_MI_RAY] >= 0 && mr[LUMEN_MI_RAY] == R->gt[p]) {
+      float L = o_tab(R->S.D, R->live, mr[LUMEN_MI_RAY], E, 0);
+      dmu_c[p] = L >= O_FLT_TINY ? -(m->mu_c * m->mu_c) : 0.0f;
+    }
+  }
+}
+
+/* one step (step.py:516) */
+static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
+  const OScene* S = &R->S;
+  const LumenSceneDesc* D = S->D;
+  const int P = R->P;
+  /* _recover: the stuck rule's push (step.py:245) */
+  float b0 = o_band(o_maxabs3(ph->x));
+  int stuck = ph->alive && ph->nz >= O_ZSBP;
+  if (stuck) {
+    float pb = O_PUSH_BANDS * b0;
+    for (int a = 0; a < 3; ++a) ph->x[a] = ph->x[a] + pb * ph->d[a];
+    ph->vol = o_locate(S, ph->x);
+    ph->cls = o_cls(S, ph->vol);
+    ph->srf = -1;
+  }
+  OKey vkey = o_fold_in(pkey, (uint32_t)ph->vertex);
+  float er0[3] = {ph->er[0], ph->er[1], ph->er[2]}, ei0[3] = {ph->ei[0], ph->ei[1], ph->ei[2]};
+  if (o_dot(er0, er0) + o_dot(ei0, ei0) < O_ZERO_STATE)
+    o_fill(ph->d, er0, ei0, o_uniform(o_fold_in(vkey, O_POL_STREAM), 0));
+  int mi = D->cls_medium[ph->cls];
+  OMed ml = o_medium_at(D, R->live, ph->lam, mi);
+  OMed mr = R->shared ? ml : o_medium_at(D, R->ref, ph->lam, mi);
+  float dmu_abs[O_MAXG], dmu_c[O_MAXG];
+  o_dmed(R, mi, ph->lam, &ml, dmu_abs, dmu_c);
+  float mu_r = mr.mu_c;
+  float s = -o_log(o_uniform(vkey, 0)) / o_max(mu_r, O_FLOOR32);
+  /* _query (step.py:260; TrackedGeometry.query, tracked.py:86) */
+  OQuery q = o_query(S, ph->x, ph->d, ph->vol, R->max_distance, ph->srf, ph->sn, s);
+  int sensor_q = q.hit ? D->vol_i[(size_t)q.vol_after * LUMEN_VOL_I + LUMEN_VI_SENSOR] : -1;
+  float dist = q.t;
+  int zero = dist <= O_ZERO_STEP_BANDS * b0;
+  /* _surface (step.py:280) */
+  int cb = q.cls_before, ca = q.cls_after;
+  int row = D->row_of[cb * D->n_cls + ca];
+  int cont = (q.cont || (zero && row < 0)) && q.hit;
+  if (cont) row = row > 0 ? row : 0;
+  /* _crossing at the live values and the reference (step.py:305) */
+  int mi_after = D->cls_medium[ca];
+  float n2l = o_index_at(D, R->live, ph->lam, mi_after);
+  float dcol[O_MAXG * LUMEN_N_COL], dprobs[O_MAXG * O_N_OUT], ddet[O_MAXG];
+  for (int p = 0; p < P; ++p)
+    for (int c = 0; c < LUMEN_N_COL; ++c)
+      dcol[p * LUMEN_N_COL + c] =
+          (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_COL + c] == R->gt[p]) ? 1.0f : 0.0f;
+  OEval le, re;
+  o_type_eval(D, R->live, row, ph->lam, ph->d, q.normal, ml.n, n2l, er0, ei0, &le, P, dcol, dprobs, ddet);
+  if (R->shared) re = le;
+  else {
+    float n2r = o_index_at(D, R->ref, ph->lam, mi_after);
+    o_type_eval(D, R->ref, row, ph->lam, ph->d, q.normal, mr.n, n2r, er0, ei0, &re, 0, 0, 0, 0);
+  }
+  if (cont) { /* a continue event: a straight pass, no deposit (step.py:298 _type_eval) */
+    for (int o = 0; o < O_N_OUT; ++o) { le.probs[o] = o == O_STRAIGHT; re.probs[o] = o == O_STRAIGHT; }
+    le.detect = 0.0f;
+    re.detect = 0.0f;
+    for (int p = 0; p < P; ++p) { for (int o = 0; o < O_N_OUT; ++o) dprobs[p * O_N_OUT + o] = 0.0f; ddet[p] = 0.0f; }
+  }
+  float p_draw[O_N_OUT], p_prop[O_N_OUT];
+  float tot = 0.0f;
+  for (int o = 0; o < O_N_OUT; ++o) { p_draw[o] = re.probs[o]; tot = o == 0 ? p_draw[0] : tot + p_draw[o]; }
+  for (int o = 0; o < O_N_OUT; ++o) p_prop[o] = tot > 0.0f ? p_draw[o] / tot : 0.0f;
+  int oc_ = o_choose(p_prop, O_N_OUT, o_uniform(vkey, 2));
+  int os_ = oc_ > 0 ? oc_ : 0;
+  int drawn = oc_ >= 0;
+  float mu = ml.mu_c;
+  float reach_live = o_exp(-mu * dist), reach_ref = o_exp(-mu_r * dist);
+  float att_if = o_exp(-ml.mu_abs * dist), att_r = o_exp(-mr.mu_abs * dist);
+  int scatter = mu_r > 0.0f && s < dist && ph->alive;
+  float v_g = O_C_VACUUM / ml.ng;
+  /* tangents of the crossing's factors */
+  float d_reach[O_MAXG], d_att[O_MAXG];
+  for (int p = 0; p < P; ++p) {
+    d_reach[p] = -(dmu_c[p] * dist) * reach_live;
+    d_att[p] = -(dmu_abs[p] * dist) * att_if;
+  }
+  /* step.py:521-526: the deposit and the lost weight */
+  int at_if = q.hit && ph->alive && row >= 0;
+  float p_det = le.detect;
+  float rr = o_ratio(reach_live, reach_ref);
+  dep->q = at_if ? ph->w * reach_live * att_if * p_det : 0.0f;
+  for (int p = 0; p < P; ++p) {
+    float f = reach_live * att_if * p_det;
+    float df = d_reach[p] * att_if * p_det + reach_live * d_att[p] * p_det + reach_live * att_if * ddet[p];
+    dep->dq[p] = at_if ? ph->dw[p] * f + ph->w * df : 0.0f;
+  }
+  float lost = (q.hit && ph->alive && row < 0 && !scatter) ? ph->w * rr * att_if : 0.0f;
+  /* _event: a bulk event or the drawn surface outcome (step.py:439) */
+  float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_sn[3], nx_er[3], nx_ei[3], nx_lam = ph->lam;
+  float nx_dw[O_MAXG];
+  int nx_cls, nx_ok, nx_far = 0;
+  float fates0, fates1, fates2, wr;
+  if (scatter) { /* _bulk (step.py:397) */
+    int next_cls = s < q.t_pass0 ? q.cls_start : (s > q.t_pass1 ? cb : o_cls(S, q.vol_at));
+    float mu_c_r = mr.mu_c;
+    /* one channel: choose(mu_c_r, u) is 0 whenever the rate is positive */
+    float e_r = o_exp(-mu_r * s), e_l = o_exp(-mu * s);
+    float path_r = mu_c_r * e_r;
+    float w_path = o_ratio(ml.mu_c * e_l, path_r);
+    float att = o_exp(-ml.mu_abs * s);
+    float w = w_path * att;
+    float w_r = o_ratio(path_r, path_r) * o_exp(-mr.mu_abs * s);
+    for (int a = 0; a < 3; ++a) nx_x[a] = ph->x[a] + s * ph->d[a];
+    float rl3[3] = {o_uniform(vkey, 3), o_uniform(vkey, 4), o_uniform(vkey, 5)};
+    o_rayleigh_sample(er0, ei0, rl3, nx_d);
+    for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+    o_project(nx_er, nx_ei, nx_d);
+    float w_at = ph->w * w_path;
+    fates0 = w_at * att * 1.0f;
+    fates1 = w_at * (1.0f - att * 1.0f);
+    fates2 = 0.0f;
+    nx_w = ph->w * w * 1.0f * 1.0f;
+    for (int p = 0; p < P; ++p) {
+      float dwp = (dmu_c[p] * e_l + ml.mu_c * (-(dmu_c[p] * s) * e_l)) / path_r;
+      if (!(path_r != 0.0f)) dwp = 0.0f;
+      float datt = -(dmu_abs[p] * s) * att;
+      float dwf = dwp * att + w_path * datt;
+      nx_dw[p] = ph->dw[p] * w + ph->w * dwf;
+    }
+    nx_cls = next_cls;
+    nx_ok = 1;
+    nx_dtime = s / v_g;
+    for (int a = 0; a < 3; ++a) nx_sn[a] = q.normal[a];
+    wr = ph->wr * w_r * 1.0f;
+  } else { /* _surface_event (step.py:362) */
+    float pl = le.probs[os_], pp = p_prop[os_];
+    float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
+    float w_if = ph->w * rr * att_if * r_live;
+    float dirn[3], wi[3] = {ph->d[0], ph->d[1], ph->d[2]};
+    const float* nrm = q.normal;
+    float eta = ml.n / n2l;
+    float out_w = 1.0f, out_wd = 1.0f;
+    int out_far = 0;
+    float s_ax[3];
+    o_s_axis(wi, nrm, s_ax);
+    Oc es, ep;
+    o_components(er0, ei0, wi, s_ax, &es, &ep);
+    for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+    switch (os_) {
+      case O_REFRACT: {
+        float cos_i = -o_dot(wi, nrm);
+        float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+        int tir = sin2_t >= 1.0f;
+        float ct2 = 1.0f - sin2_t;
+        float cos_t = ct2 > 0.0f ? sqrtf(ct2) : 0.0f;
+        if (tir) {
+          for (int a = 0; a < 3; ++a) dirn[a] = wi[a] + 2.0f * cos_i * nrm[a];
+        } else {
+          float k = eta * cos_i - cos_t;
+          for (int a = 0; a < 3; ++a) dirn[a] = eta * wi[a] + k * nrm[a];
+          o_unit(dirn);
+        }
+        float du[3] = {dirn[0], dirn[1], dirn[2]};
+        o_unit(du);
+        o_recombine(es, ep, le.amps[2], le.amps[3], s_ax, du, nx_er, nx_ei);
+        break;
+      }
+      case O_SPECULAR: {
+        float wn = o_dot(wi, nrm);
+        for (int a = 0; a < 3; ++a) dirn[a] = wi[a] - 2.0f * wn * nrm[a];
+        float du[3] = {dirn[0], dirn[1], dirn[2]};
+        o_unit(du);
+        o_recombine(es, ep, le.amps[0], le.amps[1], s_ax, du, nx_er, nx_ei);
+        break;
+      }
+      case O_BACKSCATTER:
+        for (int a = 0; a < 3; ++a) { dirn[a] = -wi[a]; nx_er[a] = -er0[a]; nx_ei[a] = -ei0[a]; }
+        break;
+      case O_DIFFUSE: {
+        o_lambert(nrm, o_uniform(vkey, 3), o_uniform(vkey, 4), dirn);
+        float h[3] = {dirn[0] - wi[0], dirn[1] - wi[1], dirn[2] - wi[2]};
+        o_unit(h);
+        o_mirror(nx_er, nx_ei, h);
+        break;
+      }
+      case O_GLOSSY: /* the facet lobe is not built in this restatement: the engine refuses such rows */
+      default:
+        for (int a = 0; a < 3; ++a) dirn[a] = wi[a];
+        break;
+    }
+    for (int a = 0; a < 3; ++a) nx_d[a] = dirn[a];
+    o_unit(nx_d);
+    int far_side = (os_ == O_STRAIGHT || os_ == O_REFRACT);
+    int far_ = (far_side || out_far) && drawn;
+    int ok = q.hit && drawn && row >= 0;
+    for (int a = 0; a < 3; ++a) nx_x[a] = ph->x[a] + q.t * ph->d[a];
+    float r_o = drawn ? (p_prop[os_] != 0.0f ? p_draw[os_] / p_prop[os_] : 0.0f) : 0.0f;
+    wr = ph->wr * (reach_ref != 0.0f ? 1.0f : 0.0f) * att_r * r_o * out_wd;
+    float w_at = ph->w * rr;
+    float s_cont = 0.0f;
+    for (int o = 0; o < O_N_OUT; ++o) s_cont = o == 0 ? le.probs[0] : s_cont + le.probs[o];
+    fates0 = ok ? w_at * att_if * s_cont : 0.0f;
+    fates1 = q.hit ? w_at * (1.0f - att_if) : 0.0f;
+    fates2 = (q.hit && row >= 0) ? w_at * att_if * (1.0f - s_cont) : 0.0f;
+    nx_w = w_if * out_w;
+    for (int p = 0; p < P; ++p) {
+      float dpl = dprobs[p * O_N_OUT + os_];
+      float dr_live = drawn ? (pp != 0.0f ? dpl / pp : 0.0f) : 0.0f;
+      float drr = reach_ref != 0.0f ? d_reach[p] / reach_ref : 0.0f;
+      float X = rr * att_if * r_live;
+      float dX = drr * att_if * r_live + rr * d_att[p] * r_live + rr * att_if * dr_live;
+      nx_dw[p] = (ph->dw[p] * X + ph->w * dX) * out_w;
+    }
+    nx_cls = far_ ? ca : cb;
+    nx_ok = ok;
+    nx_dtime = dist / v_g;
+    for (int a = 0; a < 3; ++a) nx_sn[a] = q.normal[a];
+    nx_far = far_;
+  }
+  /* step.py:529-542: the weights that end here */
+  float a_surf = ph->alive ? fates2 : 0.0f;
+  int far_end = ph->alive && !q.hit && !scatter;
+  float d_end = o_min(dist, R->max_distance);
+  float w_far = ph->w * o_ratio(o_exp(-mu * d_end), o_exp(-mu_r * d_end));
+  float att_far = o_exp(-ml.mu_abs * d_end);
+  int cut = R->max_distance < R->reach;
+  float escaped = (far_end && !cut) ? w_far * att_far : 0.0f;
+  float distance_cut = (far_end && cut) ? w_far * att_far : 0.0f;
+  float a_bulk = (ph->alive ? fates1 : 0.0f) + (far_end ? w_far * (1.0f - att_far) : 0.0f);
+  float reweighted = (ph->alive && nx_ok) ? fates0 - nx_w : 0.0f;
+  float time = ph->t + dist / v_g;
+  /* _after: the roulette and the stuck rule (step.py:464) */
+  float w_new = nx_w;
+  int low = wr < R->roulette;
+  float p_s = wr / R->roulette;
+  int keep = low ? (o_uniform(vkey, 6) < p_s) : 0;
+  int kept = low && keep, lostr = low && !keep;
+  float p_kept = kept ? p_s : 1.0f;
+  float w_in = w_new;
+  w_new = kept ? w_new / p_kept : (lostr ? 0.0f : w_new);
+  float rouletted = (ph->alive && nx_ok) ? w_in - w_new : 0.0f;
+  float wr_new = kept ? wr / p_kept : (lostr ? 0.0f : wr);
+  int alive = ph->alive && nx_ok && !lostr;
+  int nz_new = (q.hit && !scatter && dist <= O_ZERO_STEP_BANDS * b0) ? ph->nz + 1 : 0;
+  int abandon = alive && nz_new >= O_ZSBK;
+  float abandoned = abandon ? w_new : 0.0f;
+  alive = alive && !abandon;
+  float dw_new[O_MAXG];
+  for (int p = 0; p < P; ++p) dw_new[p] = kept ? nx_dw[p] / p_kept : (lostr ? 0.0f : nx_dw[p]);
+  /* _advance (step.py:495) */
+  int vol_b = s < q.t_pass0 ? q.vol_start : (s > q.t_pass1 ? q.vol_before : q.vol_at);
+  int vol = scatter ? vol_b : (nx_far ? q.vol_after : q.vol_before);
+  int held = scatter && s <= O_ZERO_STEP_BANDS * b0 && ph->srf >= 0;
+  int srf = held ? ph->srf : ((scatter || !q.hit) ? -1 : q.srf);
+  float pushed = (ph->alive && ph->nz == O_ZSBP) ? ph->w : 0.0f;
+  /* the deposit */
+  dep->sensor = at_if ? sensor_q : -1;
+  dep->time = time;
+  dep->lam = ph->lam;
+  dep->fates[0] = lost;
+  dep->fates[1] = abandoned;
+  dep->fates[2] = escaped;
+  dep->fates[3] = distance_cut;
+  dep->fates[4] = a_bulk;
+  dep->fates[5] = a_surf;
+  dep->fates[6] = rouletted;
+  dep->fates[7] = reweighted;
+  dep->pushed = pushed;
+  /* the photon after the step */
+  for (int a = 0; a < 3; ++a) { ph->x[a] = nx_x[a]; ph->d[a] = nx_d[a]; ph->er[a] = nx_er[a]; ph->ei[a] = nx_ei[a]; }
+  ph->t = ph->t + nx_dtime;
+  ph->lam = nx_lam;
+  ph->w = alive ? w_new : 0.0f;
+  ph->wr = alive ? wr_new : 0.0f;
+  for (int p = 0; p < P; ++p) ph->dw[p] = alive ? dw_new[p] : 0.0f;
+  ph->alive = alive;
+  ph->vertex += 1;
+  ph->vol = vol;
+  ph->srf = srf;
+  if (!held) for (int a = 0; a < 3; ++a) ph->sn[a] = nx_sn[a];
+  ph->nz = nz_new;
+  ph->cls = nx_cls;
+}
+
+/* ------------------------------------------------------------------------------------------------ sources */
+typedef struct ORow { float x[3], d[3], t, lam, w0, er[3], ei[3]; int event; } ORow;
+
+/* gaussian from a uniform (sources/_base.py:318): jax.random.normal's map of the same bits */
+static inline float o_gaussian(float u) {
+  float f = u - 5.9604644775390625e-8f;
+  float v = f * (1.0f - O_NORMAL_LO) + O_NORMAL_LO;
+  v = v > O_NORMAL_LO ? v : O_NORMAL_LO;
+  return O_SQRT2 * o_erfinv(v);
+}
+
+static int o_event_of(const int64_t* first, int n_ev, int64_t gid) {
+  int lo = 0, hi = n_ev - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) / 2;
+    if (first[mid] <= gid) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+/* photon gid of a procedural source (uniforms of vertex 0 of its own key under the source stream) */
+static void o_source_row(const LumenSource* src, OKey key, int64_t gid, ORow* r) {
+  OKey sk = o_fold_in(key, O_SOURCE_STREAM);
+  OKey rk = o_fold_in(o_fold_in(sk, (uint32_t)gid), 0u);
+  int e = o_event_of(src->ev_first, src->n_events, gid);
+  const float* f = src->ev_f + (size_t)e * LUMEN_EV_F;
+  r->event = e;
+  r->w0 = src->ev_w[e];
+  for (int a = 0; a < 3; ++a) { r->er[a] = 0.0f; r->ei[a] = 0.0f; }
+  if (src->kind == LUMEN_SRC_TRACK) {
+    float u0 = o_uniform(rk, 0), u1 = o_uniform(rk, 1), u2 = o_uniform(rk, 2);
+    const float* ax = f + 3;
+    float along = u0 * f[6];
+    for (int a = 0; a < 3; ++a) r->x[a] = f[a] + along * ax[a];
+    float c = src->cone_cos;
+    float sn = sqrtf(1.0f - c * c);
+    float sp, cp;
+    o_sincos2pi(u1, &sp, &cp);
+    float l[3] = {sn * cp, sn * sp, c};
+    o_to_world(l, ax, r->d);
+    r->t = f[7] + along / O_C_VACUUM;
+    r->lam = src->lam1 > src->lam0 ? src->lam0 + (src->lam1 - src->lam0) * u2 : src->lam0;
+    /* Cherenkov polarisation: in the plane of the axis and d, perpendicular to d (polar.py:89 cherenkov) */
+    float ad = o_dot(ax, r->d);
+    for (int a = 0; a < 3; ++a) r->er[a] = ad * r->d[a] - ax[a];
+    o_unit(r->er);
+    return;
+  }
+  float g[3] = {o_gaussian(o_uniform(rk, 0)), o_gaussian(o_uniform(rk, 1)), o_gaussian(o_uniform(rk, 2))};
+  o_unit(g);
+  for (int a = 0; a < 3; ++a) { r->x[a] = f[a]; r->d[a] = g[a]; }
+  float u3 = o_uniform(rk, 3);
+  r->lam = src->lam1 > src->lam0 ? src->lam0 + (src->lam1 - src->lam0) * u3 : src->lam0;
+  r->t = f[3];
+  if (src->kind == LUMEN_SRC_SCINT) {
+    float u4 = o_uniform(rk, 4), u5 = o_uniform(rk, 5);
+    float tau = u4 < src->frac1 ? src->tau1 : src->tau2;
+    r->t = f[3] + -o_log(u5) * tau;
+  }
+}
+
+/* -------------------------------------------------------------------------------------------- the photon loop */
+typedef struct OTally {
+  int S_, E, nb, P;
+  float bin0, bin_w;
+  std::vector<double> arrival, arrival_t, arrival2, hist, jac, health;
+  std::vector<long long> counts;
+} OTally;
+
+#define O_CACHE 4
+typedef struct OPhotonSums { int sensor[O_CACHE]; double sum[O_CACHE]; int n; } OPhotonSums;
+
+static void o_flush2(OTally* T, int e, OPhotonSums* ps, int j) {
+  T->arrival2[(size_t)e * T->S_ + ps->sensor[j]] += ps->sum[j] * ps->sum[j];
+}
+
+/* one photon's loop (run.py:307 item): begin, steps until it ends or reaches the vertex guard */
+static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTally* T, int32_t* rec_i,
+                     float* rec_f) {
+  const OScene* S = &R->S;
+  OPhoton ph;
+  memset(&ph, 0, sizeof(ph));
+  for (int a = 0; a < 3; ++a) { ph.x[a] = row->x[a]; ph.d[a] = row->d[a]; ph.er[a] = row->er[a]; ph.ei[a] = row->ei[a]; }
+  ph.t = row->t;
+  ph.lam = row->lam;
+  ph.w = 1.0f;
+  ph.wr = 1.0f;
+  ph.alive = 1;
+  ph.vertex = 0;
+  ph.vol = o_locate(S, ph.x);
+  ph.cls = o_cls(S, ph.vol);
+  ph.srf = -1;
+  ph.nz = 0;
+  OKey pkey = o_fold_in(key, (uint32_t)gid);
+  const double w0 = row->w0;
+  const int e = row->event;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double pushed = 0.0;
+  OPhotonSums ps;
+  ps.n = 0;
+  int n_dep = 0, first_sensor = -1;
+  double sum_q = 0.0, sum_qt = 0.0;
+  long long steps = 0;
+  while (ph.alive && ph.vertex < R->max_vertices) {
+    ODep dep;
+    o_step(R, &ph, pkey, &dep);
+    steps++;
+    for (int k = 0; k < 8; ++k) acc[k] += (double)dep.fates[k];
+    pushed += (double)dep.pushed * w0;
+    if (dep.sensor >= 0) {
+      int s = dep.sensor;
+      double v = (double)dep.q * w0;
+      size_t ix = (size_t)e * T->S_ + s;
+      T->arrival[ix] += v;
+      T->arrival_t[ix] += v * (double)dep.time;
+      if (T->nb > 0) {
+        float b = floorf((dep.time - T->bin0) / T->bin_w);
+        if (b >= 0.0f && b < (float)T->nb) T->hist[ix * T->nb + (size_t)b] += v;
+      }
+      for (int p = 0; p < R->P; ++p) T->jac[ix * R->P + p] += (double)dep.dq[p] * w0;
+      int j = 0;
+      while (j < ps.n && ps.sensor[j] != s) ++j;
+      if (j == ps.n) {
+        if (ps.n == O_CACHE) { /* the oldest entry's sum is final: flush it */
+          o_flush2(T, e, &ps, 0);
+          for (int k = 1; k < O_CACHE; ++k) { ps.sensor[k - 1] = ps.sensor[k]; ps.sum[k - 1] = ps.sum[k]; }
+          ps.n -= 1;
+          T->counts[LUMEN_C_MULTI] += 1;
+        }
+        j = ps.n++;
+        ps.sensor[j] = s;
+        ps.sum[j] = 0.0;
+      }
+      ps.sum[j] += v;
+      n_dep++;
+      if (first_sensor < 0) first_sensor = s;
+      sum_q += (double)dep.q;
+      sum_qt += (double)dep.q * (double)dep.time;
+      T->counts[LUMEN_C_DEPOSITS] += 1;
+    }
+  }
+  for (int j = 0; j < ps.n; ++j) o_flush2(T, e, &ps, j);
+  for (int k = 0; k < 8; ++k) T->health[k] += acc[k] * w0;
+  double trunc = ph.alive ? (double)ph.w * w0 : 0.0;
+  T->health[LUMEN_H_TRUNCATED] += trunc;
+  T->health[LUMEN_H_PUSHED] += pushed;
+  T->health[LUMEN_H_START] += w0;
+  T->counts[LUMEN_C_PHOTONS] += 1;
+  T->counts[LUMEN_C_STEPS] += steps;
+  if (ph.alive) T->counts[LUMEN_C_TRUNCATED] += 1;
+  if (rec_i) {
+    rec_i[0] = ph.vertex;
+    rec_i[1] = n_dep;
+    rec_i[2] = ph.alive ? 0 : 1;
+    rec_i[3] = first_sensor;
+    rec_i[4] = ph.vol;
+    rec_f[0] = (float)sum_q;
+    rec_f[1] = ph.w;
+    rec_f[2] = ph.t;
+    rec_f[3] = (float)sum_qt;
+  }
+}
+
+static int o_scene(const LumenSceneDesc* D, OScene* S) {
+  S->D = D;
+  S->n = D->n_vol;
+  S->LM = 1;
+  S->FM = 1;
+  for (int k = 0; k < D->n_kind; ++k) {
+    const int32_t* ki = D->kind_i + (size_t)k * LUMEN_KIND_I;
+    if (ki[1] > S->LM) S->LM = ki[1];
+    if (ki[1] > LUMEN_MAX_LEAVES) return LUMEN_ERR_SCENE;
+    for (int l = 0; l < ki[1]; ++l) {
+      int np = D->leaf_i[(size_t)(ki[0] + l) * LUMEN_LEAF_I + 2];
+      if (np + 1 > S->FM) S->FM = np + 1;
+    }
+  }
+  S->SU = D->n_vol + 1;
+  return LUMEN_OK;
+}
+
+static void o_run_init(ORun* R, const LumenSceneDesc* D, const float* live, const float* ref,
+                       const LumenControls* c) {
+  o_scene(D, &R->S);
+  R->live = live ? live : D->pool;
+  R->ref = ref ? ref : R->live;
+  R->shared = R->ref == R->live;
+  R->reach = D->reach;
+  R->max_distance = c->max_distance > 0.0f ? c->max_distance : D->reach;
+  R->roulette = c->roulette;
+  R->max_vertices = c->max_vertices;
+  R->P = c->n_grad;
+  for (int p = 0; p < R->P; ++p) R->gt[p] = c->grad_tab[p];
+}
+
+/* host rows in the layout of LumenRows (every pointer a host array) */
+static void o_row_of(const LumenRows* rows, const LumenSource* src, OKey key, int64_t first_id, int64_t i, ORow* r) {
+  if (rows) {
+    r->x[0] = rows->x[i]; r->x[1] = rows->y[i]; r->x[2] = rows->z[i];
+    r->d[0] = rows->dx[i]; r->d[1] = rows->dy[i]; r->d[2] = rows->dz[i];
+    r->t = rows->t[i]; r->lam = rows->lam[i]; r->w0 = rows->w[i];
+    for (int a = 0; a < 3; ++a) {
+      r->er[a] = rows->pol ? rows->pol[6 * i + a] : 0.0f;
+      r->ei[a] = rows->pol ? rows->pol[6 * i + 3 + a] : 0.0f;
+    }
+    r->event = rows->event ? rows->event[i] : 0;
+  } else {
+    o_source_row(src, key, first_id + i, r);
+  }
+}
+
+extern "C" {
+
+int32_t lumen_oracle_threefry(uint32_t k0, uint32_t k1, uint32_t x0, uint32_t x1, uint32_t* out) {
+  o_threefry(k0, k1, x0, x1, out, out + 1);
+  return 0;
+}
+
+/* uniforms(vertex_key(photon_key(key, id), vertex), n) for ids[i] (rng.py:81 uniforms) */
+int32_t lumen_oracle_uniforms(uint32_t k0, uint32_t k1, const int64_t* ids, int64_t n_ids, int32_t vertex,
+                              int32_t n, float* out) {
+  OKey key = {k0, k1};
+  for (int64_t i = 0; i < n_ids; ++i) {
+    OKey vk = o_fold_in(o_fold_in(key, (uint32_t)ids[i]), (uint32_t)vertex);
+    for (int j = 0; j < n; ++j) out[i * n + j] = o_uniform(vk, (uint32_t)j);
+  }
+  return 0;
+}
+
+/* elementwise math for the golden checks: fn 0 exp, 1 log, 2 sin 2 pi x, 3 cos 2 pi x, 4 acos, 5 cbrt, 6 erfinv,
+   7 sin, 8 cos, 9 dipole_cos, 10 gaussian */
+int32_t lumen_oracle_math(int32_t fn, const float* x, int64_t n, float* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    float s, c;
+    switch (fn) {
+      case 0: out[i] = o_exp(x[i]); break;
+      case 1: out[i] = o_log(x[i]); break;
+      case 2: o_sincos2pi(x[i], &s, &c); out[i] = s; break;
+      case 3: o_sincos2pi(x[i], &s, &c); out[i] = c; break;
+      case 4: out[i] = o_acos(x[i]); break;
+      case 5: out[i] = o_cbrt(x[i]); break;
+      case 6: out[i] = o_erfinv(x[i]); break;
+      case 7: o_sincos(x[i], &s, &c); out[i] = s; break;
+      case 8: o_sincos(x[i], &s, &c); out[i] = c; break;
+      case 9: out[i] = o_dipole_cos(x[i]); break;
+      case 10: out[i] = o_gaussian(x[i]); break;
+      default: return LUMEN_ERR_ARG;
+    }
+  }
+  return 0;
+}
+
+/* Fresnel amplitudes (fresnel.py:25) for n rows of (cos_i, n1, n2re, n2im): out 8 floats per row */
+int32_t lumen_oracle_fresnel(const float* in, int64_t n, float* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    Oc a[4];
+    o_amplitudes(in[4 * i], in[4 * i + 1], oc(in[4 * i + 2], in[4 * i + 3]), a);
+    for (int j = 0; j < 4; ++j) { out[8 * i + 2 * j] = a[j].re; out[8 * i + 2 * j + 1] = a[j].im; }
+  }
+  return 0;
+}
+
+/* basis(n) for n unit vectors: out t1, t2 (frames.py:14) */
+int32_t lumen_oracle_basis(const float* nv, int64_t n, float* out) {
+  for (int64_t i = 0; i < n; ++i) o_basis(nv + 3 * i, out + 6 * i, out + 6 * i + 3);
+  return 0;
+}
+
+int32_t lumen_oracle_locate(const LumenSceneDesc* D, const float* pts, int64_t n, int32_t* vol) {
+  OScene S;
+  int st = o_scene(D, &S);
+  if (st) return st;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) vol[i] = o_locate(&S, pts + 3 * i);
+  return 0;
+}
+
+/* the navigator query on a fixed ray set, the layout of lumen_b200_query (host arrays) */
+int32_t lumen_oracle_query(const LumenSceneDesc* D, const float* ray, const int32_t* vol, const int32_t* srf,
+                           float t_max, int64_t n, int32_t* out_i, float* out_f) {
+  OScene S;
+  int st = o_scene(D, &S);
+  if (st) return st;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    const float* o = ray + 6 * i;
+    const float* d = ray + 6 * i + 3;
+    int v = vol[i] >= 0 ? vol[i] : o_locate(&S, o);
+    int last = vol[i] >= 0 ? srf[i] : -1;
+    OQuery q = o_query(&S, o, d, v, t_max, last, 0, O_HUGE);
+    int32_t* oi = out_i + 8 * i;
+    oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
+    oi[5] = q.srf; oi[6] = q.zero;
+    oi[7] = q.hit ? D->vol_i[(size_t)q.vol_after * LUMEN_VOL_I + LUMEN_VI_SENSOR] : -1;
+    float* of = out_f + 4 * i;
+    of[0] = q.t; of[1] = q.normal[0]; of[2] = q.normal[1]; of[3] = q.normal[2];
+  }
+  return 0;
+}
+
+/* Trace photons first_id .. first_id + n - 1 (host arrays throughout; rows or src, one of them). Tallies are ADDED
+   to the host arrays of `out` (LumenTallies layout); rec_i / rec_f (optional) get the per-photon record of
+   lumen_b200_trace_photons. threads <= 0: OpenMP's default. */
+int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, const float* pool_ref,
+                           const LumenRows* rows, const LumenSource* src, uint32_t key0, uint32_t key1,
+                           int64_t first_id, int64_t n, const LumenControls* c, LumenTallies* out, int32_t* rec_i,
+                           float* rec_f, int32_t threads) {
+  if (!D || !c || !out || (!rows && !src) || n < 0) return LUMEN_ERR_ARG;
+  if (c->n_grad < 0 || c->n_grad > LUMEN_MAX_GRAD) return LUMEN_ERR_NOT_SUPPORTED;
+  ORun R;
+  o_run_init(&R, D, pool_live, pool_ref, c);
+  if (o_scene(D, &R.S)) return LUMEN_ERR_SCENE;
+  OKey key = {key0, key1};
+  const int Sn = D->n_sensor > 0 ? D->n_sensor : 1, E = out->n_events > 0 ? out->n_events : 1;
+  int nth = threads > 0 ? threads : omp_get_max_threads();
+  std::vector<OTally> parts(nth);
+  for (auto& T : parts) {
+    T.S_ = Sn; T.E = E; T.nb = out->hist ? out->n_bins : 0; T.P = c->n_grad;
+    T.bin0 = out->bin0; T.bin_w = out->bin_w;
+    T.arrival.assign((size_t)E * Sn, 0.0); T.arrival_t.assign((size_t)E * Sn, 0.0);
+    T.arrival2.assign((size_t)E * Sn, 0.0);
+    T.hist.assign((size_t)E * Sn * T.nb, 0.0);
+    T.jac.assign((size_t)E * Sn * (c->n_grad > 0 ? c->n_grad : 0), 0.0);
+    T.health.assign(LUMEN_N_HEALTH, 0.0);
+    T.counts.assign(LUMEN_N_COUNT, 0);
+  }
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nth)
+  for (int64_t i = 0; i < n; ++i) {
+    ORow r;
+    o_row_of(rows, src, key, first_id, i, &r);
+    o_photon(&R, &r, key, first_id + i, &parts[omp_get_thread_num()], rec_i ? rec_i + 5 * i : 0,
+             rec_f ? rec_f + 4 * i : 0);
+  }
+  for (auto& T : parts) {
+    for (size_t k = 0; k < T.arrival.size(); ++k) {
+      out->arrival[k] += T.arrival[k];
+      out->arrival_t[k] += T.arrival_t[k];
+      out->arrival2[k] += T.arrival2[k];
+    }
+    if (out->hist) for (size_t k = 0; k < T.hist.size(); ++k) out->hist[k] += T.hist[k];
+    if (out->jac) for (size_t k = 0; k < T.jac.size(); ++k) out->jac[k] += T.jac[k];
+    if (out->health) for (int k = 0; k < LUMEN_N_HEALTH; ++k) out->health[k] += T.health[k];
+    if (out->counts) for (int k = 0; k < LUMEN_N_COUNT; ++k) out->counts[k] += (unsigned long long)T.counts[k];
+  }
+  return 0;
+}
+
+/* emission rows of a procedural source (host): x, d, t, lam, w0, er, ei, event per photon */
+int32_t lumen_oracle_source_rows(const LumenSource* src, uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
+                                 float* out_f, int32_t* out_event) {
+  OKey key = {key0, key1};
+  for (int64_t i = 0; i < n; ++i) {
+    ORow r;
+    o_source_row(src, key, first_id + i, &r);
+    float* f = out_f + 15 * i;
+    for (int a = 0; a < 3; ++a) { f[a] = r.x[a]; f[3 + a] = r.d[a]; f[9 + a] = r.er[a]; f[12 + a] = r.ei[a]; }
+    f[6] = r.t; f[7] = r.lam; f[8] = r.w0;
+    out_event[i] = r.event;
+  }
+  return 0;
+}
+
+}  /* extern "C" */

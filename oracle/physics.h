@@ -1,0 +1,409 @@
+/*
+ * ORACLE (test infrastructure): the reference's optics at a crossing and in the bulk, restated in float32.
+ *
+ * Tables: src/lumen/media/laws.py:86 (_table: linear in photon energy, held beyond), :97 group_index.
+ * Media: src/lumen/media/bulk.py:76 rate, :88 evaluate; src/lumen/transport/medium.py:27 medium_at.
+ * Surfaces: src/lumen/surfaces/types.py:211 chained_cuts, :243-275 the three Fresnel branches, :277 Geant4's chain,
+ * :352 kernel; fresnel.py:25-75 amplitudes; polar.py (fill, project, mirror, s_axis, components, recombine,
+ * fractions); outcomes.py:36 refract; lobes.py:55 Lambert; media/phase.py:43-57 Rayleigh (polarised dipole draw).
+ * Frames: src/lumen/_core/frames.py (Duff et al. 2017 basis).
+ */
+#ifndef LUMEN_ORACLE_PHYSICS_H
+#define LUMEN_ORACLE_PHYSICS_H
+
+#include "geom.h"
+
+#define O_HC 1239.84198433200208f   /* h c in eV nm (src/lumen/units.py:20) */
+#define O_C_VACUUM 0.299792458f     /* m / ns */
+#define O_FLOOR32 1e-30f
+#define O_FLT_TINY 1.17549435e-38f
+#define O_FRESNEL_SMALL 1e-12f
+#define O_NORMAL_INCIDENCE 1.42108547152020037e-14f /* eps32^2 */
+#define O_ZERO_STATE 0.5f
+#define O_TWO_PI 6.28318530717958647692f
+#define O_PI 3.14159265358979323846f
+
+enum { O_STRAIGHT = 0, O_REFRACT, O_SPECULAR, O_BACKSCATTER, O_GLOSSY, O_DIFFUSE, O_N_OUT };
+
+/* ------------------------------------------------------------------------------------------------- tables */
+typedef struct OPools { const float* live; const float* ref; } OPools;
+
+/* value of table t at photon energy E (jnp.interp: held at the ends) and its slope in E there */
+static inline float o_tab(const LumenSceneDesc* D, const float* pool, int t, float E, float* slope) {
+  int off = D->tab[2 * t], k = D->tab[2 * t + 1];
+  const float* xe = pool + off;
+  const float* fv = pool + off + k;
+  if (slope) *slope = 0.0f;
+  if (k == 1 || E <= xe[0]) return fv[0];
+  if (E >= xe[k - 1]) return fv[k - 1];
+  int i = 1;
+  while (i < k - 1 && xe[i] <= E) ++i;
+  float dx = xe[i] - xe[i - 1];
+  float df = fv[i] - fv[i - 1];
+  float sl = df / dx;
+  if (slope) *slope = sl;
+  return fv[i - 1] + (E - xe[i - 1]) / dx * df;
+}
+
+/* rate 1 / L of a length (bulk.py:76) */
+static inline float o_rate(float L) { return L >= O_FLT_TINY ? 1.0f / L : 1.0f / O_FLT_TINY; }
+
+/* Geant4's GROUPVEL group index c / v_g at photon energy E of an index table (laws.py:156 _group_index_knot,
+   :170 geant4_group_index): knot values at the first knot, the segments' midpoints and the last knot, n + dn / d log E
+   (not below n), 1 / n_g linear in energy between them and held beyond. A one-knot (constant) table: n. */
+static inline float o_g4_group_knot(const float* e, const float* n, int k, int j) {
+  int s = j - 1 < 0 ? 0 : (j - 1 > k - 1 ? k - 1 : j - 1);
+  float slope = (n[s + 1] - n[s]) / o_log(e[s + 1] / e[s]);
+  float base = (j == 0 || j == k) ? n[j] : 0.5f * (n[s] + n[s + 1]);
+  float g = base + slope;
+  return g > base ? g : base;
+}
+static inline float o_group_index(const LumenSceneDesc* D, const float* pool, int t, float E) {
+  int off = D->tab[2 * t], kk = D->tab[2 * t + 1];
+  const float* e = pool + off;
+  const float* n = pool + off + kk;
+  if (kk == 1) return n[0];
+  int k = kk - 1;
+  /* eg: e0, the midpoints of segments 0 .. k-2, e_k */
+  float eg_[LUMEN_MAX_KNOTS + 1];
+  eg_[0] = e[0];
+  for (int i = 0; i + 1 < k; ++i) eg_[1 + i] = 0.5f * (e[i] + e[i + 1]);
+  eg_[k] = e[k];
+  int p = 0;
+  while (p < k + 1 && eg_[p] <= E) ++p; /* searchsorted, side right */
+  p = p < 1 ? 1 : (p > k ? k : p);
+  float x0 = eg_[p - 1], x1 = eg_[p];
+  float f0 = 1.0f / o_g4_group_knot(e, n, k, p - 1), f1 = 1.0f / o_g4_group_knot(e, n, k, p);
+  float f;
+  if (E < x0) f = f0;
+  else if (E > x1) f = f1;
+  else {
+    float dx = x1 - x0;
+    f = fabsf(dx) <= 1.4e-45f ? f0 : f0 + (E - x0) / dx * (f1 - f0);
+  }
+  return 1.0f / f;
+}
+
+typedef struct OMed { float n, ng, mu_abs, mu_c; } OMed;
+
+/* (n, n_g, mu_abs, mu) of medium mi at lam (medium.py:27); one bulk channel (Rayleigh) at most */
+static inline OMed o_medium_at(const LumenSceneDesc* D, const float* pool, float lam, int mi) {
+  const int32_t* m = D->med_i + (size_t)mi * LUMEN_MED_I;
+  float E = O_HC / lam;
+  OMed r = {1.0f, 1.0f, 0.0f, 0.0f};
+  if (m[LUMEN_MI_INDEX] >= 0) {
+    r.n = o_tab(D, pool, m[LUMEN_MI_INDEX], E, 0);
+    r.ng = o_group_index(D, pool, m[LUMEN_MI_INDEX], E);
+  }
+  if (m[LUMEN_MI_ABS] >= 0) r.mu_abs = o_rate(o_tab(D, pool, m[LUMEN_MI_ABS], E, 0));
+  if (m[LUMEN_MI_RAY] >= 0) r.mu_c = o_rate(o_tab(D, pool, m[LUMEN_MI_RAY], E, 0));
+  return r;
+}
+static inline float o_index_at(const LumenSceneDesc* D, const float* pool, float lam, int mi) {
+  const int32_t* m = D->med_i + (size_t)mi * LUMEN_MED_I;
+  if (m[LUMEN_MI_INDEX] < 0) return 1.0f;
+  return o_tab(D, pool, m[LUMEN_MI_INDEX], O_HC / lam, 0);
+}
+
+/* ---------------------------------------------------------------------------------------------- vectors */
+static inline void o_unit(float* v) {
+  float s = o_dot(v, v);
+  if (s > 0.0f) {
+    float r = sqrtf(s);
+    v[0] = v[0] / r; v[1] = v[1] / r; v[2] = v[2] / r;
+  }
+}
+static inline void o_cross(const float* a, const float* b, float* c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+/* frames.py:14 basis (Duff et al.) */
+static inline void o_basis(const float* n, float* t1, float* t2) {
+  float sign = n[2] >= 0.0f ? 1.0f : -1.0f;
+  float a = -1.0f / (sign + n[2]);
+  float b = n[0] * n[1] * a;
+  t1[0] = 1.0f + sign * (n[0] * n[0]) * a; t1[1] = sign * b; t1[2] = -sign * n[0];
+  t2[0] = b; t2[1] = sign + (n[1] * n[1]) * a; t2[2] = -n[1];
+}
+static inline void o_to_world(const float* l, const float* n, float* w) {
+  float t1[3], t2[3];
+  o_basis(n, t1, t2);
+  for (int a = 0; a < 3; ++a) w[a] = l[0] * t1[a] + l[1] * t2[a] + l[2] * n[a];
+}
+
+/* --------------------------------------------------------------------------------------- complex float32 */
+typedef struct Oc { float re, im; } Oc;
+static inline Oc oc(float r, float i) { Oc z = {r, i}; return z; }
+static inline Oc oc_add(Oc a, Oc b) { return oc(a.re + b.re, a.im + b.im); }
+static inline Oc oc_sub(Oc a, Oc b) { return oc(a.re - b.re, a.im - b.im); }
+static inline Oc oc_mul(Oc a, Oc b) { return oc(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static inline Oc oc_div(Oc a, Oc b) {
+  float den = b.re * b.re + b.im * b.im;
+  return oc((a.re * b.re + a.im * b.im) / den, (a.im * b.re - a.re * b.im) / den);
+}
+static inline float oc_abs2(Oc a) { return a.re * a.re + a.im * a.im; }
+static inline float oc_abs(Oc a) { return sqrtf(oc_abs2(a)); }
+/* principal square root */
+static inline Oc oc_sqrt(Oc z) {
+  float r = oc_abs(z);
+  if (r == 0.0f) return oc(0.0f, 0.0f);
+  if (z.re >= 0.0f) {
+    float t = sqrtf((r + z.re) * 0.5f);
+    return oc(t, z.im / (2.0f * t));
+  }
+  float t = sqrtf((r - z.re) * 0.5f);
+  return oc(fabsf(z.im) / (2.0f * t), z.im < 0.0f ? -t : t);
+}
+/* sqrt with Im >= 0, and 0 near 0 (fresnel.py:14 decaying_sqrt) */
+static inline Oc oc_decaying_sqrt(Oc z) {
+  if (oc_abs(z) < O_FRESNEL_SMALL) return oc(0.0f, 0.0f);
+  Oc q = oc_sqrt(z);
+  if (q.im < 0.0f) q = oc(-q.re, -q.im);
+  return q;
+}
+
+/* (r_s, r_p, t_s, t_p) from n1 into n2 at incidence cos_i (fresnel.py:25 amplitudes) */
+static inline void o_amplitudes(float cos_i, float n1, Oc n2, Oc* a) {
+  float c = cos_i < 0.0f ? 0.0f : (cos_i > 1.0f ? 1.0f : cos_i);
+  Oc c1 = oc(c, 0.0f), n1c = oc(n1, 0.0f);
+  Oc n22 = oc_mul(n2, n2);
+  Oc q = oc_decaying_sqrt(oc_sub(n22, oc_mul(oc_mul(n1c, n1c), oc(1.0f - c * c, 0.0f))));
+  Oc ds = oc_add(oc_mul(n1c, c1), q);
+  Oc dp = oc_add(oc_mul(n22, c1), oc_mul(n1c, q));
+  int ok_s = oc_abs(ds) > O_FRESNEL_SMALL, ok_p = oc_abs(dp) > O_FRESNEL_SMALL;
+  Oc two_n1c = oc_mul(oc(2.0f, 0.0f), oc_mul(n1c, c1));
+  a[0] = ok_s ? oc_div(oc_sub(oc_mul(n1c, c1), q), ds) : oc(-1.0f, 0.0f);
+  a[1] = ok_p ? oc_div(oc_sub(oc_mul(n22, c1), oc_mul(n1c, q)), dp) : oc(1.0f, 0.0f);
+  a[2] = ok_s ? oc_div(two_n1c, ds) : oc(0.0f, 0.0f);
+  a[3] = ok_p ? oc_div(oc_mul(two_n1c, n2), dp) : oc(0.0f, 0.0f);
+}
+
+/* ------------------------------------------------------------------------------------------- polarisation */
+static inline void o_normalise(float* er, float* ei) {
+  float s = o_dot(er, er) + o_dot(ei, ei);
+  if (s > O_FLOOR32) {
+    float r = 1.0f / sqrtf(s);
+    for (int a = 0; a < 3; ++a) { er[a] = er[a] * r; ei[a] = ei[a] * r; }
+  } else {
+    for (int a = 0; a < 3; ++a) { er[a] = 0.0f; ei[a] = 0.0f; }
+  }
+}
+/* an unpolarised state (E = 0) replaced by a random linear one (polar.py:57 fill) */
+static inline void o_fill(const float* d, float* er, float* ei, float rand) {
+  if (o_dot(er, er) + o_dot(ei, ei) < O_ZERO_STATE) {
+    float t1[3], t2[3], s, c;
+    o_basis(d, t1, t2);
+    o_sincos2pi(rand, &s, &c);
+    for (int a = 0; a < 3; ++a) { er[a] = c * t1[a] + s * t2[a]; ei[a] = 0.0f; }
+  }
+}
+static inline void o_project(float* er, float* ei, const float* k) {
+  float kr = o_dot(k, er), ki = o_dot(k, ei);
+  for (int a = 0; a < 3; ++a) { er[a] = er[a] - kr * k[a]; ei[a] = ei[a] - ki * k[a]; }
+  o_normalise(er, ei);
+}
+static inline void o_mirror(float* er, float* ei, const float* h) {
+  float hr = o_dot(er, h), hi = o_dot(ei, h);
+  for (int a = 0; a < 3; ++a) { er[a] = -er[a] + 2.0f * hr * h[a]; ei[a] = -ei[a] + 2.0f * hi * h[a]; }
+}
+/* the s axis unit(wi x n); at normal incidence basis(wi)'s first tangent (polar.py:100 s_axis) */
+static inline void o_s_axis(const float* wi, const float* n, float* s) {
+  float c[3];
+  o_cross(wi, n, c);
+  if (o_dot(c, c) > O_NORMAL_INCIDENCE) {
+    s[0] = c[0]; s[1] = c[1]; s[2] = c[2];
+    o_unit(s);
+  } else {
+    float t2[3];
+    o_basis(wi, s, t2);
+  }
+}
+static inline void o_components(const float* er, const float* ei, const float* wi, const float* s, Oc* es, Oc* ep) {
+  float p[3];
+  o_cross(wi, s, p);
+  *es = oc(o_dot(er, s), o_dot(ei, s));
+  *ep = oc(o_dot(er, p), o_dot(ei, p));
+}
+static inline void o_recombine(Oc es, Oc ep, Oc as, Oc ap, const float* s, const float* k, float* er, float* ei) {
+  float p[3];
+  o_cross(k, s, p);
+  Oc cs = oc_mul(as, es), cp = oc_mul(ap, ep);
+  for (int a = 0; a < 3; ++a) {
+    er[a] = cs.re * s[a] + cp.re * p[a];
+    ei[a] = cs.im * s[a] + cp.im * p[a];
+  }
+  o_normalise(er, ei);
+}
+
+/* --------------------------------------------------------------------------------------- the surface kernel */
+typedef struct OEval {
+  float probs[O_N_OUT];
+  float detect;
+  float sigma;
+  Oc amps[4];
+} OEval;
+
+/* the tangent of one row column per gradient parameter: dcol[p][c] */
+static inline float o_clip01(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
+static inline float o_dclip01(float x, float dx) { return (x >= 0.0f && x <= 1.0f) ? dx : 0.0f; }
+
+/* Geant4's chained cuts (types.py:211) of (p1..pk) -> k + 1 shares, with their tangents */
+static inline void o_chained(int k, const float* p, const float* dp, float* out, float* dout) {
+  float s = 0.0f, ds = 0.0f, prev = 0.0f, dprev = 0.0f;
+  for (int j = 0; j < k; ++j) {
+    s = j == 0 ? p[0] : s + p[j];
+    ds = j == 0 ? dp[0] : ds + dp[j];
+    float c = o_clip01(s), dc = o_dclip01(s, ds);
+    out[j] = c - prev;
+    dout[j] = dc - dprev;
+    prev = c;
+    dprev = dc;
+  }
+  out[k] = 1.0f - prev;
+  dout[k] = -dprev;
+}
+
+/* the TypeEval of surface row `row` at a crossing (types.py:352 kernel, surface_event.py:58 type_probs); `grad`:
+   the number of gradient parameters, dcolp[p * LUMEN_N_COL + c] the tangent of column c in parameter p, and
+   dprobs[p * 6 + o], ddet[p] its outputs' tangents */
+static inline void o_type_eval(const LumenSceneDesc* D, const float* pool, int row, float lam, const float* wi,
+                               const float* n, float n1, float n2, const float* er, const float* ei, OEval* ev,
+                               int grad, const float* dcolp, float* dprobs, float* ddet) {
+  for (int o = 0; o < O_N_OUT; ++o) ev->probs[o] = 0.0f;
+  ev->detect = 0.0f;
+  ev->sigma = 0.1f;
+  ev->amps[0] = oc(-1.0f, 0.0f); ev->amps[1] = oc(1.0f, 0.0f); ev->amps[2] = oc(1.0f, 0.0f); ev->amps[3] = oc(1.0f, 0.0f);
+  for (int p = 0; p < grad; ++p) { for (int o = 0; o < O_N_OUT; ++o) dprobs[p * O_N_OUT + o] = 0.0f; ddet[p] = 0.0f; }
+  if (row < 0) return;
+  const int32_t* ri = D->row_i + (size_t)row * LUMEN_ROW_I;
+  float E = O_HC / lam;
+  float col[LUMEN_N_COL];
+  for (int c = 0; c < LUMEN_N_COL; ++c) col[c] = o_tab(D, pool, ri[LUMEN_RI_COL + c], E, 0);
+  int model = ri[LUMEN_RI_MODEL], normal = ri[LUMEN_RI_NORMAL];
+  float cos_i = -(wi[0] * n[0] + wi[1] * n[1] + wi[2] * n[2]);
+  cos_i = cos_i < 0.0f ? 0.0f : (cos_i > 1.0f ? 1.0f : cos_i);
+  float Rc, split[5]; /* specular, glossy, backscatter, diffuse, refraction */
+  float dRc[LUMEN_MAX_GRAD], dsplit[LUMEN_MAX_GRAD][5];
+  if (model == 0) { /* _none: the reflection constants split R */
+    float pc[3] = {col[LUMEN_COL_PSPIKE], col[LUMEN_COL_PLOBE], col[LUMEN_COL_PBACK]};
+    float zero3[3] = {0.0f, 0.0f, 0.0f}, sh[4], dsh[4];
+    o_chained(3, pc, zero3, sh, dsh);
+    split[0] = normal ? sh[0] + sh[1] : sh[0];
+    split[1] = normal ? 0.0f : sh[1];
+    split[2] = sh[2];
+    split[3] = sh[3];
+    split[4] = 0.0f;
+    Rc = col[LUMEN_COL_R];
+    for (int p = 0; p < grad; ++p) {
+      const float* dc = dcolp + p * LUMEN_N_COL;
+      float dpc[3] = {dc[LUMEN_COL_PSPIKE], dc[LUMEN_COL_PLOBE], dc[LUMEN_COL_PBACK]};
+      o_chained(3, pc, dpc, sh, dsh);
+      dsplit[p][0] = normal ? dsh[0] + dsh[1] : dsh[0];
+      dsplit[p][1] = normal ? 0.0f : dsh[1];
+      dsplit[p][2] = dsh[2];
+      dsplit[p][3] = dsh[3];
+      dsplit[p][4] = 0.0f;
+      dRc[p] = dc[LUMEN_COL_R];
+    }
+  } else if (model == 1) { /* _real: the two media's Fresnel interface */
+    o_amplitudes(cos_i, n1, oc(n2, 0.0f), ev->amps);
+    float s_ax[3];
+    o_s_axis(wi, n, s_ax);
+    Oc es, ep;
+    o_components(er, ei, wi, s_ax, &es, &ep);
+    float F = oc_abs2(ev->amps[0]) * oc_abs2(es) + oc_abs2(ev->amps[1]) * oc_abs2(ep);
+    F = o_clip01(F);
+    split[0] = F; split[1] = 0.0f; split[2] = 0.0f; split[3] = 0.0f; split[4] = 1.0f - F;
+    Rc = col[LUMEN_COL_R];
+    for (int p = 0; p < grad; ++p) {
+      for (int j = 0; j < 5; ++j) dsplit[p][j] = 0.0f;
+      dRc[p] = dcolp[p * LUMEN_N_COL + LUMEN_COL_R];
+    }
+  } else { /* _complex: a complex index seen from a dielectric */
+    o_amplitudes(cos_i, n1, oc(col[LUMEN_COL_NR], col[LUMEN_COL_NK]), ev->amps);
+    float s_ax[3];
+    o_s_axis(wi, n, s_ax);
+    Oc es, ep;
+    o_components(er, ei, wi, s_ax, &es, &ep);
+    Rc = o_clip01(oc_abs2(ev->amps[0]) * oc_abs2(es) + oc_abs2(ev->amps[1]) * oc_abs2(ep));
+    split[0] = 1.0f; split[1] = 0.0f; split[2] = 0.0f; split[3] = 0.0f; split[4] = 0.0f;
+    for (int p = 0; p < grad; ++p) { for (int j = 0; j < 5; ++j) dsplit[p][j] = 0.0f; dRc[p] = 0.0f; }
+  }
+  /* Geant4's chain (types.py:277) */
+  float cut[2] = {Rc, col[LUMEN_COL_T]}, zc[2] = {0.0f, 0.0f}, rta[3], drta[3];
+  o_chained(2, cut, zc, rta, drta);
+  float r = rta[0], t = rta[1], a = rta[2];
+  ev->probs[O_REFRACT] = r * split[4];
+  ev->probs[O_SPECULAR] = r * split[0];
+  ev->probs[O_GLOSSY] = r * split[1];
+  ev->probs[O_BACKSCATTER] = r * split[2];
+  ev->probs[O_DIFFUSE] = r * split[3];
+  ev->probs[O_STRAIGHT] = t;
+  int far_opaque = ri[LUMEN_RI_FAR_OPAQUE];
+  if (far_opaque) { ev->probs[O_STRAIGHT] = 0.0f; ev->probs[O_REFRACT] = 0.0f; }
+  ev->detect = a * col[LUMEN_COL_EFF];
+  ev->sigma = ri[LUMEN_RI_GLISUR] ? 1.0f - col[LUMEN_COL_POLISH] : col[LUMEN_COL_SIGMA];
+  for (int p = 0; p < grad; ++p) {
+    const float* dc = dcolp + p * LUMEN_N_COL;
+    float dcut[2] = {dRc[p], dc[LUMEN_COL_T]};
+    o_chained(2, cut, dcut, rta, drta);
+    float dr = drta[0], dt = drta[1], da = drta[2];
+    float* dp = dprobs + p * O_N_OUT;
+    dp[O_REFRACT] = dr * split[4] + r * dsplit[p][4];
+    dp[O_SPECULAR] = dr * split[0] + r * dsplit[p][0];
+    dp[O_GLOSSY] = dr * split[1] + r * dsplit[p][1];
+    dp[O_BACKSCATTER] = dr * split[2] + r * dsplit[p][2];
+    dp[O_DIFFUSE] = dr * split[3] + r * dsplit[p][3];
+    dp[O_STRAIGHT] = dt;
+    if (far_opaque) { dp[O_STRAIGHT] = 0.0f; dp[O_REFRACT] = 0.0f; }
+    ddet[p] = da * col[LUMEN_COL_EFF] + a * dc[LUMEN_COL_EFF];
+  }
+}
+
+/* ------------------------------------------------------------------------------------------------- lobes */
+/* Rayleigh: the dipole cosine's inverse CDF (phase.py:50 dipole_cos) and the polarised draw (phase.py:57) */
+static inline float o_dipole_cos(float rand) {
+  float x = 1.0f - 2.0f * rand;
+  x = x < -1.0f ? -1.0f : (x > 1.0f ? 1.0f : x);
+  float s, c;
+  o_sincos((o_acos(x) - O_TWO_PI) / 3.0f, &s, &c);
+  float r = 2.0f * c;
+  return r < -1.0f ? -1.0f : (r > 1.0f ? 1.0f : r);
+}
+static inline void o_rayleigh_sample(const float* er, const float* ei, const float* rand, float* wo) {
+  float a2 = o_dot(er, er);
+  float norm2 = o_dot(er, er) + o_dot(ei, ei);
+  float axis[3];
+  const float* ax = (rand[2] * norm2 < a2) ? er : ei;
+  axis[0] = ax[0]; axis[1] = ax[1]; axis[2] = ax[2];
+  o_unit(axis);
+  float c = o_dipole_cos(rand[0]);
+  float s2 = 1.0f - c * c;
+  float s = s2 > 0.0f ? sqrtf(s2) : 0.0f;
+  float sp, cp;
+  o_sincos2pi(rand[1], &sp, &cp);
+  float l[3] = {s * cp, s * sp, c};
+  o_to_world(l, axis, wo);
+}
+/* Lambert about the facing normal n (lobes.py:55 _cosine) */
+static inline void o_lambert(const float* n, float r0, float r1, float* wo) {
+  float r = sqrtf(r0);
+  float sp, cp;
+  o_sincos2pi(r1, &sp, &cp);
+  float l[3] = {r * cp, r * sp, sqrtf(1.0f - r0)};
+  o_to_world(l, n, wo);
+}
+
+/* the cumulative draw (estimator.py:62 choose): index drawn from q with one uniform, -1 if q is all 0 */
+static inline int o_choose(const float* q, int k, float rand) {
+  float c[8];
+  float s = 0.0f;
+  for (int j = 0; j < k; ++j) { s = j == 0 ? q[0] : s + q[j]; c[j] = s; }
+  if (!(c[k - 1] > 0.0f)) return -1;
+  float thr = rand * c[k - 1];
+  for (int j = 0; j < k; ++j) if (c[j] > thr) return j;
+  return 0;
+}
+
+#endif
