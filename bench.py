@@ -1,0 +1,263 @@
+"""Benchmark: photons/s of the photon-transport hot path on B200 (one JSON line on rank 0).
+
+Workload (the plain-forward tank): a water cylinder of radius 5 m and height 10 m with 2000 inward-facing
+hemispherical PMTs (radius 0.1 m) on a barrel and end-cap grid, black-sheet walls of reflectivity 0.1, water with
+absorption length 50 m, Rayleigh length 80 m and index 1.34; 2^24 photons per GPU per step, wavelength uniform in
+300-600 nm, isotropic from one point drawn uniformly in the inner volume with a fixed host seed; outputs per-PMT
+arrivals, their second moments and 1 ns arrival-time histograms over [0, 200) ns. Synthetic: the detector is built
+from these numbers, the photons drawn from the reference's counter-based stream (seed 0).
+
+A step is one pass of the photon loop over the step's photons (the trace kernel with its FP64 tallies), inputs
+resident on the device. ``e2e`` times the same metric through the public call ``lumen_b200.simulate`` with host
+inputs and outputs (parameter pool and source records host-to-device, tallies device-to-host, every step).
+Multi-GPU: each rank traces its own photon-id range (weak scaling) and the tallies are summed by one NCCL all-reduce.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lumen_b200|reference] [--photons P]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_STEP = 208  # canonical per photon-step: SoA FP32 photon state read + written (104 B each way)
+BYTES_PHOTON = 60  # per photon: its emission row (15 float32)
+BYTES_DEPOSIT = 24  # per sensor deposit: the reference's record (sensor, q, w0, time, lam, photon)
+METRIC = "photons/s on 1 B200 (fwd; batched fwd+adjoint) at matched per-PMT MC error"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_point(seed=12345):
+    rng = np.random.default_rng(seed)
+    while True:
+        p = rng.uniform([-4.8, -4.8, -4.8], [4.8, 4.8, 4.8])
+        if np.hypot(p[0], p[1]) < 4.8:
+            return p
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, index):
+        self.index, self.rows, self.stop_ev = index, [], threading.Event()
+
+    def _run(self):
+        while not self.stop_ev.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self.stop_ev.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop_ev.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if len(r) >= 6 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 6 and r[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 6 for k in range(4) if r[2 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}  # fmt: skip
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def cpu_reference(args, det, src, n_total):
+    """The reference arm / CPU baseline: the C++ restatement of the photon loop on every host thread."""
+    import oracle
+    from lumen_b200 import _abi as A
+
+    threads = os.cpu_count() or 1
+    key = A.key_of_seed(0)
+    oracle.lib()
+    sample = args.cpu_photons
+    oracle.trace(det, key, 1024, source=src, samples=n_total, threads=threads)  # warm-up
+    ts = []
+    for _ in range(max(args.cpu_steps, 1)):
+        t0 = time.perf_counter()
+        oracle.trace(det, key, sample, source=src, samples=n_total, threads=threads)
+        ts.append(time.perf_counter() - t0)
+    dt = float(np.median(ts))
+    return dict(value=sample / dt, unit="photons/s", cores=threads, kind="port",
+                sample=f"{sample} photons of the workload (photon ids 0..{sample - 1}), median of {len(ts)} runs")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lumen_b200")
+    ap.add_argument("--photons", type=int, default=1 << 24)
+    ap.add_argument("--cpu-photons", type=int, default=1 << 17)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    from lumen_b200 import detectors, sources
+
+    det = detectors.cylinder_tank()
+    point = workload_point()
+    n = args.photons
+    src = sources.Point(position=point, n_photons=1.0, lam_range=(300.0, 600.0))
+    cfg = {"workload": "cylinder water tank, 2000 hemispherical PMTs, plain forward, 1 ns time histograms",
+           "photons_per_gpu_per_step": n, "radius_m": 5.0, "height_m": 10.0, "pmts": 2000, "wall_reflectivity": 0.1,
+           "abs_length_m": 50.0, "rayleigh_length_m": 80.0, "rindex": 1.34, "lambda_nm": [300, 600],
+           "source_point_m": [round(float(v), 4) for v in point], "time_bins": [200, 0.0, 1.0],
+           "l2": "flushed between timed steps (256 MiB write)"}  # fmt: skip
+
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        cb = cpu_reference(args, det, src, n)
+        line = {"metric": METRIC, "value": cb["value"], "unit": "photons/s", "n_gpus": args.gpus,
+                "steps": args.cpu_steps, "warmup": 1, "ms_per_step": 1e3 * args.cpu_photons / cb["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": cfg, "impl": "reference", "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    from lumen_b200 import _abi as A
+    from lumen_b200 import api
+    from lumen_b200 import make as engine_build
+    from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
+
+    world, rank, local = dist_setup(args)
+    engine_build.build()
+    dev = torch.device("cuda", local)
+    eng = Engine(det, dev)
+    key = A.key_of_seed(0)
+    first = rank * n  # this rank's photon ids
+    ds = DeviceSource(src, n * world, dev)
+    T = DeviceTallies(det.n_sensor, 1, 200, 0.0, 1.0, 0, dev)
+    c = A.controls()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def one_step():
+        T.zero_()
+        eng.trace(key, n, source=ds, first_id=first, controls=c, tallies=T, stream=stream)
+        if world > 1:
+            import torch.distributed as dist
+
+            for t in (T.arrival, T.arrival_t, T.arrival2, T.hist, T.health):
+                dist.all_reduce(t)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    counts = []
+    with Clocks(local) as clk:
+        torch.cuda.synchronize(dev)
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            one_step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+    ms = [a.elapsed_time(b) for a, b in ev]
+    cnt = T.counts.cpu().numpy()
+    ms_step = float(np.mean(ms))
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * n / (ms_step * 1e-3)
+    steps_pp = cnt[1] / max(cnt[0], 1)
+    # the trace kernel's algorithmic bytes per launch (its own duration: the step without the all-reduce)
+    alg = float(cnt[1]) * BYTES_STEP + float(cnt[0]) * BYTES_PHOTON + float(cnt[2]) * BYTES_DEPOSIT
+    pk, pk_kind = peaks()
+    ach = alg / (ms_step * 1e-3) / 1e9
+    # e2e through the public call, host buffers in and out each step
+    e2e_ms = []
+    for k in range(max(2, args.steps // 2) + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        light = api.simulate(det, src, samples=n, seed=0, time_bins=(200, 0.0, 1.0), device=dev)
+        torch.cuda.synchronize(dev)
+        if k:
+            e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    h2d = det.pool.nbytes + 8 * 4 + 8 + 8 + 4  # the parameter pool and the source's event records
+    d2h = (3 * det.n_sensor + det.n_sensor * 200 + 11) * 8 + 5 * 8
+    e2e_v = n / (np.median(e2e_ms) * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "photon_steps_per_s": world * float(cnt[1]) / (ms_step * 1e-3), "steps_per_photon": steps_pp,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
+                         "traffic": None, "peak_kind": pk_kind,
+                         "algorithmic_bytes": alg},
+            "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps, "clocks": clk.summary(),
+            "arrivals_sum": float(light.arrivals.sum())}  # fmt: skip
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_reference(args, det, src, n)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+"""The public call: ``simulate(det, source, params, *, samples, seed, ...) -> Light``, lumen's signature.
+
+Mirrors ``lumen.simulate`` (src/lumen/api.py:876) and its outputs ``Light`` (:515) and ``Health`` (:445): per sensor
+the expected photon arrivals, their Monte Carlo error from the per-photon second moment
+(src/lumen/readout/grid.py:48 ``moment_error``), the mean arrival time, optional 1 ns (or any width) arrival-time
+histograms, the health fates, and, when asked, the arrivals' derivatives in named parameters. Photon i of a run is
+keyed ``fold_in(PRNGKey(seed), i)`` (src/lumen/run.py:309), so a run is the same whatever its chunking. ``params``
+are the run's live values, ``reference`` the values every draw is made at (src/lumen/transport/estimator.py): with a
+reference held, runs at nearby values share their random numbers (common random numbers for finite differences).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from lumen_b200 import _abi as A
+from lumen_b200.engine import DeviceRows, DeviceSource, DeviceTallies, Engine
+from lumen_b200.sources import FromArrays
+
+MAX_ID = 2**31 - 1  # photon ids are int32 (src/lumen/_core/rng.py:23)
+
+
+@dataclass
+class Health:
+    """What no sensor counted (src/lumen/api.py:445): the fates every start weight ends in, and the counts."""
+
+    lost: float
+    abandoned: float
+    escaped: float
+    distance_cut: float
+    truncated: float
+    absorbed_bulk: float
+    absorbed_surface: float
+    rouletted: float
+    reweighted: float
+    pushed: float
+    records: int
+    photons: int
+    steps: int
+    start: float
+    records_dropped: int = 0
+    records_mismatch: int = 0
+    nonfinite: int = 0
+    invalid: int = 0
+
+    FATES = ("absorbed_bulk", "absorbed_surface", "lost", "escaped", "distance_cut", "abandoned", "truncated",
+             "rouletted", "reweighted")  # fmt: skip
+
+    def balance(self, start=None) -> float:
+        """Return the start weight minus every fate: 0 to float32 rounding per step at the reference values."""
+        s = self.start if start is None else start
+        return float(s) - sum(float(getattr(self, k)) for k in self.FATES)
+
+
+@dataclass
+class Light:
+    """What ``simulate`` returns (src/lumen/api.py:515); with several events every array has a leading event axis."""
+
+    arrivals: np.ndarray
+    arrivals_error: np.ndarray
+    mean_arrival_time: np.ndarray
+    health: Health
+    provenance: dict = field(default_factory=dict)
+    groups: dict | None = None  # {"time": (.., S, bins) arrival-time histograms, "time_edges": (bins + 1,)}
+    gradients: dict | None = None  # {parameter: d arrivals / d value}
+    diagnostics: object = None
+    truth: object = None
+
+    @property
+    def events(self) -> int:
+        return self.arrivals.shape[0] if self.arrivals.ndim == 2 else 0
+
+
+def moment_error(x2, x, n):
+    """Return sqrt(n / (n - 1) (sum x^2 - (sum x)^2 / n)): the standard error of a sum of n i.i.d. photons
+    (src/lumen/readout/grid.py:48)."""  # noqa: D205, D209
+    n = np.asarray(n, np.float64)
+    v = np.maximum(np.asarray(x2) - np.asarray(x) ** 2 / np.maximum(n, 1.0), 0.0)
+    return np.sqrt(n / np.maximum(n - 1.0, 1.0) * v)
+
+
+def _engine(det, device=None) -> Engine:
+    cache = det.__dict__.setdefault("_engines", {})
+    dev = torch.device(device if device is not None else "cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)  # fmt: skip
+    if dev not in cache:
+        cache[dev] = Engine(det, dev)
+    return cache[dev]
+
+
+def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, controls=None, chunk=None,
+             gradients=(), time_bins=None, device=None, stream=None) -> Light:
+    """Return the Light of ``samples`` photons of ``source`` in detector ``det`` (lumen.simulate's signature).
+
+    ``params``: {parameter name: value} overriding the detector's values (``det.params()``); ``reference``: the
+    values the draws are made at (default: ``params``). ``controls``: ``dict(roulette=0.01, max_distance=None,
+    max_vertices=2**22)``. ``chunk``: photons per launch (default: all in one launch). ``gradients``: parameter names
+    whose derivatives of the arrivals are returned (forward tangents of the reweighting estimator along each path).
+    ``time_bins``: (bins, t0, width) ns of the per-sensor arrival-time histograms.
+    """
+    eng = _engine(det, device)
+    live = det.pool_with(params)
+    ref = None if reference is None else det.pool_with({**(params or {}), **reference})
+    eng.set_pools(live, ref)
+    ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22) | (controls or {})
+    gnames = list(gradients)
+    gt = [det.params_index[k] for k in gnames]
+    c = A.controls(ctl["max_distance"] or 0.0, ctl["roulette"], ctl["max_vertices"], gt)
+    if isinstance(source, FromArrays):
+        rows = source.rows()
+        n = len(rows["x"])
+        dsrc, drows, n_ev = None, DeviceRows(rows, eng.device), source.events()
+        total = n
+    else:
+        if samples is None:
+            raise ValueError("simulate: give samples")
+        n = int(samples)
+        dsrc, drows, n_ev = DeviceSource(source, n, eng.device), None, source.events()
+        total = dsrc.total
+    if total > MAX_ID:
+        raise ValueError(f"a run traces at most {MAX_ID} photons (int32 ids)")
+    nb, t0, tw = (0, 0.0, 1.0) if time_bins is None else time_bins
+    T = DeviceTallies(det.n_sensor, n_ev, nb, t0, tw, len(gt), eng.device)
+    key = A.key_of_seed(seed)
+    step = int(chunk) if chunk else total
+    for first in range(0, total, max(step, 1)):
+        m = min(step, total - first)
+        if drows is not None and first > 0:
+            raise ValueError("explicit rows run in one launch")
+        eng.trace(key, m, source=dsrc, rows=drows, first_id=first, controls=c, tallies=T, stream=stream)
+    return _light(det, T, n_ev, total, seed, gnames, (nb, t0, tw), source)
+
+
+def _light(det, T, n_ev, samples, seed, gnames, bins, source):
+    arr = T.arrival.cpu().numpy()
+    arr_t = T.arrival_t.cpu().numpy()
+    arr2 = T.arrival2.cpu().numpy()
+    h = T.health.cpu().numpy()
+    cnt = T.counts.cpu().numpy()
+    if n_ev > 1:
+        per_ev = np.diff(source.arrays(samples)["ev_first"]) if not isinstance(source, FromArrays) else \
+            np.bincount(np.asarray(source.event), minlength=n_ev)  # fmt: skip
+        nn = per_ev[:, None].astype(np.float64)
+    else:
+        arr, arr_t, arr2 = arr[0], arr_t[0], arr2[0]
+        nn = float(samples)
+    err = moment_error(arr2, arr, nn)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        mt = np.where(arr > 0, arr_t / np.where(arr > 0, arr, 1.0), np.nan)
+    health = Health(lost=h[0], abandoned=h[1], escaped=h[2], distance_cut=h[3], absorbed_bulk=h[4],
+                    absorbed_surface=h[5], rouletted=h[6], reweighted=h[7], truncated=h[8], pushed=h[9],
+                    start=h[10], records=int(cnt[2]), photons=int(cnt[0]), steps=int(cnt[1]))  # fmt: skip
+    groups = None
+    if bins[0]:
+        hist = T.hist.cpu().numpy()
+        groups = {"time": hist if n_ev > 1 else hist[0],
+                  "time_edges": bins[1] + bins[2] * np.arange(bins[0] + 1)}  # fmt: skip
+    grads = None
+    if gnames:
+        jac = T.jac.cpu().numpy()
+        grads = {k: (jac[..., i] if n_ev > 1 else jac[0, :, i]) for i, k in enumerate(gnames)}
+    prov = dict(seed=seed, samples=samples, engine="lumen_b200", steps_per_photon=cnt[1] / max(cnt[0], 1))
+    return Light(arr, err, mt, health, prov, groups, grads)
+
+
+def pe(light: Light, qe=None, efficiency=1.0, lam=None):
+    """Return expected photoelectrons per sensor: efficiency x QE(lam) x arrivals (src/lumen/readout/detection.py:86
+    ``expected_pe``) for a source of one wavelength ``lam`` (nm); ``qe`` = (wavelengths nm, values)."""  # noqa: D205
+    q = 1.0 if qe is None else float(np.interp(lam, np.asarray(qe[0], float), np.asarray(qe[1], float)))
+    return np.asarray(efficiency) * q * light.arrivals
+
+
+def seed_key(seed: int):
+    """Return the run key of a seed: jax.random.PRNGKey(seed)'s key data."""
+    return A.key_of_seed(seed)
+
+
+def ceil_pow2(n: int) -> int:
+    return 1 << max(int(math.ceil(math.log2(max(n, 1)))), 0)

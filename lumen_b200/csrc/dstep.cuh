@@ -1,0 +1,408 @@
+// One photon step on the device (src/lumen/transport/step.py:516 `step`, with `_recover` :245, `_step_context` :318,
+// `_surface_event` :362, `_bulk` :397, `_after` :464, `_advance` :495), with forward-mode tangents of the live
+// weight in up to G gradient parameters (the reference's reweighting estimator differentiated along the fixed path).
+// Arithmetic operation for operation the CPU checker's; uniforms are drawn lazily (each is a pure function of the
+// vertex key and its index, so skipping an unused one changes nothing).
+#pragma once
+#include "dphys.cuh"
+
+namespace lb {
+
+#define D_POL_STREAM 0x9017u
+#define D_SOURCE_STREAM 0xFFFFFFFFu
+#define D_NORMAL_LO -0.99999994039535522461f
+#define D_SQRT2 1.41421356237309504880f
+
+struct Run {
+  DScene S;
+  const float* __restrict__ live;
+  const float* __restrict__ ref;
+  int shared;
+  float max_distance, roulette, reach;
+  int max_vertices;
+  int P;
+  int gt[LUMEN_MAX_GRAD];
+};
+
+struct Photon {
+  float x[3], d[3], t, lam, w, wr;
+  int alive, vertex;
+  float er[3], ei[3];
+  int vol, srf;
+  float sn[3];
+  int nz, cls;
+};
+
+struct Dep {
+  int sensor;
+  float q, time;
+  float fates[8];
+  float pushed;
+};
+
+L_DEV float d_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0.0f; }
+
+template <int G>
+L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq) {
+  const DScene& S = R.S;
+  const int P = G > 0 ? R.P : 0;
+  float b0 = d_band(d_maxabs3(ph.x));
+  int stuck = ph.alive && ph.nz >= D_ZSBP;
+  if (stuck) {
+    float pb = D_PUSH_BANDS * b0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) ph.x[a] = ph.x[a] + pb * ph.d[a];
+    ph.vol = d_locate(S, ph.x);
+    ph.cls = d_cls(S, ph.vol);
+    ph.srf = -1;
+  }
+  Key vkey = fold_in(pkey, (uint32_t)ph.vertex);
+  float er0[3] = {ph.er[0], ph.er[1], ph.er[2]}, ei0[3] = {ph.ei[0], ph.ei[1], ph.ei[2]};
+  if (d_dot(er0, er0) + d_dot(ei0, ei0) < D_ZERO_STATE) d_fill(ph.d, er0, ei0, uniform(fold_in(vkey, D_POL_STREAM), 0));
+  int mi = __ldg(S.cls_medium + ph.cls);
+  Med ml = d_medium_at(S, R.live, ph.lam, mi);
+  Med mr = R.shared ? ml : d_medium_at(S, R.ref, ph.lam, mi);
+  float dmu_abs[G > 0 ? G : 1], dmu_c[G > 0 ? G : 1];
+  if (G > 0) {
+    const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
+    int ta = __ldg(m + LUMEN_MI_ABS), tr = __ldg(m + LUMEN_MI_RAY);
+    float E = D_HC / ph.lam;
+    for (int p = 0; p < P; ++p) {
+      dmu_abs[p] = 0.0f;
+      dmu_c[p] = 0.0f;
+      if (ta >= 0 && ta == R.gt[p]) dmu_abs[p] = d_tab(S, R.live, ta, E) >= D_FLT_TINY ? -(ml.mu_abs * ml.mu_abs) : 0.0f;
+      if (tr >= 0 && tr == R.gt[p]) dmu_c[p] = d_tab(S, R.live, tr, E) >= D_FLT_TINY ? -(ml.mu_c * ml.mu_c) : 0.0f;
+    }
+  }
+  float mu_r = mr.mu_c;
+  float s = -l_log(uniform(vkey, 0)) / d_max(mu_r, D_FLOOR32);
+  Query q = d_query(S, ph.x, ph.d, ph.vol, R.max_distance, ph.srf, ph.sn, s);
+  int sensor_q = q.hit ? vI(S, q.vol_after, LUMEN_VI_SENSOR) : -1;
+  float dist = q.t;
+  int zero = dist <= D_ZERO_STEP_BANDS * b0;
+  int cb = q.cls_before, ca = q.cls_after;
+  int row = __ldg(S.row_of + cb * S.n_cls + ca);
+  int cont = (q.cont || (zero && row < 0)) && q.hit;
+  if (cont) row = row > 0 ? row : 0;
+  int mi_after = __ldg(S.cls_medium + ca);
+  float n2l = d_index_at(S, R.live, ph.lam, mi_after);
+  float dprobs[G > 0 ? G : 1][N_OUT], ddet[G > 0 ? G : 1];
+  Eval le, re;
+  d_type_eval<G>(S, R.live, row, ph.lam, ph.d, q.normal, ml.n, n2l, er0, ei0, le, P, R.gt, dprobs, ddet);
+  if (R.shared) re = le;
+  else {
+    float n2r = d_index_at(S, R.ref, ph.lam, mi_after);
+    d_type_eval<0>(S, R.ref, row, ph.lam, ph.d, q.normal, mr.n, n2r, er0, ei0, re, 0, R.gt, dprobs, ddet);
+  }
+  if (cont) {
+#pragma unroll
+    for (int o = 0; o < N_OUT; ++o) { le.probs[o] = o == STRAIGHT; re.probs[o] = o == STRAIGHT; }
+    le.detect = 0.0f;
+    re.detect = 0.0f;
+    if (G > 0)
+      for (int p = 0; p < P; ++p) {
+#pragma unroll
+        for (int o = 0; o < N_OUT; ++o) dprobs[p][o] = 0.0f;
+        ddet[p] = 0.0f;
+      }
+  }
+  float p_prop[N_OUT];
+  float tot = 0.0f;
+#pragma unroll
+  for (int o = 0; o < N_OUT; ++o) tot = o == 0 ? re.probs[0] : tot + re.probs[o];
+#pragma unroll
+  for (int o = 0; o < N_OUT; ++o) p_prop[o] = tot > 0.0f ? re.probs[o] / tot : 0.0f;
+  float mu = ml.mu_c;
+  int scatter = mu_r > 0.0f && s < dist && ph.alive;
+  int oc_ = scatter ? 0 : d_choose6(p_prop, uniform(vkey, 2));
+  int os_ = oc_ > 0 ? oc_ : 0;
+  int drawn = oc_ >= 0;
+  float reach_live = l_exp(-mu * dist), reach_ref = l_exp(-mu_r * dist);
+  float att_if = l_exp(-ml.mu_abs * dist), att_r = l_exp(-mr.mu_abs * dist);
+  float v_g = D_C_VACUUM / ml.ng;
+  int at_if = q.hit && ph.alive && row >= 0;
+  float p_det = le.detect;
+  float rr = d_ratio(reach_live, reach_ref);
+  dep.q = at_if ? ph.w * reach_live * att_if * p_det : 0.0f;
+  float d_reach[G > 0 ? G : 1], d_att[G > 0 ? G : 1];
+  if (G > 0)
+    for (int p = 0; p < P; ++p) {
+      d_reach[p] = -(dmu_c[p] * dist) * reach_live;
+      d_att[p] = -(dmu_abs[p] * dist) * att_if;
+      float f = reach_live * att_if * p_det;
+      float df = d_reach[p] * att_if * p_det + reach_live * d_att[p] * p_det + reach_live * att_if * ddet[p];
+      dq[p] = at_if ? dw[p] * f + ph.w * df : 0.0f;
+    }
+  float lost = (q.hit && ph.alive && row < 0 && !scatter) ? ph.w * rr * att_if : 0.0f;
+  float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_er[3], nx_ei[3];
+  float nx_dw[G > 0 ? G : 1];
+  int nx_cls, nx_ok, nx_far = 0;
+  float fates0, fates1, fates2, wr;
+  if (scatter) {
+    int next_cls = s < q.t_pass0 ? q.cls_start : (s > q.t_pass1 ? cb : d_cls(S, q.vol_at));
+    float mu_c_r = mr.mu_c;
+    float e_r = l_exp(-mu_r * s), e_l = l_exp(-mu * s);
+    float path_r = mu_c_r * e_r;
+    float w_path = d_ratio(ml.mu_c * e_l, path_r);
+    float att = l_exp(-ml.mu_abs * s);
+    float w = w_path * att;
+    float w_r = d_ratio(path_r, path_r) * l_exp(-mr.mu_abs * s);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) nx_x[a] = ph.x[a] + s * ph.d[a];
+    d_rayleigh_sample(er0, ei0, uniform(vkey, 3), uniform(vkey, 4), uniform(vkey, 5), nx_d);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+    d_project(nx_er, nx_ei, nx_d);
+    float w_at = ph.w * w_path;
+    fates0 = w_at * att * 1.0f;
+    fates1 = w_at * (1.0f - att * 1.0f);
+    fates2 = 0.0f;
+    nx_w = ph.w * w * 1.0f * 1.0f;
+    if (G > 0)
+      for (int p = 0; p < P; ++p) {
+        float dwp = (dmu_c[p] * e_l + ml.mu_c * (-(dmu_c[p] * s) * e_l)) / path_r;
+        if (!(path_r != 0.0f)) dwp = 0.0f;
+        float datt = -(dmu_abs[p] * s) * att;
+        float dwf = dwp * att + w_path * datt;
+        nx_dw[p] = dw[p] * w + ph.w * dwf;
+      }
+    nx_cls = next_cls;
+    nx_ok = 1;
+    nx_dtime = s / v_g;
+    wr = ph.wr * w_r * 1.0f;
+  } else {
+    float pl = le.probs[os_], pp = p_prop[os_];
+    float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
+    float w_if = ph.w * rr * att_if * r_live;
+    float dirn[3], wi[3] = {ph.d[0], ph.d[1], ph.d[2]};
+    const float* nrm = q.normal;
+    float eta = ml.n / n2l;
+    float s_ax[3];
+    d_s_axis(wi, nrm, s_ax);
+    Cf es, ep;
+    d_components(er0, ei0, wi, s_ax, &es, &ep);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+    if (os_ == REFRACT) {
+      float cos_i = -d_dot(wi, nrm);
+      float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+      int tir = sin2_t >= 1.0f;
+      float ct2 = 1.0f - sin2_t;
+      float cos_t = ct2 > 0.0f ? sqrtf(ct2) : 0.0f;
+      if (tir) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) dirn[a] = wi[a] + 2.0f * cos_i * nrm[a];
+      } else {
+        float k = eta * cos_i - cos_t;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) dirn[a] = eta * wi[a] + k * nrm[a];
+        d_unit(dirn);
+      }
+      float du[3] = {dirn[0], dirn[1], dirn[2]};
+      d_unit(du);
+      d_recombine(es, ep, le.amps[2], le.amps[3], s_ax, du, nx_er, nx_ei);
+    } else if (os_ == SPECULAR) {
+      float wn = d_dot(wi, nrm);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) dirn[a] = wi[a] - 2.0f * wn * nrm[a];
+      float du[3] = {dirn[0], dirn[1], dirn[2]};
+      d_unit(du);
+      d_recombine(es, ep, le.amps[0], le.amps[1], s_ax, du, nx_er, nx_ei);
+    } else if (os_ == BACKSCATTER) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) { dirn[a] = -wi[a]; nx_er[a] = -er0[a]; nx_ei[a] = -ei0[a]; }
+    } else if (os_ == DIFFUSE) {
+      d_lambert(nrm, uniform(vkey, 3), uniform(vkey, 4), dirn);
+      float h[3] = {dirn[0] - wi[0], dirn[1] - wi[1], dirn[2] - wi[2]};
+      d_unit(h);
+      d_mirror(nx_er, nx_ei, h);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) dirn[a] = wi[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) nx_d[a] = dirn[a];
+    d_unit(nx_d);
+    int far_side = (os_ == STRAIGHT || os_ == REFRACT);
+    int far_ = far_side && drawn;
+    int ok = q.hit && drawn && row >= 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) nx_x[a] = ph.x[a] + q.t * ph.d[a];
+    float r_o = drawn ? (p_prop[os_] != 0.0f ? re.probs[os_] / p_prop[os_] : 0.0f) : 0.0f;
+    wr = ph.wr * (reach_ref != 0.0f ? 1.0f : 0.0f) * att_r * r_o * 1.0f;
+    float w_at = ph.w * rr;
+    float s_cont = 0.0f;
+#pragma unroll
+    for (int o = 0; o < N_OUT; ++o) s_cont = o == 0 ? le.probs[0] : s_cont + le.probs[o];
+    fates0 = ok ? w_at * att_if * s_cont : 0.0f;
+    fates1 = q.hit ? w_at * (1.0f - att_if) : 0.0f;
+    fates2 = (q.hit && row >= 0) ? w_at * att_if * (1.0f - s_cont) : 0.0f;
+    nx_w = w_if * 1.0f;
+    if (G > 0)
+      for (int p = 0; p < P; ++p) {
+        float dpl = dprobs[p][os_];
+        float dr_live = drawn ? (pp != 0.0f ? dpl / pp : 0.0f) : 0.0f;
+        float drr = reach_ref != 0.0f ? d_reach[p] / reach_ref : 0.0f;
+        float X = rr * att_if * r_live;
+        float dX = drr * att_if * r_live + rr * d_att[p] * r_live + rr * att_if * dr_live;
+        nx_dw[p] = (dw[p] * X + ph.w * dX) * 1.0f;
+      }
+    nx_cls = far_ ? ca : cb;
+    nx_ok = ok;
+    nx_dtime = dist / v_g;
+    nx_far = far_;
+  }
+  float a_surf = ph.alive ? fates2 : 0.0f;
+  int far_end = ph.alive && !q.hit && !scatter;
+  float d_end = d_min(dist, R.max_distance);
+  float w_far = ph.w * d_ratio(l_exp(-mu * d_end), l_exp(-mu_r * d_end));
+  float att_far = l_exp(-ml.mu_abs * d_end);
+  int cut = R.max_distance < R.reach;
+  float escaped = (far_end && !cut) ? w_far * att_far : 0.0f;
+  float distance_cut = (far_end && cut) ? w_far * att_far : 0.0f;
+  float a_bulk = (ph.alive ? fates1 : 0.0f) + (far_end ? w_far * (1.0f - att_far) : 0.0f);
+  float reweighted = (ph.alive && nx_ok) ? fates0 - nx_w : 0.0f;
+  float time = ph.t + dist / v_g;
+  float w_new = nx_w;
+  int low = wr < R.roulette;
+  float p_s = wr / R.roulette;
+  int keep = low ? (uniform(vkey, 6) < p_s) : 0;
+  int kept = low && keep, lostr = low && !keep;
+  float p_kept = kept ? p_s : 1.0f;
+  float w_in = w_new;
+  w_new = kept ? w_new / p_kept : (lostr ? 0.0f : w_new);
+  float rouletted = (ph.alive && nx_ok) ? w_in - w_new : 0.0f;
+  float wr_new = kept ? wr / p_kept : (lostr ? 0.0f : wr);
+  int alive = ph.alive && nx_ok && !lostr;
+  int nz_new = (q.hit && !scatter && dist <= D_ZERO_STEP_BANDS * b0) ? ph.nz + 1 : 0;
+  int abandon = alive && nz_new >= D_ZSBK;
+  float abandoned = abandon ? w_new : 0.0f;
+  alive = alive && !abandon;
+  int vol_b = s < q.t_pass0 ? q.vol_start : (s > q.t_pass1 ? q.vol_before : q.vol_at);
+  int vol = scatter ? vol_b : (nx_far ? q.vol_after : q.vol_before);
+  int held = scatter && s <= D_ZERO_STEP_BANDS * b0 && ph.srf >= 0;
+  int srf = held ? ph.srf : ((scatter || !q.hit) ? -1 : q.srf);
+  float pushed = (ph.alive && ph.nz == D_ZSBP) ? ph.w : 0.0f;
+  dep.sensor = at_if ? sensor_q : -1;
+  dep.time = time;
+  dep.fates[0] = lost;
+  dep.fates[1] = abandoned;
+  dep.fates[2] = escaped;
+  dep.fates[3] = distance_cut;
+  dep.fates[4] = a_bulk;
+  dep.fates[5] = a_surf;
+  dep.fates[6] = rouletted;
+  dep.fates[7] = reweighted;
+  dep.pushed = pushed;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { ph.x[a] = nx_x[a]; ph.d[a] = nx_d[a]; ph.er[a] = nx_er[a]; ph.ei[a] = nx_ei[a]; }
+  ph.t = ph.t + nx_dtime;
+  ph.w = alive ? w_new : 0.0f;
+  ph.wr = alive ? wr_new : 0.0f;
+  if (G > 0)
+    for (int p = 0; p < P; ++p) {
+      float v = kept ? nx_dw[p] / p_kept : (lostr ? 0.0f : nx_dw[p]);
+      dw[p] = alive ? v : 0.0f;
+    }
+  ph.alive = alive;
+  ph.vertex += 1;
+  ph.vol = vol;
+  ph.srf = srf;
+  if (!held) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) ph.sn[a] = q.normal[a];
+  }
+  ph.nz = nz_new;
+  ph.cls = nx_cls;
+}
+
+// ------------------------------------------------------------------------------------------------ sources
+struct Row { float x[3], d[3], t, lam, w0, er[3], ei[3]; int event; };
+
+L_DEV float d_gaussian(float u) {
+  float f = u - 5.9604644775390625e-8f;
+  float v = f * (1.0f - D_NORMAL_LO) + D_NORMAL_LO;
+  v = v > D_NORMAL_LO ? v : D_NORMAL_LO;
+  return D_SQRT2 * l_erfinv(v);
+}
+
+L_DEV int d_event_of(const int64_t* first, int n_ev, int64_t gid) {
+  int lo = 0, hi = n_ev - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) / 2;
+    if (__ldg((const long long*)first + mid) <= gid) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+L_DEV void d_source_row(const LumenSource& src, Key key, int64_t gid, Row& r) {
+  Key sk = fold_in(key, D_SOURCE_STREAM);
+  Key rk = fold_in(fold_in(sk, (uint32_t)gid), 0u);
+  int e = d_event_of(src.ev_first, src.n_events, gid);
+  const float* f = src.ev_f + (size_t)e * LUMEN_EV_F;
+  r.event = e;
+  r.w0 = __ldg(src.ev_w + e);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { r.er[a] = 0.0f; r.ei[a] = 0.0f; }
+  if (src.kind == LUMEN_SRC_TRACK) {
+    float u0 = uniform(rk, 0), u1 = uniform(rk, 1), u2 = uniform(rk, 2);
+    float ax[3] = {__ldg(f + 3), __ldg(f + 4), __ldg(f + 5)};
+    float along = u0 * __ldg(f + 6);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.x[a] = __ldg(f + a) + along * ax[a];
+    float c = src.cone_cos;
+    float sn = sqrtf(1.0f - c * c);
+    float sp, cp;
+    l_sincos2pi(u1, &sp, &cp);
+    float l[3] = {sn * cp, sn * sp, c};
+    d_to_world(l, ax, r.d);
+    r.t = __ldg(f + 7) + along / D_C_VACUUM;
+    r.lam = src.lam1 > src.lam0 ? src.lam0 + (src.lam1 - src.lam0) * u2 : src.lam0;
+    float ad = d_dot(ax, r.d);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.er[a] = ad * r.d[a] - ax[a];
+    d_unit(r.er);
+    return;
+  }
+  float g[3] = {d_gaussian(uniform(rk, 0)), d_gaussian(uniform(rk, 1)), d_gaussian(uniform(rk, 2))};
+  d_unit(g);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { r.x[a] = __ldg(f + a); r.d[a] = g[a]; }
+  float u3 = uniform(rk, 3);
+  r.lam = src.lam1 > src.lam0 ? src.lam0 + (src.lam1 - src.lam0) * u3 : src.lam0;
+  r.t = __ldg(f + 3);
+  if (src.kind == LUMEN_SRC_SCINT) {
+    float u4 = uniform(rk, 4), u5 = uniform(rk, 5);
+    float tau = u4 < src.frac1 ? src.tau1 : src.tau2;
+    r.t = __ldg(f + 3) + -l_log(u5) * tau;
+  }
+}
+
+L_DEV void d_rows_row(const LumenRows& rows, int64_t i, Row& r) {
+  r.x[0] = __ldg(rows.x + i); r.x[1] = __ldg(rows.y + i); r.x[2] = __ldg(rows.z + i);
+  r.d[0] = __ldg(rows.dx + i); r.d[1] = __ldg(rows.dy + i); r.d[2] = __ldg(rows.dz + i);
+  r.t = __ldg(rows.t + i); r.lam = __ldg(rows.lam + i); r.w0 = __ldg(rows.w + i);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    r.er[a] = rows.pol ? __ldg(rows.pol + 6 * i + a) : 0.0f;
+    r.ei[a] = rows.pol ? __ldg(rows.pol + 6 * i + 3 + a) : 0.0f;
+  }
+  r.event = rows.event ? __ldg(rows.event + i) : 0;
+}
+
+L_DEV void d_start(const DScene& S, const Row& r, Photon& ph) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { ph.x[a] = r.x[a]; ph.d[a] = r.d[a]; ph.er[a] = r.er[a]; ph.ei[a] = r.ei[a]; ph.sn[a] = 0.0f; }
+  ph.t = r.t;
+  ph.lam = r.lam;
+  ph.w = 1.0f;
+  ph.wr = 1.0f;
+  ph.alive = 1;
+  ph.vertex = 0;
+  ph.vol = d_locate(S, ph.x);
+  ph.cls = d_cls(S, ph.vol);
+  ph.srf = -1;
+  ph.nz = 0;
+}
+
+}  // namespace lb

@@ -1,0 +1,624 @@
+// lumen_b200: the B200 photon-transport engine behind the C ABI of include/lumen_b200.h.
+//
+// The reference's photon loop (src/lumen/run.py:293-368) is a tallymap kernel with one item per photon and a lane
+// refill per step, followed by record launches that fold deposits into per-sensor cells (run.py:443-557). Here one
+// persistent kernel does both: each thread carries one photon in registers, steps it, and when it ends takes the
+// next photon id from a global counter (one atomic per warp, ballot-compacted), so lanes stay busy as paths end at
+// different steps. Deposits go straight into FP64 per-sensor tallies (arrival, arrival x time, time histograms,
+// Jacobian); the per-photon second moment is formed from a four-entry per-thread cache of the photon's per-sensor
+// sums, squared when the photon ends; health fates and counters are reduced per block before their atomics.
+//
+// Numerics: compiled with -fmad=false; every fused multiply-add is an explicit fmaf, every elementary function the
+// library's own (dmath.cuh), so a photon's path is the CPU checker's bit for bit.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/lumen_b200.h"
+#include "dstep.cuh"
+
+using namespace lb;
+
+// ------------------------------------------------------------------------------------------- error handling
+static thread_local std::string g_err;
+static int set_err(int code, const std::string& m) {
+  g_err = m;
+  return code;
+}
+#define CK(call)                                                                               \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return set_err(LUMEN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct LumenScene {
+  DScene S;
+  int dev;
+  float* pool_live;
+  float* pool_ref;  // == pool_live unless a distinct reference is set
+  int n_pool;
+  std::vector<void*> allocs;
+};
+
+// --------------------------------------------------------------------------------------------- the kernels
+struct Tally {
+  int E, S_, nb, P;
+  float bin0, bin_w;
+  double *arrival, *arrival_t, *arrival2, *hist, *jac, *health;
+  unsigned long long* counts;
+  const double* cot;  // the adjoint's cotangent (E * S_) or null
+  double* grads;      // the adjoint's output (P) or null
+};
+
+struct Launch {
+  Run R;
+  LumenRows rows;
+  LumenSource src;
+  int use_rows;
+  Key key;
+  int64_t first_id, n;
+  unsigned long long* next;  // the photon counter
+  int* abort_flag;
+  long long step_budget;
+  unsigned long long* steps_used;
+  Tally T;
+};
+
+#define CACHE 4
+
+template <int G>
+struct PhotonTally {
+  int sensor[CACHE];
+  double sum[CACHE];
+  int n;
+};
+
+__device__ __forceinline__ void flush2(const Tally& T, int e, int s, double v) {
+  if ((unsigned)e >= (unsigned)T.E || (unsigned)s >= (unsigned)T.S_) return;
+  if (T.arrival2) atomicAdd(T.arrival2 + (size_t)e * T.S_ + s, v * v);
+}
+
+template <int G>
+__device__ __forceinline__ void deposit(const Tally& T, int e, const Dep& dep, const float* dq, double w0,
+                                        PhotonTally<G>& pt) {
+  int s = dep.sensor;
+  if ((unsigned)e >= (unsigned)T.E || (unsigned)s >= (unsigned)T.S_) return;  // an event or sensor out of range
+  double v = (double)dep.q * w0;
+  size_t ix = (size_t)e * T.S_ + s;
+  if (T.arrival) {
+    atomicAdd(T.arrival + ix, v);
+    atomicAdd(T.arrival_t + ix, v * (double)dep.time);
+  }
+  if (T.nb > 0) {
+    float b = floorf((dep.time - T.bin0) / T.bin_w);
+    if (b >= 0.0f && b < (float)T.nb) atomicAdd(T.hist + ix * T.nb + (size_t)b, v);
+  }
+  if (G > 0) {
+    if (T.jac)
+      for (int p = 0; p < T.P; ++p) atomicAdd(T.jac + ix * T.P + p, (double)dq[p] * w0);
+    if (T.cot) {
+      double c = T.cot[ix];
+      if (c != 0.0)
+        for (int p = 0; p < T.P; ++p) atomicAdd(T.grads + p, c * (double)dq[p] * w0);
+    }
+  }
+  int j = 0;
+  while (j < pt.n && pt.sensor[j] != s) ++j;
+  if (j == pt.n) {
+    if (pt.n == CACHE) {
+      flush2(T, e, pt.sensor[0], pt.sum[0]);
+      for (int k = 1; k < CACHE; ++k) { pt.sensor[k - 1] = pt.sensor[k]; pt.sum[k - 1] = pt.sum[k]; }
+      pt.n -= 1;
+    }
+    j = pt.n++;
+    pt.sensor[j] = s;
+    pt.sum[j] = 0.0;
+  }
+  pt.sum[j] += v;
+}
+
+__device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
+  if (L.use_rows) d_rows_row(L.rows, i, r);
+  else d_source_row(L.src, L.key, L.first_id + i, r);
+}
+
+// The persistent photon loop: a lane refill per step (src/lumen/run.py:81 SCHEDULE = "step").
+template <int G>
+__global__ void __launch_bounds__(128) k_trace(Launch L) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  Photon ph;
+  float dw[G > 0 ? G : 1], dq[G > 0 ? G : 1];
+  PhotonTally<G> pt;
+  pt.n = 0;
+  Key pkey = {0u, 0u};
+  int active = 0, ev = 0;
+  double w0 = 0.0;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // the current photon's fates
+  double hsum[LUMEN_N_HEALTH];
+  for (int k = 0; k < LUMEN_N_HEALTH; ++k) hsum[k] = 0.0;
+  unsigned long long c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0;
+  int64_t budget_chunk = 0;
+  for (;;) {
+    unsigned need = __ballot_sync(FULL, !active);
+    if (need) {
+      int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      int abort_now = 0;
+      if (lane == leader) {
+        abort_now = L.abort_flag && *(volatile int*)L.abort_flag;
+        base = abort_now ? (unsigned long long)L.n : atomicAdd(L.next, (unsigned long long)__popc(need));
+      }
+      base = __shfl_sync(FULL, base, leader);
+      if (!active) {
+        unsigned long long g = base + __popc(need & ((1u << lane) - 1u));
+        if (g < (unsigned long long)L.n) {
+          Row r;
+          get_row(L, (int64_t)g, r);
+          d_start(L.R.S, r, ph);
+          pkey = fold_in(L.key, (uint32_t)(L.first_id + (int64_t)g));
+          w0 = (double)r.w0;
+          ev = r.event;
+          active = 1;
+          pt.n = 0;
+          for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+          if (G > 0)
+            for (int p = 0; p < L.R.P; ++p) dw[p] = 0.0f;
+        }
+      }
+    }
+    if (__ballot_sync(FULL, active) == 0) break;
+    if (active) {
+      Dep dep;
+      d_step<G>(L.R, ph, dw, pkey, dep, dq);
+      c_steps++;
+      for (int k = 0; k < 8; ++k) acc[k] += (double)dep.fates[k];
+      hsum[LUMEN_H_PUSHED] += (double)dep.pushed * w0;
+      if (dep.sensor >= 0) {
+        deposit<G>(L.T, ev, dep, dq, w0, pt);
+        c_dep++;
+      }
+      if (!ph.alive || ph.vertex >= L.R.max_vertices) {
+        for (int j = 0; j < pt.n; ++j) flush2(L.T, ev, pt.sensor[j], pt.sum[j]);
+        for (int k = 0; k < 8; ++k) hsum[k] += acc[k] * w0;
+        if (ph.alive) {
+          hsum[LUMEN_H_TRUNCATED] += (double)ph.w * w0;
+          c_trunc++;
+        }
+        hsum[LUMEN_H_START] += w0;
+        c_ph++;
+        active = 0;
+      }
+      if (L.step_budget > 0 && ++budget_chunk == 256) {
+        unsigned long long used = atomicAdd(L.steps_used, 256ull) + 256ull;
+        if (used > (unsigned long long)L.step_budget) atomicExch(L.abort_flag, 1);
+        budget_chunk = 0;
+      }
+      if (L.abort_flag && *(volatile int*)L.abort_flag) active = 0;
+    }
+  }
+  // block reduction of the health and the counters, then one atomic per block and value
+  __shared__ double sh[LUMEN_N_HEALTH][4];
+  __shared__ unsigned long long sc[LUMEN_N_COUNT][4];
+  const int warp = threadIdx.x >> 5;
+  for (int k = 0; k < LUMEN_N_HEALTH; ++k) {
+    double v = hsum[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+    if (lane == 0) sh[k][warp] = v;
+  }
+  unsigned long long cv[LUMEN_N_COUNT] = {c_ph, c_steps, c_dep, c_trunc, c_multi};
+  for (int k = 0; k < LUMEN_N_COUNT; ++k) {
+    unsigned long long v = cv[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+    if (lane == 0) sc[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < LUMEN_N_HEALTH) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[threadIdx.x][w];
+    if (v != 0.0) atomicAdd(L.T.health + threadIdx.x, v);
+  } else if (threadIdx.x >= 32 && threadIdx.x < 32 + LUMEN_N_COUNT) {
+    int k = threadIdx.x - 32;
+    unsigned long long v = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sc[k][w];
+    if (v) atomicAdd(L.T.counts + k, v);
+  }
+}
+
+// One thread per photon to its end: the per-photon record the parity tests compare exactly.
+__global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  Row r;
+  get_row(L, i, r);
+  Photon ph;
+  d_start(L.R.S, r, ph);
+  Key pkey = fold_in(L.key, (uint32_t)(L.first_id + i));
+  float dw[1], dq[1];
+  int n_dep = 0, first_sensor = -1;
+  double sum_q = 0.0, sum_qt = 0.0;
+  while (ph.alive && ph.vertex < L.R.max_vertices) {
+    Dep dep;
+    d_step<0>(L.R, ph, dw, pkey, dep, dq);
+    if (dep.sensor >= 0) {
+      n_dep++;
+      if (first_sensor < 0) first_sensor = dep.sensor;
+      sum_q += (double)dep.q;
+      sum_qt += (double)dep.q * (double)dep.time;
+    }
+  }
+  out_i[5 * i + 0] = ph.vertex;
+  out_i[5 * i + 1] = n_dep;
+  out_i[5 * i + 2] = ph.alive ? 0 : 1;
+  out_i[5 * i + 3] = first_sensor;
+  out_i[5 * i + 4] = ph.vol;
+  out_f[4 * i + 0] = (float)sum_q;
+  out_f[4 * i + 1] = ph.w;
+  out_f[4 * i + 2] = ph.t;
+  out_f[4 * i + 3] = (float)sum_qt;
+}
+
+__global__ void k_query(DScene S, const float* ray, const int32_t* vol, const int32_t* srf, float t_max, int64_t n,
+                        int32_t* out_i, float* out_f) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float o[3] = {ray[6 * i], ray[6 * i + 1], ray[6 * i + 2]};
+  float d[3] = {ray[6 * i + 3], ray[6 * i + 4], ray[6 * i + 5]};
+  int known = vol[i] >= 0 && vol[i] <= S.n;
+  int v = known ? vol[i] : d_locate(S, o);
+  int last = known ? srf[i] : -1;
+  Query q = d_query(S, o, d, v, t_max, last, nullptr, D_HUGE);
+  int32_t* oi = out_i + 8 * i;
+  oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
+  oi[5] = q.srf; oi[6] = q.zero;
+  oi[7] = q.hit ? vI(S, q.vol_after, LUMEN_VI_SENSOR) : -1;
+  float* of = out_f + 4 * i;
+  of[0] = q.t; of[1] = q.normal[0]; of[2] = q.normal[1]; of[3] = q.normal[2];
+}
+
+__global__ void k_locate(DScene S, const float* pts, int64_t n, int32_t* vol) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float x[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+  vol[i] = d_locate(S, x);
+}
+
+// ------------------------------------------------------------------------------------------- host helpers
+static int upload_raw(LumenScene* sc, const void* h, size_t bytes, void** out) {
+  *out = nullptr;
+  if (bytes == 0 || !h) return 0;
+  void* p = nullptr;
+  CK(cudaMalloc(&p, bytes));
+  sc->allocs.push_back(p);
+  CK(cudaMemcpy(p, h, bytes, cudaMemcpyHostToDevice));
+  *out = p;
+  return 0;
+}
+#define UPLOAD(field, host, count)                                                  \
+  do {                                                                              \
+    void* p_ = nullptr;                                                             \
+    e |= upload_raw(sc, (host), (size_t)(count) * sizeof(*(host)), &p_);           \
+    field = (decltype(field))p_;                                                    \
+  } while (0)
+
+static int check_desc(const LumenSceneDesc* d) {
+  if (!d || d->n_vol <= 0 || !d->vol_i || !d->vol_f || !d->kind_i || !d->leaf_f || !d->leaf_i || !d->prog_i ||
+      !d->cls_medium || !d->row_of || !d->med_i || !d->tab || !d->pool || d->n_cls <= 0 || d->n_pool <= 0)
+    return set_err(LUMEN_ERR_ARG, "scene_create: a required array is null or empty");
+  for (int k = 0; k < d->n_kind; ++k) {
+    int nl = d->kind_i[k * LUMEN_KIND_I + 1];
+    if (nl < 1 || nl > LUMEN_MAX_LEAVES) return set_err(LUMEN_ERR_SCENE, "scene_create: a solid has too many leaves");
+  }
+  for (int g = 0; g < d->n_leaf; ++g)
+    if (d->leaf_i[g * LUMEN_LEAF_I + 2] > LUMEN_MAX_PLANES)
+      return set_err(LUMEN_ERR_SCENE, "scene_create: a leaf has too many planes");
+  for (int t = 0; t < d->n_tab; ++t) {
+    int off = d->tab[2 * t], k = d->tab[2 * t + 1];
+    if (k < 1 || off < 0 || off + 2 * k > d->n_pool) return set_err(LUMEN_ERR_ARG, "scene_create: a table is out of the pool");
+  }
+  for (int m = 0; m < d->n_med; ++m) {
+    int ti = d->med_i[m * LUMEN_MED_I + LUMEN_MI_INDEX];
+    if (ti >= 0 && d->tab[2 * ti + 1] > LUMEN_MAX_KNOTS) return set_err(LUMEN_ERR_SCENE, "scene_create: an index table has too many knots");
+  }
+  for (int v = 0; v <= d->n_vol; ++v) {
+    const int32_t* vi = d->vol_i + (size_t)v * LUMEN_VOL_I;
+    if (vi[LUMEN_VI_SENSOR] >= d->n_sensor) return set_err(LUMEN_ERR_ARG, "scene_create: a sensor index is out of range");
+    if (vi[LUMEN_VI_CLS] < 0 || vi[LUMEN_VI_CLS] >= d->n_cls) return set_err(LUMEN_ERR_ARG, "scene_create: a class is out of range");
+    if (v < d->n_vol && (vi[LUMEN_VI_KIND] < 0 || vi[LUMEN_VI_KIND] >= d->n_kind)) return set_err(LUMEN_ERR_ARG, "scene_create: a kind is out of range");
+    if (vi[LUMEN_VI_NODE0] < 0 || vi[LUMEN_VI_NODE1] > d->n_node || vi[LUMEN_VI_NODE0] > vi[LUMEN_VI_NODE1]) return set_err(LUMEN_ERR_ARG, "scene_create: a BVH range is out of range");
+  }
+  for (int c = 0; c < d->n_cls; ++c)
+    if (d->cls_medium[c] < 0 || d->cls_medium[c] >= d->n_med) return set_err(LUMEN_ERR_ARG, "scene_create: a medium is out of range");
+  for (int r = 0; r < d->n_row; ++r) {
+    /* the facet lobe (GLOSSY with sigma_alpha > 0) is not built: such a row is refused */
+    const int32_t* ri = d->row_i + r * LUMEN_ROW_I;
+    int tl = ri[LUMEN_RI_COL + LUMEN_COL_PLOBE];
+    int off = d->tab[2 * tl], k = d->tab[2 * tl + 1];
+    float pl = 0.0f;
+    for (int j = 0; j < k; ++j) pl = pl > d->pool[off + k + j] ? pl : d->pool[off + k + j];
+    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && pl > 0.0f)
+      return set_err(LUMEN_ERR_SCENE, "scene_create: a surface row draws the unified facet lobe (not built)");
+  }
+  return 0;
+}
+
+static int fill_run(const LumenScene* sc, const LumenControls* c, Run& R) {
+  if (!c) return set_err(LUMEN_ERR_ARG, "controls is null");
+  if (!(c->roulette > 0.0f)) return set_err(LUMEN_ERR_ARG, "the roulette's epsilon must be > 0");
+  if (c->n_grad < 0 || c->n_grad > LUMEN_MAX_GRAD) return set_err(LUMEN_ERR_NOT_SUPPORTED, "too many gradient parameters");
+  if (c->max_vertices < 1) return set_err(LUMEN_ERR_ARG, "max_vertices must be >= 1");
+  R.S = sc->S;
+  R.live = sc->pool_live;
+  R.ref = sc->pool_ref;
+  R.shared = sc->pool_ref == sc->pool_live;
+  R.reach = sc->S.reach;
+  R.max_distance = c->max_distance > 0.0f ? c->max_distance : sc->S.reach;
+  R.roulette = c->roulette;
+  R.max_vertices = c->max_vertices;
+  R.P = c->n_grad;
+  for (int p = 0; p < LUMEN_MAX_GRAD; ++p) R.gt[p] = p < c->n_grad ? c->grad_tab[p] : -1;
+  return 0;
+}
+
+static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t k0,
+                       uint32_t k1, int64_t first_id, int64_t n, const LumenControls* c, Launch& L) {
+  memset(&L, 0, sizeof(L));
+  if (!sc) return set_err(LUMEN_ERR_ARG, "scene is null");
+  if ((rows == nullptr) == (source == nullptr)) return set_err(LUMEN_ERR_ARG, "give exactly one of rows / source");
+  if (n < 0 || first_id < 0 || first_id + n > 2147483647LL) return set_err(LUMEN_ERR_ARG, "photon ids must fit int32");
+  int st = fill_run(sc, c, L.R);
+  if (st) return st;
+  if (rows) {
+    if (!rows->x || !rows->y || !rows->z || !rows->dx || !rows->dy || !rows->dz || !rows->t || !rows->lam || !rows->w)
+      return set_err(LUMEN_ERR_ARG, "rows: a required array is null");
+    L.rows = *rows;
+    L.use_rows = 1;
+  } else {
+    if (source->n_events < 1 || !source->ev_f || !source->ev_first || !source->ev_w)
+      return set_err(LUMEN_ERR_ARG, "source: events are missing");
+    if (source->kind < 0 || source->kind > 2) return set_err(LUMEN_ERR_ARG, "source: unknown kind");
+    L.src = *source;
+  }
+  L.key.k0 = k0;
+  L.key.k1 = k1;
+  L.first_id = first_id;
+  L.n = n;
+  L.step_budget = c->step_budget;
+  return 0;
+}
+
+static int grid_for(const void* fn, int block, int* grid) {
+  int dev = 0, sms = 0, per = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0));
+  *grid = sms * (per > 0 ? per : 1);
+  return 0;
+}
+
+static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
+                     cudaStream_t stream) {
+  Tally& T = L.T;
+  T.E = out ? (out->n_events > 0 ? out->n_events : 1) : (n_events_cot > 0 ? n_events_cot : 1);
+  T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
+  T.P = L.R.P;
+  T.cot = cot;
+  T.grads = grads;
+  // scratch: the photon counter, the abort flag and the steps used (one small allocation per call)
+  unsigned long long* scratch = nullptr;
+  CK(cudaMallocAsync((void**)&scratch, 4 * sizeof(unsigned long long), stream));
+  CK(cudaMemsetAsync(scratch, 0, 4 * sizeof(unsigned long long), stream));
+  L.next = scratch;
+  L.abort_flag = (int*)(scratch + 1);
+  L.steps_used = scratch + 2;
+  // adjoint calls with no tallies of their own accumulate health and counts into the scratch's tail
+  double* dummy = nullptr;
+  if (!out) {
+    CK(cudaMallocAsync((void**)&dummy, (LUMEN_N_HEALTH + LUMEN_N_COUNT + 3) * sizeof(double), stream));
+    CK(cudaMemsetAsync(dummy, 0, (LUMEN_N_HEALTH + LUMEN_N_COUNT + 3) * sizeof(double), stream));
+    T.nb = 0;
+    T.arrival = T.arrival_t = T.arrival2 = nullptr;
+  } else {
+    T.nb = out->hist ? out->n_bins : 0;
+    T.bin0 = out->bin0;
+    T.bin_w = out->bin_w;
+    T.arrival = out->arrival;
+    T.arrival_t = out->arrival_t;
+    T.arrival2 = out->arrival2;
+    T.hist = out->hist;
+    T.jac = out->jac;
+    T.health = out->health;
+    T.counts = out->counts;
+  }
+  int st = 0;
+  const int block = 128;
+  int grid = 0;
+  if (L.n > 0) {
+    if (L.R.P > 0 || cot) {
+      if ((st = grid_for((const void*)k_trace<LUMEN_MAX_GRAD>, block, &grid))) return st;
+      if (!out) {
+        // an adjoint without tallies: a launch whose tallies are scratch (the arrival arrays are not written)
+        Launch L2 = L;
+        L2.T.health = dummy;
+        L2.T.counts = (unsigned long long*)(dummy + LUMEN_N_HEALTH);
+        k_trace<LUMEN_MAX_GRAD><<<grid, block, 0, stream>>>(L2);
+      } else {
+        k_trace<LUMEN_MAX_GRAD><<<grid, block, 0, stream>>>(L);
+      }
+    } else {
+      if ((st = grid_for((const void*)k_trace<0>, block, &grid))) return st;
+      k_trace<0><<<grid, block, 0, stream>>>(L);
+    }
+    CK(cudaGetLastError());
+  }
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaFreeAsync(scratch, stream));
+  if (dummy) CK(cudaFreeAsync(dummy, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (flag) return set_err(LUMEN_ERR_STEP_BUDGET, "the call's step budget ran out before every photon ended");
+  return 0;
+}
+
+// ------------------------------------------------------------------------------------------------- the ABI
+extern "C" {
+
+int32_t lumen_b200_abi_version(void) { return LUMEN_B200_ABI_VERSION; }
+
+const char* lumen_b200_last_error(void) { return g_err.c_str(); }
+
+int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
+  g_err.clear();
+  if (!out) return set_err(LUMEN_ERR_ARG, "out is null");
+  *out = nullptr;
+  int st = check_desc(d);
+  if (st) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(LUMEN_ERR_NO_DEVICE, "no CUDA device");
+  LumenScene* sc = new LumenScene();
+  CK(cudaGetDevice(&sc->dev));
+  DScene& S = sc->S;
+  S.n = d->n_vol;
+  S.LM = 1;
+  S.FM = 1;
+  for (int k = 0; k < d->n_kind; ++k) {
+    int l0 = d->kind_i[k * LUMEN_KIND_I], nl = d->kind_i[k * LUMEN_KIND_I + 1];
+    if (nl > S.LM) S.LM = nl;
+    for (int l = 0; l < nl; ++l) {
+      int np_ = d->leaf_i[(l0 + l) * LUMEN_LEAF_I + 2];
+      if (np_ + 1 > S.FM) S.FM = np_ + 1;
+    }
+  }
+  S.SU = d->n_vol + 1;
+  S.n_cls = d->n_cls;
+  S.n_sensor = d->n_sensor;
+  S.reach = d->reach;
+  int e = 0;
+  UPLOAD(S.vol_i, d->vol_i, (size_t)(d->n_vol + 1) * LUMEN_VOL_I);
+  UPLOAD(S.vol_f, d->vol_f, (size_t)d->n_vol * LUMEN_VOL_F);
+  UPLOAD(S.cand, d->cand, (size_t)d->n_cand);
+  UPLOAD(S.node_f, d->node_f, (size_t)d->n_node * LUMEN_NODE_F);
+  UPLOAD(S.node_i, d->node_i, (size_t)d->n_node * LUMEN_NODE_I);
+  UPLOAD(S.items, d->items, (size_t)d->n_item);
+  UPLOAD(S.kind_i, d->kind_i, (size_t)d->n_kind * LUMEN_KIND_I);
+  UPLOAD(S.leaf_f, d->leaf_f, (size_t)d->n_leaf * LUMEN_LEAF_F);
+  UPLOAD(S.leaf_i, d->leaf_i, (size_t)d->n_leaf * LUMEN_LEAF_I);
+  UPLOAD(S.plane_f, d->plane_f, (size_t)d->n_plane * LUMEN_PLANE_F);
+  UPLOAD(S.prog_i, d->prog_i, (size_t)d->n_prog * LUMEN_PROG_I);
+  UPLOAD(S.cls_medium, d->cls_medium, (size_t)d->n_cls);
+  UPLOAD(S.row_of, d->row_of, (size_t)d->n_cls * d->n_cls);
+  UPLOAD(S.med_i, d->med_i, (size_t)d->n_med * LUMEN_MED_I);
+  UPLOAD(S.row_i, d->row_i, (size_t)d->n_row * LUMEN_ROW_I);
+  UPLOAD(S.tab, d->tab, (size_t)d->n_tab * 2);
+  const float* pl = nullptr;
+  UPLOAD(pl, d->pool, (size_t)d->n_pool);
+  if (e) {
+    for (void* p : sc->allocs) cudaFree(p);
+    delete sc;
+    return LUMEN_ERR_CUDA;
+  }
+  sc->pool_live = const_cast<float*>(pl);
+  sc->pool_ref = sc->pool_live;
+  sc->n_pool = d->n_pool;
+  *out = sc;
+  return 0;
+}
+
+int32_t lumen_b200_scene_set_pools(LumenScene* sc, const float* live, const float* ref) {
+  g_err.clear();
+  if (!sc || !live) return set_err(LUMEN_ERR_ARG, "scene or live pool is null");
+  CK(cudaMemcpy(sc->pool_live, live, sc->n_pool * sizeof(float), cudaMemcpyHostToDevice));
+  if (ref && ref != live) {
+    if (sc->pool_ref == sc->pool_live) {
+      void* p = nullptr;
+      CK(cudaMalloc(&p, sc->n_pool * sizeof(float)));
+      sc->allocs.push_back(p);
+      sc->pool_ref = (float*)p;
+    }
+    CK(cudaMemcpy(sc->pool_ref, ref, sc->n_pool * sizeof(float), cudaMemcpyHostToDevice));
+  } else {
+    sc->pool_ref = sc->pool_live;
+  }
+  return 0;
+}
+
+int32_t lumen_b200_scene_destroy(LumenScene* sc) {
+  g_err.clear();
+  if (!sc) return 0;
+  for (void* p : sc->allocs) cudaFree(p);
+  delete sc;
+  return 0;
+}
+
+int32_t lumen_b200_trace(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
+                         uint32_t key1, int64_t first_id, int64_t n, const LumenControls* c, LumenTallies* out,
+                         void* stream) {
+  g_err.clear();
+  if (!out || !out->arrival || !out->arrival_t || !out->arrival2 || !out->health || !out->counts)
+    return set_err(LUMEN_ERR_ARG, "tallies: a required output is null");
+  if (c && c->n_grad > 0 && !out->jac) return set_err(LUMEN_ERR_ARG, "tallies: jac is null with gradient parameters");
+  if (out->hist && (out->n_bins <= 0 || !(out->bin_w > 0.0f))) return set_err(LUMEN_ERR_ARG, "tallies: bad histogram");
+  if (source && out->n_events < source->n_events) return set_err(LUMEN_ERR_ARG, "tallies: fewer events than the source's");
+  Launch L;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  if (st) return st;
+  return run_trace(L, out, nullptr, 0, nullptr, (cudaStream_t)stream);
+}
+
+int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
+                           uint32_t key1, int64_t first_id, int64_t n, const LumenControls* c,
+                           const double* cotangent, int32_t n_events, double* grads, void* stream) {
+  g_err.clear();
+  if (!cotangent || !grads) return set_err(LUMEN_ERR_ARG, "adjoint: cotangent and grads are required");
+  if (!c || c->n_grad <= 0) return set_err(LUMEN_ERR_ARG, "adjoint: no gradient parameters");
+  Launch L;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  if (st) return st;
+  return run_trace(L, nullptr, cotangent, n_events, grads, (cudaStream_t)stream);
+}
+
+int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, const LumenSource* source,
+                                 uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
+                                 const LumenControls* c, int32_t* out_i, float* out_f, void* stream) {
+  g_err.clear();
+  if (!out_i || !out_f) return set_err(LUMEN_ERR_ARG, "trace_photons: outputs are null");
+  Launch L;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  if (st) return st;
+  if (n == 0) return 0;
+  int block = 128;
+  int64_t grid = (n + block - 1) / block;
+  k_trace_photons<<<(unsigned)grid, block, 0, (cudaStream_t)stream>>>(L, out_i, out_f);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return 0;
+}
+
+int32_t lumen_b200_query(const LumenScene* sc, const float* ray, const int32_t* vol, const int32_t* srf, float t_max,
+                         int64_t n, int32_t* out_i, float* out_f, void* stream) {
+  g_err.clear();
+  if (!sc || !ray || !vol || !srf || !out_i || !out_f) return set_err(LUMEN_ERR_ARG, "query: a pointer is null");
+  if (n == 0) return 0;
+  int block = 128;
+  k_query<<<(unsigned)((n + block - 1) / block), block, 0, (cudaStream_t)stream>>>(sc->S, ray, vol, srf, t_max, n,
+                                                                                    out_i, out_f);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return 0;
+}
+
+int32_t lumen_b200_locate(const LumenScene* sc, const float* pts, int64_t n, int32_t* vol, void* stream) {
+  g_err.clear();
+  if (!sc || !pts || !vol) return set_err(LUMEN_ERR_ARG, "locate: a pointer is null");
+  if (n == 0) return 0;
+  int block = 128;
+  k_locate<<<(unsigned)((n + block - 1) / block), block, 0, (cudaStream_t)stream>>>(sc->S, pts, n, vol);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return 0;
+}
+
+}  // extern "C"

@@ -583,12 +583,34 @@ static inline OBest o_unit_visit(const OScene* S, const OCtx* c, int i, OBest b,
   return b;
 }
 
-/* the photon's next event in volume v: its own exit, then every daughter's first entry (navigate.py:482 enter) */
+/* the ray's slab test against volume i's padded world box (bvh.py:258 slab; navigate.py:424 _meets) */
+static inline int o_meets_box(const OScene* S, const OCtx* c, int i, const float* inv) {
+  const float* f = o_vf(S, i);
+  float lo_t = -O_HUGE * 10.0f, hi_t = O_HUGE * 10.0f;
+  for (int a = 0; a < 3; ++a) {
+    float ta = (f[LUMEN_VF_LO + a] - c->od[a]) * inv[a];
+    float tb = (f[LUMEN_VF_HI + a] - c->od[a]) * inv[a];
+    lo_t = o_max(lo_t, o_min(ta, tb));
+    hi_t = o_min(hi_t, o_max(ta, tb));
+  }
+  return lo_t <= hi_t && hi_t >= c->t_lo && lo_t <= c->t_bound + c->band;
+}
+
+/* the photon's next event in volume v: its own exit, then the first entry of every daughter whose box the ray meets
+   (navigate.py:482 enter; the winner does not depend on the order of the daughters) */
 static inline OBest o_enter(const OScene* S, const OCtx* c, int has_own, int vi) {
   OBest b = {O_HUGE, -1, -1, -1, 0, 0};
   if (has_own) b = o_unit_visit(S, c, vi, b, 1);
+  float inv[3];
+  for (int a = 0; a < 3; ++a) {
+    float dv = c->dd[a];
+    inv[a] = 1.0f / (fabsf(dv) < O_TINY_DIR ? (dv < 0.0f ? -O_TINY_DIR : O_TINY_DIR) : dv);
+  }
   const int32_t* vr = o_vi(S, c->v);
-  for (int k = 0; k < vr[LUMEN_VI_CN]; ++k) b = o_unit_visit(S, c, S->D->cand[vr[LUMEN_VI_C0] + k], b, 0);
+  for (int k = 0; k < vr[LUMEN_VI_CN]; ++k) {
+    int i = S->D->cand[vr[LUMEN_VI_C0] + k];
+    if (o_meets_box(S, c, i, inv)) b = o_unit_visit(S, c, i, b, 0);
+  }
   return b;
 }
 

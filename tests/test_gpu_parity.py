@@ -1,0 +1,147 @@
+"""Parity of the CUDA engine with the CPU checker (the oracle), through the C ABI, on the same seeded inputs.
+
+The engine evaluates each photon's path with the checker's arithmetic, operation for operation, so per-photon
+records (vertices, deposits, end, first sensor hit, last volume, and the float sums) must agree bit for bit; the FP64
+tallies agree to their summation order (atomics on the GPU, per-thread partial sums on the CPU): rel 1e-9.
+Navigator queries on fixed ray sets: hit, volumes, classes, surface codes and sensors bit-exact, t and the normal
+bit-exact (a stated tolerance of 0 ulp).
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from lumen_b200 import _abi as A
+from lumen_b200 import detectors, sources
+from lumen_b200.engine import DeviceRows, DeviceSource, DeviceTallies, Engine
+
+pytestmark = pytest.mark.gpu
+
+KEY = A.key_of_seed(0)
+RTOL = 1e-9  # FP64 tallies: summation order only
+
+
+@pytest.fixture(scope="module")
+def toy():
+    return detectors.toy_tank()
+
+
+@pytest.fixture(scope="module")
+def tank():
+    return detectors.cylinder_tank()
+
+
+@pytest.fixture(scope="module")
+def lar():
+    return detectors.lar_box()
+
+
+def _engine(det):
+    from lumen_b200 import make as build
+
+    build.build()
+    return Engine(det)
+
+
+def _records_match(det, src, n, samples=None, controls=None):
+    eng = _engine(det)
+    c = controls or A.controls()
+    ds = DeviceSource(src, samples or n)
+    gi, gf = eng.trace_photons(KEY, n, source=ds, controls=c)
+    gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+    _, (oi, of) = oracle.trace(det, KEY, n, source=src, samples=samples or n, records=True, controls=c)
+    bad = np.flatnonzero((gi != oi).any(1) | (gf.view(np.uint32) != of.view(np.uint32)).any(1))
+    return bad, gi, oi, gf, of
+
+
+def test_toy_tank_photons_bit_exact(toy, built):
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    bad, gi, oi, gf, of = _records_match(toy, src, 1 << 16, samples=1 << 18)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+def test_cylinder_tank_photons_bit_exact(tank, built):
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    bad, gi, oi, gf, of = _records_match(tank, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+def test_lar_box_photons_bit_exact(lar, built):
+    src = sources.Scintillation(position=[(0.3, 0.2, -0.4)], lam=128.0, tau=(6.0, 1500.0), fraction=0.25)
+    bad, gi, oi, gf, of = _records_match(lar, src, 1 << 11)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+def _tallies(det, src, n, controls=None, n_bins=0, pools=None):
+    eng = _engine(det)
+    if pools is not None:
+        eng.set_pools(*pools)
+    c = controls or A.controls()
+    ds = DeviceSource(src, n)
+    T = DeviceTallies(det.n_sensor, ds.n_events, n_bins, 0.0, 1.0, c.n_grad)
+    eng.trace(KEY, n, source=ds, controls=c, tallies=T)
+    O, _ = oracle.trace(det, KEY, n, source=src, samples=n, controls=c, n_events=ds.n_events, n_bins=n_bins,
+                        bin_w=1.0, pool_live=None if pools is None else pools[0],
+                        pool_ref=None if pools is None else pools[1])
+    return T, O
+
+
+def test_toy_tank_tallies_match(toy, built):
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    T, O = _tallies(toy, src, 1 << 18, n_bins=20)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL)
+    np.testing.assert_allclose(T.arrival_t.cpu().numpy(), O.arrival_t, rtol=RTOL)
+    np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
+    np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
+    np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-7, atol=1e-6)
+    assert (T.counts.cpu().numpy()[:4] == O.counts.astype(np.int64)[:4]).all()
+
+
+def test_tank_tallies_and_gradients_match(tank, built):
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R"]
+    c = A.controls(grad_tabs=[tank.params_index[k] for k in names])
+    T, O = _tallies(tank, src, 1 << 15, controls=c, n_bins=200)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+    assert (T.counts.cpu().numpy()[:4] == O.counts.astype(np.int64)[:4]).all()
+
+
+def test_reference_run_matches(tank, built):
+    """A run at live values other than the reference (draws at the reference, weights live / reference)."""
+    src = sources.Point(position=(0.0, 2.0, -1.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    live = tank.pool_with({"media/Water/absorption": 45.0, "surfaces/BlackSheet/R": 0.12})
+    T, O = _tallies(tank, src, 1 << 14, pools=(live, tank.pool))
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
+
+
+def test_batched_tracks_match(tank, built):
+    rng = np.random.default_rng(3)
+    e = 16
+    u = rng.normal(size=(e, 3))
+    src = sources.Tracks(start=rng.uniform(-3, 3, (e, 3)), direction=u, length=rng.uniform(0.5, 3.0, e),
+                         lam_range=(300.0, 600.0), counts_=rng.integers(100, 2000, e))
+    n = int(src.counts(0).sum())
+    T, O = _tallies(tank, src, n)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+
+
+@pytest.mark.parametrize("which", ["toy", "tank", "lar"])
+def test_query_and_locate_bit_exact(which, toy, tank, lar, built):
+    det = {"toy": toy, "tank": tank, "lar": lar}[which]
+    rng = np.random.default_rng(7)
+    n = 20000
+    lo, hi = det.arrays["vol_f"][0, 12:15], det.arrays["vol_f"][0, 15:18]
+    o = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    eng = _engine(det)
+    gi, gf = eng.query(o, d)
+    oi, of = oracle.query(det, o, d)
+    gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+    assert (gi == oi).all(), np.flatnonzero((gi != oi).any(1))[:10]
+    assert (gf.view(np.uint32) == of.view(np.uint32)).all()
+    gv = eng.locate(o).cpu().numpy()
+    assert (gv == oracle.locate(det, o)).all()
