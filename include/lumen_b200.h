@@ -76,9 +76,10 @@ enum { LUMEN_MI_INDEX = 0, LUMEN_MI_ABS = 1, LUMEN_MI_RAY = 2, LUMEN_MED_I = 4 }
    pool[off+k .. off+2k) values; linear in photon energy between knots, held beyond (G4PhysicsVector::Value) */
 
 #define LUMEN_MAX_GRAD 8      /* gradient parameters per call */
-#define LUMEN_MAX_LEAVES 16   /* leaves per solid */
+#define LUMEN_MAX_LEAVES 8    /* leaves per solid */
 #define LUMEN_MAX_PLANES 8    /* planes per leaf */
 #define LUMEN_MAX_KNOTS 64    /* knots of an index table (its group index is tabulated per call) */
+#define LUMEN_MAX_BVH_DEPTH 24 /* levels of a volume's daughter BVH (the traversal's stack) */
 
 /* ------------------------------------------------------------------------------------------ the detector */
 typedef struct LumenSceneDesc {

@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB = os.path.join(HERE, "liblumen_b200.so")
+LIB = os.environ.get("LUMEN_B200_LIB") or os.path.join(HERE, "liblumen_b200.so")  # a library built elsewhere: env
 
 c_i32p = ctypes.POINTER(ctypes.c_int32)
 c_f32p = ctypes.POINTER(ctypes.c_float)

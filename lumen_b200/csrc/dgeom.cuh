@@ -33,7 +33,7 @@ namespace lb {
 #define D_MAX_SCAN_PER_LEAF 4
 #define D_MAX_SCAN_EXTRA 5
 #define D_TINY_NORMAL 1.17549435e-38f
-#define D_STACK 32
+#define D_STACK LUMEN_MAX_BVH_DEPTH
 
 // the scene on the device (the LumenSceneDesc arrays, device pointers)
 struct DScene {
@@ -382,14 +382,14 @@ L_DEV float d_leaf_dist(const DScene& S, int kind, int leaf, int face, const flo
 
 L_DEV int d_clampv(const DScene& S, int item) { return item < 0 ? 0 : (item > S.n - 1 ? S.n - 1 : item); }
 
-L_DEV void d_hit_grad(const DScene& S, int item, int leaf, int face, const float* x, float* gw) {
+L_CALL void d_hit_grad(const DScene& S, int item, int leaf, int face, const float* x, float* gw) {
   int i = d_clampv(S, item);
   float xl[3], g[3];
   d_to_local_pt(S, i, x, xl);
   d_leaf_grad(S, vI(S, i, LUMEN_VI_KIND), leaf, face, xl, g);
   d_to_world_dir(S, i, g, gw);
 }
-L_DEV float d_face_dist(const DScene& S, int item, int leaf, int face, const float* x) {
+L_CALL float d_face_dist(const DScene& S, int item, int leaf, int face, const float* x) {
   int i = d_clampv(S, item);
   float xl[3];
   d_to_local_pt(S, i, x, xl);
@@ -419,7 +419,7 @@ L_DEV int d_holds_point(const DScene& S, int i, const float* x) {
   d_to_local_pt(S, i, x, xl);
   return d_inside_kind(S, vI(S, i, LUMEN_VI_KIND), xl);
 }
-L_DEV int d_ray_holds(const DScene& S, int i, const float* od, const float* dd, float t) {
+L_CALL int d_ray_holds(const DScene& S, int i, const float* od, const float* dd, float t) {
   float ol[3], dl[3];
   d_to_local_pt(S, i, od, ol);
   d_to_local_dir(S, i, dd, dl);
@@ -458,7 +458,7 @@ L_DEV int d_find(const DScene& S, int v, const float* x) {
   });
   return g;
 }
-L_DEV int d_locate(const DScene& S, const float* x) {
+L_CALL int d_locate(const DScene& S, const float* x) {
   int v = S.n;
   for (int guard = 0; guard < 64; ++guard) {
     int f = d_find(S, v, x);
@@ -475,7 +475,7 @@ L_DEV int d_find_ray(const DScene& S, int v, const float* od, const float* dd, f
   });
   return g;
 }
-L_DEV int d_settle(const DScene& S, int v, const float* od, const float* dd, float t, int crossed, float pad, int* moved) {
+L_CALL int d_settle(const DScene& S, int v, const float* od, const float* dd, float t, int crossed, float pad, int* moved) {
   int v_ = v, held = 0;
   for (int guard = 0; guard < 256; ++guard) {
     int vi = v_ < S.n - 1 ? v_ : S.n - 1;
@@ -503,7 +503,7 @@ struct Ctx {
   Side sd;
 };
 
-L_DEV int d_on_face(const DScene& S, const Ctx& c, int i, const First& fr, int kn_i) {
+L_CALL int d_on_face(const DScene& S, const Ctx& c, int i, const First& fr, int kn_i) {
   float dt = fr.t - c.t_lo;
   float lim = D_K_ON * c.band;
   int far_ = 0;
@@ -583,12 +583,11 @@ L_DEV void d_slab(const DScene& S, int node, const float* o, const float* inv, f
   *tout = hi_t;
 }
 
-// the next event in volume v: its own exit, then the first entry of every daughter the BVH does not prune
+// the next event in volume v: its own exit, then the first entry of every daughter the BVH does not prune. One
+// call site of the visit (the own solid is the first candidate, then the traversal yields one leaf item at a time).
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   Best b = {D_HUGE, -1, -1, -1, 0, 0};
-  if (has_own) b = d_unit_visit(S, c, vi, b, 1);
   int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
-  if (n0 >= n1) return b;
   float inv[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -598,41 +597,60 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   int stack[D_STACK];
   float tins[D_STACK];
   int sp = 0;
-  float tin, tout;
-  d_slab(S, n0, c.od, inv, &tin, &tout);
-  int node = (tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band) ? n0 : -1;
-  while (node >= 0) {
-    const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
-    int cnt = __ldg(ni + 1);
-    int nxt = -1;
-    if (cnt > 0) {
-      int st = __ldg(ni + 2);
-      for (int k = 0; k < cnt; ++k) b = d_unit_visit(S, c, __ldg(S.items + st + k), b, 0);
+  int node = -1;       // the traversal's next node (-1: pop or done)
+  int started = 0;     // the root has been tested
+  int pending = has_own;
+  for (;;) {
+    int item = -1, is_own = 0;
+    if (pending) {
+      item = vi;
+      is_own = 1;
+      pending = 0;
     } else {
-      int lc = node + 1;
-      int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
-      float tl, tlo, tr, tro;
-      d_slab(S, lc, c.od, inv, &tl, &tlo);
-      d_slab(S, rc, c.od, inv, &tr, &tro);
-      float lim = d_min(b.t, c.t_bound) + c.band;
-      int hl = tl <= tlo && tlo >= c.t_lo && tl <= lim;
-      int hr = tr <= tro && tro >= c.t_lo && tr <= lim;
-      int first = tl <= tr;
-      int near_ = first ? lc : rc, far_ = first ? rc : lc;
-      int h_near = first ? hl : hr, h_far = first ? hr : hl;
-      if (h_near && h_far && sp < D_STACK) {
-        stack[sp] = far_;
-        tins[sp] = first ? tr : tl;
-        sp++;
+      if (!started) {
+        started = 1;
+        if (n0 < n1) {
+          float tin, tout;
+          d_slab(S, n0, c.od, inv, &tin, &tout);
+          node = (tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band) ? n0 : -1;
+        }
       }
-      nxt = h_near ? near_ : (h_far ? far_ : -1);
+      while (item < 0) {
+        if (node < 0) {
+          float lim = d_min(b.t, c.t_bound) + c.band;
+          while (sp > 0 && tins[sp - 1] > lim) sp--;
+          if (sp == 0) break;
+          sp--;
+          node = stack[sp];
+        }
+        const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
+        int cnt = __ldg(ni + 1);
+        if (cnt > 0) {  // a leaf: one item
+          item = __ldg(S.items + __ldg(ni + 2));
+          node = -1;
+          break;
+        }
+        int lc = node + 1;
+        int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
+        float tl, tlo, tr, tro;
+        d_slab(S, lc, c.od, inv, &tl, &tlo);
+        d_slab(S, rc, c.od, inv, &tr, &tro);
+        float lim = d_min(b.t, c.t_bound) + c.band;
+        int hl = tl <= tlo && tlo >= c.t_lo && tl <= lim;
+        int hr = tr <= tro && tro >= c.t_lo && tr <= lim;
+        int first = tl <= tr;
+        int near_ = first ? lc : rc, far_ = first ? rc : lc;
+        int h_near = first ? hl : hr, h_far = first ? hr : hl;
+        if (h_near && h_far && sp < D_STACK) {
+          stack[sp] = far_;
+          tins[sp] = first ? tr : tl;
+          sp++;
+        }
+        node = h_near ? near_ : (h_far ? far_ : -1);
+      }
+      if (item < 0) break;
     }
-    if (nxt < 0) {
-      float lim = d_min(b.t, c.t_bound) + c.band;
-      while (sp > 0 && tins[sp - 1] > lim) sp--;
-      if (sp > 0) { sp--; nxt = stack[sp]; }
-    }
-    node = nxt;
+    b = d_unit_visit(S, c, item, b, is_own);
   }
   return b;
 }

@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #define L_DEV __device__ __forceinline__
+#define L_CALL __device__ __noinline__  // large functions: one copy shared by every call site (instruction cache)
 
 namespace lb {
 
@@ -172,7 +173,7 @@ struct Key { uint32_t k0, k1; };
 
 L_DEV uint32_t rotl(uint32_t x, int r) { return __funnelshift_l(x, x, r); }
 
-L_DEV void threefry(uint32_t k0, uint32_t k1, uint32_t x0, uint32_t x1, uint32_t* y0, uint32_t* y1) {
+L_CALL void threefry(uint32_t k0, uint32_t k1, uint32_t x0, uint32_t x1, uint32_t* y0, uint32_t* y1) {
   const uint32_t k2 = k0 ^ k1 ^ 0x1BD11BDAu;
   x0 += k0; x1 += k1;
 #define TF_R(r) x0 += x1; x1 = rotl(x1, r); x1 ^= x0;

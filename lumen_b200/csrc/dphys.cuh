@@ -48,7 +48,7 @@ L_DEV float d_eg(const float* e, int k, int j) {
   if (j == k) return __ldg(e + k);
   return 0.5f * (__ldg(e + j - 1) + __ldg(e + j));
 }
-L_DEV float d_group_index(const DScene& S, const float* __restrict__ pool, int t, float E) {
+L_CALL float d_group_index(const DScene& S, const float* __restrict__ pool, int t, float E) {
   int off = __ldg(S.tab + 2 * t), kk = __ldg(S.tab + 2 * t + 1);
   const float* e = pool + off;
   const float* n = pool + off + kk;
@@ -71,7 +71,7 @@ L_DEV float d_group_index(const DScene& S, const float* __restrict__ pool, int t
 
 struct Med { float n, ng, mu_abs, mu_c; };
 
-L_DEV Med d_medium_at(const DScene& S, const float* __restrict__ pool, float lam, int mi) {
+L_CALL Med d_medium_at(const DScene& S, const float* __restrict__ pool, float lam, int mi) {
   const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
   float E = D_HC / lam;
   Med r = {1.0f, 1.0f, 0.0f, 0.0f};
@@ -146,7 +146,7 @@ L_DEV Cf c_decaying_sqrt(Cf z) {
   return q;
 }
 
-L_DEV void d_amplitudes(float cos_i, float n1, Cf n2, Cf* a) {
+L_CALL void d_amplitudes(float cos_i, float n1, Cf n2, Cf* a) {
   float c = cos_i < 0.0f ? 0.0f : (cos_i > 1.0f ? 1.0f : cos_i);
   Cf c1 = cf(c, 0.0f), n1c = cf(n1, 0.0f);
   Cf n22 = c_mul(n2, n2);
@@ -251,7 +251,7 @@ L_DEV void d_chained(const float* p, const float* dp, float* out, float* dout) {
 // the TypeEval of a surface row (types.py:352 kernel); with G > 0 gradient parameters, gt[p] the table each moves,
 // the tangents dprobs[p][o], ddet[p] (a column's value moves with its table)
 template <int G>
-L_DEV void d_type_eval(const DScene& S, const float* __restrict__ pool, int row, float lam, const float* wi,
+L_CALL void d_type_eval(const DScene& S, const float* __restrict__ pool, int row, float lam, const float* wi,
                        const float* n, float n1, float n2, const float* er, const float* ei, Eval& ev, int P,
                        const int* gt, float (*dprobs)[N_OUT], float* ddet) {
 #pragma unroll
@@ -364,7 +364,7 @@ L_DEV float d_dipole_cos(float rand) {
   float r = 2.0f * c;
   return r < -1.0f ? -1.0f : (r > 1.0f ? 1.0f : r);
 }
-L_DEV void d_rayleigh_sample(const float* er, const float* ei, float r0, float r1, float r2, float* wo) {
+L_CALL void d_rayleigh_sample(const float* er, const float* ei, float r0, float r1, float r2, float* wo) {
   float a2 = d_dot(er, er);
   float norm2 = d_dot(er, er) + d_dot(ei, ei);
   float axis[3];

@@ -126,8 +126,16 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
 }
 
 // The persistent photon loop: a lane refill per step (src/lumen/run.py:81 SCHEDULE = "step").
+// 256 threads, 4 blocks per SM: 64 registers a thread, 32 warps an SM (measured best of 128/256 threads at 1-8
+// blocks: the loop is latency- and divergence-bound, so warps to switch between beat registers)
+#ifndef LUMEN_MINB
+#define LUMEN_MINB 4
+#endif
+#ifndef LUMEN_BLOCK
+#define LUMEN_BLOCK 256
+#endif
 template <int G>
-__global__ void __launch_bounds__(128) k_trace(Launch L) {
+__global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
   Photon ph;
@@ -201,8 +209,8 @@ __global__ void __launch_bounds__(128) k_trace(Launch L) {
     }
   }
   // block reduction of the health and the counters, then one atomic per block and value
-  __shared__ double sh[LUMEN_N_HEALTH][4];
-  __shared__ unsigned long long sc[LUMEN_N_COUNT][4];
+  __shared__ double sh[LUMEN_N_HEALTH][LUMEN_BLOCK / 32];
+  __shared__ unsigned long long sc[LUMEN_N_COUNT][LUMEN_BLOCK / 32];
   const int warp = threadIdx.x >> 5;
   for (int k = 0; k < LUMEN_N_HEALTH; ++k) {
     double v = hsum[k];
@@ -330,6 +338,23 @@ static int check_desc(const LumenSceneDesc* d) {
     if (v < d->n_vol && (vi[LUMEN_VI_KIND] < 0 || vi[LUMEN_VI_KIND] >= d->n_kind)) return set_err(LUMEN_ERR_ARG, "scene_create: a kind is out of range");
     if (vi[LUMEN_VI_NODE0] < 0 || vi[LUMEN_VI_NODE1] > d->n_node || vi[LUMEN_VI_NODE0] > vi[LUMEN_VI_NODE1]) return set_err(LUMEN_ERR_ARG, "scene_create: a BVH range is out of range");
   }
+  for (int v = 0; v <= d->n_vol; ++v) {  /* every daughter BVH within the traversal's stack */
+    int n0 = d->vol_i[(size_t)v * LUMEN_VOL_I + LUMEN_VI_NODE0], n1 = d->vol_i[(size_t)v * LUMEN_VOL_I + LUMEN_VI_NODE1];
+    if (n0 >= n1) continue;
+    std::vector<std::pair<int, int>> todo{{n0, 1}};
+    while (!todo.empty()) {
+      auto [nd, dp] = todo.back();
+      todo.pop_back();
+      if (nd < n0 || nd >= n1 || dp > LUMEN_MAX_BVH_DEPTH) return set_err(LUMEN_ERR_SCENE, "scene_create: a BVH is malformed or deeper than LUMEN_MAX_BVH_DEPTH");
+      if (d->node_i[(size_t)nd * LUMEN_NODE_I + 1] == 0) {
+        todo.push_back({nd + 1, dp + 1});
+        todo.push_back({d->node_i[(size_t)(nd + 1) * LUMEN_NODE_I], dp + 1});
+      } else {
+        int st = d->node_i[(size_t)nd * LUMEN_NODE_I + 2], cnt = d->node_i[(size_t)nd * LUMEN_NODE_I + 1];
+        if (st < 0 || st + cnt > d->n_item) return set_err(LUMEN_ERR_SCENE, "scene_create: a BVH leaf is out of the items");
+      }
+    }
+  }
   for (int c = 0; c < d->n_cls; ++c)
     if (d->cls_medium[c] < 0 || d->cls_medium[c] >= d->n_med) return set_err(LUMEN_ERR_ARG, "scene_create: a medium is out of range");
   for (int r = 0; r < d->n_row; ++r) {
@@ -434,7 +459,7 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
     T.counts = out->counts;
   }
   int st = 0;
-  const int block = 128;
+  const int block = LUMEN_BLOCK;
   int grid = 0;
   if (L.n > 0) {
     if (L.R.P > 0 || cot) {

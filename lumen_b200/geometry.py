@@ -22,7 +22,8 @@ import numpy as np
 # the navigator's padded world boxes (src/lumen/rules/tolerances.py:83-84)
 WORLD_BOX_PAD_REL = 1e-6
 WORLD_BOX_PAD_ABS = 1e-9
-MAX_LEAVES = 16  # include/lumen_b200.h LUMEN_MAX_LEAVES
+MAX_LEAVES = 8  # include/lumen_b200.h LUMEN_MAX_LEAVES
+MAX_BVH_DEPTH = 24  # include/lumen_b200.h LUMEN_MAX_BVH_DEPTH
 MAX_PLANES = 8
 
 
@@ -263,6 +264,19 @@ def _bvh(items, lo, hi):
     return nodes, order
 
 
+def bvh_depth(node_i, n0, n1) -> int:
+    """Return the levels of the BVH in nodes [n0, n1) (0: empty)."""
+    if n0 >= n1:
+        return 0
+    depth, todo = 0, [(n0, 1)]
+    while todo:
+        nd, dp = todo.pop()
+        depth = max(depth, dp)
+        if node_i[nd, 1] == 0:
+            todo += [(nd + 1, dp + 1), (int(node_i[nd + 1, 0]), dp + 1)]
+    return depth
+
+
 # ------------------------------------------------------------------------------------------------- the arrays
 def pad_box(lo, hi):
     """Return the box padded as the navigator's world boxes (tolerances.py:83-84)."""
@@ -333,6 +347,10 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
             node_i.append([base + nd[2], nd[3], ibase + nd[4] if nd[3] else 0, 0])
         items.extend(order)
         vol_i[v, 8] = len(node_f)
+    ni_arr = np.asarray(node_i, np.int32).reshape(-1, 4)
+    for v in range(n + 1):
+        if bvh_depth(ni_arr, vol_i[v, 7], vol_i[v, 8]) > MAX_BVH_DEPTH:
+            raise ValueError(f"volume {v}: a daughter BVH deeper than {MAX_BVH_DEPTH} levels")
     allp = np.concatenate([lo_w, hi_w]) if n else np.zeros((1, 3))
     reach = float(np.linalg.norm(allp.max(0) - allp.min(0)))
     return dict(

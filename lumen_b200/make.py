@@ -33,18 +33,19 @@ def stale() -> bool:
     return any(os.path.getmtime(f) > t for f in sources())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, out: str = OUT, defines=()) -> str:
     """Compile the engine if a source is newer than the library; return the library's path."""
-    if not force and not stale():
+    if not force and not stale() and out == OUT:
         return OUT
-    cmd = [NVCC, *FLAGS, *(["-Xptxas", "-v"] if verbose else []), "-o", OUT + ".tmp", SRC]
+    cmd = [NVCC, *FLAGS, *(["-Xptxas", "-v"] if verbose else []), *[f"-D{d}" for d in defines], "-o", out + ".tmp",
+           SRC]  # fmt: skip
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed ({r.returncode}):\n{r.stderr[-8000:]}")
     if verbose:
         print(r.stderr)
-    os.replace(OUT + ".tmp", OUT)
-    return OUT
+    os.replace(out + ".tmp", out)
+    return out
 
 
 if __name__ == "__main__":
