@@ -1,0 +1,157 @@
+"""The CPU checker (the oracle) against the reference's golden values and closed forms.
+
+- threefry2x32-20 against the Random123 known-answer vectors (the reference's RNG, src/lumen/_core/rng.py);
+- the uniforms' contract (open interval, determinism, block stability: src/lumen/_core/rng.py:81-95,
+  tests/unit/test_core.py:58-76 of the reference);
+- the float32 elementary functions against float64 (ulp bounds);
+- the tutorial tank's published run (docs/tutorial/first-hour.md:101-111 of the reference, lumen.simulate with
+  samples=2**18, seed=0): per-PMT arrivals, their errors, mean times and expected PE, to the printed digits;
+- the weight balance of every photon's fates (src/lumen/api.py:492 Health.balance);
+- closed-form sensor spheres (tests/physics/test_toys.py:126-159 of the reference).
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from lumen_b200 import _abi as A
+from lumen_b200 import api, detectors, geometry as G, optics as O, sources
+from lumen_b200.detector import build
+
+KEY0 = A.key_of_seed(0)
+
+
+def test_threefry_known_answers():
+    # Random123's known-answer vectors for threefry2x32 with 20 rounds (the ones JAX's tests pin too)
+    assert oracle.threefry(0, 0, 0, 0) == (0x6B200159, 0x99BA4EFE)
+    assert oracle.threefry(0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF) == (0x1CB996FC, 0xBB002BE7)
+    assert oracle.threefry(0x13198A2E, 0x03707344, 0x243F6A88, 0x85A308D3) == (0xC4923A9C, 0x483DF7A0)
+
+
+def test_uniforms_open_deterministic_block_stable():
+    u = oracle.uniforms(KEY0, np.arange(20000), 3, 64).astype(np.float64)
+    assert u.min() > 0.0 and u.max() < 1.0
+    assert abs(u.mean() - 0.5) < 5 * math.sqrt(1 / 12 / u.size) and abs(u.var() - 1 / 12) < 1e-3
+    assert np.array_equal(u, oracle.uniforms(KEY0, np.arange(20000), 3, 64))
+    assert np.array_equal(u[:, :8], oracle.uniforms(KEY0, np.arange(20000), 3, 8))  # a longer draw keeps the first
+    assert not np.array_equal(oracle.uniforms(KEY0, [0], 0, 8), oracle.uniforms(KEY0, [0], 1, 8))
+    k = (u * 2**23 - 0.5)
+    assert np.allclose(k, np.round(k))  # (k + 1/2) 2^-23 exactly
+
+
+@pytest.mark.parametrize("fn,lo,hi,ulps", [("exp", -80.0, 80.0, 1.0), ("log", 1e-30, 1e30, 2.0),
+                                           ("acos", -1.0, 1.0, 1.5), ("cbrt", -8.0, 8.0, 1.0)])  # fmt: skip
+def test_math_accuracy(fn, lo, hi, ulps):
+    rng = np.random.default_rng(1)
+    x = np.float32(rng.uniform(lo, hi, 200000)) if fn != "log" else np.float32(np.exp(rng.uniform(-69, 69, 200000)))
+    got = oracle.math(fn, x).astype(np.float64)
+    ref = {"exp": np.exp, "log": np.log, "acos": np.arccos, "cbrt": np.cbrt}[fn](x.astype(np.float64))
+    ulp = np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
+    assert np.max(np.abs(got - ref) / ulp) <= ulps
+
+
+def test_sincos_and_erfinv():
+    u = np.float32(np.random.default_rng(2).uniform(0, 1, 100000))
+    s, c = oracle.math("sin2pi", u), oracle.math("cos2pi", u)
+    a = 2 * np.pi * u.astype(np.float64)
+    assert np.max(np.abs(s - np.sin(a))) < 2.5e-7 and np.max(np.abs(c - np.cos(a))) < 2.5e-7
+    x = np.float32(np.random.default_rng(3).uniform(-0.999, 0.999, 100000))
+    from scipy.special import erfinv
+
+    assert np.max(np.abs(oracle.math("erfinv", x) - erfinv(x.astype(np.float64))) / np.maximum(
+        np.abs(erfinv(x.astype(np.float64))), 1e-3)) < 2e-6  # fmt: skip
+
+
+# the reference's published run of the tutorial tank (docs/tutorial/first-hour.md:101-111)
+PUB_ARRIVALS = [394.54, 913.75, 547.76, 501.74, 515.31, 528.14, 320.36, 340.68]
+PUB_ERRORS = [17.22, 26.23, 20.30, 19.43, 19.69, 19.94, 15.51, 16.03]
+PUB_TIMES = [2.613, 1.699, 2.204, 2.202, 2.208, 2.204, 2.851, 2.844]
+PUB_PE = [96.7, 223.9, 134.2, 122.9, 126.3, 129.4, 78.5, 83.5]
+TOY_QE = ([300.0, 340.0, 380.0, 420.0, 460.0, 500.0, 540.0, 580.0, 600.0],
+          [0.05, 0.20, 0.25, 0.24, 0.20, 0.14, 0.08, 0.04, 0.02])  # examples/data/toy_pmt.json  # fmt: skip
+
+
+@pytest.fixture(scope="module")
+def toy_run():
+    det = detectors.toy_tank()
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    n = 1 << 18
+    T, _ = oracle.trace(det, KEY0, n, source=src, samples=n)
+    return det, T, n
+
+
+def test_toy_tank_matches_the_published_run(toy_run):
+    det, T, n = toy_run
+    arr = T.arrival[0]
+    err = api.moment_error(T.arrival2[0], arr, n)
+    np.testing.assert_allclose(arr, PUB_ARRIVALS, atol=0.0051)
+    np.testing.assert_allclose(err, PUB_ERRORS, atol=0.0051)
+    np.testing.assert_allclose(T.arrival_t[0] / arr, PUB_TIMES, atol=0.0006)
+    q = np.interp(400.0, *TOY_QE)
+    np.testing.assert_allclose(arr * q, PUB_PE, atol=0.051)
+
+
+def test_weight_balance(toy_run):
+    det, T, n = toy_run
+    h = T.health
+    fates = h[[0, 1, 2, 3, 4, 5, 6, 7, 8]].sum()
+    assert abs(h[10] - fates) < 1e-6 * h[10]
+    tank = detectors.cylinder_tank()
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    T2, _ = oracle.trace(tank, KEY0, 1 << 13, source=src, samples=1 << 13)
+    h = T2.health
+    assert abs(h[10] - h[[0, 1, 2, 3, 4, 5, 6, 7, 8]].sum()) < 1e-5 * h[10]
+
+
+def sensor_sphere(A_, L, R, finish):
+    """A liquid sphere of radius A_ (absorption length L) in an opaque sensor whose surface reflects R."""
+    liquid = O.Material("Liquid", rindex=1.0, abslength=L)
+    box = G.Volume("Cathode", G.Box(A_ + 0.5, A_ + 0.5, A_ + 0.5), "Opaque")
+    inner = G.Volume("Inner", G.Sphere(A_), "Liquid")
+    box.place(inner, (0.0, 0.0, 0.0), name="Inner")
+    surf = O.OpticalSurface("Wall", "dielectric_metal", finish, reflectivity=R, efficiency=1.0)
+    return build(box, {"Liquid": liquid, "Opaque": O.Material("Opaque")}, borders=[("Inner", "Cathode", surf)],
+                 sensors={"s": "Cathode"})  # fmt: skip
+
+
+def test_specular_sensor_sphere_closed_form():
+    # Q = (1 - R) e^{-A/L} / (1 - R e^{-2A/L}) (tests/physics/test_toys.py:126 of the reference)
+    A_, L, R = 1.0, 5.0, 0.5
+    det = sensor_sphere(A_, L, R, "polished")
+    src = sources.Point(position=(0.0, 0.0, 0.0), n_photons=1.0, lam=400.0)
+    n = 1 << 14
+    T, _ = oracle.trace(det, KEY0, n, source=src, samples=n)
+    q = (1 - R) * math.exp(-A_ / L) / (1 - R * math.exp(-2 * A_ / L))
+    err = api.moment_error(T.arrival2[0, 0], T.arrival[0, 0], n)
+    assert abs(T.arrival[0, 0] - q) < max(4 * err, 3e-5 * q)
+
+
+def test_lambertian_sensor_sphere_closed_form():
+    # Q = (1 - R) e^{-b/2} / (1 - 2 R (1 - (1 + b) e^{-b}) / b^2), b = 2 A / L (test_toys.py:130-159)
+    A_, L, R = 1.0, 3.0, 0.6
+    det = sensor_sphere(A_, L, R, "ground")
+    src = sources.Point(position=(0.0, 0.0, 0.0), n_photons=1.0, lam=400.0)
+    n = 1 << 16
+    T, _ = oracle.trace(det, KEY0, n, source=src, samples=n)
+    b = 2 * A_ / L
+    q = (1 - R) * math.exp(-A_ / L) / (1 - 2 * R * (1 - (1 + b) * math.exp(-b)) / b**2)
+    err = api.moment_error(T.arrival2[0, 0], T.arrival[0, 0], n)
+    assert abs(T.arrival[0, 0] - q) < 4 * err, (T.arrival[0, 0], q, err)
+
+
+def test_enclosing_sensor_counts_everything_whatever_the_scattering():
+    liquid = O.Material("Liquid", rindex=1.33, rayleigh=0.3)
+    box = G.Volume("Cathode", G.Box(1.5, 1.5, 1.5), "Opaque")
+    box.place(G.Volume("Inner", G.Sphere(1.0), "Liquid"), name="Inner")
+    surf = O.OpticalSurface("Wall", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    det = build(box, {"Liquid": liquid, "Opaque": O.Material("Opaque")}, borders=[("Inner", "Cathode", surf)],
+                sensors={"s": "Cathode"})  # fmt: skip
+    n = 1 << 14
+    T, _ = oracle.trace(det, KEY0, n, source=sources.Point((0.1, 0.2, -0.3), 1.0, lam=400.0), samples=n)
+    # expected detection over the free path: unbiased, not one per photon (test_toys.py:162-172)
+    err = api.moment_error(T.arrival2[0, 0], T.arrival[0, 0], n)
+    assert abs(T.arrival[0, 0] - 1.0) < 4 * err, (T.arrival[0, 0], err)
+    assert abs(T.health[5] - 1.0) < 1e-6  # every photon's weight ends absorbed at the cathode
+    assert T.counts[1] / T.counts[0] > 3  # it scattered
