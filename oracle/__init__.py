@@ -44,6 +44,7 @@ def lib():
         L.lumen_oracle_math.argtypes = [ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_fresnel.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_basis.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_group_index.argtypes = [A.c_f32p, A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_source_rows.argtypes = [P(A.LumenSource), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
                                                ctypes.c_int64, A.c_f32p, A.c_i32p]
         del vp
@@ -90,6 +91,13 @@ def basis(n):
     out = np.zeros((len(n), 6), np.float32)
     lib().lumen_oracle_basis(A.fptr(n), len(n), A.fptr(out))
     return out[:, :3], out[:, 3:]
+
+
+def group_index(e, n, lam):
+    e, n, lam = A.np_f32(e), A.np_f32(n), A.np_f32(lam)
+    out = np.zeros_like(lam)
+    assert lib().lumen_oracle_group_index(A.fptr(e), A.fptr(n), len(e), A.fptr(lam), lam.size, A.fptr(out)) == 0
+    return out
 
 
 def locate(det, pts):

@@ -611,6 +611,19 @@ int32_t lumen_oracle_fresnel(const float* in, int64_t n, float* out) {
   return 0;
 }
 
+/* Geant4's GROUPVEL group index of an index table (energies e, values n, k knots) at wavelengths lam (laws.py:170) */
+int32_t lumen_oracle_group_index(const float* e, const float* n, int32_t k, const float* lam, int64_t m, float* out) {
+  if (k < 1 || k > LUMEN_MAX_KNOTS) return LUMEN_ERR_ARG;
+  std::vector<float> pool(2 * k);
+  for (int j = 0; j < k; ++j) { pool[j] = e[j]; pool[k + j] = n[j]; }
+  int32_t tab[2] = {0, k};
+  LumenSceneDesc D;
+  memset(&D, 0, sizeof(D));
+  D.tab = tab;
+  for (int64_t i = 0; i < m; ++i) out[i] = o_group_index(&D, pool.data(), 0, O_HC / lam[i]);
+  return 0;
+}
+
 /* basis(n) for n unit vectors: out t1, t2 (frames.py:14) */
 int32_t lumen_oracle_basis(const float* nv, int64_t n, float* out) {
   for (int64_t i = 0; i < n; ++i) o_basis(nv + 3 * i, out + 6 * i, out + 6 * i + 3);
