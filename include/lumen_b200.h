@@ -196,6 +196,24 @@ int32_t lumen_b200_adjoint(const LumenScene* scene, const LumenRows* rows, const
                            const LumenControls* controls, const double* cotangent, int32_t n_events,
                            double* grads, void* stream);
 
+/* The words of the fixed device array lumen_b200_trace_static takes its scratch from (64 x 8 bytes). */
+#define LUMEN_STATIC_SCRATCH_WORDS 64
+
+/* lumen_b200_trace for callers that cannot allocate device memory during a call. Such callers include a framework
+   whose pool owns all of the device's memory and forbids other allocations while it runs a step, and a loop that
+   must not wait on the allocator. No counterpart in the reference: lumen's loop allocates through JAX.
+   Same arguments, outputs and results as lumen_b200_trace; the caller still passes every input and output. The
+   call's own scratch (the photon counter, the abort flag and the step count: 3 of LUMEN_STATIC_SCRATCH_WORDS words)
+   comes from one fixed array in the library's device memory instead of an allocation, and a call whose scratch
+   would not fit that array is refused with LUMEN_ERR_ARG. Every GPU that loads the library holds the array until the
+   process exits. The first call on a device looks up the array's address there, with that device current, so make
+   that first call before any stream capture. All calls share the one array and leave their counts in it; each call
+   clears what must start at zero. Calls that overlap on the GPU (other streams, other host threads) race on the
+   array: run them one after another. */
+int32_t lumen_b200_trace_static(const LumenScene* scene, const LumenRows* rows, const LumenSource* source,
+                                uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
+                                const LumenControls* controls, LumenTallies* out, void* stream);
+
 /* Per-photon trace record for parity checks: for each photon, out_i[5*i ..] = vertices, deposits, end code
    (0 alive at the guard, 1 ended), first sensor hit (-1 none), last volume; out_f[4*i ..] = sum of q, final
    weight, final time, sum of q * time. Same inputs as lumen_b200_trace; device outputs. */

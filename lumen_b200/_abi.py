@@ -97,7 +97,7 @@ def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=()
 
 ENTRY_POINTS = ("lumen_b200_abi_version", "lumen_b200_last_error", "lumen_b200_scene_create",
                 "lumen_b200_scene_set_pools", "lumen_b200_scene_destroy", "lumen_b200_trace", "lumen_b200_adjoint",
-                "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate")  # fmt: skip
+                "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate", "lumen_b200_trace_static")  # fmt: skip
 
 _lib = None
 
@@ -122,6 +122,9 @@ def engine():
         lib.lumen_b200_adjoint.argtypes = [vp, ctypes.POINTER(LumenRows), ctypes.POINTER(LumenSource),
                                            ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
                                            ctypes.POINTER(LumenControls), c_f64p, ctypes.c_int32, c_f64p, vp]  # fmt: skip
+        lib.lumen_b200_trace_static.argtypes = [vp, ctypes.POINTER(LumenRows), ctypes.POINTER(LumenSource),
+                                                ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
+                                                ctypes.POINTER(LumenControls), ctypes.POINTER(LumenTallies), vp]
         lib.lumen_b200_trace_photons.argtypes = [vp, ctypes.POINTER(LumenRows), ctypes.POINTER(LumenSource),
                                                  ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64,
                                                  ctypes.POINTER(LumenControls), c_i32p, c_f32p, vp]  # fmt: skip

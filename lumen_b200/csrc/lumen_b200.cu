@@ -14,6 +14,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -488,8 +489,94 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
   return 0;
 }
 
+// ------------------------------------------------------------------------- the scratch that needs no allocation
+// lumen_b200_trace_static's scratch: a fixed array in the library's device memory (one per GPU that loads the
+// library, held until the process exits), for callers that cannot allocate during a call. Host code cannot use the
+// array's name as an address (it names a host-side stand-in); each device's address is looked up once, with that
+// device current, by cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned long long g_static_scratch[LUMEN_STATIC_SCRATCH_WORDS];
+static const int STATIC_SCRATCH_NEED = 3;  // photon counter, abort flag, steps used
+static std::mutex g_static_mu;
+static void* g_static_addr[256];
+
+static int static_scratch(unsigned long long** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return set_err(LUMEN_ERR_NO_DEVICE, "trace_static: device index out of range");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_static_scratch));
+    g_static_addr[dev] = p;
+  }
+  *out = (unsigned long long*)g_static_addr[dev];
+  return 0;
+}
+
+// run_trace with the scratch of the fixed array (no allocation, no free)
+static int run_trace_static(Launch& L, const LumenTallies* out, cudaStream_t stream) {
+  if (STATIC_SCRATCH_NEED > LUMEN_STATIC_SCRATCH_WORDS)
+    return set_err(LUMEN_ERR_ARG, "trace_static: the call needs more scratch than LUMEN_STATIC_SCRATCH_WORDS");
+  unsigned long long* scratch = nullptr;
+  int st = static_scratch(&scratch);
+  if (st) return st;
+  Tally& T = L.T;
+  T.E = out->n_events > 0 ? out->n_events : 1;
+  T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
+  T.P = L.R.P;
+  T.cot = nullptr;
+  T.grads = nullptr;
+  T.nb = out->hist ? out->n_bins : 0;
+  T.bin0 = out->bin0;
+  T.bin_w = out->bin_w;
+  T.arrival = out->arrival;
+  T.arrival_t = out->arrival_t;
+  T.arrival2 = out->arrival2;
+  T.hist = out->hist;
+  T.jac = out->jac;
+  T.health = out->health;
+  T.counts = out->counts;
+  // the array keeps the previous call's counts: clear the words this call reads before they are written
+  CK(cudaMemsetAsync(scratch, 0, STATIC_SCRATCH_NEED * sizeof(unsigned long long), stream));
+  L.next = scratch;
+  L.abort_flag = (int*)(scratch + 1);
+  L.steps_used = scratch + 2;
+  const int block = LUMEN_BLOCK;
+  int grid = 0;
+  if (L.n > 0) {
+    if (L.R.P > 0) {
+      if ((st = grid_for((const void*)k_trace<LUMEN_MAX_GRAD>, block, &grid))) return st;
+      k_trace<LUMEN_MAX_GRAD><<<grid, block, 0, stream>>>(L);
+    } else {
+      if ((st = grid_for((const void*)k_trace<0>, block, &grid))) return st;
+      k_trace<0><<<grid, block, 0, stream>>>(L);
+    }
+    CK(cudaGetLastError());
+  }
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (flag) return set_err(LUMEN_ERR_STEP_BUDGET, "the call's step budget ran out before every photon ended");
+  return 0;
+}
+
 // ------------------------------------------------------------------------------------------------- the ABI
 extern "C" {
+
+int32_t lumen_b200_trace_static(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
+                                uint32_t key1, int64_t first_id, int64_t n, const LumenControls* c, LumenTallies* out,
+                                void* stream) {
+  g_err.clear();
+  if (!out || !out->arrival || !out->arrival_t || !out->arrival2 || !out->health || !out->counts)
+    return set_err(LUMEN_ERR_ARG, "tallies: a required output is null");
+  if (c && c->n_grad > 0 && !out->jac) return set_err(LUMEN_ERR_ARG, "tallies: jac is null with gradient parameters");
+  if (out->hist && (out->n_bins <= 0 || !(out->bin_w > 0.0f))) return set_err(LUMEN_ERR_ARG, "tallies: bad histogram");
+  if (source && out->n_events < source->n_events) return set_err(LUMEN_ERR_ARG, "tallies: fewer events than the source's");
+  Launch L;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  if (st) return st;
+  return run_trace_static(L, out, (cudaStream_t)stream);
+}
 
 int32_t lumen_b200_abi_version(void) { return LUMEN_B200_ABI_VERSION; }
 
