@@ -70,7 +70,8 @@ struct Launch {
 
 #define CACHE 4
 
-template <int G>
+// the current photon's per-sensor sums (the second moment squares each at the photon's end); four entries, read and
+// written by constant index only, so they stay in registers
 struct PhotonTally {
   int sensor[CACHE];
   double sum[CACHE];
@@ -82,9 +83,15 @@ __device__ __forceinline__ void flush2(const Tally& T, int e, int s, double v) {
   if (T.arrival2) atomicAdd(T.arrival2 + (size_t)e * T.S_ + s, v * v);
 }
 
+__device__ __forceinline__ void flush_all(const Tally& T, int e, PhotonTally& pt) {
+#pragma unroll
+  for (int j = 0; j < CACHE; ++j)
+    if (j < pt.n) flush2(T, e, pt.sensor[j], pt.sum[j]);
+}
+
 template <int G>
 __device__ __forceinline__ void deposit(const Tally& T, int e, const Dep& dep, const float* dq, double w0,
-                                        PhotonTally<G>& pt) {
+                                        PhotonTally& pt) {
   int s = dep.sensor;
   if ((unsigned)e >= (unsigned)T.E || (unsigned)s >= (unsigned)T.S_) return;  // an event or sensor out of range
   double v = (double)dep.q * w0;
@@ -106,19 +113,22 @@ __device__ __forceinline__ void deposit(const Tally& T, int e, const Dep& dep, c
         for (int p = 0; p < T.P; ++p) atomicAdd(T.grads + p, c * (double)dq[p] * w0);
     }
   }
-  int j = 0;
-  while (j < pt.n && pt.sensor[j] != s) ++j;
-  if (j == pt.n) {
-    if (pt.n == CACHE) {
+  int found = 0;
+#pragma unroll
+  for (int j = 0; j < CACHE; ++j)
+    if (j < pt.n && pt.sensor[j] == s) { pt.sum[j] += v; found = 1; }
+  if (!found) {
+    if (pt.n == CACHE) {  // the oldest entry's sum is final: flush it and shift
       flush2(T, e, pt.sensor[0], pt.sum[0]);
+#pragma unroll
       for (int k = 1; k < CACHE; ++k) { pt.sensor[k - 1] = pt.sensor[k]; pt.sum[k - 1] = pt.sum[k]; }
-      pt.n -= 1;
+      pt.n = CACHE - 1;
     }
-    j = pt.n++;
-    pt.sensor[j] = s;
-    pt.sum[j] = 0.0;
+#pragma unroll
+    for (int j = 0; j < CACHE; ++j)
+      if (j == pt.n) { pt.sensor[j] = s; pt.sum[j] = v; }
+    pt.n += 1;
   }
-  pt.sum[j] += v;
 }
 
 __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
@@ -141,16 +151,18 @@ __global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
   const unsigned FULL = 0xffffffffu;
   Photon ph;
   float dw[G > 0 ? G : 1], dq[G > 0 ? G : 1];
-  PhotonTally<G> pt;
+  PhotonTally pt;
   pt.n = 0;
   Key pkey = {0u, 0u};
   int active = 0, ev = 0;
   double w0 = 0.0;
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // the current photon's fates
-  double hsum[LUMEN_N_HEALTH];
-  for (int k = 0; k < LUMEN_N_HEALTH; ++k) hsum[k] = 0.0;
-  unsigned long long c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0;
-  int64_t budget_chunk = 0;
+  // the health fates, summed per block in shared memory (a step adds its non-zero fates times the row weight): no
+  // per-thread accumulators stay live across the step
+  __shared__ double sh_health[LUMEN_N_HEALTH];
+  if (threadIdx.x < LUMEN_N_HEALTH) sh_health[threadIdx.x] = 0.0;
+  __syncthreads();
+  unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0;
+  int budget_chunk = 0;
   for (;;) {
     unsigned need = __ballot_sync(FULL, !active);
     if (need) {
@@ -173,7 +185,6 @@ __global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
           ev = r.event;
           active = 1;
           pt.n = 0;
-          for (int k = 0; k < 8; ++k) acc[k] = 0.0;
           if (G > 0)
             for (int p = 0; p < L.R.P; ++p) dw[p] = 0.0f;
         }
@@ -184,20 +195,21 @@ __global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
       Dep dep;
       d_step<G>(L.R, ph, dw, pkey, dep, dq);
       c_steps++;
-      for (int k = 0; k < 8; ++k) acc[k] += (double)dep.fates[k];
-      hsum[LUMEN_H_PUSHED] += (double)dep.pushed * w0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (dep.fates[k] != 0.0f) atomicAdd(sh_health + k, (double)dep.fates[k] * w0);
+      if (dep.pushed != 0.0f) atomicAdd(sh_health + LUMEN_H_PUSHED, (double)dep.pushed * w0);
       if (dep.sensor >= 0) {
         deposit<G>(L.T, ev, dep, dq, w0, pt);
         c_dep++;
       }
       if (!ph.alive || ph.vertex >= L.R.max_vertices) {
-        for (int j = 0; j < pt.n; ++j) flush2(L.T, ev, pt.sensor[j], pt.sum[j]);
-        for (int k = 0; k < 8; ++k) hsum[k] += acc[k] * w0;
+        flush_all(L.T, ev, pt);
         if (ph.alive) {
-          hsum[LUMEN_H_TRUNCATED] += (double)ph.w * w0;
+          atomicAdd(sh_health + LUMEN_H_TRUNCATED, (double)ph.w * w0);
           c_trunc++;
         }
-        hsum[LUMEN_H_START] += w0;
+        atomicAdd(sh_health + LUMEN_H_START, w0);
         c_ph++;
         active = 0;
       }
@@ -209,16 +221,11 @@ __global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
       if (L.abort_flag && *(volatile int*)L.abort_flag) active = 0;
     }
   }
-  // block reduction of the health and the counters, then one atomic per block and value
-  __shared__ double sh[LUMEN_N_HEALTH][LUMEN_BLOCK / 32];
+  // the block's health and counters: one atomic per block and value
   __shared__ unsigned long long sc[LUMEN_N_COUNT][LUMEN_BLOCK / 32];
   const int warp = threadIdx.x >> 5;
-  for (int k = 0; k < LUMEN_N_HEALTH; ++k) {
-    double v = hsum[k];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
-    if (lane == 0) sh[k][warp] = v;
-  }
   unsigned long long cv[LUMEN_N_COUNT] = {c_ph, c_steps, c_dep, c_trunc, c_multi};
+#pragma unroll
   for (int k = 0; k < LUMEN_N_COUNT; ++k) {
     unsigned long long v = cv[k];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
@@ -226,8 +233,7 @@ __global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
   }
   __syncthreads();
   if (threadIdx.x < LUMEN_N_HEALTH) {
-    double v = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[threadIdx.x][w];
+    double v = sh_health[threadIdx.x];
     if (v != 0.0) atomicAdd(L.T.health + threadIdx.x, v);
   } else if (threadIdx.x >= 32 && threadIdx.x < 32 + LUMEN_N_COUNT) {
     int k = threadIdx.x - 32;
