@@ -145,3 +145,23 @@ def test_query_and_locate_bit_exact(which, toy, tank, lar, built):
     assert (gf.view(np.uint32) == of.view(np.uint32)).all()
     gv = eng.locate(o).cpu().numpy()
     assert (gv == oracle.locate(det, o)).all()
+
+
+def test_adjoint_replay_contracts_the_jacobian(tank, built):
+    """lumen_b200_adjoint replays the photons from their keys: sum_s cot[s] d arrival[s] / d theta equals the
+    contraction of the trace's Jacobian, and the checker's."""
+    src = sources.Point(position=(-2.0, 1.0, 0.5), n_photons=1.0, lam_range=(300.0, 600.0))
+    names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R"]
+    c = A.controls(grad_tabs=[tank.params_index[k] for k in names])
+    n = 1 << 15
+    eng = _engine(tank)
+    ds = DeviceSource(src, n)
+    T = DeviceTallies(tank.n_sensor, 1, 0, 0.0, 1.0, c.n_grad)
+    eng.trace(KEY, n, source=ds, controls=c, tallies=T)
+    cot = np.random.default_rng(5).normal(size=(1, tank.n_sensor))
+    g = eng.adjoint(KEY, n, cot, source=ds, controls=c).cpu().numpy()
+    jac = T.jac.cpu().numpy()[0]
+    want = cot[0] @ jac
+    np.testing.assert_allclose(g, want, rtol=1e-9, atol=1e-12)
+    O, _ = oracle.trace(tank, KEY, n, source=src, samples=n, controls=c)
+    np.testing.assert_allclose(g, cot[0] @ O.jac[0], rtol=1e-7, atol=1e-12)
