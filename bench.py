@@ -129,6 +129,112 @@ def cpu_reference(args, det, src, n_total):
                 sample=f"{sample} photons of the workload (photon ids 0..{sample - 1}), median of {len(ts)} runs")
 
 
+def batched_events(seed=2024, n_events=256):
+    """256 Cherenkov-like tracks in the tank: starts uniform in the volume, isotropic directions, lengths uniform in
+    0.5-3 m (resampled until the track stays inside), cone half-angle 42 degrees, photons per event log-uniform in
+    [1e3, 1e6]."""  # noqa: D205
+    rng = np.random.default_rng(seed)
+    st, dr, ln = [], [], []
+    while len(st) < n_events:
+        p = rng.uniform(-4.7, 4.7, 3)
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        L = rng.uniform(0.5, 3.0)
+        e = p + L * u
+        if np.hypot(p[0], p[1]) < 4.7 and np.hypot(e[0], e[1]) < 4.7 and abs(e[2]) < 4.7:
+            st.append(p), dr.append(u), ln.append(L)
+    counts = np.exp(rng.uniform(np.log(1e3), np.log(1e6), n_events)).astype(np.int64)
+    return np.asarray(st), np.asarray(dr), np.asarray(ln), counts
+
+
+def run_batched(dev, det, reps=3):
+    """The batched forward + adjoint: one fused launch (arrivals and their Jacobian per event) under a CUDA graph."""
+    import torch
+
+    from lumen_b200 import _abi as A
+    from lumen_b200 import autotune, sources
+    from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
+
+    st, dr, ln, counts = batched_events()
+    src = sources.Tracks(start=st, direction=dr, length=ln, cone_angle=np.radians(42.0), n_photons=counts.astype(float),
+                         lam_range=(300.0, 600.0), counts_=counts)  # fmt: skip
+    n = int(counts.sum())
+    eng = Engine(det, dev)
+    ds = DeviceSource(src, n, dev)
+    names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R"]
+    gt = [det.params_index[k] for k in names]
+    (variant, bps), times = autotune.tune(eng, ds, 1 << 20, gt, ds.n_events, A.key_of_seed(0))
+    c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps, flags=A.F_ASYNC)
+    T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
+    key = A.key_of_seed(0)
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):  # warm-up on the side stream before capture
+        T.zero_()
+        eng.trace(key, n, source=ds, controls=c, tallies=T, stream=stream)
+    torch.cuda.synchronize(dev)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        T.zero_()
+        eng.trace(key, n, source=ds, controls=c, tallies=T, stream=stream)
+    g.replay()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    cnt = T.counts.cpu().numpy()
+    jac = T.jac.cpu().numpy()
+    m = float(np.median(ms))
+    eng.close()
+    return {"value": n / (m * 1e-3), "unit": "photons/s", "events": int(ds.n_events), "photons_per_launch": n,
+            "ms_per_launch": m, "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "gradients": names,
+            "graph": True, "autotune": {"variant": variant, "blocks_per_sm": bps,
+                                        "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}},
+            "jacobian_norm": float(np.abs(jac).sum()), "aborted": int(cnt[5])}  # fmt: skip
+
+
+def run_lar(dev, n, reps=2):
+    """The liquid-argon box: 10^4 scintillation points, forward + Jacobian over the cage reflectivity and the
+    Rayleigh length (the sensor efficiencies' derivatives are the arrivals: after tracking)."""  # noqa: D205
+    import torch
+
+    from lumen_b200 import _abi as A
+    from lumen_b200 import detectors, sources
+    from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
+
+    det = detectors.lar_box()
+    pts = np.random.default_rng(77).uniform([-2.4, -1.9, -1.9], [2.4, 1.9, 1.9], (10000, 3))
+    src = sources.Scintillation(position=pts, lam=128.0, tau=(6.0, 1500.0), fraction=0.25, n_photons=1.0)
+    eng = Engine(det, dev)
+    ds = DeviceSource(src, n, dev)
+    names = ["surfaces/CageSurface/R", "media/LAr/rayleigh"]
+    gt = [det.params_index[k] for k in names]
+    c = A.controls(grad_tabs=gt)
+    T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
+    key = A.key_of_seed(0)
+    eng.trace(key, min(n, 1 << 18), source=ds, controls=c, tallies=T)
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        T.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.trace(key, n, source=ds, controls=c, tallies=T)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    cnt = T.counts.cpu().numpy()
+    m = float(np.median(ms))
+    eng.close()
+    return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
+            "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
+            "points": 10000, "gradients": names, "arrivals_sum": float(T.arrival.sum().item())}  # fmt: skip
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -139,6 +245,8 @@ def main():
     ap.add_argument("--cpu-photons", type=int, default=1 << 17)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched and liquid-argon workloads")
+    ap.add_argument("--lar-photons", type=int, default=1 << 24)
     args = ap.parse_args()
 
     from lumen_b200 import detectors, sources
@@ -246,8 +354,11 @@ def main():
                          "traffic": None, "peak_kind": pk_kind,
                          "algorithmic_bytes": alg},
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": args.steps, "clocks": clk.summary(),
+            "gpu_launches": args.steps, "clocks": clk.summary(), "ms_steps": [round(x, 3) for x in ms],
             "arrivals_sum": float(light.arrivals.sum())}  # fmt: skip
+    if rank == 0 and not args.no_extra:
+        line["batched_fwd_adjoint"] = run_batched(dev, det)
+        line["lar_fwd_adjoint"] = run_lar(dev, args.lar_photons)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_reference(args, det, src, n)
     if world > 1:

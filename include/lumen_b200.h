@@ -138,6 +138,10 @@ typedef struct LumenSource {
 } LumenSource;
 
 /* ------------------------------------------------------------------------------------------ the controls */
+enum { LUMEN_F_ASYNC = 1 };  /* controls.flags: enqueue only (no host wait, no status read back: capturable in a
+                                 CUDA graph); a step budget that ran out then shows in counts[LUMEN_C_ABORTED] */
+enum { LUMEN_N_VARIANT = 3 };  /* launch variants: 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
+                                  2 = 256 x 3 (85 registers) */
 typedef struct LumenControls {
   float max_distance;      /* m: a query's reach (<= 0: the scene's reach) */
   float roulette;          /* epsilon > 0 (src/lumen/rules/choices.py:112) */
@@ -145,6 +149,10 @@ typedef struct LumenControls {
   int32_t n_grad;          /* gradient parameters (0..LUMEN_MAX_GRAD) */
   int32_t grad_tab[LUMEN_MAX_GRAD];  /* each parameter: the table whose values all move together (d/d value) */
   int64_t step_budget;     /* device step budget of the call (<= 0: none) */
+  int32_t flags;           /* LUMEN_F_* */
+  int32_t variant;         /* launch variant (0 .. LUMEN_N_VARIANT - 1), from the autotuner */
+  int32_t blocks_per_sm;   /* resident blocks per SM launched (<= 0: as many as fit) */
+  int32_t reserved;
 } LumenControls;
 
 /* --------------------------------------------------------------------------------------------- the tallies */
@@ -152,7 +160,8 @@ typedef struct LumenControls {
 enum { LUMEN_H_LOST = 0, LUMEN_H_ABANDONED, LUMEN_H_ESCAPED, LUMEN_H_DISTANCE_CUT, LUMEN_H_ABSORBED_BULK,
        LUMEN_H_ABSORBED_SURFACE, LUMEN_H_ROULETTED, LUMEN_H_REWEIGHTED, LUMEN_H_TRUNCATED, LUMEN_H_PUSHED,
        LUMEN_H_START, LUMEN_N_HEALTH };
-enum { LUMEN_C_PHOTONS = 0, LUMEN_C_STEPS, LUMEN_C_DEPOSITS, LUMEN_C_TRUNCATED, LUMEN_C_MULTI, LUMEN_N_COUNT };
+enum { LUMEN_C_PHOTONS = 0, LUMEN_C_STEPS, LUMEN_C_DEPOSITS, LUMEN_C_TRUNCATED, LUMEN_C_MULTI, LUMEN_C_ABORTED,
+       LUMEN_N_COUNT };
 typedef struct LumenTallies {
   int32_t n_events;          /* events tallied (>= 1) */
   int32_t n_bins;            /* time-histogram bins per sensor (0: none) */

@@ -23,10 +23,12 @@ c_u64p = ctypes.POINTER(ctypes.c_uint64)
 MAX_GRAD = 8
 N_COL = 10
 N_HEALTH = 11
-N_COUNT = 5
+N_COUNT = 6
+F_ASYNC = 1
+N_VARIANT = 3
 HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "absorbed_surface", "rouletted",
           "reweighted", "truncated", "pushed", "start")  # fmt: skip
-COUNTS = ("photons", "steps", "deposits", "truncated", "multi")
+COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted")
 SRC_POINT, SRC_TRACK, SRC_SCINT = 0, 1, 2
 EV_F = 8
 
@@ -60,7 +62,8 @@ class LumenSource(ctypes.Structure):
 class LumenControls(ctypes.Structure):
     _fields_ = [("max_distance", ctypes.c_float), ("roulette", ctypes.c_float), ("max_vertices", ctypes.c_int32),
                 ("n_grad", ctypes.c_int32), ("grad_tab", ctypes.c_int32 * MAX_GRAD),
-                ("step_budget", ctypes.c_int64)]  # fmt: skip
+                ("step_budget", ctypes.c_int64), ("flags", ctypes.c_int32), ("variant", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]  # fmt: skip
 
 
 class LumenTallies(ctypes.Structure):
@@ -81,8 +84,10 @@ def dptr(a):
     return a.ctypes.data_as(c_f64p) if a is not None and a.size else ctypes.cast(None, c_f64p)
 
 
-def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=(), step_budget=0):
+def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=(), step_budget=0, flags=0, variant=0,
+             blocks_per_sm=0):
     c = LumenControls()
+    c.flags, c.variant, c.blocks_per_sm = int(flags), int(variant), int(blocks_per_sm)
     c.max_distance = float(max_distance)
     c.roulette = float(roulette)
     c.max_vertices = int(max_vertices)

@@ -137,16 +137,12 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
 }
 
 // The persistent photon loop: a lane refill per step (src/lumen/run.py:81 SCHEDULE = "step").
-// 256 threads, 4 blocks per SM: 64 registers a thread, 32 warps an SM (measured best of 128/256 threads at 1-8
-// blocks: the loop is latency- and divergence-bound, so warps to switch between beat registers)
-#ifndef LUMEN_MINB
-#define LUMEN_MINB 4
-#endif
-#ifndef LUMEN_BLOCK
-#define LUMEN_BLOCK 256
-#endif
-template <int G>
-__global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
+// Launch shapes (LumenControls.variant): 0 = 256 threads x 4 blocks per SM (64 registers, 32 warps an SM: the
+// measured best of 128 / 256 threads at 1-8 blocks on the tank: the loop is latency- and divergence-bound, so warps
+// to switch between beat registers), 1 = 128 x 8 (64 registers), 2 = 256 x 3 (85 registers). The autotuner
+// (lumen_b200/autotune.py) picks one per workload.
+template <int G, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
   Photon ph;
@@ -222,9 +218,10 @@ __global__ void __launch_bounds__(LUMEN_BLOCK, LUMEN_MINB) k_trace(Launch L) {
     }
   }
   // the block's health and counters: one atomic per block and value
-  __shared__ unsigned long long sc[LUMEN_N_COUNT][LUMEN_BLOCK / 32];
+  __shared__ unsigned long long sc[LUMEN_N_COUNT][BLOCK / 32];
   const int warp = threadIdx.x >> 5;
-  unsigned long long cv[LUMEN_N_COUNT] = {c_ph, c_steps, c_dep, c_trunc, c_multi};
+  unsigned long long cv[LUMEN_N_COUNT] = {c_ph, c_steps, c_dep, c_trunc, c_multi, 0ull};
+  if (threadIdx.x == 0 && L.abort_flag && *(volatile int*)L.abort_flag) cv[LUMEN_C_ABORTED] = 1ull;
 #pragma unroll
   for (int k = 0; k < LUMEN_N_COUNT; ++k) {
     unsigned long long v = cv[k];
@@ -382,6 +379,7 @@ static int fill_run(const LumenScene* sc, const LumenControls* c, Run& R) {
   if (!(c->roulette > 0.0f)) return set_err(LUMEN_ERR_ARG, "the roulette's epsilon must be > 0");
   if (c->n_grad < 0 || c->n_grad > LUMEN_MAX_GRAD) return set_err(LUMEN_ERR_NOT_SUPPORTED, "too many gradient parameters");
   if (c->max_vertices < 1) return set_err(LUMEN_ERR_ARG, "max_vertices must be >= 1");
+  if (c->variant < 0 || c->variant >= LUMEN_N_VARIANT) return set_err(LUMEN_ERR_ARG, "unknown launch variant");
   R.S = sc->S;
   R.live = sc->pool_live;
   R.ref = sc->pool_ref;
@@ -431,8 +429,32 @@ static int grid_for(const void* fn, int block, int* grid) {
   return 0;
 }
 
+template <int G, int BLOCK, int MINB>
+static int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
+  int grid = 0, st = 0;
+  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB>, BLOCK, &grid))) return st;
+  if (bps > 0) {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (sms * bps < grid) grid = sms * bps;
+  }
+  k_trace<G, BLOCK, MINB><<<grid, BLOCK, 0, stream>>>(L);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+template <int G>
+static int launch_trace(const Launch& L, int variant, int bps, cudaStream_t stream) {
+  switch (variant) {
+    case 1: return launch_shape<G, 128, 8>(L, bps, stream);
+    case 2: return launch_shape<G, 256, 3>(L, bps, stream);
+    default: return launch_shape<G, 256, 4>(L, bps, stream);
+  }
+}
+
 static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, int variant = 0, int bps = 0, int async = 0) {
   Tally& T = L.T;
   T.E = out ? (out->n_events > 0 ? out->n_events : 1) : (n_events_cot > 0 ? n_events_cot : 1);
   T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
@@ -449,8 +471,8 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
   // adjoint calls with no tallies of their own accumulate health and counts into the scratch's tail
   double* dummy = nullptr;
   if (!out) {
-    CK(cudaMallocAsync((void**)&dummy, (LUMEN_N_HEALTH + LUMEN_N_COUNT + 3) * sizeof(double), stream));
-    CK(cudaMemsetAsync(dummy, 0, (LUMEN_N_HEALTH + LUMEN_N_COUNT + 3) * sizeof(double), stream));
+    CK(cudaMallocAsync((void**)&dummy, (LUMEN_N_HEALTH + LUMEN_N_COUNT + 4) * sizeof(double), stream));
+    CK(cudaMemsetAsync(dummy, 0, (LUMEN_N_HEALTH + LUMEN_N_COUNT + 4) * sizeof(double), stream));
     T.nb = 0;
     T.arrival = T.arrival_t = T.arrival2 = nullptr;
   } else {
@@ -466,25 +488,22 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
     T.counts = out->counts;
   }
   int st = 0;
-  const int block = LUMEN_BLOCK;
-  int grid = 0;
   if (L.n > 0) {
     if (L.R.P > 0 || cot) {
-      if ((st = grid_for((const void*)k_trace<LUMEN_MAX_GRAD>, block, &grid))) return st;
-      if (!out) {
-        // an adjoint without tallies: a launch whose tallies are scratch (the arrival arrays are not written)
-        Launch L2 = L;
+      Launch L2 = L;
+      if (!out) {  // an adjoint without tallies: the health and counts go to scratch (the arrivals are not written)
         L2.T.health = dummy;
         L2.T.counts = (unsigned long long*)(dummy + LUMEN_N_HEALTH);
-        k_trace<LUMEN_MAX_GRAD><<<grid, block, 0, stream>>>(L2);
-      } else {
-        k_trace<LUMEN_MAX_GRAD><<<grid, block, 0, stream>>>(L);
       }
+      if ((st = launch_trace<LUMEN_MAX_GRAD>(L2, variant, bps, stream))) return st;
     } else {
-      if ((st = grid_for((const void*)k_trace<0>, block, &grid))) return st;
-      k_trace<0><<<grid, block, 0, stream>>>(L);
+      if ((st = launch_trace<0>(L, variant, bps, stream))) return st;
     }
-    CK(cudaGetLastError());
+  }
+  if (async) {  // enqueue only: the abort flag reaches counts[LUMEN_C_ABORTED] on the device
+    CK(cudaFreeAsync(scratch, stream));
+    if (dummy) CK(cudaFreeAsync(dummy, stream));
+    return 0;
   }
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -547,17 +566,10 @@ static int run_trace_static(Launch& L, const LumenTallies* out, cudaStream_t str
   L.next = scratch;
   L.abort_flag = (int*)(scratch + 1);
   L.steps_used = scratch + 2;
-  const int block = LUMEN_BLOCK;
-  int grid = 0;
   if (L.n > 0) {
-    if (L.R.P > 0) {
-      if ((st = grid_for((const void*)k_trace<LUMEN_MAX_GRAD>, block, &grid))) return st;
-      k_trace<LUMEN_MAX_GRAD><<<grid, block, 0, stream>>>(L);
-    } else {
-      if ((st = grid_for((const void*)k_trace<0>, block, &grid))) return st;
-      k_trace<0><<<grid, block, 0, stream>>>(L);
-    }
-    CK(cudaGetLastError());
+    if (L.R.P > 0) st = launch_trace<LUMEN_MAX_GRAD>(L, 0, 0, stream);
+    else st = launch_trace<0>(L, 0, 0, stream);
+    if (st) return st;
   }
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -683,7 +695,8 @@ int32_t lumen_b200_trace(const LumenScene* sc, const LumenRows* rows, const Lume
   Launch L;
   int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
   if (st) return st;
-  return run_trace(L, out, nullptr, 0, nullptr, (cudaStream_t)stream);
+  return run_trace(L, out, nullptr, 0, nullptr, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
+                   c->flags & LUMEN_F_ASYNC);
 }
 
 int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
@@ -695,7 +708,8 @@ int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const Lu
   Launch L;
   int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
   if (st) return st;
-  return run_trace(L, nullptr, cotangent, n_events, grads, (cudaStream_t)stream);
+  return run_trace(L, nullptr, cotangent, n_events, grads, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
+                   c->flags & LUMEN_F_ASYNC);
 }
 
 int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, const LumenSource* source,
