@@ -121,10 +121,7 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
     sl = 0.0 if surf.specularlobe is None else surf.specularlobe
     bs = 0.0 if surf.backscatter is None else surf.backscatter
     cols.update({"p_spike": ss, "p_lobe": sl, "p_back": bs, "sigma_alpha": surf.sigma_alpha})
-    lobe_on = not (isinstance(sl, (int, float)) and sl == 0.0)
-    normal = int(surf.sigma_alpha == 0.0)
-    if lobe_on and not normal:
-        raise NotImplementedError("the unified facet lobe (GLOSSY with sigma_alpha > 0) is not built")
+    normal = int(surf.sigma_alpha == 0.0)  # sigma_alpha 0: the lobe reflects about the global normal (types.py:471)
     return Row(MODEL_REFLECT, normal=normal, far_opaque=int(far_opaque), cols=cols, name=surf.name)
 
 

@@ -44,6 +44,8 @@ def lib():
         L.lumen_oracle_math.argtypes = [ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_fresnel.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_basis.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_facet_path.argtypes = [ctypes.c_float, A.c_f32p, ctypes.c_uint32, ctypes.c_uint32,
+                                              ctypes.c_int64, A.c_f32p, A.c_i64p]
         L.lumen_oracle_group_index.argtypes = [A.c_f32p, A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_source_rows.argtypes = [P(A.LumenSource), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
                                                ctypes.c_int64, A.c_f32p, A.c_i32p]
@@ -98,6 +100,16 @@ def group_index(e, n, lam):
     out = np.zeros_like(lam)
     assert lib().lumen_oracle_group_index(A.fptr(e), A.fptr(n), len(e), A.fptr(lam), lam.size, A.fptr(out)) == 0
     return out
+
+
+def facet_path(sigma, wi, n, key=(0, 7)):
+    """n unified facet paths off a flat surface (normal +z): (last directions (n, 3), paths that hit a loop bound)."""
+    wi = A.np_f32(wi)
+    out = np.zeros((n, 3), np.float32)
+    capped = np.zeros(1, np.int64)
+    assert lib().lumen_oracle_facet_path(sigma, A.fptr(wi), key[0], key[1], n, A.fptr(out),
+                                         capped.ctypes.data_as(A.c_i64p)) == 0
+    return out, int(capped[0])
 
 
 def locate(det, pts):

@@ -250,7 +250,13 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
         o_mirror(nx_er, nx_ei, h);
         break;
       }
-      case O_GLOSSY: /* the facet lobe is not built in this restatement: the engine refuses such rows */
+      case O_GLOSSY: { /* the facet path at the reference width (the lobe's weight live / reference is 1 at equal
+                          widths; a run whose width moves is refused by the engine) */
+        float rl3[3] = {o_uniform(vkey, 3), o_uniform(vkey, 4), o_uniform(vkey, 5)};
+        int capped = 0;
+        o_facet_path(re.sigma, wi, nrm, rl3, dirn, nx_er, nx_ei, &capped);
+        break;
+      }
       default:
         for (int a = 0; a < 3; ++a) dirn[a] = wi[a];
         break;
@@ -621,6 +627,26 @@ int32_t lumen_oracle_group_index(const float* e, const float* n, int32_t k, cons
   memset(&D, 0, sizeof(D));
   D.tab = tab;
   for (int64_t i = 0; i < m; ++i) out[i] = o_group_index(&D, pool.data(), 0, O_HC / lam[i]);
+  return 0;
+}
+
+/* n unified facet paths off a flat surface (normal +z) for the incoming direction wi, each from three uniforms of
+   its own key (the lobe's rand); out: the last directions (n * 3), capped: paths that hit a loop bound */
+int32_t lumen_oracle_facet_path(float sigma, const float* wi, uint32_t k0, uint32_t k1, int64_t n, float* out,
+                                int64_t* capped) {
+  const float up[3] = {0.0f, 0.0f, 1.0f};
+  OKey key = {k0, k1};
+  int64_t nc = 0;
+#pragma omp parallel for reduction(+ : nc)
+  for (int64_t i = 0; i < n; ++i) {
+    OKey k = o_fold_in(key, (uint32_t)i);
+    float r[3] = {o_uniform(k, 0), o_uniform(k, 1), o_uniform(k, 2)};
+    float er[3] = {0.0f, 1.0f, 0.0f}, ei[3] = {0.0f, 0.0f, 0.0f};
+    int c = 0;
+    o_facet_path(sigma, wi, up, r, out + 3 * i, er, ei, &c);
+    nc += c;
+  }
+  *capped = nc;
   return 0;
 }
 

@@ -395,6 +395,82 @@ static inline void o_lambert(const float* n, float r0, float r1, float* wo) {
   o_to_world(l, n, wo);
 }
 
+/* ------------------------------------------------------------------------- Geant4's unified facet path (GLOSSY) */
+#include "rng.h"
+#define O_FACET_REDRAWS 4096 /* a facet draw is accepted with probability bounded below: never reached */
+#define O_FACET_PATH 256     /* facets per path: the photon leaves with probability bounded below at each */
+
+static inline void o_to_local(const float* v, const float* n, float* l) {
+  float t1[3], t2[3];
+  o_basis(n, t1, t2);
+  l[0] = o_dot(v, t1); l[1] = o_dot(v, t2); l[2] = o_dot(v, n);
+}
+/* the half-width of the azimuth arc of facets at tilt a that face V (facets.py:299 _front_arc) */
+static inline float o_front_arc(const float* V, float a) {
+  float sv = sqrtf(V[0] * V[0] + V[1] * V[1]);
+  float sa, ca;
+  o_sincos(a, &sa, &ca);
+  float ratio = V[2] * ca / o_max(sv * sa, O_FLOOR32);
+  return o_acos(-o_min(ratio, 1.0f));
+}
+/* a unified facet normal (local frame) given V . m > 0 (facets.py:306 unified_facet): the tilt by rejection from a
+   Rayleigh(sigma) proposal, the azimuth uniform in the front arc */
+static inline void o_unified_facet(float sigma, const float* V, OKey key, float* m, int* capped) {
+  float fmax = o_min(1.0f, 4.0f * sigma);
+  float a = 0.0f, u2 = 0.5f;
+  int ok = 0;
+  for (uint32_t t = 0; t < O_FACET_REDRAWS && !ok; ++t) {
+    OKey kt = o_fold_in(key, t);
+    float u0 = o_uniform(kt, 0), u1 = o_uniform(kt, 1);
+    float al = sigma * sqrtf(-2.0f * o_log(u0));
+    if (al < 1.57079632679489661923f) {
+      float sa, ca;
+      o_sincos(al, &sa, &ca);
+      ok = u1 * al * O_PI < o_min(sa, fmax) * o_front_arc(V, al);
+    }
+    a = al;
+    u2 = o_uniform(kt, 2);
+  }
+  if (!ok) *capped = 1;
+  float psi = (2.0f * u2 - 1.0f) * o_front_arc(V, a);
+  float ph = o_atan2(V[1], V[0]) + psi;
+  float sa, ca, sp, cp;
+  o_sincos(a, &sa, &ca);
+  o_sincos(ph, &sp, &cp);
+  m[0] = sa * cp; m[1] = sa * sp; m[2] = ca;
+}
+/* a raw threefry key from the three lobe uniforms (facets.py:290 seed_key) */
+static inline OKey o_seed_key(float r0, float r1, float r2) {
+  uint32_t k0 = (uint32_t)(r0 * 8388608.0f), k1 = (uint32_t)(r1 * 8388608.0f), k2 = (uint32_t)(r2 * 8388608.0f);
+  OKey k = {k0 | (k2 << 23), k1 | ((k2 >> 9) << 23)};
+  return k;
+}
+/* the facet path: a facet for the current direction and the mirror about it, until the direction leaves the surface
+   (facets.py:323 _path_of, surface_event.py:104 _facet_path_branch: the Jones vector mirrored about each facet's half
+   vector) */
+static inline void o_facet_path(float sigma, const float* wi, const float* n, const float* rand, float* wo, float* er,
+                                float* ei, int* capped) {
+  OKey key = o_seed_key(rand[0], rand[1], rand[2]);
+  float mwi[3] = {-wi[0], -wi[1], -wi[2]};
+  float V[3];
+  o_to_local(mwi, n, V);
+  float w[3] = {wi[0], wi[1], wi[2]};
+  for (uint32_t k = 0; k < O_FACET_PATH; ++k) {
+    float m[3];
+    o_unified_facet(sigma, V, o_fold_in(key, k), m, capped);
+    float vm = o_dot(V, m);
+    float L[3] = {2.0f * vm * m[0] - V[0], 2.0f * vm * m[1] - V[1], 2.0f * vm * m[2] - V[2]};
+    o_to_world(L, n, wo);
+    float h[3] = {wo[0] - w[0], wo[1] - w[1], wo[2] - w[2]};
+    o_unit(h);
+    o_mirror(er, ei, h);
+    w[0] = wo[0]; w[1] = wo[1]; w[2] = wo[2];
+    V[0] = -L[0]; V[1] = -L[1]; V[2] = -L[2];
+    if (L[2] >= 0.0f) return;
+    if (k + 1 == O_FACET_PATH) *capped = 1;
+  }
+}
+
 /* the cumulative draw (estimator.py:62 choose): index drawn from q with one uniform, -1 if q is all 0 */
 static inline int o_choose(const float* q, int k, float rand) {
   float c[8];
