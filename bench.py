@@ -302,16 +302,20 @@ def main():
             for t in (T.arrival, T.arrival_t, T.arrival2, T.hist, T.health):
                 dist.all_reduce(t)
 
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    counts = []
+    # the clock sampler starts before the warm-up (its first nvidia-smi start-up stalls the device) and samples on
+    # through the timed steps
     with Clocks(local) as clk:
+        for k in range(args.warmup):
+            flush.fill_(float(k))
+            one_step()
+        torch.cuda.synchronize(dev)
+        time.sleep(0.5)
+        clk.rows.clear()
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
         torch.cuda.synchronize(dev)
         for k in range(args.steps):
             flush.fill_(float(k))
@@ -336,7 +340,7 @@ def main():
     ach = alg / (ms_step * 1e-3) / 1e9
     # e2e through the public call, host buffers in and out each step
     e2e_ms = []
-    for k in range(max(2, args.steps // 2) + 1):
+    for k in range(max(4, args.steps) + 1):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         light = api.simulate(det, src, samples=n, seed=0, time_bins=(200, 0.0, 1.0), device=dev)
