@@ -55,40 +55,50 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+    """The SM clock and throttle reasons sampled by one ``nvidia-smi -lms 200`` process (started once, before the
+    warm-up, so that no process start-up falls in the timed region); ``mark()`` and ``close()`` bound the rows kept."""
 
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")  # fmt: skip
 
     def __init__(self, index):
-        self.index, self.rows, self.stop_ev = index, [], threading.Event()
+        self.index, self.rows, self.t0, self.t1 = index, [], None, None
 
-    def _run(self):
-        while not self.stop_ev.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self.stop_ev.wait(0.2)
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append((time.monotonic(), [x.strip() for x in line.strip().split(",")]))
 
     def __enter__(self):
-        self.t = threading.Thread(target=self._run, daemon=True)
-        self.t.start()
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)  # fmt: skip
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
         return self
 
+    def mark(self):
+        self.t0 = time.monotonic()
+
     def __exit__(self, *a):
-        self.stop_ev.set()
-        self.t.join(timeout=10)
+        self.t1 = time.monotonic()
+        if self.p is not None:
+            time.sleep(0.25)  # one more sample after the timed region
+            self.p.terminate()
+            self.p.wait(timeout=10)
+            self.t.join(timeout=10)
 
     def summary(self):
-        sm = [float(r[0]) for r in self.rows if len(r) >= 6 and r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if len(r) >= 6 and r[1].replace(".", "").isdigit()]
+        t0, t1 = self.t0 or 0.0, (self.t1 or time.monotonic()) + 0.25
+        rows = [r for t, r in self.rows if t0 <= t <= t1 and len(r) >= 6]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[k] for r in self.rows if len(r) >= 6 for k in range(4) if r[2 + k] == "Active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[2 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(sm)}  # fmt: skip
+                "reasons": reasons, "samples": len(sm), "sampler": "nvidia-smi -lms 200 (one process)"}  # fmt: skip
 
 
 def dist_setup(args):
@@ -197,16 +207,57 @@ def run_batched(dev, det, reps=3):
             "jacobian_norm": float(np.abs(jac).sum()), "aborted": int(cnt[5])}  # fmt: skip
 
 
+def run_tank_adjoint(dev, src, n, reps=2):
+    """The tank forward + Jacobian with its wall switched to ground unified, sigma_alpha 0.1: derivatives in the
+    absorption and Rayleigh lengths, the wall reflectivity and its sigma_alpha (the facet path's score) in the same
+    launch (the 2000 PMT efficiencies' derivatives are the arrivals: after tracking)."""  # noqa: D205
+    import torch
+
+    from lumen_b200 import _abi as A
+    from lumen_b200 import detectors
+    from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
+
+    det = detectors.cylinder_tank(wall_finish="ground", sigma_alpha=0.1)
+    eng = Engine(det, dev)
+    ds = DeviceSource(src, n, dev)
+    names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R",
+             "surfaces/BlackSheet/sigma_alpha"]  # fmt: skip
+    gt = [det.params_index[k] for k in names]
+    c = A.controls(grad_tabs=gt)
+    T = DeviceTallies(det.n_sensor, ds.n_events, 200, 0.0, 1.0, len(gt), dev)
+    key = A.key_of_seed(0)
+    eng.trace(key, min(n, 1 << 20), source=ds, controls=c, tallies=T)
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        T.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.trace(key, n, source=ds, controls=c, tallies=T)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    cnt = T.counts.cpu().numpy()
+    m = float(np.median(ms))
+    jac = T.jac.cpu().numpy()[0]
+    eng.close()
+    return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
+            "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
+            "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
+            "jacobian_abs_sum": [float(x) for x in np.abs(jac).sum(0)]}  # fmt: skip
+
+
 def run_lar(dev, n, reps=2):
     """The liquid-argon box: 10^4 scintillation points, forward + Jacobian over the cage reflectivity and the
-    Rayleigh length (the sensor efficiencies' derivatives are the arrivals: after tracking)."""  # noqa: D205
+    Rayleigh length (the sensor efficiencies' derivatives are the arrivals: after tracking). The cage and cathode are
+    ground unified with sigma_alpha 0.1."""  # noqa: D205
     import torch
 
     from lumen_b200 import _abi as A
     from lumen_b200 import detectors, sources
     from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
 
-    det = detectors.lar_box()
+    det = detectors.lar_box(sigma_alpha=0.1)
     pts = np.random.default_rng(77).uniform([-2.4, -1.9, -1.9], [2.4, 1.9, 1.9], (10000, 3))
     src = sources.Scintillation(position=pts, lam=128.0, tau=(6.0, 1500.0), fraction=0.25, n_photons=1.0)
     eng = Engine(det, dev)
@@ -238,7 +289,7 @@ def run_lar(dev, n, reps=2):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lumen_b200")
     ap.add_argument("--photons", type=int, default=1 << 24)
@@ -303,15 +354,13 @@ def main():
                 dist.all_reduce(t)
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    # the clock sampler starts before the warm-up (its first nvidia-smi start-up stalls the device) and samples on
-    # through the timed steps
+    # the clock sampler starts before the warm-up and samples on through the timed steps
     with Clocks(local) as clk:
         for k in range(args.warmup):
             flush.fill_(float(k))
             one_step()
         torch.cuda.synchronize(dev)
-        time.sleep(0.5)
-        clk.rows.clear()
+        clk.mark()
         if world > 1:
             import torch.distributed as dist
 
@@ -361,6 +410,7 @@ def main():
             "gpu_launches": args.steps, "clocks": clk.summary(), "ms_steps": [round(x, 3) for x in ms],
             "arrivals_sum": float(light.arrivals.sum())}  # fmt: skip
     if rank == 0 and not args.no_extra:
+        line["tank_fwd_adjoint"] = run_tank_adjoint(dev, src, n)
         line["batched_fwd_adjoint"] = run_batched(dev, det)
         line["lar_fwd_adjoint"] = run_lar(dev, args.lar_photons)
     if rank == 0 and not args.no_cpu:

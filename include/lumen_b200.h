@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 1
+#define LUMEN_B200_ABI_VERSION 2
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -81,6 +81,19 @@ enum { LUMEN_MI_INDEX = 0, LUMEN_MI_ABS = 1, LUMEN_MI_RAY = 2, LUMEN_MED_I = 4 }
 #define LUMEN_MAX_KNOTS 64    /* knots of an index table (its group index is tabulated per call) */
 #define LUMEN_MAX_BVH_DEPTH 24 /* levels of a volume's daughter BVH (the traversal's stack) */
 
+/* The unified facet lobe's tables (src/lumen/surfaces/facets.py:127 unified_tables; grid in
+   src/lumen/rules/choices.py:101 UNIFIED_TABLE): the facing share F on x = (2/pi) atan2(cos theta, sigma sin theta)
+   (NX uniform nodes of [0, 1]) by y = log sigma = Y0 + DY j, j in [J_LO, J_LO + NY), with its node derivatives Fx,
+   Fy, Fxy (each NX x NY float32, row-major: F[i * NY + j]), then log zeta = log(Z / sigma^2) and its derivative in
+   y (NY each), flat in that order. sigma_alpha of a unified facet row must lie in [exp(Y0 + DY J_LO),
+   exp(Y0 + DY (J_LO + NY - 1))] = [0.00276, 1] rad. */
+#define LUMEN_UNI_NX 257
+#define LUMEN_UNI_NY 69
+#define LUMEN_UNI_J_LO (-52)
+#define LUMEN_UNI_Y0 (-1.38629436111989061883)  /* log(1/4) */
+#define LUMEN_UNI_DY 0.08664339756999316368     /* log(2) / 8 */
+#define LUMEN_UNI_WORDS (4 * LUMEN_UNI_NX * LUMEN_UNI_NY + 2 * LUMEN_UNI_NY)
+
 /* ------------------------------------------------------------------------------------------ the detector */
 typedef struct LumenSceneDesc {
   /* geometry (the navigator's arrays, src/lumen/geometry/navigator_build.py:51, csg_build.py:30) */
@@ -105,6 +118,8 @@ typedef struct LumenSceneDesc {
   const int32_t* row_i;      /* host, n_row * LUMEN_ROW_I */
   const int32_t* tab;        /* host, n_tab * 2 */
   const float* pool;         /* host, n_pool: the table values every call reads unless set_pools replaces them */
+  const float* unified;      /* host, LUMEN_UNI_WORDS: the unified facet tables; may be null when no row draws the
+                                unified facet lobe (src/lumen/surfaces/facets.py:165 table_operands) */
 } LumenSceneDesc;
 
 typedef struct LumenScene LumenScene; /* opaque: the device copy of a LumenSceneDesc */
@@ -182,7 +197,9 @@ int32_t lumen_b200_abi_version(void);
 const char* lumen_b200_last_error(void);
 
 /* Upload a detector to the current CUDA device; replaces the reference's Navigator.operands / pack.pack device put
-   (src/lumen/geometry/navigate.py:140, src/lumen/api.py:842). */
+   (src/lumen/geometry/navigate.py:140, src/lumen/api.py:842). Unified rows with sigma_alpha > 0 draw Geant4's facet
+   path (src/lumen/surfaces/facets.py:372), weighted by its path density from desc->unified; a GLISUR row is refused
+   (LUMEN_ERR_SCENE). */
 int32_t lumen_b200_scene_create(const LumenSceneDesc* desc, LumenScene** out);
 /* Replace the live and reference parameter pools (host, n_pool floats each; ref may be null: the live pool): the
    reference's packed params and reference (src/lumen/transport/step.py:129 `operands`). */

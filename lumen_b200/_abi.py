@@ -26,6 +26,8 @@ N_HEALTH = 11
 N_COUNT = 6
 F_ASYNC = 1
 N_VARIANT = 3
+UNI_NX, UNI_NY = 257, 69
+UNI_WORDS = 4 * UNI_NX * UNI_NY + 2 * UNI_NY
 HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "absorbed_surface", "rouletted",
           "reweighted", "truncated", "pushed", "start")  # fmt: skip
 COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted")
@@ -44,7 +46,7 @@ class LumenSceneDesc(ctypes.Structure):
         ("n_cls", ctypes.c_int32), ("n_med", ctypes.c_int32), ("n_row", ctypes.c_int32), ("n_tab", ctypes.c_int32),
         ("n_pool", ctypes.c_int32), ("n_sensor", ctypes.c_int32),
         ("cls_medium", c_i32p), ("row_of", c_i32p), ("med_i", c_i32p), ("row_i", c_i32p), ("tab", c_i32p),
-        ("pool", c_f32p),
+        ("pool", c_f32p), ("unified", c_f32p),
     ]  # fmt: skip
 
 

@@ -56,6 +56,7 @@ struct DScene {
   const int32_t* __restrict__ med_i;
   const int32_t* __restrict__ row_i;
   const int32_t* __restrict__ tab;
+  const float* __restrict__ uni;  // the unified facet tables (LUMEN_UNI_WORDS), null without a unified facet row
 };
 
 L_DEV float d_dot(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }

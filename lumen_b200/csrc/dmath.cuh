@@ -139,6 +139,29 @@ L_DEV float l_acos(float x) {
   return PI - 2.0f * l_asin_small(sqrtf((1.0f + x) * 0.5f));
 }
 
+L_DEV float l_asin(float v) {
+  const float PIO2 = 1.57079632679489661923f;
+  float a = fabsf(v);
+  if (a > 1.0f) a = 1.0f;
+  float r = a <= 0.5f ? l_asin_small(a) : PIO2 - 2.0f * l_asin_small(sqrtf((1.0f - a) * 0.5f));
+  return v < 0.0f ? -r : r;
+}
+
+// atan2 from asin / acos on the octant where each is well conditioned
+L_DEV float l_atan2(float y, float x) {
+  const float PI = 3.14159265358979323846f;
+  float r = sqrtf(x * x + y * y);
+  if (r == 0.0f) return 0.0f;
+  float a;
+  if (fabsf(y) <= fabsf(x)) {
+    a = l_asin(fabsf(y) / r);
+    if (x < 0.0f) a = PI - a;
+  } else {
+    a = l_acos(x / r);
+  }
+  return y < 0.0f ? -a : a;
+}
+
 L_DEV float l_erfinv(float x) {
   float w = -l_log((1.0f - x) * (1.0f + x));
   float p;

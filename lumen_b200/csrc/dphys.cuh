@@ -387,6 +387,193 @@ L_DEV void d_lambert(const float* n, float r0, float r1, float* wo) {
   float l[3] = {r * cp, r * sp, sqrtf(1.0f - r0)};
   d_to_world(l, n, wo);
 }
+// ---------------------------------------------------------------- Geant4's unified facet path (GLOSSY), facets.py
+#define D_FACET_REDRAWS 4096  // a facet draw is accepted with a probability bounded below: never reached
+#define D_FACET_PATH 256      // facets per path: the photon leaves with a probability bounded below at each
+
+L_DEV void d_to_local(const float* v, const float* n, float* l) {
+  float t1[3], t2[3];
+  d_basis(n, t1, t2);
+  l[0] = d_dot(v, t1); l[1] = d_dot(v, t2); l[2] = d_dot(v, n);
+}
+L_DEV float d_front_arc(const float* V, float a) {
+  float sv = sqrtf(V[0] * V[0] + V[1] * V[1]);
+  float sa, ca;
+  l_sincos(a, &sa, &ca);
+  float ratio = V[2] * ca / d_max(sv * sa, D_FLOOR32);
+  return l_acos(-d_min(ratio, 1.0f));
+}
+L_CALL void d_unified_facet(float sigma, const float* V, Key key, float* m, int* capped) {
+  float fmax = d_min(1.0f, 4.0f * sigma);
+  float a = 0.0f, u2 = 0.5f;
+  int ok = 0;
+  for (uint32_t t = 0; t < D_FACET_REDRAWS && !ok; ++t) {
+    Key kt = fold_in(key, t);
+    float u0 = uniform(kt, 0), u1 = uniform(kt, 1);
+    float al = sigma * sqrtf(-2.0f * l_log(u0));
+    if (al < 1.57079632679489661923f) {
+      float sa, ca;
+      l_sincos(al, &sa, &ca);
+      ok = u1 * al * 3.14159265358979323846f < d_min(sa, fmax) * d_front_arc(V, al);
+    }
+    a = al;
+    u2 = uniform(kt, 2);
+  }
+  if (!ok) *capped = 1;
+  float psi = (2.0f * u2 - 1.0f) * d_front_arc(V, a);
+  float ph = l_atan2(V[1], V[0]) + psi;
+  float sa, ca, sp, cp;
+  l_sincos(a, &sa, &ca);
+  l_sincos(ph, &sp, &cp);
+  m[0] = sa * cp; m[1] = sa * sp; m[2] = ca;
+}
+L_DEV Key d_seed_key(float r0, float r1, float r2) {
+  uint32_t k0 = (uint32_t)(r0 * 8388608.0f), k1 = (uint32_t)(r1 * 8388608.0f), k2 = (uint32_t)(r2 * 8388608.0f);
+  Key k;
+  k.k0 = k0 | (k2 << 23);
+  k.k1 = k1 | ((k2 >> 9) << 23);
+  return k;
+}
+// ---- the unified lobe's tables (facets.py:153-207): C1 cubic Hermite of log zeta in y = log sigma, bicubic Hermite
+// of the facing share F in (x, y), each with its derivative(s) in the coordinates
+#define D_UNI_Y0 ((float)LUMEN_UNI_Y0)
+#define D_UNI_DY ((float)LUMEN_UNI_DY)
+#define D_HALF_PI 1.57079632679489661923f
+#define D_LOG_TINY (-69.07755278982137f)  // log FLOOR32: a log density off the support (facets.py:61)
+#define D_LOG_2PI 1.83787706640934548356f
+
+L_DEV void d_uni_cell(float v, int n, int* i, float* t, float* dt) {
+  float top = (float)(n - 1);
+  float f = v < 0.0f ? 0.0f : (v > top ? top : v);
+  *dt = (v < 0.0f || v > top) ? 0.0f : 1.0f;
+  int k = (int)floorf(f);
+  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+  *i = k;
+  *t = f - (float)k;
+}
+L_DEV void d_hermite(float t, float* h, float* dh) {
+  float t2 = t * t, t3 = t2 * t;
+  h[0] = 2.0f * t3 - 3.0f * t2 + 1.0f;
+  h[1] = t3 - 2.0f * t2 + t;
+  h[2] = -2.0f * t3 + 3.0f * t2;
+  h[3] = t3 - t2;
+  dh[0] = 6.0f * t2 - 6.0f * t;
+  dh[1] = 3.0f * t2 - 4.0f * t + 1.0f;
+  dh[2] = -6.0f * t2 + 6.0f * t;
+  dh[3] = 3.0f * t2 - 2.0f * t;
+}
+L_DEV float d_table_lz(const float* __restrict__ U, float y, float* dy) {
+  const float* v = U + 4 * LUMEN_UNI_NX * LUMEN_UNI_NY;
+  const float* dv = v + LUMEN_UNI_NY;
+  int j;
+  float t, dt, h[4], dh[4];
+  d_uni_cell((y - D_UNI_Y0) / D_UNI_DY - (float)LUMEN_UNI_J_LO, LUMEN_UNI_NY, &j, &t, &dt);
+  d_hermite(t, h, dh);
+  float v0 = __ldg(v + j), v1 = __ldg(v + j + 1), d0 = __ldg(dv + j), d1 = __ldg(dv + j + 1);
+  float out = h[0] * v0 + h[2] * v1 + D_UNI_DY * (h[1] * d0 + h[3] * d1);
+  float dout = dh[0] * v0 + dh[2] * v1 + D_UNI_DY * (dh[1] * d0 + dh[3] * d1);
+  *dy = dout * dt / D_UNI_DY;
+  return out;
+}
+L_DEV float d_table_front(const float* __restrict__ U, float x, float y, float* dFx, float* dFy) {
+  const int NY = LUMEN_UNI_NY, NN = LUMEN_UNI_NX * LUMEN_UNI_NY;
+  int i, j;
+  float tx, ty, dtx, dty, hx4[4], dhx4[4], hy4[4], dhy4[4];
+  d_uni_cell(x * (float)(LUMEN_UNI_NX - 1), LUMEN_UNI_NX, &i, &tx, &dtx);
+  d_uni_cell((y - D_UNI_Y0) / D_UNI_DY - (float)LUMEN_UNI_J_LO, NY, &j, &ty, &dty);
+  const float hx = 1.0f / (float)(LUMEN_UNI_NX - 1);
+  d_hermite(tx, hx4, dhx4);
+  d_hermite(ty, hy4, dhy4);
+  float out = 0.0f, ox = 0.0f, oy = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      int k = (i + di) * NY + (j + dj);
+      float a0 = __ldg(U + k), a1 = __ldg(U + NN + k), a2 = __ldg(U + 2 * NN + k), a3 = __ldg(U + 3 * NN + k);
+      float ax = hx4[2 * di], bx = hx4[2 * di + 1], ay = hy4[2 * dj], by = hy4[2 * dj + 1];
+      float dax = dhx4[2 * di], dbx = dhx4[2 * di + 1], day = dhy4[2 * dj], dby = dhy4[2 * dj + 1];
+      out = out + (ax * ay * a0 + bx * ay * hx * a1 + ax * by * D_UNI_DY * a2 + bx * by * hx * D_UNI_DY * a3);
+      ox = ox + (dax * ay * a0 + dbx * ay * hx * a1 + dax * by * D_UNI_DY * a2 + dbx * by * hx * D_UNI_DY * a3);
+      oy = oy + (ax * day * a0 + bx * day * hx * a1 + ax * dby * D_UNI_DY * a2 + bx * dby * hx * D_UNI_DY * a3);
+    }
+  *dFx = ox * dtx * (float)(LUMEN_UNI_NX - 1);
+  *dFy = oy * dty / D_UNI_DY;
+  return out;
+}
+// log p1(w1 | w0) of one unified facet reflection at width sigma and (want_d) its derivative in sigma
+// (facets.py:209 _unified_log_density, :248 _half_vector, :259 unified_facet_logpdf)
+L_CALL float d_unified_logpdf(const float* __restrict__ U, float sigma, const float* w0, const float* n,
+                              const float* w1, int want_d, float* dls) {
+  float mw[3] = {-w0[0], -w0[1], -w0[2]};
+  float V[3], W[3];
+  d_to_local(mw, n, V);
+  d_to_local(w1, n, W);
+  float H[3] = {V[0] + W[0], V[1] + W[1], V[2] + W[2]};
+  float vH = d_dot(V, H);
+  *dls = 0.0f;
+  if (!(H[2] > 0.0f && vH > 0.0f)) return D_LOG_TINY;
+  float inv = 1.0f / sqrtf(d_dot(H, H));
+  float vh = vH * inv;
+  float ch = H[2] * inv;
+  float s = sqrtf(H[0] * H[0] + H[1] * H[1]) * inv;
+  float alpha = l_atan2(s, ch);
+  float l4 = l_log(4.0f * sigma);
+  float lf = d_min(0.0f, l4);
+  float ef = l_exp(lf);
+  float ls = l_log(s > ef ? s : ef);
+  float cos_t = V[2], sin_t = sqrtf(V[0] * V[0] + V[1] * V[1]);
+  float y = l_log(sigma);
+  float dlz, dFx, dFy;
+  float lz = d_table_lz(U, y, &dlz);
+  float x = l_atan2(cos_t, sigma * sin_t) / D_HALF_PI;
+  float F = d_table_front(U, x, y, &dFx, &dFy);
+  float lp = -alpha * alpha / (2.0f * sigma * sigma) + (lf - ls) - D_LOG_2PI - 2.0f * y - lz - l_log(F);
+  lp = lp - l_log(4.0f * vh);
+  if (want_d) {
+    float is = 1.0f / sigma;
+    float dlf = l4 < 0.0f ? is : (l4 == 0.0f ? 0.5f * is : 0.0f);
+    float dsel = s > ef ? dlf : 0.0f;
+    float sb = sigma * sin_t;
+    float dx = -(cos_t * sin_t) / (cos_t * cos_t + sb * sb) / D_HALF_PI;
+    *dls = alpha * alpha / (sigma * sigma * sigma) + dsel - 2.0f * is - dlz * is - (dFx * dx + dFy * is) / F;
+  }
+  return lp;
+}
+
+// the facet path (facets.py:372 _path_of; the Jones vector mirrored about each facet's half vector,
+// surface_event.py:106 _facet_path_branch). With the tables U each facet's log density is summed: at the live width
+// into lp (with its derivative in sigma into dls where want_d), and where weigh is set at the drawn width into lr.
+L_CALL void d_facet_path(float sigma, const float* wi, const float* n, float r0, float r1, float r2, float* wo,
+                         float* er, float* ei, int* capped, const float* __restrict__ U, float sig_live, int weigh,
+                         int want_d, float* lp, float* lr, float* dls) {
+  Key key = d_seed_key(r0, r1, r2);
+  float mwi[3] = {-wi[0], -wi[1], -wi[2]};
+  float V[3];
+  d_to_local(mwi, n, V);
+  float w[3] = {wi[0], wi[1], wi[2]};
+  for (uint32_t k = 0; k < D_FACET_PATH; ++k) {
+    float m[3];
+    d_unified_facet(sigma, V, fold_in(key, k), m, capped);
+    float vm = d_dot(V, m);
+    float L[3] = {2.0f * vm * m[0] - V[0], 2.0f * vm * m[1] - V[1], 2.0f * vm * m[2] - V[2]};
+    d_to_world(L, n, wo);
+    if (U) {
+      float d;
+      *lp = *lp + d_unified_logpdf(U, sig_live, w, n, wo, want_d, &d);
+      if (want_d) *dls = *dls + d;
+      if (weigh) *lr = *lr + d_unified_logpdf(U, sigma, w, n, wo, 0, &d);
+    }
+    float h[3] = {wo[0] - w[0], wo[1] - w[1], wo[2] - w[2]};
+    d_unit(h);
+    d_mirror(er, ei, h);
+    w[0] = wo[0]; w[1] = wo[1]; w[2] = wo[2];
+    V[0] = -L[0]; V[1] = -L[1]; V[2] = -L[2];
+    if (L[2] >= 0.0f) return;
+    if (k + 1 == D_FACET_PATH) *capped = 1;
+  }
+}
+
 L_DEV int d_choose6(const float* q, float rand) {
   float c[N_OUT];
   float s = 0.0f;

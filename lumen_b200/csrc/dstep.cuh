@@ -175,6 +175,7 @@ L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float
     float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
     float w_if = ph.w * rr * att_if * r_live;
     float dirn[3], wi[3] = {ph.d[0], ph.d[1], ph.d[2]};
+    float lobe_w = 1.0f, lobe_dls = 0.0f;
     const float* nrm = q.normal;
     float eta = ml.n / n2l;
     float s_ax[3];
@@ -216,6 +217,13 @@ L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float
       float h[3] = {dirn[0] - wi[0], dirn[1] - wi[1], dirn[2] - wi[2]};
       d_unit(h);
       d_mirror(nx_er, nx_ei, h);
+    } else if (os_ == GLOSSY) {  // the facet path drawn at the reference width, weighted live over reference
+      int capped = 0;
+      float lp = 0.0f, lr = 0.0f;
+      int dens = !R.shared || P > 0;
+      d_facet_path(re.sigma, wi, nrm, uniform(vkey, 3), uniform(vkey, 4), uniform(vkey, 5), dirn, nx_er, nx_ei,
+                   &capped, dens ? S.uni : nullptr, le.sigma, !R.shared, P > 0, &lp, &lr, &lobe_dls);
+      if (!R.shared) lobe_w = l_exp(lp - lr);
     } else {
 #pragma unroll
       for (int a = 0; a < 3; ++a) dirn[a] = wi[a];
@@ -237,16 +245,19 @@ L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float
     fates0 = ok ? w_at * att_if * s_cont : 0.0f;
     fates1 = q.hit ? w_at * (1.0f - att_if) : 0.0f;
     fates2 = (q.hit && row >= 0) ? w_at * att_if * (1.0f - s_cont) : 0.0f;
-    nx_w = w_if * 1.0f;
-    if (G > 0)
+    nx_w = w_if * lobe_w;
+    if (G > 0) {
+      int t_sig = row >= 0 ? __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_COL + LUMEN_COL_SIGMA) : -1;
       for (int p = 0; p < P; ++p) {
         float dpl = dprobs[p][os_];
         float dr_live = drawn ? (pp != 0.0f ? dpl / pp : 0.0f) : 0.0f;
         float drr = reach_ref != 0.0f ? d_reach[p] / reach_ref : 0.0f;
         float X = rr * att_if * r_live;
         float dX = drr * att_if * r_live + rr * d_att[p] * r_live + rr * att_if * dr_live;
-        nx_dw[p] = (dw[p] * X + ph.w * dX) * 1.0f;
+        float dsig = (t_sig >= 0 && t_sig == R.gt[p]) ? 1.0f : 0.0f;
+        nx_dw[p] = (dw[p] * X + ph.w * dX) * lobe_w + w_if * lobe_w * (lobe_dls * dsig);
       }
+    }
     nx_cls = far_ ? ca : cb;
     nx_ok = ok;
     nx_dtime = dist / v_g;

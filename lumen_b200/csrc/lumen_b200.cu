@@ -11,6 +11,7 @@
 // Numerics: compiled with -fmad=false; every fused multiply-add is an explicit fmaf, every elementary function the
 // library's own (dmath.cuh), so a photon's path is the CPU checker's bit for bit.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -42,6 +43,8 @@ struct LumenScene {
   float* pool_ref;  // == pool_live unless a distinct reference is set
   int n_pool;
   std::vector<void*> allocs;
+  std::vector<int32_t> sigma_tabs;  // the sigma_alpha tables of the unified facet rows
+  std::vector<int32_t> tab;         // host copy of the (offset, knots) table index
 };
 
 // --------------------------------------------------------------------------------------------- the kernels
@@ -362,14 +365,25 @@ static int check_desc(const LumenSceneDesc* d) {
   for (int c = 0; c < d->n_cls; ++c)
     if (d->cls_medium[c] < 0 || d->cls_medium[c] >= d->n_med) return set_err(LUMEN_ERR_ARG, "scene_create: a medium is out of range");
   for (int r = 0; r < d->n_row; ++r) {
-    /* the facet lobe (GLOSSY with sigma_alpha > 0) is not built: such a row is refused */
     const int32_t* ri = d->row_i + r * LUMEN_ROW_I;
-    int tl = ri[LUMEN_RI_COL + LUMEN_COL_PLOBE];
-    int off = d->tab[2 * tl], k = d->tab[2 * tl + 1];
-    float pl = 0.0f;
-    for (int j = 0; j < k; ++j) pl = pl > d->pool[off + k + j] ? pl : d->pool[off + k + j];
-    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && pl > 0.0f)
-      return set_err(LUMEN_ERR_SCENE, "scene_create: a surface row draws the unified facet lobe (not built)");
+    for (int c = 0; c < LUMEN_N_COL; ++c)
+      if (ri[LUMEN_RI_COL + c] < 0 || ri[LUMEN_RI_COL + c] >= d->n_tab) return set_err(LUMEN_ERR_ARG, "scene_create: a column table is out of range");
+    if (ri[LUMEN_RI_GLISUR]) return set_err(LUMEN_ERR_SCENE, "scene_create: the GLISUR facet path is not built");
+    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && !d->unified)
+      return set_err(LUMEN_ERR_ARG, "scene_create: a unified facet row needs the unified tables (desc->unified)");
+  }
+  return 0;
+}
+
+// sigma_alpha of every unified facet row within the tables' span (src/lumen/rules/choices.py:103 SIGMA_MIN/MAX)
+static int check_widths(const LumenScene* sc, const float* pool) {
+  const double lo = exp(LUMEN_UNI_Y0 + LUMEN_UNI_DY * LUMEN_UNI_J_LO);
+  const double hi = exp(LUMEN_UNI_Y0 + LUMEN_UNI_DY * (LUMEN_UNI_J_LO + LUMEN_UNI_NY - 1));
+  for (int t : sc->sigma_tabs) {
+    int off = sc->tab[2 * t], k = sc->tab[2 * t + 1];
+    for (int j = off + k; j < off + 2 * k; ++j)
+      if (!(pool[j] >= (float)lo * 0.9999f && pool[j] <= (float)hi * 1.0001f))
+        return set_err(LUMEN_ERR_ARG, "a unified facet row's sigma_alpha is outside [0.00276, 1] rad");
   }
   return 0;
 }
@@ -645,10 +659,22 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   UPLOAD(S.tab, d->tab, (size_t)d->n_tab * 2);
   const float* pl = nullptr;
   UPLOAD(pl, d->pool, (size_t)d->n_pool);
+  S.uni = nullptr;
+  if (d->unified) UPLOAD(S.uni, d->unified, (size_t)LUMEN_UNI_WORDS);
   if (e) {
     for (void* p : sc->allocs) cudaFree(p);
     delete sc;
     return LUMEN_ERR_CUDA;
+  }
+  for (int r = 0; r < d->n_row; ++r) {
+    const int32_t* ri = d->row_i + r * LUMEN_ROW_I;
+    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL]) sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
+  }
+  sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
+  if (check_widths(sc, d->pool)) {
+    for (void* p : sc->allocs) cudaFree(p);
+    delete sc;
+    return LUMEN_ERR_ARG;
   }
   sc->pool_live = const_cast<float*>(pl);
   sc->pool_ref = sc->pool_live;
@@ -660,6 +686,7 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
 int32_t lumen_b200_scene_set_pools(LumenScene* sc, const float* live, const float* ref) {
   g_err.clear();
   if (!sc || !live) return set_err(LUMEN_ERR_ARG, "scene or live pool is null");
+  if (check_widths(sc, live) || (ref && check_widths(sc, ref))) return LUMEN_ERR_ARG;
   CK(cudaMemcpy(sc->pool_live, live, sc->n_pool * sizeof(float), cudaMemcpyHostToDevice));
   if (ref && ref != live) {
     if (sc->pool_ref == sc->pool_live) {

@@ -16,6 +16,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from lumen_b200 import facets
 from lumen_b200 import geometry as G
 from lumen_b200 import optics as O
 
@@ -89,7 +90,16 @@ class Detector:
         d.n_tab, d.n_pool, d.n_sensor = len(keep["tab"]), len(keep["pool"]), self.n_sensor
         d.cls_medium, d.row_of, d.med_i = iptr(keep["cls_medium"]), iptr(keep["row_of"]), iptr(keep["med_i"])
         d.row_i, d.tab, d.pool = iptr(keep["row_i"]), iptr(keep["tab"]), fptr(keep["pool"])
+        if self.draws_facets:  # a unified facet row (reflect, not about the global normal): the lobe's tables
+            keep["unified"] = facets.flat()
+            d.unified = fptr(keep["unified"])
         return d, keep
+
+    @property
+    def draws_facets(self) -> bool:
+        """Whether a surface row draws the unified facet lobe (its density reads the unified tables)."""
+        r = self.arrays["row_i"].reshape(-1, 16)
+        return bool(((r[:, 0] == 0) & (r[:, 1] == 0)).any())
 
 
 def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None) -> Detector:

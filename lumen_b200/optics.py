@@ -20,6 +20,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from lumen_b200 import facets
+
 HC = 1239.8419843320025  # h c in eV nm (src/lumen/units.py:20)
 HC_EV_M = HC * 1e-9
 # G4OpRayleigh::CalculateRayleighMeanFreePaths for a material named "Water" (src/lumen/rules/optics.py:98-103)
@@ -78,6 +80,7 @@ class OpticalSurface:
     finish: str = "polished"  # or "ground"
     model: str = "unified"
     sigma_alpha: float = 0.0
+    polish: float = 1.0  # GLISUR's polish (its facet radius is 1 - polish)
     reflectivity: object = None
     efficiency: object = None
     transmittance: object = None
@@ -114,14 +117,19 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
     # dielectric_metal
     R = 1.0 if surf.reflectivity is None else surf.reflectivity
     cols = {"R": R, "eff": eff, "T": 0.0 if surf.transmittance is None else surf.transmittance}
+    if surf.model == "glisur" and surf.finish != "polished" and surf.polish < 1.0:
+        raise NotImplementedError("the GLISUR facet path (dielectric_metal, glisur, ground, polish < 1) is not built")
     if surf.finish == "polished" or surf.model == "glisur":
-        cols["p_spike"] = 1.0  # polished: the mirror (types.py:573 SPECULAR_METAL)
+        cols["p_spike"] = 1.0  # polished, or GLISUR at polish 1: the mirror (types.py:573 SPECULAR_METAL)
         return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
     ss = 0.0 if surf.specularspike is None else surf.specularspike
     sl = 0.0 if surf.specularlobe is None else surf.specularlobe
     bs = 0.0 if surf.backscatter is None else surf.backscatter
     cols.update({"p_spike": ss, "p_lobe": sl, "p_back": bs, "sigma_alpha": surf.sigma_alpha})
     normal = int(surf.sigma_alpha == 0.0)  # sigma_alpha 0: the lobe reflects about the global normal (types.py:471)
+    if not normal and not (facets.SIGMA_MIN <= surf.sigma_alpha <= facets.SIGMA_MAX):
+        raise ValueError(f"surface {surf.name}: sigma_alpha {surf.sigma_alpha} outside the unified tables' span "
+                         f"[{facets.SIGMA_MIN:.5f}, {facets.SIGMA_MAX}] rad (or exactly 0)")  # fmt: skip
     return Row(MODEL_REFLECT, normal=normal, far_opaque=int(far_opaque), cols=cols, name=surf.name)
 
 

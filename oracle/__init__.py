@@ -45,7 +45,9 @@ def lib():
         L.lumen_oracle_fresnel.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_basis.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_facet_path.argtypes = [ctypes.c_float, A.c_f32p, ctypes.c_uint32, ctypes.c_uint32,
-                                              ctypes.c_int64, A.c_f32p, A.c_i64p]
+                                              ctypes.c_int64, A.c_f32p, A.c_i64p, A.c_f32p, ctypes.c_float, A.c_f32p,
+                                              ctypes.c_int32]  # fmt: skip
+        L.lumen_oracle_unified.argtypes = [A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_group_index.argtypes = [A.c_f32p, A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_source_rows.argtypes = [P(A.LumenSource), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
                                                ctypes.c_int64, A.c_f32p, A.c_i32p]
@@ -102,14 +104,34 @@ def group_index(e, n, lam):
     return out
 
 
-def facet_path(sigma, wi, n, key=(0, 7)):
-    """n unified facet paths off a flat surface (normal +z): (last directions (n, 3), paths that hit a loop bound)."""
+def facet_path(sigma, wi, n, key=(0, 7), *, sig_live=None, one=False):
+    """n unified facet paths off a flat surface (normal +z): (last directions (n, 3), paths that hit a loop bound),
+    and with ``sig_live`` also the paths' log densities (n, 3): at sig_live, at sigma, d / d sig_live of the first.
+    ``one``: single facet reflections instead of paths."""  # noqa: D205, D209
+    from lumen_b200 import facets
+
     wi = A.np_f32(wi)
     out = np.zeros((n, 3), np.float32)
     capped = np.zeros(1, np.int64)
+    U = facets.flat() if sig_live is not None else None
+    dens = np.zeros((n, 3), np.float32) if U is not None else None
     assert lib().lumen_oracle_facet_path(sigma, A.fptr(wi), key[0], key[1], n, A.fptr(out),
-                                         capped.ctypes.data_as(A.c_i64p)) == 0
-    return out, int(capped[0])
+                                         capped.ctypes.data_as(A.c_i64p), A.fptr(U),
+                                         0.0 if sig_live is None else sig_live, A.fptr(dens), int(one)) == 0  # fmt: skip
+    return (out, int(capped[0])) if U is None else (out, int(capped[0]), dens)
+
+
+def unified(fn, inp, U=None):
+    """The unified tables and density (lumen_oracle_unified): fn 0 log zeta at y; 1 F at (x, y); 2 log p1 at
+    (sigma, w0, n, w1). Returns the values with their derivatives, one row per input."""  # noqa: D205, D209
+    from lumen_b200 import facets
+
+    U = facets.flat() if U is None else A.np_f32(U)
+    width, nout = {0: (1, 2), 1: (2, 3), 2: (10, 2)}[fn]
+    inp = A.np_f32(inp).reshape(-1, width)
+    out = np.zeros((len(inp), nout), np.float32)
+    assert lib().lumen_oracle_unified(A.fptr(U), fn, A.fptr(inp), len(inp), A.fptr(out)) == 0
+    return out
 
 
 def locate(det, pts):

@@ -206,7 +206,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
     float dirn[3], wi[3] = {ph->d[0], ph->d[1], ph->d[2]};
     const float* nrm = q.normal;
     float eta = ml.n / n2l;
-    float out_w = 1.0f, out_wd = 1.0f;
+    float out_w = 1.0f, out_wd = 1.0f, lobe_dls = 0.0f;
     int out_far = 0;
     float s_ax[3];
     o_s_axis(wi, nrm, s_ax);
@@ -250,11 +250,16 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
         o_mirror(nx_er, nx_ei, h);
         break;
       }
-      case O_GLOSSY: { /* the facet path at the reference width (the lobe's weight live / reference is 1 at equal
-                          widths; a run whose width moves is refused by the engine) */
+      case O_GLOSSY: { /* the facet path drawn at the reference width, weighted by its path density live over
+                          reference (surface_event.py:106 _facet_path_branch): 1 without a reference, whose
+                          derivative is the path's score in sigma */
         float rl3[3] = {o_uniform(vkey, 3), o_uniform(vkey, 4), o_uniform(vkey, 5)};
         int capped = 0;
-        o_facet_path(re.sigma, wi, nrm, rl3, dirn, nx_er, nx_ei, &capped);
+        float lp = 0.0f, lr = 0.0f;
+        int dens = !R->shared || P > 0;
+        o_facet_path(re.sigma, wi, nrm, rl3, dirn, nx_er, nx_ei, &capped, dens ? D->unified : 0, le.sigma,
+                     !R->shared, &lp, &lr, P > 0 ? &lobe_dls : 0);
+        if (!R->shared) out_w = o_exp(lp - lr);
         break;
       }
       default:
@@ -282,7 +287,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
       float drr = reach_ref != 0.0f ? d_reach[p] / reach_ref : 0.0f;
       float X = rr * att_if * r_live;
       float dX = drr * att_if * r_live + rr * d_att[p] * r_live + rr * att_if * dr_live;
-      nx_dw[p] = (ph->dw[p] * X + ph->w * dX) * out_w;
+      nx_dw[p] = (ph->dw[p] * X + ph->w * dX) * out_w + w_if * out_w * (lobe_dls * dcol[p * LUMEN_N_COL + LUMEN_COL_SIGMA]);
     }
     nx_cls = far_ ? ca : cb;
     nx_ok = ok;
@@ -631,9 +636,11 @@ int32_t lumen_oracle_group_index(const float* e, const float* n, int32_t k, cons
 }
 
 /* n unified facet paths off a flat surface (normal +z) for the incoming direction wi, each from three uniforms of
-   its own key (the lobe's rand); out: the last directions (n * 3), capped: paths that hit a loop bound */
+   its own key (the lobe's rand); out: the last directions (n * 3), capped: paths that hit a loop bound. With the
+   tables U (else null), dens (n * 3) gets each path's log density at sig_live, at sigma, and the former's derivative
+   in sig_live. With one set, each draw is a single facet reflection (its direction may point into the surface). */
 int32_t lumen_oracle_facet_path(float sigma, const float* wi, uint32_t k0, uint32_t k1, int64_t n, float* out,
-                                int64_t* capped) {
+                                int64_t* capped, const float* U, float sig_live, float* dens, int32_t one) {
   const float up[3] = {0.0f, 0.0f, 1.0f};
   OKey key = {k0, k1};
   int64_t nc = 0;
@@ -643,10 +650,44 @@ int32_t lumen_oracle_facet_path(float sigma, const float* wi, uint32_t k0, uint3
     float r[3] = {o_uniform(k, 0), o_uniform(k, 1), o_uniform(k, 2)};
     float er[3] = {0.0f, 1.0f, 0.0f}, ei[3] = {0.0f, 0.0f, 0.0f};
     int c = 0;
-    o_facet_path(sigma, wi, up, r, out + 3 * i, er, ei, &c);
+    float lp = 0.0f, lr = 0.0f, dls = 0.0f;
+    if (one) { /* the path's first facet alone */
+      float mwi[3] = {-wi[0], -wi[1], -wi[2]}, V[3], m[3];
+      o_to_local(mwi, up, V);
+      o_unified_facet(sigma, V, o_fold_in(o_seed_key(r[0], r[1], r[2]), 0), m, &c);
+      float vm = o_dot(V, m);
+      float L[3] = {2.0f * vm * m[0] - V[0], 2.0f * vm * m[1] - V[1], 2.0f * vm * m[2] - V[2]};
+      o_to_world(L, up, out + 3 * i);
+      if (U) {
+        lp = o_unified_logpdf(U, sig_live, wi, up, out + 3 * i, &dls);
+        lr = o_unified_logpdf(U, sigma, wi, up, out + 3 * i, 0);
+      }
+    } else {
+      o_facet_path(sigma, wi, up, r, out + 3 * i, er, ei, &c, U, sig_live, 1, &lp, &lr, &dls);
+    }
+    if (U) { dens[3 * i] = lp; dens[3 * i + 1] = lr; dens[3 * i + 2] = dls; }
     nc += c;
   }
   *capped = nc;
+  return 0;
+}
+
+/* The unified tables and density on n inputs (in, out per fn): 0 log zeta at y = log sigma (y -> lz, dlz/dy);
+   1 F at (x, y) (-> F, dF/dx, dF/dy); 2 one facet reflection's log density at (sigma, w0 (3), normal (3), w1 (3))
+   (-> log p1, d log p1 / d sigma) */
+int32_t lumen_oracle_unified(const float* U, int32_t fn, const float* in, int64_t n, float* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    if (fn == 0) {
+      out[2 * i] = o_table_lz(U, in[i], out + 2 * i + 1);
+    } else if (fn == 1) {
+      out[3 * i] = o_table_front(U, in[2 * i], in[2 * i + 1], out + 3 * i + 1, out + 3 * i + 2);
+    } else if (fn == 2) {
+      const float* a = in + 10 * i;
+      out[2 * i] = o_unified_logpdf(U, a[0], a + 1, a + 4, a + 7, out + 2 * i + 1);
+    } else {
+      return 1;
+    }
+  }
   return 0;
 }
 

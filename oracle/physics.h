@@ -405,7 +405,7 @@ static inline void o_to_local(const float* v, const float* n, float* l) {
   o_basis(n, t1, t2);
   l[0] = o_dot(v, t1); l[1] = o_dot(v, t2); l[2] = o_dot(v, n);
 }
-/* the half-width of the azimuth arc of facets at tilt a that face V (facets.py:299 _front_arc) */
+/* the half-width of the azimuth arc of facets at tilt a that face V (facets.py:311 _front_arc) */
 static inline float o_front_arc(const float* V, float a) {
   float sv = sqrtf(V[0] * V[0] + V[1] * V[1]);
   float sa, ca;
@@ -413,7 +413,7 @@ static inline float o_front_arc(const float* V, float a) {
   float ratio = V[2] * ca / o_max(sv * sa, O_FLOOR32);
   return o_acos(-o_min(ratio, 1.0f));
 }
-/* a unified facet normal (local frame) given V . m > 0 (facets.py:306 unified_facet): the tilt by rejection from a
+/* a unified facet normal (local frame) given V . m > 0 (facets.py:318 unified_facet): the tilt by rejection from a
    Rayleigh(sigma) proposal, the azimuth uniform in the front arc */
 static inline void o_unified_facet(float sigma, const float* V, OKey key, float* m, int* capped) {
   float fmax = o_min(1.0f, 4.0f * sigma);
@@ -439,17 +439,134 @@ static inline void o_unified_facet(float sigma, const float* V, OKey key, float*
   o_sincos(ph, &sp, &cp);
   m[0] = sa * cp; m[1] = sa * sp; m[2] = ca;
 }
-/* a raw threefry key from the three lobe uniforms (facets.py:290 seed_key) */
+/* a raw threefry key from the three lobe uniforms (facets.py:303 seed_key) */
 static inline OKey o_seed_key(float r0, float r1, float r2) {
   uint32_t k0 = (uint32_t)(r0 * 8388608.0f), k1 = (uint32_t)(r1 * 8388608.0f), k2 = (uint32_t)(r2 * 8388608.0f);
   OKey k = {k0 | (k2 << 23), k1 | ((k2 >> 9) << 23)};
   return k;
 }
+/* ---- the unified lobe's tables, read as the reference reads them (facets.py:153-207): a C1 cubic Hermite of
+   log zeta = log(Z / sigma^2) in y = log sigma, a bicubic Hermite of the facing share F in (x, y); each also returns
+   its derivative(s) in the coordinates */
+#define O_UNI_Y0 ((float)LUMEN_UNI_Y0)
+#define O_UNI_DY ((float)LUMEN_UNI_DY)
+#define O_HALF_PI 1.57079632679489661923f
+#define O_LOG_TINY (-69.07755278982137f) /* log FLOOR32: a log density off the support (facets.py:61) */
+#define O_LOG_2PI 1.83787706640934548356f
+
+/* the cell of coordinate v among n nodes: index, offset t and dt / dv (0 where v is clamped) (facets.py:159 _cell) */
+static inline void o_uni_cell(float v, int n, int* i, float* t, float* dt) {
+  float top = (float)(n - 1);
+  float f = v < 0.0f ? 0.0f : (v > top ? top : v);
+  *dt = (v < 0.0f || v > top) ? 0.0f : 1.0f;
+  int k = (int)floorf(f);
+  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+  *i = k;
+  *t = f - (float)k;
+}
+/* the cubic Hermite basis (a0, b0, a1, b1) at t and its derivative in t (facets.py:153 _hermite) */
+static inline void o_hermite(float t, float* h, float* dh) {
+  float t2 = t * t, t3 = t2 * t;
+  h[0] = 2.0f * t3 - 3.0f * t2 + 1.0f;
+  h[1] = t3 - 2.0f * t2 + t;
+  h[2] = -2.0f * t3 + 3.0f * t2;
+  h[3] = t3 - t2;
+  dh[0] = 6.0f * t2 - 6.0f * t;
+  dh[1] = 3.0f * t2 - 4.0f * t + 1.0f;
+  dh[2] = -6.0f * t2 + 6.0f * t;
+  dh[3] = 3.0f * t2 - 2.0f * t;
+}
+/* log zeta at y = log sigma and d / dy (facets.py:170 table_lz) */
+static inline float o_table_lz(const float* U, float y, float* dy) {
+  const float* v = U + 4 * LUMEN_UNI_NX * LUMEN_UNI_NY;
+  const float* dv = v + LUMEN_UNI_NY;
+  int j;
+  float t, dt, h[4], dh[4];
+  o_uni_cell((y - O_UNI_Y0) / O_UNI_DY - (float)LUMEN_UNI_J_LO, LUMEN_UNI_NY, &j, &t, &dt);
+  o_hermite(t, h, dh);
+  float out = h[0] * v[j] + h[2] * v[j + 1] + O_UNI_DY * (h[1] * dv[j] + h[3] * dv[j + 1]);
+  float dout = dh[0] * v[j] + dh[2] * v[j + 1] + O_UNI_DY * (dh[1] * dv[j] + dh[3] * dv[j + 1]);
+  *dy = dout * dt / O_UNI_DY;
+  return out;
+}
+/* F at (x, y = log sigma) and its derivatives in x and y (facets.py:180 table_front) */
+static inline float o_table_front(const float* U, float x, float y, float* dFx, float* dFy) {
+  const int NY = LUMEN_UNI_NY, NN = LUMEN_UNI_NX * LUMEN_UNI_NY;
+  const float* A[4] = {U, U + NN, U + 2 * NN, U + 3 * NN}; /* F, Fx, Fy, Fxy */
+  int i, j;
+  float tx, ty, dtx, dty, hx4[4], dhx4[4], hy4[4], dhy4[4];
+  o_uni_cell(x * (float)(LUMEN_UNI_NX - 1), LUMEN_UNI_NX, &i, &tx, &dtx);
+  o_uni_cell((y - O_UNI_Y0) / O_UNI_DY - (float)LUMEN_UNI_J_LO, NY, &j, &ty, &dty);
+  const float hx = 1.0f / (float)(LUMEN_UNI_NX - 1);
+  o_hermite(tx, hx4, dhx4);
+  o_hermite(ty, hy4, dhy4);
+  float out = 0.0f, ox = 0.0f, oy = 0.0f;
+  for (int di = 0; di < 2; ++di)
+    for (int dj = 0; dj < 2; ++dj) {
+      int k = (i + di) * NY + (j + dj);
+      float ax = hx4[2 * di], bx = hx4[2 * di + 1], ay = hy4[2 * dj], by = hy4[2 * dj + 1];
+      float dax = dhx4[2 * di], dbx = dhx4[2 * di + 1], day = dhy4[2 * dj], dby = dhy4[2 * dj + 1];
+      out = out + (ax * ay * A[0][k] + bx * ay * hx * A[1][k] + ax * by * O_UNI_DY * A[2][k] +
+                   bx * by * hx * O_UNI_DY * A[3][k]);
+      ox = ox + (dax * ay * A[0][k] + dbx * ay * hx * A[1][k] + dax * by * O_UNI_DY * A[2][k] +
+                 dbx * by * hx * O_UNI_DY * A[3][k]);
+      oy = oy + (ax * day * A[0][k] + bx * day * hx * A[1][k] + ax * dby * O_UNI_DY * A[2][k] +
+                 bx * dby * hx * O_UNI_DY * A[3][k]);
+    }
+  *dFx = ox * dtx * (float)(LUMEN_UNI_NX - 1);
+  *dFy = oy * dty / O_UNI_DY;
+  return out;
+}
+/* log p1(w1 | w0) of one unified facet reflection at width sigma, D(h) / (4 F V . h) with h the half vector, and
+   (dls, when given) its derivative in sigma; O_LOG_TINY off the support (facets.py:209 _unified_log_density, :248
+   _half_vector, :259 unified_facet_logpdf) */
+static inline float o_unified_logpdf(const float* U, float sigma, const float* w0, const float* n, const float* w1,
+                                     float* dls) {
+  float mw[3] = {-w0[0], -w0[1], -w0[2]};
+  float V[3], W[3];
+  o_to_local(mw, n, V);
+  o_to_local(w1, n, W);
+  float H[3] = {V[0] + W[0], V[1] + W[1], V[2] + W[2]};
+  float vH = o_dot(V, H);
+  if (!(H[2] > 0.0f && vH > 0.0f)) {
+    if (dls) *dls = 0.0f;
+    return O_LOG_TINY;
+  }
+  float inv = 1.0f / sqrtf(o_dot(H, H));
+  float vh = vH * inv;
+  float ch = H[2] * inv;
+  float s = sqrtf(H[0] * H[0] + H[1] * H[1]) * inv; /* sin(alpha), from the tangential part */
+  float alpha = o_atan2(s, ch);
+  float l4 = o_log(4.0f * sigma);
+  float lf = o_min(0.0f, l4); /* log f_max */
+  float ef = o_exp(lf);
+  float ls = o_log(s > ef ? s : ef);
+  float cos_t = V[2], sin_t = sqrtf(V[0] * V[0] + V[1] * V[1]);
+  float y = o_log(sigma);
+  float dlz, dFx, dFy;
+  float lz = o_table_lz(U, y, &dlz);
+  float x = o_atan2(cos_t, sigma * sin_t) / O_HALF_PI;
+  float F = o_table_front(U, x, y, &dFx, &dFy);
+  float lp = -alpha * alpha / (2.0f * sigma * sigma) + (lf - ls) - O_LOG_2PI - 2.0f * y - lz - o_log(F);
+  lp = lp - o_log(4.0f * vh);
+  if (dls) {
+    float is = 1.0f / sigma;
+    float dlf = l4 < 0.0f ? is : (l4 == 0.0f ? 0.5f * is : 0.0f); /* a tie splits the derivative */
+    float dsel = s > ef ? dlf : 0.0f;
+    float sb = sigma * sin_t;
+    float dx = -(cos_t * sin_t) / (cos_t * cos_t + sb * sb) / O_HALF_PI;
+    *dls = alpha * alpha / (sigma * sigma * sigma) + dsel - 2.0f * is - dlz * is - (dFx * dx + dFy * is) / F;
+  }
+  return lp;
+}
+
 /* the facet path: a facet for the current direction and the mirror about it, until the direction leaves the surface
-   (facets.py:323 _path_of, surface_event.py:104 _facet_path_branch: the Jones vector mirrored about each facet's half
-   vector) */
+   (facets.py:372 _path_of, surface_event.py:106 _facet_path_branch: the Jones vector mirrored about each facet's half
+   vector). With the tables U, each facet's log density is summed: at the live width into lp (its derivative in
+   sigma into dls, when given) and, where weigh is set, at the drawn (reference) width into lr. */
 static inline void o_facet_path(float sigma, const float* wi, const float* n, const float* rand, float* wo, float* er,
-                                float* ei, int* capped) {
+                                float* ei, int* capped, const float* U, float sig_live, int weigh, float* lp,
+                                float* lr, float* dls) {
   OKey key = o_seed_key(rand[0], rand[1], rand[2]);
   float mwi[3] = {-wi[0], -wi[1], -wi[2]};
   float V[3];
@@ -461,6 +578,12 @@ static inline void o_facet_path(float sigma, const float* wi, const float* n, co
     float vm = o_dot(V, m);
     float L[3] = {2.0f * vm * m[0] - V[0], 2.0f * vm * m[1] - V[1], 2.0f * vm * m[2] - V[2]};
     o_to_world(L, n, wo);
+    if (U) {
+      float d = 0.0f;
+      *lp = *lp + o_unified_logpdf(U, sig_live, w, n, wo, dls ? &d : 0);
+      if (dls) *dls = *dls + d;
+      if (weigh) *lr = *lr + o_unified_logpdf(U, sigma, w, n, wo, 0);
+    }
     float h[3] = {wo[0] - w[0], wo[1] - w[1], wo[2] - w[2]};
     o_unit(h);
     o_mirror(er, ei, h);

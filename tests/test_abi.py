@@ -26,7 +26,7 @@ def test_library_exports_every_declared_entry_point(built):
 
 def test_abi_version_and_argument_errors(built):
     lib = A.engine()
-    assert lib.lumen_b200_abi_version() == 1
+    assert lib.lumen_b200_abi_version() == 2
     h = ctypes.c_void_p()
     assert lib.lumen_b200_scene_create(None, ctypes.byref(h)) == 1  # LUMEN_ERR_ARG before any device call
     assert b"null" in lib.lumen_b200_last_error()
@@ -35,3 +35,26 @@ def test_abi_version_and_argument_errors(built):
     d.n_sensor = 1  # sensor indices past it: refused on the host
     assert lib.lumen_b200_scene_create(ctypes.byref(d), ctypes.byref(h)) == 1
     assert lib.lumen_b200_trace(None, None, None, 0, 0, 0, 1, None, None, None) == 1
+    # a unified facet row needs the lobe's tables: refused on the host when they are missing
+    fdet = detectors.cylinder_tank(n_pmt=20, wall_finish="ground", sigma_alpha=0.1)
+    d, keep = fdet.desc()
+    assert keep["unified"].size == A.UNI_WORDS
+    d.unified = A.fptr(None)
+    assert lib.lumen_b200_scene_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    assert b"unified tables" in lib.lumen_b200_last_error()
+
+
+def test_header_constants_match_the_python_mirrors():
+    from lumen_b200 import facets
+
+    h = open(HEADER).read()
+
+    def define(name):
+        return float(re.search(rf"#define {name}\s+\(?(-?[0-9.]+)\)?", h).group(1))
+
+    assert int(define("LUMEN_UNI_NX")) == A.UNI_NX == facets.NX
+    assert int(define("LUMEN_UNI_NY")) == A.UNI_NY == facets.NY
+    assert int(define("LUMEN_UNI_J_LO")) == facets.J_LO
+    assert abs(define("LUMEN_UNI_Y0") - facets.Y0) < 1e-15 and abs(define("LUMEN_UNI_DY") - facets.DY) < 1e-15
+    assert int(define("LUMEN_MAX_GRAD")) == A.MAX_GRAD
+    assert facets.WORDS == A.UNI_WORDS
