@@ -155,8 +155,11 @@ typedef struct LumenSource {
 /* ------------------------------------------------------------------------------------------ the controls */
 enum { LUMEN_F_ASYNC = 1 };  /* controls.flags: enqueue only (no host wait, no status read back: capturable in a
                                  CUDA graph); a step budget that ran out then shows in counts[LUMEN_C_ABORTED] */
-enum { LUMEN_N_VARIANT = 3 };  /* launch variants: 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
-                                  2 = 256 x 3 (85 registers) */
+enum { LUMEN_VARIANT_WAVEFRONT = 3, LUMEN_N_VARIANT = 4 };
+/* launch variants: the persistent photon loop at 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
+   2 = 256 x 3 (85 registers); 3 = the wavefront: rounds of two kernels (the query; the rest of the step and the
+   refill) over a pool of slots in HBM, launched from a host loop that reads a live-slot count back every four rounds
+   (not with LUMEN_F_ASYNC). Every variant gives the same photons the same paths. */
 typedef struct LumenControls {
   float max_distance;      /* m: a query's reach (<= 0: the scene's reach) */
   float roulette;          /* epsilon > 0 (src/lumen/rules/choices.py:112) */

@@ -25,7 +25,8 @@ N_COL = 10
 N_HEALTH = 11
 N_COUNT = 6
 F_ASYNC = 1
-N_VARIANT = 3
+N_VARIANT = 4
+VARIANT_WAVEFRONT = 3
 UNI_NX, UNI_NY = 257, 69
 UNI_WORDS = 4 * UNI_NX * UNI_NY + 2 * UNI_NY
 HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "absorbed_surface", "rouletted",

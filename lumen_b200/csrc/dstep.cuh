@@ -42,28 +42,55 @@ struct Dep {
 
 L_DEV float d_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0.0f; }
 
-template <int G>
-L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq) {
+// What a step computes before its query and uses after it: the vertex key, the band at the step's start (before a
+// stuck push), the free path drawn at the reference, the medium at the live and reference values. The polarisation
+// state after the fill is written back into the photon.
+struct Pre {
+  Key vkey;
+  float b0, s;
+  Med ml, mr;
+};
+
+// the step up to its query: the stuck push, the vertex key, the polarisation fill, the media, the free path
+// (step.py:318 _step_context, :245 _recover)
+L_DEV void d_pre(const Run& R, Photon& ph, Key pkey, Pre& pr) {
   const DScene& S = R.S;
-  const int P = G > 0 ? R.P : 0;
-  float b0 = d_band(d_maxabs3(ph.x));
+  pr.b0 = d_band(d_maxabs3(ph.x));
   int stuck = ph.alive && ph.nz >= D_ZSBP;
   if (stuck) {
-    float pb = D_PUSH_BANDS * b0;
+    float pb = D_PUSH_BANDS * pr.b0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) ph.x[a] = ph.x[a] + pb * ph.d[a];
     ph.vol = d_locate(S, ph.x);
     ph.cls = d_cls(S, ph.vol);
     ph.srf = -1;
   }
-  Key vkey = fold_in(pkey, (uint32_t)ph.vertex);
-  float er0[3] = {ph.er[0], ph.er[1], ph.er[2]}, ei0[3] = {ph.ei[0], ph.ei[1], ph.ei[2]};
-  if (d_dot(er0, er0) + d_dot(ei0, ei0) < D_ZERO_STATE) d_fill(ph.d, er0, ei0, uniform(fold_in(vkey, D_POL_STREAM), 0));
+  pr.vkey = fold_in(pkey, (uint32_t)ph.vertex);
+  if (d_dot(ph.er, ph.er) + d_dot(ph.ei, ph.ei) < D_ZERO_STATE)
+    d_fill(ph.d, ph.er, ph.ei, uniform(fold_in(pr.vkey, D_POL_STREAM), 0));
   int mi = __ldg(S.cls_medium + ph.cls);
-  Med ml = d_medium_at(S, R.live, ph.lam, mi);
-  Med mr = R.shared ? ml : d_medium_at(S, R.ref, ph.lam, mi);
+  pr.ml = d_medium_at(S, R.live, ph.lam, mi);
+  pr.mr = R.shared ? pr.ml : d_medium_at(S, R.ref, ph.lam, mi);
+  pr.s = -l_log(uniform(pr.vkey, 0)) / d_max(pr.mr.mu_c, D_FLOOR32);
+}
+
+L_DEV Query d_step_query(const Run& R, const Photon& ph, const Pre& pr) {
+  return d_query(R.S, ph.x, ph.d, ph.vol, R.max_distance, ph.srf, ph.sn, pr.s);
+}
+
+// the step after its query (step.py:516 step: the crossing, the event, the deposit, the roulette)
+template <int G>
+L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Query& q, Dep& dep, float* dq) {
+  const DScene& S = R.S;
+  const int P = G > 0 ? R.P : 0;
+  const float b0 = pr.b0, s = pr.s;
+  const Key vkey = pr.vkey;
+  const Med& ml = pr.ml;
+  const Med& mr = pr.mr;
+  float er0[3] = {ph.er[0], ph.er[1], ph.er[2]}, ei0[3] = {ph.ei[0], ph.ei[1], ph.ei[2]};
   float dmu_abs[G > 0 ? G : 1], dmu_c[G > 0 ? G : 1];
   if (G > 0) {
+    int mi = __ldg(S.cls_medium + ph.cls);
     const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
     int ta = __ldg(m + LUMEN_MI_ABS), tr = __ldg(m + LUMEN_MI_RAY);
     float E = D_HC / ph.lam;
@@ -75,8 +102,6 @@ L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float
     }
   }
   float mu_r = mr.mu_c;
-  float s = -l_log(uniform(vkey, 0)) / d_max(mu_r, D_FLOOR32);
-  Query q = d_query(S, ph.x, ph.d, ph.vol, R.max_distance, ph.srf, ph.sn, s);
   int sensor_q = q.hit ? vI(S, q.vol_after, LUMEN_VI_SENSOR) : -1;
   float dist = q.t;
   int zero = dist <= D_ZERO_STEP_BANDS * b0;
@@ -325,6 +350,15 @@ L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float
   }
   ph.nz = nz_new;
   ph.cls = nx_cls;
+}
+
+// one whole step: the megakernel's (k_trace)
+template <int G>
+L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq) {
+  Pre pr;
+  d_pre(R, ph, pkey, pr);
+  Query q = d_step_query(R, ph, pr);
+  d_post<G>(R, ph, dw, pr, q, dep, dq);
 }
 
 // ------------------------------------------------------------------------------------------------ sources

@@ -92,11 +92,37 @@ __device__ __forceinline__ void flush_all(const Tally& T, int e, PhotonTally& pt
     if (j < pt.n) flush2(T, e, pt.sensor[j], pt.sum[j]);
 }
 
+// adds one deposit to the tallies; returns 1 where the photon's sensor-sum cache was full (its oldest sum flushed)
+// adds every lane's non-zero health fates (times its row weight) to the block's shared sums: a warp sum first, then
+// one shared atomic per fate and warp (lanes with nothing to add pass zeros; every lane of the warp must call it)
+__device__ __forceinline__ void health_add(double* sh, const Dep& dep, double w0, int on) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    float f = on ? (k < 8 ? dep.fates[k] : dep.pushed) : 0.0f;
+    if (!__any_sync(FULL, f != 0.0f)) continue;
+    double v = f != 0.0f ? (double)f * w0 : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    if (lane == 0) atomicAdd(sh + (k < 8 ? k : LUMEN_H_PUSHED), v);
+  }
+}
+
+// adds v (per lane, 0 for none) to a shared sum: one warp sum and one atomic per warp (every lane must call it)
+__device__ __forceinline__ void warp_add(double* sh, double v) {
+  const unsigned FULL = 0xffffffffu;
+  if (!__any_sync(FULL, v != 0.0)) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(sh, v);
+}
+
 template <int G>
-__device__ __forceinline__ void deposit(const Tally& T, int e, const Dep& dep, const float* dq, double w0,
-                                        PhotonTally& pt) {
+__device__ __forceinline__ int deposit(const Tally& T, int e, const Dep& dep, const float* dq, double w0,
+                                       PhotonTally& pt) {
   int s = dep.sensor;
-  if ((unsigned)e >= (unsigned)T.E || (unsigned)s >= (unsigned)T.S_) return;  // an event or sensor out of range
+  if ((unsigned)e >= (unsigned)T.E || (unsigned)s >= (unsigned)T.S_) return 0;  // an event or sensor out of range
   double v = (double)dep.q * w0;
   size_t ix = (size_t)e * T.S_ + s;
   if (T.arrival) {
@@ -116,7 +142,7 @@ __device__ __forceinline__ void deposit(const Tally& T, int e, const Dep& dep, c
         for (int p = 0; p < T.P; ++p) atomicAdd(T.grads + p, c * (double)dq[p] * w0);
     }
   }
-  int found = 0;
+  int found = 0, evicted = 0;
 #pragma unroll
   for (int j = 0; j < CACHE; ++j)
     if (j < pt.n && pt.sensor[j] == s) { pt.sum[j] += v; found = 1; }
@@ -126,12 +152,14 @@ __device__ __forceinline__ void deposit(const Tally& T, int e, const Dep& dep, c
 #pragma unroll
       for (int k = 1; k < CACHE; ++k) { pt.sensor[k - 1] = pt.sensor[k]; pt.sum[k - 1] = pt.sum[k]; }
       pt.n = CACHE - 1;
+      evicted = 1;
     }
 #pragma unroll
     for (int j = 0; j < CACHE; ++j)
       if (j == pt.n) { pt.sensor[j] = s; pt.sum[j] = v; }
     pt.n += 1;
   }
+  return evicted;
 }
 
 __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
@@ -190,25 +218,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
       }
     }
     if (__ballot_sync(FULL, active) == 0) break;
+    Dep dep;
+    int stepped = active;
+    double start_w = 0.0, trunc_w = 0.0;
+    if (active) d_step<G>(L.R, ph, dw, pkey, dep, dq);
+    health_add(sh_health, dep, w0, stepped);
     if (active) {
-      Dep dep;
-      d_step<G>(L.R, ph, dw, pkey, dep, dq);
       c_steps++;
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if (dep.fates[k] != 0.0f) atomicAdd(sh_health + k, (double)dep.fates[k] * w0);
-      if (dep.pushed != 0.0f) atomicAdd(sh_health + LUMEN_H_PUSHED, (double)dep.pushed * w0);
       if (dep.sensor >= 0) {
-        deposit<G>(L.T, ev, dep, dq, w0, pt);
+        c_multi += deposit<G>(L.T, ev, dep, dq, w0, pt);
         c_dep++;
       }
       if (!ph.alive || ph.vertex >= L.R.max_vertices) {
         flush_all(L.T, ev, pt);
         if (ph.alive) {
-          atomicAdd(sh_health + LUMEN_H_TRUNCATED, (double)ph.w * w0);
+          trunc_w = (double)ph.w * w0;
           c_trunc++;
         }
-        atomicAdd(sh_health + LUMEN_H_START, w0);
+        start_w = w0;
         c_ph++;
         active = 0;
       }
@@ -219,6 +246,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
       }
       if (L.abort_flag && *(volatile int*)L.abort_flag) active = 0;
     }
+    warp_add(sh_health + LUMEN_H_START, start_w);
+    warp_add(sh_health + LUMEN_H_TRUNCATED, trunc_w);
   }
   // the block's health and counters: one atomic per block and value
   __shared__ unsigned long long sc[LUMEN_N_COUNT][BLOCK / 32];
@@ -240,6 +269,168 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
     unsigned long long v = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sc[k][w];
     if (v) atomicAdd(L.T.counts + k, v);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ the wavefront
+// The photon loop as rounds over a pool of W slots held in HBM (launch variant LUMEN_VARIANT_WAVEFRONT): per round,
+// k_wave_query runs every live slot's step up to and including its navigator query, and k_wave_step the rest of the
+// step, the deposit, the photon's end and the slot's refill from the source. Each kernel is a part of the
+// megakernel's code with its own registers; the state crosses HBM between them, word-major (word k of slot i at
+// buf[k * W + i]) so that every load and store of a warp is one contiguous 128-byte access.
+struct WaveExtra {  // what a slot carries besides the photon: its key, event, row weight and sensor-sum cache
+  Key pkey;
+  int ev, pad;
+  double w0;
+  PhotonTally pt;
+};
+
+struct Wave {
+  uint32_t* ph;     // W x sizeof(Photon) / 4
+  uint32_t* ex;     // W x sizeof(WaveExtra) / 4
+  uint32_t* pre;    // W x sizeof(Pre) / 4
+  uint32_t* q;      // W x sizeof(Query) / 4
+  float* dw;        // W x LUMEN_MAX_GRAD (gradient runs)
+  int32_t* act;     // W: the slot holds a live photon
+  unsigned long long* live;  // slots live after the last k_wave_step (zeroed before each)
+  int W;
+};
+
+template <class T>
+__device__ __forceinline__ void wv_ld(const uint32_t* b, int W, int i, T& v) {
+  static_assert(sizeof(T) % 4 == 0, "word-major records hold whole words");
+  uint32_t* w = reinterpret_cast<uint32_t*>(&v);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(T) / 4); ++k) w[k] = b[(size_t)k * W + i];
+}
+template <class T>
+__device__ __forceinline__ void wv_st(uint32_t* b, int W, int i, const T& v) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(&v);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(T) / 4); ++k) b[(size_t)k * W + i] = w[k];
+}
+
+template <int G>
+__global__ void __launch_bounds__(256, 2) k_wave_query(Launch L, Wave V) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.W || !V.act[i]) return;
+  if (L.abort_flag && *(volatile int*)L.abort_flag) return;
+  Photon ph;
+  WaveExtra ex;
+  wv_ld(V.ph, V.W, i, ph);
+  wv_ld(V.ex, V.W, i, ex);
+  Pre pr;
+  d_pre(L.R, ph, ex.pkey, pr);
+  Query q = d_step_query(L.R, ph, pr);
+  wv_st(V.ph, V.W, i, ph);
+  wv_st(V.pre, V.W, i, pr);
+  wv_st(V.q, V.W, i, q);
+}
+
+template <int G>
+__global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  __shared__ double sh_health[LUMEN_N_HEALTH];
+  __shared__ unsigned long long sc[LUMEN_N_COUNT + 1][8];
+  if (threadIdx.x < LUMEN_N_HEALTH) sh_health[threadIdx.x] = 0.0;
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int in = i < V.W;
+  int aborted = L.abort_flag && *(volatile int*)L.abort_flag;
+  int act = in && !aborted && V.act[i];
+  unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0;
+  Photon ph;
+  WaveExtra ex;
+  float dw[G > 0 ? G : 1], dq[G > 0 ? G : 1];
+  Dep dep;
+  const int stepped = act;
+  double start_w = 0.0, trunc_w = 0.0;
+  if (act) {
+    wv_ld(V.ph, V.W, i, ph);
+    wv_ld(V.ex, V.W, i, ex);
+    Pre pr;
+    Query q;
+    wv_ld(V.pre, V.W, i, pr);
+    wv_ld(V.q, V.W, i, q);
+    if (G > 0)
+      for (int p = 0; p < L.R.P; ++p) dw[p] = V.dw[(size_t)p * V.W + i];
+    d_post<G>(L.R, ph, dw, pr, q, dep, dq);
+    c_steps++;
+    if (dep.sensor >= 0) {
+      c_multi += deposit<G>(L.T, ex.ev, dep, dq, ex.w0, ex.pt);
+      c_dep++;
+    }
+    if (!ph.alive || ph.vertex >= L.R.max_vertices) {
+      flush_all(L.T, ex.ev, ex.pt);
+      if (ph.alive) {
+        trunc_w = (double)ph.w * ex.w0;
+        c_trunc++;
+      }
+      start_w = ex.w0;
+      c_ph++;
+      act = 0;
+    }
+  }
+  health_add(sh_health, dep, stepped ? ex.w0 : 0.0, stepped);
+  warp_add(sh_health + LUMEN_H_START, start_w);
+  warp_add(sh_health + LUMEN_H_TRUNCATED, trunc_w);
+  // the refill: free slots take consecutive photon ids, one atomic per warp
+  int need = in && !act && !aborted;
+  unsigned m = __ballot_sync(FULL, need);
+  if (m) {
+    int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(L.next, (unsigned long long)__popc(m));
+    base = __shfl_sync(FULL, base, leader);
+    if (need) {
+      unsigned long long g = base + __popc(m & ((1u << lane) - 1u));
+      if (g < (unsigned long long)L.n) {
+        Row r;
+        get_row(L, (int64_t)g, r);
+        d_start(L.R.S, r, ph);
+        ex.pkey = fold_in(L.key, (uint32_t)(L.first_id + (int64_t)g));
+        ex.w0 = (double)r.w0;
+        ex.ev = r.event;
+        ex.pad = 0;
+        ex.pt.n = 0;
+        if (G > 0)
+          for (int p = 0; p < L.R.P; ++p) dw[p] = 0.0f;
+        act = 1;
+      }
+    }
+  }
+  if (in) {
+    if (act) {
+      wv_st(V.ph, V.W, i, ph);
+      wv_st(V.ex, V.W, i, ex);
+      if (G > 0)
+        for (int p = 0; p < L.R.P; ++p) V.dw[(size_t)p * V.W + i] = dw[p];
+    }
+    V.act[i] = act;
+  }
+  // the block's health, counters and live slots: one atomic per block and value
+  const int warp = threadIdx.x >> 5;
+  unsigned long long cv[LUMEN_N_COUNT + 1] = {c_ph, c_steps, c_dep, c_trunc, c_multi, 0ull, (unsigned long long)act};
+#pragma unroll
+  for (int k = 0; k < LUMEN_N_COUNT + 1; ++k) {
+    unsigned long long v = cv[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+    if (lane == 0) sc[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < LUMEN_N_HEALTH) {
+    double v = sh_health[threadIdx.x];
+    if (v != 0.0) atomicAdd(L.T.health + threadIdx.x, v);
+  } else if (threadIdx.x >= 32 && threadIdx.x < 32 + LUMEN_N_COUNT + 1) {
+    int k = threadIdx.x - 32;
+    unsigned long long v = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sc[k][w];
+    if (v) atomicAdd(k < LUMEN_N_COUNT ? L.T.counts + k : V.live, v);
+    if (k == LUMEN_C_STEPS && v && L.step_budget > 0) {  // the call's step budget, counted per block
+      unsigned long long used = atomicAdd(L.steps_used, v) + v;
+      if (used > (unsigned long long)L.step_budget) atomicExch(L.abort_flag, 1);
+    }
   }
 }
 
@@ -467,15 +658,60 @@ static int launch_trace(const Launch& L, int variant, int bps, cudaStream_t stre
   }
 }
 
+// The wavefront's rounds (LUMEN_VARIANT_WAVEFRONT): a fill, then query and step kernels until no slot is live. The
+// pool holds up to LUMEN_WAVE_POOL slots (about 350 bytes each with gradients), allocated on the call's stream.
+#define LUMEN_WAVE_POOL (1 << 21)
+template <int G>
+static int run_wave(const Launch& L, unsigned long long* live, cudaStream_t stream) {
+  int64_t want = L.n < LUMEN_WAVE_POOL ? L.n : LUMEN_WAVE_POOL;
+  int W = (int)((want + 255) / 256 * 256);
+  const size_t nph = sizeof(Photon) / 4, nex = sizeof(WaveExtra) / 4, npre = sizeof(Pre) / 4, nq = sizeof(Query) / 4;
+  const size_t ng = G > 0 ? LUMEN_MAX_GRAD : 0;
+  size_t words = (size_t)W * (nph + nex + npre + nq + ng + 1);
+  uint32_t* buf = nullptr;
+  CK(cudaMallocAsync((void**)&buf, words * 4, stream));
+  Wave V;
+  V.W = W;
+  V.ph = buf;
+  V.ex = V.ph + (size_t)W * nph;
+  V.pre = V.ex + (size_t)W * nex;
+  V.q = V.pre + (size_t)W * npre;
+  V.dw = (float*)(V.q + (size_t)W * nq);
+  V.act = (int32_t*)(V.dw + (size_t)W * ng);
+  V.live = live;
+  const int grid = W / 256;
+  CK(cudaMemsetAsync(V.act, 0, (size_t)W * 4, stream));
+  k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);  // the fill: every slot takes a photon
+  CK(cudaGetLastError());
+  int st = 0;
+  for (long long r = 0;; ++r) {
+    k_wave_query<G><<<grid, 256, 0, stream>>>(L, V);
+    CK(cudaMemsetAsync(V.live, 0, sizeof(unsigned long long), stream));
+    k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
+    CK(cudaGetLastError());
+    if ((r & 3) == 3) {
+      unsigned long long h = 0;
+      CK(cudaMemcpyAsync(&h, V.live, sizeof(h), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      if (h == 0) break;
+    }
+  }
+  CK(cudaFreeAsync(buf, stream));
+  return st;
+}
+
 static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
                      cudaStream_t stream, int variant = 0, int bps = 0, int async = 0) {
+  if (variant == LUMEN_VARIANT_WAVEFRONT && async)
+    return set_err(LUMEN_ERR_ARG, "the wavefront variant reads its rounds back on the host: not with LUMEN_F_ASYNC");
   Tally& T = L.T;
   T.E = out ? (out->n_events > 0 ? out->n_events : 1) : (n_events_cot > 0 ? n_events_cot : 1);
   T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
   T.P = L.R.P;
   T.cot = cot;
   T.grads = grads;
-  // scratch: the photon counter, the abort flag and the steps used (one small allocation per call)
+  // scratch: the photon counter, the abort flag, the steps used and the wavefront's live slots (one small allocation
+  // per call)
   unsigned long long* scratch = nullptr;
   CK(cudaMallocAsync((void**)&scratch, 4 * sizeof(unsigned long long), stream));
   CK(cudaMemsetAsync(scratch, 0, 4 * sizeof(unsigned long long), stream));
@@ -509,9 +745,13 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
         L2.T.health = dummy;
         L2.T.counts = (unsigned long long*)(dummy + LUMEN_N_HEALTH);
       }
-      if ((st = launch_trace<LUMEN_MAX_GRAD>(L2, variant, bps, stream))) return st;
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<LUMEN_MAX_GRAD>(L2, scratch + 3, stream)
+                                              : launch_trace<LUMEN_MAX_GRAD>(L2, variant, bps, stream);
+      if (st) return st;
     } else {
-      if ((st = launch_trace<0>(L, variant, bps, stream))) return st;
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, scratch + 3, stream)
+                                              : launch_trace<0>(L, variant, bps, stream);
+      if (st) return st;
     }
   }
   if (async) {  // enqueue only: the abort flag reaches counts[LUMEN_C_ABORTED] on the device

@@ -104,7 +104,7 @@ def test_toy_tank_tallies_match(toy, built):
     np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
     np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
     np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-7, atol=1e-6)
-    assert (T.counts.cpu().numpy()[:4] == O.counts.astype(np.int64)[:4]).all()
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
 
 
 def test_tank_tallies_and_gradients_match(tank, built):
@@ -115,7 +115,7 @@ def test_tank_tallies_and_gradients_match(tank, built):
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
-    assert (T.counts.cpu().numpy()[:4] == O.counts.astype(np.int64)[:4]).all()
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
 
 
 def test_reference_run_matches(tank, built):
@@ -199,7 +199,7 @@ def test_facet_tank_sigma_gradients_match(facet_tank, built):
     T, O = _tallies(facet_tank, src, 1 << 15, controls=c, n_bins=200)
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
-    assert (T.counts.cpu().numpy()[:4] == O.counts.astype(np.int64)[:4]).all()
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
 
 
 def test_facet_reference_run_matches(facet_tank, built):
@@ -209,3 +209,37 @@ def test_facet_reference_run_matches(facet_tank, built):
     T, O = _tallies(facet_tank, src, 1 << 14, pools=(live, facet_tank.pool))
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("which", ["tank", "facet_lar"])
+def test_wavefront_tallies_match(which, tank, facet_lar, built):
+    """The wavefront launch (rounds of a query kernel and a step kernel over slots in HBM): the same tallies."""
+    if which == "tank":
+        det = tank
+        src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+        names, n = ["media/Water/absorption", "surfaces/BlackSheet/R"], 1 << 15
+    else:
+        det = facet_lar
+        src = sources.Scintillation(position=[(0.3, 0.2, -0.4), (-1.0, 1.0, 0.5)], lam=128.0, tau=(6.0, 1500.0),
+                                    fraction=0.25)  # fmt: skip
+        names, n = ["surfaces/CageSurface/R", "media/LAr/rayleigh"], 1 << 12
+    for grads in ((), names):
+        c = A.controls(grad_tabs=[det.params_index[k] for k in grads], variant=A.VARIANT_WAVEFRONT)
+        T, O = _tallies(det, src, n, controls=c, n_bins=50)
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
+        np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-7, atol=1e-6)
+        if grads:
+            np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+        assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+
+
+def test_wavefront_refuses_asynchronous_calls(tank, built):
+    eng = _engine(tank)
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam=400.0)
+    ds = DeviceSource(src, 1024)
+    T = DeviceTallies(tank.n_sensor, 1, 0, 0.0, 1.0, 0)
+    c = A.controls(variant=A.VARIANT_WAVEFRONT, flags=A.F_ASYNC)
+    with pytest.raises(Exception, match="LUMEN_F_ASYNC"):
+        eng.trace(KEY, 1024, source=ds, controls=c, tallies=T)

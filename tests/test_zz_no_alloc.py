@@ -43,6 +43,6 @@ def test_static_trace_matches_trace_on_two_calls():
             np.testing.assert_allclose(getattr(T, name).cpu().numpy(), getattr(ref, name).cpu().numpy(), rtol=1e-9,
                                        atol=1e-15, err_msg=name)  # fmt: skip
         np.testing.assert_allclose(T.health.cpu().numpy(), ref.health.cpu().numpy(), rtol=1e-7, atol=1e-9)
-        assert (T.counts.cpu().numpy()[:4] == ref.counts.cpu().numpy()[:4]).all()
+        assert (T.counts.cpu().numpy()[:5] == ref.counts.cpu().numpy()[:5]).all()
         assert T.counts.cpu().numpy()[0] == n
     eng.close()
