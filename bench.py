@@ -173,7 +173,7 @@ def run_batched(dev, det, reps=3):
     ds = DeviceSource(src, n, dev)
     names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R"]
     gt = [det.params_index[k] for k in names]
-    (variant, bps), times = autotune.tune(eng, ds, 1 << 20, gt, ds.n_events, A.key_of_seed(0))
+    (variant, bps), times = autotune.tune(eng, ds, 1 << 20, gt, ds.n_events, A.key_of_seed(0), asynchronous=True)
     c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps, flags=A.F_ASYNC)
     T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
@@ -214,7 +214,7 @@ def run_tank_adjoint(dev, src, n, reps=2):
     import torch
 
     from lumen_b200 import _abi as A
-    from lumen_b200 import detectors
+    from lumen_b200 import autotune, detectors
     from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
 
     det = detectors.cylinder_tank(wall_finish="ground", sigma_alpha=0.1)
@@ -223,7 +223,8 @@ def run_tank_adjoint(dev, src, n, reps=2):
     names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R",
              "surfaces/BlackSheet/sigma_alpha"]  # fmt: skip
     gt = [det.params_index[k] for k in names]
-    c = A.controls(grad_tabs=gt)
+    (variant, bps), times = autotune.tune(eng, ds, 1 << 21, gt, ds.n_events, A.key_of_seed(0))
+    c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps)
     T = DeviceTallies(det.n_sensor, ds.n_events, 200, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
     eng.trace(key, min(n, 1 << 20), source=ds, controls=c, tallies=T)
@@ -244,6 +245,8 @@ def run_tank_adjoint(dev, src, n, reps=2):
     return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
             "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
+            "autotune": {"variant": variant, "blocks_per_sm": bps,
+                         "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}},
             "jacobian_abs_sum": [float(x) for x in np.abs(jac).sum(0)]}  # fmt: skip
 
 
@@ -254,7 +257,7 @@ def run_lar(dev, n, reps=2):
     import torch
 
     from lumen_b200 import _abi as A
-    from lumen_b200 import detectors, sources
+    from lumen_b200 import autotune, detectors, sources
     from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
 
     det = detectors.lar_box(sigma_alpha=0.1)
@@ -264,7 +267,8 @@ def run_lar(dev, n, reps=2):
     ds = DeviceSource(src, n, dev)
     names = ["surfaces/CageSurface/R", "media/LAr/rayleigh"]
     gt = [det.params_index[k] for k in names]
-    c = A.controls(grad_tabs=gt)
+    (variant, bps), times = autotune.tune(eng, ds, 1 << 18, gt, ds.n_events, A.key_of_seed(0))
+    c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps)
     T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
     eng.trace(key, min(n, 1 << 18), source=ds, controls=c, tallies=T)
@@ -283,7 +287,9 @@ def run_lar(dev, n, reps=2):
     eng.close()
     return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
-            "points": 10000, "gradients": names, "arrivals_sum": float(T.arrival.sum().item())}  # fmt: skip
+            "points": 10000, "gradients": names, "arrivals_sum": float(T.arrival.sum().item()),
+            "autotune": {"variant": variant, "blocks_per_sm": bps,
+                         "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}}}  # fmt: skip
 
 
 def main():

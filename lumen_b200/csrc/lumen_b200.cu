@@ -311,7 +311,7 @@ __device__ __forceinline__ void wv_st(uint32_t* b, int W, int i, const T& v) {
 }
 
 template <int G>
-__global__ void __launch_bounds__(256, 2) k_wave_query(Launch L, Wave V) {
+__global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V.W || !V.act[i]) return;
   if (L.abort_flag && *(volatile int*)L.abort_flag) return;
