@@ -223,7 +223,8 @@ def run_tank_adjoint(dev, src, n, reps=2):
     names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R",
              "surfaces/BlackSheet/sigma_alpha"]  # fmt: skip
     gt = [det.params_index[k] for k in names]
-    (variant, bps), times = autotune.tune(eng, ds, 1 << 21, gt, ds.n_events, A.key_of_seed(0))
+    # a sample of several pool fills: the wavefront's last rounds run few photons, a cost a one-fill sample overstates
+    (variant, bps), times = autotune.tune(eng, ds, min(n, 1 << 23), gt, ds.n_events, A.key_of_seed(0), reps=1)
     c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps)
     T = DeviceTallies(det.n_sensor, ds.n_events, 200, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
@@ -267,7 +268,7 @@ def run_lar(dev, n, reps=2):
     ds = DeviceSource(src, n, dev)
     names = ["surfaces/CageSurface/R", "media/LAr/rayleigh"]
     gt = [det.params_index[k] for k in names]
-    (variant, bps), times = autotune.tune(eng, ds, 1 << 18, gt, ds.n_events, A.key_of_seed(0))
+    (variant, bps), times = autotune.tune(eng, ds, min(n, 1 << 20), gt, ds.n_events, A.key_of_seed(0), reps=1)
     c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps)
     T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)

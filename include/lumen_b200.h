@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 2
+#define LUMEN_B200_ABI_VERSION 3
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -120,6 +120,14 @@ typedef struct LumenSceneDesc {
   const float* pool;         /* host, n_pool: the table values every call reads unless set_pools replaces them */
   const float* unified;      /* host, LUMEN_UNI_WORDS: the unified facet tables; may be null when no row draws the
                                 unified facet lobe (src/lumen/surfaces/facets.py:165 table_operands) */
+  /* sensor reach (src/lumen/geometry/reach.py:66 build): a bulk step's query stops just past its free path where the
+     segment to its component's box exit meets no sensor box, an exact speed-up. All null / 0: never bounded. */
+  int32_t n_comp, n_fnode;
+  const int32_t* comp;       /* host, n_vol + 1: each volume's component (volumes joined by crossings without a
+                                vertex); the outside's is -1 */
+  const float* comp_box;     /* host, n_comp * 6: each component's padded box (lo, hi) */
+  const float* fnode_f;      /* host, n_fnode * LUMEN_NODE_F: a depth-first tree over the padded sensor boxes */
+  const int32_t* fnode_i;    /* host, n_fnode * LUMEN_NODE_I: skip (the node after the subtree), count (> 0: a leaf) */
 } LumenSceneDesc;
 
 typedef struct LumenScene LumenScene; /* opaque: the device copy of a LumenSceneDesc */
@@ -153,8 +161,10 @@ typedef struct LumenSource {
 } LumenSource;
 
 /* ------------------------------------------------------------------------------------------ the controls */
-enum { LUMEN_F_ASYNC = 1 };  /* controls.flags: enqueue only (no host wait, no status read back: capturable in a
+enum { LUMEN_F_ASYNC = 1,   /* controls.flags: enqueue only (no host wait, no status read back: capturable in a
                                  CUDA graph); a step budget that ran out then shows in counts[LUMEN_C_ABORTED] */
+       LUMEN_F_REACH = 2 };  /* bound bulk steps' queries by the scene's sensor reach (exact: every tally is the same;
+                                off by default, a speed-up only where bulk steps are common and sensors far) */
 enum { LUMEN_VARIANT_WAVEFRONT = 3, LUMEN_N_VARIANT = 4 };
 /* launch variants: the persistent photon loop at 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
    2 = 256 x 3 (85 registers); 3 = the wavefront: rounds of two kernels (the query; the rest of the step and the

@@ -25,6 +25,7 @@ N_COL = 10
 N_HEALTH = 11
 N_COUNT = 6
 F_ASYNC = 1
+F_REACH = 2
 N_VARIANT = 4
 VARIANT_WAVEFRONT = 3
 UNI_NX, UNI_NY = 257, 69
@@ -48,6 +49,8 @@ class LumenSceneDesc(ctypes.Structure):
         ("n_pool", ctypes.c_int32), ("n_sensor", ctypes.c_int32),
         ("cls_medium", c_i32p), ("row_of", c_i32p), ("med_i", c_i32p), ("row_i", c_i32p), ("tab", c_i32p),
         ("pool", c_f32p), ("unified", c_f32p),
+        ("n_comp", ctypes.c_int32), ("n_fnode", ctypes.c_int32), ("comp", c_i32p), ("comp_box", c_f32p),
+        ("fnode_f", c_f32p), ("fnode_i", c_i32p),
     ]  # fmt: skip
 
 

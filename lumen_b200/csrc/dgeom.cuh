@@ -57,6 +57,11 @@ struct DScene {
   const int32_t* __restrict__ row_i;
   const int32_t* __restrict__ tab;
   const float* __restrict__ uni;  // the unified facet tables (LUMEN_UNI_WORDS), null without a unified facet row
+  const int32_t* __restrict__ comp;   // sensor reach: each volume's component (null: never bounded)
+  const float* __restrict__ comp_box;
+  const float* __restrict__ fnode_f;
+  const int32_t* __restrict__ fnode_i;
+  int n_fnode;
 };
 
 L_DEV float d_dot(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
@@ -570,8 +575,9 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
 }
 
 // slab test of a node's box (bvh.py:258)
-L_DEV void d_slab(const DScene& S, int node, const float* o, const float* inv, float* tin, float* tout) {
-  const float* nf = S.node_f + (size_t)node * LUMEN_NODE_F;
+L_DEV void d_slab(const float* __restrict__ node_f, int node, const float* o, const float* inv, float* tin,
+                  float* tout) {
+  const float* nf = node_f + (size_t)node * LUMEN_NODE_F;
   float lo_t = -D_HUGE * 10.0f, hi_t = D_HUGE * 10.0f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -612,7 +618,7 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
         started = 1;
         if (n0 < n1) {
           float tin, tout;
-          d_slab(S, n0, c.od, inv, &tin, &tout);
+          d_slab(S.node_f, n0, c.od, inv, &tin, &tout);
           node = (tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band) ? n0 : -1;
         }
       }
@@ -634,8 +640,8 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
         int lc = node + 1;
         int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
         float tl, tlo, tr, tro;
-        d_slab(S, lc, c.od, inv, &tl, &tlo);
-        d_slab(S, rc, c.od, inv, &tr, &tro);
+        d_slab(S.node_f, lc, c.od, inv, &tl, &tlo);
+        d_slab(S.node_f, rc, c.od, inv, &tr, &tro);
         float lim = d_min(b.t, c.t_bound) + c.band;
         int hl = tl <= tlo && tlo >= c.t_lo && tl <= lim;
         int hr = tr <= tro && tro >= c.t_lo && tr <= lim;
@@ -819,6 +825,43 @@ L_DEV Query d_query(const DScene& S, const float* o, const float* d, int vol, fl
   q.vol_at = pz_vat;
   q.rounds = it;
   return q;
+}
+
+// ------------------------------------------------------------------------------------------------ sensor reach
+// The query's bound for a bulk step (src/lumen/geometry/reach.py:201 ReachGeometry.query): where the photon, not on a
+// surface, starts inside its component's box, its free path s ends before the box's exit T, and the segment [0, T]
+// meets no sensor box, every crossing it can deposit at lies beyond s, so the query may stop at s plus the
+// navigator's own look-ahead ((GRAZE K_ON + 2) bands): the same arithmetic for every round that starts before s
+L_DEV float d_reach_bound(const DScene& S, const float* x, const float* d, int vol, int srf, float s, float t_max) {
+  if (!S.comp || srf >= 0 || vol < 0 || vol > S.n) return t_max;
+  int c = __ldg(S.comp + vol);
+  if (c < 0) return t_max;
+  float inv[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float dv = d[a];
+    inv[a] = 1.0f / (fabsf(dv) < D_TINY_DIR ? (dv < 0.0f ? -D_TINY_DIR : D_TINY_DIR) : dv);
+  }
+  const float* cb = S.comp_box + (size_t)c * 6;
+  float tin = -D_HUGE * 10.0f, tout = D_HUGE * 10.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float ta = (__ldg(cb + a) - x[a]) * inv[a];
+    float tb = (__ldg(cb + 3 + a) - x[a]) * inv[a];
+    tin = d_max(tin, d_min(ta, tb));
+    tout = d_min(tout, d_max(ta, tb));
+  }
+  if (!(tin <= 0.0f && s < tout && s < t_max)) return t_max;
+  for (int node = 0, guard = 0; node < S.n_fnode && guard < S.n_fnode; ++guard) {  // any sensor box on [0, T]
+    float ti, to;
+    d_slab(S.fnode_f, node, x, inv, &ti, &to);
+    int hit = ti <= to && to >= 0.0f && ti <= tout;
+    int leaf = __ldg(S.fnode_i + (size_t)node * LUMEN_NODE_I + 1) > 0;
+    if (hit && leaf) return t_max;
+    node = (hit && !leaf) ? node + 1 : __ldg(S.fnode_i + (size_t)node * LUMEN_NODE_I);
+  }
+  float look = (D_GRAZE * D_K_ON + 2.0f) * d_band(d_maxabs3(x) + s);
+  return d_min(t_max, s + look);
 }
 
 }  // namespace lb

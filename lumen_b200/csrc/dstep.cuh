@@ -22,6 +22,7 @@ struct Run {
   int max_vertices;
   int P;
   int gt[LUMEN_MAX_GRAD];
+  int reach_on;  // LUMEN_F_REACH: bulk steps' queries bounded by the sensor reach
 };
 
 struct Photon {
@@ -74,8 +75,11 @@ L_DEV void d_pre(const Run& R, Photon& ph, Key pkey, Pre& pr) {
   pr.s = -l_log(uniform(pr.vkey, 0)) / d_max(pr.mr.mu_c, D_FLOOR32);
 }
 
+// the step's query, bounded just past the free path where no sensor can be met (step.py:260 _query with
+// reach.py's bound; the same result as the unbounded query on everything the step reads)
 L_DEV Query d_step_query(const Run& R, const Photon& ph, const Pre& pr) {
-  return d_query(R.S, ph.x, ph.d, ph.vol, R.max_distance, ph.srf, ph.sn, pr.s);
+  float tm = R.reach_on ? d_reach_bound(R.S, ph.x, ph.d, ph.vol, ph.srf, pr.s, R.max_distance) : R.max_distance;
+  return d_query(R.S, ph.x, ph.d, ph.vol, tm, ph.srf, ph.sn, pr.s);
 }
 
 // the step after its query (step.py:516 step: the crossing, the event, the deposit, the roulette)
@@ -110,14 +114,40 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
   int cont = (q.cont || (zero && row < 0)) && q.hit;
   if (cont) row = row > 0 ? row : 0;
   int mi_after = __ldg(S.cls_medium + ca);
-  float n2l = d_index_at(S, R.live, ph.lam, mi_after);
+  int scatter = mu_r > 0.0f && s < dist && ph.alive;
+  // A bulk step reads of the crossing's surface row only its detected share (the expected deposit at the crossing),
+  // and that share is a * eff: where eff is 0 at this wavelength and moves with no gradient parameter, the row's
+  // evaluation is not needed (its outcome probabilities are read by a surface event only)
+  int need_eval = !scatter;
+  if (scatter && q.hit && ph.alive && row >= 0 && !cont) {
+    int te = __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_COL + LUMEN_COL_EFF);
+    need_eval = d_tab(S, R.live, te, D_HC / ph.lam) != 0.0f;
+    if (G > 0)
+      for (int p = 0; p < P; ++p) need_eval = need_eval || te == R.gt[p];
+  }
   float dprobs[G > 0 ? G : 1][N_OUT], ddet[G > 0 ? G : 1];
   Eval le, re;
-  d_type_eval<G>(S, R.live, row, ph.lam, ph.d, q.normal, ml.n, n2l, er0, ei0, le, P, R.gt, dprobs, ddet);
-  if (R.shared) re = le;
-  else {
-    float n2r = d_index_at(S, R.ref, ph.lam, mi_after);
-    d_type_eval<0>(S, R.ref, row, ph.lam, ph.d, q.normal, mr.n, n2r, er0, ei0, re, 0, R.gt, dprobs, ddet);
+  float n2l = 1.0f;  // the far side's live index (a surface event always evaluates the row)
+  if (need_eval) {
+    n2l = d_index_at(S, R.live, ph.lam, mi_after);
+    d_type_eval<G>(S, R.live, row, ph.lam, ph.d, q.normal, ml.n, n2l, er0, ei0, le, P, R.gt, dprobs, ddet);
+    if (R.shared || scatter) re = le;  // a bulk step reads no reference probability
+    else {
+      float n2r = d_index_at(S, R.ref, ph.lam, mi_after);
+      d_type_eval<0>(S, R.ref, row, ph.lam, ph.d, q.normal, mr.n, n2r, er0, ei0, re, 0, R.gt, dprobs, ddet);
+    }
+  } else {
+#pragma unroll
+    for (int o = 0; o < N_OUT; ++o) le.probs[o] = 0.0f;
+    le.detect = 0.0f;
+    le.sigma = 0.1f;
+    re = le;
+    if (G > 0)
+      for (int p = 0; p < P; ++p) {
+#pragma unroll
+        for (int o = 0; o < N_OUT; ++o) dprobs[p][o] = 0.0f;
+        ddet[p] = 0.0f;
+      }
   }
   if (cont) {
 #pragma unroll
@@ -138,7 +168,6 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
 #pragma unroll
   for (int o = 0; o < N_OUT; ++o) p_prop[o] = tot > 0.0f ? re.probs[o] / tot : 0.0f;
   float mu = ml.mu_c;
-  int scatter = mu_r > 0.0f && s < dist && ph.alive;
   int oc_ = scatter ? 0 : d_choose6(p_prop, uniform(vkey, 2));
   int os_ = oc_ > 0 ? oc_ : 0;
   int drawn = oc_ >= 0;

@@ -563,6 +563,16 @@ static int check_desc(const LumenSceneDesc* d) {
     if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && !d->unified)
       return set_err(LUMEN_ERR_ARG, "scene_create: a unified facet row needs the unified tables (desc->unified)");
   }
+  if (d->comp) {  // the sensor reach arrays
+    if (!d->comp_box || d->n_comp <= 0 || d->n_fnode < 0 || (d->n_fnode > 0 && (!d->fnode_f || !d->fnode_i)))
+      return set_err(LUMEN_ERR_ARG, "scene_create: inconsistent sensor reach arrays");
+    for (int v = 0; v <= d->n_vol; ++v)
+      if (d->comp[v] < -1 || d->comp[v] >= d->n_comp) return set_err(LUMEN_ERR_ARG, "scene_create: a component is out of range");
+    for (int k = 0; k < d->n_fnode; ++k) {
+      int sk = d->fnode_i[(size_t)k * LUMEN_NODE_I];
+      if (sk <= k || sk > d->n_fnode) return set_err(LUMEN_ERR_ARG, "scene_create: a sensor-box tree skip is out of order");
+    }
+  }
   return 0;
 }
 
@@ -595,6 +605,7 @@ static int fill_run(const LumenScene* sc, const LumenControls* c, Run& R) {
   R.max_vertices = c->max_vertices;
   R.P = c->n_grad;
   for (int p = 0; p < LUMEN_MAX_GRAD; ++p) R.gt[p] = p < c->n_grad ? c->grad_tab[p] : -1;
+  R.reach_on = (c->flags & LUMEN_F_REACH) && sc->S.comp != nullptr;
   return 0;
 }
 
@@ -901,6 +912,19 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   UPLOAD(pl, d->pool, (size_t)d->n_pool);
   S.uni = nullptr;
   if (d->unified) UPLOAD(S.uni, d->unified, (size_t)LUMEN_UNI_WORDS);
+  S.comp = nullptr;
+  S.comp_box = S.fnode_f = nullptr;
+  S.fnode_i = nullptr;
+  S.n_fnode = 0;
+  if (d->comp) {
+    UPLOAD(S.comp, d->comp, (size_t)d->n_vol + 1);
+    UPLOAD(S.comp_box, d->comp_box, (size_t)d->n_comp * 6);
+    if (d->n_fnode > 0) {
+      UPLOAD(S.fnode_f, d->fnode_f, (size_t)d->n_fnode * LUMEN_NODE_F);
+      UPLOAD(S.fnode_i, d->fnode_i, (size_t)d->n_fnode * LUMEN_NODE_I);
+    }
+    S.n_fnode = d->n_fnode;
+  }
   if (e) {
     for (void* p : sc->allocs) cudaFree(p);
     delete sc;

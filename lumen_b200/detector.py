@@ -93,6 +93,12 @@ class Detector:
         if self.draws_facets:  # a unified facet row (reflect, not about the global normal): the lobe's tables
             keep["unified"] = facets.flat()
             d.unified = fptr(keep["unified"])
+        r = G.reach_arrays(a)  # the sensor reach of bulk steps' queries
+        for k, v in r.items():
+            keep[k] = v
+        d.n_comp, d.n_fnode = len(r["comp_box"]), len(r["fnode_i"])
+        d.comp, d.comp_box = iptr(keep["comp"]), fptr(keep["comp_box"])
+        d.fnode_f, d.fnode_i = fptr(keep["fnode_f"]), iptr(keep["fnode_i"])
         return d, keep
 
     @property

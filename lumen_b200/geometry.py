@@ -277,6 +277,55 @@ def bvh_depth(node_i, n0, n1) -> int:
     return depth
 
 
+# ------------------------------------------------------------------------------------------------ sensor reach
+BAND_ULPS_EPS = 8.0 * 2.0**-23  # the navigator's band: BAND_ULPS float32 ulps of the coordinate scale, plus a floor
+BAND_FLOOR = 1e-9
+K_ON = 4.0
+
+
+def reach_arrays(arrays) -> dict:
+    """Return the arrays that let a bulk step's query stop just past its free path (src/lumen/geometry/reach.py:66
+    ``build``): per volume its COMPONENT (the volumes joined to it by crossings without a vertex: a parent and a
+    daughter of one class), each component's box (the union of its members' padded world boxes), and a skip-pointer
+    tree over every sensor volume's box; the component and sensor boxes padded by the contact tolerance at the scene's
+    scale (K_ON bands). The outside has no component (-1).
+    """
+    vol_i, vol_f = arrays["vol_i"], np.asarray(arrays["vol_f"], np.float64)
+    n = int(arrays["n_vol"])
+    parent, cls, sensor = vol_i[:n, 1], vol_i[:, 2], vol_i[:n, 3]
+    root = list(range(n))
+
+    def find(a):
+        while root[a] != a:
+            root[a] = root[root[a]]
+            a = root[a]
+        return a
+
+    for v in range(n):
+        p = int(parent[v])
+        if p < n and cls[v] == cls[p]:
+            ra, rb = find(v), find(p)
+            if ra != rb:
+                root[rb] = ra
+    roots = [find(v) for v in range(n)]
+    uniq, comp = np.unique(np.asarray(roots, np.int64), return_inverse=True) if n else (np.zeros(0), np.zeros(0))
+    lo_w, hi_w = vol_f[:n, 12:15], vol_f[:n, 15:18]
+    scale = float(np.max(np.abs(np.concatenate([lo_w, hi_w])))) if n else 1.0
+    pad = K_ON * (BAND_ULPS_EPS * scale + BAND_FLOOR)
+    c_lo = np.full((len(uniq), 3), np.inf)
+    c_hi = np.full((len(uniq), 3), -np.inf)
+    np.minimum.at(c_lo, comp, lo_w)
+    np.maximum.at(c_hi, comp, hi_w)
+    sv = np.flatnonzero(sensor >= 0)
+    f_lo, f_hi = lo_w - pad, hi_w + pad
+    nodes, _ = _bvh(sv.astype(np.int64), f_lo, f_hi)
+    fnode_f = np.asarray([[*nd[0], *nd[1]] for nd in nodes], np.float32).reshape(-1, 6)
+    fnode_i = np.asarray([[nd[2], nd[3], 0, 0] for nd in nodes], np.int32).reshape(-1, 4)
+    return dict(comp=np.append(comp, -1).astype(np.int32),
+                comp_box=np.concatenate([c_lo - pad, c_hi + pad], 1).astype(np.float32).reshape(-1, 6),
+                fnode_f=fnode_f, fnode_i=fnode_i)  # fmt: skip
+
+
 # ------------------------------------------------------------------------------------------------- the arrays
 def pad_box(lo, hi):
     """Return the box padded as the navigator's world boxes (tolerances.py:83-84)."""

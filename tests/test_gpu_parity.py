@@ -243,3 +243,18 @@ def test_wavefront_refuses_asynchronous_calls(tank, built):
     c = A.controls(variant=A.VARIANT_WAVEFRONT, flags=A.F_ASYNC)
     with pytest.raises(Exception, match="LUMEN_F_ASYNC"):
         eng.trace(KEY, 1024, source=ds, controls=c, tallies=T)
+
+
+@pytest.mark.parametrize("which", ["tank", "lar", "facet_lar"])
+def test_sensor_reach_bound_changes_no_photon(which, tank, lar, facet_lar, built):
+    """LUMEN_F_REACH (src/lumen/geometry/reach.py): bulk steps' queries stop just past the free path where no sensor
+    can be met; every photon's record is still the unbounded checker's, bit for bit."""
+    c = A.controls(flags=A.F_REACH)
+    if which == "tank":
+        src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+        bad, gi, oi, gf, of = _records_match(tank, src, 1 << 14, controls=c)
+    else:
+        det = lar if which == "lar" else facet_lar
+        src = sources.Scintillation(position=[(0.3, 0.2, -0.4)], lam=128.0, tau=(6.0, 1500.0), fraction=0.25)
+        bad, gi, oi, gf, of = _records_match(det, src, 1 << 11, controls=c)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
