@@ -37,6 +37,11 @@ METRIC = "photons/s on 1 B200 (fwd; batched fwd+adjoint) at matched per-PMT MC e
 L2_FLUSH_BYTES = 256 << 20
 
 
+# DRAM bytes per photon of k_trace<0,256,4> on the tank workload: ncu's dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch of 2^20 photons (2.556 GB + 3.611 GB), almost all of it local memory; it grows with the photons
+TRAFFIC_PER_PHOTON = (2.556263e9 + 3.611490e9) / 1048576
+
+
 def workload_point(seed=12345):
     rng = np.random.default_rng(seed)
     while True:
@@ -305,6 +310,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched and liquid-argon workloads")
     ap.add_argument("--lar-photons", type=int, default=1 << 24)
+    ap.add_argument("--variant", type=int, default=0, help="the headline workload's launch variant (3: wavefront)")
     args = ap.parse_args()
 
     from lumen_b200 import detectors, sources
@@ -347,7 +353,7 @@ def main():
     first = rank * n  # this rank's photon ids
     ds = DeviceSource(src, n * world, dev)
     T = DeviceTallies(det.n_sensor, 1, 200, 0.0, 1.0, 0, dev)
-    c = A.controls()
+    c = A.controls(variant=args.variant)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -411,10 +417,14 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "photon_steps_per_s": world * float(cnt[1]) / (ms_step * 1e-3), "steps_per_photon": steps_pp,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
-                         "traffic": None, "peak_kind": pk_kind,
-                         "algorithmic_bytes": alg},
+                         "traffic": TRAFFIC_PER_PHOTON * n if args.variant == 0 else None, "peak_kind": pk_kind,
+                         "algorithmic_bytes": alg,
+                         "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-photon launch "
+                                         "of k_trace<0,256,4> on this workload (6.17 GB), scaled by photons"},
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": args.steps, "clocks": clk.summary(), "ms_steps": [round(x, 3) for x in ms],
+            # one launch of the persistent loop per step (the wavefront's rounds are counted by no host-side number)
+            "gpu_launches": args.steps if args.variant != 3 else None, "launch_variant": args.variant,
+            "clocks": clk.summary(), "ms_steps": [round(x, 3) for x in ms],
             "arrivals_sum": float(light.arrivals.sum())}  # fmt: skip
     if rank == 0 and not args.no_extra:
         line["tank_fwd_adjoint"] = run_tank_adjoint(dev, src, n)
