@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 3
+#define LUMEN_B200_ABI_VERSION 4
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -70,8 +70,17 @@ enum { LUMEN_COL_R = 0, LUMEN_COL_T, LUMEN_COL_EFF, LUMEN_COL_PSPIKE, LUMEN_COL_
        LUMEN_COL_SIGMA, LUMEN_COL_POLISH, LUMEN_COL_NR, LUMEN_COL_NK, LUMEN_N_COL };
 enum { LUMEN_RI_MODEL = 0, LUMEN_RI_NORMAL = 1, LUMEN_RI_GLISUR = 2, LUMEN_RI_FAR_OPAQUE = 3,
        LUMEN_RI_PER_NORMAL = 4, LUMEN_RI_COL = 6, LUMEN_ROW_I = 16 };
-/* Medium ints: index table (-1 opaque), absorption-length table (-1 none), Rayleigh-length table (-1 none) */
-enum { LUMEN_MI_INDEX = 0, LUMEN_MI_ABS = 1, LUMEN_MI_RAY = 2, LUMEN_MED_I = 4 };
+/* Medium ints, one table index each (-1: none), src/lumen/media/bulk.py:45 Medium with its channels in Geant4's order
+   (bulk.py:21 CHANNEL_ORDER): the index (-1: opaque), the absorption length, the Rayleigh length; the Mie (G4OpMieHG)
+   length and its lobe constants g_forward, g_backward, forward_ratio (MIEHG, MIEHG_FORWARD, MIEHG_BACKWARD,
+   MIEHG_FORWARD_RATIO); the WLS (G4OpWLS) absorption length, mean photons, time constant (ns) and emission spectrum
+   (WLSABSLENGTH, WLSMEANNUMBERPHOTONS, WLSTIMECONSTANT, WLSCOMPONENT: energies as the knots, intensities as the
+   values); then the WLS time profile as a plain int (0: delta, Geant4's default; 1: exponential). A channel whose
+   length table is -1 is absent. */
+enum { LUMEN_MI_INDEX = 0, LUMEN_MI_ABS = 1, LUMEN_MI_RAY = 2, LUMEN_MI_MIE = 3, LUMEN_MI_MIE_GF = 4,
+       LUMEN_MI_MIE_GB = 5, LUMEN_MI_MIE_R = 6, LUMEN_MI_WLS = 7, LUMEN_MI_WLS_YIELD = 8, LUMEN_MI_WLS_TAU = 9,
+       LUMEN_MI_WLS_SPEC = 10, LUMEN_MI_WLS_PROFILE = 11, LUMEN_MED_I = 16 };
+enum { LUMEN_N_CHANNEL = 3 };  /* bulk channels: Rayleigh, Mie, WLS */
 /* Table t: tab[2t] = offset into a pool, tab[2t+1] = knots k >= 1; pool[off .. off+k) energies (eV, ascending),
    pool[off+k .. off+2k) values; linear in photon energy between knots, held beyond (G4PhysicsVector::Value) */
 

@@ -69,19 +69,39 @@ L_CALL float d_group_index(const DScene& S, const float* __restrict__ pool, int 
   return 1.0f / f;
 }
 
-struct Med { float n, ng, mu_abs, mu_c; };
+struct Med { float n, ng, mu_abs, mu_c; };  // mu_c: the channels' rates summed
 
+// the length table of channel c (Rayleigh, Mie, WLS: bulk.py:21 CHANNEL_ORDER) of a medium record, -1 if absent
+L_DEV int d_channel_tab(const int32_t* m, int c) {
+  return __ldg(m + (c == 0 ? LUMEN_MI_RAY : (c == 1 ? LUMEN_MI_MIE : LUMEN_MI_WLS)));
+}
+
+// the channels' rates of medium mi at lam (bulk.py:88 evaluate's mu), 0 for an absent channel
+L_DEV void d_channel_rates(const DScene& S, const float* __restrict__ pool, float lam, int mi, float* ch) {
+  const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
+  float E = D_HC / lam;
+#pragma unroll
+  for (int c = 0; c < LUMEN_N_CHANNEL; ++c) {
+    int t = d_channel_tab(m, c);
+    ch[c] = t >= 0 ? d_rate(d_tab(S, pool, t, E)) : 0.0f;
+  }
+}
+
+// (n, n_g, mu_abs, the channels' rates summed) of medium mi at lam (medium.py:27, bulk.py:88 evaluate); a bulk event
+// reads the channels' own rates again (d_channel_rates: the same values)
 L_CALL Med d_medium_at(const DScene& S, const float* __restrict__ pool, float lam, int mi) {
   const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
   float E = D_HC / lam;
   Med r = {1.0f, 1.0f, 0.0f, 0.0f};
-  int ti = __ldg(m + LUMEN_MI_INDEX), ta = __ldg(m + LUMEN_MI_ABS), tr = __ldg(m + LUMEN_MI_RAY);
+  int ti = __ldg(m + LUMEN_MI_INDEX), ta = __ldg(m + LUMEN_MI_ABS);
   if (ti >= 0) {
     r.n = d_tab(S, pool, ti, E);
     r.ng = d_group_index(S, pool, ti, E);
   }
   if (ta >= 0) r.mu_abs = d_rate(d_tab(S, pool, ta, E));
-  if (tr >= 0) r.mu_c = d_rate(d_tab(S, pool, tr, E));
+  float ch[LUMEN_N_CHANNEL];
+  d_channel_rates(S, pool, lam, mi, ch);
+  r.mu_c = (ch[0] + ch[1]) + ch[2];
   return r;
 }
 L_DEV float d_index_at(const DScene& S, const float* __restrict__ pool, float lam, int mi) {

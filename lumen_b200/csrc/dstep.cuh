@@ -4,7 +4,7 @@
 // Arithmetic operation for operation the CPU checker's; uniforms are drawn lazily (each is a pure function of the
 // vertex key and its index, so skipping an unused one changes nothing).
 #pragma once
-#include "dphys.cuh"
+#include "dmedia.cuh"
 
 namespace lb {
 
@@ -92,17 +92,23 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
   const Med& ml = pr.ml;
   const Med& mr = pr.mr;
   float er0[3] = {ph.er[0], ph.er[1], ph.er[2]}, ei0[3] = {ph.ei[0], ph.ei[1], ph.ei[2]};
-  float dmu_abs[G > 0 ? G : 1], dmu_c[G > 0 ? G : 1];
+  const int mi = __ldg(S.cls_medium + ph.cls);
+  float dmu_abs[G > 0 ? G : 1], dmu_c[G > 0 ? G : 1], dch[G > 0 ? G : 1][LUMEN_N_CHANNEL];
   if (G > 0) {
-    int mi = __ldg(S.cls_medium + ph.cls);
     const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
-    int ta = __ldg(m + LUMEN_MI_ABS), tr = __ldg(m + LUMEN_MI_RAY);
+    int ta = __ldg(m + LUMEN_MI_ABS);
     float E = D_HC / ph.lam;
     for (int p = 0; p < P; ++p) {
       dmu_abs[p] = 0.0f;
-      dmu_c[p] = 0.0f;
       if (ta >= 0 && ta == R.gt[p]) dmu_abs[p] = d_tab(S, R.live, ta, E) >= D_FLT_TINY ? -(ml.mu_abs * ml.mu_abs) : 0.0f;
-      if (tr >= 0 && tr == R.gt[p]) dmu_c[p] = d_tab(S, R.live, tr, E) >= D_FLT_TINY ? -(ml.mu_c * ml.mu_c) : 0.0f;
+#pragma unroll
+      for (int c = 0; c < LUMEN_N_CHANNEL; ++c) {
+        int t = d_channel_tab(m, c);
+        float L = (t >= 0 && t == R.gt[p]) ? d_tab(S, R.live, t, E) : 0.0f;
+        float rc = d_rate(L);
+        dch[p][c] = (t >= 0 && t == R.gt[p] && L >= D_FLT_TINY) ? -(rc * rc) : 0.0f;
+      }
+      dmu_c[p] = (dch[p][0] + dch[p][1]) + dch[p][2];
     }
   }
   float mu_r = mr.mu_c;
@@ -188,42 +194,70 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
       dq[p] = at_if ? dw[p] * f + ph.w * df : 0.0f;
     }
   float lost = (q.hit && ph.alive && row < 0 && !scatter) ? ph.w * rr * att_if : 0.0f;
-  float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_er[3], nx_ei[3];
+  float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_er[3], nx_ei[3], nx_lam = ph.lam;
   float nx_dw[G > 0 ? G : 1];
   int nx_cls, nx_ok, nx_far = 0;
   float fates0, fates1, fates2, wr;
   if (scatter) {
     int next_cls = s < q.t_pass0 ? q.cls_start : (s > q.t_pass1 ? cb : d_cls(S, q.vol_at));
-    float mu_c_r = mr.mu_c;
+    // the channel drawn from the reference rates (estimator.choose, uniform 1); with one channel present it is that
+    // channel whatever the uniform
+    float chl[LUMEN_N_CHANNEL], chr_[LUMEN_N_CHANNEL];
+    d_channel_rates(S, R.live, ph.lam, mi, chl);
+    if (R.shared) {
+#pragma unroll
+      for (int c = 0; c < LUMEN_N_CHANNEL; ++c) chr_[c] = chl[c];
+    } else {
+      d_channel_rates(S, R.ref, ph.lam, mi, chr_);
+    }
+    int n_ch = (chr_[0] > 0.0f) + (chr_[1] > 0.0f) + (chr_[2] > 0.0f);
+    int cs = chr_[0] > 0.0f ? 0 : (chr_[1] > 0.0f ? 1 : 2);
+    if (n_ch > 1) {
+      float c0 = chr_[0], c1 = c0 + chr_[1], c2 = c1 + chr_[2];
+      float thr = uniform(vkey, 1) * c2;
+      cs = c0 > thr ? 0 : (c1 > thr ? 1 : (c2 > thr ? 2 : 0));
+    }
+    float mu_c_r = chr_[cs], mu_c_l = chl[cs];
     float e_r = l_exp(-mu_r * s), e_l = l_exp(-mu * s);
     float path_r = mu_c_r * e_r;
-    float w_path = d_ratio(ml.mu_c * e_l, path_r);
+    float w_path = d_ratio(mu_c_l * e_l, path_r);
     float att = l_exp(-ml.mu_abs * s);
     float w = w_path * att;
     float w_r = d_ratio(path_r, path_r) * l_exp(-mr.mu_abs * s);
 #pragma unroll
     for (int a = 0; a < 3; ++a) nx_x[a] = ph.x[a] + s * ph.d[a];
-    d_rayleigh_sample(er0, ei0, uniform(vkey, 3), uniform(vkey, 4), uniform(vkey, 5), nx_d);
+    float rlw = 1.0f, y_w = 1.0f, y_r = 1.0f, delay = 0.0f;
+    Bulk2 b2;
+    if (cs == 0) {  // Rayleigh: the polarised dipole draw, the state projected (phase.py:57)
+      d_rayleigh_sample(er0, ei0, uniform(vkey, 3), uniform(vkey, 4), uniform(vkey, 5), nx_d);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
-    d_project(nx_er, nx_ei, nx_d);
+      for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+      d_project(nx_er, nx_ei, nx_d);
+    } else {  // Mie (G4OpMieHG) or WLS (G4OpWLS)
+      d_bulk_other(S, R.live, R.ref, R.shared, cs, mi, ph.lam, ph.d, er0, ei0, vkey, P, R.gt, b2);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) { nx_d[a] = b2.d[a]; nx_er[a] = b2.er[a]; nx_ei[a] = b2.ei[a]; }
+      rlw = b2.rlw; y_w = b2.y_w; y_r = b2.y_r; delay = b2.delay;
+      nx_lam = b2.lam;
+    }
     float w_at = ph.w * w_path;
-    fates0 = w_at * att * 1.0f;
-    fates1 = w_at * (1.0f - att * 1.0f);
+    fates0 = w_at * att * y_w;
+    fates1 = w_at * (1.0f - att * y_w);
     fates2 = 0.0f;
-    nx_w = ph.w * w * 1.0f * 1.0f;
+    nx_w = ph.w * w * rlw * y_w;
     if (G > 0)
       for (int p = 0; p < P; ++p) {
-        float dwp = (dmu_c[p] * e_l + ml.mu_c * (-(dmu_c[p] * s) * e_l)) / path_r;
+        float dwp = (dch[p][cs] * e_l + mu_c_l * (-(dmu_c[p] * s) * e_l)) / path_r;
         if (!(path_r != 0.0f)) dwp = 0.0f;
         float datt = -(dmu_abs[p] * s) * att;
         float dwf = dwp * att + w_path * datt;
-        nx_dw[p] = dw[p] * w + ph.w * dwf;
+        if (cs == 0) nx_dw[p] = dw[p] * w + ph.w * dwf;
+        else nx_dw[p] = (dw[p] * w + ph.w * dwf) * rlw * y_w + ph.w * w * rlw * (b2.dlob[p] * y_w + b2.dyld[p]);
       }
     nx_cls = next_cls;
     nx_ok = 1;
-    nx_dtime = s / v_g;
-    wr = ph.wr * w_r * 1.0f;
+    nx_dtime = s / v_g + delay;
+    wr = ph.wr * w_r * y_r;
   } else {
     float pl = le.probs[os_], pp = p_prop[os_];
     float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
@@ -362,6 +396,7 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
 #pragma unroll
   for (int a = 0; a < 3; ++a) { ph.x[a] = nx_x[a]; ph.d[a] = nx_d[a]; ph.er[a] = nx_er[a]; ph.ei[a] = nx_ei[a]; }
   ph.t = ph.t + nx_dtime;
+  ph.lam = nx_lam;
   ph.w = alive ? w_new : 0.0f;
   ph.wr = alive ? wr_new : 0.0f;
   if (G > 0)

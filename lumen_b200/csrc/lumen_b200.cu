@@ -45,6 +45,7 @@ struct LumenScene {
   std::vector<void*> allocs;
   std::vector<int32_t> sigma_tabs;  // the sigma_alpha tables of the unified facet rows
   std::vector<int32_t> tab;         // host copy of the (offset, knots) table index
+  std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
 };
 
 // --------------------------------------------------------------------------------------------- the kernels
@@ -525,6 +526,18 @@ static int check_desc(const LumenSceneDesc* d) {
     int off = d->tab[2 * t], k = d->tab[2 * t + 1];
     if (k < 1 || off < 0 || off + 2 * k > d->n_pool) return set_err(LUMEN_ERR_ARG, "scene_create: a table is out of the pool");
   }
+  for (int m = 0; m < d->n_med; ++m) {  // every medium's tables in range; a Mie or WLS channel with its constants
+    const int32_t* mr = d->med_i + (size_t)m * LUMEN_MED_I;
+    for (int f = 0; f <= LUMEN_MI_WLS_SPEC; ++f)
+      if (mr[f] < -1 || mr[f] >= d->n_tab) return set_err(LUMEN_ERR_ARG, "scene_create: a medium table is out of range");
+    if (mr[LUMEN_MI_MIE] >= 0 && (mr[LUMEN_MI_MIE_GF] < 0 || mr[LUMEN_MI_MIE_GB] < 0 || mr[LUMEN_MI_MIE_R] < 0))
+      return set_err(LUMEN_ERR_ARG, "scene_create: a Mie channel without its lobe constants");
+    if (mr[LUMEN_MI_WLS] >= 0 && (mr[LUMEN_MI_WLS_YIELD] < 0 || mr[LUMEN_MI_WLS_TAU] < 0 || mr[LUMEN_MI_WLS_SPEC] < 0 ||
+                                  d->tab[2 * mr[LUMEN_MI_WLS_SPEC] + 1] < 2 ||
+                                  (mr[LUMEN_MI_WLS_PROFILE] != 0 && mr[LUMEN_MI_WLS_PROFILE] != 1)))
+      return set_err(LUMEN_ERR_ARG, "scene_create: a WLS channel without its yield, time constant, spectrum (>= 2 "
+                                    "knots) or profile (0 delta, 1 exponential)");
+  }
   for (int m = 0; m < d->n_med; ++m) {
     int ti = d->med_i[m * LUMEN_MED_I + LUMEN_MI_INDEX];
     if (ti >= 0 && d->tab[2 * ti + 1] > LUMEN_MAX_KNOTS) return set_err(LUMEN_ERR_SCENE, "scene_create: an index table has too many knots");
@@ -603,6 +616,10 @@ static int fill_run(const LumenScene* sc, const LumenControls* c, Run& R) {
   R.max_distance = c->max_distance > 0.0f ? c->max_distance : sc->S.reach;
   R.roulette = c->roulette;
   R.max_vertices = c->max_vertices;
+  for (int p = 0; p < c->n_grad; ++p)
+    for (int t : sc->spectrum_tabs)
+      if (c->grad_tab[p] == t)
+        return set_err(LUMEN_ERR_NOT_SUPPORTED, "a WLS emission spectrum as a gradient parameter is not built");
   R.P = c->n_grad;
   for (int p = 0; p < LUMEN_MAX_GRAD; ++p) R.gt[p] = p < c->n_grad ? c->grad_tab[p] : -1;
   R.reach_on = (c->flags & LUMEN_F_REACH) && sc->S.comp != nullptr;
@@ -935,6 +952,10 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
     if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL]) sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
   }
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
+  for (int m = 0; m < d->n_med; ++m) {
+    const int32_t* mr = d->med_i + (size_t)m * LUMEN_MED_I;
+    if (mr[LUMEN_MI_WLS] >= 0) sc->spectrum_tabs.push_back(mr[LUMEN_MI_WLS_SPEC]);
+  }
   if (check_widths(sc, d->pool)) {
     for (void* p : sc->allocs) cudaFree(p);
     delete sc;

@@ -155,7 +155,7 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     # media
     pool = O.Pool()
     med_names = sorted(set(cls_mat))
-    med_i = np.full((len(med_names), 4), -1, np.int32)
+    med_i = np.full((len(med_names), 16), -1, np.int32)
     opaque = {}
     for m, name in enumerate(med_names):
         mat = materials[name]
@@ -169,6 +169,17 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             ray = O.water_rayleigh(O.table(mat.rindex))
         if ray is not None and mat.rindex is not None:
             med_i[m, 2] = pool.add(ray, f"media/{name}/rayleigh")
+        if mat.mie is not None and mat.rindex is not None:  # G4OpMieHG: the length and the lobe's constants
+            med_i[m, 3] = pool.add(mat.mie, f"media/{name}/mie")
+            med_i[m, 4] = pool.add(float(mat.mie_forward), f"media/{name}/mie_g_forward")
+            med_i[m, 5] = pool.add(float(mat.mie_backward), f"media/{name}/mie_g_backward")
+            med_i[m, 6] = pool.add(float(mat.mie_forward_ratio), f"media/{name}/mie_forward_ratio")
+        if mat.wls is not None and mat.rindex is not None:  # G4OpWLS: the absorption length and the emission
+            med_i[m, 7] = pool.add(mat.wls, f"media/{name}/wls")
+            med_i[m, 8] = pool.add(float(mat.wls_mean), f"media/{name}/wls_yield")
+            med_i[m, 9] = pool.add(float(mat.wls_tau), f"media/{name}/wls_tau")
+            med_i[m, 10] = pool.add(tuple(np.asarray(x, np.float64) for x in mat.wls_spectrum), f"media/{name}/wls_spectrum")
+            med_i[m, 11] = 1 if mat.wls_profile == "exponential" else 0
     mi_of = {n: i for i, n in enumerate(med_names)}
     cls_medium = np.asarray([mi_of[m] for m in cls_mat] + [mi_of[cls_mat[0]] if cls_mat else 0], np.int32)
     # surface rows per crossed class pair

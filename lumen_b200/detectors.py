@@ -42,6 +42,32 @@ def toy_tank() -> D.Detector:
     return D.build(tank, {"Water": water, "Photocathode": cathode}, borders=borders, sensors={"pmt": "PMT"})
 
 
+def scintillator_cube(mie=2.0, wls=1.0, rayleigh=5.0, profile="exponential") -> D.Detector:
+    """Return the tutorial tank's geometry filled with a synthetic liquid scintillator whose bulk has all three of
+    Geant4's channels: Rayleigh, Mie (G4OpMieHG, MIEHG ``mie`` m, forward 0.9, backward 0.3, forward ratio 0.8) and a
+    wavelength shifter (G4OpWLS, WLSABSLENGTH ``wls`` m: absorbs below ~410 nm, re-emits a 390-500 nm band with 0.9
+    photons per absorbed one after a ``profile`` 2 ns delay)."""  # noqa: D205
+    e_abs = [1.5, 2.5, 2.9, 3.0, 3.2, 5.0]
+    lab = O.Material("LAB", rindex=([1.5, 2.5, 3.5, 5.0], [1.47, 1.48, 1.50, 1.53]), abslength=20.0,
+                     rayleigh=rayleigh, mie=mie, mie_forward=0.9, mie_backward=0.3, mie_forward_ratio=0.8,
+                     wls=(e_abs, [100.0 * wls, 100.0 * wls, 20.0 * wls, wls, wls, wls]),
+                     wls_spectrum=([2.3, 2.5, 2.7, 2.9, 3.1, 3.2], [0.0, 0.4, 1.0, 0.7, 0.1, 0.0]),
+                     wls_mean=0.9, wls_tau=2.0, wls_profile=profile)  # fmt: skip
+    cathode = O.Material("Photocathode")
+    pmt = G.Volume("PMT", G.Tube(rmax=50 * MM, dz=10 * MM), "Photocathode")
+    tank = G.Volume("TankLV", G.Box(0.5, 0.5, 0.5), "LAB")
+    places = [((0, 0, -480), None), ((0, 0, 480), None), ((-480, 0, 0), ("y", 90)), ((480, 0, 0), ("y", 90)),
+              ((0, -480, 0), ("x", 90)), ((0, 480, 0), ("x", 90)), ((-250, 0, -480), None), ((250, 0, -480), None)]
+    for i, (p, r) in enumerate(places):
+        rot = None if r is None else G.gdml_rotation(**{r[0]: r[1]})
+        tank.place(pmt, np.asarray(p, float) * MM, rot, name=f"PMT_{i}", copy=i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.5, sigma_alpha=0.2, specularlobe=0.5)
+    borders = [("TankLV", f"PMT_{i}", surf) for i in range(8)]
+    return D.build(tank, {"LAB": lab, "Photocathode": cathode}, borders=borders, skins={"TankLV": wall},
+                   sensors={"pmt": "PMT"})  # fmt: skip
+
+
 def _grid_tank(n_pmt, radius, half_h, r_pmt, inset):
     """Return (positions, inward axes) of n_pmt PMTs on a regular barrel and end-cap grid."""
     area = 2 * math.pi * radius * 2 * half_h + 2 * math.pi * radius**2

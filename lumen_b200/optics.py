@@ -63,12 +63,54 @@ def water_rayleigh(rindex):
 @dataclass
 class Material:
     """A medium: RINDEX (None: opaque), ABSLENGTH (m, None: no absorption), RAYLEIGH (m; None: Geant4's water
-    table for a material named Water, else no scattering). Tables are (energies eV, values) or constants."""  # noqa: D205
+    table for a material named Water, else no scattering). Tables are (energies eV, values) or constants.
+
+    Mie scattering (G4OpMieHG, src/lumen/rules/optics.py:357 mie_constants): ``mie`` the length MIEHG (m) with the
+    constants ``mie_forward`` (MIEHG_FORWARD), ``mie_backward`` (MIEHG_BACKWARD), ``mie_forward_ratio``
+    (MIEHG_FORWARD_RATIO). Wavelength shifting (G4OpWLS, optics.py:337 _wls_channel): ``wls`` the absorption length
+    WLSABSLENGTH (m), ``wls_spectrum`` the WLSCOMPONENT table (energies eV, intensities), ``wls_mean`` the mean
+    photons per absorbed one (WLSMEANNUMBERPHOTONS, 1 when absent), ``wls_tau`` WLSTIMECONSTANT (ns, 0 when absent),
+    ``wls_profile`` "delta" (Geant4's default) or "exponential".
+    """  # noqa: D205
 
     name: str
     rindex: object = None
     abslength: object = None
     rayleigh: object = None
+    mie: object = None
+    mie_forward: float = 0.0
+    mie_backward: float = 0.0
+    mie_forward_ratio: float | None = None
+    wls: object = None
+    wls_spectrum: object = None
+    wls_mean: float = 1.0
+    wls_tau: float = 0.0
+    wls_profile: str = "delta"
+
+    def __post_init__(self):
+        """Refuse what G4OpMieHG / G4OpWLS would abort on or the reference refuses (optics.py:337-380)."""
+        if self.mie is not None:
+            if self.mie_forward_ratio is None:
+                raise ValueError(f"{self.name}: MIEHG without MIEHG_FORWARD_RATIO (G4OpMieHG aborts at the first Mie "
+                                 "event)")  # fmt: skip
+            if not 0.0 <= self.mie_forward_ratio <= 1.0:
+                raise ValueError(f"{self.name}: MIEHG_FORWARD_RATIO {self.mie_forward_ratio} outside [0, 1]")
+            for g in (self.mie_forward, self.mie_backward):
+                if not abs(g) <= MIE_G_MAX:
+                    raise ValueError(f"{self.name}: a Mie asymmetry |g| above {MIE_G_MAX}")
+        if self.wls is not None:
+            if self.wls_spectrum is None:
+                raise ValueError(f"{self.name}: WLSABSLENGTH without WLSCOMPONENT (G4OpWLS absorbs and emits nothing)")
+            e, v = (np.asarray(x, np.float64) for x in self.wls_spectrum)
+            if np.any(v < 0) or not np.sum(0.5 * (v[1:] + v[:-1]) * np.diff(e)) > 0:
+                raise ValueError(f"{self.name}: WLSCOMPONENT needs a non-negative intensity with positive integral")
+            if self.wls_profile not in ("delta", "exponential"):
+                raise ValueError(f"{self.name}: wls_profile {self.wls_profile!r} is not 'delta' or 'exponential'")
+            if not (self.wls_mean >= 0.0 and self.wls_tau >= 0.0):
+                raise ValueError(f"{self.name}: WLSMEANNUMBERPHOTONS and WLSTIMECONSTANT must be >= 0")
+
+
+MIE_G_MAX = 0.999  # the largest |g| of a Mie lobe (src/lumen/rules/choices.py:99)
 
 
 @dataclass

@@ -48,6 +48,12 @@ def lib():
                                               ctypes.c_int64, A.c_f32p, A.c_i64p, A.c_f32p, ctypes.c_float, A.c_f32p,
                                               ctypes.c_int32]  # fmt: skip
         L.lumen_oracle_unified.argtypes = [A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_mie.argtypes = [ctypes.c_float] * 3 + [A.c_f32p, ctypes.c_uint32, ctypes.c_uint32,
+                                                               ctypes.c_int64, A.c_f32p, A.c_f32p]  # fmt: skip
+        L.lumen_oracle_mie_logpdf.argtypes = [ctypes.c_float] * 3 + [A.c_f32p, A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_wls.argtypes = [A.c_f32p, A.c_f32p, A.c_f32p, ctypes.c_int32, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_float, ctypes.c_int32, ctypes.c_float, ctypes.c_uint32,
+                                       ctypes.c_uint32, ctypes.c_int64, A.c_f32p]  # fmt: skip
         L.lumen_oracle_group_index.argtypes = [A.c_f32p, A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_source_rows.argtypes = [P(A.LumenSource), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
                                                ctypes.c_int64, A.c_f32p, A.c_i32p]
@@ -242,3 +248,29 @@ def source_rows(source, key, n, first_id=0, samples=None):
     ev = np.zeros(n, np.int32)
     lib().lumen_oracle_source_rows(ctypes.byref(ss), key[0], key[1], first_id, n, A.fptr(out_f), A.iptr(ev))
     return out_f, ev
+
+
+def mie(gf, gb, ratio, wi, n, key=(0, 9)):
+    """n G4OpMieHG draws about wi: (directions (n, 3), their log densities (n,))."""
+    wi = A.np_f32(wi)
+    out = np.zeros((n, 3), np.float32)
+    lp = np.zeros(n, np.float32)
+    assert lib().lumen_oracle_mie(gf, gb, ratio, A.fptr(wi), key[0], key[1], n, A.fptr(out), A.fptr(lp)) == 0
+    return out, lp
+
+
+def mie_logpdf(gf, gb, ratio, wi, wo):
+    """The Mie log density at directions wo (n, 3) about wi and its derivatives in (gf, gb, ratio): (n, 4)."""
+    wi, wo = A.np_f32(wi), A.np_f32(wo).reshape(-1, 3)
+    out = np.zeros((len(wo), 4), np.float32)
+    assert lib().lumen_oracle_mie_logpdf(gf, gb, ratio, A.fptr(wi), A.fptr(wo), len(wo), A.fptr(out)) == 0
+    return out
+
+
+def wls(energy, s_live, s_ref, lam_in, n, *, yield_live=1.0, yield_ref=1.0, tau=0.0, exponential=False, key=(0, 11)):
+    """n G4OpWLS emissions of photons absorbed at lam_in: (n, 4) wavelength, delay, weight, reference weight."""
+    e, sl, sr = A.np_f32(energy), A.np_f32(s_live), A.np_f32(s_ref)
+    out = np.zeros((n, 4), np.float32)
+    assert lib().lumen_oracle_wls(A.fptr(e), A.fptr(sl), A.fptr(sr), len(e), yield_live, yield_ref, tau,
+                                  int(exponential), lam_in, key[0], key[1], n, A.fptr(out)) == 0  # fmt: skip
+    return out

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "physics.h"
+#include "media.h"
 #include "rng.h"
 
 #define O_SOURCE_STREAM 0xFFFFFFFFu
@@ -58,21 +59,27 @@ typedef struct ODep {
 
 static inline float o_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0.0f; }
 
-/* tangents of a medium's rates in the gradient parameters: d(1/L)/dL = -1/L^2 where L's table moves */
-static inline void o_dmed(const ORun* R, int mi, float lam, const OMed* m, float* dmu_abs, float* dmu_c) {
+/* tangents of a medium's rates in the gradient parameters: d(1/L)/dL = -1/L^2 where L's table moves; per channel
+   (dch, p-major) and their sum (dmu_c) */
+static inline void o_dmed(const ORun* R, int mi, float lam, const OMed* m, float* dmu_abs, float* dmu_c, float* dch) {
   const int32_t* mr = R->S.D->med_i + (size_t)mi * LUMEN_MED_I;
   float E = O_HC / lam;
   for (int p = 0; p < R->P; ++p) {
     dmu_abs[p] = 0.0f;
-    dmu_c[p] = 0.0f;
     if (mr[LUMEN_MI_ABS] >= 0 && mr[LUMEN_MI_ABS] == R->gt[p]) {
       float L = o_tab(R->S.D, R->live, mr[LUMEN_MI_ABS], E, 0);
       dmu_abs[p] = L >= O_FLT_TINY ? -(m->mu_abs * m->mu_abs) : 0.0f;
     }
-    if (mr[LUMEN_MI_RAY] >= 0 && mr[LUMEN_MI_RAY] == R->gt[p]) {
-      float L = o_tab(R->S.D, R->live, mr[LUMEN_MI_RAY], E, 0);
-      dmu_c[p] = L >= O_FLT_TINY ? -(m->mu_c * m->mu_c) : 0.0f;
+    for (int c = 0; c < LUMEN_N_CHANNEL; ++c) {
+      int t = o_channel_tab(mr, c);
+      float v = 0.0f;
+      if (t >= 0 && t == R->gt[p]) {
+        float L = o_tab(R->S.D, R->live, t, E, 0);
+        v = L >= O_FLT_TINY ? -(m->ch[c] * m->ch[c]) : 0.0f;
+      }
+      dch[p * LUMEN_N_CHANNEL + c] = v;
     }
+    dmu_c[p] = (dch[p * LUMEN_N_CHANNEL] + dch[p * LUMEN_N_CHANNEL + 1]) + dch[p * LUMEN_N_CHANNEL + 2];
   }
 }
 
@@ -98,8 +105,8 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   int mi = D->cls_medium[ph->cls];
   OMed ml = o_medium_at(D, R->live, ph->lam, mi);
   OMed mr = R->shared ? ml : o_medium_at(D, R->ref, ph->lam, mi);
-  float dmu_abs[O_MAXG], dmu_c[O_MAXG];
-  o_dmed(R, mi, ph->lam, &ml, dmu_abs, dmu_c);
+  float dmu_abs[O_MAXG], dmu_c[O_MAXG], dch[O_MAXG * LUMEN_N_CHANNEL];
+  o_dmed(R, mi, ph->lam, &ml, dmu_abs, dmu_c, dch);
   float mu_r = mr.mu_c;
   float s = -o_log(o_uniform(vkey, 0)) / o_max(mu_r, O_FLOOR32);
   /* _query (step.py:260; TrackedGeometry.query, tracked.py:86) */
@@ -169,36 +176,81 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   float fates0, fates1, fates2, wr;
   if (scatter) { /* _bulk (step.py:397) */
     int next_cls = s < q.t_pass0 ? q.cls_start : (s > q.t_pass1 ? cb : o_cls(S, q.vol_at));
-    float mu_c_r = mr.mu_c;
-    /* one channel: choose(mu_c_r, u) is 0 whenever the rate is positive */
+    /* the channel drawn from the reference rates (estimator.choose, uniform 1); with one channel present it is that
+       channel whatever the uniform */
+    int n_ch = (mr.ch[0] > 0.0f) + (mr.ch[1] > 0.0f) + (mr.ch[2] > 0.0f);
+    int cs = n_ch > 1 ? o_choose(mr.ch, LUMEN_N_CHANNEL, o_uniform(vkey, 1)) : (mr.ch[0] > 0.0f ? 0 : (mr.ch[1] > 0.0f ? 1 : 2));
+    cs = cs < 0 ? 0 : cs;
+    float mu_c_r = mr.ch[cs];
     float e_r = o_exp(-mu_r * s), e_l = o_exp(-mu * s);
     float path_r = mu_c_r * e_r;
-    float w_path = o_ratio(ml.mu_c * e_l, path_r);
+    float w_path = o_ratio(ml.ch[cs] * e_l, path_r);
     float att = o_exp(-ml.mu_abs * s);
     float w = w_path * att;
     float w_r = o_ratio(path_r, path_r) * o_exp(-mr.mu_abs * s);
     for (int a = 0; a < 3; ++a) nx_x[a] = ph->x[a] + s * ph->d[a];
     float rl3[3] = {o_uniform(vkey, 3), o_uniform(vkey, 4), o_uniform(vkey, 5)};
-    o_rayleigh_sample(er0, ei0, rl3, nx_d);
-    for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
-    o_project(nx_er, nx_ei, nx_d);
+    float rlw = 1.0f, y_w = 1.0f, y_r = 1.0f, delay = 0.0f;
+    float dlob[O_MAXG], dyld[O_MAXG];
+    for (int p = 0; p < P; ++p) { dlob[p] = 0.0f; dyld[p] = 0.0f; }
+    const int32_t* mrec = D->med_i + (size_t)mi * LUMEN_MED_I;
+    float Eph = O_HC / ph->lam;
+    if (cs == 0) { /* Rayleigh: the polarised dipole draw, the state projected (phase.py:57) */
+      o_rayleigh_sample(er0, ei0, rl3, nx_d);
+      for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+      o_project(nx_er, nx_ei, nx_d);
+    } else if (cs == 1) { /* Mie (G4OpMieHG): drawn at the reference constants, weighted live / reference */
+      int tg[3] = {mrec[LUMEN_MI_MIE_GF], mrec[LUMEN_MI_MIE_GB], mrec[LUMEN_MI_MIE_R]};
+      float pl[3], pr[3];
+      for (int k = 0; k < 3; ++k) {
+        pl[k] = o_tab(D, R->live, tg[k], Eph, 0);
+        pr[k] = R->shared ? pl[k] : o_tab(D, R->ref, tg[k], Eph, 0);
+      }
+      o_mie_sample(pr[0], pr[1], pr[2], ph->d, rl3, nx_d);
+      float dl[3];
+      float lp = o_mie_logpdf(pl[0], pl[1], pl[2], ph->d, nx_d, dl);
+      if (!R->shared) rlw = o_exp(lp - o_mie_logpdf(pr[0], pr[1], pr[2], ph->d, nx_d, 0));
+      for (int p = 0; p < P; ++p)
+        for (int k = 0; k < 3; ++k)
+          if (tg[k] == R->gt[p]) dlob[p] = dlob[p] + dl[k];
+      for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
+      o_project(nx_er, nx_ei, nx_d);
+    } else { /* WLS (G4OpWLS): isotropic, unpolarised, re-emitted at the record's wavelength after its delay */
+      o_isotropic(ph->d, rl3[0], rl3[1], nx_d);
+      for (int a = 0; a < 3; ++a) { nx_er[a] = 0.0f; nx_ei[a] = 0.0f; }
+      int ts = mrec[LUMEN_MI_WLS_SPEC], ty = mrec[LUMEN_MI_WLS_YIELD], tt = mrec[LUMEN_MI_WLS_TAU];
+      const float* pl_ = R->live + D->tab[2 * ts];
+      const float* pr_ = R->ref + D->tab[2 * ts];
+      int ks = D->tab[2 * ts + 1];
+      float yl = o_tab(D, R->live, ty, Eph, 0), yr = R->shared ? yl : o_tab(D, R->ref, ty, Eph, 0);
+      float tau = o_tab(D, R->live, tt, Eph, 0);
+      OEmit em = o_wls_emit(pl_, pl_ + ks, ks, pr_, pr_ + ks, ks, yl, yr, tau, mrec[LUMEN_MI_WLS_PROFILE] == 1, ph->lam,
+                            o_uniform(vkey, 7), o_uniform(vkey, 8));
+      y_w = em.w;
+      y_r = em.w_r;
+      delay = em.delay;
+      nx_lam = em.lam;
+      for (int p = 0; p < P; ++p)
+        if (ty == R->gt[p]) dyld[p] = em.dyield;
+    }
     float w_at = ph->w * w_path;
-    fates0 = w_at * att * 1.0f;
-    fates1 = w_at * (1.0f - att * 1.0f);
+    fates0 = w_at * att * y_w;
+    fates1 = w_at * (1.0f - att * y_w);
     fates2 = 0.0f;
-    nx_w = ph->w * w * 1.0f * 1.0f;
+    nx_w = ph->w * w * rlw * y_w;
     for (int p = 0; p < P; ++p) {
-      float dwp = (dmu_c[p] * e_l + ml.mu_c * (-(dmu_c[p] * s) * e_l)) / path_r;
+      float dwp = (dch[p * LUMEN_N_CHANNEL + cs] * e_l + ml.ch[cs] * (-(dmu_c[p] * s) * e_l)) / path_r;
       if (!(path_r != 0.0f)) dwp = 0.0f;
       float datt = -(dmu_abs[p] * s) * att;
       float dwf = dwp * att + w_path * datt;
-      nx_dw[p] = ph->dw[p] * w + ph->w * dwf;
+      if (cs == 0) nx_dw[p] = ph->dw[p] * w + ph->w * dwf;
+      else nx_dw[p] = (ph->dw[p] * w + ph->w * dwf) * rlw * y_w + ph->w * w * rlw * (dlob[p] * y_w + dyld[p]);
     }
     nx_cls = next_cls;
     nx_ok = 1;
-    nx_dtime = s / v_g;
+    nx_dtime = s / v_g + delay;
     for (int a = 0; a < 3; ++a) nx_sn[a] = q.normal[a];
-    wr = ph->wr * w_r * 1.0f;
+    wr = ph->wr * w_r * y_r;
   } else { /* _surface_event (step.py:362) */
     float pl = le.probs[os_], pp = p_prop[os_];
     float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
@@ -669,6 +721,42 @@ int32_t lumen_oracle_facet_path(float sigma, const float* wi, uint32_t k0, uint3
     nc += c;
   }
   *capped = nc;
+  return 0;
+}
+
+/* n Mie draws (G4OpMieHG) about wi at constants (gf, gb, ratio), each from three uniforms of its own key: out the
+   directions (n * 3), lp their log densities (n) */
+int32_t lumen_oracle_mie(float gf, float gb, float ratio, const float* wi, uint32_t k0, uint32_t k1, int64_t n,
+                         float* out, float* lp) {
+  OKey key = {k0, k1};
+#pragma omp parallel for
+  for (int64_t i = 0; i < n; ++i) {
+    OKey k = o_fold_in(key, (uint32_t)i);
+    float r[3] = {o_uniform(k, 0), o_uniform(k, 1), o_uniform(k, 2)};
+    o_mie_sample(gf, gb, ratio, wi, r, out + 3 * i);
+    lp[i] = o_mie_logpdf(gf, gb, ratio, wi, out + 3 * i, 0);
+  }
+  return 0;
+}
+/* The Mie log density at n given directions (n * 3) about wi, with its derivatives in (gf, gb, ratio): out n * 4 */
+int32_t lumen_oracle_mie_logpdf(float gf, float gb, float ratio, const float* wi, const float* wo, int64_t n,
+                                float* out) {
+  for (int64_t i = 0; i < n; ++i) out[4 * i] = o_mie_logpdf(gf, gb, ratio, wi, wo + 3 * i, out + 4 * i + 1);
+  return 0;
+}
+/* n G4OpWLS emissions of photons absorbed at lam_in from the spectra (live e, s; reference er, sr: k knots each),
+   each from two uniforms of its own key: out n * 4 (wavelength, delay, weight, reference weight) */
+int32_t lumen_oracle_wls(const float* e, const float* sl, const float* sr, int32_t k, float yield_l, float yield_r,
+                         float tau, int32_t exponential, float lam_in, uint32_t k0, uint32_t k1, int64_t n,
+                         float* out) {
+  OKey key = {k0, k1};
+#pragma omp parallel for
+  for (int64_t i = 0; i < n; ++i) {
+    OKey kk = o_fold_in(key, (uint32_t)i);
+    OEmit em = o_wls_emit(e, sl, k, e, sr, k, yield_l, yield_r, tau, exponential, lam_in, o_uniform(kk, 0),
+                          o_uniform(kk, 1));
+    out[4 * i] = em.lam; out[4 * i + 1] = em.delay; out[4 * i + 2] = em.w; out[4 * i + 3] = em.w_r;
+  }
   return 0;
 }
 

@@ -84,19 +84,28 @@ static inline float o_group_index(const LumenSceneDesc* D, const float* pool, in
   return 1.0f / f;
 }
 
-typedef struct OMed { float n, ng, mu_abs, mu_c; } OMed;
+typedef struct OMed { float n, ng, mu_abs, mu_c, ch[LUMEN_N_CHANNEL]; } OMed;
 
-/* (n, n_g, mu_abs, mu) of medium mi at lam (medium.py:27); one bulk channel (Rayleigh) at most */
+/* the length table of channel c (Rayleigh, Mie, WLS: bulk.py:21 CHANNEL_ORDER) of a medium record, -1 if absent */
+static inline int o_channel_tab(const int32_t* m, int c) {
+  return m[c == 0 ? LUMEN_MI_RAY : (c == 1 ? LUMEN_MI_MIE : LUMEN_MI_WLS)];
+}
+
+/* (n, n_g, mu_abs, the channels' rates and their sum) of medium mi at lam (medium.py:27, bulk.py:88 evaluate) */
 static inline OMed o_medium_at(const LumenSceneDesc* D, const float* pool, float lam, int mi) {
   const int32_t* m = D->med_i + (size_t)mi * LUMEN_MED_I;
   float E = O_HC / lam;
-  OMed r = {1.0f, 1.0f, 0.0f, 0.0f};
+  OMed r = {1.0f, 1.0f, 0.0f, 0.0f, {0.0f, 0.0f, 0.0f}};
   if (m[LUMEN_MI_INDEX] >= 0) {
     r.n = o_tab(D, pool, m[LUMEN_MI_INDEX], E, 0);
     r.ng = o_group_index(D, pool, m[LUMEN_MI_INDEX], E);
   }
   if (m[LUMEN_MI_ABS] >= 0) r.mu_abs = o_rate(o_tab(D, pool, m[LUMEN_MI_ABS], E, 0));
-  if (m[LUMEN_MI_RAY] >= 0) r.mu_c = o_rate(o_tab(D, pool, m[LUMEN_MI_RAY], E, 0));
+  for (int c = 0; c < LUMEN_N_CHANNEL; ++c) {
+    int t = o_channel_tab(m, c);
+    if (t >= 0) r.ch[c] = o_rate(o_tab(D, pool, t, E, 0));
+  }
+  r.mu_c = (r.ch[0] + r.ch[1]) + r.ch[2];
   return r;
 }
 static inline float o_index_at(const LumenSceneDesc* D, const float* pool, float lam, int mi) {

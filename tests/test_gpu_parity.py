@@ -258,3 +258,32 @@ def test_sensor_reach_bound_changes_no_photon(which, tank, lar, facet_lar, built
         src = sources.Scintillation(position=[(0.3, 0.2, -0.4)], lam=128.0, tau=(6.0, 1500.0), fraction=0.25)
         bad, gi, oi, gf, of = _records_match(det, src, 1 << 11, controls=c)
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+@pytest.fixture(scope="module")
+def scint():
+    return detectors.scintillator_cube()
+
+
+def test_scintillator_cube_photons_bit_exact(scint, built):
+    """Rayleigh, Mie (G4OpMieHG) and WLS (G4OpWLS) channels in one medium: every photon's record is the checker's."""
+    src = sources.Point(position=(0.1, 0.0, 0.05), n_photons=1.0, lam_range=(330.0, 480.0))
+    bad, gi, oi, gf, of = _records_match(scint, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+@pytest.mark.parametrize("variant", [0, 3])
+def test_scintillator_cube_tallies_gradients_and_reference(variant, scint, built):
+    src = sources.Point(position=(0.1, 0.0, 0.05), n_photons=1.0, lam_range=(330.0, 480.0))
+    names = ["media/LAB/mie", "media/LAB/wls", "media/LAB/mie_g_forward", "media/LAB/wls_yield", "media/LAB/rayleigh"]
+    c = A.controls(grad_tabs=[scint.params_index[k] for k in names], variant=variant)
+    T, O = _tallies(scint, src, 1 << 14, controls=c, n_bins=50)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
+    np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+    live = scint.pool_with({"media/LAB/mie_g_forward": 0.85, "media/LAB/wls_yield": 0.8,
+                            "media/LAB/mie_forward_ratio": 0.75})  # fmt: skip
+    T, O = _tallies(scint, src, 1 << 13, controls=A.controls(variant=variant), pools=(live, scint.pool))
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
