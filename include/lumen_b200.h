@@ -64,7 +64,8 @@ enum { LUMEN_PLANE_F = 4 };
 /* Program op: op (0 push leaf arg, 1 union, 2 intersection, 3 subtraction), arg */
 enum { LUMEN_PROG_I = 2 };
 
-/* Surface table: row ints of LUMEN_ROW_I: model (0 reflect, 1 dielectric, 2 complex index), normal, glisur,
+/* Surface table: row ints of LUMEN_ROW_I: model (0 reflect, 1 dielectric, 2 complex index), normal, glisur (the
+   GLOSSY lobe: 0 the unified facet path, 1 GLISUR's on a metal, 2 GLISUR's reflecting or refracting facets),
    far_opaque, per_normal, then one table index per column (LUMEN_COL_*) read at the photon energy */
 enum { LUMEN_COL_R = 0, LUMEN_COL_T, LUMEN_COL_EFF, LUMEN_COL_PSPIKE, LUMEN_COL_PLOBE, LUMEN_COL_PBACK,
        LUMEN_COL_SIGMA, LUMEN_COL_POLISH, LUMEN_COL_NR, LUMEN_COL_NK, LUMEN_N_COL };
@@ -220,8 +221,8 @@ const char* lumen_b200_last_error(void);
 
 /* Upload a detector to the current CUDA device; replaces the reference's Navigator.operands / pack.pack device put
    (src/lumen/geometry/navigate.py:140, src/lumen/api.py:842). Unified rows with sigma_alpha > 0 draw Geant4's facet
-   path (src/lumen/surfaces/facets.py:372), weighted by its path density from desc->unified; a GLISUR row is refused
-   (LUMEN_ERR_SCENE). */
+   path (src/lumen/surfaces/facets.py:372), weighted by its path density from desc->unified; GLISUR rows (polish < 1)
+   draw GLISUR's facet paths (facets.py:341-548). */
 int32_t lumen_b200_scene_create(const LumenSceneDesc* desc, LumenScene** out);
 /* Replace the live and reference parameter pools (host, n_pool floats each; ref may be null: the live pool): the
    reference's packed params and reference (src/lumen/transport/step.py:129 `operands`). */

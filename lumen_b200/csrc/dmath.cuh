@@ -162,6 +162,15 @@ L_DEV float l_atan2(float y, float x) {
   return y < 0.0f ? -a : a;
 }
 
+// the cube root: exp(log|x| / 3) and one Newton step on y^3 = |x|
+L_DEV float l_cbrt(float x) {
+  if (x == 0.0f) return 0.0f;
+  float a = x < 0.0f ? -x : x;
+  float y = l_exp(l_log(a) * 0.333333343267440796f);
+  y = y - (y * y * y - a) / (3.0f * y * y);
+  return x < 0.0f ? -y : y;
+}
+
 L_DEV float l_erfinv(float x) {
   float w = -l_log((1.0f - x) * (1.0f + x));
   float p;

@@ -10,19 +10,6 @@ namespace lb {
 #define D_DEFENSIVE 0.01f  // the defensive mixture's share (src/lumen/rules/choices.py:113)
 #define D_WLS_TRIES 100.0f  // G4OpWLS's redraws of an energy below the absorbed one (spectra.py:22)
 
-// log(1 + x) and exp(y) - 1 by Kahan's corrections (Goldberg 1991, Theorem 4)
-L_DEV float l_log1p(float x) {
-  float u = 1.0f + x;
-  if (u == 1.0f) return x;
-  return l_log(u) * x / (u - 1.0f);
-}
-L_DEV float l_expm1(float y) {
-  float u = l_exp(y);
-  if (u == 1.0f) return y;
-  float um = u - 1.0f;
-  if (um == -1.0f) return -1.0f;
-  return um * y / l_log(u);
-}
 
 // ------------------------------------------------------------------------------------------------- the Mie lobe
 L_DEV void d_mie_hg_cos(float g, float r, float* cm, float* cp) {

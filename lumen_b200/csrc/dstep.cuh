@@ -263,7 +263,8 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
     float w_if = ph.w * rr * att_if * r_live;
     float dirn[3], wi[3] = {ph.d[0], ph.d[1], ph.d[2]};
-    float lobe_w = 1.0f, lobe_dls = 0.0f;
+    float lobe_w = 1.0f, lobe_dls = 0.0f, lobe_wd = 1.0f, lobe_sign = 1.0f;  // GLISUR: r = 1 - polish
+    int lobe_far = 0;
     const float* nrm = q.normal;
     float eta = ml.n / n2l;
     float s_ax[3];
@@ -305,13 +306,25 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
       float h[3] = {dirn[0] - wi[0], dirn[1] - wi[1], dirn[2] - wi[2]};
       d_unit(h);
       d_mirror(nx_er, nx_ei, h);
-    } else if (os_ == GLOSSY) {  // the facet path drawn at the reference width, weighted live over reference
+    } else if (os_ == GLOSSY) {
       int capped = 0;
-      float lp = 0.0f, lr = 0.0f;
-      int dens = !R.shared || P > 0;
-      d_facet_path(re.sigma, wi, nrm, uniform(vkey, 3), uniform(vkey, 4), uniform(vkey, 5), dirn, nx_er, nx_ei,
-                   &capped, dens ? S.uni : nullptr, le.sigma, !R.shared, P > 0, &lp, &lr, &lobe_dls);
-      if (!R.shared) lobe_w = l_exp(lp - lr);
+      int gl = __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_GLISUR);
+      float u3 = uniform(vkey, 3), u4 = uniform(vkey, 4), u5 = uniform(vkey, 5);
+      if (gl == 0) {  // the unified facet path drawn at the reference width, weighted live over reference
+        float lp = 0.0f, lr = 0.0f;
+        int dens = !R.shared || P > 0;
+        d_facet_path(re.sigma, wi, nrm, u3, u4, u5, dirn, nx_er, nx_ei, &capped, dens ? S.uni : nullptr, le.sigma,
+                     !R.shared, P > 0, &lp, &lr, &lobe_dls);
+        if (!R.shared) lobe_w = l_exp(lp - lr);
+      } else if (gl == 1) {  // GLISUR metal: the cover at the reference width (1 - polish), exact over cover
+        lobe_w = d_glisur_metal_path(re.sigma, le.sigma, wi, nrm, u3, u4, u5, D_GLISUR_COVER, dirn, nx_er, nx_ei,
+                                     &capped, &lobe_wd, &lobe_dls);
+        lobe_sign = -1.0f;
+      } else {  // GLISUR dielectric: each facet reflects or refracts at the live indices, possibly ending beyond
+        lobe_w = d_glisur_dielectric_path(re.sigma, le.sigma, ml.n, n2l, wi, nrm, u3, u4, u5, D_GLISUR_COVER, dirn,
+                                          nx_er, nx_ei, &lobe_far, &capped, &lobe_wd, &lobe_dls);
+        lobe_sign = -1.0f;
+      }
     } else {
 #pragma unroll
       for (int a = 0; a < 3; ++a) dirn[a] = wi[a];
@@ -320,12 +333,12 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     for (int a = 0; a < 3; ++a) nx_d[a] = dirn[a];
     d_unit(nx_d);
     int far_side = (os_ == STRAIGHT || os_ == REFRACT);
-    int far_ = far_side && drawn;
+    int far_ = (far_side || lobe_far) && drawn;
     int ok = q.hit && drawn && row >= 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) nx_x[a] = ph.x[a] + q.t * ph.d[a];
     float r_o = drawn ? (p_prop[os_] != 0.0f ? re.probs[os_] / p_prop[os_] : 0.0f) : 0.0f;
-    wr = ph.wr * (reach_ref != 0.0f ? 1.0f : 0.0f) * att_r * r_o * 1.0f;
+    wr = ph.wr * (reach_ref != 0.0f ? 1.0f : 0.0f) * att_r * r_o * lobe_wd;
     float w_at = ph.w * rr;
     float s_cont = 0.0f;
 #pragma unroll
@@ -335,14 +348,15 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     fates2 = (q.hit && row >= 0) ? w_at * att_if * (1.0f - s_cont) : 0.0f;
     nx_w = w_if * lobe_w;
     if (G > 0) {
-      int t_sig = row >= 0 ? __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_COL + LUMEN_COL_SIGMA) : -1;
+      int t_sig = row >= 0 ? __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_COL +
+                                  (lobe_sign > 0.0f ? LUMEN_COL_SIGMA : LUMEN_COL_POLISH)) : -1;
       for (int p = 0; p < P; ++p) {
         float dpl = dprobs[p][os_];
         float dr_live = drawn ? (pp != 0.0f ? dpl / pp : 0.0f) : 0.0f;
         float drr = reach_ref != 0.0f ? d_reach[p] / reach_ref : 0.0f;
         float X = rr * att_if * r_live;
         float dX = drr * att_if * r_live + rr * d_att[p] * r_live + rr * att_if * dr_live;
-        float dsig = (t_sig >= 0 && t_sig == R.gt[p]) ? 1.0f : 0.0f;
+        float dsig = (t_sig >= 0 && t_sig == R.gt[p]) ? lobe_sign : 0.0f;
         nx_dw[p] = (dw[p] * X + ph.w * dX) * lobe_w + w_if * lobe_w * (lobe_dls * dsig);
       }
     }

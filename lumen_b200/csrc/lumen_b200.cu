@@ -572,8 +572,10 @@ static int check_desc(const LumenSceneDesc* d) {
     const int32_t* ri = d->row_i + r * LUMEN_ROW_I;
     for (int c = 0; c < LUMEN_N_COL; ++c)
       if (ri[LUMEN_RI_COL + c] < 0 || ri[LUMEN_RI_COL + c] >= d->n_tab) return set_err(LUMEN_ERR_ARG, "scene_create: a column table is out of range");
-    if (ri[LUMEN_RI_GLISUR]) return set_err(LUMEN_ERR_SCENE, "scene_create: the GLISUR facet path is not built");
-    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && !d->unified)
+    if (ri[LUMEN_RI_GLISUR] < 0 || ri[LUMEN_RI_GLISUR] > 2)
+      return set_err(LUMEN_ERR_ARG, "scene_create: a row's glisur flag is not 0 (unified), 1 (GLISUR metal) or 2 "
+                                    "(GLISUR dielectric)");
+    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && !ri[LUMEN_RI_GLISUR] && !d->unified)
       return set_err(LUMEN_ERR_ARG, "scene_create: a unified facet row needs the unified tables (desc->unified)");
   }
   if (d->comp) {  // the sensor reach arrays
@@ -949,7 +951,8 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   }
   for (int r = 0; r < d->n_row; ++r) {
     const int32_t* ri = d->row_i + r * LUMEN_ROW_I;
-    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL]) sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
+    if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && !ri[LUMEN_RI_GLISUR])
+      sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
   }
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
   for (int m = 0; m < d->n_med; ++m) {

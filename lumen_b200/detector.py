@@ -105,7 +105,7 @@ class Detector:
     def draws_facets(self) -> bool:
         """Whether a surface row draws the unified facet lobe (its density reads the unified tables)."""
         r = self.arrays["row_i"].reshape(-1, 16)
-        return bool(((r[:, 0] == 0) & (r[:, 1] == 0)).any())
+        return bool(((r[:, 0] == 0) & (r[:, 1] == 0) & (r[:, 2] == 0)).any())
 
 
 def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None) -> Detector:

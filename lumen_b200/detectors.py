@@ -68,6 +68,33 @@ def scintillator_cube(mie=2.0, wls=1.0, rayleigh=5.0, profile="exponential") -> 
                    sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def glisur_tank(polish_wall=0.8, polish_block=0.7) -> D.Detector:
+    """Return the tutorial tank with GLISUR ground surfaces: the walls a GLISUR metal (R 0.7, polish ``polish_wall``)
+    and an acrylic block (n 1.49, 30 x 30 x 20 cm) inside behind GLISUR ground dielectric borders both ways (polish
+    ``polish_block``: facets that reflect or refract with Fresnel's shares)."""  # noqa: D205
+    water = O.Material("Water", rindex=([1.5, 2.5, 3.5, 5.0], [1.332, 1.336, 1.345, 1.366]), abslength=30.0,
+                       rayleigh=20.0)  # fmt: skip
+    acrylic = O.Material("Acrylic", rindex=1.49, abslength=5.0)
+    cathode = O.Material("Photocathode")
+    pmt = G.Volume("PMT", G.Tube(rmax=50 * MM, dz=10 * MM), "Photocathode")
+    tank = G.Volume("TankLV", G.Box(0.5, 0.5, 0.5), "Water")
+    block = G.Volume("Block", G.Box(0.15, 0.15, 0.1), "Acrylic")
+    tank.place(block, (0.0, 0.0, -0.2), name="Block")
+    places = [((0, 0, -480), None), ((0, 0, 480), None), ((-480, 0, 0), ("y", 90)), ((480, 0, 0), ("y", 90)),
+              ((0, -480, 0), ("x", 90)), ((0, 480, 0), ("x", 90)), ((-250, 0, -480), None), ((250, 0, -480), None)]
+    for i, (p, r) in enumerate(places):
+        rot = None if r is None else G.gdml_rotation(**{r[0]: r[1]})
+        tank.place(pmt, np.asarray(p, float) * MM, rot, name=f"PMT_{i}", copy=i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", model="glisur", polish=polish_wall,
+                            reflectivity=0.7)  # fmt: skip
+    into = O.OpticalSurface("BlockIn", "dielectric_dielectric", "ground", model="glisur", polish=polish_block)
+    out = O.OpticalSurface("BlockOut", "dielectric_dielectric", "ground", model="glisur", polish=polish_block)
+    borders = [("TankLV", f"PMT_{i}", surf) for i in range(8)] + [("TankLV", "Block", into), ("Block", "TankLV", out)]
+    return D.build(tank, {"Water": water, "Acrylic": acrylic, "Photocathode": cathode}, borders=borders,
+                   skins={"TankLV": wall}, sensors={"pmt": "PMT"})  # fmt: skip
+
+
 def _grid_tank(n_pmt, radius, half_h, r_pmt, inset):
     """Return (positions, inward axes) of n_pmt PMTs on a regular barrel and end-cap grid."""
     area = 2 * math.pi * radius * 2 * half_h + 2 * math.pi * radius**2

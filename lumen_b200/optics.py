@@ -151,8 +151,15 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
     """Return the row of a Geant4 surface (types.py:445-493 types, :557 no_detection)."""
     eff = surf.efficiency if (sensor and surf.efficiency is not None) else 0.0
     if surf.type == "dielectric_dielectric":
-        if surf.finish != "polished":
-            raise NotImplementedError("dielectric_dielectric ground (GLISUR / unified facets) is not built")
+        if surf.finish != "polished" and surf.model == "glisur" and surf.polish < 1.0:
+            # GLISUR_DIELECTRIC (types.py:463): the cuts, then below R the GLISUR facet path that reflects or refracts
+            # at each facet, between R and R + T straight on
+            cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
+                    "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff, "p_spike": 0.0,
+                    "p_lobe": 1.0, "p_back": 0.0, "polish": float(surf.polish)}  # fmt: skip
+            return Row(MODEL_REFLECT, glisur=2, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+        if surf.finish != "polished" and not (surf.model == "glisur" and surf.polish >= 1.0):
+            raise NotImplementedError("dielectric_dielectric ground with the unified model is not built")
         cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
                 "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff}  # fmt: skip
         return Row(MODEL_DIELECTRIC, far_opaque=int(far_opaque), cols=cols, name=surf.name)
@@ -160,7 +167,9 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
     R = 1.0 if surf.reflectivity is None else surf.reflectivity
     cols = {"R": R, "eff": eff, "T": 0.0 if surf.transmittance is None else surf.transmittance}
     if surf.model == "glisur" and surf.finish != "polished" and surf.polish < 1.0:
-        raise NotImplementedError("the GLISUR facet path (dielectric_metal, glisur, ground, polish < 1) is not built")
+        # GLISUR_METAL (types.py:459): R into the GLISUR facet path of radius 1 - polish
+        cols.update({"p_spike": 0.0, "p_lobe": 1.0, "p_back": 0.0, "polish": float(surf.polish)})
+        return Row(MODEL_REFLECT, glisur=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
     if surf.finish == "polished" or surf.model == "glisur":
         cols["p_spike"] = 1.0  # polished, or GLISUR at polish 1: the mirror (types.py:573 SPECULAR_METAL)
         return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)

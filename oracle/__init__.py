@@ -48,6 +48,9 @@ def lib():
                                               ctypes.c_int64, A.c_f32p, A.c_i64p, A.c_f32p, ctypes.c_float, A.c_f32p,
                                               ctypes.c_int32]  # fmt: skip
         L.lumen_oracle_unified.argtypes = [A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_glisur.argtypes = [ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, A.c_f32p,
+                                          A.c_f32p, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
+                                          A.c_f32p, A.c_i64p]  # fmt: skip
         L.lumen_oracle_mie.argtypes = [ctypes.c_float] * 3 + [A.c_f32p, ctypes.c_uint32, ctypes.c_uint32,
                                                                ctypes.c_int64, A.c_f32p, A.c_f32p]  # fmt: skip
         L.lumen_oracle_mie_logpdf.argtypes = [ctypes.c_float] * 3 + [A.c_f32p, A.c_f32p, ctypes.c_int64, A.c_f32p]
@@ -274,3 +277,15 @@ def wls(energy, s_live, s_ref, lam_in, n, *, yield_live=1.0, yield_ref=1.0, tau=
     assert lib().lumen_oracle_wls(A.fptr(e), A.fptr(sl), A.fptr(sr), len(e), yield_live, yield_ref, tau,
                                   int(exponential), lam_in, key[0], key[1], n, A.fptr(out)) == 0  # fmt: skip
     return out
+
+
+def glisur(kind, polish, wi, er, *, n1=1.0, n2=1.0, e=0.0, key=(0, 13)):
+    """GLISUR facet paths off a flat surface (normal +z): kind "metal" or "dielectric", one per row of er (n, 3) (the
+    photons' linear states); e the cover's share (0: Geant4's draw). Returns (last directions (n, 3), far (n,),
+    path weights (n,), d/dr of the log weights (n,), paths that hit a loop bound)."""  # noqa: D205, D209
+    wi, er = A.np_f32(wi), A.np_f32(er).reshape(-1, 3)
+    out = np.zeros((len(er), 6), np.float32)
+    capped = np.zeros(1, np.int64)
+    assert lib().lumen_oracle_glisur(1 if kind == "metal" else 2, polish, n1, n2, A.fptr(wi), A.fptr(er), e, key[0],
+                                     key[1], len(er), A.fptr(out), capped.ctypes.data_as(A.c_i64p)) == 0  # fmt: skip
+    return out[:, :3], out[:, 3] > 0.5, out[:, 4], out[:, 5], int(capped[0])

@@ -210,4 +210,19 @@ static inline float o_erfinv(float x) {
   return p * x;
 }
 
+/* log(1 + x) and exp(y) - 1 by Kahan's corrections (D. Goldberg, "What every computer scientist should know about
+   floating-point arithmetic", 1991, Theorem 4): exact where the plain forms cancel */
+static inline float o_log1p(float x) {
+  float u = 1.0f + x;
+  if (u == 1.0f) return x;
+  return o_log(u) * x / (u - 1.0f);
+}
+static inline float o_expm1(float y) {
+  float u = o_exp(y);
+  if (u == 1.0f) return y;
+  float um = u - 1.0f;
+  if (um == -1.0f) return -1.0f;
+  return um * y / o_log(u);
+}
+
 #endif

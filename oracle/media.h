@@ -12,20 +12,6 @@
 #define O_EPS32 1.1920928955078125e-7f
 #define O_WLS_TRIES 100.0f     /* G4OpWLS's redraws of an energy below the absorbed one (spectra.py:22) */
 
-/* log(1 + x) and exp(y) - 1 by Kahan's corrections (D. Goldberg, "What every computer scientist should know about
-   floating-point arithmetic", 1991, Theorem 4): exact where the plain forms cancel */
-static inline float o_log1p(float x) {
-  float u = 1.0f + x;
-  if (u == 1.0f) return x;
-  return o_log(u) * x / (u - 1.0f);
-}
-static inline float o_expm1(float y) {
-  float u = o_exp(y);
-  if (u == 1.0f) return y;
-  float um = u - 1.0f;
-  if (um == -1.0f) return -1.0f;
-  return um * y / o_log(u);
-}
 
 /* ----------------------------------------------------------------------------------------- the Mie lobe */
 /* (1 - mu, 1 + mu) of G4OpMieHG's Henyey-Greenstein draw at asymmetry g (phase.py:113 mie_hg_cos: the inverse CDF in

@@ -258,7 +258,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
     float dirn[3], wi[3] = {ph->d[0], ph->d[1], ph->d[2]};
     const float* nrm = q.normal;
     float eta = ml.n / n2l;
-    float out_w = 1.0f, out_wd = 1.0f, lobe_dls = 0.0f;
+    float out_w = 1.0f, out_wd = 1.0f, lobe_dls = 0.0f, lobe_sign = 1.0f; /* GLISUR: r = 1 - polish */
     int out_far = 0;
     float s_ax[3];
     o_s_axis(wi, nrm, s_ax);
@@ -302,16 +302,28 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
         o_mirror(nx_er, nx_ei, h);
         break;
       }
-      case O_GLOSSY: { /* the facet path drawn at the reference width, weighted by its path density live over
-                          reference (surface_event.py:106 _facet_path_branch): 1 without a reference, whose
-                          derivative is the path's score in sigma */
+      case O_GLOSSY: {
         float rl3[3] = {o_uniform(vkey, 3), o_uniform(vkey, 4), o_uniform(vkey, 5)};
         int capped = 0;
-        float lp = 0.0f, lr = 0.0f;
-        int dens = !R->shared || P > 0;
-        o_facet_path(re.sigma, wi, nrm, rl3, dirn, nx_er, nx_ei, &capped, dens ? D->unified : 0, le.sigma,
-                     !R->shared, &lp, &lr, P > 0 ? &lobe_dls : 0);
-        if (!R->shared) out_w = o_exp(lp - lr);
+        int gl = D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_GLISUR];
+        if (gl == 0) { /* the unified facet path drawn at the reference width, weighted by its path density live over
+                          reference (surface_event.py:106 _facet_path_branch): 1 without a reference, whose
+                          derivative is the path's score in sigma */
+          float lp = 0.0f, lr = 0.0f;
+          int dens = !R->shared || P > 0;
+          o_facet_path(re.sigma, wi, nrm, rl3, dirn, nx_er, nx_ei, &capped, dens ? D->unified : 0, le.sigma,
+                       !R->shared, &lp, &lr, P > 0 ? &lobe_dls : 0);
+          if (!R->shared) out_w = o_exp(lp - lr);
+        } else if (gl == 1) { /* GLISUR metal: drawn from the cover at the reference width (1 - polish), weighted by
+                                 the exact path density over the cover's; the drawn weight is the cover's support */
+          out_w = o_glisur_metal_path(re.sigma, le.sigma, wi, nrm, rl3, O_GLISUR_COVER, dirn, nx_er, nx_ei, &capped,
+                                      &out_wd, &lobe_dls);
+          lobe_sign = -1.0f;
+        } else { /* GLISUR dielectric: each facet reflects or refracts at the live indices, possibly ending beyond */
+          out_w = o_glisur_dielectric_path(re.sigma, le.sigma, ml.n, n2l, wi, nrm, rl3, O_GLISUR_COVER, dirn, nx_er,
+                                           nx_ei, &out_far, &capped, &out_wd, &lobe_dls);
+          lobe_sign = -1.0f;
+        }
         break;
       }
       default:
@@ -339,7 +351,8 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
       float drr = reach_ref != 0.0f ? d_reach[p] / reach_ref : 0.0f;
       float X = rr * att_if * r_live;
       float dX = drr * att_if * r_live + rr * d_att[p] * r_live + rr * att_if * dr_live;
-      nx_dw[p] = (ph->dw[p] * X + ph->w * dX) * out_w + w_if * out_w * (lobe_dls * dcol[p * LUMEN_N_COL + LUMEN_COL_SIGMA]);
+      float dwid = lobe_sign > 0.0f ? dcol[p * LUMEN_N_COL + LUMEN_COL_SIGMA] : -dcol[p * LUMEN_N_COL + LUMEN_COL_POLISH];
+      nx_dw[p] = (ph->dw[p] * X + ph->w * dX) * out_w + w_if * out_w * (lobe_dls * dwid);
     }
     nx_cls = far_ ? ca : cb;
     nx_ok = ok;
@@ -757,6 +770,34 @@ int32_t lumen_oracle_wls(const float* e, const float* sl, const float* sr, int32
                           o_uniform(kk, 1));
     out[4 * i] = em.lam; out[4 * i + 1] = em.delay; out[4 * i + 2] = em.w; out[4 * i + 3] = em.w_r;
   }
+  return 0;
+}
+
+/* n GLISUR facet paths off a flat surface (normal +z): kind 1 metal, 2 dielectric (indices n1 incident, n2 far), at
+   r = 1 - polish, each from three uniforms of its own key, with the photon's Jones vector er (n * 3, real linear
+   states); e the cover's share (0: Geant4's draw). out n * 6: the last direction, the far flag, the path weight,
+   d/dr of the log weight */
+int32_t lumen_oracle_glisur(int32_t kind, float polish, float n1, float n2, const float* wi, const float* er_in,
+                            float e, uint32_t k0, uint32_t k1, int64_t n, float* out, int64_t* capped) {
+  const float up[3] = {0.0f, 0.0f, 1.0f};
+  OKey key = {k0, k1};
+  int64_t nc = 0;
+  float r = 1.0f - polish;
+#pragma omp parallel for reduction(+ : nc)
+  for (int64_t i = 0; i < n; ++i) {
+    OKey k = o_fold_in(key, (uint32_t)i);
+    float rr[3] = {o_uniform(k, 0), o_uniform(k, 1), o_uniform(k, 2)};
+    float er[3] = {er_in[3 * i], er_in[3 * i + 1], er_in[3 * i + 2]}, ei[3] = {0.0f, 0.0f, 0.0f};
+    int c = 0, far = 0;
+    float on = 0.0f, dl = 0.0f, w;
+    if (kind == 1) w = o_glisur_metal_path(r, r, wi, up, rr, e, out + 6 * i, er, ei, &c, &on, &dl);
+    else w = o_glisur_dielectric_path(r, r, n1, n2, wi, up, rr, e, out + 6 * i, er, ei, &far, &c, &on, &dl);
+    out[6 * i + 3] = (float)far;
+    out[6 * i + 4] = w;
+    out[6 * i + 5] = dl;
+    nc += c;
+  }
+  *capped = nc;
   return 0;
 }
 

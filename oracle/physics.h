@@ -22,6 +22,7 @@
 #define O_ZERO_STATE 0.5f
 #define O_TWO_PI 6.28318530717958647692f
 #define O_PI 3.14159265358979323846f
+#define O_LOG_2_3 (-0.405465108108164381978f) /* log(2/3) */
 
 enum { O_STRAIGHT = 0, O_REFRACT, O_SPECULAR, O_BACKSCATTER, O_GLOSSY, O_DIFFUSE, O_N_OUT };
 
@@ -601,6 +602,260 @@ static inline void o_facet_path(float sigma, const float* wi, const float* n, co
     if (L[2] >= 0.0f) return;
     if (k + 1 == O_FACET_PATH) *capped = 1;
   }
+}
+
+/* ---------------------------------------------------------------------------------------- GLISUR facets */
+#define O_SHELL_STREAM 0xFFFFFFFFu     /* the vertex key's fold choosing the facet's cover part (rng.py:31) */
+#define O_FRESNEL_STREAM 0xFFFFFFFEu   /* a dielectric facet's reflect-or-refract uniform (rng.py:34) */
+#define O_GLISUR_COVER 0.01f           /* the defensive share of the shell (src/lumen/rules/choices.py:113) */
+#define O_INDEX_MATCH (128.0f * 1.1920928955078125e-7f) /* indices one at a facet (choices.py:98) */
+#define O_PI 3.14159265358979323846f
+
+/* a GLISUR facet normal (local frame): M = e_z + r s, s uniform in the unit ball (on its sphere when the facet's
+   one cover draw says so), redrawn until V . M > 0 (facets.py:341 glisur_facet) */
+static inline void o_glisur_facet(float r, const float* V, OKey key, float e, float* m, int* capped) {
+  int shell = e > 0.0f && o_uniform(o_fold_in(key, O_SHELL_STREAM), 0) < e;
+  float M[3] = {0.0f, 0.0f, 1.0f};
+  int ok = 0;
+  for (uint32_t t = 0; t < O_FACET_REDRAWS && !ok; ++t) {
+    OKey kt = o_fold_in(key, t);
+    float u0 = o_uniform(kt, 0), u1 = o_uniform(kt, 1), u2 = o_uniform(kt, 2);
+    float z = 1.0f - 2.0f * u1;
+    float s2 = 1.0f - z * z;
+    float sxy = s2 > 0.0f ? sqrtf(s2) : 0.0f;
+    float sp, cp;
+    o_sincos2pi(u2, &sp, &cp);
+    float rad = shell ? 1.0f : o_cbrt(u0);
+    float C[3] = {0.0f + r * rad * (sxy * cp), 0.0f + r * rad * (sxy * sp), 1.0f + r * rad * z};
+    if (o_dot(V, C) > 0.0f) { M[0] = C[0]; M[1] = C[1]; M[2] = C[2]; ok = 1; }
+  }
+  if (!ok) *capped = 1;
+  float inv = 1.0f / sqrtf(o_dot(M, M));
+  m[0] = M[0] * inv; m[1] = M[1] * inv; m[2] = M[2] * inv;
+}
+/* the log volume of the ball B(n, r) on the photon's side of V . M = 0 (h = V . n; facets.py:226), and d/dr */
+static inline float o_glisur_log_volume(float r, float h, float* dr) {
+  float d = o_max(r - h, 0.0f);
+  float v = 4.0f / 3.0f * O_PI * r * r * r - O_PI * d * d * (2.0f * r + h) / 3.0f;
+  if (dr) {
+    float dd = r - h > 0.0f ? 1.0f : 0.0f;
+    *dr = (4.0f * O_PI * r * r - O_PI * (2.0f * d * dd * (2.0f * r + h) + 2.0f * d * d) / 3.0f) / v;
+  }
+  return o_log(v);
+}
+/* the log area of the sphere |M - n| = r on the photon's side (facets.py:268) */
+static inline float o_glisur_log_area(float r, float h) {
+  return o_log(h >= r ? 4.0f * O_PI * r * r : 2.0f * O_PI * r * (r + o_min(h, r)));
+}
+/* (log p_m, on the support) of the facet direction M (any length) at width r (facets.py:232), d/dr when asked */
+static inline float o_glisur_log_density(float r, const float* V, const float* M, int* ok, float* dr) {
+  float m2 = o_dot(M, M);
+  float inv = 1.0f / sqrtf(m2);
+  float c = M[2] * inv;
+  float s2 = (M[0] * M[0] + M[1] * M[1]) / m2;
+  float q2 = r * r - s2;
+  *ok = q2 > 0.0f && c > 0.0f && o_dot(V, M) > 0.0f;
+  float q2s = *ok ? q2 : r * r;
+  float cs = *ok ? c : 1.0f;
+  float dv;
+  float lp = O_LOG_2_3 + 0.5f * o_log(q2s) + o_log(3.0f * cs * cs + q2s) -
+             o_glisur_log_volume(r, V[2], dr ? &dv : 0);
+  if (dr) *dr = *ok ? r / q2s + 2.0f * r / (3.0f * cs * cs + q2s) - dv : 0.0f;
+  return lp;
+}
+/* log(exp a + exp b), the larger first */
+static inline float o_logaddexp(float a, float b) {
+  float mx = o_max(a, b), mn = o_min(a, b);
+  return mx + o_log1p(o_exp(mn - mx));
+}
+/* (log of (1 - e) p_m + e p_shell, on the support) for the facet direction M (facets.py:273) */
+static inline float o_glisur_log_proposal(float r, const float* V, const float* M, float e, int* ok) {
+  float lp = o_glisur_log_density(r, V, M, ok, 0);
+  float m2 = o_dot(M, M);
+  float c = *ok ? M[2] * (1.0f / sqrtf(m2)) : 1.0f;
+  float q2 = *ok ? r * r - (M[0] * M[0] + M[1] * M[1]) / m2 : r * r;
+  float ls = o_log(2.0f * r) + o_log(c * c + q2) - 0.5f * o_log(q2) - o_glisur_log_area(r, V[2]);
+  return o_logaddexp(o_log1p(-e) + lp, o_log(e) + ls);
+}
+/* one GLISUR metal facet reflection's log density (exact, cover 0) or its cover's, LOG_TINY off the support
+   (facets.py:283, :295), with d/dr of the exact one */
+static inline float o_glisur_logpdf(float r, const float* w0, const float* n, const float* w1, float e, float* dr) {
+  float mw[3] = {-w0[0], -w0[1], -w0[2]};
+  float V[3], W[3];
+  o_to_local(mw, n, V);
+  o_to_local(w1, n, W);
+  float H[3] = {V[0] + W[0], V[1] + W[1], V[2] + W[2]};
+  int good = H[2] > 0.0f && o_dot(V, H) > 0.0f;
+  if (dr) *dr = 0.0f;
+  if (!good) return O_LOG_TINY;
+  float vh = o_dot(V, H) * (1.0f / sqrtf(o_dot(H, H)));
+  int ok;
+  float lq = e > 0.0f ? o_glisur_log_proposal(r, V, H, e, &ok) : o_glisur_log_density(r, V, H, &ok, dr);
+  if (!ok) {
+    if (dr) *dr = 0.0f;
+    return O_LOG_TINY;
+  }
+  return lq - o_log(4.0f * vh);
+}
+/* the GLISUR metal facet path drawn from the cover at the reference width r_ref, weighted by its exact path density
+   at r_live over the cover's (surface_event.py:106 with the covered lobe); returns the weight, *on the drawn weight
+   (the path on the cover's support), *dlr d/dr_live of the log weight */
+static inline float o_glisur_metal_path(float r_ref, float r_live, const float* wi, const float* n, const float* rand,
+                                        float e, float* wo, float* er, float* ei, int* capped, float* on_,
+                                        float* dlr) {
+  OKey key = o_seed_key(rand[0], rand[1], rand[2]);
+  float mwi[3] = {-wi[0], -wi[1], -wi[2]};
+  float V[3];
+  o_to_local(mwi, n, V);
+  float w[3] = {wi[0], wi[1], wi[2]};
+  float lp = 0.0f, lr = 0.0f, dl = 0.0f;
+  for (uint32_t k = 0; k < O_FACET_PATH; ++k) {
+    float m[3];
+    o_glisur_facet(r_ref, V, o_fold_in(key, k), e, m, capped);
+    float vm = o_dot(V, m);
+    float L[3] = {2.0f * vm * m[0] - V[0], 2.0f * vm * m[1] - V[1], 2.0f * vm * m[2] - V[2]};
+    o_to_world(L, n, wo);
+    float d;
+    lp = lp + o_glisur_logpdf(r_live, w, n, wo, 0.0f, &d);
+    dl = dl + d;
+    lr = lr + o_glisur_logpdf(r_ref, w, n, wo, e, 0);
+    float h[3] = {wo[0] - w[0], wo[1] - w[1], wo[2] - w[2]};
+    o_unit(h);
+    o_mirror(er, ei, h);
+    w[0] = wo[0]; w[1] = wo[1]; w[2] = wo[2];
+    V[0] = -L[0]; V[1] = -L[1]; V[2] = -L[2];
+    if (L[2] >= 0.0f) break;
+    if (k + 1 == O_FACET_PATH) *capped = 1;
+  }
+  int on = lr > 0.5f * O_LOG_TINY;
+  *on_ = on ? 1.0f : 0.0f;
+  *dlr = on ? dl : 0.0f;
+  return on ? o_exp(lp - lr) : 0.0f;
+}
+
+/* ---- the GLISUR dielectric facet path (facets.py:487 _dielectric_path_of, :453 dielectric_event_logpdf) */
+static inline int o_matched(float na, float nb) { return fabsf(na - nb) <= O_INDEX_MATCH * o_max(na, nb); }
+/* (R, s axis, components, amplitudes) of the state going w0 onto the facet m from n_a into n_b (facets.py:443) */
+static inline float o_interface(const float* w0, const float* m, float na, float nb, const float* er, const float* ei,
+                                float* s_ax, Oc* es, Oc* ep, Oc* amps) {
+  o_s_axis(w0, m, s_ax);
+  o_components(er, ei, w0, s_ax, es, ep);
+  o_amplitudes(-o_dot(w0, m), na, oc(nb, 0.0f), amps);
+  float R = oc_abs2(amps[0]) * oc_abs2(*es) + oc_abs2(amps[1]) * oc_abs2(*ep);
+  return R < 0.0f ? 0.0f : (R > 1.0f ? 1.0f : R);
+}
+/* Snell's refraction of w at facing normal m (outcomes.py:36 refract), the mirror under total reflection */
+static inline void o_refract_dir(const float* w, const float* m, float eta, float* wo) {
+  float cos_i = -o_dot(w, m);
+  float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+  if (sin2_t >= 1.0f) {
+    for (int a = 0; a < 3; ++a) wo[a] = w[a] + 2.0f * cos_i * m[a];
+    return;
+  }
+  float ct2 = 1.0f - sin2_t;
+  float cos_t = ct2 > 0.0f ? sqrtf(ct2) : 0.0f;
+  float k = eta * cos_i - cos_t;
+  for (int a = 0; a < 3; ++a) wo[a] = eta * w[a] + k * m[a];
+  o_unit(wo);
+}
+/* one dielectric facet event's log density (exact or the cover's), the Jones vector after it, d/dr (exact) */
+static inline float o_dielectric_event_lp(float r, float n1, float n2, const float* n, const float* w0,
+                                          const float* w1, int refracted, float side, float e, const float* er,
+                                          const float* ei, float* er1, float* ei1, float* dr) {
+  float na = side > 0.0f ? n1 : n2, nb = side > 0.0f ? n2 : n1;
+  float N[3] = {side * n[0], side * n[1], side * n[2]};
+  int matched = o_matched(na, nb);
+  float m[3];
+  if (refracted && !matched) {
+    float sg = nb - na > 0.0f ? 1.0f : (nb - na < 0.0f ? -1.0f : 0.0f);
+    float u[3] = {na * w0[0] - nb * w1[0], na * w0[1] - nb * w1[1], na * w0[2] - nb * w1[2]};
+    o_unit(u);
+    m[0] = u[0] * sg; m[1] = u[1] * sg; m[2] = u[2] * sg;
+  } else {
+    m[0] = w1[0] - w0[0]; m[1] = w1[1] - w0[1]; m[2] = w1[2] - w0[2];
+    o_unit(m);
+  }
+  float cos1 = -o_dot(w0, m), cos2 = -o_dot(w1, m);
+  float mw[3] = {-w0[0], -w0[1], -w0[2]}, Vl[3], Ml[3];
+  o_to_local(mw, N, Vl);
+  o_to_local(m, N, Ml);
+  int ok;
+  float lpm = e > 0.0f ? o_glisur_log_proposal(r, Vl, Ml, e, &ok) : o_glisur_log_density(r, Vl, Ml, &ok, dr);
+  float s_ax[3];
+  Oc es, ep, amps[4];
+  float R = o_interface(w0, m, na, nb, er, ei, s_ax, &es, &ep, amps);
+  ok = ok && cos1 > 0.0f && (refracted ? cos2 > 0.0f : cos2 < 0.0f);
+  float c1 = ok ? cos1 : 1.0f, c2 = ok ? fabsf(cos2) : 1.0f;
+  float lrf = lpm + o_log(o_max(R, O_FLOOR32)) - o_log(4.0f * c1);
+  float gap = (ok && !matched) ? fabsf(nb * c2 - na * c1) : 1.0f;
+  float lt = lpm + o_log(o_max(1.0f - R, O_FLOOR32)) + 2.0f * o_log(nb) + o_log(c2) - 2.0f * o_log(gap);
+  float lp = refracted ? (matched ? 0.0f : lt) : lrf;
+  ok = ok || (refracted && matched);
+  int straight = refracted && matched;
+  if (straight) {
+    for (int a = 0; a < 3; ++a) { er1[a] = er[a]; ei1[a] = ei[a]; }
+  } else {
+    o_recombine(es, ep, refracted ? amps[2] : amps[0], refracted ? amps[3] : amps[1], s_ax, w1, er1, ei1);
+  }
+  if (dr && (!ok || straight)) *dr = 0.0f;
+  return ok ? lp : O_LOG_TINY;
+}
+/* the GLISUR dielectric facet path drawn from the cover at the reference width, at the live indices (n1 the incident
+   medium's, n2 the far one's) and state; weighted by its exact path density at r_live over the cover's at r_ref,
+   its Jones vector the live one (surface_event.py:137 _dielectric_path_branch); *far: it ends beyond the surface */
+static inline float o_glisur_dielectric_path(float r_ref, float r_live, float n1, float n2, const float* wi,
+                                             const float* n, const float* rand, float e, float* wo, float* er,
+                                             float* ei, int* far_, int* capped, float* on_, float* dlr) {
+  OKey key = o_seed_key(rand[0], rand[1], rand[2]);
+  float w[3] = {wi[0], wi[1], wi[2]}, wv[3] = {wi[0], wi[1], wi[2]};
+  float side = 1.0f;
+  float er_d[3] = {er[0], er[1], er[2]}, ei_d[3] = {ei[0], ei[1], ei[2]}; /* the draw's state */
+  float er_r[3] = {er[0], er[1], er[2]}, ei_r[3] = {ei[0], ei[1], ei[2]}; /* the cover's density's state */
+  float lp = 0.0f, lr = 0.0f, dl = 0.0f;
+  int far = 0;
+  for (uint32_t k = 0; k < O_FACET_PATH; ++k) {
+    float N[3] = {side * n[0], side * n[1], side * n[2]};
+    float na = side > 0.0f ? n1 : n2, nb = side > 0.0f ? n2 : n1;
+    OKey kk = o_fold_in(key, k);
+    float mw[3] = {-w[0], -w[1], -w[2]}, Vl[3];
+    o_to_local(mw, N, Vl);
+    if (!(Vl[2] > 0.0f)) { Vl[0] = 0.0f; Vl[1] = 0.0f; Vl[2] = 1.0f; }
+    float ml[3], m[3];
+    o_glisur_facet(r_ref, Vl, kk, e, ml, capped);
+    o_to_world(ml, N, m);
+    float s_ax[3];
+    Oc es, ep, amps[4];
+    float R = o_interface(w, m, na, nb, er_d, ei_d, s_ax, &es, &ep, amps);
+    int refr = o_uniform(o_fold_in(kk, O_FRESNEL_STREAM), 0) >= R;
+    float w1[3];
+    if (refr) {
+      if (o_matched(na, nb)) { w1[0] = w[0]; w1[1] = w[1]; w1[2] = w[2]; }
+      else o_refract_dir(w, m, na / nb, w1);
+    } else {
+      float wm = o_dot(w, m);
+      for (int a = 0; a < 3; ++a) w1[a] = w[a] - 2.0f * wm * m[a];
+    }
+    float er1[3], ei1[3];
+    o_recombine(es, ep, refr ? amps[2] : amps[0], refr ? amps[3] : amps[1], s_ax, w1, er1, ei1);
+    float dot = o_dot(w1, N);
+    int end = refr ? dot <= 0.0f : dot >= 0.0f;
+    /* the visit: the live density with the live state, the cover's with its own state */
+    float d, erl[3], eil[3], err2[3], eir2[3];
+    lp = lp + o_dielectric_event_lp(r_live, n1, n2, n, wv, w1, refr, side, 0.0f, er, ei, erl, eil, &d);
+    dl = dl + d;
+    lr = lr + o_dielectric_event_lp(r_ref, n1, n2, n, wv, w1, refr, side, e, er_r, ei_r, err2, eir2, 0);
+    for (int a = 0; a < 3; ++a) { er[a] = erl[a]; ei[a] = eil[a]; er_r[a] = err2[a]; ei_r[a] = eir2[a]; }
+    for (int a = 0; a < 3; ++a) { er_d[a] = er1[a]; ei_d[a] = ei1[a]; w[a] = w1[a]; wv[a] = w1[a]; wo[a] = w1[a]; }
+    if (refr && !end) side = -side;
+    far = far ^ refr;
+    if (end) break;
+    if (k + 1 == O_FACET_PATH) *capped = 1;
+  }
+  *far_ = far;
+  int on = lr > 0.5f * O_LOG_TINY;
+  *on_ = on ? 1.0f : 0.0f;
+  *dlr = on ? dl : 0.0f;
+  return on ? o_exp(lp - lr) : 0.0f;
 }
 
 /* the cumulative draw (estimator.py:62 choose): index drawn from q with one uniform, -1 if q is all 0 */

@@ -287,3 +287,31 @@ def test_scintillator_cube_tallies_gradients_and_reference(variant, scint, built
     T, O = _tallies(scint, src, 1 << 13, controls=A.controls(variant=variant), pools=(live, scint.pool))
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
+
+
+@pytest.fixture(scope="module")
+def glisur():
+    return detectors.glisur_tank()
+
+
+def test_glisur_tank_photons_bit_exact(glisur, built):
+    """GLISUR ground surfaces: a metal wall (cover-drawn facet paths) and a dielectric block (facets that reflect or
+    refract, paths that end beyond the surface): every photon's record is the checker's."""
+    src = sources.Point(position=(0.1, 0.0, 0.05), n_photons=1.0, lam=400.0)
+    bad, gi, oi, gf, of = _records_match(glisur, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+@pytest.mark.parametrize("variant", [0, 3])
+def test_glisur_tank_tallies_gradients_and_reference(variant, glisur, built):
+    src = sources.Point(position=(0.1, 0.0, 0.05), n_photons=1.0, lam=400.0)
+    names = ["surfaces/Wall/polish", "surfaces/BlockIn/polish", "surfaces/BlockOut/polish", "surfaces/Wall/R"]
+    c = A.controls(grad_tabs=[glisur.params_index[k] for k in names], variant=variant)
+    T, O = _tallies(glisur, src, 1 << 14, controls=c, n_bins=50)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+    live = glisur.pool_with({"surfaces/Wall/polish": 0.82, "surfaces/BlockIn/polish": 0.72})
+    T, O = _tallies(glisur, src, 1 << 13, controls=A.controls(variant=variant), pools=(live, glisur.pool))
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
