@@ -832,7 +832,7 @@ L_DEV Query d_query(const DScene& S, const float* o, const float* d, int vol, fl
 // surface, starts inside its component's box, its free path s ends before the box's exit T, and the segment [0, T]
 // meets no sensor box, every crossing it can deposit at lies beyond s, so the query may stop at s plus the
 // navigator's own look-ahead ((GRAZE K_ON + 2) bands): the same arithmetic for every round that starts before s
-L_DEV float d_reach_bound(const DScene& S, const float* x, const float* d, int vol, int srf, float s, float t_max) {
+L_CALL float d_reach_bound(const DScene& S, const float* x, const float* d, int vol, int srf, float s, float t_max) {
   if (!S.comp || srf >= 0 || vol < 0 || vol > S.n) return t_max;
   int c = __ldg(S.comp + vol);
   if (c < 0) return t_max;

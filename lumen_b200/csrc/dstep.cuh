@@ -82,6 +82,38 @@ L_DEV Query d_step_query(const Run& R, const Photon& ph, const Pre& pr) {
   return d_query(R.S, ph.x, ph.d, ph.vol, tm, ph.srf, ph.sn, pr.s);
 }
 
+// The GLOSSY outcome's facet path by the row's lobe (surface_event.py:106 _facet_path_branch, :137
+// _dielectric_path_branch): the unified path drawn at the reference width and weighted live over reference, or GLISUR's
+// metal or dielectric path drawn from the cover at the reference width (1 - polish) and weighted exact over cover.
+// Out of line: a detector without glossy rows carries none of it in the step's registers.
+struct Glossy {
+  float d[3];
+  float w, wd, dls, sign;
+  int far;
+};
+L_CALL void d_glossy(const Run& R, int row, float sig_r, float sig_l, float n1, float n2, const float* wi,
+                     const float* nrm, Key vkey, int want_d, float* er, float* ei, Glossy& g) {
+  const DScene& S = R.S;
+  int capped = 0;
+  int gl = __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_GLISUR);
+  float u3 = uniform(vkey, 3), u4 = uniform(vkey, 4), u5 = uniform(vkey, 5);
+  g.w = 1.0f; g.wd = 1.0f; g.dls = 0.0f; g.sign = 1.0f; g.far = 0;
+  if (gl == 0) {
+    float lp = 0.0f, lr = 0.0f;
+    int dens = !R.shared || want_d;
+    d_facet_path(sig_r, wi, nrm, u3, u4, u5, g.d, er, ei, &capped, dens ? S.uni : nullptr, sig_l, !R.shared, want_d,
+                 &lp, &lr, &g.dls);
+    if (!R.shared) g.w = l_exp(lp - lr);
+  } else if (gl == 1) {
+    g.w = d_glisur_metal_path(sig_r, sig_l, wi, nrm, u3, u4, u5, D_GLISUR_COVER, g.d, er, ei, &capped, &g.wd, &g.dls);
+    g.sign = -1.0f;
+  } else {
+    g.w = d_glisur_dielectric_path(sig_r, sig_l, n1, n2, wi, nrm, u3, u4, u5, D_GLISUR_COVER, g.d, er, ei, &g.far,
+                                   &capped, &g.wd, &g.dls);
+    g.sign = -1.0f;
+  }
+}
+
 // the step after its query (step.py:516 step: the crossing, the event, the deposit, the roulette)
 template <int G>
 L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Query& q, Dep& dep, float* dq) {
@@ -203,12 +235,19 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     // the channel drawn from the reference rates (estimator.choose, uniform 1); with one channel present it is that
     // channel whatever the uniform
     float chl[LUMEN_N_CHANNEL], chr_[LUMEN_N_CHANNEL];
-    d_channel_rates(S, R.live, ph.lam, mi, chl);
-    if (R.shared) {
-#pragma unroll
-      for (int c = 0; c < LUMEN_N_CHANNEL; ++c) chr_[c] = chl[c];
+    const int32_t* mrec = S.med_i + (size_t)mi * LUMEN_MED_I;
+    if (__ldg(mrec + LUMEN_MI_MIE) < 0 && __ldg(mrec + LUMEN_MI_WLS) < 0) {
+      // Rayleigh alone: the summed rate is the Rayleigh rate itself (plus exact zeros)
+      chl[0] = ml.mu_c; chl[1] = 0.0f; chl[2] = 0.0f;
+      chr_[0] = mr.mu_c; chr_[1] = 0.0f; chr_[2] = 0.0f;
     } else {
-      d_channel_rates(S, R.ref, ph.lam, mi, chr_);
+      d_channel_rates(S, R.live, ph.lam, mi, chl);
+      if (R.shared) {
+#pragma unroll
+        for (int c = 0; c < LUMEN_N_CHANNEL; ++c) chr_[c] = chl[c];
+      } else {
+        d_channel_rates(S, R.ref, ph.lam, mi, chr_);
+      }
     }
     int n_ch = (chr_[0] > 0.0f) + (chr_[1] > 0.0f) + (chr_[2] > 0.0f);
     int cs = chr_[0] > 0.0f ? 0 : (chr_[1] > 0.0f ? 1 : 2);
@@ -307,24 +346,11 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
       d_unit(h);
       d_mirror(nx_er, nx_ei, h);
     } else if (os_ == GLOSSY) {
-      int capped = 0;
-      int gl = __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_GLISUR);
-      float u3 = uniform(vkey, 3), u4 = uniform(vkey, 4), u5 = uniform(vkey, 5);
-      if (gl == 0) {  // the unified facet path drawn at the reference width, weighted live over reference
-        float lp = 0.0f, lr = 0.0f;
-        int dens = !R.shared || P > 0;
-        d_facet_path(re.sigma, wi, nrm, u3, u4, u5, dirn, nx_er, nx_ei, &capped, dens ? S.uni : nullptr, le.sigma,
-                     !R.shared, P > 0, &lp, &lr, &lobe_dls);
-        if (!R.shared) lobe_w = l_exp(lp - lr);
-      } else if (gl == 1) {  // GLISUR metal: the cover at the reference width (1 - polish), exact over cover
-        lobe_w = d_glisur_metal_path(re.sigma, le.sigma, wi, nrm, u3, u4, u5, D_GLISUR_COVER, dirn, nx_er, nx_ei,
-                                     &capped, &lobe_wd, &lobe_dls);
-        lobe_sign = -1.0f;
-      } else {  // GLISUR dielectric: each facet reflects or refracts at the live indices, possibly ending beyond
-        lobe_w = d_glisur_dielectric_path(re.sigma, le.sigma, ml.n, n2l, wi, nrm, u3, u4, u5, D_GLISUR_COVER, dirn,
-                                          nx_er, nx_ei, &lobe_far, &capped, &lobe_wd, &lobe_dls);
-        lobe_sign = -1.0f;
-      }
+      Glossy gy;
+      d_glossy(R, row, re.sigma, le.sigma, ml.n, n2l, wi, nrm, vkey, P > 0, nx_er, nx_ei, gy);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) dirn[a] = gy.d[a];
+      lobe_w = gy.w; lobe_wd = gy.wd; lobe_dls = gy.dls; lobe_sign = gy.sign; lobe_far = gy.far;
     } else {
 #pragma unroll
       for (int a = 0; a < 3; ++a) dirn[a] = wi[a];
