@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 4
+#define LUMEN_B200_ABI_VERSION 5
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -104,6 +104,11 @@ enum { LUMEN_N_CHANNEL = 3 };  /* bulk channels: Rayleigh, Mie, WLS */
 #define LUMEN_UNI_DY 0.08664339756999316368     /* log(2) / 8 */
 #define LUMEN_UNI_WORDS (4 * LUMEN_UNI_NX * LUMEN_UNI_NY + 2 * LUMEN_UNI_NY)
 
+/* the diffusion jump's grid records */
+enum { LUMEN_JUMP_F = 4, LUMEN_JUMP_I = 8 };
+#define LUMEN_JUMP_STEPS 65536 /* a walk's scatterings at most: any stopping time is exact in law (fastpath.py:5-10);
+                                  this one bounds a lane's loop */
+
 /* ------------------------------------------------------------------------------------------ the detector */
 typedef struct LumenSceneDesc {
   /* geometry (the navigator's arrays, src/lumen/geometry/navigator_build.py:51, csg_build.py:30) */
@@ -138,6 +143,14 @@ typedef struct LumenSceneDesc {
   const float* comp_box;     /* host, n_comp * 6: each component's padded box (lo, hi) */
   const float* fnode_f;      /* host, n_fnode * LUMEN_NODE_F: a depth-first tree over the padded sensor boxes */
   const int32_t* fnode_i;    /* host, n_fnode * LUMEN_NODE_I: skip (the node after the subtree), count (> 0: a leaf) */
+  /* the diffusion jump (src/lumen/transport/fastpath.py): one proven clearance grid per medium the jump can act in
+     (Rayleigh its only channel), used with LUMEN_F_JUMP. 0 / null: no grid. */
+  int32_t n_jump;
+  const float* jump_f;       /* host, n_jump * LUMEN_JUMP_F: the grid's origin (3, m) and spacing (m) */
+  const int32_t* jump_i;     /* host, n_jump * LUMEN_JUMP_I: medium, nodes per axis (3), first node in clear */
+  int64_t n_clear;
+  const float* clear;        /* host, n_clear: the grids' clearances (m) at their nodes, node (i, j, k) at
+                                first + (i * n1 + j) * n2 + k */
 } LumenSceneDesc;
 
 typedef struct LumenScene LumenScene; /* opaque: the device copy of a LumenSceneDesc */
@@ -173,8 +186,10 @@ typedef struct LumenSource {
 /* ------------------------------------------------------------------------------------------ the controls */
 enum { LUMEN_F_ASYNC = 1,   /* controls.flags: enqueue only (no host wait, no status read back: capturable in a
                                  CUDA graph); a step budget that ran out then shows in counts[LUMEN_C_ABORTED] */
-       LUMEN_F_REACH = 2 };  /* bound bulk steps' queries by the scene's sensor reach (exact: every tally is the same;
+       LUMEN_F_REACH = 2,    /* bound bulk steps' queries by the scene's sensor reach (exact: every tally is the same;
                                 off by default, a speed-up only where bulk steps are common and sensors far) */
+       LUMEN_F_JUMP = 4 };   /* the diffusion jump at bulk Rayleigh events (fastpath.py; lumen.simulate's default):
+                                the same estimator in law as the plain walk, not the same photons */
 enum { LUMEN_VARIANT_WAVEFRONT = 3, LUMEN_N_VARIANT = 4 };
 /* launch variants: the persistent photon loop at 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
    2 = 256 x 3 (85 registers); 3 = the wavefront: rounds of two kernels (the query; the rest of the step and the

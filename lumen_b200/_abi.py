@@ -26,6 +26,7 @@ N_HEALTH = 11
 N_COUNT = 6
 F_ASYNC = 1
 F_REACH = 2
+F_JUMP = 4
 N_VARIANT = 4
 VARIANT_WAVEFRONT = 3
 UNI_NX, UNI_NY = 257, 69
@@ -51,6 +52,8 @@ class LumenSceneDesc(ctypes.Structure):
         ("pool", c_f32p), ("unified", c_f32p),
         ("n_comp", ctypes.c_int32), ("n_fnode", ctypes.c_int32), ("comp", c_i32p), ("comp_box", c_f32p),
         ("fnode_f", c_f32p), ("fnode_i", c_i32p),
+        ("n_jump", ctypes.c_int32), ("jump_f", c_f32p), ("jump_i", c_i32p), ("n_clear", ctypes.c_int64),
+        ("clear", c_f32p),
     ]  # fmt: skip
 
 

@@ -98,7 +98,8 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
 
     ``params``: {parameter name: value} overriding the detector's values (``det.params()``); ``reference``: the
     values the draws are made at (default: ``params``). ``controls``: ``dict(roulette=0.01, max_distance=None,
-    max_vertices=2**22, variant=None)``; ``variant`` picks the launch (``LumenControls.variant``; default: the
+    max_vertices=2**22, variant=None, jump=True)``; ``jump`` the diffusion jump (on, as lumen.simulate's default: where a
+    medium and volume allow it; the same estimator in law as the plain walk); ``variant`` picks the launch (``LumenControls.variant``; default: the
     wavefront where derivatives are asked for, the persistent loop otherwise, the measured faster of the two on the
     tank workloads). ``chunk``: photons per launch (default: all in one launch). ``gradients``: parameter names
     whose derivatives of the arrivals are returned (forward tangents of the reweighting estimator along each path).
@@ -108,11 +109,12 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     live = det.pool_with(params)
     ref = None if reference is None else det.pool_with({**(params or {}), **reference})
     eng.set_pools(live, ref)
-    ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22, variant=None) | (controls or {})
+    ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22, variant=None, jump=True) | (controls or {})
     gnames = list(gradients)
     gt = [det.params_index[k] for k in gnames]
     variant = ctl["variant"] if ctl["variant"] is not None else (A.VARIANT_WAVEFRONT if gt else 0)
-    c = A.controls(ctl["max_distance"] or 0.0, ctl["roulette"], ctl["max_vertices"], gt, variant=variant)
+    flags = A.F_JUMP if ctl["jump"] else 0  # the diffusion jump on, as lumen.simulate (src/lumen/api.py:1157)
+    c = A.controls(ctl["max_distance"] or 0.0, ctl["roulette"], ctl["max_vertices"], gt, variant=variant, flags=flags)
     if isinstance(source, FromArrays):
         rows = source.rows()
         n = len(rows["x"])

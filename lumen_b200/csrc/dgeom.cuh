@@ -62,6 +62,10 @@ struct DScene {
   const float* __restrict__ fnode_f;
   const int32_t* __restrict__ fnode_i;
   int n_fnode;
+  const int32_t* __restrict__ med_jump;  // the diffusion jump: each medium's grid (-1 none; null: no grid at all)
+  const float* __restrict__ jump_f;
+  const int32_t* __restrict__ jump_i;
+  const float* __restrict__ clear;
 };
 
 L_DEV float d_dot(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }

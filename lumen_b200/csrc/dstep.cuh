@@ -23,7 +23,69 @@ struct Run {
   int P;
   int gt[LUMEN_MAX_GRAD];
   int reach_on;  // LUMEN_F_REACH: bulk steps' queries bounded by the sensor reach
+  int jump_on;   // LUMEN_F_JUMP: the diffusion jump at bulk Rayleigh events
 };
+
+// ------------------------------------------------------------------------------------------ the diffusion jump
+#define D_JUMP_STREAM 0x7A11u  // the vertex key's fold for the walk's own uniforms (rng.py:25)
+struct Jmp {
+  int ok, n;
+  float y[3], d[3], er[3], L;
+};
+// the walk at a bulk Rayleigh event inside the proven clear ball at xs (fastpath.py:174 diffuse): free paths at the
+// reference rate, the polarised Rayleigh draw and projection, until a flight leaves the ball (the photon put at the
+// crossing) or the budget ceil((c mu_r)^2) of scatterings (at most LUMEN_JUMP_STEPS) is spent
+L_CALL void d_diffuse(const DScene& S, int mi, const float* xs, const float* d0, const float* er0, const float* ei0,
+                      float mu_r, int alive, Key vkey, Jmp& J) {
+  J.ok = 0; J.n = 0; J.L = 0.0f;
+  for (int a = 0; a < 3; ++a) { J.y[a] = 0.0f; J.d[a] = d0[a]; J.er[a] = er0[a]; }
+  int g = __ldg(S.med_jump + mi);
+  if (g < 0) return;
+  const float* jf = S.jump_f + (size_t)g * LUMEN_JUMP_F;
+  const int32_t* ji = S.jump_i + (size_t)g * LUMEN_JUMP_I;
+  float h = __ldg(jf + 3);
+  int inside = 1, idx[3];
+  float node[3];
+  for (int a = 0; a < 3; ++a) {
+    float fi = (xs[a] - __ldg(jf + a)) / h;
+    int na = __ldg(ji + 1 + a);
+    inside = inside && fi > -0.5f && fi < (float)na - 0.5f;
+    int i = (int)floorf(fi + 0.5f);
+    i = i < 0 ? 0 : (i > na - 1 ? na - 1 : i);
+    idx[a] = i;
+    node[a] = __ldg(jf + a) + h * (float)i;
+  }
+  float dx[3] = {xs[0] - node[0], xs[1] - node[1], xs[2] - node[2]};
+  float c = __ldg(S.clear + __ldg(ji + 4) + ((int64_t)idx[0] * __ldg(ji + 2) + idx[1]) * __ldg(ji + 3) + idx[2]) -
+            sqrtf(d_dot(dx, dx));
+  int lin = ei0[0] == 0.0f && ei0[1] == 0.0f && ei0[2] == 0.0f;
+  if (!(inside && c > 0.0f && lin && alive && mu_r > 0.0f)) return;
+  J.ok = 1;
+  float cm = c * mu_r;
+  int budget = (int)ceilf(d_min(cm * cm, (float)LUMEN_JUMP_STEPS));
+  Key jkey = fold_in(vkey, D_JUMP_STREAM);
+  const float zero[3] = {0.0f, 0.0f, 0.0f};
+  int out = 0;
+  for (int j = 0; j < budget && !out; ++j) {
+    Key kj = fold_in(jkey, (uint32_t)j);
+    float u0 = uniform(kj, 0);
+    float s = -l_log(u0) / mu_r;
+    float by = d_dot(J.y, J.d);
+    float t = -by + sqrtf(d_max(by * by - (d_dot(J.y, J.y) - c * c), 0.0f));
+    out = s >= t;
+    float k[3];
+    d_rayleigh_sample(J.er, zero, uniform(kj, 1), uniform(kj, 2), uniform(kj, 3), k);
+    float e2[3] = {J.er[0], J.er[1], J.er[2]}, z2[3] = {0.0f, 0.0f, 0.0f};
+    d_project(e2, z2, k);
+    float st = out ? t : s;
+    for (int a = 0; a < 3; ++a) J.y[a] = J.y[a] + st * J.d[a];
+    J.L = J.L + st;
+    if (!out) {
+      for (int a = 0; a < 3; ++a) { J.d[a] = k[a]; J.er[a] = e2[a]; }
+      J.n += 1;
+    }
+  }
+}
 
 struct Photon {
   float x[3], d[3], t, lam, w, wr;
@@ -267,11 +329,20 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     for (int a = 0; a < 3; ++a) nx_x[a] = ph.x[a] + s * ph.d[a];
     float rlw = 1.0f, y_w = 1.0f, y_r = 1.0f, delay = 0.0f;
     Bulk2 b2;
+    Jmp J;
+    J.ok = 0;
     if (cs == 0) {  // Rayleigh: the polarised dipole draw, the state projected (phase.py:57)
       d_rayleigh_sample(er0, ei0, uniform(vkey, 3), uniform(vkey, 4), uniform(vkey, 5), nx_d);
 #pragma unroll
       for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
       d_project(nx_er, nx_ei, nx_d);
+      if (R.jump_on) {  // the diffusion jump (step.py:421)
+        d_diffuse(S, mi, nx_x, nx_d, nx_er, nx_ei, mu_r, ph.alive, vkey, J);
+        if (J.ok) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a) { nx_x[a] = nx_x[a] + J.y[a]; nx_d[a] = J.d[a]; nx_er[a] = J.er[a]; }
+        }
+      }
     } else {  // Mie (G4OpMieHG) or WLS (G4OpWLS)
       d_bulk_other(S, R.live, R.ref, R.shared, cs, mi, ph.lam, ph.d, er0, ei0, vkey, P, R.gt, b2);
 #pragma unroll
@@ -284,6 +355,14 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     fates1 = w_at * (1.0f - att * y_w);
     fates2 = 0.0f;
     nx_w = ph.w * w * rlw * y_w;
+    float wj = 1.0f;
+    if (J.ok) {  // the walk's likelihood ratio (fastpath.py:212): its absorption and its path, live over reference
+      float lr = l_log(d_max(mu, D_FLOOR32) / d_max(mu_r, D_FLOOR32));
+      wj = l_exp(-ml.mu_abs * J.L) * l_exp((float)J.n * lr - (mu - mu_r) * J.L);
+      fates1 = fates1 + fates0 * (1.0f - wj);
+      fates0 = fates0 * wj;
+      nx_w = nx_w * wj;
+    }
     if (G > 0)
       for (int p = 0; p < P; ++p) {
         float dwp = (dch[p][cs] * e_l + mu_c_l * (-(dmu_c[p] * s) * e_l)) / path_r;
@@ -292,11 +371,18 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
         float dwf = dwp * att + w_path * datt;
         if (cs == 0) nx_dw[p] = dw[p] * w + ph.w * dwf;
         else nx_dw[p] = (dw[p] * w + ph.w * dwf) * rlw * y_w + ph.w * w * rlw * (b2.dlob[p] * y_w + b2.dyld[p]);
+        if (J.ok) {
+          float dlr = mu > D_FLOOR32 ? dmu_c[p] / mu : 0.0f;
+          float dwj = wj * (-(dmu_abs[p] * J.L) + (float)J.n * dlr - dmu_c[p] * J.L);
+          nx_dw[p] = nx_dw[p] * wj + ph.w * w * dwj;
+        }
       }
     nx_cls = next_cls;
     nx_ok = 1;
     nx_dtime = s / v_g + delay;
+    if (J.ok) nx_dtime = nx_dtime + J.L / v_g;
     wr = ph.wr * w_r * y_r;
+    if (J.ok) wr = wr * l_exp(-mr.mu_abs * J.L);
   } else {
     float pl = le.probs[os_], pp = p_prop[os_];
     float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;

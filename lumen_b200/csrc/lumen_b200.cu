@@ -578,6 +578,17 @@ static int check_desc(const LumenSceneDesc* d) {
     if (ri[LUMEN_RI_MODEL] == 0 && !ri[LUMEN_RI_NORMAL] && !ri[LUMEN_RI_GLISUR] && !d->unified)
       return set_err(LUMEN_ERR_ARG, "scene_create: a unified facet row needs the unified tables (desc->unified)");
   }
+  if (d->n_jump > 0) {  // the diffusion jump's grids: a medium each, nodes inside the clearance array
+    if (!d->jump_f || !d->jump_i || !d->clear || d->n_clear <= 0)
+      return set_err(LUMEN_ERR_ARG, "scene_create: inconsistent diffusion jump arrays");
+    for (int g = 0; g < d->n_jump; ++g) {
+      const int32_t* ji = d->jump_i + (size_t)g * LUMEN_JUMP_I;
+      int64_t nn = (int64_t)ji[1] * ji[2] * ji[3];
+      if (ji[0] < 0 || ji[0] >= d->n_med || ji[1] < 1 || ji[2] < 1 || ji[3] < 1 || ji[4] < 0 || ji[4] + nn > d->n_clear ||
+          !(d->jump_f[(size_t)g * LUMEN_JUMP_F + 3] > 0.0f))
+        return set_err(LUMEN_ERR_ARG, "scene_create: a diffusion jump grid is out of range");
+    }
+  }
   if (d->comp) {  // the sensor reach arrays
     if (!d->comp_box || d->n_comp <= 0 || d->n_fnode < 0 || (d->n_fnode > 0 && (!d->fnode_f || !d->fnode_i)))
       return set_err(LUMEN_ERR_ARG, "scene_create: inconsistent sensor reach arrays");
@@ -625,6 +636,7 @@ static int fill_run(const LumenScene* sc, const LumenControls* c, Run& R) {
   R.P = c->n_grad;
   for (int p = 0; p < LUMEN_MAX_GRAD; ++p) R.gt[p] = p < c->n_grad ? c->grad_tab[p] : -1;
   R.reach_on = (c->flags & LUMEN_F_REACH) && sc->S.comp != nullptr;
+  R.jump_on = (c->flags & LUMEN_F_JUMP) && sc->S.med_jump != nullptr;
   return 0;
 }
 
@@ -943,6 +955,18 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
       UPLOAD(S.fnode_i, d->fnode_i, (size_t)d->n_fnode * LUMEN_NODE_I);
     }
     S.n_fnode = d->n_fnode;
+  }
+  S.med_jump = nullptr;
+  S.jump_f = nullptr;
+  S.jump_i = nullptr;
+  S.clear = nullptr;
+  if (d->n_jump > 0) {  // the diffusion jump's grids, and each medium's grid index
+    std::vector<int32_t> mj(d->n_med > 0 ? d->n_med : 1, -1);
+    for (int g = 0; g < d->n_jump; ++g) mj[d->jump_i[(size_t)g * LUMEN_JUMP_I]] = g;
+    UPLOAD(S.med_jump, mj.data(), mj.size());
+    UPLOAD(S.jump_f, d->jump_f, (size_t)d->n_jump * LUMEN_JUMP_F);
+    UPLOAD(S.jump_i, d->jump_i, (size_t)d->n_jump * LUMEN_JUMP_I);
+    UPLOAD(S.clear, d->clear, (size_t)d->n_clear);
   }
   if (e) {
     for (void* p : sc->allocs) cudaFree(p);

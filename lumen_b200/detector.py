@@ -18,6 +18,7 @@ import numpy as np
 
 from lumen_b200 import facets
 from lumen_b200 import geometry as G
+from lumen_b200 import jump as J
 from lumen_b200 import optics as O
 
 OUTSIDE = "OUT"
@@ -99,6 +100,8 @@ class Detector:
         d.n_comp, d.n_fnode = len(r["comp_box"]), len(r["fnode_i"])
         d.comp, d.comp_box = iptr(keep["comp"]), fptr(keep["comp_box"])
         d.fnode_f, d.fnode_i = fptr(keep["fnode_f"]), iptr(keep["fnode_i"])
+        d.n_jump, d.n_clear = len(keep["jump_i"]), len(keep["clear"])
+        d.jump_f, d.jump_i, d.clear = fptr(keep["jump_f"]), iptr(keep["jump_i"]), fptr(keep["clear"])
         return d, keep
 
     @property
@@ -230,6 +233,17 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     arrays = dict(nav)
     arrays.update(n_cls=n_cls, cls_medium=cls_medium, row_of=row_of.ravel().astype(np.int32), med_i=med_i,
                   row_i=row_i, tab=tab)  # fmt: skip
+    # the diffusion jump's clearance grids (media whose only channel is Rayleigh; src/lumen/transport/fastpath.py:96)
+    media = []
+    for m in range(len(med_names)):
+        ok = med_i[m, 0] >= 0 and med_i[m, 2] >= 0 and med_i[m, 3] < 0 and med_i[m, 7] < 0
+        lam = 0.0
+        if ok:
+            off, k = tab[med_i[m, 2]]
+            lam = float(np.min(data[off + k:off + 2 * k].astype(np.float64)))
+        media.append((ok, lam))
+    jp = J.prepare(arrays, cls_medium[np.asarray(vol_cls, np.int64)], media)
+    arrays.update(jump_f=jp["jump_f"], jump_i=jp["jump_i"], clear=jp["clear"], jump_report=jp["report"])
     st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
     cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}
     return Detector(arrays, data, params_index, st, names, cls_names, groups)

@@ -95,6 +95,25 @@ def glisur_tank(polish_wall=0.8, polish_block=0.7) -> D.Detector:
                    skins={"TankLV": wall}, sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def fog_box(half=4.0, rayleigh=0.5, abs_len=30.0) -> D.Detector:
+    """Return a cube of half-width ``half`` m filled with a strongly scattering medium (Rayleigh length ``rayleigh``
+    m: the diffusion jump's domain, a volume at least 4 scattering lengths across), a dark 1 m block inside, and
+    sensor discs (r 0.3 m) on four of its faces."""  # noqa: D205
+    fog = O.Material("Fog", rindex=1.33, abslength=abs_len, rayleigh=rayleigh)
+    steel = O.Material("Steel")
+    box = G.Volume("FogBox", G.Box(half, half, half), "Fog")
+    block = G.Volume("Block", G.Box(0.5, 0.5, 0.5), "Steel")
+    box.place(block, (1.5, -1.0, 0.5), name="Block")
+    disc = G.Volume("Sensor", G.Tube(rmax=0.3, dz=0.01), "Steel")
+    faces = [((-half + 0.02, 0.0, 0.0), (1.0, 0.0, 0.0)), ((half - 0.02, 1.0, 0.0), (-1.0, 0.0, 0.0)),
+             ((0.0, -half + 0.02, 1.0), (0.0, 1.0, 0.0)), ((0.5, 0.0, half - 0.02), (0.0, 0.0, -1.0))]
+    for i, (p, ax) in enumerate(faces):
+        box.place(disc, p, _frame_z(ax), name=f"Sensor_{i}", copy=i)
+    sens = O.OpticalSurface("SensorSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    borders = [("FogBox", f"Sensor_{i}", sens) for i in range(len(faces))]
+    return D.build(box, {"Fog": fog, "Steel": steel}, borders=borders, sensors={"sensor": "Sensor"})
+
+
 def _grid_tank(n_pmt, radius, half_h, r_pmt, inset):
     """Return (positions, inward axes) of n_pmt PMTs on a regular barrel and end-cap grid."""
     area = 2 * math.pi * radius * 2 * half_h + 2 * math.pi * radius**2

@@ -37,6 +37,7 @@ typedef struct ORun {
   int max_vertices;
   int P;
   int gt[O_MAXG];
+  int jump; /* LUMEN_F_JUMP */
 } ORun;
 
 typedef struct OPhoton {
@@ -58,6 +59,69 @@ typedef struct ODep {
 } ODep;
 
 static inline float o_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0.0f; }
+
+/* ------------------------------------------------------------------------------------------ the diffusion jump */
+#define O_JUMP_STREAM 0x7A11u /* the vertex key's fold for the walk's own uniforms (rng.py:25) */
+typedef struct OJump { int ok, n; float y[3], d[3], er[3], L; } OJump;
+
+/* the walk at a bulk Rayleigh event inside the proven clear ball at xs (fastpath.py:174 diffuse): free paths at the
+   reference rate, the polarised Rayleigh draw and projection, until a flight leaves the ball (the photon put at the
+   crossing) or the budget ceil((c mu_r)^2) of scatterings is spent; identity where it does not apply */
+static OJump o_diffuse(const LumenSceneDesc* D, int mi, const float* xs, const float* d0, const float* er0,
+                       const float* ei0, float mu_r, int alive, OKey vkey) {
+  OJump J;
+  J.ok = 0; J.n = 0; J.L = 0.0f;
+  for (int a = 0; a < 3; ++a) { J.y[a] = 0.0f; J.d[a] = d0[a]; J.er[a] = er0[a]; }
+  int g = -1;
+  for (int k = 0; k < D->n_jump; ++k)
+    if (D->jump_i[(size_t)k * LUMEN_JUMP_I] == mi) g = k;
+  if (g < 0) return J;
+  const float* jf = D->jump_f + (size_t)g * LUMEN_JUMP_F;
+  const int32_t* ji = D->jump_i + (size_t)g * LUMEN_JUMP_I;
+  float h = jf[3];
+  int inside = 1, idx[3];
+  float node[3];
+  for (int a = 0; a < 3; ++a) {
+    float fi = (xs[a] - jf[a]) / h;
+    int na = ji[1 + a];
+    inside = inside && fi > -0.5f && fi < (float)na - 0.5f;
+    int i = (int)floorf(fi + 0.5f);
+    i = i < 0 ? 0 : (i > na - 1 ? na - 1 : i);
+    idx[a] = i;
+    node[a] = jf[a] + h * (float)i;
+  }
+  float dx[3] = {xs[0] - node[0], xs[1] - node[1], xs[2] - node[2]};
+  float c = D->clear[ji[4] + ((int64_t)idx[0] * ji[2] + idx[1]) * ji[3] + idx[2]] - sqrtf(o_dot(dx, dx));
+  int lin = ei0[0] == 0.0f && ei0[1] == 0.0f && ei0[2] == 0.0f;
+  if (!(inside && c > 0.0f && lin && alive && mu_r > 0.0f)) return J;
+  J.ok = 1;
+  float cm = c * mu_r;
+  int budget = (int)ceilf(o_min(cm * cm, (float)LUMEN_JUMP_STEPS));
+  OKey jkey = o_fold_in(vkey, O_JUMP_STREAM);
+  const float zero[3] = {0.0f, 0.0f, 0.0f};
+  int out = 0;
+  for (int j = 0; j < budget && !out; ++j) {
+    OKey kj = o_fold_in(jkey, (uint32_t)j);
+    float u0 = o_uniform(kj, 0);
+    float u3[3] = {o_uniform(kj, 1), o_uniform(kj, 2), o_uniform(kj, 3)};
+    float s = -o_log(u0) / mu_r;
+    float by = o_dot(J.y, J.d);
+    float t = -by + sqrtf(o_max(by * by - (o_dot(J.y, J.y) - c * c), 0.0f));
+    out = s >= t;
+    float k[3];
+    o_rayleigh_sample(J.er, zero, u3, k);
+    float e2[3] = {J.er[0], J.er[1], J.er[2]}, z2[3] = {0.0f, 0.0f, 0.0f};
+    o_project(e2, z2, k);
+    float st = out ? t : s;
+    for (int a = 0; a < 3; ++a) J.y[a] = J.y[a] + st * J.d[a];
+    J.L = J.L + st;
+    if (!out) {
+      for (int a = 0; a < 3; ++a) { J.d[a] = k[a]; J.er[a] = e2[a]; }
+      J.n += 1;
+    }
+  }
+  return J;
+}
 
 /* tangents of a medium's rates in the gradient parameters: d(1/L)/dL = -1/L^2 where L's table moves; per channel
    (dch, p-major) and their sum (dmu_c) */
@@ -195,10 +259,18 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
     for (int p = 0; p < P; ++p) { dlob[p] = 0.0f; dyld[p] = 0.0f; }
     const int32_t* mrec = D->med_i + (size_t)mi * LUMEN_MED_I;
     float Eph = O_HC / ph->lam;
+    OJump J;
+    J.ok = 0;
     if (cs == 0) { /* Rayleigh: the polarised dipole draw, the state projected (phase.py:57) */
       o_rayleigh_sample(er0, ei0, rl3, nx_d);
       for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
       o_project(nx_er, nx_ei, nx_d);
+      if (R->jump) { /* the diffusion jump (step.py:421): the walk's factor on the weight, its time on the clock */
+        J = o_diffuse(D, mi, nx_x, nx_d, nx_er, nx_ei, mu_r, ph->alive, vkey);
+        if (J.ok) {
+          for (int a = 0; a < 3; ++a) { nx_x[a] = nx_x[a] + J.y[a]; nx_d[a] = J.d[a]; nx_er[a] = J.er[a]; }
+        }
+      }
     } else if (cs == 1) { /* Mie (G4OpMieHG): drawn at the reference constants, weighted live / reference */
       int tg[3] = {mrec[LUMEN_MI_MIE_GF], mrec[LUMEN_MI_MIE_GB], mrec[LUMEN_MI_MIE_R]};
       float pl[3], pr[3];
@@ -238,6 +310,14 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
     fates1 = w_at * (1.0f - att * y_w);
     fates2 = 0.0f;
     nx_w = ph->w * w * rlw * y_w;
+    float wj = 1.0f;
+    if (J.ok) { /* the walk's likelihood ratio (fastpath.py:212): its absorption and its path, live over reference */
+      float lr = o_log(o_max(mu, O_FLOOR32) / o_max(mu_r, O_FLOOR32));
+      wj = o_exp(-ml.mu_abs * J.L) * o_exp((float)J.n * lr - (mu - mu_r) * J.L);
+      fates1 = fates1 + fates0 * (1.0f - wj);
+      fates0 = fates0 * wj;
+      nx_w = nx_w * wj;
+    }
     for (int p = 0; p < P; ++p) {
       float dwp = (dch[p * LUMEN_N_CHANNEL + cs] * e_l + ml.ch[cs] * (-(dmu_c[p] * s) * e_l)) / path_r;
       if (!(path_r != 0.0f)) dwp = 0.0f;
@@ -245,12 +325,19 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
       float dwf = dwp * att + w_path * datt;
       if (cs == 0) nx_dw[p] = ph->dw[p] * w + ph->w * dwf;
       else nx_dw[p] = (ph->dw[p] * w + ph->w * dwf) * rlw * y_w + ph->w * w * rlw * (dlob[p] * y_w + dyld[p]);
+      if (J.ok) {
+        float dlr = mu > O_FLOOR32 ? dmu_c[p] / mu : 0.0f;
+        float dwj = wj * (-(dmu_abs[p] * J.L) + (float)J.n * dlr - dmu_c[p] * J.L);
+        nx_dw[p] = nx_dw[p] * wj + ph->w * w * dwj;
+      }
     }
     nx_cls = next_cls;
     nx_ok = 1;
     nx_dtime = s / v_g + delay;
+    if (J.ok) nx_dtime = nx_dtime + J.L / v_g;
     for (int a = 0; a < 3; ++a) nx_sn[a] = q.normal[a];
     wr = ph->wr * w_r * y_r;
+    if (J.ok) wr = wr * o_exp(-mr.mu_abs * J.L);
   } else { /* _surface_event (step.py:362) */
     float pl = le.probs[os_], pp = p_prop[os_];
     float r_live = drawn ? (pp != 0.0f ? pl / pp : 0.0f) : 0.0f;
@@ -617,6 +704,7 @@ static void o_run_init(ORun* R, const LumenSceneDesc* D, const float* live, cons
   R->roulette = c->roulette;
   R->max_vertices = c->max_vertices;
   R->P = c->n_grad;
+  R->jump = (c->flags & LUMEN_F_JUMP) && D->n_jump > 0;
   for (int p = 0; p < R->P; ++p) R->gt[p] = c->grad_tab[p];
 }
 

@@ -315,3 +315,35 @@ def test_glisur_tank_tallies_gradients_and_reference(variant, glisur, built):
     T, O = _tallies(glisur, src, 1 << 13, controls=A.controls(variant=variant), pools=(live, glisur.pool))
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
+
+
+@pytest.fixture(scope="module")
+def fog():
+    return detectors.fog_box()
+
+
+FOG_SRC = sources.Point(position=(-1.0, 0.5, -0.5), n_photons=1.0, lam=400.0)
+
+
+def test_fog_box_jump_photons_bit_exact(fog, built):
+    """The diffusion jump (a Rayleigh walk inside the clearance grid's proven ball): every photon's record is the
+    checker's, with the jump on and off."""
+    for flags in (A.F_JUMP, 0):
+        bad, gi, oi, gf, of = _records_match(fog, FOG_SRC, 1 << 13, controls=A.controls(flags=flags))
+        assert len(bad) == 0, f"{flags}: {len(bad)} differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+@pytest.mark.parametrize("variant", [0, 3])
+def test_fog_box_jump_tallies_gradients_and_reference(variant, fog, built):
+    names = ["media/Fog/rayleigh", "media/Fog/absorption", "media/Fog/index"]
+    c = A.controls(grad_tabs=[fog.params_index[k] for k in names], variant=variant, flags=A.F_JUMP)
+    T, O = _tallies(fog, FOG_SRC, 1 << 14, controls=c, n_bins=50)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
+    np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+    live = fog.pool_with({"media/Fog/rayleigh": 0.55, "media/Fog/absorption": 28.0})
+    T, O = _tallies(fog, FOG_SRC, 1 << 13, controls=A.controls(variant=variant, flags=A.F_JUMP),
+                    pools=(live, fog.pool))  # fmt: skip
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
