@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 5
+#define LUMEN_B200_ABI_VERSION 6
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -31,7 +31,10 @@ typedef enum LumenStatus {
   LUMEN_ERR_SCENE = 3,        /* the scene uses a feature this engine does not build (see lumen_b200_last_error) */
   LUMEN_ERR_STEP_BUDGET = 4,  /* the device step budget of the call ran out before every photon ended */
   LUMEN_ERR_NO_DEVICE = 5,    /* no CUDA device, or not an sm_100 device */
-  LUMEN_ERR_NOT_SUPPORTED = 6 /* a request outside this build (e.g. more gradient parameters than LUMEN_MAX_GRAD) */
+  LUMEN_ERR_NOT_SUPPORTED = 6, /* a request outside this build (e.g. more gradient parameters than LUMEN_MAX_GRAD) */
+  LUMEN_ERR_RECORDS = 7       /* the deposit records outgrew LumenTallies.rec_capacity (src/lumen/run.py:236
+                                 RecordsOverflow): counts[LUMEN_C_RECORDS] is the capacity needed; the groups' cells
+                                 are not filled, every other tally is */
 } LumenStatus;
 
 /* ---------------------------------------------------------------------------------------------- array layouts */
@@ -214,7 +217,44 @@ enum { LUMEN_H_LOST = 0, LUMEN_H_ABANDONED, LUMEN_H_ESCAPED, LUMEN_H_DISTANCE_CU
        LUMEN_H_ABSORBED_SURFACE, LUMEN_H_ROULETTED, LUMEN_H_REWEIGHTED, LUMEN_H_TRUNCATED, LUMEN_H_PUSHED,
        LUMEN_H_START, LUMEN_N_HEALTH };
 enum { LUMEN_C_PHOTONS = 0, LUMEN_C_STEPS, LUMEN_C_DEPOSITS, LUMEN_C_TRUNCATED, LUMEN_C_MULTI, LUMEN_C_ABORTED,
-       LUMEN_N_COUNT };
+       LUMEN_C_RECORDS, LUMEN_N_COUNT };
+
+/* ------------------------------------------------------------------------------------ the readout groups */
+/* The histograms of src/lumen/readout/grid.py filled from the deposit records (src/lumen/readout/fill.py:88
+   readout), per sensor group: charge (S, *axes) on the deposit's features, its per-photon second moment charge2, and
+   on a timed grid the time nodes t0 + j dt (S, *delay_axes, nt) with the cubic Lagrange split and the late / early
+   overflow (q and q t). A deposit's features are read in the frame of the sensor's placement (the volume entered,
+   src/lumen/transport/step.py:663 sensor_frame): src/lumen/sensors/features.py BUILTIN. */
+enum { LUMEN_FEAT_WAVELENGTH = 0, LUMEN_FEAT_THETA, LUMEN_FEAT_COS_INCIDENCE, LUMEN_FEAT_GENERATION, LUMEN_FEAT_X,
+       LUMEN_FEAT_Y, LUMEN_FEAT_Z, LUMEN_FEAT_RHO, LUMEN_N_FEAT };
+#define LUMEN_MAX_AXES 4      /* charge axes + delay axes of one group */
+#define LUMEN_MAX_GROUPS 8
+typedef struct LumenAxis {    /* grid.py:63 Axis */
+  int32_t feature;            /* LUMEN_FEAT_* */
+  int32_t n;                  /* values (>= 2, ascending) */
+  int32_t knots;              /* 1: hat functions on the values (n cells, constant beyond the ends); 0: cells between
+                                 the values as edges (n - 1 cells; none outside) */
+  int32_t reserved;
+  const float* values;        /* device (host for the checker), n */
+} LumenAxis;
+typedef struct LumenGroup {   /* one sensor group's grid (grid.py:100 Grid) and its cells */
+  int32_t n_axes, n_delay;    /* the charge axes, then the delay axes, in axes[] */
+  int32_t nt;                 /* time nodes (0: no time histogram) */
+  int32_t weighted;           /* the time histogram weighted by `weights` read at the deposit's charge cells */
+  int32_t normalise;          /* each deposit times its surface's 1 / A_n (rows flagged LUMEN_RI_PER_NORMAL) */
+  int32_t n_sensors;          /* the group's sensors */
+  float t0, dt;               /* ns: the first node and the spacing */
+  LumenAxis axes[LUMEN_MAX_AXES];
+  const int32_t* index;       /* device, n_sensor: each detector sensor's position in the group (-1: not in it);
+                                 null: every sensor, in order */
+  const float* weights;       /* device, the acceptance per charge cell (the group's cells), or null: none */
+  double* charge;             /* device, n_events * n_sensors * cells: sum of q w0 x the cell weight */
+  double* charge2;            /* same: sum over photons of (the photon's adds to the cell)^2 */
+  double* time;               /* device, n_events * n_sensors * delay cells * nt (nt > 0; else null) */
+  double* over_q;             /* device, n_events * n_sensors * delay cells * 2: [late, early] q */
+  double* over_qt;            /* same: q t */
+} LumenGroup;
+#define LUMEN_REC_WORDS 20    /* one deposit record (80 bytes): the readout groups' scratch */
 typedef struct LumenTallies {
   int32_t n_events;          /* events tallied (>= 1) */
   int32_t n_bins;            /* time-histogram bins per sensor (0: none) */
@@ -226,6 +266,15 @@ typedef struct LumenTallies {
   double* jac;               /* device, n_events * n_sensor * n_grad: d arrival / d parameter, or null */
   double* health;            /* device, LUMEN_N_HEALTH: the fates summed over photons (times w0) */
   unsigned long long* counts;/* device, LUMEN_N_COUNT */
+  /* the readout groups (n_groups 0: none; lumen_b200_trace only): the trace appends a record per sensor deposit to
+     `records` (device scratch of rec_capacity * LUMEN_REC_WORDS 32-bit words, 16-byte aligned), then bins them */
+  int32_t n_groups;
+  int32_t reserved;
+  const LumenGroup* groups;  /* host, n_groups */
+  double* pe2;               /* device, n_events * n_sensor, or null: per photon (its q x the group's acceptance at its
+                                charge cells)^2, the pe moment of src/lumen/readout/fill.py:200 */
+  void* records;
+  int64_t rec_capacity;
 } LumenTallies;
 
 /* ------------------------------------------------------------------------------------------- entry points */

@@ -23,7 +23,12 @@ c_u64p = ctypes.POINTER(ctypes.c_uint64)
 MAX_GRAD = 8
 N_COL = 10
 N_HEALTH = 11
-N_COUNT = 6
+N_COUNT = 7
+C_RECORDS = 6
+ERR_RECORDS = 7
+MAX_AXES = 4
+MAX_GROUPS = 8
+REC_WORDS = 20
 F_ASYNC = 1
 F_REACH = 2
 F_JUMP = 4
@@ -33,7 +38,8 @@ UNI_NX, UNI_NY = 257, 69
 UNI_WORDS = 4 * UNI_NX * UNI_NY + 2 * UNI_NY
 HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "absorbed_surface", "rouletted",
           "reweighted", "truncated", "pushed", "start")  # fmt: skip
-COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted")
+COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted", "records")
+FEATURES = ("wavelength", "theta", "cos_incidence", "generation", "x", "y", "z", "rho")  # LUMEN_FEAT_* order
 SRC_POINT, SRC_TRACK, SRC_SCINT = 0, 1, 2
 EV_F = 8
 
@@ -75,10 +81,25 @@ class LumenControls(ctypes.Structure):
                 ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]  # fmt: skip
 
 
+class LumenAxis(ctypes.Structure):
+    _fields_ = [("feature", ctypes.c_int32), ("n", ctypes.c_int32), ("knots", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("values", c_f32p)]  # fmt: skip
+
+
+class LumenGroup(ctypes.Structure):
+    _fields_ = [("n_axes", ctypes.c_int32), ("n_delay", ctypes.c_int32), ("nt", ctypes.c_int32),
+                ("weighted", ctypes.c_int32), ("normalise", ctypes.c_int32), ("n_sensors", ctypes.c_int32),
+                ("t0", ctypes.c_float), ("dt", ctypes.c_float), ("axes", LumenAxis * MAX_AXES),
+                ("index", c_i32p), ("weights", c_f32p), ("charge", c_f64p), ("charge2", c_f64p), ("time", c_f64p),
+                ("over_q", c_f64p), ("over_qt", c_f64p)]  # fmt: skip
+
+
 class LumenTallies(ctypes.Structure):
     _fields_ = [("n_events", ctypes.c_int32), ("n_bins", ctypes.c_int32), ("bin0", ctypes.c_float),
                 ("bin_w", ctypes.c_float), ("arrival", c_f64p), ("arrival_t", c_f64p), ("arrival2", c_f64p),
-                ("hist", c_f64p), ("jac", c_f64p), ("health", c_f64p), ("counts", c_u64p)]  # fmt: skip
+                ("hist", c_f64p), ("jac", c_f64p), ("health", c_f64p), ("counts", c_u64p),
+                ("n_groups", ctypes.c_int32), ("reserved", ctypes.c_int32), ("groups", ctypes.POINTER(LumenGroup)),
+                ("pe2", c_f64p), ("records", ctypes.c_void_p), ("rec_capacity", ctypes.c_int64)]  # fmt: skip
 
 
 def iptr(a):
@@ -151,11 +172,23 @@ def engine():
     return _lib
 
 
+class EngineError(RuntimeError):
+    """A non-zero status of the engine (``code``: LUMEN_ERR_*)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"lumen_b200 status {code}: {msg}")
+        self.code = code
+
+
+class RecordsOverflow(EngineError):
+    """The deposit records outgrew the scratch (LUMEN_ERR_RECORDS; src/lumen/run.py:236 RecordsOverflow)."""
+
+
 def check(status: int):
     """Raise the engine's error for a non-zero status."""
     if status != 0:
         msg = engine().lumen_b200_last_error().decode(errors="replace")
-        raise RuntimeError(f"lumen_b200 status {status}: {msg}")
+        raise (RecordsOverflow if status == ERR_RECORDS else EngineError)(status, msg)
 
 
 def key_of_seed(seed: int):

@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from lumen_b200 import _abi as A
+from lumen_b200 import readout as RO
 from lumen_b200.engine import DeviceRows, DeviceSource, DeviceTallies, Engine
 from lumen_b200.sources import FromArrays
 
@@ -65,9 +66,9 @@ class Light:
     mean_arrival_time: np.ndarray
     health: Health
     provenance: dict = field(default_factory=dict)
-    groups: dict | None = None  # {"time": (.., S, bins) arrival-time histograms, "time_edges": (bins + 1,)}
+    groups: dict | None = None  # {readout group: lumen_b200.readout.Histograms} (the run's ``groups``)
     gradients: dict | None = None  # {parameter: d arrivals / d value}
-    diagnostics: object = None
+    diagnostics: dict | None = None  # "time" (.., S, bins) arrival-time histograms and "time_edges" (``time_bins``)
     truth: object = None
 
     @property
@@ -93,7 +94,7 @@ def _engine(det, device=None) -> Engine:
 
 
 def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, controls=None, chunk=None,
-             gradients=(), time_bins=None, device=None, stream=None) -> Light:
+             gradients=(), time_bins=None, groups=None, records=None, device=None, stream=None) -> Light:
     """Return the Light of ``samples`` photons of ``source`` in detector ``det`` (lumen.simulate's signature).
 
     ``params``: {parameter name: value} overriding the detector's values (``det.params()``); ``reference``: the
@@ -103,7 +104,11 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     wavefront where derivatives are asked for, the persistent loop otherwise, the measured faster of the two on the
     tank workloads). ``chunk``: photons per launch (default: all in one launch). ``gradients``: parameter names
     whose derivatives of the arrivals are returned (forward tangents of the reweighting estimator along each path).
-    ``time_bins``: (bins, t0, width) ns of the per-sensor arrival-time histograms.
+    ``time_bins``: (bins, t0, width) ns of the per-sensor arrival-time histograms (``Light.diagnostics``).
+    ``groups``: the readout groups' histograms to fill ({name: lumen_b200.readout.Grid or Group}: a Grid's sensors
+    are the detector's group of that name, else every sensor) into ``Light.groups`` (src/lumen/readout/grid.py
+    Histograms); ``records``: the deposit records one launch may keep for them (default 2 per photon, at least 2^16;
+    a launch that outgrows it is re-run with room for what it needed, as the reference's RecordsOverflow retry).
     """
     eng = _engine(det, device)
     live = det.pool_with(params)
@@ -130,17 +135,31 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
         raise ValueError(f"a run traces at most {MAX_ID} photons (int32 ids)")
     nb, t0, tw = (0, 0.0, 1.0) if time_bins is None else time_bins
     T = DeviceTallies(det.n_sensor, n_ev, nb, t0, tw, len(gt), eng.device)
-    key = A.key_of_seed(seed)
+    G = None
     step = int(chunk) if chunk else total
-    for first in range(0, total, max(step, 1)):
-        m = min(step, total - first)
-        if drows is not None and first > 0:
-            raise ValueError("explicit rows run in one launch")
-        eng.trace(key, m, source=dsrc, rows=drows, first_id=first, controls=c, tallies=T, stream=stream)
-    return _light(det, T, n_ev, total, seed, gnames, (nb, t0, tw), source)
+    if groups:
+        G = RO.GroupCells(det, groups, n_ev, eng.device)
+        T.attach_groups(G, int(records) if records else max(1 << 16, 2 * min(step, total)))
+    key = A.key_of_seed(seed)
+    for _attempt in range(4):
+        try:
+            for first in range(0, total, max(step, 1)):
+                m = min(step, total - first)
+                if drows is not None and first > 0:
+                    raise ValueError("explicit rows run in one launch")
+                before = int(T.counts[A.C_RECORDS].item()) if G is not None else 0
+                eng.trace(key, m, source=dsrc, rows=drows, first_id=first, controls=c, tallies=T, stream=stream)
+            break
+        except A.RecordsOverflow:  # the launch's records outgrew the scratch: every tally again with room for them
+            need = int(T.counts[A.C_RECORDS].item()) - before
+            T.zero_()
+            T.attach_groups(G, need + need // 4 + 1024)
+    else:
+        raise A.RecordsOverflow(A.ERR_RECORDS, "the deposit records kept outgrowing the scratch")
+    return _light(det, T, n_ev, total, seed, gnames, (nb, t0, tw), source, G)
 
 
-def _light(det, T, n_ev, samples, seed, gnames, bins, source):
+def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):
     arr = T.arrival.cpu().numpy()
     arr_t = T.arrival_t.cpu().numpy()
     arr2 = T.arrival2.cpu().numpy()
@@ -159,24 +178,52 @@ def _light(det, T, n_ev, samples, seed, gnames, bins, source):
     health = Health(lost=h[0], abandoned=h[1], escaped=h[2], distance_cut=h[3], absorbed_bulk=h[4],
                     absorbed_surface=h[5], rouletted=h[6], reweighted=h[7], truncated=h[8], pushed=h[9],
                     start=h[10], records=int(cnt[2]), photons=int(cnt[0]), steps=int(cnt[1]))  # fmt: skip
-    groups = None
+    diag = None
     if bins[0]:
         hist = T.hist.cpu().numpy()
-        groups = {"time": hist if n_ev > 1 else hist[0],
-                  "time_edges": bins[1] + bins[2] * np.arange(bins[0] + 1)}  # fmt: skip
+        diag = {"time": hist if n_ev > 1 else hist[0], "time_edges": bins[1] + bins[2] * np.arange(bins[0] + 1)}
+    groups = G.histograms(nn) if G is not None else None
     grads = None
     if gnames:
         jac = T.jac.cpu().numpy()
         grads = {k: (jac[..., i] if n_ev > 1 else jac[0, :, i]) for i, k in enumerate(gnames)}
     prov = dict(seed=seed, samples=samples, engine="lumen_b200", steps_per_photon=cnt[1] / max(cnt[0], 1))
-    return Light(arr, err, mt, health, prov, groups, grads)
+    return Light(arr, err, mt, health, prov, groups, grads, diag)
 
 
-def pe(light: Light, qe=None, efficiency=1.0, lam=None):
-    """Return expected photoelectrons per sensor: efficiency x QE(lam) x arrivals (src/lumen/readout/detection.py:86
-    ``expected_pe``) for a source of one wavelength ``lam`` (nm); ``qe`` = (wavelengths nm, values)."""  # noqa: D205
+def pe(light: Light, values=None, *, qe=None, efficiency=1.0, lam=None):
+    """Return expected photoelectrons per sensor (src/lumen/readout/detection.py:91 ``pe``).
+
+    With readout groups: ``values`` = {group: {"tables": [(axis names, values over those axes' cells), ...] (the sensor
+    model's acceptance tables, e.g. the QE on the wavelength knots), "efficiency": scalar or per sensor}}; each
+    group's charge histogram contracted with its tables, times the efficiency, at its sensors (0 at a sensor of no
+    group). Without: efficiency x QE(lam) x arrivals for a source of one wavelength ``lam`` (nm); ``qe`` =
+    (wavelengths nm, values).
+    """
+    if values is not None:
+        out = np.zeros(light.arrivals.shape, np.float64)
+        for name, h in (light.groups or {}).items():
+            v = values.get(name)
+            if v is None:
+                continue
+            acc = RO.tables_acceptance(h.grid, v.get("tables", ()))
+            ids = np.arange(out.shape[-1]) if h.sensors is None else np.asarray(h.sensors, np.int64)
+            out[..., ids] = RO.expected_pe(h, acc, v.get("efficiency", 1.0))
+        return out
     q = 1.0 if qe is None else float(np.interp(lam, np.asarray(qe[0], float), np.asarray(qe[1], float)))
     return np.asarray(efficiency) * q * light.arrivals
+
+
+def pe_error(light: Light):
+    """Return each sensor's pe Monte Carlo error at the groups' acceptance the run was given (``Group.weights`` and
+    ``efficiency``; src/lumen/readout/detection.py:106 ``pe_error``); 0 at a sensor of no such group."""  # noqa: D205, D209
+    out = np.zeros(light.arrivals.shape, np.float64)
+    for h in (light.groups or {}).values():
+        if h.pe_error is None:
+            continue
+        ids = np.arange(out.shape[-1]) if h.sensors is None else np.asarray(h.sensors, np.int64)
+        out[..., ids] = h.pe_error
+    return out
 
 
 def seed_key(seed: int):

@@ -24,6 +24,9 @@ struct Run {
   int gt[LUMEN_MAX_GRAD];
   int reach_on;  // LUMEN_F_REACH: bulk steps' queries bounded by the sensor reach
   int jump_on;   // LUMEN_F_JUMP: the diffusion jump at bulk Rayleigh events
+  uint32_t* rec;                // the deposit records of the readout groups (LUMEN_REC_WORDS each), or null
+  long long rec_cap;            // records the scratch holds
+  unsigned long long* rec_n;    // the call's record counter
 };
 
 // ------------------------------------------------------------------------------------------ the diffusion jump
@@ -94,7 +97,61 @@ struct Photon {
   int vol, srf;
   float sn[3];
   int nz, cls;
+  int gen;   // re-emissions so far (state.py Photon.gen: a WLS channel event adds one)
+  int last;  // the photon's last deposit record (-1: none; the readout groups only)
 };
+
+// ----------------------------------------------------------------------------------- the deposit records
+// A_n: the share of a row absorbed and detected at normal incidence with eff 1, at the photon's wavelength and the
+// crossing's incoming index, unpolarised (types.py:397 normal_absorptance, :391 _normal_incidence): the chain's
+// absorbed rest of the cut reflectance (the R column; for a complex index the unpolarised Fresnel reflectance
+// 0.5 (|r_s|^2 + |r_p|^2), fresnel.py:53) and T
+L_DEV float d_normal_absorptance(const DScene& S, const float* __restrict__ pool, int row, float lam, float n1,
+                                 const float* nrm) {
+  const int32_t* ri = S.row_i + (size_t)row * LUMEN_ROW_I;
+  float E = D_HC / lam;
+  float Rc = d_tab(S, pool, __ldg(ri + LUMEN_RI_COL + LUMEN_COL_R), E);
+  if (__ldg(ri + LUMEN_RI_MODEL) == 2) {
+    float cos_i = d_clip01(-((-nrm[0] * nrm[0] + -nrm[1] * nrm[1]) + -nrm[2] * nrm[2]));
+    Cf amps[4];
+    d_amplitudes(cos_i, n1, cf(d_tab(S, pool, __ldg(ri + LUMEN_RI_COL + LUMEN_COL_NR), E),
+                               d_tab(S, pool, __ldg(ri + LUMEN_RI_COL + LUMEN_COL_NK), E)), amps);
+    Rc = d_clip01(0.5f * (c_abs2(amps[0]) + c_abs2(amps[1])));
+  }
+  float cut[2] = {Rc, d_tab(S, pool, __ldg(ri + LUMEN_RI_COL + LUMEN_COL_T), E)}, zc[2] = {0.0f, 0.0f}, rta[3], drta[3];
+  d_chained<2>(cut, zc, rta, drta);
+  return rta[2];
+}
+
+// appends one deposit record (step.py:546 the deposit's local fields, before the sensor frame: the crossing point,
+// the direction and the normal in world coordinates, the volume entered, the re-emission count, 1 / A_n on a row
+// flagged per_normal) and returns its index (-1 past the scratch's capacity); prev links the photon's records
+L_CALL int d_record(const Run& R, int prev, int sensor, float q, float time, float lam, int gen, int row, float n1,
+                    int vol, const float* x, const float* d, const float* nrm) {
+  const DScene& S = R.S;
+  float inv_an = 1.0f;
+  if (row >= 0 && __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL)) {
+    float an = d_normal_absorptance(S, R.live, row, lam, n1, nrm);
+    inv_an = an > 0.0f ? 1.0f / an : 0.0f;
+  }
+  unsigned long long k = atomicAdd(R.rec_n, 1ull);
+  if (k >= (unsigned long long)R.rec_cap) return -1;
+  float4* r = reinterpret_cast<float4*>(R.rec + k * LUMEN_REC_WORDS);
+  r[0] = make_float4(__int_as_float(prev), __int_as_float(sensor), q, time);
+  r[1] = make_float4(lam, inv_an, __int_as_float(gen), __int_as_float(vol));
+  r[2] = make_float4(x[0], x[1], x[2], d[0]);
+  r[3] = make_float4(d[1], d[2], nrm[0], nrm[1]);
+  r[4] = make_float4(nrm[2], __int_as_float(0), 0.0f, __int_as_float(0));
+  return (int)k;
+}
+
+// marks a photon's last record as the head of its chain, with the photon's row weight and event
+L_DEV void d_record_head(const Run& R, int last, float w0, int ev) {
+  uint32_t* r = R.rec + (size_t)last * LUMEN_REC_WORDS;
+  r[17] = 1u;
+  r[18] = __float_as_uint(w0);
+  r[19] = (uint32_t)ev;
+}
 
 struct Dep {
   int sensor;
@@ -289,6 +346,7 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
     }
   float lost = (q.hit && ph.alive && row < 0 && !scatter) ? ph.w * rr * att_if : 0.0f;
   float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_er[3], nx_ei[3], nx_lam = ph.lam;
+  int nx_gen = ph.gen;
   float nx_dw[G > 0 ? G : 1];
   int nx_cls, nx_ok, nx_far = 0;
   float fates0, fates1, fates2, wr;
@@ -349,6 +407,7 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
       for (int a = 0; a < 3; ++a) { nx_d[a] = b2.d[a]; nx_er[a] = b2.er[a]; nx_ei[a] = b2.ei[a]; }
       rlw = b2.rlw; y_w = b2.y_w; y_r = b2.y_r; delay = b2.delay;
       nx_lam = b2.lam;
+      nx_gen = ph.gen + (cs == 2);  // a WLS event re-emits (medium.py:126 reemitted)
     }
     float w_at = ph.w * w_path;
     fates0 = w_at * att * y_w;
@@ -510,6 +569,11 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
   float pushed = (ph.alive && ph.nz == D_ZSBP) ? ph.w : 0.0f;
   dep.sensor = at_if ? sensor_q : -1;
   dep.time = time;
+  if (R.rec && dep.sensor >= 0) {  // the readout groups' record, at the crossing (step.py:687 _local)
+    float xc[3] = {ph.x[0] + dist * ph.d[0], ph.x[1] + dist * ph.d[1], ph.x[2] + dist * ph.d[2]};
+    ph.last = d_record(R, ph.last, dep.sensor, dep.q, time, ph.lam, ph.gen, row, ml.n, q.vol_after, xc, ph.d,
+                       q.normal);
+  }
   dep.fates[0] = lost;
   dep.fates[1] = abandoned;
   dep.fates[2] = escaped;
@@ -523,6 +587,7 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
   for (int a = 0; a < 3; ++a) { ph.x[a] = nx_x[a]; ph.d[a] = nx_d[a]; ph.er[a] = nx_er[a]; ph.ei[a] = nx_ei[a]; }
   ph.t = ph.t + nx_dtime;
   ph.lam = nx_lam;
+  ph.gen = nx_gen;
   ph.w = alive ? w_new : 0.0f;
   ph.wr = alive ? wr_new : 0.0f;
   if (G > 0)
@@ -638,6 +703,8 @@ L_DEV void d_start(const DScene& S, const Row& r, Photon& ph) {
   ph.cls = d_cls(S, ph.vol);
   ph.srf = -1;
   ph.nz = 0;
+  ph.gen = 0;
+  ph.last = -1;
 }
 
 }  // namespace lb

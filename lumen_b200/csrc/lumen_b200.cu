@@ -21,6 +21,7 @@
 
 #include "../../include/lumen_b200.h"
 #include "dstep.cuh"
+#include "dreadout.cuh"
 
 using namespace lb;
 
@@ -232,6 +233,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
       }
       if (!ph.alive || ph.vertex >= L.R.max_vertices) {
         flush_all(L.T, ev, pt);
+        if (L.R.rec && ph.last >= 0) d_record_head(L.R, ph.last, (float)w0, ev);
         if (ph.alive) {
           trunc_w = (double)ph.w * w0;
           c_trunc++;
@@ -253,7 +255,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   // the block's health and counters: one atomic per block and value
   __shared__ unsigned long long sc[LUMEN_N_COUNT][BLOCK / 32];
   const int warp = threadIdx.x >> 5;
-  unsigned long long cv[LUMEN_N_COUNT] = {c_ph, c_steps, c_dep, c_trunc, c_multi, 0ull};
+  unsigned long long cv[LUMEN_N_COUNT] = {};
+  cv[LUMEN_C_PHOTONS] = c_ph;
+  cv[LUMEN_C_STEPS] = c_steps;
+  cv[LUMEN_C_DEPOSITS] = c_dep;
+  cv[LUMEN_C_TRUNCATED] = c_trunc;
+  cv[LUMEN_C_MULTI] = c_multi;
   if (threadIdx.x == 0 && L.abort_flag && *(volatile int*)L.abort_flag) cv[LUMEN_C_ABORTED] = 1ull;
 #pragma unroll
   for (int k = 0; k < LUMEN_N_COUNT; ++k) {
@@ -364,6 +371,7 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
     }
     if (!ph.alive || ph.vertex >= L.R.max_vertices) {
       flush_all(L.T, ex.ev, ex.pt);
+      if (L.R.rec && ph.last >= 0) d_record_head(L.R, ph.last, (float)ex.w0, ex.ev);
       if (ph.alive) {
         trunc_w = (double)ph.w * ex.w0;
         c_trunc++;
@@ -412,7 +420,13 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
   }
   // the block's health, counters and live slots: one atomic per block and value
   const int warp = threadIdx.x >> 5;
-  unsigned long long cv[LUMEN_N_COUNT + 1] = {c_ph, c_steps, c_dep, c_trunc, c_multi, 0ull, (unsigned long long)act};
+  unsigned long long cv[LUMEN_N_COUNT + 1] = {};
+  cv[LUMEN_C_PHOTONS] = c_ph;
+  cv[LUMEN_C_STEPS] = c_steps;
+  cv[LUMEN_C_DEPOSITS] = c_dep;
+  cv[LUMEN_C_TRUNCATED] = c_trunc;
+  cv[LUMEN_C_MULTI] = c_multi;
+  cv[LUMEN_N_COUNT] = (unsigned long long)act;  // the live slots
 #pragma unroll
   for (int k = 0; k < LUMEN_N_COUNT + 1; ++k) {
     unsigned long long v = cv[k];
@@ -742,6 +756,53 @@ static int run_wave(const Launch& L, unsigned long long* live, cudaStream_t stre
   return st;
 }
 
+// ------------------------------------------------------------------------------------ the readout groups
+static int check_groups(int n_sensor, const LumenTallies* out) {
+  if (out->n_groups < 0 || out->n_groups > LUMEN_MAX_GROUPS) return set_err(LUMEN_ERR_ARG, "groups: 0 .. LUMEN_MAX_GROUPS");
+  if (!out->groups) return set_err(LUMEN_ERR_ARG, "groups: the array is null");
+  if (!out->records || ((uintptr_t)out->records & 15) || out->rec_capacity <= 0 || out->rec_capacity > 2147483647LL)
+    return set_err(LUMEN_ERR_ARG, "groups: records must be a 16-byte aligned scratch of 1 .. 2^31 - 1 records");
+  for (int g = 0; g < out->n_groups; ++g) {
+    const LumenGroup& G = out->groups[g];
+    const std::string w = "group " + std::to_string(g) + ": ";
+    if (G.n_axes < 0 || G.n_delay < 0 || G.n_axes + G.n_delay > LUMEN_MAX_AXES)
+      return set_err(LUMEN_ERR_ARG, w + "at most LUMEN_MAX_AXES axes");
+    for (int a = 0; a < G.n_axes + G.n_delay; ++a) {
+      const LumenAxis& A = G.axes[a];
+      if (A.feature < 0 || A.feature >= LUMEN_N_FEAT) return set_err(LUMEN_ERR_ARG, w + "unknown feature");
+      if (A.n < 2 || !A.values) return set_err(LUMEN_ERR_ARG, w + "an axis needs two values or more");
+    }
+    if (G.n_sensors <= 0 || (!G.index && G.n_sensors != n_sensor))
+      return set_err(LUMEN_ERR_ARG, w + "n_sensors: the group's sensors (every detector sensor without an index)");
+    if (!G.charge || !G.charge2) return set_err(LUMEN_ERR_ARG, w + "charge and charge2 are required");
+    if (G.nt < 0 || (G.nt > 0 && (!(G.dt > 0.0f) || !G.time || !G.over_q || !G.over_qt)))
+      return set_err(LUMEN_ERR_ARG, w + "a timed grid needs dt > 0, time, over_q and over_qt");
+    if (G.weighted && !G.weights) return set_err(LUMEN_ERR_ARG, w + "a weighted grid needs its weights");
+  }
+  return 0;
+}
+
+static int launch_bin(const Launch& L, const LumenTallies* out, cudaStream_t stream) {
+  Bin B;
+  memset(&B, 0, sizeof(B));
+  for (int g = 0; g < out->n_groups; ++g) B.g[g] = out->groups[g];
+  B.n_groups = out->n_groups;
+  B.E = L.T.E;
+  B.S_ = L.T.S_;
+  B.rec = L.R.rec;
+  B.n = L.R.rec_n;
+  B.cap = L.R.rec_cap;
+  B.pe2 = out->pe2;
+  B.vol_f = L.R.S.vol_f;
+  B.counts = out->counts;
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  k_bin<<<sms * 8, 256, 0, stream>>>(B);
+  CK(cudaGetLastError());
+  return 0;
+}
+
 static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
                      cudaStream_t stream, int variant = 0, int bps = 0, int async = 0) {
   if (variant == LUMEN_VARIANT_WAVEFRONT && async)
@@ -752,14 +813,24 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
   T.P = L.R.P;
   T.cot = cot;
   T.grads = grads;
-  // scratch: the photon counter, the abort flag, the steps used and the wavefront's live slots (one small allocation
-  // per call)
+  // scratch: the photon counter, the abort flag, the steps used, the wavefront's live slots and the record count (one
+  // small allocation per call)
+  const int groups = out && out->n_groups > 0;
+  if (groups) {
+    int gs = check_groups(L.R.S.n_sensor, out);
+    if (gs) return gs;
+  }
   unsigned long long* scratch = nullptr;
-  CK(cudaMallocAsync((void**)&scratch, 4 * sizeof(unsigned long long), stream));
-  CK(cudaMemsetAsync(scratch, 0, 4 * sizeof(unsigned long long), stream));
+  CK(cudaMallocAsync((void**)&scratch, 5 * sizeof(unsigned long long), stream));
+  CK(cudaMemsetAsync(scratch, 0, 5 * sizeof(unsigned long long), stream));
   L.next = scratch;
   L.abort_flag = (int*)(scratch + 1);
   L.steps_used = scratch + 2;
+  if (groups) {
+    L.R.rec = (uint32_t*)out->records;
+    L.R.rec_cap = out->rec_capacity;
+    L.R.rec_n = scratch + 4;
+  }
   // adjoint calls with no tallies of their own accumulate health and counts into the scratch's tail
   double* dummy = nullptr;
   if (!out) {
@@ -796,17 +867,23 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
       if (st) return st;
     }
   }
+  if (groups && (st = launch_bin(L, out, stream))) return st;
   if (async) {  // enqueue only: the abort flag reaches counts[LUMEN_C_ABORTED] on the device
     CK(cudaFreeAsync(scratch, stream));
     if (dummy) CK(cudaFreeAsync(dummy, stream));
     return 0;
   }
   int flag = 0;
+  unsigned long long n_rec = 0;
   CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(&n_rec, scratch + 4, sizeof(n_rec), cudaMemcpyDeviceToHost, stream));
   CK(cudaFreeAsync(scratch, stream));
   if (dummy) CK(cudaFreeAsync(dummy, stream));
   CK(cudaStreamSynchronize(stream));
   if (flag) return set_err(LUMEN_ERR_STEP_BUDGET, "the call's step budget ran out before every photon ended");
+  if (groups && n_rec > (unsigned long long)out->rec_capacity)
+    return set_err(LUMEN_ERR_RECORDS, "the deposit records outgrew rec_capacity (" + std::to_string(n_rec) +
+                                          " needed): the groups are not filled");
   return 0;
 }
 
@@ -816,7 +893,7 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
 // array's name as an address (it names a host-side stand-in); each device's address is looked up once, with that
 // device current, by cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned long long g_static_scratch[LUMEN_STATIC_SCRATCH_WORDS];
-static const int STATIC_SCRATCH_NEED = 3;  // photon counter, abort flag, steps used
+static const int STATIC_SCRATCH_NEED = 4;  // photon counter, abort flag, steps used, record count
 static std::mutex g_static_mu;
 static void* g_static_addr[256];
 
@@ -857,20 +934,33 @@ static int run_trace_static(Launch& L, const LumenTallies* out, cudaStream_t str
   T.jac = out->jac;
   T.health = out->health;
   T.counts = out->counts;
+  const int groups = out->n_groups > 0;
+  if (groups && (st = check_groups(L.R.S.n_sensor, out))) return st;
   // the array keeps the previous call's counts: clear the words this call reads before they are written
   CK(cudaMemsetAsync(scratch, 0, STATIC_SCRATCH_NEED * sizeof(unsigned long long), stream));
   L.next = scratch;
   L.abort_flag = (int*)(scratch + 1);
   L.steps_used = scratch + 2;
+  if (groups) {
+    L.R.rec = (uint32_t*)out->records;
+    L.R.rec_cap = out->rec_capacity;
+    L.R.rec_n = scratch + 3;
+  }
   if (L.n > 0) {
     if (L.R.P > 0) st = launch_trace<LUMEN_MAX_GRAD>(L, 0, 0, stream);
     else st = launch_trace<0>(L, 0, 0, stream);
     if (st) return st;
   }
+  if (groups && (st = launch_bin(L, out, stream))) return st;
   int flag = 0;
+  unsigned long long n_rec = 0;
   CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(&n_rec, scratch + 3, sizeof(n_rec), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   if (flag) return set_err(LUMEN_ERR_STEP_BUDGET, "the call's step budget ran out before every photon ended");
+  if (groups && n_rec > (unsigned long long)out->rec_capacity)
+    return set_err(LUMEN_ERR_RECORDS, "the deposit records outgrew rec_capacity (" + std::to_string(n_rec) +
+                                          " needed): the groups are not filled");
   return 0;
 }
 

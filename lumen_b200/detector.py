@@ -111,13 +111,17 @@ class Detector:
         return bool(((r[:, 0] == 0) & (r[:, 1] == 0) & (r[:, 2] == 0)).any())
 
 
-def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None) -> Detector:
+def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None,
+          after_tracking=()) -> Detector:
     """Return the Detector of the volume tree ``top`` (the detector volume, placed at the origin).
 
     ``materials``: {name: Material}. ``borders``: [(pv from, pv to, OpticalSurface)] (Geant4 border surfaces, ordered);
     ``skins``: {lv name: OpticalSurface}. ``sensors``: {group: lv name}: every placement of that logical volume is a
     sensor, counted where a crossing's surface into it deposits (the ``border_into`` rule). Light that leaves ``top``
     is absorbed there (the detector volume's boundary, as the reference's recipe ``detector_volume``).
+    ``after_tracking``: sensor groups whose sensor model applies its QE after tracking: their rows detect every
+    absorption (eff 1) and are read per normal incidence (types.py:576 per_normal: a deposit carries 1 / A_n, by
+    which a normalising readout grid divides it).
     """
     skins = skins or {}
     sensors = sensors or {}
@@ -204,25 +208,30 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             if surf is None and not into_out and cls_lv[cb].name in skins:
                 surf = skins[cls_lv[cb].name]
             is_sensor = (not into_out) and cls_lv[cb].name in sensor_lv
+            per_normal = int(is_sensor and sensor_lv[cls_lv[cb].name] in set(after_tracking))
             if surf is None:
                 if into_out or from_out or opaque[cls_mat[cb]] or opaque[cls_mat[ca]]:
                     surf = O.ABSORBER  # the detector volume's boundary; Geant4's NoRINDEX
                 else:
                     surf = O.OpticalSurface("__fresnel__", "dielectric_dielectric", "polished")
-            key = (surf.name, is_sensor, far_opq, id(surf))
+            key = (surf.name, is_sensor, far_opq, id(surf), per_normal)
             if key not in row_key:
-                row = O.surface_row(surf, is_sensor, far_opq)
+                row = O.surface_row(surf, is_sensor, far_opq, 1.0 if per_normal else None)
                 row.sensor = is_sensor
+                row.per_normal = per_normal
                 row_key[key] = len(rows)
                 rows.append(row)
             row_of[ca, cb] = row_key[key]
     row_i = np.zeros((len(rows), 16), np.int32)
     col_tab = {}  # one table per (surface, column): every row of a surface reads (and moves with) the same values
     for r, row in enumerate(rows):
-        row_i[r, 0:4] = [row.model, row.normal, row.glisur, row.far_opaque]
+        row_i[r, 0:5] = [row.model, row.normal, row.glisur, row.far_opaque, row.per_normal]
         for c, col in enumerate(O.COLUMNS):
             if col not in row.cols or (col == "eff" and not row.sensor):
                 row_i[r, 6 + c] = neutral[col]
+                continue
+            if col == "eff" and row.per_normal:  # every absorption entering is counted: eff 1, not a parameter
+                row_i[r, 6 + c] = pool.add(1.0)
                 continue
             k = (row.name, col)
             if k not in col_tab:

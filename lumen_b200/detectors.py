@@ -42,6 +42,35 @@ def toy_tank() -> D.Detector:
     return D.build(tank, {"Water": water, "Photocathode": cathode}, borders=borders, sensors={"pmt": "PMT"})
 
 
+def readout_tank(after_tracking=True) -> D.Detector:
+    """Return the scintillator cube's tank (Rayleigh, Mie and WLS in the bulk, a ground half-reflecting wall) with two
+    sensor groups: six PMTs ("pmt") whose cathodes have a complex index (RINDEX 2.7, KINDEX 1.5: a photocathode
+    reflecting specularly) and whose sensor model applies its QE after tracking (``after_tracking``: every absorption
+    counted, deposits carrying 1 / A_n), and two reference PMTs ("ref") with a half-reflecting metal cathode of
+    efficiency 0.8."""  # noqa: D205
+    e_abs = [1.5, 2.5, 2.9, 3.0, 3.2, 5.0]
+    lab = O.Material("LAB", rindex=([1.5, 2.5, 3.5, 5.0], [1.47, 1.48, 1.50, 1.53]), abslength=20.0, rayleigh=5.0,
+                     mie=2.0, mie_forward=0.9, mie_backward=0.3, mie_forward_ratio=0.8,
+                     wls=(e_abs, [100.0, 100.0, 20.0, 1.0, 1.0, 1.0]),
+                     wls_spectrum=([2.3, 2.5, 2.7, 2.9, 3.1, 3.2], [0.0, 0.4, 1.0, 0.7, 0.1, 0.0]),
+                     wls_mean=0.9, wls_tau=2.0, wls_profile="exponential")  # fmt: skip
+    cathode = O.Material("Photocathode")
+    pmt = G.Volume("PMT", G.Tube(rmax=50 * MM, dz=10 * MM), "Photocathode")
+    ref = G.Volume("RefPMT", G.Tube(rmax=50 * MM, dz=10 * MM), "Photocathode")
+    tank = G.Volume("TankLV", G.Box(0.5, 0.5, 0.5), "LAB")
+    places = [((0, 0, -480), None), ((0, 0, 480), None), ((-480, 0, 0), ("y", 90)), ((480, 0, 0), ("y", 90)),
+              ((0, -480, 0), ("x", 90)), ((0, 480, 0), ("x", 90)), ((-250, 0, -480), None), ((250, 0, -480), None)]
+    for i, (p, r) in enumerate(places):
+        rot = None if r is None else G.gdml_rotation(**{r[0]: r[1]})
+        tank.place(ref if i in (2, 6) else pmt, np.asarray(p, float) * MM, rot, name=f"PMT_{i}", copy=i)
+    photo = O.OpticalSurface("Cathode", "dielectric_metal", "polished", efficiency=0.9, rindex=2.7, kindex=1.5)
+    metal = O.OpticalSurface("RefCathode", "dielectric_metal", "polished", reflectivity=0.5, efficiency=0.8)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.5, sigma_alpha=0.2, specularlobe=0.5)
+    borders = [("TankLV", f"PMT_{i}", metal if i in (2, 6) else photo) for i in range(8)]
+    return D.build(tank, {"LAB": lab, "Photocathode": cathode}, borders=borders, skins={"TankLV": wall},
+                   sensors={"pmt": "PMT", "ref": "RefPMT"}, after_tracking=("pmt",) if after_tracking else ())
+
+
 def scintillator_cube(mie=2.0, wls=1.0, rayleigh=5.0, profile="exponential") -> D.Detector:
     """Return the tutorial tank's geometry filled with a synthetic liquid scintillator whose bulk has all three of
     Geant4's channels: Rayleigh, Mie (G4OpMieHG, MIEHG ``mie`` m, forward 0.9, backward 0.3, forward ratio 0.8) and a

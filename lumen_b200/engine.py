@@ -49,10 +49,21 @@ class DeviceTallies:
         t.counts = ctypes.cast(ctypes.c_void_p(self.counts.data_ptr()), A.c_u64p)
         self.c = t
 
+    def attach_groups(self, groups, capacity: int):
+        """Fill the readout groups ``groups`` (a ``lumen_b200.readout.GroupCells`` on this device) from a records
+        scratch of ``capacity`` deposits (a trace whose deposits outgrow it raises ``RecordsOverflow``)."""  # noqa: D205, D209
+        self.groups = groups
+        self.records = torch.empty((max(int(capacity), 1), A.REC_WORDS), dtype=torch.int32,
+                                   device=self.arrival.device)  # fmt: skip
+        groups.attach(self.c, self.records, self.records.shape[0])
+        return self
+
     def zero_(self):
         for v in (self.arrival, self.arrival_t, self.arrival2, self.hist, self.jac, self.health, self.counts):
             if v is not None:
                 v.zero_()
+        if getattr(self, "groups", None) is not None:
+            self.groups.zero_()
         return self
 
 

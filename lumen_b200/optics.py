@@ -129,6 +129,8 @@ class OpticalSurface:
     specularspike: object = None
     specularlobe: object = None
     backscatter: object = None
+    rindex: object = None  # a dielectric_metal surface's complex index (RINDEX, KINDEX): a photocathode
+    kindex: object = None
 
 
 ABSORBER = OpticalSurface("__absorber__", "dielectric_metal", "polished", reflectivity=0.0)
@@ -145,11 +147,29 @@ class Row:
     cols: dict = field(default_factory=dict)  # column -> table
     name: str = ""
     sensor: bool = False
+    per_normal: int = 0  # read for a sensor model applying its QE after tracking: eff 1, deposits carry 1 / A_n
 
 
-def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
-    """Return the row of a Geant4 surface (types.py:445-493 types, :557 no_detection)."""
+def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=None) -> Row:
+    """Return the row of a Geant4 surface (types.py:445-493 types, :557 no_detection); ``entry_eff``: a sensor's
+    detection on entry instead of EFFICIENCY (1 where its sensor model applies the QE after tracking,
+    src/lumen/rules/sensors.py:29 entry_efficiency)."""
     eff = surf.efficiency if (sensor and surf.efficiency is not None) else 0.0
+    if sensor and entry_eff is not None:
+        eff = float(entry_eff)
+    if surf.type == "dielectric_dielectric" and surf.finish in ("polishedfrontpainted", "groundfrontpainted"):
+        # PAINTED_T (types.py:483): R specular (polished) or Lambertian (ground), T straight, the rest absorbed
+        cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
+                "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff,
+                "p_spike": 1.0 if surf.finish == "polishedfrontpainted" else 0.0, "p_lobe": 0.0, "p_back": 0.0}  # fmt: skip
+        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+    if surf.type == "dielectric_metal" and (surf.rindex is not None or surf.kindex is not None):
+        # PHOTOCATHODE (types.py:455): the complex index's Fresnel reflectance, specular; the rest detected with eff
+        if surf.rindex is None or surf.kindex is None or surf.finish != "polished":
+            raise NotImplementedError(f"surface {surf.name}: a complex index needs RINDEX and KINDEX, polished")
+        cols = {"nr": surf.rindex, "nk": surf.kindex, "eff": eff,
+                "T": 0.0 if surf.transmittance is None else surf.transmittance}  # fmt: skip
+        return Row(MODEL_COMPLEX, far_opaque=int(far_opaque), cols=cols, name=surf.name)
     if surf.type == "dielectric_dielectric":
         if surf.finish != "polished" and surf.model == "glisur" and surf.polish < 1.0:
             # GLISUR_DIELECTRIC (types.py:463): the cuts, then below R the GLISUR facet path that reflects or refracts

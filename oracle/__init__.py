@@ -226,11 +226,24 @@ def host_source(src, samples):
 
 
 def trace(det, key, n, *, rows=None, source=None, samples=None, first_id=0, pool_live=None, pool_ref=None,
-          controls=None, n_events=1, n_bins=0, bin0=0.0, bin_w=1.0, records=False, threads=0):
-    """Trace photons first_id .. first_id + n - 1 on the CPU; return (Tallies, (rec_i, rec_f) or None)."""
+          controls=None, n_events=1, n_bins=0, bin0=0.0, bin_w=1.0, records=False, threads=0, groups=None,
+          deposits=0):
+    """Trace photons first_id .. first_id + n - 1 on the CPU; return (Tallies, (rec_i, rec_f) or None).
+
+    ``groups``: readout groups ({name: Grid or Group}, lumen_b200.readout): their cells in ``Tallies.groups`` (a host
+    GroupCells); ``deposits`` > 0: up to that many deposit records, in photon order and the engine's layout, in
+    ``Tallies.deposits`` ((deposits, LUMEN_REC_WORDS) uint32).
+    """
     d, keep = det.desc()
     c = controls or A.controls()
     T = Tallies(det.n_sensor, n_events, n_bins, bin0, bin_w, c.n_grad)
+    T.groups = T.deposits = None
+    if groups:
+        from lumen_b200.readout import GroupCells
+
+        T.groups = GroupCells(det, groups, n_events)
+        T.deposits = np.zeros((deposits, A.REC_WORDS), np.uint32) if deposits else None
+        T.groups.attach(T.c, T.deposits, deposits)
     rr, rkeep = host_rows(rows) if rows is not None else (None, None)
     ss, skeep = host_source(source, samples or n) if source is not None else (None, None)
     live = None if pool_live is None else A.np_f32(pool_live)

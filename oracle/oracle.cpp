@@ -16,11 +16,13 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "physics.h"
 #include "media.h"
 #include "rng.h"
+#include "readout.h"
 
 #define O_SOURCE_STREAM 0xFFFFFFFFu
 #define O_POL_STREAM 0x9017u
@@ -47,6 +49,7 @@ typedef struct OPhoton {
   int vol, srf;
   float sn[3];
   int nz, cls;
+  int gen; /* re-emissions so far (state.py Photon.gen) */
   float dw[O_MAXG];
 } OPhoton;
 
@@ -56,6 +59,7 @@ typedef struct ODep {
   float fates[8]; /* lost, abandoned, escaped, distance_cut, absorbed_bulk, absorbed_surface, rouletted, reweighted */
   float pushed;
   float dq[O_MAXG];
+  ORec rec; /* at a sensor deposit: what the readout groups read (step.py:546) */
 } ODep;
 
 static inline float o_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0.0f; }
@@ -235,6 +239,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   float lost = (q.hit && ph->alive && row < 0 && !scatter) ? ph->w * rr * att_if : 0.0f;
   /* _event: a bulk event or the drawn surface outcome (step.py:439) */
   float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_sn[3], nx_er[3], nx_ei[3], nx_lam = ph->lam;
+  int nx_gen = ph->gen;
   float nx_dw[O_MAXG];
   int nx_cls, nx_ok, nx_far = 0;
   float fates0, fates1, fates2, wr;
@@ -302,6 +307,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
       y_r = em.w_r;
       delay = em.delay;
       nx_lam = em.lam;
+      nx_gen = ph->gen + 1; /* medium.py:126: the WLS channel re-emits */
       for (int p = 0; p < P; ++p)
         if (ty == R->gt[p]) dyld[p] = em.dyield;
     }
@@ -487,6 +493,21 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   dep->sensor = at_if ? sensor_q : -1;
   dep->time = time;
   dep->lam = ph->lam;
+  if (dep->sensor >= 0) { /* step.py:687 _local: the crossing point, direction and normal; the sensor's volume */
+    ORec* rc = &dep->rec;
+    rc->sensor = dep->sensor;
+    rc->q = dep->q;
+    rc->time = time;
+    rc->lam = ph->lam;
+    rc->gen = ph->gen;
+    rc->vol = q.vol_after;
+    for (int a = 0; a < 3; ++a) { rc->x[a] = ph->x[a] + dist * ph->d[a]; rc->d[a] = ph->d[a]; rc->n[a] = q.normal[a]; }
+    rc->inv_an = 1.0f;
+    if (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL]) {
+      float an = o_normal_absorptance(D, R->live, row, ph->lam, ml.n, q.normal);
+      rc->inv_an = an > 0.0f ? 1.0f / an : 0.0f;
+    }
+  }
   dep->fates[0] = lost;
   dep->fates[1] = abandoned;
   dep->fates[2] = escaped;
@@ -500,6 +521,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   for (int a = 0; a < 3; ++a) { ph->x[a] = nx_x[a]; ph->d[a] = nx_d[a]; ph->er[a] = nx_er[a]; ph->ei[a] = nx_ei[a]; }
   ph->t = ph->t + nx_dtime;
   ph->lam = nx_lam;
+  ph->gen = nx_gen;
   ph->w = alive ? w_new : 0.0f;
   ph->wr = alive ? wr_new : 0.0f;
   for (int p = 0; p < P; ++p) ph->dw[p] = alive ? dw_new[p] : 0.0f;
@@ -588,9 +610,20 @@ static void o_flush2(OTally* T, int e, OPhotonSums* ps, int j) {
   T->arrival2[(size_t)e * T->S_ + ps->sensor[j]] += ps->sum[j] * ps->sum[j];
 }
 
+/* a thread's readout groups: the cells, and the photons' records when the caller asks for them (photon id, record,
+   the photon's row weight and event) */
+typedef struct OGroupCtx {
+  const LumenTallies* out;
+  OGroupT T;
+  int keep;
+  std::vector<int64_t> photon;
+  std::vector<ORec> recs;
+  std::vector<std::pair<float, int>> w0_ev;
+} OGroupCtx;
+
 /* one photon's loop (run.py:307 item): begin, steps until it ends or reaches the vertex guard */
 static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTally* T, int32_t* rec_i,
-                     float* rec_f) {
+                     float* rec_f, OGroupCtx* gc) {
   const OScene* S = &R->S;
   OPhoton ph;
   memset(&ph, 0, sizeof(ph));
@@ -615,6 +648,7 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
   int n_dep = 0, first_sensor = -1;
   double sum_q = 0.0, sum_qt = 0.0;
   long long steps = 0;
+  std::vector<ORec> recs;
   while (ph.alive && ph.vertex < R->max_vertices) {
     ODep dep;
     o_step(R, &ph, pkey, &dep);
@@ -647,6 +681,7 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
       }
       ps.sum[j] += v;
       n_dep++;
+      if (gc) recs.push_back(dep.rec);
       if (first_sensor < 0) first_sensor = s;
       sum_q += (double)dep.q;
       sum_qt += (double)dep.q * (double)dep.time;
@@ -654,6 +689,15 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
     }
   }
   for (int j = 0; j < ps.n; ++j) o_flush2(T, e, &ps, j);
+  if (gc && !recs.empty()) {
+    if (e >= 0 && e < T->E) o_bin_photon(R->S.D, gc->out, recs, w0, e, T->S_, &gc->T);
+    if (gc->keep)
+      for (const ORec& rc : recs) {
+        gc->photon.push_back(gid);
+        gc->recs.push_back(rc);
+        gc->w0_ev.push_back({(float)w0, e});
+      }
+  }
   for (int k = 0; k < 8; ++k) T->health[k] += acc[k] * w0;
   double trunc = ph.alive ? (double)ph.w * w0 : 0.0;
   T->health[LUMEN_H_TRUNCATED] += trunc;
@@ -962,6 +1006,14 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
   const int Sn = D->n_sensor > 0 ? D->n_sensor : 1, E = out->n_events > 0 ? out->n_events : 1;
   int nth = threads > 0 ? threads : omp_get_max_threads();
   std::vector<OTally> parts(nth);
+  const int groups = out->n_groups > 0;
+  if (groups && (out->n_groups > LUMEN_MAX_GROUPS || !out->groups)) return LUMEN_ERR_ARG;
+  std::vector<OGroupCtx> gparts(groups ? nth : 0);
+  for (auto& G : gparts) {
+    G.out = out;
+    G.keep = out->records != 0;
+    o_groups_init(&G.T, out, E, Sn);
+  }
   for (auto& T : parts) {
     T.S_ = Sn; T.E = E; T.nb = out->hist ? out->n_bins : 0; T.P = c->n_grad;
     T.bin0 = out->bin0; T.bin_w = out->bin_w;
@@ -977,7 +1029,47 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
     ORow r;
     o_row_of(rows, src, key, first_id, i, &r);
     o_photon(&R, &r, key, first_id + i, &parts[omp_get_thread_num()], rec_i ? rec_i + 5 * i : 0,
-             rec_f ? rec_f + 4 * i : 0);
+             rec_f ? rec_f + 4 * i : 0, groups ? &gparts[omp_get_thread_num()] : 0);
+  }
+  if (groups) { /* the threads' cells, and the records in photon order (the engine's layout, LUMEN_REC_WORDS each) */
+    for (auto& G : gparts) {
+      for (int g = 0; g < out->n_groups; ++g) {
+        const LumenGroup& LG = out->groups[g];
+        for (size_t k = 0; k < G.T.charge[g].size(); ++k) { LG.charge[k] += G.T.charge[g][k]; LG.charge2[k] += G.T.charge2[g][k]; }
+        for (size_t k = 0; k < G.T.time[g].size(); ++k) LG.time[k] += G.T.time[g][k];
+        for (size_t k = 0; k < G.T.over_q[g].size(); ++k) { LG.over_q[k] += G.T.over_q[g][k]; LG.over_qt[k] += G.T.over_qt[g][k]; }
+      }
+      if (out->pe2) for (size_t k = 0; k < G.T.pe2.size(); ++k) out->pe2[k] += G.T.pe2[k];
+    }
+    std::vector<std::pair<int64_t, std::pair<int, size_t>>> order; /* (photon, (thread, index)) */
+    for (int t = 0; t < (int)gparts.size(); ++t)
+      for (size_t k = 0; k < gparts[t].recs.size(); ++k) order.push_back({gparts[t].photon[k], {t, k}});
+    std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    if (out->counts) out->counts[LUMEN_C_RECORDS] += (unsigned long long)order.size();
+    if (out->records) {
+      uint32_t* w = (uint32_t*)out->records;
+      int64_t n_out = (int64_t)order.size() < out->rec_capacity ? (int64_t)order.size() : out->rec_capacity;
+      for (int64_t k = 0; k < n_out; ++k) {
+        const OGroupCtx& G = gparts[order[k].second.first];
+        const size_t j = order[k].second.second;
+        const ORec& rc = G.recs[j];
+        uint32_t* o = w + k * LUMEN_REC_WORDS;
+        float f[LUMEN_REC_WORDS];
+        memset(f, 0, sizeof(f));
+        memcpy(o, f, sizeof(f));
+        const int first = k == 0 || order[k - 1].first != order[k].first;
+        const int last = k + 1 == (int64_t)order.size() || order[k + 1].first != order[k].first;
+        int32_t iv[4] = {first ? -1 : (int32_t)(k - 1), rc.sensor, rc.gen, rc.vol};
+        memcpy(o + 0, &iv[0], 4); memcpy(o + 1, &iv[1], 4); memcpy(o + 6, &iv[2], 4); memcpy(o + 7, &iv[3], 4);
+        memcpy(o + 2, &rc.q, 4); memcpy(o + 3, &rc.time, 4); memcpy(o + 4, &rc.lam, 4); memcpy(o + 5, &rc.inv_an, 4);
+        memcpy(o + 8, rc.x, 12); memcpy(o + 11, rc.d, 12); memcpy(o + 14, rc.n, 12);
+        if (last) {
+          o[17] = 1u;
+          memcpy(o + 18, &G.w0_ev[j].first, 4);
+          memcpy(o + 19, &G.w0_ev[j].second, 4);
+        }
+      }
+    }
   }
   for (auto& T : parts) {
     for (size_t k = 0; k < T.arrival.size(); ++k) {
