@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 6
+#define LUMEN_B200_ABI_VERSION 7
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -173,8 +173,12 @@ typedef struct LumenRows {
    the call belongs to the event e with ev_first[e] <= first_id + i < ev_first[e + 1]. */
 enum { LUMEN_SRC_POINT = 0,   /* isotropic point (sources/point.py:73): ev_f = x y z, time */
        LUMEN_SRC_TRACK = 1,   /* straight track emitting on a cone: ev_f = x y z (start), ux uy uz (unit), length, time */
-       LUMEN_SRC_SCINT = 2 }; /* isotropic scintillation point with a two-exponential profile: ev_f = x y z, time */
-enum { LUMEN_EV_F = 8 };
+       LUMEN_SRC_SCINT = 2,   /* isotropic scintillation point with a two-exponential profile: ev_f = x y z, time */
+       LUMEN_SRC_CHERENKOV = 3 }; /* a charged segment's Cherenkov light (src/lumen/sources/cherenkov.py:65
+                                    CherenkovSegment): ev_f = x y z (start), ux uy uz (unit), length, time, beta,
+                                    charge, the event's photons; the medium's RINDEX table `rindex_tab` read at the live
+                                    values; wavelengths over [lam0, lam1] (its span) */
+enum { LUMEN_EV_F = 12 };
 typedef struct LumenSource {
   int32_t kind;
   int32_t n_events;
@@ -184,6 +188,8 @@ typedef struct LumenSource {
   float lam0, lam1;         /* nm: a fixed wavelength (lam1 <= lam0) or uniform in [lam0, lam1] */
   float cone_cos;           /* LUMEN_SRC_TRACK: cosine of the cone half-angle */
   float tau1, tau2, frac1;  /* LUMEN_SRC_SCINT: decay times (ns) and the first component's share */
+  int32_t rindex_tab;       /* LUMEN_SRC_CHERENKOV: the medium's RINDEX table (a gradient parameter it may not be) */
+  int32_t reserved;
 } LumenSource;
 
 /* ------------------------------------------------------------------------------------------ the controls */

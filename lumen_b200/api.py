@@ -129,7 +129,7 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
         if samples is None:
             raise ValueError("simulate: give samples")
         n = int(samples)
-        dsrc, drows, n_ev = DeviceSource(source, n, eng.device), None, source.events()
+        dsrc, drows, n_ev = DeviceSource(source, n, eng.device, det), None, source.events()
         total = dsrc.total
     if total > MAX_ID:
         raise ValueError(f"a run traces at most {MAX_ID} photons (int32 ids)")
@@ -166,7 +166,7 @@ def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):
     h = T.health.cpu().numpy()
     cnt = T.counts.cpu().numpy()
     if n_ev > 1:
-        per_ev = np.diff(source.arrays(samples)["ev_first"]) if not isinstance(source, FromArrays) else \
+        per_ev = np.diff(source.arrays(samples, det)["ev_first"]) if not isinstance(source, FromArrays) else \
             np.bincount(np.asarray(source.event), minlength=n_ev)  # fmt: skip
         nn = per_ev[:, None].astype(np.float64)
     else:

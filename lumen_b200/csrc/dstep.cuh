@@ -635,7 +635,11 @@ L_DEV int d_event_of(const int64_t* first, int n_ev, int64_t gid) {
   return lo;
 }
 
-L_DEV void d_source_row(const LumenSource& src, Key key, int64_t gid, Row& r) {
+// 2 pi alpha (Frank-Tamm), the product formed in double and rounded once, as the reference's constant expression
+#define D_TWO_PI_ALPHA ((float)(6.283185307179586 * (1.0 / 137.035999084)))
+
+L_DEV void d_source_row(const DScene& S, const float* __restrict__ pool, const LumenSource& src, Key key, int64_t gid,
+                        Row& r) {
   Key sk = fold_in(key, D_SOURCE_STREAM);
   Key rk = fold_in(fold_in(sk, (uint32_t)gid), 0u);
   int e = d_event_of(src.ev_first, src.n_events, gid);
@@ -659,6 +663,35 @@ L_DEV void d_source_row(const LumenSource& src, Key key, int64_t gid, Row& r) {
     r.t = __ldg(f + 7) + along / D_C_VACUUM;
     r.lam = src.lam1 > src.lam0 ? src.lam0 + (src.lam1 - src.lam0) * u2 : src.lam0;
     float ad = d_dot(ax, r.d);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.er[a] = ad * r.d[a] - ax[a];
+    d_unit(r.er);
+    return;
+  }
+  if (src.kind == LUMEN_SRC_CHERENKOV) {  // cherenkov.py:33 cone: uniforms lam, pos, phi
+    float u0 = uniform(rk, 0), u1 = uniform(rk, 1), u2 = uniform(rk, 2);
+    float ax[3] = {__ldg(f + 3), __ldg(f + 4), __ldg(f + 5)};
+    const float len = __ldg(f + 6), beta = __ldg(f + 8), charge = __ldg(f + 9), samples = __ldg(f + 10);
+    float zq = 1.0f / src.lam0 - 1.0f / src.lam1;
+    float lam = 1.0f / (1.0f / src.lam0 - u0 * zq);  // ~ 1 / lam^2 over the index table's span
+    float n = d_tab(S, pool, src.rindex_tab, D_HC / lam);
+    float bn2 = beta * beta * n * n;
+    int emits = 1.0f - 1.0f / bn2 > 0.0f;
+    float s = emits ? 1.0f - 1.0f / bn2 : 0.0f;
+    r.w0 = D_TWO_PI_ALPHA * (charge * charge) * len * s * zq / samples * 1e9f;  // photons per nm -> per m
+    float cos_c = emits ? 1.0f / (beta * n) : 1.0f;
+    float sq = 1.0f - cos_c * cos_c;
+    float sin_c = sq > 0.0f ? sqrtf(sq) : 0.0f;
+    float sp, cp;
+    l_sincos2pi(u2, &sp, &cp);
+    float l[3] = {sin_c * cp, sin_c * sp, cos_c};
+    d_to_world(l, ax, r.d);
+    float xs = u1 * len;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.x[a] = __ldg(f + a) + xs * ax[a];
+    r.t = __ldg(f + 7) + xs / (beta * D_C_VACUUM);
+    r.lam = lam;
+    float ad = d_dot(ax, r.d);  // Geant4's polarisation (polar.py:81 cherenkov)
 #pragma unroll
     for (int a = 0; a < 3; ++a) r.er[a] = ad * r.d[a] - ax[a];
     d_unit(r.er);

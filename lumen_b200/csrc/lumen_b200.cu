@@ -166,7 +166,7 @@ __device__ __forceinline__ int deposit(const Tally& T, int e, const Dep& dep, co
 
 __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
   if (L.use_rows) d_rows_row(L.rows, i, r);
-  else d_source_row(L.src, L.key, L.first_id + i, r);
+  else d_source_row(L.R.S, L.R.live, L.src, L.key, L.first_id + i, r);
 }
 
 // The persistent photon loop: a lane refill per step (src/lumen/run.py:81 SCHEDULE = "step").
@@ -670,7 +670,17 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   } else {
     if (source->n_events < 1 || !source->ev_f || !source->ev_first || !source->ev_w)
       return set_err(LUMEN_ERR_ARG, "source: events are missing");
-    if (source->kind < 0 || source->kind > 2) return set_err(LUMEN_ERR_ARG, "source: unknown kind");
+    if (source->kind < 0 || source->kind > LUMEN_SRC_CHERENKOV) return set_err(LUMEN_ERR_ARG, "source: unknown kind");
+    if (source->kind == LUMEN_SRC_CHERENKOV) {
+      if (source->rindex_tab < 0 || source->rindex_tab >= (int)(sc->tab.size() / 2))
+        return set_err(LUMEN_ERR_ARG, "source: a Cherenkov segment needs its medium's RINDEX table");
+      if (!(source->lam0 > 0.0f) || !(source->lam1 >= source->lam0))
+        return set_err(LUMEN_ERR_ARG, "source: a Cherenkov segment's wavelengths span [lam0, lam1] nm, lam0 > 0");
+      for (int p = 0; p < (c ? c->n_grad : 0); ++p)
+        if (c->grad_tab[p] == source->rindex_tab)
+          return set_err(LUMEN_ERR_NOT_SUPPORTED, "the index of a Cherenkov segment's medium moves its photons' "
+                                                  "directions: a pathwise derivative, not a reweighting one");
+    }
     L.src = *source;
   }
   L.key.k0 = k0;

@@ -70,8 +70,8 @@ class DeviceTallies:
 class DeviceSource:
     """A procedural source's arrays on the device (LumenSource layout)."""
 
-    def __init__(self, src, samples, device="cuda"):
-        a = src.arrays(samples)
+    def __init__(self, src, samples, device="cuda", det=None):
+        a = src.arrays(samples, det)
         self.ev_f = torch.as_tensor(np.ascontiguousarray(a["ev_f"], np.float32), device=device)
         self.ev_first = torch.as_tensor(np.ascontiguousarray(a["ev_first"], np.int64), device=device)
         self.ev_w = torch.as_tensor(np.ascontiguousarray(a["ev_w"], np.float32), device=device)
@@ -80,6 +80,7 @@ class DeviceSource:
         s.ev_f, s.ev_first, s.ev_w = _f32p(self.ev_f), _i64p(self.ev_first), _f32p(self.ev_w)
         s.lam0, s.lam1, s.cone_cos = a["lam0"], a["lam1"], a["cone_cos"]
         s.tau1, s.tau2, s.frac1 = a["tau1"], a["tau2"], a["frac1"]
+        s.rindex_tab = a.get("rindex_tab", -1)
         self.c = s
         self.n_events = len(a["ev_w"])
         self.total = int(a["ev_first"][-1])

@@ -10,6 +10,8 @@ assigns photon ids to events by contiguous ranges of uneven sizes (``counts``), 
 - ``Tracks(start, direction, length, cone_angle, ...)``: straight tracks emitting on a cone of fixed half-angle about
   their direction (a Cherenkov-like source; linear polarisation in the plane of track and photon, polar.py:89).
 - ``Scintillation(position, tau=(tau1, tau2), fraction)``: isotropic points with a two-exponential time profile.
+- ``CherenkovSegment(material, start, direction, length, beta, charge, time)``: the Frank-Tamm light of charged
+  segments (src/lumen/sources/cherenkov.py:65), one event per segment, on the medium's live RINDEX.
 - ``FromArrays(x, d, t, lam, w, pol)``: explicit rows (src/lumen/sources/arrays.py:24).
 """
 
@@ -63,7 +65,7 @@ class Point(Source):
         base[: samples - base.sum()] += 1
         return base
 
-    def arrays(self, samples):
+    def arrays(self, samples, det=None):
         e = self.events()
         pos = _events(self.position, e, 3)
         ev_f = np.zeros((e, A.EV_F), np.float32)
@@ -98,7 +100,7 @@ class Tracks(Source):
         base[: samples - base.sum()] += 1
         return base
 
-    def arrays(self, samples):
+    def arrays(self, samples, det=None):
         e = self.events()
         ev_f = np.zeros((e, A.EV_F), np.float32)
         ev_f[:, 0:3] = _events(self.start, e, 3)
@@ -135,7 +137,7 @@ class Scintillation(Source):
         base[: samples - base.sum()] += 1
         return base
 
-    def arrays(self, samples):
+    def arrays(self, samples, det=None):
         e = self.events()
         ev_f = np.zeros((e, A.EV_F), np.float32)
         ev_f[:, 0:3] = _events(self.position, e, 3)
@@ -143,6 +145,62 @@ class Scintillation(Source):
         out = _common(self, A.SRC_SCINT, ev_f, self.counts(samples), self.n_photons)
         out.update(tau1=float(self.tau[0]), tau2=float(self.tau[1]), frac1=float(self.fraction))
         return out
+
+
+HC = 1239.84198433200208  # eV nm (src/lumen/units.py:20)
+
+
+@dataclass
+class CherenkovSegment(Source):
+    """A charge ``charge`` (e) from ``start`` (m) along the unit ``direction`` for ``length`` m at ``beta`` in
+    ``material``, at ``time`` ns at the start (src/lumen/sources/cherenkov.py:65): cos theta = 1 / (beta n(lam)), the
+    wavelength ~ 1 / lam^2 over the span of the medium's RINDEX table, the weight Frank-Tamm's photons per sample
+    2 pi alpha z^2 L (1 - 1 / (beta n)^2)_+ (1 / lam_min - 1 / lam_max) / samples, Geant4's polarisation. Several
+    segments (rows of start, direction, length, beta, charge, time): one event each."""  # noqa: D205
+
+    material: str
+    start: object = (0.0, 0.0, 0.0)
+    direction: object = (0.0, 0.0, 1.0)
+    length: object = 1.0
+    beta: object = 1.0
+    charge: object = 1.0
+    time: object = 0.0
+    counts_: object = None
+
+    def events(self):
+        return len(np.asarray(self.start, np.float32).reshape(-1, 3))
+
+    def counts(self, samples):
+        if self.counts_ is not None:
+            return np.asarray(self.counts_, np.int64)
+        e = self.events()
+        base = np.full(e, samples // e, np.int64)
+        base[: samples - base.sum()] += 1
+        return base
+
+    def arrays(self, samples, det=None):
+        if det is None:
+            raise ValueError("CherenkovSegment: the detector holds its medium's RINDEX (pass det)")
+        name = f"media/{self.material}/index"
+        if name not in det.params_index:
+            raise ValueError(f"CherenkovSegment: no medium {self.material!r} with an index in the detector")
+        tab = det.params_index[name]
+        off, k = (int(v) for v in det.arrays["tab"][tab])
+        e = np.asarray(det.pool[off:off + k], np.float32)  # the table's knots (energies, eV)
+        lam0, lam1 = np.float32(HC) / e.max(), np.float32(HC) / e.min()  # cherenkov.py:56 bounds
+        n_ev = self.events()
+        cnt = self.counts(samples)
+        ev_f = np.zeros((n_ev, A.EV_F), np.float32)
+        ev_f[:, 0:3] = _events(self.start, n_ev, 3)
+        u = np.asarray(_events(self.direction, n_ev, 3), np.float64)
+        ev_f[:, 3:6] = u / np.linalg.norm(u, axis=1, keepdims=True)
+        for col, v in ((6, self.length), (7, self.time), (8, self.beta), (9, self.charge)):
+            ev_f[:, col] = np.broadcast_to(np.asarray(v, np.float32), (n_ev,))
+        ev_f[:, 10] = cnt.astype(np.float32)  # the event's samples (the weight's divisor)
+        first = np.zeros(n_ev + 1, np.int64)
+        first[1:] = np.cumsum(cnt)
+        return dict(kind=A.SRC_CHERENKOV, ev_f=ev_f, ev_first=first, ev_w=np.ones(n_ev, np.float32),
+                    lam0=float(lam0), lam1=float(lam1), cone_cos=1.0, tau1=0.0, tau2=0.0, frac1=0.0, rindex_tab=tab)  # fmt: skip
 
 
 def _common(src, kind, ev_f, cnt, n_photons):

@@ -58,8 +58,8 @@ def lib():
                                        ctypes.c_float, ctypes.c_int32, ctypes.c_float, ctypes.c_uint32,
                                        ctypes.c_uint32, ctypes.c_int64, A.c_f32p]  # fmt: skip
         L.lumen_oracle_group_index.argtypes = [A.c_f32p, A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
-        L.lumen_oracle_source_rows.argtypes = [P(A.LumenSource), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int64,
-                                               ctypes.c_int64, A.c_f32p, A.c_i32p]
+        L.lumen_oracle_source_rows.argtypes = [P(A.LumenSceneDesc), A.c_f32p, P(A.LumenSource), ctypes.c_uint32,
+                                               ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64, A.c_f32p, A.c_i32p]
         del vp
         _lib = L
     return _lib
@@ -212,9 +212,9 @@ def host_rows(rows: dict):
     return r, keep
 
 
-def host_source(src, samples):
+def host_source(src, samples, det=None):
     """Return (LumenSource over host arrays, keepalive) of a lumen_b200.sources.Source's arrays."""
-    a = src.arrays(samples)
+    a = src.arrays(samples, det)
     keep = {"ev_f": A.np_f32(a["ev_f"]), "ev_first": np.ascontiguousarray(a["ev_first"], np.int64),
             "ev_w": A.np_f32(a["ev_w"])}  # fmt: skip
     s = A.LumenSource()
@@ -222,6 +222,7 @@ def host_source(src, samples):
     s.ev_f, s.ev_first, s.ev_w = A.fptr(keep["ev_f"]), keep["ev_first"].ctypes.data_as(A.c_i64p), A.fptr(keep["ev_w"])
     s.lam0, s.lam1, s.cone_cos = a["lam0"], a["lam1"], a["cone_cos"]
     s.tau1, s.tau2, s.frac1 = a["tau1"], a["tau2"], a["frac1"]
+    s.rindex_tab = a.get("rindex_tab", -1)
     return s, keep
 
 
@@ -245,7 +246,7 @@ def trace(det, key, n, *, rows=None, source=None, samples=None, first_id=0, pool
         T.deposits = np.zeros((deposits, A.REC_WORDS), np.uint32) if deposits else None
         T.groups.attach(T.c, T.deposits, deposits)
     rr, rkeep = host_rows(rows) if rows is not None else (None, None)
-    ss, skeep = host_source(source, samples or n) if source is not None else (None, None)
+    ss, skeep = host_source(source, samples or n, det) if source is not None else (None, None)
     live = None if pool_live is None else A.np_f32(pool_live)
     ref = None if pool_ref is None else A.np_f32(pool_ref)
     rec_i = np.zeros((n, 5), np.int32) if records else None
@@ -258,11 +259,17 @@ def trace(det, key, n, *, rows=None, source=None, samples=None, first_id=0, pool
     return T, ((rec_i, rec_f) if records else None)
 
 
-def source_rows(source, key, n, first_id=0, samples=None):
-    ss, skeep = host_source(source, samples or n)
+def source_rows(source, key, n, first_id=0, samples=None, det=None, pool=None):
+    """The emission rows of a procedural source (n, 15: x, d, t, lam, w0, er, ei) and their events; ``det`` (and
+    ``pool``, the live values: default the detector's) for a Cherenkov segment's medium."""  # noqa: D205, D209
+    ss, skeep = host_source(source, samples or n, det)
+    d, dkeep = det.desc() if det is not None else (None, None)
+    pl = None if pool is None else A.np_f32(pool)
     out_f = np.zeros((n, 15), np.float32)
     ev = np.zeros(n, np.int32)
-    lib().lumen_oracle_source_rows(ctypes.byref(ss), key[0], key[1], first_id, n, A.fptr(out_f), A.iptr(ev))
+    st = lib().lumen_oracle_source_rows(ctypes.byref(d) if d is not None else None, A.fptr(pl), ctypes.byref(ss),
+                                        key[0], key[1], first_id, n, A.fptr(out_f), A.iptr(ev))  # fmt: skip
+    assert st == 0, f"oracle status {st}"
     return out_f, ev
 
 

@@ -555,7 +555,11 @@ static int o_event_of(const int64_t* first, int n_ev, int64_t gid) {
 }
 
 /* photon gid of a procedural source (uniforms of vertex 0 of its own key under the source stream) */
-static void o_source_row(const LumenSource* src, OKey key, int64_t gid, ORow* r) {
+/* 2 pi alpha for Frank-Tamm (units.py:16 FINE_STRUCTURE): the product in double, rounded once */
+static const float O_TWO_PI_ALPHA = (float)(6.283185307179586 * (1.0 / 137.035999084));
+
+static void o_source_row(const LumenSceneDesc* D, const float* pool, const LumenSource* src, OKey key, int64_t gid,
+                         ORow* r) {
   OKey sk = o_fold_in(key, O_SOURCE_STREAM);
   OKey rk = o_fold_in(o_fold_in(sk, (uint32_t)gid), 0u);
   int e = o_event_of(src->ev_first, src->n_events, gid);
@@ -577,6 +581,33 @@ static void o_source_row(const LumenSource* src, OKey key, int64_t gid, ORow* r)
     r->t = f[7] + along / O_C_VACUUM;
     r->lam = src->lam1 > src->lam0 ? src->lam0 + (src->lam1 - src->lam0) * u2 : src->lam0;
     /* Cherenkov polarisation: in the plane of the axis and d, perpendicular to d (polar.py:89 cherenkov) */
+    float ad = o_dot(ax, r->d);
+    for (int a = 0; a < 3; ++a) r->er[a] = ad * r->d[a] - ax[a];
+    o_unit(r->er);
+    return;
+  }
+  if (src->kind == LUMEN_SRC_CHERENKOV) { /* cherenkov.py:33 cone: a Frank-Tamm photon of the segment */
+    float u_lam = o_uniform(rk, 0), u_pos = o_uniform(rk, 1), u_phi = o_uniform(rk, 2);
+    const float* ax = f + 3;
+    const float len = f[6], beta = f[8], charge = f[9], samples = f[10];
+    const float zq = 1.0f / src->lam0 - 1.0f / src->lam1;
+    const float lam = 1.0f / (1.0f / src->lam0 - u_lam * zq);
+    const float n = o_tab(D, pool, src->rindex_tab, O_HC / lam, 0);
+    const float bn2 = beta * beta * n * n;
+    const int emits = 1.0f - 1.0f / bn2 > 0.0f;
+    const float s = emits ? 1.0f - 1.0f / bn2 : 0.0f;
+    r->w0 = O_TWO_PI_ALPHA * (charge * charge) * len * s * zq / samples * 1e9f;
+    const float cos_c = emits ? 1.0f / (beta * n) : 1.0f;
+    const float sq = 1.0f - cos_c * cos_c;
+    const float sin_c = sq > 0.0f ? sqrtf(sq) : 0.0f;
+    float sp, cp;
+    o_sincos2pi(u_phi, &sp, &cp);
+    float l[3] = {sin_c * cp, sin_c * sp, cos_c};
+    o_to_world(l, ax, r->d);
+    const float xs = u_pos * len;
+    for (int a = 0; a < 3; ++a) r->x[a] = f[a] + xs * ax[a];
+    r->t = f[7] + xs / (beta * O_C_VACUUM);
+    r->lam = lam;
     float ad = o_dot(ax, r->d);
     for (int a = 0; a < 3; ++a) r->er[a] = ad * r->d[a] - ax[a];
     o_unit(r->er);
@@ -753,7 +784,8 @@ static void o_run_init(ORun* R, const LumenSceneDesc* D, const float* live, cons
 }
 
 /* host rows in the layout of LumenRows (every pointer a host array) */
-static void o_row_of(const LumenRows* rows, const LumenSource* src, OKey key, int64_t first_id, int64_t i, ORow* r) {
+static void o_row_of(const ORun* R, const LumenRows* rows, const LumenSource* src, OKey key, int64_t first_id,
+                     int64_t i, ORow* r) {
   if (rows) {
     r->x[0] = rows->x[i]; r->x[1] = rows->y[i]; r->x[2] = rows->z[i];
     r->d[0] = rows->dx[i]; r->d[1] = rows->dy[i]; r->d[2] = rows->dz[i];
@@ -764,7 +796,7 @@ static void o_row_of(const LumenRows* rows, const LumenSource* src, OKey key, in
     }
     r->event = rows->event ? rows->event[i] : 0;
   } else {
-    o_source_row(src, key, first_id + i, r);
+    o_source_row(R->S.D, R->live, src, key, first_id + i, r);
   }
 }
 
@@ -1027,7 +1059,7 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nth)
   for (int64_t i = 0; i < n; ++i) {
     ORow r;
-    o_row_of(rows, src, key, first_id, i, &r);
+    o_row_of(&R, rows, src, key, first_id, i, &r);
     o_photon(&R, &r, key, first_id + i, &parts[omp_get_thread_num()], rec_i ? rec_i + 5 * i : 0,
              rec_f ? rec_f + 4 * i : 0, groups ? &gparts[omp_get_thread_num()] : 0);
   }
@@ -1085,13 +1117,16 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
   return 0;
 }
 
-/* emission rows of a procedural source (host): x, d, t, lam, w0, er, ei, event per photon */
-int32_t lumen_oracle_source_rows(const LumenSource* src, uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
-                                 float* out_f, int32_t* out_event) {
+/* emission rows of a procedural source (host): x, d, t, lam, w0, er, ei, event per photon; D and pool (the live
+   values) are read by a Cherenkov segment only */
+int32_t lumen_oracle_source_rows(const LumenSceneDesc* D, const float* pool, const LumenSource* src, uint32_t key0,
+                                 uint32_t key1, int64_t first_id, int64_t n, float* out_f, int32_t* out_event) {
   OKey key = {key0, key1};
+  if (src->kind == LUMEN_SRC_CHERENKOV && !D) return LUMEN_ERR_ARG;
+  const float* pl = pool ? pool : (D ? D->pool : 0);
   for (int64_t i = 0; i < n; ++i) {
     ORow r;
-    o_source_row(src, key, first_id + i, &r);
+    o_source_row(D, pl, src, key, first_id + i, &r);
     float* f = out_f + 15 * i;
     for (int a = 0; a < 3; ++a) { f[a] = r.x[a]; f[3 + a] = r.d[a]; f[9 + a] = r.er[a]; f[12 + a] = r.ei[a]; }
     f[6] = r.t; f[7] = r.lam; f[8] = r.w0;

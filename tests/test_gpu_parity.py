@@ -347,3 +347,29 @@ def test_fog_box_jump_tallies_gradients_and_reference(variant, fog, built):
                     pools=(live, fog.pool))  # fmt: skip
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
     np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
+
+
+CHER = sources.CherenkovSegment("Water", start=[(0.0, 0.0, -0.2), (-0.36, 0.0, 0.0)], direction=[(0, 0, 1), (1, 0, 0)],
+                                length=[0.3, 0.12], beta=[0.99, 0.999], charge=[1.0, 2.0])  # fmt: skip
+
+
+def test_cherenkov_segments_bit_exact(toy, built):
+    """Cherenkov segments (src/lumen/sources/cherenkov.py:65): every photon's record and the two events' tallies are
+    the checker's; the gradient in the medium's index (which moves the cone) is refused."""
+    n = 1 << 14
+    eng = _engine(toy)
+    ds = DeviceSource(CHER, n, det=toy)
+    gi, gf = eng.trace_photons(KEY, n, source=ds, controls=A.controls())
+    _, (oi, of) = oracle.trace(toy, KEY, n, source=CHER, samples=n, records=True, n_events=2)
+    gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+    bad = np.flatnonzero((gi != oi).any(1) | (gf.view(np.uint32) != of.view(np.uint32)).any(1))
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}"
+    T = DeviceTallies(toy.n_sensor, 2, 50, 0.0, 1.0, 0)
+    eng.trace(KEY, n, source=ds, controls=A.controls(), tallies=T)
+    O, _ = oracle.trace(toy, KEY, n, source=CHER, samples=n, n_events=2, n_bins=50)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
+    np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-9)
+    T = DeviceTallies(toy.n_sensor, 2, 0, 0.0, 1.0, 1)
+    with pytest.raises(A.EngineError):
+        eng.trace(KEY, n, source=ds, controls=A.controls(grad_tabs=[toy.params_index["media/Water/index"]]), tallies=T)
