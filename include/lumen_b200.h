@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 7
+#define LUMEN_B200_ABI_VERSION 8
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -178,6 +178,14 @@ enum { LUMEN_SRC_POINT = 0,   /* isotropic point (sources/point.py:73): ev_f = x
                                     CherenkovSegment): ev_f = x y z (start), ux uy uz (unit), length, time, beta,
                                     charge, the event's photons; the medium's RINDEX table `rindex_tab` read at the live
                                     values; wavelengths over [lam0, lam1] (its span) */
+enum { LUMEN_SRC_SCINT_MATERIAL = 4 }; /* a material's scintillation light (src/lumen/sources/scintillation.py:100):
+                                    a flash at a point or along a charged segment; ev_f = x0 y0 z0, t0, x1 y1 z1, t1,
+                                    energy (MeV), birks (m / MeV); the material's tables in `mat` */
+/* LumenSource.mat of LUMEN_SRC_SCINT_MATERIAL: the components (1..3), the segment flag (0: a point at x0, t0), the
+   rise flag (the components' rise times), the yield per MeV table, then per component (-1 where absent) its spectrum,
+   decay time and rise time tables, then the three share yields (SCINTILLATIONYIELDi; -1: Geant4's defaults 1, 0, 0) */
+enum { LUMEN_SM_N = 0, LUMEN_SM_SEGMENT, LUMEN_SM_RISES, LUMEN_SM_YIELD, LUMEN_SM_SPEC = 4, LUMEN_SM_TAU = 7,
+       LUMEN_SM_RISE = 10, LUMEN_SM_SHARE = 13, LUMEN_SM_WORDS = 16 };
 enum { LUMEN_EV_F = 12 };
 typedef struct LumenSource {
   int32_t kind;
@@ -190,6 +198,7 @@ typedef struct LumenSource {
   float tau1, tau2, frac1;  /* LUMEN_SRC_SCINT: decay times (ns) and the first component's share */
   int32_t rindex_tab;       /* LUMEN_SRC_CHERENKOV: the medium's RINDEX table (a gradient parameter it may not be) */
   int32_t reserved;
+  int32_t mat[LUMEN_SM_WORDS]; /* LUMEN_SRC_SCINT_MATERIAL: its tables (LUMEN_SM_*; none a gradient parameter) */
 } LumenSource;
 
 /* ------------------------------------------------------------------------------------------ the controls */

@@ -40,7 +40,8 @@ HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "abso
           "reweighted", "truncated", "pushed", "start")  # fmt: skip
 COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted", "records")
 FEATURES = ("wavelength", "theta", "cos_incidence", "generation", "x", "y", "z", "rho")  # LUMEN_FEAT_* order
-SRC_POINT, SRC_TRACK, SRC_SCINT, SRC_CHERENKOV = 0, 1, 2, 3
+SRC_POINT, SRC_TRACK, SRC_SCINT, SRC_CHERENKOV, SRC_SCINT_MATERIAL = 0, 1, 2, 3, 4
+SM_N, SM_SEGMENT, SM_RISES, SM_YIELD, SM_SPEC, SM_TAU, SM_RISE, SM_SHARE, SM_WORDS = 0, 1, 2, 3, 4, 7, 10, 13, 16
 EV_F = 12
 
 
@@ -72,7 +73,7 @@ class LumenSource(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("n_events", ctypes.c_int32), ("ev_f", c_f32p), ("ev_first", c_i64p),
                 ("ev_w", c_f32p), ("lam0", ctypes.c_float), ("lam1", ctypes.c_float), ("cone_cos", ctypes.c_float),
                 ("tau1", ctypes.c_float), ("tau2", ctypes.c_float), ("frac1", ctypes.c_float),
-                ("rindex_tab", ctypes.c_int32), ("reserved", ctypes.c_int32)]  # fmt: skip
+                ("rindex_tab", ctypes.c_int32), ("reserved", ctypes.c_int32), ("mat", ctypes.c_int32 * 16)]  # fmt: skip
 
 
 class LumenControls(ctypes.Structure):

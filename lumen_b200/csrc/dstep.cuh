@@ -638,8 +638,105 @@ L_DEV int d_event_of(const int64_t* first, int n_ev, int64_t gid) {
 // 2 pi alpha (Frank-Tamm), the product formed in double and rounded once, as the reference's constant expression
 #define D_TWO_PI_ALPHA ((float)(6.283185307179586 * (1.0 / 137.035999084)))
 
-L_DEV void d_source_row(const DScene& S, const float* __restrict__ pool, const LumenSource& src, Key key, int64_t gid,
-                        Row& r) {
+// the components' shares of a material's light (scintillation.py:48 shares): one takes all; two y1 / s and the rest;
+// three y_i / s, s = y1 + y2 + y3 (Geant4's default yields 1, 0, 0)
+L_DEV void d_scint_shares(const DScene& S, const float* __restrict__ pool, const int32_t* m, float* f) {
+  int nc = m[LUMEN_SM_N];
+  float y[3];
+  for (int i = 0; i < 3; ++i) {
+    int t = m[LUMEN_SM_SHARE + i];
+    y[i] = t >= 0 ? d_tab(S, pool, t, 1.0f) : (i == 0 ? 1.0f : 0.0f);
+  }
+  float s = (y[0] + y[1]) + y[2];
+  f[0] = 1.0f; f[1] = 0.0f; f[2] = 0.0f;
+  if (nc == 2) { f[0] = y[0] / s; f[1] = 1.0f - y[0] / s; }
+  if (nc == 3) { f[0] = y[0] / s; f[1] = y[1] / s; f[2] = y[2] / s; }
+}
+
+// a photon of a material's scintillation (scintillation.py:69 flash): the component drawn at the reference shares under
+// the one defensive mixture (estimator.py:101 defensive_q) and moved to one with light (_base.py:298 lit), its
+// wavelength drawn from its reference spectrum under the defensive cover and weighted to the live one (_base.py:337),
+// an isotropic direction, the component's decay (and rise) delay, a point or a place along the segment
+L_CALL void d_scint_row(const DScene& S, const float* __restrict__ live, const float* __restrict__ ref,
+                        const LumenSource& src, const float* f, Key rk, Row& r) {
+  const int32_t* m = src.mat;
+  const int nc = m[LUMEN_SM_N], seg = m[LUMEN_SM_SEGMENT], rises = m[LUMEN_SM_RISES];
+  float fl[3], q[3];
+  d_scint_shares(S, live, m, fl);
+  d_scint_shares(S, ref, m, q);
+  int n_off = 0;
+  for (int i = 0; i < nc; ++i) n_off += q[i] <= 0.0f;
+  if (n_off > 0) {  // the defensive mixture: a component of share 0 gets e / (1 - e) / n, then all normalised
+    float eps = (float)(0.01 / 0.99) / (float)n_off, sum = 0.0f;
+    for (int i = 0; i < nc; ++i) { q[i] = q[i] <= 0.0f ? eps : q[i]; sum = i == 0 ? q[i] : sum + q[i]; }
+    for (int i = 0; i < nc; ++i) q[i] = q[i] / sum;
+  }
+  const float u_lam = uniform(rk, 0), u_d0 = uniform(rk, 1), u_d1 = uniform(rk, 2), u_c = uniform(rk, 3);
+  const float u_t = uniform(rk, 4);
+  int c = 0;
+  float cs = 0.0f;
+  for (int i = 0; i + 1 < nc; ++i) {
+    cs = i == 0 ? q[0] : cs + q[i];
+    c += u_c >= cs;
+  }
+  int nxt = nc, last = 0;  // lit: the first share above zero at or after c, else the last one
+  for (int i = nc - 1; i >= 0; --i)
+    if (q[i] > 0.0f && i >= c) nxt = i;
+  for (int i = 0; i < nc; ++i)
+    if (q[i] > 0.0f) last = i;
+  c = nxt < last ? nxt : last;
+  // the wavelength: the reference spectrum under the cover, the live density over the drawn one
+  const int ts = m[LUMEN_SM_SPEC + c];
+  const int off = __ldg(S.tab + 2 * ts), k = __ldg(S.tab + 2 * ts + 1);
+  const float* er_ = ref + off;
+  const float* el = live + off;
+  DSpec qs = d_spec(er_, er_ + k, k, 1);
+  r.lam = D_HC / d_spec_invert(qs, u_lam);
+  const float energy = D_HC / r.lam;
+  const float wt = d_safe_div(d_spec_density(el, el + k, k, 0, energy), d_spec_density(er_, er_ + k, k, 1, energy));
+  // the direction: z = 1 - 2 u, phi = 2 pi u'
+  const float z = 1.0f - 2.0f * u_d0;
+  const float sq = 1.0f - z * z;
+  const float rr = sq > 0.0f ? sqrtf(sq) : 0.0f;
+  float sp, cp;
+  l_sincos2pi(u_d1, &sp, &cp);
+  r.d[0] = rr * cp; r.d[1] = rr * sp; r.d[2] = z;
+  // the delay: Exp(tau), plus Exp(tau rise / (tau + rise)) with rise times (emission.py:48)
+  const float tau = d_tab(S, live, m[LUMEN_SM_TAU + c], 1.0f);
+  float delay = -tau * l_log(u_t);
+  if (rises) {
+    const float u_r = uniform(rk, 5 + seg);
+    const float rise = d_tab(S, live, m[LUMEN_SM_RISE + c], 1.0f);
+    const float s2 = tau + rise;
+    delay = delay + -(tau * rise / (s2 > 0.0f ? s2 : 1.0f)) * l_log(u_r);
+  }
+  // the photons: the yield times the energy, Birks-quenched along a segment (scintillation.py:42 visible_energy)
+  const float yl = d_tab(S, live, m[LUMEN_SM_YIELD], 1.0f);
+  const float edep = __ldg(f + 8), birks = __ldg(f + 9);
+  float n_ph;
+  if (seg) {
+    float dx = __ldg(f + 4) - __ldg(f + 0), dy = __ldg(f + 5) - __ldg(f + 1), dz = __ldg(f + 6) - __ldg(f + 2);
+    float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+    float qb = 1.0f + birks * edep / (len > 0.0f ? len : 1.0f);
+    n_ph = yl * ((len > 0.0f && edep > 0.0f) ? edep / qb : d_max(edep, 0.0f));
+  } else {
+    n_ph = yl * edep;
+  }
+  r.w0 = n_ph / __ldg(f + 10) * d_safe_div(fl[c], q[c]) * wt;
+  if (seg) {
+    const float u = uniform(rk, 5);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.x[a] = __ldg(f + a) + u * (__ldg(f + 4 + a) - __ldg(f + a));
+    r.t = __ldg(f + 3) + u * (__ldg(f + 7) - __ldg(f + 3)) + delay;
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r.x[a] = __ldg(f + a);
+    r.t = __ldg(f + 3) + delay;
+  }
+}
+
+L_DEV void d_source_row(const DScene& S, const float* __restrict__ pool, const float* __restrict__ ref,
+                        const LumenSource& src, Key key, int64_t gid, Row& r) {
   Key sk = fold_in(key, D_SOURCE_STREAM);
   Key rk = fold_in(fold_in(sk, (uint32_t)gid), 0u);
   int e = d_event_of(src.ev_first, src.n_events, gid);
@@ -666,6 +763,10 @@ L_DEV void d_source_row(const DScene& S, const float* __restrict__ pool, const L
 #pragma unroll
     for (int a = 0; a < 3; ++a) r.er[a] = ad * r.d[a] - ax[a];
     d_unit(r.er);
+    return;
+  }
+  if (src.kind == LUMEN_SRC_SCINT_MATERIAL) {
+    d_scint_row(S, pool, ref, src, f, rk, r);
     return;
   }
   if (src.kind == LUMEN_SRC_CHERENKOV) {  // cherenkov.py:33 cone: uniforms lam, pos, phi

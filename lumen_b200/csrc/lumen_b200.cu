@@ -166,7 +166,7 @@ __device__ __forceinline__ int deposit(const Tally& T, int e, const Dep& dep, co
 
 __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
   if (L.use_rows) d_rows_row(L.rows, i, r);
-  else d_source_row(L.R.S, L.R.live, L.src, L.key, L.first_id + i, r);
+  else d_source_row(L.R.S, L.R.live, L.R.ref, L.src, L.key, L.first_id + i, r);
 }
 
 // The persistent photon loop: a lane refill per step (src/lumen/run.py:81 SCHEDULE = "step").
@@ -670,7 +670,22 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   } else {
     if (source->n_events < 1 || !source->ev_f || !source->ev_first || !source->ev_w)
       return set_err(LUMEN_ERR_ARG, "source: events are missing");
-    if (source->kind < 0 || source->kind > LUMEN_SRC_CHERENKOV) return set_err(LUMEN_ERR_ARG, "source: unknown kind");
+    if (source->kind < 0 || source->kind > LUMEN_SRC_SCINT_MATERIAL) return set_err(LUMEN_ERR_ARG, "source: unknown kind");
+    if (source->kind == LUMEN_SRC_SCINT_MATERIAL) {
+      const int32_t* m = source->mat;
+      const int nt = (int)(sc->tab.size() / 2), nc = m[LUMEN_SM_N];
+      auto ok = [&](int t) { return t >= 0 && t < nt; };
+      int good = nc >= 1 && nc <= 3 && ok(m[LUMEN_SM_YIELD]);
+      for (int i = 0; i < nc && good; ++i)
+        good = ok(m[LUMEN_SM_SPEC + i]) && ok(m[LUMEN_SM_TAU + i]) && (!m[LUMEN_SM_RISES] || ok(m[LUMEN_SM_RISE + i]));
+      for (int i = 0; i < 3 && good; ++i) good = m[LUMEN_SM_SHARE + i] == -1 || ok(m[LUMEN_SM_SHARE + i]);
+      if (!good) return set_err(LUMEN_ERR_ARG, "source: a scintillation material's tables are incomplete");
+      for (int p = 0; p < (c ? c->n_grad : 0); ++p)
+        for (int w = LUMEN_SM_YIELD; w < LUMEN_SM_WORDS; ++w)
+          if (m[w] >= 0 && c->grad_tab[p] == m[w])
+            return set_err(LUMEN_ERR_NOT_SUPPORTED, "a scintillation source's own tables are not gradient parameters "
+                                                    "of this engine");
+    }
     if (source->kind == LUMEN_SRC_CHERENKOV) {
       if (source->rindex_tab < 0 || source->rindex_tab >= (int)(sc->tab.size() / 2))
         return set_err(LUMEN_ERR_ARG, "source: a Cherenkov segment needs its medium's RINDEX table");

@@ -187,6 +187,15 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             med_i[m, 9] = pool.add(float(mat.wls_tau), f"media/{name}/wls_tau")
             med_i[m, 10] = pool.add(tuple(np.asarray(x, np.float64) for x in mat.wls_spectrum), f"media/{name}/wls_spectrum")
             med_i[m, 11] = 1 if mat.wls_profile == "exponential" else 0
+        if mat.scint_components:  # a scintillation source's tables (sources.ScintillationPoint reads them by name)
+            pool.add(float(mat.scint_yield), f"media/{name}/scint_yield")
+            for i, comp in enumerate(mat.scint_components, 1):
+                pool.add(tuple(np.asarray(x, np.float64) for x in comp["spectrum"]), f"media/{name}/scint_spectrum{i}")
+                pool.add(float(comp["tau"]), f"media/{name}/scint_tau{i}")
+                if comp.get("rise") is not None:
+                    pool.add(float(comp["rise"]), f"media/{name}/scint_rise{i}")
+            for i, y in enumerate(mat.scint_shares or (), 1):
+                pool.add(float(y), f"media/{name}/scint_share{i}")
     mi_of = {n: i for i, n in enumerate(med_names)}
     cls_medium = np.asarray([mi_of[m] for m in cls_mat] + [mi_of[cls_mat[0]] if cls_mat else 0], np.int32)
     # surface rows per crossed class pair

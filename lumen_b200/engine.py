@@ -81,6 +81,8 @@ class DeviceSource:
         s.lam0, s.lam1, s.cone_cos = a["lam0"], a["lam1"], a["cone_cos"]
         s.tau1, s.tau2, s.frac1 = a["tau1"], a["tau2"], a["frac1"]
         s.rindex_tab = a.get("rindex_tab", -1)
+        if "mat" in a:
+            s.mat[:] = [int(v) for v in a["mat"]]
         self.c = s
         self.n_events = len(a["ev_w"])
         self.total = int(a["ev_first"][-1])

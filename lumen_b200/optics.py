@@ -71,6 +71,12 @@ class Material:
     WLSABSLENGTH (m), ``wls_spectrum`` the WLSCOMPONENT table (energies eV, intensities), ``wls_mean`` the mean
     photons per absorbed one (WLSMEANNUMBERPHOTONS, 1 when absent), ``wls_tau`` WLSTIMECONSTANT (ns, 0 when absent),
     ``wls_profile`` "delta" (Geant4's default) or "exponential".
+
+    Scintillation (G4Scintillation, Geant4 11 keys, src/lumen/sources/scintillation.py): ``scint_yield``
+    SCINTILLATIONYIELD (photons / MeV); ``scint_components`` up to three dicts, in order, with ``spectrum``
+    (SCINTILLATIONCOMPONENTi: energies eV, intensities), ``tau`` (SCINTILLATIONTIMECONSTANTi, ns) and ``rise``
+    (SCINTILLATIONRISETIMEi, ns; all or none of the components); ``scint_shares`` the SCINTILLATIONYIELDi (None:
+    Geant4's defaults 1, 0, 0). The material's light is a source's (``sources.ScintillationPoint``), not the bulk's.
     """  # noqa: D205
 
     name: str
@@ -86,6 +92,9 @@ class Material:
     wls_mean: float = 1.0
     wls_tau: float = 0.0
     wls_profile: str = "delta"
+    scint_yield: float | None = None
+    scint_components: tuple = ()
+    scint_shares: tuple | None = None
 
     def __post_init__(self):
         """Refuse what G4OpMieHG / G4OpWLS would abort on or the reference refuses (optics.py:337-380)."""
@@ -98,6 +107,15 @@ class Material:
             for g in (self.mie_forward, self.mie_backward):
                 if not abs(g) <= MIE_G_MAX:
                     raise ValueError(f"{self.name}: a Mie asymmetry |g| above {MIE_G_MAX}")
+        if self.scint_components:
+            if self.scint_yield is None or not 1 <= len(self.scint_components) <= 3:
+                raise ValueError(f"{self.name}: scintillation needs SCINTILLATIONYIELD and one to three components")
+            rises = [c.get("rise") is not None for c in self.scint_components]
+            if any(rises) and not all(rises):
+                raise ValueError(f"{self.name}: a rise time for every component or for none")
+            for c in self.scint_components:
+                if c.get("spectrum") is None or c.get("tau") is None:
+                    raise ValueError(f"{self.name}: a component without its spectrum or decay time (Geant4 aborts)")
         if self.wls is not None:
             if self.wls_spectrum is None:
                 raise ValueError(f"{self.name}: WLSABSLENGTH without WLSCOMPONENT (G4OpWLS absorbs and emits nothing)")

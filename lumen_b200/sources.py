@@ -12,6 +12,9 @@ assigns photon ids to events by contiguous ranges of uneven sizes (``counts``), 
 - ``Scintillation(position, tau=(tau1, tau2), fraction)``: isotropic points with a two-exponential time profile.
 - ``CherenkovSegment(material, start, direction, length, beta, charge, time)``: the Frank-Tamm light of charged
   segments (src/lumen/sources/cherenkov.py:65), one event per segment, on the medium's live RINDEX.
+- ``ScintillationPoint(material, position, energy, time)`` / ``ScintillationSegment(material, start, end, t_start,
+  t_end, energy, birks)``: a material's scintillation light (src/lumen/sources/scintillation.py:172, :182), one event
+  per deposit: its components, spectra, decay and rise times and yield from the detector's tables.
 - ``FromArrays(x, d, t, lam, w, pol)``: explicit rows (src/lumen/sources/arrays.py:24).
 """
 
@@ -201,6 +204,98 @@ class CherenkovSegment(Source):
         first[1:] = np.cumsum(cnt)
         return dict(kind=A.SRC_CHERENKOV, ev_f=ev_f, ev_first=first, ev_w=np.ones(n_ev, np.float32),
                     lam0=float(lam0), lam1=float(lam1), cone_cos=1.0, tau1=0.0, tau2=0.0, frac1=0.0, rindex_tab=tab)  # fmt: skip
+
+
+def _scint_mat(det, material):
+    """The LumenSource.mat words of a material's scintillation tables in the detector."""
+    pi = det.params_index
+    m = f"media/{material}/"
+    if m + "scint_yield" not in pi:
+        raise ValueError(f"{material}: no scintillation (SCINTILLATIONYIELD and its components) in the detector")
+    n = sum(1 for i in (1, 2, 3) if f"{m}scint_spectrum{i}" in pi)
+    words = np.full(A.SM_WORDS, -1, np.int32)
+    rises = all(f"{m}scint_rise{i}" in pi for i in range(1, n + 1))
+    words[A.SM_N], words[A.SM_SEGMENT], words[A.SM_RISES], words[A.SM_YIELD] = n, 0, int(rises), pi[m + "scint_yield"]
+    for i in range(n):
+        words[A.SM_SPEC + i] = pi[f"{m}scint_spectrum{i + 1}"]
+        words[A.SM_TAU + i] = pi[f"{m}scint_tau{i + 1}"]
+        if rises:
+            words[A.SM_RISE + i] = pi[f"{m}scint_rise{i + 1}"]
+    for i in range(3):
+        words[A.SM_SHARE + i] = pi.get(f"{m}scint_share{i + 1}", -1)
+    return words
+
+
+@dataclass
+class ScintillationPoint(Source):
+    """``energy`` (MeV) deposited at ``position`` (m) at ``time`` (ns) in ``material`` (src/lumen/sources/
+    scintillation.py:172): its light's photons are the yield times the energy; rows of position, energy and time are
+    one event each."""  # noqa: D205
+
+    material: str
+    position: object = (0.0, 0.0, 0.0)
+    energy: object = 1.0
+    time: object = 0.0
+    counts_: object = None
+    SEGMENT = False
+
+    def events(self):
+        return len(np.asarray(self.position, np.float32).reshape(-1, 3))
+
+    def counts(self, samples):
+        if self.counts_ is not None:
+            return np.asarray(self.counts_, np.int64)
+        e = self.events()
+        base = np.full(e, samples // e, np.int64)
+        base[: samples - base.sum()] += 1
+        return base
+
+    def _ev(self, n_ev):
+        ev_f = np.zeros((n_ev, A.EV_F), np.float32)
+        ev_f[:, 0:3] = _events(self.position, n_ev, 3)
+        ev_f[:, 3] = np.broadcast_to(np.asarray(self.time, np.float32), (n_ev,))
+        ev_f[:, 8] = np.broadcast_to(np.asarray(self.energy, np.float32), (n_ev,))
+        return ev_f
+
+    def arrays(self, samples, det=None):
+        if det is None:
+            raise ValueError("a scintillation source reads its material's tables from the detector (pass det)")
+        n_ev = self.events()
+        cnt = self.counts(samples)
+        ev_f = self._ev(n_ev)
+        ev_f[:, 10] = cnt.astype(np.float32)  # the event's samples (the weight's divisor)
+        mat = _scint_mat(det, self.material)
+        mat[A.SM_SEGMENT] = int(self.SEGMENT)
+        first = np.zeros(n_ev + 1, np.int64)
+        first[1:] = np.cumsum(cnt)
+        return dict(kind=A.SRC_SCINT_MATERIAL, ev_f=ev_f, ev_first=first, ev_w=np.ones(n_ev, np.float32), lam0=0.0,
+                    lam1=0.0, cone_cos=1.0, tau1=0.0, tau2=0.0, frac1=0.0, mat=mat)  # fmt: skip
+
+
+@dataclass
+class ScintillationSegment(ScintillationPoint):
+    """A charged step from ``start`` (at ``t_start`` ns) to ``end`` (``t_end``) depositing ``energy`` MeV, quenched by
+    Birks' law with ``birks`` (m / MeV) (src/lumen/sources/scintillation.py:182); photons uniform along it."""  # noqa: D205
+
+    start: object = (0.0, 0.0, 0.0)
+    end: object = (0.0, 0.0, 0.0)
+    t_start: object = 0.0
+    t_end: object = 0.0
+    birks: object = 0.0
+    SEGMENT = True
+
+    def events(self):
+        return len(np.asarray(self.start, np.float32).reshape(-1, 3))
+
+    def _ev(self, n_ev):
+        ev_f = np.zeros((n_ev, A.EV_F), np.float32)
+        ev_f[:, 0:3] = _events(self.start, n_ev, 3)
+        ev_f[:, 3] = np.broadcast_to(np.asarray(self.t_start, np.float32), (n_ev,))
+        ev_f[:, 4:7] = _events(self.end, n_ev, 3)
+        ev_f[:, 7] = np.broadcast_to(np.asarray(self.t_end, np.float32), (n_ev,))
+        ev_f[:, 8] = np.broadcast_to(np.asarray(self.energy, np.float32), (n_ev,))
+        ev_f[:, 9] = np.broadcast_to(np.asarray(self.birks, np.float32), (n_ev,))
+        return ev_f
 
 
 def _common(src, kind, ev_f, cnt, n_photons):

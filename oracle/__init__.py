@@ -58,7 +58,7 @@ def lib():
                                        ctypes.c_float, ctypes.c_int32, ctypes.c_float, ctypes.c_uint32,
                                        ctypes.c_uint32, ctypes.c_int64, A.c_f32p]  # fmt: skip
         L.lumen_oracle_group_index.argtypes = [A.c_f32p, A.c_f32p, ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
-        L.lumen_oracle_source_rows.argtypes = [P(A.LumenSceneDesc), A.c_f32p, P(A.LumenSource), ctypes.c_uint32,
+        L.lumen_oracle_source_rows.argtypes = [P(A.LumenSceneDesc), A.c_f32p, A.c_f32p, P(A.LumenSource), ctypes.c_uint32,
                                                ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64, A.c_f32p, A.c_i32p]
         del vp
         _lib = L
@@ -223,6 +223,8 @@ def host_source(src, samples, det=None):
     s.lam0, s.lam1, s.cone_cos = a["lam0"], a["lam1"], a["cone_cos"]
     s.tau1, s.tau2, s.frac1 = a["tau1"], a["tau2"], a["frac1"]
     s.rindex_tab = a.get("rindex_tab", -1)
+    if "mat" in a:
+        s.mat[:] = [int(v) for v in a["mat"]]
     return s, keep
 
 
@@ -259,15 +261,16 @@ def trace(det, key, n, *, rows=None, source=None, samples=None, first_id=0, pool
     return T, ((rec_i, rec_f) if records else None)
 
 
-def source_rows(source, key, n, first_id=0, samples=None, det=None, pool=None):
+def source_rows(source, key, n, first_id=0, samples=None, det=None, pool=None, pool_ref=None):
     """The emission rows of a procedural source (n, 15: x, d, t, lam, w0, er, ei) and their events; ``det`` (and
     ``pool``, the live values: default the detector's) for a Cherenkov segment's medium."""  # noqa: D205, D209
     ss, skeep = host_source(source, samples or n, det)
     d, dkeep = det.desc() if det is not None else (None, None)
     pl = None if pool is None else A.np_f32(pool)
+    rf = None if pool_ref is None else A.np_f32(pool_ref)
     out_f = np.zeros((n, 15), np.float32)
     ev = np.zeros(n, np.int32)
-    st = lib().lumen_oracle_source_rows(ctypes.byref(d) if d is not None else None, A.fptr(pl), ctypes.byref(ss),
+    st = lib().lumen_oracle_source_rows(ctypes.byref(d) if d is not None else None, A.fptr(pl), A.fptr(rf), ctypes.byref(ss),
                                         key[0], key[1], first_id, n, A.fptr(out_f), A.iptr(ev))  # fmt: skip
     assert st == 0, f"oracle status {st}"
     return out_f, ev

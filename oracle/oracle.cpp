@@ -558,8 +558,95 @@ static int o_event_of(const int64_t* first, int n_ev, int64_t gid) {
 /* 2 pi alpha for Frank-Tamm (units.py:16 FINE_STRUCTURE): the product in double, rounded once */
 static const float O_TWO_PI_ALPHA = (float)(6.283185307179586 * (1.0 / 137.035999084));
 
-static void o_source_row(const LumenSceneDesc* D, const float* pool, const LumenSource* src, OKey key, int64_t gid,
-                         ORow* r) {
+/* a material's scintillation photon (scintillation.py:69 flash; shares :48; the component's defensive draw,
+   estimator.py:101, and _base.py:298 lit; the wavelength _base.py:337; the delays emission.py:48) */
+static void o_scint_shares(const LumenSceneDesc* D, const float* pool, const int32_t* m, float* f) {
+  float y[3];
+  for (int i = 0; i < 3; ++i) {
+    int t = m[LUMEN_SM_SHARE + i];
+    y[i] = t >= 0 ? o_tab(D, pool, t, 1.0f, 0) : (i == 0 ? 1.0f : 0.0f);
+  }
+  const float s = (y[0] + y[1]) + y[2];
+  f[0] = 1.0f; f[1] = 0.0f; f[2] = 0.0f;
+  if (m[LUMEN_SM_N] == 2) { f[0] = y[0] / s; f[1] = 1.0f - y[0] / s; }
+  if (m[LUMEN_SM_N] == 3) for (int i = 0; i < 3; ++i) f[i] = y[i] / s;
+}
+
+static void o_scint_row(const LumenSceneDesc* D, const float* live, const float* ref, const LumenSource* src,
+                        const float* f, OKey rk, ORow* r) {
+  const int32_t* m = src->mat;
+  const int nc = m[LUMEN_SM_N], seg = m[LUMEN_SM_SEGMENT];
+  float fl[3], q[3];
+  o_scint_shares(D, live, m, fl);
+  o_scint_shares(D, ref, m, q);
+  int zeros = 0;
+  for (int i = 0; i < nc; ++i) zeros += q[i] <= 0.0f ? 1 : 0;
+  if (zeros) {
+    const float eps = (float)(0.01 / 0.99) / (float)zeros;
+    float tot = 0.0f;
+    for (int i = 0; i < nc; ++i) {
+      if (q[i] <= 0.0f) q[i] = eps;
+      tot = i == 0 ? q[i] : tot + q[i];
+    }
+    for (int i = 0; i < nc; ++i) q[i] = q[i] / tot;
+  }
+  float u_lam = o_uniform(rk, 0), u_z = o_uniform(rk, 1), u_phi = o_uniform(rk, 2), u_comp = o_uniform(rk, 3);
+  float u_time = o_uniform(rk, 4);
+  int c = 0;
+  float cum = 0.0f;
+  for (int i = 0; i < nc - 1; ++i) {
+    cum = i == 0 ? q[0] : cum + q[i];
+    if (u_comp >= cum) ++c;
+  }
+  int first_lit = nc, last_lit = 0;
+  for (int i = 0; i < nc; ++i) {
+    if (q[i] > 0.0f) last_lit = i;
+    if (q[i] > 0.0f && i >= c && first_lit == nc) first_lit = i;
+  }
+  c = first_lit < last_lit ? first_lit : last_lit;
+  const int ts = m[LUMEN_SM_SPEC + c];
+  const float* kr = ref + D->tab[2 * ts];
+  const float* kl = live + D->tab[2 * ts];
+  const int k = D->tab[2 * ts + 1];
+  OSpec qs = o_spec(kr, kr + k, k, 1);
+  r->lam = O_HC / o_spec_invert(&qs, u_lam);
+  const float energy = O_HC / r->lam;
+  const float wt = o_safe_div(o_spec_density(kl, kl + k, k, 0, energy), o_spec_density(kr, kr + k, k, 1, energy));
+  const float z = 1.0f - 2.0f * u_z;
+  const float sz = 1.0f - z * z;
+  const float rho = sz > 0.0f ? sqrtf(sz) : 0.0f;
+  float sp, cp;
+  o_sincos2pi(u_phi, &sp, &cp);
+  r->d[0] = rho * cp; r->d[1] = rho * sp; r->d[2] = z;
+  const float tau = o_tab(D, live, m[LUMEN_SM_TAU + c], 1.0f, 0);
+  float delay = -tau * o_log(u_time);
+  if (m[LUMEN_SM_RISES]) {
+    const float rise = o_tab(D, live, m[LUMEN_SM_RISE + c], 1.0f, 0);
+    const float s = tau + rise;
+    delay = delay + -(tau * rise / (s > 0.0f ? s : 1.0f)) * o_log(o_uniform(rk, 5 + seg));
+  }
+  const float yl = o_tab(D, live, m[LUMEN_SM_YIELD], 1.0f, 0);
+  const float edep = f[8], birks = f[9];
+  float n_ph = yl * edep;
+  if (seg) { /* Birks' law along the segment (scintillation.py:42 visible_energy) */
+    float v[3] = {f[4] - f[0], f[5] - f[1], f[6] - f[2]};
+    float len = sqrtf((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+    float quench = 1.0f + birks * edep / (len > 0.0f ? len : 1.0f);
+    n_ph = yl * ((len > 0.0f && edep > 0.0f) ? edep / quench : (edep > 0.0f ? edep : 0.0f));
+  }
+  r->w0 = n_ph / f[10] * o_safe_div(fl[c], q[c]) * wt;
+  if (seg) {
+    const float u = o_uniform(rk, 5);
+    for (int a = 0; a < 3; ++a) r->x[a] = f[a] + u * (f[4 + a] - f[a]);
+    r->t = f[3] + u * (f[7] - f[3]) + delay;
+  } else {
+    for (int a = 0; a < 3; ++a) r->x[a] = f[a];
+    r->t = f[3] + delay;
+  }
+}
+
+static void o_source_row(const LumenSceneDesc* D, const float* pool, const float* ref, const LumenSource* src,
+                         OKey key, int64_t gid, ORow* r) {
   OKey sk = o_fold_in(key, O_SOURCE_STREAM);
   OKey rk = o_fold_in(o_fold_in(sk, (uint32_t)gid), 0u);
   int e = o_event_of(src->ev_first, src->n_events, gid);
@@ -584,6 +671,10 @@ static void o_source_row(const LumenSceneDesc* D, const float* pool, const Lumen
     float ad = o_dot(ax, r->d);
     for (int a = 0; a < 3; ++a) r->er[a] = ad * r->d[a] - ax[a];
     o_unit(r->er);
+    return;
+  }
+  if (src->kind == LUMEN_SRC_SCINT_MATERIAL) {
+    o_scint_row(D, pool, ref, src, f, rk, r);
     return;
   }
   if (src->kind == LUMEN_SRC_CHERENKOV) { /* cherenkov.py:33 cone: a Frank-Tamm photon of the segment */
@@ -796,7 +887,7 @@ static void o_row_of(const ORun* R, const LumenRows* rows, const LumenSource* sr
     }
     r->event = rows->event ? rows->event[i] : 0;
   } else {
-    o_source_row(R->S.D, R->live, src, key, first_id + i, r);
+    o_source_row(R->S.D, R->live, R->ref, src, key, first_id + i, r);
   }
 }
 
@@ -1117,16 +1208,18 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
   return 0;
 }
 
-/* emission rows of a procedural source (host): x, d, t, lam, w0, er, ei, event per photon; D and pool (the live
-   values) are read by a Cherenkov segment only */
-int32_t lumen_oracle_source_rows(const LumenSceneDesc* D, const float* pool, const LumenSource* src, uint32_t key0,
-                                 uint32_t key1, int64_t first_id, int64_t n, float* out_f, int32_t* out_event) {
+/* emission rows of a procedural source (host): x, d, t, lam, w0, er, ei, event per photon; D, pool (the live values)
+   and ref (the reference's; null: the live) are read by the Cherenkov and the material scintillation sources */
+int32_t lumen_oracle_source_rows(const LumenSceneDesc* D, const float* pool, const float* ref, const LumenSource* src,
+                                 uint32_t key0, uint32_t key1, int64_t first_id, int64_t n, float* out_f,
+                                 int32_t* out_event) {
   OKey key = {key0, key1};
-  if (src->kind == LUMEN_SRC_CHERENKOV && !D) return LUMEN_ERR_ARG;
+  if ((src->kind == LUMEN_SRC_CHERENKOV || src->kind == LUMEN_SRC_SCINT_MATERIAL) && !D) return LUMEN_ERR_ARG;
   const float* pl = pool ? pool : (D ? D->pool : 0);
+  const float* rf = ref ? ref : pl;
   for (int64_t i = 0; i < n; ++i) {
     ORow r;
-    o_source_row(D, pl, src, key, first_id + i, &r);
+    o_source_row(D, pl, rf, src, key, first_id + i, &r);
     float* f = out_f + 15 * i;
     for (int a = 0; a < 3; ++a) { f[a] = r.x[a]; f[3 + a] = r.d[a]; f[9 + a] = r.er[a]; f[12 + a] = r.ei[a]; }
     f[6] = r.t; f[7] = r.lam; f[8] = r.w0;

@@ -373,3 +373,35 @@ def test_cherenkov_segments_bit_exact(toy, built):
     T = DeviceTallies(toy.n_sensor, 2, 0, 0.0, 1.0, 1)
     with pytest.raises(A.EngineError):
         eng.trace(KEY, n, source=ds, controls=A.controls(grad_tabs=[toy.params_index["media/Water/index"]]), tallies=T)
+
+
+def test_material_scintillation_bit_exact(built):
+    """A material's scintillation (src/lumen/sources/scintillation.py: ScintillationPoint, ScintillationSegment with
+    Birks' law), drawn at reference shares (1, 0) under the defensive mixture and weighted to live (0.25, 0.75): every
+    photon's record and the tallies are the checker's; the source's own tables are refused as gradient parameters."""
+    det = detectors.scintillating_tank()
+    live = det.pool_with({"media/Scint/scint_share1": 0.25, "media/Scint/scint_share2": 0.75})
+    ref = det.pool_with({"media/Scint/scint_share1": 1.0, "media/Scint/scint_share2": 0.0})
+    n = 1 << 14
+    eng = _engine(det)
+    eng.set_pools(live, ref)
+    for src in (sources.ScintillationPoint("Scint", position=[(0.0, 0.0, 0.0), (0.2, 0.1, -0.3)], energy=[1.0, 0.5]),
+                sources.ScintillationSegment("Scint", start=(-0.2, 0.0, 0.1), end=(0.2, 0.1, -0.1), t_start=1.0,
+                                             t_end=3.0, energy=4.0, birks=0.1)):  # fmt: skip
+        ds = DeviceSource(src, n, det=det)
+        gi, gf = eng.trace_photons(KEY, n, source=ds, controls=A.controls())
+        _, (oi, of) = oracle.trace(det, KEY, n, source=src, samples=n, records=True, pool_live=live, pool_ref=ref,
+                                   n_events=ds.n_events)  # fmt: skip
+        gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+        bad = np.flatnonzero((gi != oi).any(1) | (gf.view(np.uint32) != of.view(np.uint32)).any(1))
+        assert len(bad) == 0, f"{type(src).__name__}: {len(bad)} photons differ, first {bad[:5]}"
+        T = DeviceTallies(det.n_sensor, ds.n_events, 50, 0.0, 20.0, 0)
+        eng.trace(KEY, n, source=ds, controls=A.controls(), tallies=T)
+        O, _ = oracle.trace(det, KEY, n, source=src, samples=n, n_events=ds.n_events, n_bins=50, bin_w=20.0,
+                            pool_live=live, pool_ref=ref)  # fmt: skip
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.hist.cpu().numpy(), O.hist, rtol=RTOL, atol=1e-12)
+    T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, 1)
+    with pytest.raises(A.EngineError):
+        eng.trace(KEY, n, source=ds, controls=A.controls(grad_tabs=[det.params_index["media/Scint/scint_yield"]]),
+                  tallies=T)  # fmt: skip
