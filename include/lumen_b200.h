@@ -60,7 +60,9 @@ enum { LUMEN_KIND_I = 4 };
 /* Leaf: float og (3) plane origin, oq (3) quadric origin, A (9, row-major), b (3), c, sa = max |A_ij| */
 enum { LUMEN_LF_OG = 0, LUMEN_LF_OQ = 3, LUMEN_LF_A = 6, LUMEN_LF_B = 15, LUMEN_LF_C = 18, LUMEN_LF_SA = 19,
        LUMEN_LEAF_F = 20 };
-/* Leaf ints: typ (0: planes only, 1: quadric and planes), p0 (first plane), np (planes) */
+/* Leaf ints: typ (0: planes only, 1: quadric and planes, 2: a solid torus {(rho - R)^2 + z^2 <= r^2} in canonical
+   coordinates u = M (x - og), M row-major at LUMEN_LF_A, R at LUMEN_LF_B, r at LUMEN_LF_B + 1; a torus reads no
+   planes), p0 (first plane), np (planes) */
 enum { LUMEN_LEAF_I = 4 };
 /* Plane: n (3), h — the leaf holds n . (x - og) <= h */
 enum { LUMEN_PLANE_F = 4 };

@@ -163,6 +163,158 @@ L_DEV void d_quad_line(const float* lf, const float* y, const float* d, float* L
   *R1 = has1 ? inf : -inf;
 }
 
+// ------------------------------------------------------------------------------------------------ the torus
+// leaf_kernels.py:212 torus_set: the interval set (two slots) of a solid torus about z along a unit ray o + s d in its
+// canonical frame. g(s) = (rho - R)^2 + z^2 - r^2 has at most two inflection points (closed form); they split the
+// bracket on the padded bounding sphere into convex / concave / convex parts with one extremum each (bisection on g'),
+// giving at most six monotone pieces with one root at most (bisection on the membership)
+#define D_BISECT 40                // bisections in float32: the mantissa plus a margin
+#define D_TORUS_BRACKET_ULPS 64.0f
+#define D_TORUS_AXIAL 1e-12f       // a squared xy direction below this is along the axis
+#define D_TORUS_PAD_REL 1e-4f      // the pretests' pad, relative to R + r
+
+L_DEV float d_torus_g(float R, float r, const float* oc, const float* d, float s) {
+  float x = oc[0] + s * d[0], y = oc[1] + s * d[1], z = oc[2] + s * d[2];
+  float rho2 = x * x + y * y;
+  float rho = sqrtf(d_max(rho2, 0.0f));
+  float dr = (rho2 - R * R) / (rho + R);  // rho - R without the cancellation of rho and R
+  return dr * dr + z * z - r * r;
+}
+L_DEV float d_torus_dg(float R, const float* oc, const float* d, float s) {
+  float x = oc[0] + s * d[0], y = oc[1] + s * d[1], z = oc[2] + s * d[2];
+  float rho2 = x * x + y * y;
+  float rho = sqrtf(d_max(rho2, D_TINY_NORMAL));
+  float dr = (rho2 - R * R) / (rho + R);
+  float drho = (x * d[0] + y * d[1]) / rho;
+  return 2.0f * dr * drho + 2.0f * z * d[2];
+}
+
+// the exact pretests of the whole line (csg.py:175 _torus_window, the window unbounded): the padded ball, the slab
+// |z| <= r, the annulus R - r <= rho <= R + r. A window of the line that misses the torus holds none of its roots, so
+// solving on the whole line gives every window the reference's memberships.
+L_DEV int d_torus_meets(float R, float r, const float* ol, const float* du) {
+  const float Rb = (R + r) * (1.0f + D_TORUS_PAD_REL);
+  float bb = ol[0] * du[0] + ol[1] * du[1] + ol[2] * du[2];
+  float disc = Rb * Rb - (ol[0] * ol[0] + ol[1] * ol[1] + ol[2] * ol[2] - bb * bb);
+  float sq = sqrtf(d_max(disc, 0.0f));
+  float s_lo = -bb - sq, s_hi = -bb + sq;
+  int meet = disc > 0.0f && s_lo <= s_hi;
+  const float pad = D_TORUS_PAD_REL * (R + r), rz = r + pad;
+  int small = fabsf(du[2]) < D_PARALLEL;
+  float iz = 1.0f / (small ? 1.0f : du[2]);
+  float za = (-rz - ol[2]) * iz, zb = (rz - ol[2]) * iz;
+  if (!small) { s_lo = d_max(s_lo, d_min(za, zb)); s_hi = d_min(s_hi, d_max(za, zb)); }
+  meet = meet && s_lo <= s_hi && (!small || fabsf(ol[2]) <= rz);
+  float qa = du[0] * du[0] + du[1] * du[1], qb = ol[0] * du[0] + ol[1] * du[1], qc = ol[0] * ol[0] + ol[1] * ol[1];
+  float sm = d_min(d_max(-qb / (qa > D_PARALLEL ? qa : 1.0f), s_lo), s_hi);
+  float r2_min = qa > D_PARALLEL ? (qa * sm * sm + 2.0f * qb * sm + qc) : qc;
+  float r2_max = d_max(qa * s_lo * s_lo + 2.0f * qb * s_lo + qc, qa * s_hi * s_hi + 2.0f * qb * s_hi + qc);
+  float r_out = R + r + pad, r_in = d_max(R - r - pad, 0.0f);
+  return meet && r2_min <= r_out * r_out && r2_max >= r_in * r_in;
+}
+
+L_CALL void d_torus_set(float R, float r, const float* od, const float* dd, float* lo, float* hi) {
+  const float inf = D_HUGE;
+  float t_c = -((od[0] * dd[0] + od[1] * dd[1]) + od[2] * dd[2]);
+  float oc[3] = {od[0] + t_c * dd[0], od[1] + t_c * dd[1], od[2] + t_c * dd[2]};
+  float q0 = (oc[0] * oc[0] + oc[1] * oc[1]) + oc[2] * oc[2];
+  const float Rb = (R + r) * (1.0f + D_TORUS_BRACKET_ULPS * D_EPS32);
+  float b0 = (oc[0] * dd[0] + oc[1] * dd[1]) + oc[2] * dd[2];
+  float disc = Rb * Rb - q0 + b0 * b0;
+  int hit_b = disc > 0.0f;
+  float sq = sqrtf(hit_b ? disc : 1.0f);
+  float s_lo = -b0 - sq, s_hi = -b0 + sq;
+  float a = dd[0] * dd[0] + dd[1] * dd[1];
+  float bxy = oc[0] * dd[0] + oc[1] * dd[1];
+  float cxy = oc[0] * oc[0] + oc[1] * oc[1];
+  int a_ok = a > D_TORUS_AXIAL;
+  float a_s = a_ok ? a : 1.0f;
+  float s_v = a_ok ? -bxy / a_s : 0.0f;
+  float m2 = d_max(a_ok ? cxy - bxy * bxy / a_s : cxy, 0.0f);
+  float ci = l_cbrt(R * a * m2);
+  float w2 = (ci * ci - m2) / a_s;  // the inflection points s_v -+ w
+  int has_w = a_ok && w2 > 0.0f;
+  float w = sqrtf(has_w ? w2 : 0.0f);
+  float p1 = d_min(d_max(s_v - w, s_lo), s_hi), p2 = d_min(d_max(s_v + w, s_lo), s_hi);
+  // the extrema: a minimum on [s_lo, p1] (g' increasing), the maximum on [p1, p2], a minimum on [p2, s_hi]
+  float el[3] = {s_lo, p1, p2}, eh[3] = {p1, p2, s_hi}, e[3];
+  for (int k = 0; k < 3; ++k) {
+    float l = el[k], h = eh[k];
+    for (int it = 0; it < D_BISECT; ++it) {
+      float mid = 0.5f * (l + h);
+      float gm = d_torus_dg(R, oc, dd, mid);
+      int right = k == 1 ? gm > 0.0f : gm < 0.0f;
+      l = right ? mid : l;
+      h = right ? h : mid;
+    }
+    e[k] = 0.5f * (l + h);
+  }
+  // the roots: one per monotone piece whose ends differ in membership
+  const float knots[7] = {s_lo, e[0], p1, e[1], p2, e[2], s_hi};
+  float t[6];
+  for (int k = 0; k < 6; ++k) {
+    float xl = knots[k], xr = knots[k + 1];
+    int inl = d_torus_g(R, r, oc, dd, xl) <= 0.0f, inr = d_torus_g(R, r, oc, dd, xr) <= 0.0f;
+    float l = xl, h = xr;
+    for (int it = 0; it < D_BISECT; ++it) {
+      float mid = 0.5f * (l + h);
+      int same = (d_torus_g(R, r, oc, dd, mid) <= 0.0f) == inl;
+      l = same ? mid : l;
+      h = same ? h : mid;
+    }
+    t[k] = (inl != inr && xr > xl && hit_b) ? 0.5f * (l + h) + t_c : inf;
+  }
+  for (int i = 1; i < 6; ++i)  // ascending (insertion)
+    for (int j = i; j > 0 && t[j] < t[j - 1]; --j) { float x = t[j]; t[j] = t[j - 1]; t[j - 1] = x; }
+  // outside at the bracket's start: the roots alternate entry and exit
+  int ok0 = t[1] < D_BIG, ok1 = t[3] < D_BIG;
+  lo[0] = ok0 ? t[0] : inf; hi[0] = ok0 ? t[1] : inf;
+  lo[1] = ok1 ? t[2] : inf; hi[1] = ok1 ? t[3] : inf;
+}
+
+// a torus leaf's intervals along o + t d (kind frame): its canonical frame u = M (x - og), the unit ray there, the
+// roots scaled back (csg.py:207 _t_iv); out of line, returned by value (the quadric-only scenes' step pays a branch)
+L_DEV float4 d_torus_line(const float* lf, const float* o, const float* d) {
+  const float* M = lf + LUMEN_LF_A;
+  const float R = __ldg(lf + LUMEN_LF_B), r = __ldg(lf + LUMEN_LF_B + 1);
+  float xl[3] = {o[0] - __ldg(lf + 0), o[1] - __ldg(lf + 1), o[2] - __ldg(lf + 2)}, ol[3], dl[3];
+  d_Av(M, xl, ol);
+  d_Av(M, d, dl);
+  float kk = sqrtf(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
+  float du[3] = {dl[0] / kk, dl[1] / kk, dl[2] / kk};
+  float lo[2] = {D_HUGE, D_HUGE}, hi[2] = {D_HUGE, D_HUGE};
+  if (d_torus_meets(R, r, ol, du)) d_torus_set(R, r, ol, du, lo, hi);
+  return make_float4(fabsf(lo[0]) < D_BIG ? lo[0] / kk : lo[0], fabsf(hi[0]) < D_BIG ? hi[0] / kk : hi[0],
+                     fabsf(lo[1]) < D_BIG ? lo[1] / kk : lo[1], fabsf(hi[1]) < D_BIG ? hi[1] / kk : hi[1]);
+}
+
+// a torus leaf's Iv (it reads no planes: each piece its own roots, face 0; the non-empty piece first); out of line,
+// the ray and the result by value, so that a scan over quadric and plane leaves keeps its registers
+L_CALL Iv d_torus_iv(const float* lf, float3 ov, float3 dv) {
+  const float o[3] = {ov.x, ov.y, ov.z}, d[3] = {dv.x, dv.y, dv.z};
+  float4 tv = d_torus_line(lf, o, d);
+  const float inf = D_HUGE;
+  Iv r;
+  int ok0 = tv.x < tv.y, ok1 = tv.z < tv.w;
+  r.lo0 = ok0 ? tv.x : inf; r.hi0 = ok0 ? tv.y : inf; r.f_lo0 = ok0 ? 0 : -1; r.f_hi0 = ok0 ? 0 : -1;
+  r.lo1 = ok1 ? tv.z : inf; r.hi1 = ok1 ? tv.w : inf; r.f_lo1 = ok1 ? 0 : -1; r.f_hi1 = ok1 ? 0 : -1;
+  if (!ok0 && ok1) {
+    Iv s = r;
+    r.lo0 = s.lo1; r.hi0 = s.hi1; r.f_lo0 = s.f_lo1; r.f_hi0 = s.f_hi1;
+    r.lo1 = s.lo0; r.hi1 = s.hi0; r.f_lo1 = s.f_lo0; r.f_hi1 = s.f_hi0;
+  }
+  return r;
+}
+
+// whether the torus holds x (kind frame): (rho - R)^2 + z^2 <= r^2 in its canonical frame (csg.py:301 _inside_leaf)
+L_DEV int d_torus_holds(const float* lf, const float* x) {
+  float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)}, u[3];
+  d_Av(lf + LUMEN_LF_A, xl, u);
+  const float R = __ldg(lf + LUMEN_LF_B), r = __ldg(lf + LUMEN_LF_B + 1);
+  float dr = sqrtf(u[0] * u[0] + u[1] * u[1]) - R;
+  return dr * dr + u[2] * u[2] <= r * r;
+}
+
 L_DEV Iv d_leaf_iv(const DScene& S, int g, const float* o, const float* d) {
   const float* lf = S.leaf_f + (size_t)g * LUMEN_LEAF_F;
   const int32_t* li = S.leaf_i + (size_t)g * LUMEN_LEAF_I;
@@ -223,6 +375,7 @@ L_DEV int d_inside_leaf(const DScene& S, int g, const float* x) {
     const float* p = S.plane_f + (size_t)(p0 + k) * LUMEN_PLANE_F;
     pl = pl && (__ldg(p) * xl[0] + __ldg(p + 1) * xl[1] + __ldg(p + 2) * xl[2] <= __ldg(p + 3));
   }
+  if (__ldg(li) == 2) return d_torus_holds(lf, x);
   if (__ldg(li) != 1) return pl;
   float Ay[3];
   d_Av(lf + LUMEN_LF_A, y, Ay);
@@ -277,12 +430,20 @@ L_DEV int d_mem_at(const DScene& S, const Scan& s, float t, int use_on) {
   });
 }
 
+// TORUS: the instantiation reads torus leaves (scenes without one run the instantiation without their code)
+template <int TORUS>
 L_DEV void d_scan_init(const DScene& S, Scan& s, int kind, const float* o, const float* d, float t1) {
   s.kind = kind;
   const int32_t* k = S.kind_i + (size_t)kind * LUMEN_KIND_I;
   s.nl = __ldg(k + 1);
   int l0 = __ldg(k);
-  for (int l = 0; l < s.nl; ++l) s.iv[l] = d_leaf_iv(S, l0 + l, o, d);
+  for (int l = 0; l < s.nl; ++l) {
+    if (TORUS && __ldg(S.leaf_i + (size_t)(l0 + l) * LUMEN_LEAF_I) == 2)
+      s.iv[l] = d_torus_iv(S.leaf_f + (size_t)(l0 + l) * LUMEN_LEAF_F, make_float3(o[0], o[1], o[2]),
+                           make_float3(d[0], d[1], d[2]));
+    else
+      s.iv[l] = d_leaf_iv(S, l0 + l, o, d);
+  }
   s.xa = d_max(d_max(fabsf(o[0]), fabsf(o[1])), fabsf(o[2]));
   s.t1 = t1;
   s.want = -1;
@@ -361,6 +522,17 @@ L_DEV void d_leaf_grad(const DScene& S, int kind, int leaf, int face, const floa
     g[0] = __ldg(p); g[1] = __ldg(p + 1); g[2] = __ldg(p + 2);
     return;
   }
+  if (__ldg(li) == 2) {  // M^T of the canonical gradient of ((rho - R)^2 + z^2 - r^2) / 2 (csg.py:452 leaf_grad)
+    const float* M = lf + LUMEN_LF_A;
+    float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)}, u[3];
+    d_Av(M, xl, u);
+    float rho = sqrtf(d_max(u[0] * u[0] + u[1] * u[1], D_DIVISOR_FLOOR));
+    float k = (rho - __ldg(lf + LUMEN_LF_B)) / rho;
+    float gu[3] = {k * u[0], k * u[1], u[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[a] = (__ldg(M + a) * gu[0] + __ldg(M + 3 + a) * gu[1]) + __ldg(M + 6 + a) * gu[2];
+    return;
+  }
   float y[3] = {x[0] - __ldg(lf + 3), x[1] - __ldg(lf + 4), x[2] - __ldg(lf + 5)};
   float Ay[3];
   d_Av(lf + LUMEN_LF_A, y, Ay);
@@ -378,6 +550,11 @@ L_DEV float d_leaf_dist(const DScene& S, int kind, int leaf, int face, const flo
     const float* p = S.plane_f + (size_t)(__ldg(li + 1) + face - 1) * LUMEN_PLANE_F;
     float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)};
     f = __ldg(p) * xl[0] + __ldg(p + 1) * xl[1] + __ldg(p + 2) * xl[2] - __ldg(p + 3);
+  } else if (__ldg(li) == 2) {  // ((rho - R)^2 + z^2 - r^2) / 2 (csg.py:470 leaf_dist)
+    float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)}, u[3];
+    d_Av(lf + LUMEN_LF_A, xl, u);
+    float dr = sqrtf(u[0] * u[0] + u[1] * u[1]) - __ldg(lf + LUMEN_LF_B), rr = __ldg(lf + LUMEN_LF_B + 1);
+    f = 0.5f * (dr * dr + u[2] * u[2] - rr * rr);
   } else {
     float y[3] = {x[0] - __ldg(lf + 3), x[1] - __ldg(lf + 4), x[2] - __ldg(lf + 5)};
     float Ay[3];
@@ -434,7 +611,7 @@ L_CALL int d_ray_holds(const DScene& S, int i, const float* od, const float* dd,
   d_to_local_pt(S, i, od, ol);
   d_to_local_dir(S, i, dd, dl);
   Scan s;
-  d_scan_init(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, D_HUGE);
+  d_scan_init<1>(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, D_HUGE);
   return d_mem_at(S, s, t, 0);
 }
 L_DEV int d_level_wins(const DScene& S, int item, int found, int excl) {
@@ -535,6 +712,7 @@ L_DEV int d_entry_wins(const DScene& S, float t, int item, const Best& b) {
   return t < b.t || (t == b.t && (b.own || d_rank(S, item) > d_rank(S, b.item)));
 }
 
+template <int TORUS>
 L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own) {
   const Side& sd = c.sd;
   float bnd = c.t_bound + c.band;
@@ -545,7 +723,7 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   float t_on = c.t_lo + D_K_ON * c.band / d_max(fabsf(sd.s), 1.0f / D_GRAZE);
   int lf_on = kn_i ? sd.leaf : -2;
   Scan s;
-  d_scan_init(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, bnd);
+  d_scan_init<TORUS>(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, bnd);
   s.want = is_own ? 0 : 1;
   s.has_init = 1; s.init_known = kn_i; s.init_inside = is_own;
   s.has_skip = 1; s.skip_leaf = lf_on; s.skip_face = sd.face; s.skip_entry = sd.entry; s.skip_thi = D_HUGE;
@@ -596,6 +774,7 @@ L_DEV void d_slab(const float* __restrict__ node_f, int node, const float* o, co
 
 // the next event in volume v: its own exit, then the first entry of every daughter the BVH does not prune. One
 // call site of the visit (the own solid is the first candidate, then the traversal yields one leaf item at a time).
+template <int TORUS>
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   Best b = {D_HUGE, -1, -1, -1, 0, 0};
   int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
@@ -661,7 +840,7 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
       }
       if (item < 0) break;
     }
-    b = d_unit_visit(S, c, item, b, is_own);
+    b = d_unit_visit<TORUS>(S, c, item, b, is_own);
   }
   return b;
 }
@@ -677,6 +856,7 @@ struct Query {
   int n_pass, vol_at, srf, rounds;
 };
 
+template <int TORUS>
 L_DEV Query d_query(const DScene& S, const float* o, const float* d, int vol, float t_max, int last, const float* sn,
                     float s_at) {
   const int OUT = S.n;
@@ -716,7 +896,7 @@ L_DEV Query d_query(const DScene& S, const float* o, const float* d, int vol, fl
     c.od[0] = o[0]; c.od[1] = o[1]; c.od[2] = o[2];
     c.dd[0] = d[0]; c.dd[1] = d[1]; c.dd[2] = d[2];
     c.t_lo = t_lo; c.t_bound = t_max; c.last = ls.item; c.band = band; c.sd = sd;
-    Best ev = d_enter(S, c, has_own, vi);
+    Best ev = d_enter<TORUS>(S, c, has_own, vi);
     float t_c = ev.t;
     int u_in = ev.item, l_in = ev.leaf, f_in = ev.face, z_in = ev.zero, is_own = ev.own;
     int hit = t_c < t_max;

@@ -196,9 +196,10 @@ L_DEV void d_pre(const Run& R, Photon& ph, Key pkey, Pre& pr) {
 
 // the step's query, bounded just past the free path where no sensor can be met (step.py:260 _query with
 // reach.py's bound; the same result as the unbounded query on everything the step reads)
+template <int TORUS>
 L_DEV Query d_step_query(const Run& R, const Photon& ph, const Pre& pr) {
   float tm = R.reach_on ? d_reach_bound(R.S, ph.x, ph.d, ph.vol, ph.srf, pr.s, R.max_distance) : R.max_distance;
-  return d_query(R.S, ph.x, ph.d, ph.vol, tm, ph.srf, ph.sn, pr.s);
+  return d_query<TORUS>(R.S, ph.x, ph.d, ph.vol, tm, ph.srf, ph.sn, pr.s);
 }
 
 // The GLOSSY outcome's facet path by the row's lobe (surface_event.py:106 _facet_path_branch, :137
@@ -608,11 +609,11 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
 }
 
 // one whole step: the megakernel's (k_trace)
-template <int G>
+template <int G, int TORUS>
 L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq) {
   Pre pr;
   d_pre(R, ph, pkey, pr);
-  Query q = d_step_query(R, ph, pr);
+  Query q = d_step_query<TORUS>(R, ph, pr);
   d_post<G>(R, ph, dw, pr, q, dep, dq);
 }
 

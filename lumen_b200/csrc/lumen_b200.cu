@@ -47,6 +47,7 @@ struct LumenScene {
   std::vector<int32_t> sigma_tabs;  // the sigma_alpha tables of the unified facet rows
   std::vector<int32_t> tab;         // host copy of the (offset, knots) table index
   std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
+  int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
 };
 
 // --------------------------------------------------------------------------------------------- the kernels
@@ -71,6 +72,7 @@ struct Launch {
   long long step_budget;
   unsigned long long* steps_used;
   Tally T;
+  int torus;  // the scene has a torus leaf (host side: picks the instantiation)
 };
 
 #define CACHE 4
@@ -173,8 +175,9 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
 // Launch shapes (LumenControls.variant): 0 = 256 threads x 4 blocks per SM (64 registers, 32 warps an SM: the
 // measured best of 128 / 256 threads at 1-8 blocks on the tank: the loop is latency- and divergence-bound, so warps
 // to switch between beat registers), 1 = 128 x 8 (64 registers), 2 = 256 x 3 (85 registers). The autotuner
-// (lumen_b200/autotune.py) picks one per workload.
-template <int G, int BLOCK, int MINB>
+// (lumen_b200/autotune.py) picks one per workload. TORUS: the instantiation with the torus leaf code, run for scenes
+// with a torus (shape 0 only); the others are compiled without it, so a scene without one pays nothing for it.
+template <int G, int BLOCK, int MINB, int TORUS>
 __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
     Dep dep;
     int stepped = active;
     double start_w = 0.0, trunc_w = 0.0;
-    if (active) d_step<G>(L.R, ph, dw, pkey, dep, dq);
+    if (active) d_step<G, TORUS>(L.R, ph, dw, pkey, dep, dq);
     health_add(sh_health, dep, w0, stepped);
     if (active) {
       c_steps++;
@@ -318,7 +321,7 @@ __device__ __forceinline__ void wv_st(uint32_t* b, int W, int i, const T& v) {
   for (int k = 0; k < (int)(sizeof(T) / 4); ++k) b[(size_t)k * W + i] = w[k];
 }
 
-template <int G>
+template <int G, int TORUS>
 __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V.W || !V.act[i]) return;
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   wv_ld(V.ex, V.W, i, ex);
   Pre pr;
   d_pre(L.R, ph, ex.pkey, pr);
-  Query q = d_step_query(L.R, ph, pr);
+  Query q = d_step_query<TORUS>(L.R, ph, pr);
   wv_st(V.ph, V.W, i, ph);
   wv_st(V.pre, V.W, i, pr);
   wv_st(V.q, V.W, i, q);
@@ -463,7 +466,7 @@ __global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
   double sum_q = 0.0, sum_qt = 0.0;
   while (ph.alive && ph.vertex < L.R.max_vertices) {
     Dep dep;
-    d_step<0>(L.R, ph, dw, pkey, dep, dq);
+    d_step<0, 1>(L.R, ph, dw, pkey, dep, dq);
     if (dep.sensor >= 0) {
       n_dep++;
       if (first_sensor < 0) first_sensor = dep.sensor;
@@ -491,7 +494,7 @@ __global__ void k_query(DScene S, const float* ray, const int32_t* vol, const in
   int known = vol[i] >= 0 && vol[i] <= S.n;
   int v = known ? vol[i] : d_locate(S, o);
   int last = known ? srf[i] : -1;
-  Query q = d_query(S, o, d, v, t_max, last, nullptr, D_HUGE);
+  Query q = d_query<1>(S, o, d, v, t_max, last, nullptr, D_HUGE);
   int32_t* oi = out_i + 8 * i;
   oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
   oi[5] = q.srf; oi[6] = q.zero;
@@ -703,6 +706,7 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   L.first_id = first_id;
   L.n = n;
   L.step_budget = c->step_budget;
+  L.torus = sc->has_torus;
   return 0;
 }
 
@@ -715,27 +719,28 @@ static int grid_for(const void* fn, int block, int* grid) {
   return 0;
 }
 
-template <int G, int BLOCK, int MINB>
+template <int G, int BLOCK, int MINB, int TORUS>
 static int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
   int grid = 0, st = 0;
-  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB>, BLOCK, &grid))) return st;
+  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS>, BLOCK, &grid))) return st;
   if (bps > 0) {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (sms * bps < grid) grid = sms * bps;
   }
-  k_trace<G, BLOCK, MINB><<<grid, BLOCK, 0, stream>>>(L);
+  k_trace<G, BLOCK, MINB, TORUS><<<grid, BLOCK, 0, stream>>>(L);
   CK(cudaGetLastError());
   return 0;
 }
 
 template <int G>
 static int launch_trace(const Launch& L, int variant, int bps, cudaStream_t stream) {
+  if (L.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream);  // tori: shape 0 whatever the variant
   switch (variant) {
-    case 1: return launch_shape<G, 128, 8>(L, bps, stream);
-    case 2: return launch_shape<G, 256, 3>(L, bps, stream);
-    default: return launch_shape<G, 256, 4>(L, bps, stream);
+    case 1: return launch_shape<G, 128, 8, 0>(L, bps, stream);
+    case 2: return launch_shape<G, 256, 3, 0>(L, bps, stream);
+    default: return launch_shape<G, 256, 4, 0>(L, bps, stream);
   }
 }
 
@@ -766,7 +771,8 @@ static int run_wave(const Launch& L, unsigned long long* live, cudaStream_t stre
   CK(cudaGetLastError());
   int st = 0;
   for (long long r = 0;; ++r) {
-    k_wave_query<G><<<grid, 256, 0, stream>>>(L, V);
+    if (L.torus) k_wave_query<G, 1><<<grid, 256, 0, stream>>>(L, V);
+    else k_wave_query<G, 0><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaMemsetAsync(V.live, 0, sizeof(unsigned long long), stream));
     k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaGetLastError());
@@ -1094,6 +1100,8 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
       sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
   }
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
+  sc->has_torus = 0;
+  for (int l = 0; l < d->n_leaf; ++l) sc->has_torus = sc->has_torus || d->leaf_i[(size_t)l * LUMEN_LEAF_I] == 2;
   for (int m = 0; m < d->n_med; ++m) {
     const int32_t* mr = d->med_i + (size_t)m * LUMEN_MED_I;
     if (mr[LUMEN_MI_WLS] >= 0) sc->spectrum_tabs.push_back(mr[LUMEN_MI_WLS_SPEC]);

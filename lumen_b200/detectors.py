@@ -94,6 +94,37 @@ def scintillating_tank() -> D.Detector:
     return D.build(tank, {"Scint": scint, "Photocathode": cathode}, borders=borders, sensors={"pmt": "PMT"})
 
 
+def solids_box() -> D.Detector:
+    """Return a 3 m water box holding one glass copy of each solid of the catalogue beyond the benchmarks' (tori,
+    cones, sphere shells with phi and theta ranges, ellipsoids, elliptical tubes and cones, paraboloids, hyperboloids,
+    polycones, polyhedra, trapezoids, tetrahedra, a phi-cut tube), each rotated, and 8 sensor discs on two walls."""  # noqa: D205
+    water = O.Material("Water", rindex=1.33, abslength=30.0, rayleigh=10.0)
+    glass = O.Material("Glass", rindex=1.5, abslength=5.0)
+    cathode = O.Material("Photocathode")
+    box = G.Volume("Box", G.Box(1.5, 1.5, 1.5), "Water")
+    solids = [G.Torus(0.15, 0.35, 0.05, 0.5, 4.5), G.Torus(0.1, 0.3), G.Cons(0.1, 0.3, 0.05, 0.2, 0.3, 0.3, 4.0),
+              G.SphereShell(0.35, 0.15, 0.5, 2.0, 0.3, 1.5), G.SphereShell(0.3, 0.0, 1.0, 5.0, 1.2, 1.4),
+              G.Ellipsoid(0.3, 0.2, 0.35, -0.2, 0.3), G.EllipticalTube(0.3, 0.2, 0.3), G.EllipticalCone(0.5, 0.3, 0.5, 0.3),
+              G.Paraboloid(0.1, 0.3, 0.3), G.Hype(0.1, 0.3, 0.3, 0.5, 0.3),
+              G.Polycone(((0.0, 0.2, -0.3), (0.05, 0.3, 0.0), (0.0, 0.1, 0.3)), 0.2, 5.0),
+              G.Polyhedra(((0.0, 0.2, -0.3), (0.05, 0.3, 0.3)), 6, 0.0, 5.0), G.Trd(0.2, 0.1, 0.3, 0.2, 0.3),
+              G.Trap(0.3, 0.2, 0.3, 0.3, 0.2, 0.26, 0.1, 0.2, 0.15, 0.19, 0.1),
+              G.Tet((0, 0, 0), (0.4, 0, 0), (0, 0.4, 0), (0, 0, 0.4)), G.Tube(0.3, 0.3, 0.1, 1.0, 2.0)]  # fmt: skip
+    for k, s in enumerate(solids):
+        i, j = divmod(k, 4)
+        rot = G.rotation("x", 17.0 * k) @ G.rotation("z", 31.0 * k)
+        box.place(G.Volume(f"S{k}", s, "Glass"), ((i - 1.5) * 0.7, (j - 1.5) * 0.7, 0.0), rot, name=f"S{k}")
+    pmt = G.Volume("PMT", G.Tube(rmax=0.15, dz=0.01), "Photocathode")
+    for i in range(4):
+        box.place(pmt, (-0.75 + 0.5 * i, 0.0, -1.48), None, name=f"PMT_{i}", copy=i)
+        box.place(pmt, (-0.75 + 0.5 * i, 0.0, 1.48), None, name=f"PMT_{4 + i}", copy=4 + i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.6, sigma_alpha=0.2, specularlobe=0.5)
+    borders = [("Box", f"PMT_{i}", surf) for i in range(8)]
+    return D.build(box, {"Water": water, "Glass": glass, "Photocathode": cathode}, borders=borders,
+                   skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
+
+
 def scintillator_cube(mie=2.0, wls=1.0, rayleigh=5.0, profile="exponential") -> D.Detector:
     """Return the tutorial tank's geometry filled with a synthetic liquid scintillator whose bulk has all three of
     Geant4's channels: Rayleigh, Mie (G4OpMieHG, MIEHG ``mie`` m, forward 0.9, backward 0.3, forward ratio 0.8) and a

@@ -7,9 +7,12 @@ the same instructions on different data (src/lumen/geometry/csg.py module docstr
 arrays is the C ABI's (include/lumen_b200.h): volume records, daughter lists, a BVH per volume over its daughters'
 world boxes (depth-first, skip pointers, one item per leaf), kinds, leaves, planes and programs.
 
-Scope: boxes, tubes (full phi, optional inner radius), spheres (full, or a hemisphere in z), and their unions,
-subtractions and intersections with a placement of the second operand; volumes nest in a tree (daughters inside their
-mother, siblings disjoint or touching).
+Scope: the Geant4 solids of the reference's catalogue whose faces are planes, quadrics or tori (solids.py:477-772):
+boxes, tubes, cones, spheres (radii, phi and theta ranges), orbs, ellipsoids, elliptical tubes and cones, paraboloids,
+hyperboloids, polycones, polyhedra, tori (a torus leaf, leaf_kernels.py:212) and the convex polytopes (trd, para, trap,
+tet, planar generic trap); their unions, subtractions and intersections with a placement of the second operand; at
+most LUMEN_MAX_LEAVES leaves a solid. Volumes nest in a tree (daughters inside their mother, siblings disjoint or
+touching).
 """
 
 from __future__ import annotations
@@ -30,7 +33,9 @@ MAX_PLANES = 8
 # ------------------------------------------------------------------------------------------------------ leaves
 @dataclass
 class Leaf:
-    """One leaf in its solid's frame: optional quadric (A, b, c about oq) and planes n.(x - og) <= h."""
+    """One leaf in its solid's frame: optional quadric (A, b, c about oq) and planes n.(x - og) <= h; or a solid
+    torus {(rho - R)^2 + z^2 <= r^2} of ``torus`` = (R, r) in the canonical coordinates u = M (x - og)
+    (src/lumen/geometry/solids.py:88 TorusLeaf: M is the inverse of its placement's linear map; no planes)."""  # noqa: D205
 
     has_q: bool
     A: np.ndarray = field(default_factory=lambda: np.zeros((3, 3)))
@@ -40,11 +45,13 @@ class Leaf:
     og: np.ndarray = field(default_factory=lambda: np.zeros(3))
     N: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
     H: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    torus: tuple | None = None
+    M: np.ndarray = field(default_factory=lambda: np.eye(3))
 
     def moved(self, R: np.ndarray, p: np.ndarray) -> Leaf:
         """Return the leaf placed by x' = R x + p (its frame rotated and shifted)."""
         return Leaf(self.has_q, R @ self.A @ R.T, R @ self.b, self.c, R @ self.oq + p, R @ self.og + p,
-                    self.N @ R.T, self.H.copy())  # fmt: skip
+                    self.N @ R.T, self.H.copy(), self.torus, self.M @ R.T)  # fmt: skip
 
 
 @dataclass
@@ -62,6 +69,40 @@ class Solid:
 
     def lower(self) -> Lowered:  # pragma: no cover - abstract
         raise NotImplementedError
+
+
+FULL_PHI_TOL = 1e-12  # rad: a phi range this close to 2 pi is the full circle (src/lumen/rules/tolerances.py:104)
+ANGLE_TOL = 1e-12
+
+
+def _combine(op: int, la: Lowered, lb: Lowered, lo, hi) -> Lowered:
+    """Return ``la op lb`` (1 union, 2 intersection, 3 subtraction), both in one frame, with the box (lo, hi)."""
+    k = len(la.leaves)
+    prog = list(la.program) + [(o, a + k) if o == 0 else (o, a) for o, a in lb.program] + [(op, 0)]
+    return Lowered(la.leaves + lb.leaves, prog, np.asarray(lo, float), np.asarray(hi, float))
+
+
+def phi_wedge(sphi: float, dphi: float) -> Lowered:
+    """Return {phi in [sphi, sphi + dphi]} (dphi < 2 pi) as planes through the z axis: one leaf of two half-spaces
+    when dphi <= pi, else the union of the two (src/lumen/geometry/solids.py:290 phi_wedge); its box unbounded."""  # noqa: D205
+    ephi = sphi + dphi
+    n1 = np.array([math.sin(sphi), -math.cos(sphi), 0.0])
+    n2 = np.array([-math.sin(ephi), math.cos(ephi), 0.0])
+    big = np.full(3, np.inf)
+    if dphi <= math.pi + ANGLE_TOL:
+        return Lowered([Leaf(False, N=np.stack([n1, n2]), H=np.zeros(2))], [(0, 0)], -big, big)
+    a = Lowered([Leaf(False, N=n1[None], H=np.zeros(1))], [(0, 0)], -big, big)
+    b = Lowered([Leaf(False, N=n2[None], H=np.zeros(1))], [(0, 0)], -big, big)
+    return _combine(1, a, b, -big, big)
+
+
+def with_phi(low: Lowered, sphi: float, dphi: float) -> Lowered:
+    """Return a solid cut to the phi range [sphi, sphi + dphi] (rad; the full circle: itself)."""
+    if not dphi > 0.0:
+        raise ValueError(f"phi range {dphi} <= 0: Geant4's constructor aborts (invalid dphi)")
+    if dphi >= 2.0 * math.pi - FULL_PHI_TOL:
+        return low
+    return _combine(2, low, phi_wedge(sphi, dphi), low.lo, low.hi)
 
 
 def _slab_planes(hx, hy, hz):
@@ -86,11 +127,13 @@ class Box(Solid):
 
 @dataclass
 class Tube(Solid):
-    """G4Tubs with a full phi range: radii and half length (m)."""
+    """G4Tubs: radii and half length (m), the phi range [sphi, sphi + dphi] (rad)."""
 
     rmax: float
     dz: float
     rmin: float = 0.0
+    sphi: float = 0.0
+    dphi: float = 2.0 * math.pi
 
     def lower(self):
         A = np.diag([1.0, 1.0, 0.0])
@@ -99,9 +142,35 @@ class Tube(Solid):
         outer = Leaf(True, A=A, c=-self.rmax**2, N=N, H=H)
         h = np.array([self.rmax, self.rmax, self.dz])
         if self.rmin <= 0.0:
-            return Lowered([outer], [(0, 0)], -h, h)
-        inner = Leaf(True, A=A.copy(), c=-self.rmin**2)
-        return Lowered([outer, inner], [(0, 0), (0, 1), (3, 0)], -h, h)
+            low = Lowered([outer], [(0, 0)], -h, h)
+        else:
+            inner = Leaf(True, A=A.copy(), c=-self.rmin**2)
+            low = Lowered([outer, inner], [(0, 0), (0, 1), (3, 0)], -h, h)
+        return with_phi(low, self.sphi, self.dphi)
+
+
+@dataclass
+class Torus(Solid):
+    """G4Torus (src/lumen/geometry/solids.py:697 g4_torus): swept radius ``rtor``, tube radii ``rmin`` and ``rmax``
+    (m), the phi range [sphi, sphi + dphi] (rad)."""  # noqa: D205
+
+    rmax: float
+    rtor: float
+    rmin: float = 0.0
+    sphi: float = 0.0
+    dphi: float = 2.0 * math.pi
+
+    def lower(self):
+        if not (0.0 <= self.rmin < self.rmax <= self.rtor):
+            raise ValueError(f"Torus: 0 <= rmin < rmax <= rtor, got {self.rmin}, {self.rmax}, {self.rtor}")
+        big = self.rtor + self.rmax
+        h = np.array([big, big, self.rmax])
+        outer = Leaf(False, torus=(float(self.rtor), float(self.rmax)))
+        low = Lowered([outer], [(0, 0)], -h, h)
+        if self.rmin > 0.0:
+            low = _combine(3, low, Lowered([Leaf(False, torus=(float(self.rtor), float(self.rmin)))], [(0, 0)], -h, h),
+                           -h, h)  # fmt: skip
+        return with_phi(low, self.sphi, self.dphi)
 
 
 @dataclass
@@ -124,6 +193,441 @@ class Sphere(Solid):
         else:
             hi[2] = 0.0
         return Lowered([leaf], [(0, 0)], lo, hi)
+
+
+# --------------------------------------------------------------------- the rest of the Geant4 catalogue (solids.py)
+CYLINDER_REL = 1e-15  # a frustum whose radii agree to this (relative) is a cylinder (tolerances.py:106)
+Z_TOL = 1e-15  # m: polycone / polyhedra sections thinner than this are dropped (tolerances.py:107)
+DEGENERATE_FACE = 1e-14  # a face normal this small (relative to the size squared) has collapsed (tolerances.py:111)
+VERTEX_TOL = 1e-9  # relative: a vertex beyond a face plane by more than this is not convex (tolerances.py:112)
+G4CONS_ZERO_RMIN = 1e-6  # m: G4Cons's inner radius standing in for a zero one opposite a non-zero one (1e3 kRadTolerance)
+FULL = 2.0 * math.pi
+
+
+def _one(leaf: Leaf, lo, hi) -> Lowered:
+    return Lowered([leaf], [(0, 0)], np.asarray(lo, float), np.asarray(hi, float))
+
+
+def _unbounded(leaf: Leaf) -> Lowered:
+    return _one(leaf, np.full(3, -np.inf), np.full(3, np.inf))
+
+
+def _planes_leaf(planes, origin=(0.0, 0.0, 0.0)) -> Leaf:
+    """The intersection of the half-spaces [(n, h)] (n . x <= h, absolute offsets) as a plane leaf at ``origin``."""
+    o = np.asarray(origin, float)
+    N = np.asarray([n for n, _ in planes], float).reshape(-1, 3)
+    H = np.asarray([h - float(np.dot(n, o)) for n, h in planes], float)
+    return Leaf(False, og=o.copy(), oq=o.copy(), N=N, H=H)
+
+
+def _frustum(z1, r1, z2, r2, caps=True, selector=True) -> Leaf:
+    """rho <= r(z), r linear from r1 at z1 to r2 at z2 (z1 < z2), origin at the section's middle: the quadric
+    rho^2 - (r0 + k z)^2 <= 0 with the nappe r0 + k z >= 0 (solids.py:253 q_frustum)."""  # noqa: D205
+    zm = 0.5 * (z1 + z2)
+    o = np.array([0.0, 0.0, zm])
+    N, H = ([[0, 0, 1.0], [0, 0, -1.0]], [z2 - zm, -(z1 - zm)]) if caps else ([], [])
+    if abs(r2 - r1) < CYLINDER_REL * max(1.0, abs(r1)):
+        return Leaf(True, A=np.diag([1.0, 1.0, 0.0]), c=-r1 * r1, oq=o, og=o.copy(),
+                    N=np.asarray(N, float).reshape(-1, 3), H=np.asarray(H, float))  # fmt: skip
+    k = (r2 - r1) / (z2 - z1)
+    r0 = 0.5 * (r1 + r2)
+    if selector:
+        N, H = [*N, [0.0, 0.0, -k]], [*H, r0]
+    return Leaf(True, A=np.diag([1.0, 1.0, -k * k]), b=np.array([0.0, 0.0, -r0 * k]), c=-r0 * r0, oq=o,
+                og=o.copy(), N=np.asarray(N, float).reshape(-1, 3), H=np.asarray(H, float))  # fmt: skip
+
+
+def _cone_theta(theta, up=True) -> Leaf:
+    """The solid cone of half-angle theta < pi / 2 about +z (up) or -z, apex at the origin."""
+    t2 = math.tan(theta) ** 2
+    return Leaf(True, A=np.diag([1.0, 1.0, -t2]), N=np.array([[0.0, 0.0, -1.0 if up else 1.0]]), H=np.zeros(1))
+
+
+def _halfspace(n, h) -> Leaf:
+    return Leaf(False, N=np.asarray([n], float), H=np.array([float(h)]))
+
+
+def convex_polytope(verts, faces) -> Lowered:
+    """The convex polytope of vertices and faces (index lists, any orientation), one plane leaf at the centroid; a
+    vertex set that is not convex is refused (solids.py:332 polytope_from_faces)."""
+    V = np.asarray(verts, float)
+    cen = V.mean(0)
+    planes = []
+    for fc in faces:
+        P = V[list(fc)]
+        nrm = np.cross(P[2] - P[0], P[3] - P[1]) if len(P) >= 4 else np.cross(P[1] - P[0], P[2] - P[0])
+        ln = float(np.linalg.norm(nrm))
+        if ln < DEGENERATE_FACE * max(1.0, float(np.abs(V).max()) ** 2):
+            continue  # a collapsed face
+        nrm = nrm / ln
+        h = float(np.dot(nrm, P.mean(0)))
+        if np.dot(nrm, cen) > h:
+            nrm, h = -nrm, -h
+        planes.append((nrm, h))
+    tol = VERTEX_TOL * max(1.0, float(np.abs(V).max()))
+    if any(float(np.max(V @ n - h)) > tol for n, h in planes):
+        raise ValueError("convex_polytope: the vertices are not convex in position (a concave base or a twisted face)")
+    if len(planes) > MAX_PLANES:
+        raise ValueError(f"convex_polytope: {len(planes)} faces, at most {MAX_PLANES}")
+    return _one(_planes_leaf(planes, cen), V.min(0), V.max(0))
+
+
+HEX_FACES = [(0, 1, 3, 2), (4, 5, 7, 6), (0, 1, 5, 4), (2, 3, 7, 6), (0, 2, 6, 4), (1, 3, 7, 5)]
+
+
+@dataclass
+class Cons(Solid):
+    """G4Cons: inner and outer radii at -dz and +dz, half length dz (m), phi range (solids.py:509 g4_cone)."""
+
+    rmin1: float
+    rmax1: float
+    rmin2: float
+    rmax2: float
+    dz: float
+    sphi: float = 0.0
+    dphi: float = FULL
+
+    def lower(self):
+        r1, r2 = self.rmin1, self.rmin2
+        if r1 == 0.0 and r2 > 0.0:
+            r1 = G4CONS_ZERO_RMIN
+        if r2 == 0.0 and r1 > 0.0:
+            r2 = G4CONS_ZERO_RMIN
+        big = max(self.rmax1, self.rmax2)
+        lo, hi = (-big, -big, -self.dz), (big, big, self.dz)
+        low = _one(_frustum(-self.dz, self.rmax1, self.dz, self.rmax2), lo, hi)
+        if r1 > 0.0 or r2 > 0.0:
+            low = _combine(3, low, _unbounded(_frustum(-self.dz, r1, self.dz, r2, caps=False)), lo, hi)
+        return with_phi(low, self.sphi, self.dphi)
+
+
+@dataclass
+class SphereShell(Solid):
+    """G4Sphere: radii rmin, rmax (m), phi range [sphi, sphi + dphi] and theta range [stheta, stheta + dtheta]
+    (rad; solids.py:626 g4_sphere, :600 _theta_cut)."""  # noqa: D205
+
+    rmax: float
+    rmin: float = 0.0
+    sphi: float = 0.0
+    dphi: float = FULL
+    stheta: float = 0.0
+    dtheta: float = math.pi
+
+    def lower(self):
+        r = self.rmax
+        lo, hi = (-r, -r, -r), (r, r, r)
+        low = _one(Leaf(True, A=np.eye(3), c=-r * r), lo, hi)
+        if self.rmin > 0.0:
+            low = _combine(3, low, _unbounded(Leaf(True, A=np.eye(3), c=-self.rmin**2)), lo, hi)
+        low = with_phi(low, self.sphi, self.dphi)
+        ts, te, h = self.stheta, self.stheta + self.dtheta, 0.5 * math.pi
+        if ts > ANGLE_TOL:  # theta < ts removed
+            if abs(ts - h) < ANGLE_TOL:
+                low = _combine(3, low, _unbounded(_halfspace((0, 0, -1), 0.0)), lo, hi)
+            elif ts < h:
+                low = _combine(3, low, _unbounded(_cone_theta(ts, up=True)), lo, hi)
+            else:
+                low = _combine(2, low, _unbounded(_cone_theta(math.pi - ts, up=False)), lo, hi)
+        if te < math.pi - ANGLE_TOL:  # theta <= te kept
+            if abs(te - h) < ANGLE_TOL:
+                low = _combine(2, low, _unbounded(_halfspace((0, 0, -1), 0.0)), lo, hi)
+            elif te < h:
+                low = _combine(2, low, _unbounded(_cone_theta(te, up=True)), lo, hi)
+            else:
+                low = _combine(3, low, _unbounded(_cone_theta(math.pi - te, up=False)), lo, hi)
+        return low
+
+
+@dataclass
+class Orb(Solid):
+    """G4Orb of radius r (m)."""
+
+    r: float
+
+    def lower(self):
+        return _one(Leaf(True, A=np.eye(3), c=-self.r**2), (-self.r,) * 3, (self.r,) * 3)
+
+
+@dataclass
+class Ellipsoid(Solid):
+    """G4Ellipsoid of semi-axes ax, by, cz (m) cut to [zcut1, zcut2] (both 0: no cut; clamped to [-cz, cz])."""
+
+    ax: float
+    by: float
+    cz: float
+    zcut1: float = 0.0
+    zcut2: float = 0.0
+
+    def lower(self):
+        a, b, c = self.ax, self.by, self.cz
+        lo, hi = (-c, c) if (self.zcut1 == 0.0 and self.zcut2 == 0.0) else (max(self.zcut1, -c), min(self.zcut2, c))
+        N, H = [], []
+        if hi < c:
+            N, H = [*N, [0, 0, 1.0]], [*H, hi]
+        if lo > -c:
+            N, H = [*N, [0, 0, -1.0]], [*H, -lo]
+        leaf = Leaf(True, A=np.diag([1 / a**2, 1 / b**2, 1 / c**2]), c=-1.0, N=np.asarray(N, float).reshape(-1, 3),
+                    H=np.asarray(H, float))  # fmt: skip
+        return _one(leaf, (-a, -b, lo), (a, b, hi))
+
+
+@dataclass
+class EllipticalTube(Solid):
+    """G4EllipticalTube of semi-axes dx, dy and half length dz (m)."""
+
+    dx: float
+    dy: float
+    dz: float
+
+    def lower(self):
+        leaf = Leaf(True, A=np.diag([1 / self.dx**2, 1 / self.dy**2, 0.0]), c=-1.0,
+                    N=np.array([[0, 0, 1.0], [0, 0, -1.0]]), H=np.array([self.dz, self.dz]))  # fmt: skip
+        return _one(leaf, (-self.dx, -self.dy, -self.dz), (self.dx, self.dy, self.dz))
+
+
+@dataclass
+class EllipticalCone(Solid):
+    """G4EllipticalCone: (x / dx)^2 + (y / dy)^2 <= (zmax - z)^2, |z| <= min(zcut, zmax) (dx, dy unitless)."""
+
+    dx: float
+    dy: float
+    zmax: float
+    zcut: float
+
+    def lower(self):
+        zm, zt = self.zmax, min(self.zcut, self.zmax)
+        leaf = Leaf(True, A=np.diag([1 / self.dx**2, 1 / self.dy**2, -1.0]), b=np.array([0.0, 0.0, zm]), c=-zm * zm,
+                    N=np.array([[0, 0, 1.0], [0, 0, -1.0], [0, 0, 1.0]]), H=np.array([zt, zt, zm]))  # fmt: skip
+        rx, ry = self.dx * (zm + zt), self.dy * (zm + zt)
+        return _one(leaf, (-rx, -ry, -zt), (rx, ry, zt))
+
+
+@dataclass
+class Paraboloid(Solid):
+    """G4Paraboloid of radii rlo at -dz and rhi at +dz (m): rho^2 <= k1 z + k2."""
+
+    rlo: float
+    rhi: float
+    dz: float
+
+    def lower(self):
+        k1 = (self.rhi**2 - self.rlo**2) / (2.0 * self.dz)
+        k2 = 0.5 * (self.rhi**2 + self.rlo**2)
+        leaf = Leaf(True, A=np.diag([1.0, 1.0, 0.0]), b=np.array([0.0, 0.0, -0.5 * k1]), c=-k2,
+                    N=np.array([[0, 0, 1.0], [0, 0, -1.0]]), H=np.array([self.dz, self.dz]))  # fmt: skip
+        return _one(leaf, (-self.rhi, -self.rhi, -self.dz), (self.rhi, self.rhi, self.dz))
+
+
+@dataclass
+class Hype(Solid):
+    """G4Hype: rho^2 <= rmax^2 + tan^2(outst) z^2 and >= rmin^2 + tan^2(inst) z^2, |z| <= dz (m, rad)."""
+
+    rmin: float
+    rmax: float
+    inst: float
+    outst: float
+    dz: float
+
+    def lower(self):
+        to2, ti2 = math.tan(self.outst) ** 2, math.tan(self.inst) ** 2
+        big = math.sqrt(self.rmax**2 + to2 * self.dz**2)
+        lo, hi = (-big, -big, -self.dz), (big, big, self.dz)
+        low = _one(Leaf(True, A=np.diag([1.0, 1.0, -to2]), c=-self.rmax**2, N=np.array([[0, 0, 1.0], [0, 0, -1.0]]),
+                        H=np.array([self.dz, self.dz])), lo, hi)  # fmt: skip
+        if self.rmin > 0.0 or self.inst > 0.0:
+            low = _combine(3, low, _unbounded(Leaf(True, A=np.diag([1.0, 1.0, -ti2]), c=-self.rmin**2)), lo, hi)
+        return low
+
+
+def _merge_affine(zs, rel=1e-12):
+    """[(z, rmin, rmax)] without the interior z-planes across which both radii stay affine in z (one straight
+    section: Geant4's RemoveRedundantVertices; solids.py:528 merge_affine)."""  # noqa: D205
+    out = list(zs[:1])
+    for k in range(1, len(zs)):
+        if k + 1 < len(zs):
+            (za, ia, oa), (zb, ib, ob), (zc, ic, oc) = out[-1], zs[k], zs[k + 1]
+            if (zb - za) * (zc - zb) > 0:
+                f = (zb - za) / (zc - za)
+                tol = rel * max(1.0, abs(za), abs(zc), abs(oa), abs(oc))
+                if abs(ia + f * (ic - ia) - ib) <= tol and abs(oa + f * (oc - oa) - ob) <= tol:
+                    continue
+        out.append(zs[k])
+    return out
+
+
+def _sections(zs):
+    for (za, ia, oa), (zb, ib, ob) in zip(zs[:-1], zs[1:], strict=True):
+        if abs(zb - za) < Z_TOL:
+            continue
+        if zb < za:
+            za, ia, oa, zb, ib, ob = zb, ib, ob, za, ia, oa
+        yield za, ia, oa, zb, ib, ob
+
+
+def _union_all(parts, lo, hi) -> Lowered:
+    if not parts:
+        raise ValueError("a solid with no part: every section is thinner than the z tolerance")
+    out = parts[0]
+    for p in parts[1:]:
+        out = _combine(1, out, p, lo, hi)
+    return Lowered(out.leaves, out.program, np.asarray(lo, float), np.asarray(hi, float))
+
+
+@dataclass
+class Polycone(Solid):
+    """G4Polycone of z-planes [(rmin, rmax, z)] (m) and phi range (dphi <= 0: the full circle; solids.py:556)."""
+
+    zplanes: tuple
+    sphi: float = 0.0
+    dphi: float = FULL
+
+    def lower(self):
+        zs = _merge_affine([(z, rmin, rmax) for rmin, rmax, z in self.zplanes])
+        big = max(z[2] for z in zs)
+        lo, hi = (-big, -big, min(z[0] for z in zs)), (big, big, max(z[0] for z in zs))
+        secs = []
+        for za, ia, oa, zb, ib, ob in _sections(zs):
+            s = _one(_frustum(za, oa, zb, ob), lo, hi)
+            if ia > 0 or ib > 0:
+                s = _combine(3, s, _unbounded(_frustum(za, ia, zb, ib, caps=False)), lo, hi)
+            secs.append(s)
+        return with_phi(_union_all(secs, lo, hi), self.sphi, FULL if self.dphi <= 0.0 else self.dphi)
+
+
+@dataclass
+class Polyhedra(Solid):
+    """G4Polyhedra of z-planes [(rmin, rmax, z)] whose radii are the distances to the sides (apothems), ``nsides``
+    sides over the phi range (dphi <= 0: the full circle; solids.py:588)."""  # noqa: D205
+
+    zplanes: tuple
+    nsides: int
+    sphi: float = 0.0
+    dphi: float = FULL
+
+    def _section(self, za, aa, zb, ab, caps):
+        dphi = FULL if self.dphi <= 0.0 else self.dphi
+        k = (ab - aa) / (zb - za)
+        planes = []
+        for i in range(self.nsides):
+            ph = self.sphi + (i + 0.5) * dphi / self.nsides
+            planes.append((np.array([math.cos(ph), math.sin(ph), -k]), aa - k * za))
+        if caps:
+            planes += [((0, 0, 1.0), zb), ((0, 0, -1.0), -za)]
+        return _planes_leaf(planes, (0.0, 0.0, 0.5 * (za + zb)))
+
+    def lower(self):
+        zs = _merge_affine([(z, rmin, rmax) for rmin, rmax, z in self.zplanes])
+        full = self.dphi >= FULL - FULL_PHI_TOL or self.dphi <= 0.0
+        dph = (FULL if self.dphi <= 0 else self.dphi) / self.nsides
+        big = max(z[2] for z in zs) / math.cos(0.5 * min(dph, math.pi - 1e-6))
+        lo, hi = (-big, -big, min(z[0] for z in zs)), (big, big, max(z[0] for z in zs))
+        secs = []
+        for za, ia, oa, zb, ib, ob in _sections(zs):
+            s = _one(self._section(za, oa, zb, ob, True), lo, hi)
+            if ia > 0 or ib > 0:
+                s = _combine(3, s, _unbounded(self._section(za, ia, zb, ib, False)), lo, hi)
+            secs.append(s)
+        low = _union_all(secs, lo, hi)
+        return low if full else _combine(2, low, phi_wedge(self.sphi, self.dphi), lo, hi)
+
+
+@dataclass
+class Trd(Solid):
+    """G4Trd: half lengths dx1, dy1 at -dz and dx2, dy2 at +dz (m)."""
+
+    dx1: float
+    dx2: float
+    dy1: float
+    dy2: float
+    dz: float
+
+    def lower(self):
+        a, b, c, d, z = self.dx1, self.dx2, self.dy1, self.dy2, self.dz
+        verts = [(-a, -c, -z), (a, -c, -z), (-a, c, -z), (a, c, -z), (-b, -d, z), (b, -d, z), (-b, d, z), (b, d, z)]
+        return convex_polytope(verts, HEX_FACES)
+
+
+@dataclass
+class Para(Solid):
+    """G4Para: half lengths dx, dy, dz (m) and the angles alpha, theta, phi (rad)."""
+
+    dx: float
+    dy: float
+    dz: float
+    alpha: float
+    theta: float
+    phi: float
+
+    def lower(self):
+        ta, tt = math.tan(self.alpha), math.tan(self.theta)
+        verts = []
+        for sz in (-1, 1):
+            for sy in (-1, 1):
+                for sx in (-1, 1):
+                    Z, Y = sz * self.dz, sy * self.dy
+                    verts.append((sx * self.dx + Y * ta + Z * tt * math.cos(self.phi), Y + Z * tt * math.sin(self.phi), Z))
+        return convex_polytope(verts, HEX_FACES)
+
+
+@dataclass
+class Trap(Solid):
+    """G4Trap: half length dz, the axis's theta and phi, and at -dz / +dz the half lengths dy1 (dx1, dx2 at -/+dy1)
+    and the angle alpha1, dy2 (dx3, dx4) and alpha2 (m, rad)."""  # noqa: D205
+
+    dz: float
+    theta: float
+    phi: float
+    dy1: float
+    dx1: float
+    dx2: float
+    alpha1: float
+    dy2: float
+    dx3: float
+    dx4: float
+    alpha2: float
+
+    def lower(self):
+        dz, tth = self.dz, math.tan(self.theta)
+        cph, sph = math.cos(self.phi), math.sin(self.phi)
+        t1, t2 = math.tan(self.alpha1), math.tan(self.alpha2)
+        verts = []
+        for s, dy, xa, xb, t in ((-1, self.dy1, self.dx1, self.dx2, t1), (1, self.dy2, self.dx3, self.dx4, t2)):
+            cx, cy = s * dz * tth * cph, s * dz * tth * sph
+            verts += [(cx - dy * t - xa, cy - dy, s * dz), (cx - dy * t + xa, cy - dy, s * dz),
+                      (cx + dy * t - xb, cy + dy, s * dz), (cx + dy * t + xb, cy + dy, s * dz)]  # fmt: skip
+        return convex_polytope(verts, HEX_FACES)
+
+
+@dataclass
+class Tet(Solid):
+    """G4Tet of four vertices (m)."""
+
+    v1: tuple
+    v2: tuple
+    v3: tuple
+    v4: tuple
+
+    def lower(self):
+        return convex_polytope([self.v1, self.v2, self.v3, self.v4], [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)])
+
+
+@dataclass
+class GenericTrap(Solid):
+    """G4GenericTrap with planar faces: eight (x, y) vertices, 0..3 at -dz and 4..7 at +dz (m); a twisted face is
+    refused."""  # noqa: D205
+
+    verts_xy: tuple
+    dz: float
+
+    def lower(self):
+        V = np.asarray([(x, y, -self.dz) for x, y in self.verts_xy[:4]] + [(x, y, self.dz) for x, y in self.verts_xy[4:]])
+        for i in range(4):
+            j = (i + 1) % 4
+            P = V[[i, j, j + 4, i + 4]]
+            nrm = np.cross(P[2] - P[0], P[3] - P[1])
+            if np.linalg.norm(nrm) > 0 and abs(np.dot(nrm / np.linalg.norm(nrm), P[1] - P[0])) > 1e-9:
+                raise NotImplementedError("GenericTrap with a twisted (non-planar) face")
+        return convex_polytope(V, [(0, 1, 2, 3), (4, 5, 6, 7)] + [(i, (i + 1) % 4, (i + 1) % 4 + 4, i + 4) for i in range(4)])
 
 
 @dataclass
@@ -352,6 +856,10 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         for lf in low.leaves:
             if lf.N.shape[0] > MAX_PLANES:
                 raise ValueError(f"a leaf of {lf.N.shape[0]} planes: at most {MAX_PLANES}")
+            if lf.torus is not None:  # typ 2: M at the quadric's A, R and r after it
+                leaf_f.append(np.concatenate([lf.og, lf.og, lf.M.ravel(), [lf.torus[0], lf.torus[1], 0.0, 0.0, 0.0]]))
+                leaf_i.append([2, len(plane_f), 0, 0])
+                continue
             sa = float(np.max(np.abs(lf.A))) if lf.has_q else 0.0
             leaf_f.append(np.concatenate([lf.og, lf.oq, lf.A.ravel(), lf.b, [lf.c, sa]]))
             leaf_i.append([1 if lf.has_q else 0, len(plane_f), lf.N.shape[0], 0])

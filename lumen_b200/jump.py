@@ -8,7 +8,8 @@ navigator's own arrays:
 - a volume whose box does not hold the node: the distance to that box (the solid lies inside it);
 - else the minimum over the volume's leaves of a lower bound of the distance to the leaf's surfaces (a boolean's
   surface lies in the union of its leaves'): a plane's distance |n . y - h| / |n| (exact), a quadric
-  f = y'Ay + 2b'y + c's the root r >= 0 of ||A|| r^2 + |grad f| r = |f| (f keeps its sign within r);
+  f = y'Ay + 2b'y + c's the root r >= 0 of ||A|| r^2 + |grad f| r = |f| (f keeps its sign within r); a torus's
+  |sqrt((rho - R)^2 + z^2) - r| in its canonical coordinates u = M (x - og), over ||M||;
 
 minus the navigator's band at the grid's scale, rounded down to float32, at most ``cap`` (the largest half-width of
 the medium's volumes: no point of it is farther from a surface). The device reads c(x) = clear[node] - |x - node| at
@@ -38,6 +39,12 @@ def _leaf_bound(arrays, g, xl):
     li = arrays["leaf_i"][g]
     out = np.full(len(xl), np.inf)
     og = lf[0:3]
+    if int(li[0]) == 2:  # a torus: |sqrt((rho - R)^2 + z^2) - r| in u = M (x - og), over ||M|| (clearance.py:17)
+        M = lf[6:15].reshape(3, 3)
+        u = (xl - og) @ M.T
+        rho = np.hypot(u[:, 0], u[:, 1])
+        du = np.abs(np.hypot(rho - lf[15], u[:, 2]) - lf[16])
+        return du / float(np.linalg.norm(M, 2))
     for k in range(int(li[2])):
         p = np.asarray(arrays["plane_f"][int(li[1]) + k], np.float64)
         nn = max(float(np.linalg.norm(p[:3])), 1e-300)

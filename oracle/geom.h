@@ -10,6 +10,8 @@
 #ifndef LUMEN_ORACLE_GEOM_H
 #define LUMEN_ORACLE_GEOM_H
 
+#include <algorithm>
+
 #include "../include/lumen_b200.h"
 #include "lmath.h"
 
@@ -145,6 +147,119 @@ static inline void o_quad_line(const float* lf, const float* y, const float* d, 
 }
 
 /* a leaf's two intervals along o + t d (kind frame): csg.py:116 _planes, :138 _q_iv */
+/* ------------------------------------------------------------------------------------------------ the torus */
+/* leaf_kernels.py:212 torus_set on a unit ray o + s d in the torus's canonical frame: g(s) = (rho - R)^2 + z^2 - r^2
+   bracketed on the padded bounding sphere, split at its (closed-form) inflection points, the extrema and then the
+   roots of the six monotone pieces found by bisection; csg.py:175 the whole line's ball / slab / annulus pretests */
+#define O_BISECT 40
+#define O_TORUS_BRACKET_ULPS 64.0f
+#define O_TORUS_AXIAL 1e-12f
+#define O_TORUS_PAD_REL 1e-4f
+
+static inline float o_torus_g(float R, float r, const float* oc, const float* d, float s) {
+  const float p[3] = {oc[0] + s * d[0], oc[1] + s * d[1], oc[2] + s * d[2]};
+  const float rho2 = p[0] * p[0] + p[1] * p[1];
+  const float dr = (rho2 - R * R) / (sqrtf(o_max(rho2, 0.0f)) + R);
+  return dr * dr + p[2] * p[2] - r * r;
+}
+static inline float o_torus_dg(float R, const float* oc, const float* d, float s) {
+  const float p[3] = {oc[0] + s * d[0], oc[1] + s * d[1], oc[2] + s * d[2]};
+  const float rho2 = p[0] * p[0] + p[1] * p[1];
+  const float rho = sqrtf(o_max(rho2, O_TINY_NORMAL));
+  const float dr = (rho2 - R * R) / (rho + R);
+  return 2.0f * dr * ((p[0] * d[0] + p[1] * d[1]) / rho) + 2.0f * p[2] * d[2];
+}
+static inline int o_torus_meets(float R, float r, const float* o, const float* d) {
+  const float Rb = (R + r) * (1.0f + O_TORUS_PAD_REL);
+  const float bb = o[0] * d[0] + o[1] * d[1] + o[2] * d[2];
+  const float disc = Rb * Rb - (o[0] * o[0] + o[1] * o[1] + o[2] * o[2] - bb * bb);
+  const float sq = sqrtf(o_max(disc, 0.0f));
+  float lo = -bb - sq, hi = -bb + sq;
+  int meet = disc > 0.0f && lo <= hi;
+  const float pad = O_TORUS_PAD_REL * (R + r), rz = r + pad;
+  const int flat = fabsf(d[2]) < O_PARALLEL;
+  const float iz = 1.0f / (flat ? 1.0f : d[2]);
+  if (!flat) {
+    const float za = (-rz - o[2]) * iz, zb = (rz - o[2]) * iz;
+    lo = o_max(lo, o_min(za, zb));
+    hi = o_min(hi, o_max(za, zb));
+  }
+  meet = meet && lo <= hi && (!flat || fabsf(o[2]) <= rz);
+  const float qa = d[0] * d[0] + d[1] * d[1], qb = o[0] * d[0] + o[1] * d[1], qc = o[0] * o[0] + o[1] * o[1];
+  const float sm = o_min(o_max(-qb / (qa > O_PARALLEL ? qa : 1.0f), lo), hi);
+  const float near2 = qa > O_PARALLEL ? qa * sm * sm + 2.0f * qb * sm + qc : qc;
+  const float far2 = o_max(qa * lo * lo + 2.0f * qb * lo + qc, qa * hi * hi + 2.0f * qb * hi + qc);
+  const float rout = R + r + pad, rin = o_max(R - r - pad, 0.0f);
+  return meet && near2 <= rout * rout && far2 >= rin * rin;
+}
+static inline void o_torus_set(float R, float r, const float* o, const float* d, float* lo, float* hi) {
+  const float tc = -((o[0] * d[0] + o[1] * d[1]) + o[2] * d[2]);
+  const float oc[3] = {o[0] + tc * d[0], o[1] + tc * d[1], o[2] + tc * d[2]};
+  const float q0 = (oc[0] * oc[0] + oc[1] * oc[1]) + oc[2] * oc[2];
+  const float Rb = (R + r) * (1.0f + O_TORUS_BRACKET_ULPS * O_EPS32);
+  const float b0 = (oc[0] * d[0] + oc[1] * d[1]) + oc[2] * d[2];
+  const float disc = Rb * Rb - q0 + b0 * b0;
+  const int in_ball = disc > 0.0f;
+  const float sq = sqrtf(in_ball ? disc : 1.0f);
+  const float s0 = -b0 - sq, s1 = -b0 + sq;
+  const float a = d[0] * d[0] + d[1] * d[1];
+  const float bxy = oc[0] * d[0] + oc[1] * d[1];
+  const float cxy = oc[0] * oc[0] + oc[1] * oc[1];
+  const int off_axis = a > O_TORUS_AXIAL;
+  const float as = off_axis ? a : 1.0f;
+  const float sv = off_axis ? -bxy / as : 0.0f;
+  const float m2 = o_max(off_axis ? cxy - bxy * bxy / as : cxy, 0.0f);
+  const float cr = o_cbrt(R * a * m2);
+  const float w2 = (cr * cr - m2) / as;
+  const float w = sqrtf(off_axis && w2 > 0.0f ? w2 : 0.0f);
+  const float p1 = o_min(o_max(sv - w, s0), s1), p2 = o_min(o_max(sv + w, s0), s1);
+  const float a0[3] = {s0, p1, p2}, a1[3] = {p1, p2, s1};
+  float ex[3];
+  for (int k = 0; k < 3; ++k) { /* g' rises through its minima, falls through its maximum */
+    float l = a0[k], h = a1[k];
+    for (int it = 0; it < O_BISECT; ++it) {
+      const float m = 0.5f * (l + h);
+      const float gp = o_torus_dg(R, oc, d, m);
+      if (k == 1 ? gp > 0.0f : gp < 0.0f) l = m; else h = m;
+    }
+    ex[k] = 0.5f * (l + h);
+  }
+  const float kn[7] = {s0, ex[0], p1, ex[1], p2, ex[2], s1};
+  float roots[6];
+  for (int k = 0; k < 6; ++k) {
+    const int in_l = o_torus_g(R, r, oc, d, kn[k]) <= 0.0f, in_r = o_torus_g(R, r, oc, d, kn[k + 1]) <= 0.0f;
+    float l = kn[k], h = kn[k + 1];
+    for (int it = 0; it < O_BISECT; ++it) {
+      const float m = 0.5f * (l + h);
+      if ((o_torus_g(R, r, oc, d, m) <= 0.0f) == in_l) l = m; else h = m;
+    }
+    roots[k] = (in_l != in_r && kn[k + 1] > kn[k] && in_ball) ? 0.5f * (l + h) + tc : O_HUGE;
+  }
+  std::sort(roots, roots + 6);
+  const int ok0 = roots[1] < O_BIG, ok1 = roots[3] < O_BIG;
+  lo[0] = ok0 ? roots[0] : O_HUGE; hi[0] = ok0 ? roots[1] : O_HUGE;
+  lo[1] = ok1 ? roots[2] : O_HUGE; hi[1] = ok1 ? roots[3] : O_HUGE;
+}
+/* a torus leaf along o + t d (kind frame): canonical frame u = M (x - og), the unit ray, the roots scaled back
+   (csg.py:207 _t_iv) */
+static inline void o_torus_line(const float* lf, const float* o, const float* d, float* L0, float* R0, float* L1,
+                                float* R1) {
+  const float* M = lf + LUMEN_LF_A;
+  const float R = lf[LUMEN_LF_B], r = lf[LUMEN_LF_B + 1];
+  const float xl[3] = {o[0] - lf[0], o[1] - lf[1], o[2] - lf[2]};
+  float ou[3], dl[3];
+  o_Av(M, xl, ou);
+  o_Av(M, d, dl);
+  const float kk = sqrtf(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
+  const float du[3] = {dl[0] / kk, dl[1] / kk, dl[2] / kk};
+  float lo[2] = {O_HUGE, O_HUGE}, hi[2] = {O_HUGE, O_HUGE};
+  if (o_torus_meets(R, r, ou, du)) o_torus_set(R, r, ou, du, lo, hi);
+  *L0 = fabsf(lo[0]) < O_BIG ? lo[0] / kk : lo[0];
+  *R0 = fabsf(hi[0]) < O_BIG ? hi[0] / kk : hi[0];
+  *L1 = fabsf(lo[1]) < O_BIG ? lo[1] / kk : lo[1];
+  *R1 = fabsf(hi[1]) < O_BIG ? hi[1] / kk : hi[1];
+}
+
 static inline OIv o_leaf_iv(const OScene* S, int g, const float* o, const float* d) {
   const float* lf = o_lf(S, g);
   const int32_t* li = o_li(S, g);
@@ -169,6 +284,10 @@ static inline OIv o_leaf_iv(const OScene* S, int g, const float* o, const float*
   float L0 = -inf, R0 = inf, L1 = inf, R1 = -inf;
   int L0q = 0, R0q = 0;
   if (has_q) o_quad_line(lf, y, d, &L0, &R0, &L0q, &R0q, &L1, &R1);
+  if (li[0] == 2) {
+    o_torus_line(lf, o, d, &L0, &R0, &L1, &R1);
+    L0q = R0q = 1;
+  }
   OIv r;
   /* clip each piece by the slab */
   {
@@ -181,7 +300,7 @@ static inline OIv o_leaf_iv(const OScene* S, int g, const float* o, const float*
   {
     float lo = o_max(L1, t0p), hi = o_min(R1, t1p);
     int flo = L1 > t0p ? 0 : f0p;
-    int fhi = R1 < t1p ? f1p : f1p; /* R1 is never a quadric root (Rq false) */
+    int fhi = R1 < t1p ? 0 : f1p; /* a quadric's second piece is unbounded above; a torus's ends at a root */
     int ok = lo < hi && !ep;
     r.lo1 = ok ? lo : inf; r.hi1 = ok ? hi : inf; r.f_lo1 = ok ? flo : -1; r.f_hi1 = ok ? fhi : -1;
   }
@@ -203,6 +322,12 @@ static inline int o_inside_leaf(const OScene* S, int g, const float* x) {
   for (int k = 0; k < li[2]; ++k) {
     const float* p = o_pl(S, li[1] + k);
     pl = pl && (p[0] * xl[0] + p[1] * xl[1] + p[2] * xl[2] <= p[3]);
+  }
+  if (li[0] == 2) { /* the torus reads no planes: (rho - R)^2 + z^2 <= r^2 */
+    float u[3];
+    o_Av(lf + LUMEN_LF_A, xl, u);
+    const float dr = sqrtf(u[0] * u[0] + u[1] * u[1]) - lf[LUMEN_LF_B];
+    return dr * dr + u[2] * u[2] <= lf[LUMEN_LF_B + 1] * lf[LUMEN_LF_B + 1];
   }
   if (li[0] != 1) return pl;
   float Ay[3];
@@ -363,6 +488,17 @@ static inline void o_leaf_grad(const OScene* S, int kind, int leaf, int face, co
     g[0] = p[0]; g[1] = p[1]; g[2] = p[2];
     return;
   }
+  if (li[0] == 2) { /* M^T ((rho - R) / rho u_x, (rho - R) / rho u_y, u_z) */
+    const float* M = lf + LUMEN_LF_A;
+    const float xl[3] = {x[0] - lf[0], x[1] - lf[1], x[2] - lf[2]};
+    float u[3];
+    o_Av(M, xl, u);
+    const float rho = sqrtf(o_max(u[0] * u[0] + u[1] * u[1], O_DIVISOR_FLOOR));
+    const float k = (rho - lf[LUMEN_LF_B]) / rho;
+    const float gu[3] = {k * u[0], k * u[1], u[2]};
+    for (int a = 0; a < 3; ++a) g[a] = (M[a] * gu[0] + M[3 + a] * gu[1]) + M[6 + a] * gu[2];
+    return;
+  }
   float y[3] = {x[0] - lf[LUMEN_LF_OQ], x[1] - lf[LUMEN_LF_OQ + 1], x[2] - lf[LUMEN_LF_OQ + 2]};
   float Ay[3];
   o_Av(lf + LUMEN_LF_A, y, Ay);
@@ -379,6 +515,12 @@ static inline float o_leaf_dist(const OScene* S, int kind, int leaf, int face, c
     const float* p = o_pl(S, li[1] + face - 1);
     float xl[3] = {x[0] - lf[LUMEN_LF_OG], x[1] - lf[LUMEN_LF_OG + 1], x[2] - lf[LUMEN_LF_OG + 2]};
     f = p[0] * xl[0] + p[1] * xl[1] + p[2] * xl[2] - p[3];
+  } else if (li[0] == 2) {
+    const float xl[3] = {x[0] - lf[0], x[1] - lf[1], x[2] - lf[2]};
+    float u[3];
+    o_Av(lf + LUMEN_LF_A, xl, u);
+    const float dr = sqrtf(u[0] * u[0] + u[1] * u[1]) - lf[LUMEN_LF_B], r = lf[LUMEN_LF_B + 1];
+    f = 0.5f * (dr * dr + u[2] * u[2] - r * r);
   } else {
     float y[3] = {x[0] - lf[LUMEN_LF_OQ], x[1] - lf[LUMEN_LF_OQ + 1], x[2] - lf[LUMEN_LF_OQ + 2]};
     float Ay[3];

@@ -138,9 +138,14 @@ def test_batched_tracks_match(tank, built):
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
 
 
-@pytest.mark.parametrize("which", ["toy", "tank", "lar"])
-def test_query_and_locate_bit_exact(which, toy, tank, lar, built):
-    det = {"toy": toy, "tank": tank, "lar": lar}[which]
+@pytest.fixture(scope="module")
+def solids():
+    return detectors.solids_box()
+
+
+@pytest.mark.parametrize("which", ["toy", "tank", "lar", "solids"])
+def test_query_and_locate_bit_exact(which, toy, tank, lar, solids, built):
+    det = {"toy": toy, "tank": tank, "lar": lar, "solids": solids}[which]
     rng = np.random.default_rng(7)
     n = 20000
     lo, hi = det.arrays["vol_f"][0, 12:15], det.arrays["vol_f"][0, 15:18]
@@ -405,3 +410,11 @@ def test_material_scintillation_bit_exact(built):
     with pytest.raises(A.EngineError):
         eng.trace(KEY, n, source=ds, controls=A.controls(grad_tabs=[det.params_index["media/Scint/scint_yield"]]),
                   tallies=T)  # fmt: skip
+
+
+def test_solids_box_photons_bit_exact(solids, built):
+    """Photons refracting through every solid of the catalogue (tori by bisection, cones, shells cut in phi and theta,
+    quadrics, polycones, polyhedra, polytopes): every photon's record is the checker's."""
+    src = sources.Point(position=(0.05, 0.02, -0.6), n_photons=1.0, lam=400.0)
+    bad, gi, oi, gf, of = _records_match(solids, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
