@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 8
+#define LUMEN_B200_ABI_VERSION 9
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -208,8 +208,18 @@ enum { LUMEN_F_ASYNC = 1,   /* controls.flags: enqueue only (no host wait, no st
                                  CUDA graph); a step budget that ran out then shows in counts[LUMEN_C_ABORTED] */
        LUMEN_F_REACH = 2,    /* bound bulk steps' queries by the scene's sensor reach (exact: every tally is the same;
                                 off by default, a speed-up only where bulk steps are common and sensors far) */
-       LUMEN_F_JUMP = 4 };   /* the diffusion jump at bulk Rayleigh events (fastpath.py; lumen.simulate's default):
+       LUMEN_F_JUMP = 4,     /* the diffusion jump at bulk Rayleigh events (fastpath.py; lumen.simulate's default):
                                 the same estimator in law as the plain walk, not the same photons */
+       LUMEN_F_TRUTH = 8 };  /* truth rows (src/lumen/readout/truth.py): each photon carries its analog photon
+                                (src/lumen/transport/state.py:30 Analog, step.py:625 _analog_crossing, :649
+                                _analog_roulette) and writes its record to LumenTallies.truth; forward runs at one set
+                                of values only (no gradient parameters, no distinct reference pool), the persistent
+                                loop (shape 0) whatever the variant, row weights <= 1 */
+/* A photon's analog record (LumenTallies.truth, one per photon of the call, 32-bit words): the sensor it was absorbed
+   on (-1: none), the time (ns) and wavelength (nm) there, the sensor row's 1 / A_n (1 unless read per normal
+   incidence), the crossing point (m, world) and the volume entered */
+enum { LUMEN_TR_SENSOR = 0, LUMEN_TR_TIME, LUMEN_TR_LAM, LUMEN_TR_SCALE, LUMEN_TR_POS, LUMEN_TR_VOL = 7,
+       LUMEN_TRUTH_WORDS = 8 };
 enum { LUMEN_VARIANT_WAVEFRONT = 3, LUMEN_N_VARIANT = 4 };
 /* launch variants: the persistent photon loop at 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
    2 = 256 x 3 (85 registers); 3 = the wavefront: rounds of two kernels (the query; the rest of the step and the
@@ -292,6 +302,7 @@ typedef struct LumenTallies {
                                 charge cells)^2, the pe moment of src/lumen/readout/fill.py:200 */
   void* records;
   int64_t rec_capacity;
+  float* truth;              /* device, n (the call's photons) * LUMEN_TRUTH_WORDS: the analog records (LUMEN_F_TRUTH) */
 } LumenTallies;
 
 /* ------------------------------------------------------------------------------------------- entry points */

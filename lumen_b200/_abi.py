@@ -32,6 +32,8 @@ REC_WORDS = 20
 F_ASYNC = 1
 F_REACH = 2
 F_JUMP = 4
+F_TRUTH = 8
+TRUTH_WORDS = 8
 N_VARIANT = 4
 VARIANT_WAVEFRONT = 3
 UNI_NX, UNI_NY = 257, 69
@@ -101,7 +103,8 @@ class LumenTallies(ctypes.Structure):
                 ("bin_w", ctypes.c_float), ("arrival", c_f64p), ("arrival_t", c_f64p), ("arrival2", c_f64p),
                 ("hist", c_f64p), ("jac", c_f64p), ("health", c_f64p), ("counts", c_u64p),
                 ("n_groups", ctypes.c_int32), ("reserved", ctypes.c_int32), ("groups", ctypes.POINTER(LumenGroup)),
-                ("pe2", c_f64p), ("records", ctypes.c_void_p), ("rec_capacity", ctypes.c_int64)]  # fmt: skip
+                ("pe2", c_f64p), ("records", ctypes.c_void_p), ("rec_capacity", ctypes.c_int64),
+                ("truth", c_f32p)]  # fmt: skip
 
 
 def iptr(a):

@@ -19,6 +19,7 @@ import torch
 
 from lumen_b200 import _abi as A
 from lumen_b200 import readout as RO
+from lumen_b200 import truth as TR
 from lumen_b200.engine import DeviceRows, DeviceSource, DeviceTallies, Engine
 from lumen_b200.sources import FromArrays
 
@@ -94,7 +95,7 @@ def _engine(det, device=None) -> Engine:
 
 
 def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, controls=None, chunk=None,
-             gradients=(), time_bins=None, groups=None, records=None, device=None, stream=None) -> Light:
+             gradients=(), time_bins=None, groups=None, records=None, truth=None, device=None, stream=None) -> Light:
     """Return the Light of ``samples`` photons of ``source`` in detector ``det`` (lumen.simulate's signature).
 
     ``params``: {parameter name: value} overriding the detector's values (``det.params()``); ``reference``: the
@@ -109,6 +110,9 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     are the detector's group of that name, else every sensor) into ``Light.groups`` (src/lumen/readout/grid.py
     Histograms); ``records``: the deposit records one launch may keep for them (default 2 per photon, at least 2^16;
     a launch that outgrows it is re-run with room for what it needed, as the reference's RecordsOverflow retry).
+    ``truth``: a ``lumen_b200.truth.Truth``: the run's truth rows in ``Light.truth`` (``TruthHits``: each photon's
+    analog record thinned by detection at the groups' efficiency and acceptance). Not differentiable; at one set of
+    values (no ``reference``); each source row at most one photon (samples >= the photons emitted).
     """
     eng = _engine(det, device)
     live = det.pool_with(params)
@@ -119,6 +123,16 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     gt = [det.params_index[k] for k in gnames]
     variant = ctl["variant"] if ctl["variant"] is not None else (A.VARIANT_WAVEFRONT if gt else 0)
     flags = A.F_JUMP if ctl["jump"] else 0  # the diffusion jump on, as lumen.simulate (src/lumen/api.py:1157)
+    if truth is not None:  # src/lumen/api.py:1296 _truth_setup
+        if not isinstance(truth, TR.Truth):
+            raise ValueError(f"simulate: truth is a lumen_b200.truth.Truth, got {truth!r}")
+        if gt:
+            raise ValueError("simulate: truth rows are not differentiable; take the derivative of a run without truth=")
+        if reference is not None:
+            raise ValueError("simulate: truth rows decide each photon's fate at the run's own values; leave reference out")
+        if not ctl["roulette"] <= 1.0:
+            raise ValueError("simulate: with truth rows the roulette must be <= 1")
+        flags |= A.F_TRUTH
     c = A.controls(ctl["max_distance"] or 0.0, ctl["roulette"], ctl["max_vertices"], gt, variant=variant, flags=flags)
     if isinstance(source, FromArrays):
         rows = source.rows()
@@ -133,6 +147,14 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
         total = dsrc.total
     if total > MAX_ID:
         raise ValueError(f"a run traces at most {MAX_ID} photons (int32 ids)")
+    if truth is not None:
+        if isinstance(source, FromArrays):
+            TR.check_weights(drows.w.cpu().numpy() if hasattr(drows, "w") else source.rows()["w"])
+        elif dsrc.c.kind in (A.SRC_CHERENKOV, A.SRC_SCINT_MATERIAL):
+            raise ValueError("simulate: truth rows need row weights known before the run (<= 1 photon each); a "
+                             "Cherenkov or material scintillation source weighs its rows on the device")
+        else:
+            TR.check_weights(source.arrays(n, det)["ev_w"])
     nb, t0, tw = (0, 0.0, 1.0) if time_bins is None else time_bins
     T = DeviceTallies(det.n_sensor, n_ev, nb, t0, tw, len(gt), eng.device)
     G = None
@@ -141,14 +163,22 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
         G = RO.GroupCells(det, groups, n_ev, eng.device)
         T.attach_groups(G, int(records) if records else max(1 << 16, 2 * min(step, total)))
     key = A.key_of_seed(seed)
+    hits = None
     for _attempt in range(4):
         try:
+            hits = []
             for first in range(0, total, max(step, 1)):
                 m = min(step, total - first)
                 if drows is not None and first > 0:
                     raise ValueError("explicit rows run in one launch")
                 before = int(T.counts[A.C_RECORDS].item()) if G is not None else 0
+                if truth is not None:
+                    T.attach_truth(m)
                 eng.trace(key, m, source=dsrc, rows=drows, first_id=first, controls=c, tallies=T, stream=stream)
+                if truth is not None:
+                    hits.append(TR.rows(truth, det, T.truth.cpu().numpy()[:m], key, first,
+                                        _labels(source, dsrc, first, m, n_ev),
+                                        dict(zip(G.names, G.groups)) if G is not None else None))  # fmt: skip
             break
         except A.RecordsOverflow:  # the launch's records outgrew the scratch: every tally again with room for them
             need = int(T.counts[A.C_RECORDS].item()) - before
@@ -156,7 +186,21 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
             T.attach_groups(G, need + need // 4 + 1024)
     else:
         raise A.RecordsOverflow(A.ERR_RECORDS, "the deposit records kept outgrowing the scratch")
-    return _light(det, T, n_ev, total, seed, gnames, (nb, t0, tw), source, G)
+    light = _light(det, T, n_ev, total, seed, gnames, (nb, t0, tw), source, G)
+    if truth is not None:
+        light.truth = TR.join(hits, total)
+    return light
+
+
+def _labels(source, dsrc, first, m, n_ev):
+    """The events of photons first .. first + m - 1 (None with one event: label -1)."""
+    if n_ev <= 1:
+        return None
+    ids = first + np.arange(m)
+    if isinstance(source, FromArrays):
+        return np.asarray(source.event, np.int32)[ids]
+    ev_first = dsrc.ev_first.cpu().numpy()
+    return (np.searchsorted(ev_first, ids, side="right") - 1).astype(np.int32)
 
 
 def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):

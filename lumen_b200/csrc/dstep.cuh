@@ -235,8 +235,19 @@ L_CALL void d_glossy(const Run& R, int row, float sig_r, float sig_l, float n1, 
 }
 
 // the step after its query (step.py:516 step: the crossing, the event, the deposit, the roulette)
-template <int G>
-L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Query& q, Dep& dep, float* dq) {
+// the analog photon riding on a tracked one (truth rows; state.py:30 Analog): x uniform on [0, w) while its fate is
+// open (inf once decided), k its row's analog weight (<= 1), and at its cathode absorption the sensor (-1 none), time,
+// wavelength, the row's 1 / A_n, the crossing point and the volume entered
+#define D_ANALOG_STREAM 0x7A4A1061u  // the photon key's fold of its analog uniform (rng.py:23)
+struct Ana {
+  float x, k;
+  int sensor;
+  float time, lam, scale, pos[3];
+  int vol;
+};
+
+template <int G, int ANALOG = 0>
+L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Query& q, Dep& dep, float* dq, Ana& an) {
   const DScene& S = R.S;
   const int P = G > 0 ? R.P : 0;
   const float b0 = pr.b0, s = pr.s;
@@ -551,9 +562,39 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
   float w_new = nx_w;
   int low = wr < R.roulette;
   float p_s = wr / R.roulette;
-  int keep = low ? (uniform(vkey, 6) < p_s) : 0;
+  int keep;
+  if (ANALOG) {
+    // step.py:625 _analog_crossing: absorbed at the crossing's reached share (x < share), else x - share; decided
+    // once x is beyond the weight the event leaves
+    const float inf = __int_as_float(0x7f800000);
+    float share = (at_if && !scatter) ? ph.w * att_if * p_det : 0.0f;
+    if (an.x < share) {
+      an.sensor = at_if ? sensor_q : -1;
+      an.time = time;
+      an.lam = ph.lam;
+      an.scale = 1.0f;
+      if (row >= 0 && __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL)) {
+        float a = d_normal_absorptance(S, R.live, row, ph.lam, ml.n, q.normal);
+        an.scale = a > 0.0f ? 1.0f / a : 0.0f;
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) an.pos[a] = ph.x[a] + dist * ph.d[a];
+      an.vol = q.vol_after;
+      an.x = inf;
+    } else {
+      float xr = an.x - share;
+      an.x = xr < nx_w ? xr : inf;
+    }
+    // step.py:649 _analog_roulette: an open analog fate is always kept; the keep's total stays p_s
+    float pi = wr * an.k;
+    float extra = (p_s - pi) / (pi < 1.0f ? 1.0f - pi : 1.0f);
+    keep = low ? (an.x < inf || uniform(vkey, 6) < extra) : 0;
+  } else {
+    keep = low ? (uniform(vkey, 6) < p_s) : 0;
+  }
   int kept = low && keep, lostr = low && !keep;
   float p_kept = kept ? p_s : 1.0f;
+  if (ANALOG && kept && an.x < __int_as_float(0x7f800000)) an.x = an.x / p_kept;
   float w_in = w_new;
   w_new = kept ? w_new / p_kept : (lostr ? 0.0f : w_new);
   float rouletted = (ph.alive && nx_ok) ? w_in - w_new : 0.0f;
@@ -609,12 +650,12 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
 }
 
 // one whole step: the megakernel's (k_trace)
-template <int G, int TORUS>
-L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq) {
+template <int G, int TORUS, int ANALOG = 0>
+L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq, Ana& an) {
   Pre pr;
   d_pre(R, ph, pkey, pr);
   Query q = d_step_query<TORUS>(R, ph, pr);
-  d_post<G>(R, ph, dw, pr, q, dep, dq);
+  d_post<G, ANALOG>(R, ph, dw, pr, q, dep, dq, an);
 }
 
 // ------------------------------------------------------------------------------------------------ sources

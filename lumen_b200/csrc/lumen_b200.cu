@@ -72,7 +72,13 @@ struct Launch {
   long long step_budget;
   unsigned long long* steps_used;
   Tally T;
-  int torus;  // the scene has a torus leaf (host side: picks the instantiation)
+  float* truth;  // the photons' analog records (truth rows, LUMEN_F_TRUTH: the ANALOG instantiation), else null
+};
+
+// what picks a launch's instantiation, host side: the scene has a torus leaf; the run keeps truth rows
+struct Pick {
+  int torus;
+  int analog;
 };
 
 #define CACHE 4
@@ -177,7 +183,8 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
 // to switch between beat registers), 1 = 128 x 8 (64 registers), 2 = 256 x 3 (85 registers). The autotuner
 // (lumen_b200/autotune.py) picks one per workload. TORUS: the instantiation with the torus leaf code, run for scenes
 // with a torus (shape 0 only); the others are compiled without it, so a scene without one pays nothing for it.
-template <int G, int BLOCK, int MINB, int TORUS>
+// ANALOG: each photon carries its analog photon and writes its record (truth rows: LUMEN_F_TRUTH; G = 0, shape 0).
+template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
@@ -188,6 +195,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   Key pkey = {0u, 0u};
   int active = 0, ev = 0;
   double w0 = 0.0;
+  Ana an;
+  int64_t gi = 0;
   // the health fates, summed per block in shared memory (a step adds its non-zero fates times the row weight): no
   // per-thread accumulators stay live across the step
   __shared__ double sh_health[LUMEN_N_HEALTH];
@@ -219,6 +228,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
           pt.n = 0;
           if (G > 0)
             for (int p = 0; p < L.R.P; ++p) dw[p] = 0.0f;
+          if (ANALOG) {  // run.py:319: one uniform of its own stream, open with probability k (state.py:58)
+            float u = uniform(fold_in(pkey, D_ANALOG_STREAM), 0);
+            an.k = r.w0;
+            an.x = u < an.k ? u / (an.k > 0.0f ? an.k : 1.0f) : __int_as_float(0x7f800000);
+            an.sensor = -1;
+            an.time = 0.0f; an.lam = 0.0f; an.scale = 1.0f;
+            an.pos[0] = an.pos[1] = an.pos[2] = 0.0f;
+            an.vol = -1;
+            gi = (int64_t)g;
+          }
         }
       }
     }
@@ -226,7 +245,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
     Dep dep;
     int stepped = active;
     double start_w = 0.0, trunc_w = 0.0;
-    if (active) d_step<G, TORUS>(L.R, ph, dw, pkey, dep, dq);
+    if (active) d_step<G, TORUS, ANALOG>(L.R, ph, dw, pkey, dep, dq, an);
     health_add(sh_health, dep, w0, stepped);
     if (active) {
       c_steps++;
@@ -237,6 +256,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
       if (!ph.alive || ph.vertex >= L.R.max_vertices) {
         flush_all(L.T, ev, pt);
         if (L.R.rec && ph.last >= 0) d_record_head(L.R, ph.last, (float)w0, ev);
+        if (ANALOG) {  // the photon's analog record (run.py:350 per_item)
+          float* tr = L.truth + (size_t)gi * LUMEN_TRUTH_WORDS;
+          tr[LUMEN_TR_SENSOR] = __int_as_float(an.sensor);
+          tr[LUMEN_TR_TIME] = an.time;
+          tr[LUMEN_TR_LAM] = an.lam;
+          tr[LUMEN_TR_SCALE] = an.scale;
+          tr[LUMEN_TR_POS] = an.pos[0]; tr[LUMEN_TR_POS + 1] = an.pos[1]; tr[LUMEN_TR_POS + 2] = an.pos[2];
+          tr[LUMEN_TR_VOL] = __int_as_float(an.vol);
+        }
         if (ph.alive) {
           trunc_w = (double)ph.w * w0;
           c_trunc++;
@@ -366,7 +394,8 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
     wv_ld(V.q, V.W, i, q);
     if (G > 0)
       for (int p = 0; p < L.R.P; ++p) dw[p] = V.dw[(size_t)p * V.W + i];
-    d_post<G>(L.R, ph, dw, pr, q, dep, dq);
+    Ana an;
+    d_post<G>(L.R, ph, dw, pr, q, dep, dq, an);
     c_steps++;
     if (dep.sensor >= 0) {
       c_multi += deposit<G>(L.T, ex.ev, dep, dq, ex.w0, ex.pt);
@@ -466,7 +495,8 @@ __global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
   double sum_q = 0.0, sum_qt = 0.0;
   while (ph.alive && ph.vertex < L.R.max_vertices) {
     Dep dep;
-    d_step<0, 1>(L.R, ph, dw, pkey, dep, dq);
+    Ana an;
+    d_step<0, 1>(L.R, ph, dw, pkey, dep, dq, an);
     if (dep.sensor >= 0) {
       n_dep++;
       if (first_sensor < 0) first_sensor = dep.sensor;
@@ -658,7 +688,7 @@ static int fill_run(const LumenScene* sc, const LumenControls* c, Run& R) {
 }
 
 static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t k0,
-                       uint32_t k1, int64_t first_id, int64_t n, const LumenControls* c, Launch& L) {
+                       uint32_t k1, int64_t first_id, int64_t n, const LumenControls* c, Launch& L, Pick& pk) {
   memset(&L, 0, sizeof(L));
   if (!sc) return set_err(LUMEN_ERR_ARG, "scene is null");
   if ((rows == nullptr) == (source == nullptr)) return set_err(LUMEN_ERR_ARG, "give exactly one of rows / source");
@@ -706,7 +736,11 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   L.first_id = first_id;
   L.n = n;
   L.step_budget = c->step_budget;
-  L.torus = sc->has_torus;
+  pk.torus = sc->has_torus;
+  pk.analog = (c->flags & LUMEN_F_TRUTH) != 0;
+  if (pk.analog && (c->n_grad > 0 || !L.R.shared))
+    return set_err(LUMEN_ERR_ARG, "truth rows decide each photon's fate at one set of values: no gradient parameters "
+                                  "and no reference pool of its own");
   return 0;
 }
 
@@ -719,24 +753,28 @@ static int grid_for(const void* fn, int block, int* grid) {
   return 0;
 }
 
-template <int G, int BLOCK, int MINB, int TORUS>
+template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0>
 static int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
   int grid = 0, st = 0;
-  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS>, BLOCK, &grid))) return st;
+  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS, ANALOG>, BLOCK, &grid))) return st;
   if (bps > 0) {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (sms * bps < grid) grid = sms * bps;
   }
-  k_trace<G, BLOCK, MINB, TORUS><<<grid, BLOCK, 0, stream>>>(L);
+  k_trace<G, BLOCK, MINB, TORUS, ANALOG><<<grid, BLOCK, 0, stream>>>(L);
   CK(cudaGetLastError());
   return 0;
 }
 
 template <int G>
-static int launch_trace(const Launch& L, int variant, int bps, cudaStream_t stream) {
-  if (L.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream);  // tori: shape 0 whatever the variant
+static int launch_trace(const Launch& L, const Pick& pk, int variant, int bps, cudaStream_t stream) {
+  if constexpr (G == 0) {
+    if (L.truth)  // truth rows: the analog instantiation of shape 0
+      return pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream) : launch_shape<0, 256, 4, 0, 1>(L, bps, stream);
+  }
+  if (pk.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream);  // tori: shape 0 whatever the variant
   switch (variant) {
     case 1: return launch_shape<G, 128, 8, 0>(L, bps, stream);
     case 2: return launch_shape<G, 256, 3, 0>(L, bps, stream);
@@ -748,7 +786,7 @@ static int launch_trace(const Launch& L, int variant, int bps, cudaStream_t stre
 // pool holds up to LUMEN_WAVE_POOL slots (about 350 bytes each with gradients), allocated on the call's stream.
 #define LUMEN_WAVE_POOL (1 << 21)
 template <int G>
-static int run_wave(const Launch& L, unsigned long long* live, cudaStream_t stream) {
+static int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStream_t stream) {
   int64_t want = L.n < LUMEN_WAVE_POOL ? L.n : LUMEN_WAVE_POOL;
   int W = (int)((want + 255) / 256 * 256);
   const size_t nph = sizeof(Photon) / 4, nex = sizeof(WaveExtra) / 4, npre = sizeof(Pre) / 4, nq = sizeof(Query) / 4;
@@ -771,7 +809,7 @@ static int run_wave(const Launch& L, unsigned long long* live, cudaStream_t stre
   CK(cudaGetLastError());
   int st = 0;
   for (long long r = 0;; ++r) {
-    if (L.torus) k_wave_query<G, 1><<<grid, 256, 0, stream>>>(L, V);
+    if (pk.torus) k_wave_query<G, 1><<<grid, 256, 0, stream>>>(L, V);
     else k_wave_query<G, 0><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaMemsetAsync(V.live, 0, sizeof(unsigned long long), stream));
     k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
@@ -834,7 +872,7 @@ static int launch_bin(const Launch& L, const LumenTallies* out, cudaStream_t str
   return 0;
 }
 
-static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
+static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
                      cudaStream_t stream, int variant = 0, int bps = 0, int async = 0) {
   if (variant == LUMEN_VARIANT_WAVEFRONT && async)
     return set_err(LUMEN_ERR_ARG, "the wavefront variant reads its rounds back on the host: not with LUMEN_F_ASYNC");
@@ -843,6 +881,11 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
   T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
   T.P = L.R.P;
   T.cot = cot;
+  if (pk.analog) {  // truth rows: the persistent loop writes each photon's analog record
+    if (!out || !out->truth) return set_err(LUMEN_ERR_ARG, "LUMEN_F_TRUTH: tallies.truth (n records) is required");
+    L.truth = out->truth;
+    if (variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;
+  }
   T.grads = grads;
   // scratch: the photon counter, the abort flag, the steps used, the wavefront's live slots and the record count (one
   // small allocation per call)
@@ -889,12 +932,12 @@ static int run_trace(Launch& L, const LumenTallies* out, const double* cot, int 
         L2.T.health = dummy;
         L2.T.counts = (unsigned long long*)(dummy + LUMEN_N_HEALTH);
       }
-      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<LUMEN_MAX_GRAD>(L2, scratch + 3, stream)
-                                              : launch_trace<LUMEN_MAX_GRAD>(L2, variant, bps, stream);
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<LUMEN_MAX_GRAD>(L2, pk, scratch + 3, stream)
+                                              : launch_trace<LUMEN_MAX_GRAD>(L2, pk, variant, bps, stream);
       if (st) return st;
     } else {
-      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, scratch + 3, stream)
-                                              : launch_trace<0>(L, variant, bps, stream);
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, pk, scratch + 3, stream)
+                                              : launch_trace<0>(L, pk, variant, bps, stream);
       if (st) return st;
     }
   }
@@ -943,7 +986,7 @@ static int static_scratch(unsigned long long** out) {
 }
 
 // run_trace with the scratch of the fixed array (no allocation, no free)
-static int run_trace_static(Launch& L, const LumenTallies* out, cudaStream_t stream) {
+static int run_trace_static(Launch& L, Pick pk, const LumenTallies* out, cudaStream_t stream) {
   if (STATIC_SCRATCH_NEED > LUMEN_STATIC_SCRATCH_WORDS)
     return set_err(LUMEN_ERR_ARG, "trace_static: the call needs more scratch than LUMEN_STATIC_SCRATCH_WORDS");
   unsigned long long* scratch = nullptr;
@@ -954,6 +997,10 @@ static int run_trace_static(Launch& L, const LumenTallies* out, cudaStream_t str
   T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
   T.P = L.R.P;
   T.cot = nullptr;
+  if (pk.analog) {
+    if (!out->truth) return set_err(LUMEN_ERR_ARG, "LUMEN_F_TRUTH: tallies.truth (n records) is required");
+    L.truth = out->truth;
+  }
   T.grads = nullptr;
   T.nb = out->hist ? out->n_bins : 0;
   T.bin0 = out->bin0;
@@ -978,8 +1025,8 @@ static int run_trace_static(Launch& L, const LumenTallies* out, cudaStream_t str
     L.R.rec_n = scratch + 3;
   }
   if (L.n > 0) {
-    if (L.R.P > 0) st = launch_trace<LUMEN_MAX_GRAD>(L, 0, 0, stream);
-    else st = launch_trace<0>(L, 0, 0, stream);
+    if (L.R.P > 0) st = launch_trace<LUMEN_MAX_GRAD>(L, pk, 0, 0, stream);
+    else st = launch_trace<0>(L, pk, 0, 0, stream);
     if (st) return st;
   }
   if (groups && (st = launch_bin(L, out, stream))) return st;
@@ -1008,9 +1055,10 @@ int32_t lumen_b200_trace_static(const LumenScene* sc, const LumenRows* rows, con
   if (out->hist && (out->n_bins <= 0 || !(out->bin_w > 0.0f))) return set_err(LUMEN_ERR_ARG, "tallies: bad histogram");
   if (source && out->n_events < source->n_events) return set_err(LUMEN_ERR_ARG, "tallies: fewer events than the source's");
   Launch L;
-  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  Pick pk;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
-  return run_trace_static(L, out, (cudaStream_t)stream);
+  return run_trace_static(L, pk, out, (cudaStream_t)stream);
 }
 
 int32_t lumen_b200_abi_version(void) { return LUMEN_B200_ABI_VERSION; }
@@ -1155,9 +1203,10 @@ int32_t lumen_b200_trace(const LumenScene* sc, const LumenRows* rows, const Lume
   if (out->hist && (out->n_bins <= 0 || !(out->bin_w > 0.0f))) return set_err(LUMEN_ERR_ARG, "tallies: bad histogram");
   if (source && out->n_events < source->n_events) return set_err(LUMEN_ERR_ARG, "tallies: fewer events than the source's");
   Launch L;
-  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  Pick pk;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
-  return run_trace(L, out, nullptr, 0, nullptr, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
+  return run_trace(L, pk, out, nullptr, 0, nullptr, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
                    c->flags & LUMEN_F_ASYNC);
 }
 
@@ -1168,9 +1217,11 @@ int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const Lu
   if (!cotangent || !grads) return set_err(LUMEN_ERR_ARG, "adjoint: cotangent and grads are required");
   if (!c || c->n_grad <= 0) return set_err(LUMEN_ERR_ARG, "adjoint: no gradient parameters");
   Launch L;
-  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  Pick pk;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
-  return run_trace(L, nullptr, cotangent, n_events, grads, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
+  if (pk.analog) return set_err(LUMEN_ERR_ARG, "the adjoint replays no truth rows");
+  return run_trace(L, pk, nullptr, cotangent, n_events, grads, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
                    c->flags & LUMEN_F_ASYNC);
 }
 
@@ -1180,7 +1231,8 @@ int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, co
   g_err.clear();
   if (!out_i || !out_f) return set_err(LUMEN_ERR_ARG, "trace_photons: outputs are null");
   Launch L;
-  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L);
+  Pick pk;
+  int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
   if (n == 0) return 0;
   int block = 128;

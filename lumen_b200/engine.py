@@ -49,6 +49,12 @@ class DeviceTallies:
         t.counts = ctypes.cast(ctypes.c_void_p(self.counts.data_ptr()), A.c_u64p)
         self.c = t
 
+    def attach_truth(self, n: int):
+        """Keep each of the next call's ``n`` photons' analog records (LUMEN_F_TRUTH) in ``self.truth``."""
+        self.truth = torch.zeros((max(int(n), 1), A.TRUTH_WORDS), dtype=torch.float32, device=self.arrival.device)
+        self.c.truth = _f32p(self.truth)
+        return self
+
     def attach_groups(self, groups, capacity: int):
         """Fill the readout groups ``groups`` (a ``lumen_b200.readout.GroupCells`` on this device) from a records
         scratch of ``capacity`` deposits (a trace whose deposits outgrow it raises ``RecordsOverflow``)."""  # noqa: D205, D209

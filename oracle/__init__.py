@@ -230,17 +230,21 @@ def host_source(src, samples, det=None):
 
 def trace(det, key, n, *, rows=None, source=None, samples=None, first_id=0, pool_live=None, pool_ref=None,
           controls=None, n_events=1, n_bins=0, bin0=0.0, bin_w=1.0, records=False, threads=0, groups=None,
-          deposits=0):
+          deposits=0, truth=False):
     """Trace photons first_id .. first_id + n - 1 on the CPU; return (Tallies, (rec_i, rec_f) or None).
 
     ``groups``: readout groups ({name: Grid or Group}, lumen_b200.readout): their cells in ``Tallies.groups`` (a host
     GroupCells); ``deposits`` > 0: up to that many deposit records, in photon order and the engine's layout, in
-    ``Tallies.deposits`` ((deposits, LUMEN_REC_WORDS) uint32).
+    ``Tallies.deposits`` ((deposits, LUMEN_REC_WORDS) uint32); ``truth``: each photon's analog record in
+    ``Tallies.truth`` ((n, LUMEN_TRUTH_WORDS) float32; with LUMEN_F_TRUTH in the controls' flags).
     """
     d, keep = det.desc()
     c = controls or A.controls()
     T = Tallies(det.n_sensor, n_events, n_bins, bin0, bin_w, c.n_grad)
-    T.groups = T.deposits = None
+    T.groups = T.deposits = T.truth = None
+    if truth:
+        T.truth = np.zeros((n, A.TRUTH_WORDS), np.float32)
+        T.c.truth = A.fptr(T.truth)
     if groups:
         from lumen_b200.readout import GroupCells
 

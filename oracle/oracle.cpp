@@ -40,6 +40,7 @@ typedef struct ORun {
   int P;
   int gt[O_MAXG];
   int jump; /* LUMEN_F_JUMP */
+  int analog; /* LUMEN_F_TRUTH */
 } ORun;
 
 typedef struct OPhoton {
@@ -51,6 +52,12 @@ typedef struct OPhoton {
   int nz, cls;
   int gen; /* re-emissions so far (state.py Photon.gen) */
   float dw[O_MAXG];
+  /* the analog photon (truth rows, state.py:30 Analog): its place x in the weight (inf: decided), its weight k, and
+     at its cathode absorption the sensor, time, wavelength, 1 / A_n, crossing point and volume entered */
+  float ax, ak;
+  int asensor;
+  float atime, alam, ascale, apos[3];
+  int avol;
 } OPhoton;
 
 typedef struct ODep {
@@ -469,9 +476,37 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   float w_new = nx_w;
   int low = wr < R->roulette;
   float p_s = wr / R->roulette;
-  int keep = low ? (o_uniform(vkey, 6) < p_s) : 0;
+  int keep = 0;
+  if (R->analog) {
+    /* step.py:625 _analog_crossing: the analog photon is absorbed where x falls in the crossing's reached share;
+       past the weight the event leaves its fate was another loss (decided) */
+    const float share = (at_if && !scatter) ? ph->w * att_if * p_det : 0.0f;
+    if (ph->ax < share) {
+      ph->asensor = at_if ? sensor_q : -1;
+      ph->atime = time;
+      ph->alam = ph->lam;
+      ph->ascale = 1.0f;
+      if (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL]) {
+        const float an = o_normal_absorptance(D, R->live, row, ph->lam, ml.n, q.normal);
+        ph->ascale = an > 0.0f ? 1.0f / an : 0.0f;
+      }
+      for (int a = 0; a < 3; ++a) ph->apos[a] = ph->x[a] + dist * ph->d[a];
+      ph->avol = q.vol_after;
+      ph->ax = INFINITY;
+    } else {
+      const float left = ph->ax - share;
+      ph->ax = left < nx_w ? left : INFINITY;
+    }
+    /* step.py:649 _analog_roulette: kept while the analog fate is open, so that the keep's total is p_s */
+    const float pi = wr * ph->ak;
+    const float extra = (p_s - pi) / (pi < 1.0f ? 1.0f - pi : 1.0f);
+    if (low) keep = std::isfinite(ph->ax) || o_uniform(vkey, 6) < extra;
+  } else if (low) {
+    keep = o_uniform(vkey, 6) < p_s;
+  }
   int kept = low && keep, lostr = low && !keep;
   float p_kept = kept ? p_s : 1.0f;
+  if (R->analog && kept && std::isfinite(ph->ax)) ph->ax = ph->ax / p_kept;
   float w_in = w_new;
   w_new = kept ? w_new / p_kept : (lostr ? 0.0f : w_new);
   float rouletted = (ph->alive && nx_ok) ? w_in - w_new : 0.0f;
@@ -745,7 +780,7 @@ typedef struct OGroupCtx {
 
 /* one photon's loop (run.py:307 item): begin, steps until it ends or reaches the vertex guard */
 static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTally* T, int32_t* rec_i,
-                     float* rec_f, OGroupCtx* gc) {
+                     float* rec_f, OGroupCtx* gc, float* truth) {
   const OScene* S = &R->S;
   OPhoton ph;
   memset(&ph, 0, sizeof(ph));
@@ -763,6 +798,14 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
   OKey pkey = o_fold_in(key, (uint32_t)gid);
   const double w0 = row->w0;
   const int e = row->event;
+  if (R->analog) { /* run.py:319: one uniform of the photon's analog stream; open with probability k (state.py:58) */
+    const float u = o_uniform(o_fold_in(pkey, 0x7A4A1061u), 0);
+    ph.ak = row->w0;
+    ph.ax = u < ph.ak ? u / (ph.ak > 0.0f ? ph.ak : 1.0f) : INFINITY;
+    ph.asensor = -1;
+    ph.ascale = 1.0f;
+    ph.avol = -1;
+  }
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double pushed = 0.0;
   OPhotonSums ps;
@@ -828,6 +871,14 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
   T->counts[LUMEN_C_PHOTONS] += 1;
   T->counts[LUMEN_C_STEPS] += steps;
   if (ph.alive) T->counts[LUMEN_C_TRUNCATED] += 1;
+  if (truth) { /* the photon's analog record (run.py:350) */
+    memcpy(truth + LUMEN_TR_SENSOR, &ph.asensor, 4);
+    truth[LUMEN_TR_TIME] = ph.atime;
+    truth[LUMEN_TR_LAM] = ph.alam;
+    truth[LUMEN_TR_SCALE] = ph.ascale;
+    for (int a = 0; a < 3; ++a) truth[LUMEN_TR_POS + a] = ph.apos[a];
+    memcpy(truth + LUMEN_TR_VOL, &ph.avol, 4);
+  }
   if (rec_i) {
     rec_i[0] = ph.vertex;
     rec_i[1] = n_dep;
@@ -871,6 +922,7 @@ static void o_run_init(ORun* R, const LumenSceneDesc* D, const float* live, cons
   R->max_vertices = c->max_vertices;
   R->P = c->n_grad;
   R->jump = (c->flags & LUMEN_F_JUMP) && D->n_jump > 0;
+  R->analog = (c->flags & LUMEN_F_TRUTH) != 0;
   for (int p = 0; p < R->P; ++p) R->gt[p] = c->grad_tab[p];
 }
 
@@ -1152,7 +1204,8 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
     ORow r;
     o_row_of(&R, rows, src, key, first_id, i, &r);
     o_photon(&R, &r, key, first_id + i, &parts[omp_get_thread_num()], rec_i ? rec_i + 5 * i : 0,
-             rec_f ? rec_f + 4 * i : 0, groups ? &gparts[omp_get_thread_num()] : 0);
+             rec_f ? rec_f + 4 * i : 0, groups ? &gparts[omp_get_thread_num()] : 0,
+             (R.analog && out->truth) ? out->truth + (size_t)LUMEN_TRUTH_WORDS * i : 0);
   }
   if (groups) { /* the threads' cells, and the records in photon order (the engine's layout, LUMEN_REC_WORDS each) */
     for (auto& G : gparts) {

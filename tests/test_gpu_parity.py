@@ -418,3 +418,47 @@ def test_solids_box_photons_bit_exact(solids, built):
     src = sources.Point(position=(0.05, 0.02, -0.6), n_photons=1.0, lam=400.0)
     bad, gi, oi, gf, of = _records_match(solids, src, 1 << 14)
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+@pytest.mark.parametrize(("which", "variant"), [("readout", 0), ("toy", 3)])
+def test_truth_records_bit_exact(which, variant, toy, built):
+    """Truth rows (LUMEN_F_TRUTH): each photon's analog record (sensor, time, wavelength, 1 / A_n, the crossing point,
+    the volume) is the checker's bit for bit, and so are the arrivals of the run whose roulette keeps open analog
+    fates; a wavefront request runs the persistent loop."""
+    det = detectors.readout_tank() if which == "readout" else toy
+    src = sources.Point(position=(0.1, 0.0, 0.05), n_photons=float(1 << 14), lam_range=(330.0, 480.0))
+    n = 1 << 14
+    eng = _engine(det)
+    ds = DeviceSource(src, n)
+    c = A.controls(roulette=0.05, flags=A.F_TRUTH, variant=variant)
+    T = DeviceTallies(det.n_sensor, 1, 0, 0.0, 1.0, 0).attach_truth(n)
+    eng.trace(KEY, n, source=ds, controls=c, tallies=T)
+    O, _ = oracle.trace(det, KEY, n, source=src, samples=n, controls=c, truth=True)
+    g = T.truth.cpu().numpy()
+    bad = np.flatnonzero((g.view(np.uint32) != O.truth.view(np.uint32)).any(1))
+    assert len(bad) == 0, f"{len(bad)} records differ, first {bad[:5]}: gpu {g[bad[:2]]} cpu {O.truth[bad[:2]]}"
+    assert (g[:, 0].view(np.int32) >= 0).sum() > 50
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+
+
+def test_simulate_truth_rows(toy, built):
+    from lumen_b200 import api
+    from lumen_b200 import truth as TR
+
+    n = 1 << 14
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=float(n), lam=400.0)
+    light = api.simulate(toy, src, samples=n, seed=0, truth=TR.Truth(keep="absorbed", angle=True, position=True),
+                         controls={"jump": False})  # fmt: skip
+    O, _ = oracle.trace(toy, KEY, n, source=src, samples=n, controls=A.controls(flags=A.F_TRUTH), truth=True)
+    want = TR.rows(TR.Truth(keep="absorbed", angle=True, position=True), toy, O.truth, KEY, 0, None)
+    h = light.truth
+    np.testing.assert_array_equal(h.photon, want.photon)
+    np.testing.assert_array_equal(h.sensor, want.sensor)
+    np.testing.assert_array_equal(h.time, want.time)
+    np.testing.assert_array_equal(h.detected, want.detected)
+    assert h.detected.all() and len(h.photon) > 50  # counting sensors: every absorbed photon is detected
+    pos = h.position.astype(np.float64)  # on the PMT discs (r 0.05, half height 0.01): a face or the side
+    assert ((np.abs(np.abs(pos[:, 2]) - 0.01) < 1e-5) | (np.abs(np.hypot(pos[:, 0], pos[:, 1]) - 0.05) < 1e-5)).all()
+    with pytest.raises(ValueError):
+        api.simulate(toy, sources.Point(position=(0.0, 0.0, 0.1), n_photons=2.0 * n, lam=400.0), samples=n,
+                     truth=TR.Truth())  # fmt: skip
