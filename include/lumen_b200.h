@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 9
+#define LUMEN_B200_ABI_VERSION 10
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -156,7 +156,20 @@ typedef struct LumenSceneDesc {
   int64_t n_clear;
   const float* clear;        /* host, n_clear: the grids' clearances (m) at their nodes, node (i, j, k) at
                                 first + (i * n1 + j) * n2 + k */
+  /* the navigator's precision (src/lumen/rules/navigation.py:96 Precision, the load option precision=): with
+     LUMEN_PREC_FLOAT64 the navigator (frames, BVH boxes, leaf coefficients, plane slabs, roots, intervals and the
+     band) and the photon's position are float64 and the physics stays float32, as the reference's float64 navigator.
+     The float64 arrays below then hold the same geometry as vol_f, node_f, leaf_f and plane_f, built in float64 (not
+     widened from the float32 arrays); null with LUMEN_PREC_FLOAT32. The sensor reach and the jump grids stay float32
+     in either precision, as the reference's (src/lumen/geometry/reach.py:88, transport/fastpath.py:177). */
+  int32_t precision;
+  const double* vol_f64;     /* host, n_vol * LUMEN_VOL_F */
+  const double* node_f64;    /* host, n_node * LUMEN_NODE_F */
+  const double* leaf_f64;    /* host, n_leaf * LUMEN_LEAF_F */
+  const double* plane_f64;   /* host, n_plane * LUMEN_PLANE_F */
 } LumenSceneDesc;
+
+enum { LUMEN_PREC_FLOAT32 = 0, LUMEN_PREC_FLOAT64 = 1 };
 
 typedef struct LumenScene LumenScene; /* opaque: the device copy of a LumenSceneDesc */
 
@@ -371,6 +384,14 @@ int32_t lumen_b200_query(const LumenScene* scene, const float* ray, const int32_
 
 /* Volume holding each point (src/lumen/geometry/navigate.py:226 `locate`): device pts (n * 3) -> vol (n). */
 int32_t lumen_b200_locate(const LumenScene* scene, const float* pts, int64_t n, int32_t* vol, void* stream);
+
+/* lumen_b200_query and lumen_b200_locate in the navigator's own precision on a float64 scene (LUMEN_PREC_FLOAT64): the
+   rays (n * 6), t_max, the points (n * 3) and out_f's t are float64 (out_f: n * 4 doubles, the normal widened from
+   the float32 the step reads). A float32 scene refuses them with LUMEN_ERR_ARG, as lumen_b200_query and
+   lumen_b200_locate are refused on a float64 scene. */
+int32_t lumen_b200_query64(const LumenScene* scene, const double* ray, const int32_t* vol, const int32_t* srf,
+                           double t_max, int64_t n, int32_t* out_i, double* out_f, void* stream);
+int32_t lumen_b200_locate64(const LumenScene* scene, const double* pts, int64_t n, int32_t* vol, void* stream);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,8 @@ class LumenSceneDesc(ctypes.Structure):
         ("fnode_f", c_f32p), ("fnode_i", c_i32p),
         ("n_jump", ctypes.c_int32), ("jump_f", c_f32p), ("jump_i", c_i32p), ("n_clear", ctypes.c_int64),
         ("clear", c_f32p),
+        ("precision", ctypes.c_int32), ("vol_f64", c_f64p), ("node_f64", c_f64p), ("leaf_f64", c_f64p),
+        ("plane_f64", c_f64p),
     ]  # fmt: skip
 
 
@@ -137,7 +139,8 @@ def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=()
 
 ENTRY_POINTS = ("lumen_b200_abi_version", "lumen_b200_last_error", "lumen_b200_scene_create",
                 "lumen_b200_scene_set_pools", "lumen_b200_scene_destroy", "lumen_b200_trace", "lumen_b200_adjoint",
-                "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate", "lumen_b200_trace_static")  # fmt: skip
+                "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate", "lumen_b200_trace_static",
+                "lumen_b200_query64", "lumen_b200_locate64")  # fmt: skip
 
 _lib = None
 
@@ -171,6 +174,9 @@ def engine():
         lib.lumen_b200_query.argtypes = [vp, c_f32p, c_i32p, c_i32p, ctypes.c_float, ctypes.c_int64, c_i32p, c_f32p,
                                          vp]  # fmt: skip
         lib.lumen_b200_locate.argtypes = [vp, c_f32p, ctypes.c_int64, c_i32p, vp]
+        lib.lumen_b200_query64.argtypes = [vp, c_f64p, c_i32p, c_i32p, ctypes.c_double, ctypes.c_int64, c_i32p,
+                                           c_f64p, vp]  # fmt: skip
+        lib.lumen_b200_locate64.argtypes = [vp, c_f64p, ctypes.c_int64, c_i32p, vp]
         for name in ENTRY_POINTS[2:]:
             getattr(lib, name).restype = ctypes.c_int32
         _lib = lib

@@ -1,5 +1,7 @@
 // The navigator on the device: CSG leaf intervals, the postfix boolean, first_change, and Geant4 volume tracking
-// with surface identity, over per-volume BVHs of the daughters' world boxes.
+// with surface identity, over per-volume BVHs of the daughters' world boxes. The body (dnav.cuh) is compiled in both
+// of the reference's precisions: nav32 (float32, the default) and nav64 (float64 navigator: the load option
+// precision="float64", src/lumen/rules/navigation.py:96); nav_* below pick one by the position's type.
 //
 // Semantics follow src/lumen/geometry/csg.py (first_change :417, _nearest :369, _change :395, _mem_at :346,
 // _program :320, _q_iv :138, _planes :116), leaf_kernels.py:81 (quad_line), navigate.py (_unit_visit :376,
@@ -41,7 +43,7 @@ struct DScene {
   int n_cls, n_sensor;
   float reach;
   const int32_t* __restrict__ vol_i;
-  const float* __restrict__ vol_f;
+  const float* __restrict__ vol_f;  // vol_f, node_f, leaf_f, plane_f: float64 data on a float64 scene (nav64)
   const int32_t* __restrict__ cand;
   const float* __restrict__ node_f;
   const int32_t* __restrict__ node_i;
@@ -86,768 +88,22 @@ L_DEV int d_cls(const DScene& S, int v) { return vI(S, v, LUMEN_VI_CLS); }
 L_DEV int d_parent(const DScene& S, int v) { return vI(S, v, LUMEN_VI_PARENT); }
 L_DEV int d_rank(const DScene& S, int i) { return i >= 0 ? -vI(S, i, LUMEN_VI_PRIO) : 0; }
 
-L_DEV void d_to_local_pt(const DScene& S, int i, const float* x, float* xl) {
-  const float* f = S.vol_f + (size_t)i * LUMEN_VOL_F;
-  float v0 = x[0] - __ldg(f + 9), v1 = x[1] - __ldg(f + 10), v2 = x[2] - __ldg(f + 11);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) xl[a] = __ldg(f + a) * v0 + __ldg(f + 3 + a) * v1 + __ldg(f + 6 + a) * v2;
-}
-L_DEV void d_to_local_dir(const DScene& S, int i, const float* d, float* dl) {
-  const float* f = S.vol_f + (size_t)i * LUMEN_VOL_F;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) dl[a] = __ldg(f + a) * d[0] + __ldg(f + 3 + a) * d[1] + __ldg(f + 6 + a) * d[2];
-}
-L_DEV void d_to_world_dir(const DScene& S, int i, const float* g, float* gw) {
-  const float* f = S.vol_f + (size_t)i * LUMEN_VOL_F;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) gw[a] = __ldg(f + 3 * a) * g[0] + __ldg(f + 3 * a + 1) * g[1] + __ldg(f + 3 * a + 2) * g[2];
-}
 
-// ------------------------------------------------------------------------------------------- leaf intervals
-struct Iv { float lo0, hi0; int f_lo0, f_hi0; float lo1, hi1; int f_lo1, f_hi1; };
+// the precision-generic helpers of the body: overloads in float and double
+L_DEV float n_sqrt(float x) { return sqrtf(x); }
+L_DEV double n_sqrt(double x) { return sqrt(x); }
+L_DEV float n_abs(float x) { return fabsf(x); }
+L_DEV double n_abs(double x) { return fabs(x); }
+L_DEV float n_cbrt(float x) { return l_cbrt(x); }
+L_DEV double n_cbrt(double x) { return l_cbrt64(x); }
+// a constant's value in the body's precision: the float32 literal in float, the float64 literal in double
+#define NK(x) (sizeof(NF) == 4 ? (NF)(x##f) : (NF)(x))
 
-L_DEV void d_Av(const float* A, const float* v, float* out) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a) out[a] = __ldg(A + 3 * a) * v[0] + __ldg(A + 3 * a + 1) * v[1] + __ldg(A + 3 * a + 2) * v[2];
-}
-L_DEV float d_dotg(const float* g, const float* v) { return __ldg(g) * v[0] + __ldg(g + 1) * v[1] + __ldg(g + 2) * v[2]; }
-
-L_DEV void d_quad_line(const float* lf, const float* y, const float* d, float* L0, float* R0, int* L0q, int* R0q,
-                       float* L1, float* R1) {
-  const float* A = lf + LUMEN_LF_A;
-  const float* b = lf + LUMEN_LF_B;
-  float c = __ldg(lf + LUMEN_LF_C), sa = __ldg(lf + LUMEN_LF_SA);
-  const float inf = D_HUGE;
-  float t_o = -d_dot(y, d);
-  float y0[3] = {y[0] + t_o * d[0], y[1] + t_o * d[1], y[2] + t_o * d[2]};
-  float Ad[3];
-  d_Av(A, d, Ad);
-  float alpha = d_dot(Ad, d);
-  int lin = fabsf(alpha) < d_max(D_LINEAR_REL * sa, D_DIVISOR_FLOOR);
-  float bdd = d_dotg(b, d);
-  float Ay0[3];
-  d_Av(A, y0, Ay0);
-  float beta0 = d_dot(Ay0, d) + bdd;
-  float gam0 = (d_dot(y0, Ay0) + 2.0f * d_dotg(b, y0)) + c;
-  int near_ = !lin && (alpha * gam0 > 0.5f * beta0 * beta0);
-  float t_c = t_o + (near_ ? -beta0 / alpha : 0.0f);
-  float yc[3] = {y[0] + t_c * d[0], y[1] + t_c * d[1], y[2] + t_c * d[2]};
-  float Ayc[3];
-  d_Av(A, yc, Ayc);
-  float beta = d_dot(Ayc, d) + bdd;
-  float gam = (d_dot(yc, Ayc) + 2.0f * d_dotg(b, yc)) + c;
-  float D = beta * beta - alpha * gam;
-  int Dpos = D > D_TANGENT_ULPS * D_EPS32 * (beta * beta + fabsf(alpha * gam));
-  float sD = sqrtf(Dpos ? D : 1.0f);
-  float sgn = beta >= 0.0f ? 1.0f : -1.0f;
-  float s_ = -(beta + sgn * (Dpos ? sD : 0.0f));
-  int s_ok = fabsf(s_) > D_DIVISOR_FLOOR;
-  float r1 = lin ? inf : s_ / alpha;
-  float r2 = s_ok ? gam / s_ : 0.0f;
-  float rmin = d_min(r1, r2) + t_c;
-  float rmax = d_max(r1, r2) + t_c;
-  int b_small = fabsf(beta) < D_DIVISOR_FLOOR;
-  float tl = t_c - gam / (b_small ? 1.0f : 2.0f * beta);
-  int lin_ent = lin && !b_small && beta < 0.0f;
-  int lin_ext = lin && !b_small && beta > 0.0f;
-  int lin_all = lin && b_small && gam <= 0.0f;
-  int pos = !lin && alpha > 0.0f;
-  int neg = !lin && alpha < 0.0f;
-  *L0 = pos ? (Dpos ? rmin : inf) : (neg ? -inf : (lin_ent ? tl : ((lin_ext || lin_all) ? -inf : inf)));
-  *R0 = pos ? (Dpos ? rmax : -inf)
-            : (neg ? (Dpos ? rmin : inf) : (lin_ext ? tl : ((lin_ent || lin_all) ? inf : -inf)));
-  *L0q = (pos && Dpos) || lin_ent;
-  *R0q = (pos && Dpos) || (neg && Dpos) || lin_ext;
-  int has1 = neg && Dpos;
-  *L1 = has1 ? rmax : inf;
-  *R1 = has1 ? inf : -inf;
-}
-
-// ------------------------------------------------------------------------------------------------ the torus
-// leaf_kernels.py:212 torus_set: the interval set (two slots) of a solid torus about z along a unit ray o + s d in its
-// canonical frame. g(s) = (rho - R)^2 + z^2 - r^2 has at most two inflection points (closed form); they split the
-// bracket on the padded bounding sphere into convex / concave / convex parts with one extremum each (bisection on g'),
-// giving at most six monotone pieces with one root at most (bisection on the membership)
-#define D_BISECT 40                // bisections in float32: the mantissa plus a margin
-#define D_TORUS_BRACKET_ULPS 64.0f
-#define D_TORUS_AXIAL 1e-12f       // a squared xy direction below this is along the axis
-#define D_TORUS_PAD_REL 1e-4f      // the pretests' pad, relative to R + r
-
-L_DEV float d_torus_g(float R, float r, const float* oc, const float* d, float s) {
-  float x = oc[0] + s * d[0], y = oc[1] + s * d[1], z = oc[2] + s * d[2];
-  float rho2 = x * x + y * y;
-  float rho = sqrtf(d_max(rho2, 0.0f));
-  float dr = (rho2 - R * R) / (rho + R);  // rho - R without the cancellation of rho and R
-  return dr * dr + z * z - r * r;
-}
-L_DEV float d_torus_dg(float R, const float* oc, const float* d, float s) {
-  float x = oc[0] + s * d[0], y = oc[1] + s * d[1], z = oc[2] + s * d[2];
-  float rho2 = x * x + y * y;
-  float rho = sqrtf(d_max(rho2, D_TINY_NORMAL));
-  float dr = (rho2 - R * R) / (rho + R);
-  float drho = (x * d[0] + y * d[1]) / rho;
-  return 2.0f * dr * drho + 2.0f * z * d[2];
-}
-
-// the exact pretests of the whole line (csg.py:175 _torus_window, the window unbounded): the padded ball, the slab
-// |z| <= r, the annulus R - r <= rho <= R + r. A window of the line that misses the torus holds none of its roots, so
-// solving on the whole line gives every window the reference's memberships.
-L_DEV int d_torus_meets(float R, float r, const float* ol, const float* du) {
-  const float Rb = (R + r) * (1.0f + D_TORUS_PAD_REL);
-  float bb = ol[0] * du[0] + ol[1] * du[1] + ol[2] * du[2];
-  float disc = Rb * Rb - (ol[0] * ol[0] + ol[1] * ol[1] + ol[2] * ol[2] - bb * bb);
-  float sq = sqrtf(d_max(disc, 0.0f));
-  float s_lo = -bb - sq, s_hi = -bb + sq;
-  int meet = disc > 0.0f && s_lo <= s_hi;
-  const float pad = D_TORUS_PAD_REL * (R + r), rz = r + pad;
-  int small = fabsf(du[2]) < D_PARALLEL;
-  float iz = 1.0f / (small ? 1.0f : du[2]);
-  float za = (-rz - ol[2]) * iz, zb = (rz - ol[2]) * iz;
-  if (!small) { s_lo = d_max(s_lo, d_min(za, zb)); s_hi = d_min(s_hi, d_max(za, zb)); }
-  meet = meet && s_lo <= s_hi && (!small || fabsf(ol[2]) <= rz);
-  float qa = du[0] * du[0] + du[1] * du[1], qb = ol[0] * du[0] + ol[1] * du[1], qc = ol[0] * ol[0] + ol[1] * ol[1];
-  float sm = d_min(d_max(-qb / (qa > D_PARALLEL ? qa : 1.0f), s_lo), s_hi);
-  float r2_min = qa > D_PARALLEL ? (qa * sm * sm + 2.0f * qb * sm + qc) : qc;
-  float r2_max = d_max(qa * s_lo * s_lo + 2.0f * qb * s_lo + qc, qa * s_hi * s_hi + 2.0f * qb * s_hi + qc);
-  float r_out = R + r + pad, r_in = d_max(R - r - pad, 0.0f);
-  return meet && r2_min <= r_out * r_out && r2_max >= r_in * r_in;
-}
-
-L_CALL void d_torus_set(float R, float r, const float* od, const float* dd, float* lo, float* hi) {
-  const float inf = D_HUGE;
-  float t_c = -((od[0] * dd[0] + od[1] * dd[1]) + od[2] * dd[2]);
-  float oc[3] = {od[0] + t_c * dd[0], od[1] + t_c * dd[1], od[2] + t_c * dd[2]};
-  float q0 = (oc[0] * oc[0] + oc[1] * oc[1]) + oc[2] * oc[2];
-  const float Rb = (R + r) * (1.0f + D_TORUS_BRACKET_ULPS * D_EPS32);
-  float b0 = (oc[0] * dd[0] + oc[1] * dd[1]) + oc[2] * dd[2];
-  float disc = Rb * Rb - q0 + b0 * b0;
-  int hit_b = disc > 0.0f;
-  float sq = sqrtf(hit_b ? disc : 1.0f);
-  float s_lo = -b0 - sq, s_hi = -b0 + sq;
-  float a = dd[0] * dd[0] + dd[1] * dd[1];
-  float bxy = oc[0] * dd[0] + oc[1] * dd[1];
-  float cxy = oc[0] * oc[0] + oc[1] * oc[1];
-  int a_ok = a > D_TORUS_AXIAL;
-  float a_s = a_ok ? a : 1.0f;
-  float s_v = a_ok ? -bxy / a_s : 0.0f;
-  float m2 = d_max(a_ok ? cxy - bxy * bxy / a_s : cxy, 0.0f);
-  float ci = l_cbrt(R * a * m2);
-  float w2 = (ci * ci - m2) / a_s;  // the inflection points s_v -+ w
-  int has_w = a_ok && w2 > 0.0f;
-  float w = sqrtf(has_w ? w2 : 0.0f);
-  float p1 = d_min(d_max(s_v - w, s_lo), s_hi), p2 = d_min(d_max(s_v + w, s_lo), s_hi);
-  // the extrema: a minimum on [s_lo, p1] (g' increasing), the maximum on [p1, p2], a minimum on [p2, s_hi]
-  float el[3] = {s_lo, p1, p2}, eh[3] = {p1, p2, s_hi}, e[3];
-  for (int k = 0; k < 3; ++k) {
-    float l = el[k], h = eh[k];
-    for (int it = 0; it < D_BISECT; ++it) {
-      float mid = 0.5f * (l + h);
-      float gm = d_torus_dg(R, oc, dd, mid);
-      int right = k == 1 ? gm > 0.0f : gm < 0.0f;
-      l = right ? mid : l;
-      h = right ? h : mid;
-    }
-    e[k] = 0.5f * (l + h);
-  }
-  // the roots: one per monotone piece whose ends differ in membership
-  const float knots[7] = {s_lo, e[0], p1, e[1], p2, e[2], s_hi};
-  float t[6];
-  for (int k = 0; k < 6; ++k) {
-    float xl = knots[k], xr = knots[k + 1];
-    int inl = d_torus_g(R, r, oc, dd, xl) <= 0.0f, inr = d_torus_g(R, r, oc, dd, xr) <= 0.0f;
-    float l = xl, h = xr;
-    for (int it = 0; it < D_BISECT; ++it) {
-      float mid = 0.5f * (l + h);
-      int same = (d_torus_g(R, r, oc, dd, mid) <= 0.0f) == inl;
-      l = same ? mid : l;
-      h = same ? h : mid;
-    }
-    t[k] = (inl != inr && xr > xl && hit_b) ? 0.5f * (l + h) + t_c : inf;
-  }
-  for (int i = 1; i < 6; ++i)  // ascending (insertion)
-    for (int j = i; j > 0 && t[j] < t[j - 1]; --j) { float x = t[j]; t[j] = t[j - 1]; t[j - 1] = x; }
-  // outside at the bracket's start: the roots alternate entry and exit
-  int ok0 = t[1] < D_BIG, ok1 = t[3] < D_BIG;
-  lo[0] = ok0 ? t[0] : inf; hi[0] = ok0 ? t[1] : inf;
-  lo[1] = ok1 ? t[2] : inf; hi[1] = ok1 ? t[3] : inf;
-}
-
-// a torus leaf's intervals along o + t d (kind frame): its canonical frame u = M (x - og), the unit ray there, the
-// roots scaled back (csg.py:207 _t_iv); out of line, returned by value (the quadric-only scenes' step pays a branch)
-L_DEV float4 d_torus_line(const float* lf, const float* o, const float* d) {
-  const float* M = lf + LUMEN_LF_A;
-  const float R = __ldg(lf + LUMEN_LF_B), r = __ldg(lf + LUMEN_LF_B + 1);
-  float xl[3] = {o[0] - __ldg(lf + 0), o[1] - __ldg(lf + 1), o[2] - __ldg(lf + 2)}, ol[3], dl[3];
-  d_Av(M, xl, ol);
-  d_Av(M, d, dl);
-  float kk = sqrtf(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
-  float du[3] = {dl[0] / kk, dl[1] / kk, dl[2] / kk};
-  float lo[2] = {D_HUGE, D_HUGE}, hi[2] = {D_HUGE, D_HUGE};
-  if (d_torus_meets(R, r, ol, du)) d_torus_set(R, r, ol, du, lo, hi);
-  return make_float4(fabsf(lo[0]) < D_BIG ? lo[0] / kk : lo[0], fabsf(hi[0]) < D_BIG ? hi[0] / kk : hi[0],
-                     fabsf(lo[1]) < D_BIG ? lo[1] / kk : lo[1], fabsf(hi[1]) < D_BIG ? hi[1] / kk : hi[1]);
-}
-
-// a torus leaf's Iv (it reads no planes: each piece its own roots, face 0; the non-empty piece first); out of line,
-// the ray and the result by value, so that a scan over quadric and plane leaves keeps its registers
-L_CALL Iv d_torus_iv(const float* lf, float3 ov, float3 dv) {
-  const float o[3] = {ov.x, ov.y, ov.z}, d[3] = {dv.x, dv.y, dv.z};
-  float4 tv = d_torus_line(lf, o, d);
-  const float inf = D_HUGE;
-  Iv r;
-  int ok0 = tv.x < tv.y, ok1 = tv.z < tv.w;
-  r.lo0 = ok0 ? tv.x : inf; r.hi0 = ok0 ? tv.y : inf; r.f_lo0 = ok0 ? 0 : -1; r.f_hi0 = ok0 ? 0 : -1;
-  r.lo1 = ok1 ? tv.z : inf; r.hi1 = ok1 ? tv.w : inf; r.f_lo1 = ok1 ? 0 : -1; r.f_hi1 = ok1 ? 0 : -1;
-  if (!ok0 && ok1) {
-    Iv s = r;
-    r.lo0 = s.lo1; r.hi0 = s.hi1; r.f_lo0 = s.f_lo1; r.f_hi0 = s.f_hi1;
-    r.lo1 = s.lo0; r.hi1 = s.hi0; r.f_lo1 = s.f_lo0; r.f_hi1 = s.f_hi0;
-  }
-  return r;
-}
-
-// whether the torus holds x (kind frame): (rho - R)^2 + z^2 <= r^2 in its canonical frame (csg.py:301 _inside_leaf)
-L_DEV int d_torus_holds(const float* lf, const float* x) {
-  float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)}, u[3];
-  d_Av(lf + LUMEN_LF_A, xl, u);
-  const float R = __ldg(lf + LUMEN_LF_B), r = __ldg(lf + LUMEN_LF_B + 1);
-  float dr = sqrtf(u[0] * u[0] + u[1] * u[1]) - R;
-  return dr * dr + u[2] * u[2] <= r * r;
-}
-
-L_DEV Iv d_leaf_iv(const DScene& S, int g, const float* o, const float* d) {
-  const float* lf = S.leaf_f + (size_t)g * LUMEN_LEAF_F;
-  const int32_t* li = S.leaf_i + (size_t)g * LUMEN_LEAF_I;
-  const float inf = D_HUGE;
-  float y[3] = {o[0] - __ldg(lf + 3), o[1] - __ldg(lf + 4), o[2] - __ldg(lf + 5)};
-  float ol[3] = {o[0] - __ldg(lf + 0), o[1] - __ldg(lf + 1), o[2] - __ldg(lf + 2)};
-  float t0p = -inf, t1p = inf;
-  int f0p = -1, f1p = -1, ep = 0;
-  int p0 = __ldg(li + 1), np_ = __ldg(li + 2);
-  for (int k = 0; k < np_; ++k) {
-    const float* pl = S.plane_f + (size_t)(p0 + k) * LUMEN_PLANE_F;
-    float n0 = __ldg(pl), n1 = __ldg(pl + 1), n2 = __ldg(pl + 2), h = __ldg(pl + 3);
-    float nd = n0 * d[0] + n1 * d[1] + n2 * d[2];
-    float rhs = h - (n0 * ol[0] + n1 * ol[1] + n2 * ol[2]);
-    int par = fabsf(nd) < D_PARALLEL;
-    float tp = rhs / (par ? 1.0f : nd);
-    float ent = nd < -D_PARALLEL ? tp : -inf;
-    float ext = nd > D_PARALLEL ? tp : inf;
-    if (ent > t0p) { t0p = ent; f0p = k + 1; }
-    if (ext < t1p) { t1p = ext; f1p = k + 1; }
-    ep = ep || (par && rhs < 0.0f);
-  }
-  int has_q = __ldg(li) == 1;
-  float L0 = -inf, R0 = inf, L1 = inf, R1 = -inf;
-  int L0q = 0, R0q = 0;
-  if (has_q) d_quad_line(lf, y, d, &L0, &R0, &L0q, &R0q, &L1, &R1);
-  Iv r;
-  {
-    float lo = d_max(L0, t0p), hi = d_min(R0, t1p);
-    int flo = L0 > t0p ? (L0q ? 0 : f0p) : f0p;
-    int fhi = R0 < t1p ? (R0q ? 0 : f1p) : f1p;
-    int ok = lo < hi && !ep;
-    r.lo0 = ok ? lo : inf; r.hi0 = ok ? hi : inf; r.f_lo0 = ok ? flo : -1; r.f_hi0 = ok ? fhi : -1;
-  }
-  {
-    float lo = d_max(L1, t0p), hi = d_min(R1, t1p);
-    int flo = L1 > t0p ? 0 : f0p;
-    int fhi = f1p;
-    int ok = lo < hi && !ep;
-    r.lo1 = ok ? lo : inf; r.hi1 = ok ? hi : inf; r.f_lo1 = ok ? flo : -1; r.f_hi1 = ok ? fhi : -1;
-  }
-  if (r.lo0 >= inf && r.lo1 < inf) {
-    Iv s = r;
-    r.lo0 = s.lo1; r.hi0 = s.hi1; r.f_lo0 = s.f_lo1; r.f_hi0 = s.f_hi1;
-    r.lo1 = s.lo0; r.hi1 = s.hi0; r.f_lo1 = s.f_lo0; r.f_hi1 = s.f_hi0;
-  }
-  return r;
-}
-
-L_DEV int d_inside_leaf(const DScene& S, int g, const float* x) {
-  const float* lf = S.leaf_f + (size_t)g * LUMEN_LEAF_F;
-  const int32_t* li = S.leaf_i + (size_t)g * LUMEN_LEAF_I;
-  float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)};
-  float y[3] = {x[0] - __ldg(lf + 3), x[1] - __ldg(lf + 4), x[2] - __ldg(lf + 5)};
-  int pl = 1;
-  int p0 = __ldg(li + 1), np_ = __ldg(li + 2);
-  for (int k = 0; k < np_; ++k) {
-    const float* p = S.plane_f + (size_t)(p0 + k) * LUMEN_PLANE_F;
-    pl = pl && (__ldg(p) * xl[0] + __ldg(p + 1) * xl[1] + __ldg(p + 2) * xl[2] <= __ldg(p + 3));
-  }
-  if (__ldg(li) == 2) return d_torus_holds(lf, x);
-  if (__ldg(li) != 1) return pl;
-  float Ay[3];
-  d_Av(lf + LUMEN_LF_A, y, Ay);
-  const float* b = lf + LUMEN_LF_B;
-  float qv = (d_dot(y, Ay) + 2.0f * (__ldg(b) * y[0] + __ldg(b + 1) * y[1] + __ldg(b + 2) * y[2])) + __ldg(lf + LUMEN_LF_C);
-  return pl && qv <= 0.0f;
-}
-
-// the kind's postfix program over a membership functor
-template <class F>
-L_DEV int d_program(const DScene& S, int kind, F member) {
-  const int32_t* k = S.kind_i + (size_t)kind * LUMEN_KIND_I;
-  int p0 = __ldg(k + 2), pl = __ldg(k + 3);
-  int32_t s = 0;
-  for (int p = 0; p < pl; ++p) {
-    int op = __ldg(S.prog_i + (size_t)(p0 + p) * 2), arg = __ldg(S.prog_i + (size_t)(p0 + p) * 2 + 1);
-    int32_t bb = s & 1, aa = (s >> 1) & 1;
-    int32_t r = op == 1 ? (aa | bb) : (op == 2 ? (aa & bb) : (aa & (1 - bb)));
-    if (op == 0) s = (s << 1) | (member(arg) & 1);
-    else s = ((s >> 2) << 1) | r;
-  }
-  return (s & 1) == 1;
-}
-
-L_DEV int d_inside_kind(const DScene& S, int kind, const float* x) {
-  int l0 = __ldg(S.kind_i + (size_t)kind * LUMEN_KIND_I);
-  return d_program(S, kind, [&](int l) { return d_inside_leaf(S, l0 + l, x); });
-}
-
-// ----------------------------------------------------------------------------------------- first_change
-struct Scan {
-  int kind, nl;
-  Iv iv[LUMEN_MAX_LEAVES];
-  float xa, t1;
-  int want;
-  int has_init, init_known, init_inside;
-  int has_skip, skip_leaf, skip_face, skip_entry;
-  float skip_thi;
-  int has_on, on_leaf, on_inside;
-  float on_tend, hend;
-};
-
-L_DEV float d_scan_band(const Scan& s, float t) { return d_band(s.xa + fabsf(t)); }
-
-L_DEV int d_mem_at(const DScene& S, const Scan& s, float t, int use_on) {
-  int on = s.has_on && use_on;
-  return d_program(S, s.kind, [&](int l) {
-    const Iv& v = s.iv[l];
-    int m = (v.lo0 <= t && t < v.hi0) || (v.lo1 <= t && t < v.hi1);
-    if (on && l == s.on_leaf && t < s.hend) m = s.on_inside;
-    return m;
-  });
-}
-
-// TORUS: the instantiation reads torus leaves (scenes without one run the instantiation without their code)
-template <int TORUS>
-L_DEV void d_scan_init(const DScene& S, Scan& s, int kind, const float* o, const float* d, float t1) {
-  s.kind = kind;
-  const int32_t* k = S.kind_i + (size_t)kind * LUMEN_KIND_I;
-  s.nl = __ldg(k + 1);
-  int l0 = __ldg(k);
-  for (int l = 0; l < s.nl; ++l) {
-    if (TORUS && __ldg(S.leaf_i + (size_t)(l0 + l) * LUMEN_LEAF_I) == 2)
-      s.iv[l] = d_torus_iv(S.leaf_f + (size_t)(l0 + l) * LUMEN_LEAF_F, make_float3(o[0], o[1], o[2]),
-                           make_float3(d[0], d[1], d[2]));
-    else
-      s.iv[l] = d_leaf_iv(S, l0 + l, o, d);
-  }
-  s.xa = d_max(d_max(fabsf(o[0]), fabsf(o[1])), fabsf(o[2]));
-  s.t1 = t1;
-  s.want = -1;
-  s.has_init = s.has_skip = s.has_on = 0;
-  s.hend = -D_HUGE;
-}
-
-struct First { int hit; float t; int inside, leaf, face; };
-struct Fc { int hit; float t; int inside, leaf, face, inside0; First first; };
-
-L_DEV void d_nearest(const Scan& s, float t_cur, float* e1o, int* lbo, int* fco, int* eko) {
-  float e1 = D_HUGE;
-  int lb = -1, fc = -1, ek = 0;
-  for (int l = 0; l < s.nl; ++l) {
-    const Iv& v = s.iv[l];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      float ep = j == 0 ? v.lo0 : (j == 1 ? v.hi0 : (j == 2 ? v.lo1 : v.hi1));
-      int fp = j == 0 ? v.f_lo0 : (j == 1 ? v.f_hi0 : (j == 2 ? v.f_lo1 : v.f_hi1));
-      int en = (j & 1) == 0;
-      int ok = fabsf(ep) < D_BIG && ep <= s.t1 && ep > t_cur && ep < e1;
-      if (s.has_skip) ok = ok && !(l == s.skip_leaf && fp == s.skip_face && s.skip_entry == en && ep < s.skip_thi);
-      if (ok) { e1 = ep; lb = l; fc = fp; ek = en; }
-    }
-  }
-  *e1o = e1; *lbo = lb; *fco = fc; *eko = ek;
-}
-
-L_DEV Fc d_first_change(const DScene& S, Scan& s, float t0) {
-  float t_cur = t0;
-  int done = 0, now = 0, lb_h = -1, fc_h = -1, now0 = 0, it = 0;
-  First fs = {0, D_HUGE, 0, -1, -1};
-  s.hend = s.has_on ? s.on_tend : -D_HUGE;
-  while (!done && t_cur < D_HUGE && it < D_MAX_SCAN_PER_LEAF * s.nl + D_MAX_SCAN_EXTRA) {
-    int first = it == 0;
-    float e; int lb, fc, ek;
-    if (first) { e = t0; lb = -1; fc = -1; ek = 0; }
-    else d_nearest(s, t_cur, &e, &lb, &fc, &ek);
-    int has = first || e < D_HUGE;
-    float tp = first ? t0 : e + d_scan_band(s, e);
-    if (s.has_on && !first && has && lb == s.on_leaf && ek != s.on_inside) s.hend = d_min(s.hend, e);
-    int aft;
-    if (!s.has_init) aft = has ? d_mem_at(S, s, tp, 1) : now;
-    else if (has && !(first && s.init_known)) aft = d_mem_at(S, s, tp, 1);
-    else aft = (first && s.init_known) ? s.init_inside : now;
-    if (first) now0 = aft;
-    int chg = !first && has && aft != now;
-    int vis = s.want < 0 ? chg : (chg && aft == s.want);
-    int nw = chg && !fs.hit;
-    if (nw) { fs.t = e; fs.inside = aft; fs.leaf = lb; fs.face = fc; }
-    fs.hit = fs.hit || chg;
-    if (has) now = aft;
-    float t_nx = first ? t0 : (vis ? e : (has ? tp : D_HUGE));
-    if (vis) { lb_h = lb; fc_h = fc; }
-    done = vis;
-    t_cur = t_nx;
-    it += 1;
-  }
-  Fc r;
-  r.hit = done;
-  r.t = done ? t_cur : s.t1;
-  r.inside = done ? now : now0;
-  r.leaf = lb_h;
-  r.face = fc_h;
-  r.inside0 = now0;
-  r.first = fs;
-  return r;
-}
-
-L_DEV void d_leaf_grad(const DScene& S, int kind, int leaf, int face, const float* x, float* g) {
-  int gi = __ldg(S.kind_i + (size_t)kind * LUMEN_KIND_I) + (leaf > 0 ? leaf : 0);
-  const float* lf = S.leaf_f + (size_t)gi * LUMEN_LEAF_F;
-  const int32_t* li = S.leaf_i + (size_t)gi * LUMEN_LEAF_I;
-  if (face >= 1) {
-    const float* p = S.plane_f + (size_t)(__ldg(li + 1) + face - 1) * LUMEN_PLANE_F;
-    g[0] = __ldg(p); g[1] = __ldg(p + 1); g[2] = __ldg(p + 2);
-    return;
-  }
-  if (__ldg(li) == 2) {  // M^T of the canonical gradient of ((rho - R)^2 + z^2 - r^2) / 2 (csg.py:452 leaf_grad)
-    const float* M = lf + LUMEN_LF_A;
-    float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)}, u[3];
-    d_Av(M, xl, u);
-    float rho = sqrtf(d_max(u[0] * u[0] + u[1] * u[1], D_DIVISOR_FLOOR));
-    float k = (rho - __ldg(lf + LUMEN_LF_B)) / rho;
-    float gu[3] = {k * u[0], k * u[1], u[2]};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) g[a] = (__ldg(M + a) * gu[0] + __ldg(M + 3 + a) * gu[1]) + __ldg(M + 6 + a) * gu[2];
-    return;
-  }
-  float y[3] = {x[0] - __ldg(lf + 3), x[1] - __ldg(lf + 4), x[2] - __ldg(lf + 5)};
-  float Ay[3];
-  d_Av(lf + LUMEN_LF_A, y, Ay);
-  const float* b = lf + LUMEN_LF_B;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) g[a] = 2.0f * (Ay[a] + __ldg(b + a));
-}
-
-L_DEV float d_leaf_dist(const DScene& S, int kind, int leaf, int face, const float* x) {
-  int gi = __ldg(S.kind_i + (size_t)kind * LUMEN_KIND_I) + (leaf > 0 ? leaf : 0);
-  const float* lf = S.leaf_f + (size_t)gi * LUMEN_LEAF_F;
-  const int32_t* li = S.leaf_i + (size_t)gi * LUMEN_LEAF_I;
-  float f;
-  if (face >= 1) {
-    const float* p = S.plane_f + (size_t)(__ldg(li + 1) + face - 1) * LUMEN_PLANE_F;
-    float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)};
-    f = __ldg(p) * xl[0] + __ldg(p + 1) * xl[1] + __ldg(p + 2) * xl[2] - __ldg(p + 3);
-  } else if (__ldg(li) == 2) {  // ((rho - R)^2 + z^2 - r^2) / 2 (csg.py:470 leaf_dist)
-    float xl[3] = {x[0] - __ldg(lf + 0), x[1] - __ldg(lf + 1), x[2] - __ldg(lf + 2)}, u[3];
-    d_Av(lf + LUMEN_LF_A, xl, u);
-    float dr = sqrtf(u[0] * u[0] + u[1] * u[1]) - __ldg(lf + LUMEN_LF_B), rr = __ldg(lf + LUMEN_LF_B + 1);
-    f = 0.5f * (dr * dr + u[2] * u[2] - rr * rr);
-  } else {
-    float y[3] = {x[0] - __ldg(lf + 3), x[1] - __ldg(lf + 4), x[2] - __ldg(lf + 5)};
-    float Ay[3];
-    d_Av(lf + LUMEN_LF_A, y, Ay);
-    const float* b = lf + LUMEN_LF_B;
-    f = (d_dot(y, Ay) + 2.0f * (__ldg(b) * y[0] + __ldg(b + 1) * y[1] + __ldg(b + 2) * y[2])) + __ldg(lf + LUMEN_LF_C);
-  }
-  float g[3];
-  d_leaf_grad(S, kind, leaf, face, x, g);
-  return fabsf(f) / d_safe_norm(g);
-}
-
-L_DEV int d_clampv(const DScene& S, int item) { return item < 0 ? 0 : (item > S.n - 1 ? S.n - 1 : item); }
-
-L_CALL void d_hit_grad(const DScene& S, int item, int leaf, int face, const float* x, float* gw) {
-  int i = d_clampv(S, item);
-  float xl[3], g[3];
-  d_to_local_pt(S, i, x, xl);
-  d_leaf_grad(S, vI(S, i, LUMEN_VI_KIND), leaf, face, xl, g);
-  d_to_world_dir(S, i, g, gw);
-}
-L_CALL float d_face_dist(const DScene& S, int item, int leaf, int face, const float* x) {
-  int i = d_clampv(S, item);
-  float xl[3];
-  d_to_local_pt(S, i, x, xl);
-  return d_leaf_dist(S, vI(S, i, LUMEN_VI_KIND), leaf, face, xl);
-}
-
-L_DEV int d_srf_pack(const DScene& S, int item, int leaf, int face, int o, int e) {
-  if (item < 0 || leaf < 0 || face < 0) return item;
-  return S.SU + ((item * S.LM + leaf) * S.FM + face) * 4 + 2 * o + e;
-}
-struct Srf { int item, leaf, face, o, known, e; };
-L_DEV Srf d_srf_decode(const DScene& S, int s) {
-  Srf r;
-  if (s < S.SU) { r.item = s; r.leaf = -1; r.face = -1; r.o = 0; r.known = 0; r.e = 0; return r; }
-  int u = s - S.SU;
-  r.e = u % 2; u /= 2;
-  r.o = u % 2; u /= 2;
-  r.face = u % S.FM; u /= S.FM;
-  r.leaf = u % S.LM; u /= S.LM;
-  r.item = u;
-  r.known = 1;
-  return r;
-}
-
-L_DEV int d_holds_point(const DScene& S, int i, const float* x) {
-  float xl[3];
-  d_to_local_pt(S, i, x, xl);
-  return d_inside_kind(S, vI(S, i, LUMEN_VI_KIND), xl);
-}
-L_CALL int d_ray_holds(const DScene& S, int i, const float* od, const float* dd, float t) {
-  float ol[3], dl[3];
-  d_to_local_pt(S, i, od, ol);
-  d_to_local_dir(S, i, dd, dl);
-  Scan s;
-  d_scan_init<1>(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, D_HUGE);
-  return d_mem_at(S, s, t, 0);
-}
-L_DEV int d_level_wins(const DScene& S, int item, int found, int excl) {
-  return (found < 0 || d_rank(S, item) > d_rank(S, found)) && item != excl && item < S.n;
-}
-
-// the BVH point scan: every daughter of v whose padded box holds x, visited by `visit`
-template <class F>
-L_DEV void d_point_scan(const DScene& S, int v, const float* x, float pad, F visit) {
-  int n0 = vI(S, v, LUMEN_VI_NODE0), n1 = vI(S, v, LUMEN_VI_NODE1);
-  int node = n0;
-  while (node < n1) {
-    const float* nf = S.node_f + (size_t)node * LUMEN_NODE_F;
-    int inside = (__ldg(nf) - pad <= x[0] && x[0] <= __ldg(nf + 3) + pad) &&
-                 (__ldg(nf + 1) - pad <= x[1] && x[1] <= __ldg(nf + 4) + pad) &&
-                 (__ldg(nf + 2) - pad <= x[2] && x[2] <= __ldg(nf + 5) + pad);
-    const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
-    int cnt = __ldg(ni + 1);
-    if (inside && cnt > 0) {
-      int st = __ldg(ni + 2);
-      for (int k = 0; k < cnt; ++k) visit(__ldg(S.items + st + k));
-    }
-    node = (inside && cnt == 0) ? node + 1 : __ldg(ni);
-  }
-}
-
-L_DEV int d_find(const DScene& S, int v, const float* x) {
-  int g = -1;
-  d_point_scan(S, v, x, 0.0f, [&](int i) {
-    if (d_level_wins(S, i, g, -1) && d_holds_point(S, i, x)) g = i;
-  });
-  return g;
-}
-L_CALL int d_locate(const DScene& S, const float* x) {
-  int v = S.n;
-  for (int guard = 0; guard < 64; ++guard) {
-    int f = d_find(S, v, x);
-    if (f < 0) return v;
-    v = f;
-  }
-  return v;
-}
-L_DEV int d_find_ray(const DScene& S, int v, const float* od, const float* dd, float t, int excl, float pad) {
-  float x[3] = {od[0] + t * dd[0], od[1] + t * dd[1], od[2] + t * dd[2]};
-  int g = -1;
-  d_point_scan(S, v, x, pad, [&](int i) {
-    if (d_level_wins(S, i, g, excl) && d_ray_holds(S, i, od, dd, t)) g = i;
-  });
-  return g;
-}
-L_CALL int d_settle(const DScene& S, int v, const float* od, const float* dd, float t, int crossed, float pad, int* moved) {
-  int v_ = v, held = 0;
-  for (int guard = 0; guard < 256; ++guard) {
-    int vi = v_ < S.n - 1 ? v_ : S.n - 1;
-    int test = !held && v_ < S.n && v_ != crossed;
-    int ins = !test || d_ray_holds(S, vi, od, dd, t);
-    int f = ins ? d_find_ray(S, v_, od, dd, t, crossed, pad) : -1;
-    int nv = ins ? (f >= 0 ? f : v_) : d_parent(S, v_ < S.n ? v_ : S.n);
-    held = ins && f >= 0;
-    if (f < 0 && ins) break;
-    v_ = nv;
-  }
-  *moved = v_ != v;
-  return v_;
-}
-
-// --------------------------------------------------------------------------------------------- a visit
-struct Side { int known, leaf, face; float s; int entry; };
-struct Best { float t; int item, leaf, face, zero, own; };
-struct Ctx {
-  int v;
-  float od[3], dd[3];
-  float t_lo, t_bound;
-  int last;
-  float band;
-  Side sd;
-};
-
-L_CALL int d_on_face(const DScene& S, const Ctx& c, int i, const First& fr, int kn_i) {
-  float dt = fr.t - c.t_lo;
-  float lim = D_K_ON * c.band;
-  int far_ = 0;
-  if (!kn_i && fr.hit && dt >= lim && dt < D_GRAZE * lim) {
-    float x0[3] = {c.od[0] + c.t_lo * c.dd[0], c.od[1] + c.t_lo * c.dd[1], c.od[2] + c.t_lo * c.dd[2]};
-    float xc[3] = {c.od[0] + fr.t * c.dd[0], c.od[1] + fr.t * c.dd[1], c.od[2] + fr.t * c.dd[2]};
-    int lf = fr.leaf > 0 ? fr.leaf : 0;
-    float g0[3], gc[3];
-    d_hit_grad(S, i, lf, fr.face, x0, g0);
-    d_hit_grad(S, i, lf, fr.face, xc, gc);
-    float s0 = d_dot(g0, c.dd) / d_safe_norm(g0);
-    int other_way = (s0 * d_dot(gc, c.dd) < 0.0f) && (fabsf(s0) > 1.0f / D_GRAZE);
-    far_ = (d_face_dist(S, i, lf, fr.face, x0) < lim) && !other_way;
-  }
-  return !kn_i && fr.hit && (dt < lim || far_);
-}
-
-L_DEV int d_entry_wins(const DScene& S, float t, int item, const Best& b) {
-  return t < b.t || (t == b.t && (b.own || d_rank(S, item) > d_rank(S, b.item)));
-}
-
-template <int TORUS>
-L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own) {
-  const Side& sd = c.sd;
-  float bnd = c.t_bound + c.band;
-  float ol[3], dl[3];
-  d_to_local_pt(S, i, c.od, ol);
-  d_to_local_dir(S, i, c.dd, dl);
-  int kn_i = sd.known && i == c.last;
-  float t_on = c.t_lo + D_K_ON * c.band / d_max(fabsf(sd.s), 1.0f / D_GRAZE);
-  int lf_on = kn_i ? sd.leaf : -2;
-  Scan s;
-  d_scan_init<TORUS>(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, bnd);
-  s.want = is_own ? 0 : 1;
-  s.has_init = 1; s.init_known = kn_i; s.init_inside = is_own;
-  s.has_skip = 1; s.skip_leaf = lf_on; s.skip_face = sd.face; s.skip_entry = sd.entry; s.skip_thi = D_HUGE;
-  s.has_on = 1; s.on_leaf = lf_on; s.on_inside = sd.entry; s.on_tend = t_on;
-  Fc r = d_first_change(S, s, c.t_lo);
-  int h = r.hit, lf = r.leaf, f = r.face;
-  float t = r.t;
-  int on = d_on_face(S, c, i, r.first, kn_i);
-  int by_s = kn_i && (is_own ? sd.s > 0.0f : sd.s < 0.0f);
-  int ins = kn_i ? (is_own ? (sd.s <= 0.0f && h) : sd.s < 0.0f) : (on ? r.first.inside : r.inside0);
-  h = h && (is_own || !ins);
-  int zero = is_own ? !ins : (ins && (i != c.last || kn_i));
-  if (zero) {
-    lf = by_s ? sd.leaf : (on ? r.first.leaf : -1);
-    f = by_s ? sd.face : (on ? r.first.face : -1);
-  }
-  int by_on = zero && on && !by_s;
-  int apart = 0;
-  if (by_on) {
-    float x0[3] = {c.od[0] + c.t_lo * c.dd[0], c.od[1] + c.t_lo * c.dd[1], c.od[2] + c.t_lo * c.dd[2]};
-    apart = d_face_dist(S, i, lf > 0 ? lf : 0, f, x0) > c.band;
-  }
-  float te = apart ? r.first.t : (zero ? c.t_lo : (h ? t : D_HUGE));
-  int wins = d_entry_wins(S, te, i, b);
-  int better = is_own || (!is_own && (zero || h) && wins);
-  if (better) {
-    Best nb = {te, i, lf, f, zero && !apart, is_own};
-    return nb;
-  }
-  return b;
-}
-
-// slab test of a node's box (bvh.py:258)
-L_DEV void d_slab(const float* __restrict__ node_f, int node, const float* o, const float* inv, float* tin,
-                  float* tout) {
-  const float* nf = node_f + (size_t)node * LUMEN_NODE_F;
-  float lo_t = -D_HUGE * 10.0f, hi_t = D_HUGE * 10.0f;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float ta = (__ldg(nf + a) - o[a]) * inv[a];
-    float tb = (__ldg(nf + 3 + a) - o[a]) * inv[a];
-    lo_t = d_max(lo_t, d_min(ta, tb));
-    hi_t = d_min(hi_t, d_max(ta, tb));
-  }
-  *tin = lo_t;
-  *tout = hi_t;
-}
-
-// the next event in volume v: its own exit, then the first entry of every daughter the BVH does not prune. One
-// call site of the visit (the own solid is the first candidate, then the traversal yields one leaf item at a time).
-template <int TORUS>
-L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
-  Best b = {D_HUGE, -1, -1, -1, 0, 0};
-  int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
-  float inv[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float dv = c.dd[a];
-    inv[a] = 1.0f / (fabsf(dv) < D_TINY_DIR ? (dv < 0.0f ? -D_TINY_DIR : D_TINY_DIR) : dv);
-  }
-  int stack[D_STACK];
-  float tins[D_STACK];
-  int sp = 0;
-  int node = -1;       // the traversal's next node (-1: pop or done)
-  int started = 0;     // the root has been tested
-  int pending = has_own;
-  for (;;) {
-    int item = -1, is_own = 0;
-    if (pending) {
-      item = vi;
-      is_own = 1;
-      pending = 0;
-    } else {
-      if (!started) {
-        started = 1;
-        if (n0 < n1) {
-          float tin, tout;
-          d_slab(S.node_f, n0, c.od, inv, &tin, &tout);
-          node = (tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band) ? n0 : -1;
-        }
-      }
-      while (item < 0) {
-        if (node < 0) {
-          float lim = d_min(b.t, c.t_bound) + c.band;
-          while (sp > 0 && tins[sp - 1] > lim) sp--;
-          if (sp == 0) break;
-          sp--;
-          node = stack[sp];
-        }
-        const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
-        int cnt = __ldg(ni + 1);
-        if (cnt > 0) {  // a leaf: one item
-          item = __ldg(S.items + __ldg(ni + 2));
-          node = -1;
-          break;
-        }
-        int lc = node + 1;
-        int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
-        float tl, tlo, tr, tro;
-        d_slab(S.node_f, lc, c.od, inv, &tl, &tlo);
-        d_slab(S.node_f, rc, c.od, inv, &tr, &tro);
-        float lim = d_min(b.t, c.t_bound) + c.band;
-        int hl = tl <= tlo && tlo >= c.t_lo && tl <= lim;
-        int hr = tr <= tro && tro >= c.t_lo && tr <= lim;
-        int first = tl <= tr;
-        int near_ = first ? lc : rc, far_ = first ? rc : lc;
-        int h_near = first ? hl : hr, h_far = first ? hr : hl;
-        if (h_near && h_far && sp < D_STACK) {
-          stack[sp] = far_;
-          tins[sp] = first ? tr : tl;
-          sp++;
-        }
-        node = h_near ? near_ : (h_far ? far_ : -1);
-      }
-      if (item < 0) break;
-    }
-    b = d_unit_visit<TORUS>(S, c, item, b, is_own);
-  }
-  return b;
-}
-
-// ------------------------------------------------------------------------------------------------ the query
-struct Query {
-  float t;
+// a query's result (navigate.py:617 _finish as the step reads it, step.py:260 _query): t in the navigator's precision
+// (for the position), every other float in float32
+template <class NF>
+struct QueryT {
+  NF t;
   int hit, cont;
   int vol_after, vol_before, vol_start, cls_before, cls_start, cls_after;
   float normal[3];
@@ -856,196 +112,65 @@ struct Query {
   int n_pass, vol_at, srf, rounds;
 };
 
-template <int TORUS>
-L_DEV Query d_query(const DScene& S, const float* o, const float* d, int vol, float t_max, int last, const float* sn,
-                    float s_at) {
-  const int OUT = S.n;
-  float xa = d_maxabs3(o);
-  int cls0 = d_cls(S, vol);
-  Srf l0 = d_srf_decode(S, last);
-  int kn0 = l0.known;
-  float t_lo = 0.0f;
-  int v = vol, last_ = last, done = 0, it = 0;
-  float rec_t = D_HUGE;
-  int rec_item = -1, rec_leaf = -1, rec_face = -1, rec_zero = 0, rec_vb = vol, rec_vis = 0;
-  int cur = cls0;
-  float pz_tp0 = D_HUGE, pz_tp1 = D_HUGE, pz_tin = 0.0f;
-  int pz_np = 0, pz_vend = vol, pz_hit = 0, pz_vat = vol, pz_zc = 0, pz_vin = vol;
-  int guard = 0;
-  while (!done) {
-    float band = d_band(xa + fabsf(t_lo));
-    int vi = v < OUT - 1 ? v : OUT - 1;
-    int has_own = v < OUT;
-    Srf ls = d_srf_decode(S, last_);
-    Side sd = {ls.known, ls.leaf, ls.face, 0.0f, 0};
-    if (ls.known) {
-      if (sn) {
-        sd.s = d_dot(sn, d) * (ls.e ? 1.0f : -1.0f);
-        sd.entry = sd.s * (ls.o ? 1.0f : -1.0f) < 0.0f;
-      } else {
-        float x0[3] = {o[0] + t_lo * d[0], o[1] + t_lo * d[1], o[2] + t_lo * d[2]};
-        float g[3];
-        d_hit_grad(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
-        float gd = d_dot(g, d);
-        sd.s = gd / d_safe_norm(g) * (ls.o ? 1.0f : -1.0f);
-        sd.entry = gd < 0.0f;
-      }
-    }
-    Ctx c;
-    c.v = v;
-    c.od[0] = o[0]; c.od[1] = o[1]; c.od[2] = o[2];
-    c.dd[0] = d[0]; c.dd[1] = d[1]; c.dd[2] = d[2];
-    c.t_lo = t_lo; c.t_bound = t_max; c.last = ls.item; c.band = band; c.sd = sd;
-    Best ev = d_enter<TORUS>(S, c, has_own, vi);
-    float t_c = ev.t;
-    int u_in = ev.item, l_in = ev.leaf, f_in = ev.face, z_in = ev.zero, is_own = ev.own;
-    int hit = t_c < t_max;
-    float step = d_band(xa + fabsf(hit ? t_c : t_lo));
-    int nxt = v, moved = 0;
-    {
-      int go_in = !is_own;
-      int uc = u_in < 0 ? 0 : (u_in > OUT - 1 ? OUT - 1 : u_in);
-      int up = d_parent(S, v < OUT ? v : OUT);
-      int nx0 = go_in ? u_in : up;
-      int unit_x = go_in ? u_in : vi;
-      int off = hit && l_in >= 0;
-      float od2[3] = {o[0], o[1], o[2]};
-      if (off) {
-        float x[3] = {o[0] + t_c * d[0], o[1] + t_c * d[1], o[2] + t_c * d[2]};
-        int itm = is_own ? vi : uc;
-        int lf = l_in > 0 ? l_in : 0;
-        float g[3];
-        d_hit_grad(S, itm, lf, f_in, x, g);
-        float gn = d_safe_norm(g);
-        float n_[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
-        float m = d_face_dist(S, itm, lf, f_in, x) + D_RELOCATE_BANDS * d_band(d_maxabs3(x));
-        float sg = d_dot(n_, d) < 0.0f ? -1.0f : 1.0f;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) od2[a] = o[a] + m * sg * n_[a];
-      }
-      float tr = off ? t_c : t_c + step;
-      if (hit) nxt = d_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
-      else { nxt = nx0; moved = 0; }
-    }
-    int item = !is_own ? u_in : vi;
-    int after = d_cls(S, hit ? nxt : v);
-    int zl = hit && it > 0 && (z_in || t_c - pz_tin <= D_ZERO_STEP_BANDS * band);
-    int touched = zl;
-    if (!zl && hit && it > 0 && v < OUT && after != cur) {
-      float xm[3];
-      float tm = 0.5f * (pz_tin + t_c);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) xm[a] = o[a] + tm * d[a];
-      touched = !d_holds_point(S, vi, xm);
-    }
-    if (touched) cur = d_cls(S, pz_vin);
-    int v_b = touched ? pz_vin : v;
-    int vis = hit && after != cur;
-    int inv_ = hit && !vis;
-    int zc = (inv_ && t_c - t_lo <= D_ZERO_STEP_BANDS * band) ? pz_zc + 1 : 0;
-    if (inv_ && pz_tp0 == D_HUGE) pz_tp0 = t_c;
-    if (inv_) pz_tp1 = t_c;
-    pz_np += inv_;
-    if (inv_) pz_vend = nxt;
-    pz_hit = hit;
-    if (inv_ && t_c <= s_at) pz_vat = nxt;
-    pz_zc = zc;
-    int n_vin = hit ? v_b : pz_vin;
-    float n_tin = hit ? t_c : pz_tin;
-    pz_vin = n_vin;
-    pz_tin = n_tin;
-    done = !hit || vis || zc >= D_ZSBP;
-    if (hit) { rec_t = t_c; rec_item = item; rec_leaf = l_in; rec_face = f_in; rec_zero = z_in; rec_vb = v_b; rec_vis = vis; }
-    t_lo = moved ? t_c + step : t_c;
-    if (hit) v = nxt;
-    last_ = item;
-    it += 1;
-    if (hit) cur = after;
-    if (++guard > 4096) break;
-  }
-  Query q;
-  float bt = rec_t;
-  int bi = rec_item, bl = rec_leaf, bf = rec_face, zero = rec_zero, vb = rec_vb;
-  int vis_end = rec_vis;
-  int cont = !vis_end && pz_hit && pz_zc >= D_ZSBP;
-  int hit = (vis_end || cont) && bt < t_max;
-  float px = bt < D_HUGE ? bt : 0.0f;
-  float xh[3] = {o[0] + px * d[0], o[1] + px * d[1], o[2] + px * d[2]};
-  float g[3];
-  d_hit_grad(S, bi, bl > 0 ? bl : 0, bf, xh, g);
-  float gn = d_safe_norm(g);
-  float nrm[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
-  float fb[3] = {-d[0], -d[1], -d[2]};
-  if (sn) {
-    int sat = hit && zero && bl < 0 && kn0 && bt <= 0.0f;
-    if (sat) {
-      float sl = d_safe_norm(sn);
-      fb[0] = sn[0] / sl; fb[1] = sn[1] / sl; fb[2] = sn[2] / sl;
-    }
-  }
-  if (!(hit && bl >= 0)) { nrm[0] = fb[0]; nrm[1] = fb[1]; nrm[2] = fb[2]; }
-  float gd = d_dot(g, d);
-  int entry = bi != vb;
-  q.srf = hit ? d_srf_pack(S, bi, bl, bf, entry ? gd < 0.0f : gd > 0.0f, entry) : -1;
-  if (nrm[0] * d[0] + nrm[1] * d[1] + nrm[2] * d[2] > 0.0f) { nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2]; }
-  vb = hit ? vb : pz_vend;
-  q.t = hit ? bt : t_max;
-  q.hit = hit;
-  q.cont = cont;
-  q.vol_after = hit ? v : vol;
-  q.vol_before = vb;
-  q.vol_start = vol;
-  q.cls_before = d_cls(S, vb);
-  q.cls_start = cls0;
-  q.cls_after = hit ? cur : d_cls(S, vb);
-  q.normal[0] = nrm[0]; q.normal[1] = nrm[1]; q.normal[2] = nrm[2];
-  q.item = hit ? bi : -1;
-  q.leaf = bl;
-  q.face = bf;
-  q.zero = hit && zero;
-  q.t_pass0 = pz_tp0;
-  q.t_pass1 = pz_tp1;
-  q.n_pass = pz_np;
-  q.vol_at = pz_vat;
-  q.rounds = it;
-  return q;
-}
+namespace nav32 {
+using NF = float;
+using NF3 = float3;
+using NF4 = float4;
+#define NAV_IS64 0
+#define NAV_VOL(S) (S).vol_f
+#define NAV_NODE(S) (S).node_f
+#define NAV_LEAF(S) (S).leaf_f
+#define NAV_PLANE(S) (S).plane_f
+#include "dnav.cuh"
+#undef NAV_IS64
+#undef NAV_VOL
+#undef NAV_NODE
+#undef NAV_LEAF
+#undef NAV_PLANE
+}  // namespace nav32
 
-// ------------------------------------------------------------------------------------------------ sensor reach
-// The query's bound for a bulk step (src/lumen/geometry/reach.py:201 ReachGeometry.query): where the photon, not on a
-// surface, starts inside its component's box, its free path s ends before the box's exit T, and the segment [0, T]
-// meets no sensor box, every crossing it can deposit at lies beyond s, so the query may stop at s plus the
-// navigator's own look-ahead ((GRAZE K_ON + 2) bands): the same arithmetic for every round that starts before s
-L_CALL float d_reach_bound(const DScene& S, const float* x, const float* d, int vol, int srf, float s, float t_max) {
-  if (!S.comp || srf >= 0 || vol < 0 || vol > S.n) return t_max;
-  int c = __ldg(S.comp + vol);
-  if (c < 0) return t_max;
-  float inv[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float dv = d[a];
-    inv[a] = 1.0f / (fabsf(dv) < D_TINY_DIR ? (dv < 0.0f ? -D_TINY_DIR : D_TINY_DIR) : dv);
-  }
-  const float* cb = S.comp_box + (size_t)c * 6;
-  float tin = -D_HUGE * 10.0f, tout = D_HUGE * 10.0f;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float ta = (__ldg(cb + a) - x[a]) * inv[a];
-    float tb = (__ldg(cb + 3 + a) - x[a]) * inv[a];
-    tin = d_max(tin, d_min(ta, tb));
-    tout = d_min(tout, d_max(ta, tb));
-  }
-  if (!(tin <= 0.0f && s < tout && s < t_max)) return t_max;
-  for (int node = 0, guard = 0; node < S.n_fnode && guard < S.n_fnode; ++guard) {  // any sensor box on [0, T]
-    float ti, to;
-    d_slab(S.fnode_f, node, x, inv, &ti, &to);
-    int hit = ti <= to && to >= 0.0f && ti <= tout;
-    int leaf = __ldg(S.fnode_i + (size_t)node * LUMEN_NODE_I + 1) > 0;
-    if (hit && leaf) return t_max;
-    node = (hit && !leaf) ? node + 1 : __ldg(S.fnode_i + (size_t)node * LUMEN_NODE_I);
-  }
-  float look = (D_GRAZE * D_K_ON + 2.0f) * d_band(d_maxabs3(x) + s);
-  return d_min(t_max, s + look);
+namespace nav64 {
+using NF = double;
+using NF3 = double3;
+using NF4 = double4;
+#define NAV_IS64 1
+#define NAV_VOL(S) reinterpret_cast<const double*>((S).vol_f)
+#define NAV_NODE(S) reinterpret_cast<const double*>((S).node_f)
+#define NAV_LEAF(S) reinterpret_cast<const double*>((S).leaf_f)
+#define NAV_PLANE(S) reinterpret_cast<const double*>((S).plane_f)
+#include "dnav.cuh"
+#undef NAV_IS64
+#undef NAV_VOL
+#undef NAV_NODE
+#undef NAV_LEAF
+#undef NAV_PLANE
+}  // namespace nav64
+
+using Query = QueryT<float>;
+
+// the step's entry points, by the position's precision
+L_DEV float nav_band(float scale) { return nav32::d_band(scale); }
+L_DEV double nav_band(double scale) { return nav64::d_band(scale); }
+L_DEV float nav_maxabs3(const float* x) { return nav32::d_maxabs3(x); }
+L_DEV double nav_maxabs3(const double* x) { return nav64::d_maxabs3(x); }
+L_DEV int nav_locate(const DScene& S, const float* x) { return nav32::d_locate(S, x); }
+L_DEV int nav_locate(const DScene& S, const double* x) { return nav64::d_locate(S, x); }
+template <int TORUS>
+L_DEV QueryT<float> nav_query(const DScene& S, const float* o, const float* d, int vol, float t_max, int last,
+                              const float* sn, float s_at) {
+  return nav32::d_query<TORUS>(S, o, d, vol, t_max, last, sn, s_at);
+}
+template <int TORUS>
+L_DEV QueryT<double> nav_query(const DScene& S, const double* o, const double* d, int vol, double t_max, int last,
+                               const float* sn, double s_at) {
+  return nav64::d_query<TORUS>(S, o, d, vol, t_max, last, sn, s_at);
+}
+L_DEV float nav_reach_bound(const DScene& S, const float* x, const float* d, int vol, int srf, float s, float t_max) {
+  return nav32::d_reach_bound(S, x, d, vol, srf, s, t_max);
+}
+L_DEV double nav_reach_bound(const DScene& S, const double* x, const float* d, int vol, int srf, float s,
+                             double t_max) {
+  return nav64::d_reach_bound(S, x, d, vol, srf, s, t_max);
 }
 
 }  // namespace lb

@@ -171,6 +171,23 @@ L_DEV float l_cbrt(float x) {
   return x < 0.0f ? -y : y;
 }
 
+// the cube root in float64 (the float64 navigator's torus): the float32 cube root of |x| (brought into float32's
+// normal range by powers of 2^96) as the start, then two Newton steps on y^3 = |x|, each squaring the relative error
+// (about 2^-22 -> 2^-44 -> below an ulp)
+L_DEV double l_cbrt64(double x) {
+  if (x == 0.0) return 0.0;
+  double a = x < 0.0 ? -x : x;
+  int k = 0;
+  for (int i = 0; i < 12 && a < 1e-30; ++i) { a = a * 79228162514264337593543950336.0; --k; }
+  for (int i = 0; i < 12 && a > 1e30; ++i) { a = a * 1.26217744835361888865876570445245796747713029617443680e-29; ++k; }
+  double y = (double)l_cbrt((float)a);
+  y = y - (y * y * y - a) / (3.0 * y * y);
+  y = y - (y * y * y - a) / (3.0 * y * y);
+  for (; k < 0; ++k) y = y * 2.3283064365386962890625e-10;
+  for (; k > 0; --k) y = y * 4294967296.0;
+  return x < 0.0 ? -y : y;
+}
+
 L_DEV float l_erfinv(float x) {
   float w = -l_log((1.0f - x) * (1.0f + x));
   float p;

@@ -90,8 +90,12 @@ L_CALL void d_diffuse(const DScene& S, int mi, const float* xs, const float* d0,
   }
 }
 
-struct Photon {
-  float x[3], d[3], t, lam, w, wr;
+// NF: the position's precision, the navigator's (float32, or float64 with the float64 navigator: state.py:120 start's
+// `position`); every other field float32
+template <class NF>
+struct PhotonT {
+  NF x[3];
+  float d[3], t, lam, w, wr;
   int alive, vertex;
   float er[3], ei[3];
   int vol, srf;
@@ -100,6 +104,7 @@ struct Photon {
   int gen;   // re-emissions so far (state.py Photon.gen: a WLS channel event adds one)
   int last;  // the photon's last deposit record (-1: none; the readout groups only)
 };
+using Photon = PhotonT<float>;
 
 // ----------------------------------------------------------------------------------- the deposit records
 // A_n: the share of a row absorbed and detected at normal incidence with eff 1, at the photon's wavelength and the
@@ -165,23 +170,27 @@ L_DEV float d_ratio(float live, float ref) { return ref != 0.0f ? live / ref : 0
 // What a step computes before its query and uses after it: the vertex key, the band at the step's start (before a
 // stuck push), the free path drawn at the reference, the medium at the live and reference values. The polarisation
 // state after the fill is written back into the photon.
-struct Pre {
+template <class NF>
+struct PreT {
   Key vkey;
-  float b0, s;
+  NF b0;  // the band at the start, in the navigator's precision (step.py:252)
+  float s;
   Med ml, mr;
 };
+using Pre = PreT<float>;
 
 // the step up to its query: the stuck push, the vertex key, the polarisation fill, the media, the free path
 // (step.py:318 _step_context, :245 _recover)
-L_DEV void d_pre(const Run& R, Photon& ph, Key pkey, Pre& pr) {
+template <class NF>
+L_DEV void d_pre(const Run& R, PhotonT<NF>& ph, Key pkey, PreT<NF>& pr) {
   const DScene& S = R.S;
-  pr.b0 = d_band(d_maxabs3(ph.x));
+  pr.b0 = nav_band(nav_maxabs3(ph.x));
   int stuck = ph.alive && ph.nz >= D_ZSBP;
   if (stuck) {
-    float pb = D_PUSH_BANDS * pr.b0;
+    NF pb = D_PUSH_BANDS * pr.b0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) ph.x[a] = ph.x[a] + pb * ph.d[a];
-    ph.vol = d_locate(S, ph.x);
+    ph.vol = nav_locate(S, ph.x);
     ph.cls = d_cls(S, ph.vol);
     ph.srf = -1;
   }
@@ -196,10 +205,15 @@ L_DEV void d_pre(const Run& R, Photon& ph, Key pkey, Pre& pr) {
 
 // the step's query, bounded just past the free path where no sensor can be met (step.py:260 _query with
 // reach.py's bound; the same result as the unbounded query on everything the step reads)
-template <int TORUS>
-L_DEV Query d_step_query(const Run& R, const Photon& ph, const Pre& pr) {
-  float tm = R.reach_on ? d_reach_bound(R.S, ph.x, ph.d, ph.vol, ph.srf, pr.s, R.max_distance) : R.max_distance;
-  return d_query<TORUS>(R.S, ph.x, ph.d, ph.vol, tm, ph.srf, ph.sn, pr.s);
+template <int TORUS, class NF>
+L_DEV QueryT<NF> d_step_query(const Run& R, const PhotonT<NF>& ph, const PreT<NF>& pr) {
+  NF tm = R.reach_on ? nav_reach_bound(R.S, ph.x, ph.d, ph.vol, ph.srf, pr.s, (NF)R.max_distance) : (NF)R.max_distance;
+  if constexpr (sizeof(NF) == 8) {  // the direction read in the navigator's precision (navigate.py:682)
+    const NF dd[3] = {ph.d[0], ph.d[1], ph.d[2]};
+    return nav_query<TORUS>(R.S, ph.x, dd, ph.vol, tm, ph.srf, ph.sn, (NF)pr.s);
+  } else {
+    return nav_query<TORUS>(R.S, ph.x, ph.d, ph.vol, tm, ph.srf, ph.sn, pr.s);
+  }
 }
 
 // The GLOSSY outcome's facet path by the row's lobe (surface_event.py:106 _facet_path_branch, :137
@@ -246,11 +260,13 @@ struct Ana {
   int vol;
 };
 
-template <int G, int ANALOG = 0>
-L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Query& q, Dep& dep, float* dq, Ana& an) {
+template <int G, int ANALOG = 0, class NF = float>
+L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, const QueryT<NF>& q, Dep& dep,
+                  float* dq, Ana& an) {
   const DScene& S = R.S;
   const int P = G > 0 ? R.P : 0;
-  const float b0 = pr.b0, s = pr.s;
+  const NF b0 = pr.b0;
+  const float s = pr.s;
   const Key vkey = pr.vkey;
   const Med& ml = pr.ml;
   const Med& mr = pr.mr;
@@ -357,7 +373,8 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
       dq[p] = at_if ? dw[p] * f + ph.w * df : 0.0f;
     }
   float lost = (q.hit && ph.alive && row < 0 && !scatter) ? ph.w * rr * att_if : 0.0f;
-  float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_er[3], nx_ei[3], nx_lam = ph.lam;
+  NF nx_x[3];
+  float nx_d[3], nx_w, nx_dtime, nx_er[3], nx_ei[3], nx_lam = ph.lam;
   int nx_gen = ph.gen;
   float nx_dw[G > 0 ? G : 1];
   int nx_cls, nx_ok, nx_far = 0;
@@ -407,7 +424,12 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
       for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
       d_project(nx_er, nx_ei, nx_d);
       if (R.jump_on) {  // the diffusion jump (step.py:421)
-        d_diffuse(S, mi, nx_x, nx_d, nx_er, nx_ei, mu_r, ph.alive, vkey, J);
+        if constexpr (sizeof(NF) == 8) {  // the grids are float32: the walk acts at x in float32 (fastpath.py:177)
+          const float xs[3] = {(float)nx_x[0], (float)nx_x[1], (float)nx_x[2]};
+          d_diffuse(S, mi, xs, nx_d, nx_er, nx_ei, mu_r, ph.alive, vkey, J);
+        } else {
+          d_diffuse(S, mi, nx_x, nx_d, nx_er, nx_ei, mu_r, ph.alive, vkey, J);
+        }
         if (J.ok) {
 #pragma unroll
           for (int a = 0; a < 3; ++a) { nx_x[a] = nx_x[a] + J.y[a]; nx_d[a] = J.d[a]; nx_er[a] = J.er[a]; }
@@ -578,7 +600,7 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
         an.scale = a > 0.0f ? 1.0f / a : 0.0f;
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) an.pos[a] = ph.x[a] + dist * ph.d[a];
+      for (int a = 0; a < 3; ++a) an.pos[a] = (float)(ph.x[a] + q.t * ph.d[a]);
       an.vol = q.vol_after;
       an.x = inf;
     } else {
@@ -612,7 +634,7 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
   dep.sensor = at_if ? sensor_q : -1;
   dep.time = time;
   if (R.rec && dep.sensor >= 0) {  // the readout groups' record, at the crossing (step.py:687 _local)
-    float xc[3] = {ph.x[0] + dist * ph.d[0], ph.x[1] + dist * ph.d[1], ph.x[2] + dist * ph.d[2]};
+    float xc[3] = {(float)(ph.x[0] + q.t * ph.d[0]), (float)(ph.x[1] + q.t * ph.d[1]), (float)(ph.x[2] + q.t * ph.d[2])};
     ph.last = d_record(R, ph.last, dep.sensor, dep.q, time, ph.lam, ph.gen, row, ml.n, q.vol_after, xc, ph.d,
                        q.normal);
   }
@@ -650,11 +672,11 @@ L_DEV void d_post(const Run& R, Photon& ph, float* dw, const Pre& pr, const Quer
 }
 
 // one whole step: the megakernel's (k_trace)
-template <int G, int TORUS, int ANALOG = 0>
-L_DEV void d_step(const Run& R, Photon& ph, float* dw, Key pkey, Dep& dep, float* dq, Ana& an) {
-  Pre pr;
+template <int G, int TORUS, int ANALOG = 0, class NF = float>
+L_DEV void d_step(const Run& R, PhotonT<NF>& ph, float* dw, Key pkey, Dep& dep, float* dq, Ana& an) {
+  PreT<NF> pr;
   d_pre(R, ph, pkey, pr);
-  Query q = d_step_query<TORUS>(R, ph, pr);
+  QueryT<NF> q = d_step_query<TORUS>(R, ph, pr);
   d_post<G, ANALOG>(R, ph, dw, pr, q, dep, dq, an);
 }
 
@@ -866,7 +888,8 @@ L_DEV void d_rows_row(const LumenRows& rows, int64_t i, Row& r) {
   r.event = rows.event ? __ldg(rows.event + i) : 0;
 }
 
-L_DEV void d_start(const DScene& S, const Row& r, Photon& ph) {
+template <class NF>
+L_DEV void d_start(const DScene& S, const Row& r, PhotonT<NF>& ph) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) { ph.x[a] = r.x[a]; ph.d[a] = r.d[a]; ph.er[a] = r.er[a]; ph.ei[a] = r.ei[a]; ph.sn[a] = 0.0f; }
   ph.t = r.t;
@@ -875,7 +898,7 @@ L_DEV void d_start(const DScene& S, const Row& r, Photon& ph) {
   ph.wr = 1.0f;
   ph.alive = 1;
   ph.vertex = 0;
-  ph.vol = d_locate(S, ph.x);
+  ph.vol = nav_locate(S, ph.x);
   ph.cls = d_cls(S, ph.vol);
   ph.srf = -1;
   ph.nz = 0;

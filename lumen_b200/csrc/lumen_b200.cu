@@ -48,7 +48,13 @@ struct LumenScene {
   std::vector<int32_t> tab;         // host copy of the (offset, knots) table index
   std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
   int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
+  int nav64;                           // LUMEN_PREC_FLOAT64: S's vol_f, node_f, leaf_f, plane_f hold float64 data
+  const float* vol_f32;                // the float32 frames (the readout groups' binning reads them in either precision)
 };
+
+// the position's precision of an instantiation: NAV64 = 1 the float64 navigator's (LUMEN_PREC_FLOAT64)
+template <int NAV64> struct NavOf { using F = float; };
+template <> struct NavOf<1> { using F = double; };
 
 // --------------------------------------------------------------------------------------------- the kernels
 struct Tally {
@@ -79,6 +85,8 @@ struct Launch {
 struct Pick {
   int torus;
   int analog;
+  int nav64;               // the scene's navigator is float64
+  const float* vol_f32;    // the scene's float32 frames (the readout binning)
 };
 
 #define CACHE 4
@@ -184,11 +192,12 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
 // (lumen_b200/autotune.py) picks one per workload. TORUS: the instantiation with the torus leaf code, run for scenes
 // with a torus (shape 0 only); the others are compiled without it, so a scene without one pays nothing for it.
 // ANALOG: each photon carries its analog photon and writes its record (truth rows: LUMEN_F_TRUTH; G = 0, shape 0).
-template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0>
+// NAV64: the float64 navigator and position (a LUMEN_PREC_FLOAT64 scene; shape 0, with the torus code).
+template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0, int NAV64 = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
-  Photon ph;
+  PhotonT<typename NavOf<NAV64>::F> ph;
   float dw[G > 0 ? G : 1], dq[G > 0 ? G : 1];
   PhotonTally pt;
   pt.n = 0;
@@ -482,12 +491,13 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
 }
 
 // One thread per photon to its end: the per-photon record the parity tests compare exactly.
+template <int NAV64>
 __global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
   Row r;
   get_row(L, i, r);
-  Photon ph;
+  PhotonT<typename NavOf<NAV64>::F> ph;
   d_start(L.R.S, r, ph);
   Key pkey = fold_in(L.key, (uint32_t)(L.first_id + i));
   float dw[1], dq[1];
@@ -515,29 +525,31 @@ __global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
   out_f[4 * i + 3] = (float)sum_qt;
 }
 
-__global__ void k_query(DScene S, const float* ray, const int32_t* vol, const int32_t* srf, float t_max, int64_t n,
-                        int32_t* out_i, float* out_f) {
+template <class NF>
+__global__ void k_query(DScene S, const NF* ray, const int32_t* vol, const int32_t* srf, NF t_max, int64_t n,
+                        int32_t* out_i, NF* out_f) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float o[3] = {ray[6 * i], ray[6 * i + 1], ray[6 * i + 2]};
-  float d[3] = {ray[6 * i + 3], ray[6 * i + 4], ray[6 * i + 5]};
+  NF o[3] = {ray[6 * i], ray[6 * i + 1], ray[6 * i + 2]};
+  NF d[3] = {ray[6 * i + 3], ray[6 * i + 4], ray[6 * i + 5]};
   int known = vol[i] >= 0 && vol[i] <= S.n;
-  int v = known ? vol[i] : d_locate(S, o);
+  int v = known ? vol[i] : nav_locate(S, o);
   int last = known ? srf[i] : -1;
-  Query q = d_query<1>(S, o, d, v, t_max, last, nullptr, D_HUGE);
+  QueryT<NF> q = nav_query<1>(S, o, d, v, t_max, last, nullptr, sizeof(NF) == 4 ? (NF)D_HUGE : (NF)1e30);
   int32_t* oi = out_i + 8 * i;
   oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
   oi[5] = q.srf; oi[6] = q.zero;
   oi[7] = q.hit ? vI(S, q.vol_after, LUMEN_VI_SENSOR) : -1;
-  float* of = out_f + 4 * i;
+  NF* of = out_f + 4 * i;
   of[0] = q.t; of[1] = q.normal[0]; of[2] = q.normal[1]; of[3] = q.normal[2];
 }
 
-__global__ void k_locate(DScene S, const float* pts, int64_t n, int32_t* vol) {
+template <class NF>
+__global__ void k_locate(DScene S, const NF* pts, int64_t n, int32_t* vol) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float x[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
-  vol[i] = d_locate(S, x);
+  NF x[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+  vol[i] = nav_locate(S, x);
 }
 
 // ------------------------------------------------------------------------------------------- host helpers
@@ -562,6 +574,11 @@ static int check_desc(const LumenSceneDesc* d) {
   if (!d || d->n_vol <= 0 || !d->vol_i || !d->vol_f || !d->kind_i || !d->leaf_f || !d->leaf_i || !d->prog_i ||
       !d->cls_medium || !d->row_of || !d->med_i || !d->tab || !d->pool || d->n_cls <= 0 || d->n_pool <= 0)
     return set_err(LUMEN_ERR_ARG, "scene_create: a required array is null or empty");
+  if (d->precision != LUMEN_PREC_FLOAT32 && d->precision != LUMEN_PREC_FLOAT64)
+    return set_err(LUMEN_ERR_ARG, "scene_create: precision is LUMEN_PREC_FLOAT32 or LUMEN_PREC_FLOAT64");
+  if (d->precision == LUMEN_PREC_FLOAT64 && (!d->vol_f64 || !d->leaf_f64 || (d->n_node > 0 && !d->node_f64) ||
+                                             (d->n_plane > 0 && !d->plane_f64)))
+    return set_err(LUMEN_ERR_ARG, "scene_create: a float64 scene without its float64 geometry arrays");
   for (int k = 0; k < d->n_kind; ++k) {
     int nl = d->kind_i[k * LUMEN_KIND_I + 1];
     if (nl < 1 || nl > LUMEN_MAX_LEAVES) return set_err(LUMEN_ERR_SCENE, "scene_create: a solid has too many leaves");
@@ -737,6 +754,8 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   L.n = n;
   L.step_budget = c->step_budget;
   pk.torus = sc->has_torus;
+  pk.nav64 = sc->nav64;
+  pk.vol_f32 = sc->vol_f32;
   pk.analog = (c->flags & LUMEN_F_TRUTH) != 0;
   if (pk.analog && (c->n_grad > 0 || !L.R.shared))
     return set_err(LUMEN_ERR_ARG, "truth rows decide each photon's fate at one set of values: no gradient parameters "
@@ -753,23 +772,28 @@ static int grid_for(const void* fn, int block, int* grid) {
   return 0;
 }
 
-template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0>
+template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0, int NAV64 = 0>
 static int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
   int grid = 0, st = 0;
-  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS, ANALOG>, BLOCK, &grid))) return st;
+  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS, ANALOG, NAV64>, BLOCK, &grid))) return st;
   if (bps > 0) {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (sms * bps < grid) grid = sms * bps;
   }
-  k_trace<G, BLOCK, MINB, TORUS, ANALOG><<<grid, BLOCK, 0, stream>>>(L);
+  k_trace<G, BLOCK, MINB, TORUS, ANALOG, NAV64><<<grid, BLOCK, 0, stream>>>(L);
   CK(cudaGetLastError());
   return 0;
 }
 
 template <int G>
 static int launch_trace(const Launch& L, const Pick& pk, int variant, int bps, cudaStream_t stream) {
+  if (pk.nav64) {  // the float64 navigator: shape 0 with the torus code, whatever the variant
+    if constexpr (G == 0)
+      if (L.truth) return launch_shape<0, 256, 4, 1, 1, 1>(L, bps, stream);
+    return launch_shape<G, 256, 4, 1, 0, 1>(L, bps, stream);
+  }
   if constexpr (G == 0) {
     if (L.truth)  // truth rows: the analog instantiation of shape 0
       return pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream) : launch_shape<0, 256, 4, 0, 1>(L, bps, stream);
@@ -851,7 +875,7 @@ static int check_groups(int n_sensor, const LumenTallies* out) {
   return 0;
 }
 
-static int launch_bin(const Launch& L, const LumenTallies* out, cudaStream_t stream) {
+static int launch_bin(const Launch& L, const Pick& pk, const LumenTallies* out, cudaStream_t stream) {
   Bin B;
   memset(&B, 0, sizeof(B));
   for (int g = 0; g < out->n_groups; ++g) B.g[g] = out->groups[g];
@@ -862,7 +886,7 @@ static int launch_bin(const Launch& L, const LumenTallies* out, cudaStream_t str
   B.n = L.R.rec_n;
   B.cap = L.R.rec_cap;
   B.pe2 = out->pe2;
-  B.vol_f = L.R.S.vol_f;
+  B.vol_f = pk.vol_f32;
   B.counts = out->counts;
   int dev = 0, sms = 0;
   CK(cudaGetDevice(&dev));
@@ -886,6 +910,7 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
     L.truth = out->truth;
     if (variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;
   }
+  if (pk.nav64 && variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;  // the wavefront's slots hold float32 positions
   T.grads = grads;
   // scratch: the photon counter, the abort flag, the steps used, the wavefront's live slots and the record count (one
   // small allocation per call)
@@ -941,7 +966,7 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
       if (st) return st;
     }
   }
-  if (groups && (st = launch_bin(L, out, stream))) return st;
+  if (groups && (st = launch_bin(L, pk, out, stream))) return st;
   if (async) {  // enqueue only: the abort flag reaches counts[LUMEN_C_ABORTED] on the device
     CK(cudaFreeAsync(scratch, stream));
     if (dummy) CK(cudaFreeAsync(dummy, stream));
@@ -1029,7 +1054,7 @@ static int run_trace_static(Launch& L, Pick pk, const LumenTallies* out, cudaStr
     else st = launch_trace<0>(L, pk, 0, 0, stream);
     if (st) return st;
   }
-  if (groups && (st = launch_bin(L, out, stream))) return st;
+  if (groups && (st = launch_bin(L, pk, out, stream))) return st;
   int flag = 0;
   unsigned long long n_rec = 0;
   CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -1103,6 +1128,19 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   UPLOAD(S.leaf_i, d->leaf_i, (size_t)d->n_leaf * LUMEN_LEAF_I);
   UPLOAD(S.plane_f, d->plane_f, (size_t)d->n_plane * LUMEN_PLANE_F);
   UPLOAD(S.prog_i, d->prog_i, (size_t)d->n_prog * LUMEN_PROG_I);
+  sc->nav64 = d->precision == LUMEN_PREC_FLOAT64;
+  sc->vol_f32 = S.vol_f;
+  if (sc->nav64) {  // the float64 navigator reads its arrays through the same pointers (checked non-null above)
+    const double *vd = nullptr, *nd = nullptr, *ld = nullptr, *pd = nullptr;
+    UPLOAD(vd, d->vol_f64, (size_t)d->n_vol * LUMEN_VOL_F);
+    UPLOAD(nd, d->node_f64, (size_t)d->n_node * LUMEN_NODE_F);
+    UPLOAD(ld, d->leaf_f64, (size_t)d->n_leaf * LUMEN_LEAF_F);
+    UPLOAD(pd, d->plane_f64, (size_t)d->n_plane * LUMEN_PLANE_F);
+    S.vol_f = reinterpret_cast<const float*>(vd);
+    S.node_f = reinterpret_cast<const float*>(nd);
+    S.leaf_f = reinterpret_cast<const float*>(ld);
+    S.plane_f = reinterpret_cast<const float*>(pd);
+  }
   UPLOAD(S.cls_medium, d->cls_medium, (size_t)d->n_cls);
   UPLOAD(S.row_of, d->row_of, (size_t)d->n_cls * d->n_cls);
   UPLOAD(S.med_i, d->med_i, (size_t)d->n_med * LUMEN_MED_I);
@@ -1237,7 +1275,8 @@ int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, co
   if (n == 0) return 0;
   int block = 128;
   int64_t grid = (n + block - 1) / block;
-  k_trace_photons<<<(unsigned)grid, block, 0, (cudaStream_t)stream>>>(L, out_i, out_f);
+  if (pk.nav64) k_trace_photons<1><<<(unsigned)grid, block, 0, (cudaStream_t)stream>>>(L, out_i, out_f);
+  else k_trace_photons<0><<<(unsigned)grid, block, 0, (cudaStream_t)stream>>>(L, out_i, out_f);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize((cudaStream_t)stream));
   return 0;
@@ -1247,6 +1286,7 @@ int32_t lumen_b200_query(const LumenScene* sc, const float* ray, const int32_t* 
                          int64_t n, int32_t* out_i, float* out_f, void* stream) {
   g_err.clear();
   if (!sc || !ray || !vol || !srf || !out_i || !out_f) return set_err(LUMEN_ERR_ARG, "query: a pointer is null");
+  if (sc->nav64) return set_err(LUMEN_ERR_ARG, "query: a float64 scene: use lumen_b200_query64");
   if (n == 0) return 0;
   int block = 128;
   k_query<<<(unsigned)((n + block - 1) / block), block, 0, (cudaStream_t)stream>>>(sc->S, ray, vol, srf, t_max, n,
@@ -1259,6 +1299,33 @@ int32_t lumen_b200_query(const LumenScene* sc, const float* ray, const int32_t* 
 int32_t lumen_b200_locate(const LumenScene* sc, const float* pts, int64_t n, int32_t* vol, void* stream) {
   g_err.clear();
   if (!sc || !pts || !vol) return set_err(LUMEN_ERR_ARG, "locate: a pointer is null");
+  if (sc->nav64) return set_err(LUMEN_ERR_ARG, "locate: a float64 scene: use lumen_b200_locate64");
+  if (n == 0) return 0;
+  int block = 128;
+  k_locate<<<(unsigned)((n + block - 1) / block), block, 0, (cudaStream_t)stream>>>(sc->S, pts, n, vol);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return 0;
+}
+
+int32_t lumen_b200_query64(const LumenScene* sc, const double* ray, const int32_t* vol, const int32_t* srf,
+                           double t_max, int64_t n, int32_t* out_i, double* out_f, void* stream) {
+  g_err.clear();
+  if (!sc || !ray || !vol || !srf || !out_i || !out_f) return set_err(LUMEN_ERR_ARG, "query64: a pointer is null");
+  if (!sc->nav64) return set_err(LUMEN_ERR_ARG, "query64: a float32 scene: use lumen_b200_query");
+  if (n == 0) return 0;
+  int block = 128;
+  k_query<<<(unsigned)((n + block - 1) / block), block, 0, (cudaStream_t)stream>>>(sc->S, ray, vol, srf, t_max, n,
+                                                                                    out_i, out_f);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return 0;
+}
+
+int32_t lumen_b200_locate64(const LumenScene* sc, const double* pts, int64_t n, int32_t* vol, void* stream) {
+  g_err.clear();
+  if (!sc || !pts || !vol) return set_err(LUMEN_ERR_ARG, "locate64: a pointer is null");
+  if (!sc->nav64) return set_err(LUMEN_ERR_ARG, "locate64: a float32 scene: use lumen_b200_locate");
   if (n == 0) return 0;
   int block = 128;
   k_locate<<<(unsigned)((n + block - 1) / block), block, 0, (cudaStream_t)stream>>>(sc->S, pts, n, vol);

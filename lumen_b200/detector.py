@@ -12,6 +12,7 @@ per crossed class pair, a medium per class) and src/lumen/build/tracked.py:181 (
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -22,6 +23,7 @@ from lumen_b200 import jump as J
 from lumen_b200 import optics as O
 
 OUTSIDE = "OUT"
+PRECISIONS = ("float32", "float64")
 
 
 @dataclass
@@ -45,6 +47,15 @@ class Detector:
     names: list
     classes: dict = field(default_factory=dict)
     groups: dict = field(default_factory=dict)  # sensor group -> sensor indices
+    precision: str = "float32"  # the navigator's: "float32" or "float64" (src/lumen/rules/navigation.py:96)
+
+    def with_precision(self, precision: str) -> Detector:
+        """Return this detector with the navigator in ``precision`` ("float32" or "float64"): the reference's load
+        option ``precision=`` (docs/dev/decisions.md:332). float64 runs the navigator (frames, boxes, leaves, roots,
+        intervals, the band) and the photon's position in float64, the physics in float32."""
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision {precision!r} is not one of {PRECISIONS}")
+        return dataclasses.replace(self, precision=precision)
 
     @property
     def n_sensor(self) -> int:
@@ -73,7 +84,7 @@ class Detector:
     # ------------------------------------------------------------------------------------ the C ABI's descriptor
     def desc(self):
         """Return (LumenSceneDesc, keepalive) over this detector's arrays (host pointers)."""
-        from lumen_b200._abi import LumenSceneDesc, iptr, fptr
+        from lumen_b200._abi import LumenSceneDesc, dptr, fptr, iptr
 
         a = self.arrays
         keep = {k: np.ascontiguousarray(v) for k, v in a.items() if isinstance(v, np.ndarray)}
@@ -86,6 +97,10 @@ class Detector:
         d.node_f, d.node_i, d.items = fptr(keep["node_f"]), iptr(keep["node_i"]), iptr(keep["items"])
         d.kind_i, d.leaf_f, d.leaf_i = iptr(keep["kind_i"]), fptr(keep["leaf_f"]), iptr(keep["leaf_i"])
         d.plane_f, d.prog_i = fptr(keep["plane_f"]), iptr(keep["prog_i"])
+        if self.precision == "float64":  # the float64 navigator's arrays
+            d.precision = 1
+            d.vol_f64, d.node_f64 = dptr(keep["vol_f64"]), dptr(keep["node_f64"])
+            d.leaf_f64, d.plane_f64 = dptr(keep["leaf_f64"]), dptr(keep["plane_f64"])
         d.reach = ctypes.c_float(a["reach"])
         d.n_cls, d.n_med, d.n_row = a["n_cls"], len(keep["med_i"]), len(keep["row_i"])
         d.n_tab, d.n_pool, d.n_sensor = len(keep["tab"]), len(keep["pool"]), self.n_sensor
@@ -112,7 +127,7 @@ class Detector:
 
 
 def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None,
-          after_tracking=()) -> Detector:
+          after_tracking=(), precision="float32") -> Detector:
     """Return the Detector of the volume tree ``top`` (the detector volume, placed at the origin).
 
     ``materials``: {name: Material}. ``borders``: [(pv from, pv to, OpticalSurface)] (Geant4 border surfaces, ordered);
@@ -121,7 +136,8 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     is absorbed there (the detector volume's boundary, as the reference's recipe ``detector_volume``).
     ``after_tracking``: sensor groups whose sensor model applies its QE after tracking: their rows detect every
     absorption (eff 1) and are read per normal incidence (types.py:576 per_normal: a deposit carries 1 / A_n, by
-    which a normalising readout grid divides it).
+    which a normalising readout grid divides it). ``precision``: the navigator's ("float32", or "float64":
+    ``Detector.with_precision``).
     """
     skins = skins or {}
     sensors = sensors or {}
@@ -264,4 +280,4 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     arrays.update(jump_f=jp["jump_f"], jump_i=jp["jump_i"], clear=jp["clear"], jump_report=jp["report"])
     st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
     cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}
-    return Detector(arrays, data, params_index, st, names, cls_names, groups)
+    return Detector(arrays, data, params_index, st, names, cls_names, groups).with_precision(precision)

@@ -125,6 +125,29 @@ def solids_box() -> D.Detector:
                    skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def coated_panel(thickness=3e-6, distance=5.0, precision="float32") -> D.Detector:
+    """Return a 12 m water box with a 2 x 2 m acrylic backing 20 cm thick at x = ``distance`` m, coated on its front
+    face with a TPB-like layer ``thickness`` m thick (rindex 1.6), and 4 photocathode discs (r 0.3 m) behind it: the
+    case the reference's float64 navigator is for (docs/dev/decisions.md:340): float32's band at 5 m is 4.8 um, so
+    float32 steps over a 3 um coating that float64 enters."""  # noqa: D205
+    water = O.Material("Water", rindex=1.33, abslength=40.0, rayleigh=40.0)
+    acrylic = O.Material("Acrylic", rindex=1.49, abslength=5.0)
+    tpb = O.Material("TPB", rindex=1.6, abslength=1.0)
+    cathode = O.Material("Photocathode")
+    world = G.Volume("World", G.Box(6.0, 6.0, 6.0), "Water")
+    world.place(G.Volume("Backing", G.Box(0.1, 1.0, 1.0), "Acrylic"), (distance + 0.1, 0.0, 0.0), None, name="Backing")
+    world.place(G.Volume("Coating", G.Box(0.5 * thickness, 1.0, 1.0), "TPB"), (distance - 0.5 * thickness, 0.0, 0.0),
+                None, name="Coating")  # fmt: skip
+    pmt = G.Volume("PMT", G.Tube(rmax=0.3, dz=0.01), "Photocathode")
+    rot = G.rotation("y", 90.0)  # the discs' axis along x
+    for k, (y, z) in enumerate(((-0.45, -0.45), (-0.45, 0.45), (0.45, -0.45), (0.45, 0.45))):
+        world.place(pmt, (distance + 0.25, y, z), rot, name=f"PMT_{k}", copy=k)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    borders = [("World", f"PMT_{k}", surf) for k in range(4)]
+    return D.build(world, {"Water": water, "Acrylic": acrylic, "TPB": tpb, "Photocathode": cathode}, borders=borders,
+                   sensors={"pmt": "PMT"}, precision=precision)  # fmt: skip
+
+
 def scintillator_cube(mie=2.0, wls=1.0, rayleigh=5.0, profile="exponential") -> D.Detector:
     """Return the tutorial tank's geometry filled with a synthetic liquid scintillator whose bulk has all three of
     Geant4's channels: Rayleigh, Mie (G4OpMieHG, MIEHG ``mie`` m, forward 0.9, backward 0.3, forward ratio 0.8) and a

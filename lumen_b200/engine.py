@@ -194,8 +194,11 @@ class Engine:
         return out_i, out_f
 
     def query(self, o, d, vol=None, srf=None, t_max=None):
-        o = torch.as_tensor(np.asarray(o, np.float32).reshape(-1, 3), device=self.device)
-        d = torch.as_tensor(np.asarray(d, np.float32).reshape(-1, 3), device=self.device)
+        """The navigator query per ray (lumen_b200_query; lumen_b200_query64 in float64 on a float64 detector)."""
+        f64 = self.det.precision == "float64"
+        dt, tt = (np.float64, torch.float64) if f64 else (np.float32, torch.float32)
+        o = torch.as_tensor(np.asarray(o, dt).reshape(-1, 3), device=self.device)
+        d = torch.as_tensor(np.asarray(d, dt).reshape(-1, 3), device=self.device)
         n = o.shape[0]
         ray = torch.cat([o, d], 1).contiguous()
         vol = torch.full((n,), -1, dtype=torch.int32, device=self.device) if vol is None else \
@@ -203,16 +206,26 @@ class Engine:
         srf = torch.full((n,), -1, dtype=torch.int32, device=self.device) if srf is None else \
             torch.as_tensor(np.asarray(srf, np.int32), device=self.device)  # fmt: skip
         out_i = torch.zeros((n, 8), dtype=torch.int32, device=self.device)
-        out_f = torch.zeros((n, 4), dtype=torch.float32, device=self.device)
+        out_f = torch.zeros((n, 4), dtype=tt, device=self.device)
         tm = self.det.arrays["reach"] if t_max is None else t_max
         with torch.cuda.device(self.device):
-            A.check(self.lib.lumen_b200_query(self.h, _f32p(ray), _i32p(vol), _i32p(srf), ctypes.c_float(tm), n,
-                                              _i32p(out_i), _f32p(out_f), self._stream(None)))  # fmt: skip
+            if f64:
+                A.check(self.lib.lumen_b200_query64(self.h, _f64p(ray), _i32p(vol), _i32p(srf), ctypes.c_double(tm),
+                                                    n, _i32p(out_i), _f64p(out_f), self._stream(None)))  # fmt: skip
+            else:
+                A.check(self.lib.lumen_b200_query(self.h, _f32p(ray), _i32p(vol), _i32p(srf), ctypes.c_float(tm), n,
+                                                  _i32p(out_i), _f32p(out_f), self._stream(None)))  # fmt: skip
         return out_i, out_f
 
     def locate(self, pts):
-        p = torch.as_tensor(np.asarray(pts, np.float32).reshape(-1, 3), device=self.device).contiguous()
+        """The volume holding each point (lumen_b200_locate; lumen_b200_locate64 on a float64 detector)."""
+        f64 = self.det.precision == "float64"
+        dt = np.float64 if f64 else np.float32
+        p = torch.as_tensor(np.asarray(pts, dt).reshape(-1, 3), device=self.device).contiguous()
         vol = torch.zeros(p.shape[0], dtype=torch.int32, device=self.device)
         with torch.cuda.device(self.device):
-            A.check(self.lib.lumen_b200_locate(self.h, _f32p(p), p.shape[0], _i32p(vol), self._stream(None)))
+            if f64:
+                A.check(self.lib.lumen_b200_locate64(self.h, _f64p(p), p.shape[0], _i32p(vol), self._stream(None)))
+            else:
+                A.check(self.lib.lumen_b200_locate(self.h, _f32p(p), p.shape[0], _i32p(vol), self._stream(None)))
         return vol

@@ -838,6 +838,24 @@ def pad_box(lo, hi):
     return lo - pad, hi + pad
 
 
+def _node_boxes64(node_i, items, lo, hi) -> np.ndarray:
+    """Return the BVH nodes' boxes in float64 over the float32 BVH's topology (depth-first with skips: a node's left
+    child follows it, its right child is the left child's skip): a leaf the union of its items' float64 boxes, an inner
+    node the union of its children's, bottom-up."""
+    out = np.zeros((len(node_i), 6))
+    for k in range(len(node_i) - 1, -1, -1):
+        cnt, st = int(node_i[k, 1]), int(node_i[k, 2])
+        if cnt > 0:
+            it = items[st:st + cnt]
+            out[k, :3], out[k, 3:] = lo[it].min(0), hi[it].max(0)
+        else:
+            lc = k + 1
+            rc = int(node_i[lc, 0])
+            out[k, :3] = np.minimum(out[lc, :3], out[rc, :3])
+            out[k, 3:] = np.maximum(out[lc, 3:], out[rc, 3:])
+    return out
+
+
 def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=None) -> dict:
     """Return the navigator's flat arrays (include/lumen_b200.h layouts) of the placed volumes."""
     n = len(placed)
@@ -910,8 +928,13 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
             raise ValueError(f"volume {v}: a daughter BVH deeper than {MAX_BVH_DEPTH} levels")
     allp = np.concatenate([lo_w, hi_w]) if n else np.zeros((1, 3))
     reach = float(np.linalg.norm(allp.max(0) - allp.min(0)))
+    items_a = np.asarray(items, np.int64)
     return dict(
         n_vol=n, vol_i=vol_i, vol_f=vol_f.astype(np.float32), cand=np.asarray(cand, np.int32),
+        # the float64 navigator's arrays (LUMEN_PREC_FLOAT64): the same geometry in float64, the BVH's topology shared
+        vol_f64=vol_f.copy(), leaf_f64=np.asarray(leaf_f, np.float64).reshape(-1, 20),
+        plane_f64=np.asarray(plane_f, np.float64).reshape(-1, 4),
+        node_f64=_node_boxes64(ni_arr, items_a, lo_w, hi_w),
         node_f=np.asarray(node_f, np.float32).reshape(-1, 6), node_i=np.asarray(node_i, np.int32).reshape(-1, 4),
         items=np.asarray(items, np.int32), kind_i=np.asarray(kind_i, np.int32).reshape(-1, 4),
         leaf_f=np.asarray(leaf_f, np.float32).reshape(-1, 20), leaf_i=np.asarray(leaf_i, np.int32).reshape(-1, 4),

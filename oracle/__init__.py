@@ -38,6 +38,9 @@ def lib():
         L.lumen_oracle_query.argtypes = [P(A.LumenSceneDesc), A.c_f32p, A.c_i32p, A.c_i32p, ctypes.c_float,
                                          ctypes.c_int64, A.c_i32p, A.c_f32p]
         L.lumen_oracle_locate.argtypes = [P(A.LumenSceneDesc), A.c_f32p, ctypes.c_int64, A.c_i32p]
+        L.lumen_oracle_query64.argtypes = [P(A.LumenSceneDesc), A.c_f64p, A.c_i32p, A.c_i32p, ctypes.c_double,
+                                           ctypes.c_int64, A.c_i32p, A.c_f64p]
+        L.lumen_oracle_locate64.argtypes = [P(A.LumenSceneDesc), A.c_f64p, ctypes.c_int64, A.c_i32p]
         L.lumen_oracle_uniforms.argtypes = [ctypes.c_uint32, ctypes.c_uint32, A.c_i64p, ctypes.c_int64,
                                             ctypes.c_int32, ctypes.c_int32, A.c_f32p]
         L.lumen_oracle_threefry.argtypes = [ctypes.c_uint32] * 4 + [P(ctypes.c_uint32)]
@@ -144,7 +147,14 @@ def unified(fn, inp, U=None):
 
 
 def locate(det, pts):
+    """The volume holding each point, in the detector's navigator precision (float64 points on a float64 one)."""
     d, keep = det.desc()
+    if det.precision == "float64":
+        pts = np.ascontiguousarray(np.asarray(pts, np.float64).reshape(-1, 3))
+        vol = np.zeros(len(pts), np.int32)
+        st = lib().lumen_oracle_locate64(ctypes.byref(d), A.dptr(pts), len(pts), A.iptr(vol))
+        assert st == 0, st
+        return vol
     pts = A.np_f32(pts).reshape(-1, 3)
     vol = np.zeros(len(pts), np.int32)
     st = lib().lumen_oracle_locate(ctypes.byref(d), A.fptr(pts), len(pts), A.iptr(vol))
@@ -153,18 +163,25 @@ def locate(det, pts):
 
 
 def query(det, o, dvec, vol=None, srf=None, t_max=None):
-    """The navigator query per ray (the layout of lumen_b200_query): (out_i (n, 8), out_f (n, 4))."""
+    """The navigator query per ray (the layout of lumen_b200_query): (out_i (n, 8), out_f (n, 4)); in float64
+    (rays, t_max and out_f) on a float64 detector (lumen_b200_query64)."""  # noqa: D205, D209
     d, keep = det.desc()
-    o, dvec = A.np_f32(o).reshape(-1, 3), A.np_f32(dvec).reshape(-1, 3)
+    f64 = det.precision == "float64"
+    dt = np.float64 if f64 else np.float32
+    o, dvec = np.asarray(o, dt).reshape(-1, 3), np.asarray(dvec, dt).reshape(-1, 3)
     n = len(o)
-    ray = np.ascontiguousarray(np.concatenate([o, dvec], 1), np.float32)
+    ray = np.ascontiguousarray(np.concatenate([o, dvec], 1), dt)
     vol = np.full(n, -1, np.int32) if vol is None else np.ascontiguousarray(vol, np.int32)
     srf = np.full(n, -1, np.int32) if srf is None else np.ascontiguousarray(srf, np.int32)
     out_i = np.zeros((n, 8), np.int32)
-    out_f = np.zeros((n, 4), np.float32)
+    out_f = np.zeros((n, 4), dt)
     tm = det.arrays["reach"] if t_max is None else t_max
-    st = lib().lumen_oracle_query(ctypes.byref(d), A.fptr(ray), A.iptr(vol), A.iptr(srf), ctypes.c_float(tm), n,
-                                  A.iptr(out_i), A.fptr(out_f))  # fmt: skip
+    if f64:
+        st = lib().lumen_oracle_query64(ctypes.byref(d), A.dptr(ray), A.iptr(vol), A.iptr(srf), ctypes.c_double(tm),
+                                        n, A.iptr(out_i), A.dptr(out_f))  # fmt: skip
+    else:
+        st = lib().lumen_oracle_query(ctypes.byref(d), A.fptr(ray), A.iptr(vol), A.iptr(srf), ctypes.c_float(tm), n,
+                                      A.iptr(out_i), A.fptr(out_f))  # fmt: skip
     assert st == 0, st
     return out_i, out_f
 

@@ -12,7 +12,7 @@
  *  - sin / cos of 2 pi u: exact quarter-turn reduction of 4u, then the same polynomials.
  *  - asin / acos: asin x = x + x^3 P(x^2) on |x| <= 1/2 (P a least-squares fit on Chebyshev nodes, float64, to
  *    (asin x - x) / x^3), acos by the half-angle identities beyond.
- *  - cbrt: exp(log|x| / 3) and one Newton step.
+ *  - cbrt: exp(log|x| / 3) and one Newton step; in float64 that root and two Newton steps in float64.
  *  - erfinv: M. Giles, "Approximating the erfinv function" (GPU Computing Gems Jade, 2011), single precision.
  */
 #ifndef LUMEN_ORACLE_LMATH_H
@@ -178,6 +178,22 @@ static inline float o_cbrt(float x) {
   float y = o_exp(o_log(a) * 0.333333343267440796f);
   y = y - (y * y * y - a) / (3.0f * y * y);
   return x < 0.0f ? -y : y;
+}
+
+/* the cube root in float64 (the float64 navigator's torus): the float32 cube root of |x| (brought into float32's
+   normal range by powers of 2^96) as the start, then two Newton steps on y^3 = |x| */
+static inline double o_cbrt64(double x) {
+  if (x == 0.0) return 0.0;
+  double a = x < 0.0 ? -x : x;
+  int k = 0;
+  for (int i = 0; i < 12 && a < 1e-30; ++i) { a = a * 79228162514264337593543950336.0; --k; }
+  for (int i = 0; i < 12 && a > 1e30; ++i) { a = a * 1.26217744835361888865876570445245796747713029617443680e-29; ++k; }
+  double y = (double)o_cbrt((float)a);
+  y = y - (y * y * y - a) / (3.0 * y * y);
+  y = y - (y * y * y - a) / (3.0 * y * y);
+  for (; k < 0; ++k) y = y * 2.3283064365386962890625e-10;
+  for (; k > 0; --k) y = y * 4294967296.0;
+  return x < 0.0 ? -y : y;
 }
 
 /* M. Giles' single-precision erfinv (published coefficients), x in (-1, 1) */

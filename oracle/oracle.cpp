@@ -43,8 +43,11 @@ typedef struct ORun {
   int analog; /* LUMEN_F_TRUTH */
 } ORun;
 
-typedef struct OPhoton {
-  float x[3], d[3], t, lam, w, wr;
+/* NF: the position's precision, the navigator's (state.py:120 start's `position`); every other field float32 */
+template <class NF>
+struct OPhotonT {
+  NF x[3];
+  float d[3], t, lam, w, wr;
   int alive, vertex;
   float er[3], ei[3];
   int vol, srf;
@@ -58,7 +61,7 @@ typedef struct OPhoton {
   int asensor;
   float atime, alam, ascale, apos[3];
   int avol;
-} OPhoton;
+};
 
 typedef struct ODep {
   int sensor;
@@ -158,18 +161,19 @@ static inline void o_dmed(const ORun* R, int mi, float lam, const OMed* m, float
   }
 }
 
-/* one step (step.py:516) */
-static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
+/* one step (step.py:516); NF the navigator's precision */
+template <class NF>
+static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
   const OScene* S = &R->S;
   const LumenSceneDesc* D = S->D;
   const int P = R->P;
   /* _recover: the stuck rule's push (step.py:245) */
-  float b0 = o_band(o_maxabs3(ph->x));
+  NF b0 = onav_band(onav_maxabs3(ph->x));
   int stuck = ph->alive && ph->nz >= O_ZSBP;
   if (stuck) {
-    float pb = O_PUSH_BANDS * b0;
+    NF pb = O_PUSH_BANDS * b0;
     for (int a = 0; a < 3; ++a) ph->x[a] = ph->x[a] + pb * ph->d[a];
-    ph->vol = o_locate(S, ph->x);
+    ph->vol = onav_locate(S, ph->x);
     ph->cls = o_cls(S, ph->vol);
     ph->srf = -1;
   }
@@ -185,7 +189,8 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   float mu_r = mr.mu_c;
   float s = -o_log(o_uniform(vkey, 0)) / o_max(mu_r, O_FLOOR32);
   /* _query (step.py:260; TrackedGeometry.query, tracked.py:86) */
-  OQuery q = o_query(S, ph->x, ph->d, ph->vol, R->max_distance, ph->srf, ph->sn, s);
+  const NF dd[3] = {ph->d[0], ph->d[1], ph->d[2]}; /* the direction in the navigator's precision (navigate.py:682) */
+  OQueryT<NF> q = onav_query(S, ph->x, dd, ph->vol, (NF)R->max_distance, ph->srf, ph->sn, (NF)s);
   int sensor_q = q.hit ? D->vol_i[(size_t)q.vol_after * LUMEN_VOL_I + LUMEN_VI_SENSOR] : -1;
   float dist = q.t;
   int zero = dist <= O_ZERO_STEP_BANDS * b0;
@@ -245,7 +250,8 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
   }
   float lost = (q.hit && ph->alive && row < 0 && !scatter) ? ph->w * rr * att_if : 0.0f;
   /* _event: a bulk event or the drawn surface outcome (step.py:439) */
-  float nx_x[3], nx_d[3], nx_w, nx_dtime, nx_sn[3], nx_er[3], nx_ei[3], nx_lam = ph->lam;
+  NF nx_x[3];
+  float nx_d[3], nx_w, nx_dtime, nx_sn[3], nx_er[3], nx_ei[3], nx_lam = ph->lam;
   int nx_gen = ph->gen;
   float nx_dw[O_MAXG];
   int nx_cls, nx_ok, nx_far = 0;
@@ -278,7 +284,8 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
       for (int a = 0; a < 3; ++a) { nx_er[a] = er0[a]; nx_ei[a] = ei0[a]; }
       o_project(nx_er, nx_ei, nx_d);
       if (R->jump) { /* the diffusion jump (step.py:421): the walk's factor on the weight, its time on the clock */
-        J = o_diffuse(D, mi, nx_x, nx_d, nx_er, nx_ei, mu_r, ph->alive, vkey);
+        const float xs[3] = {(float)nx_x[0], (float)nx_x[1], (float)nx_x[2]}; /* the grids are float32 (fastpath.py:177) */
+        J = o_diffuse(D, mi, xs, nx_d, nx_er, nx_ei, mu_r, ph->alive, vkey);
         if (J.ok) {
           for (int a = 0; a < 3; ++a) { nx_x[a] = nx_x[a] + J.y[a]; nx_d[a] = J.d[a]; nx_er[a] = J.er[a]; }
         }
@@ -490,7 +497,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
         const float an = o_normal_absorptance(D, R->live, row, ph->lam, ml.n, q.normal);
         ph->ascale = an > 0.0f ? 1.0f / an : 0.0f;
       }
-      for (int a = 0; a < 3; ++a) ph->apos[a] = ph->x[a] + dist * ph->d[a];
+      for (int a = 0; a < 3; ++a) ph->apos[a] = (float)(ph->x[a] + q.t * ph->d[a]);
       ph->avol = q.vol_after;
       ph->ax = INFINITY;
     } else {
@@ -536,7 +543,7 @@ static void o_step(const ORun* R, OPhoton* ph, OKey pkey, ODep* dep) {
     rc->lam = ph->lam;
     rc->gen = ph->gen;
     rc->vol = q.vol_after;
-    for (int a = 0; a < 3; ++a) { rc->x[a] = ph->x[a] + dist * ph->d[a]; rc->d[a] = ph->d[a]; rc->n[a] = q.normal[a]; }
+    for (int a = 0; a < 3; ++a) { rc->x[a] = (float)(ph->x[a] + q.t * ph->d[a]); rc->d[a] = ph->d[a]; rc->n[a] = q.normal[a]; }
     rc->inv_an = 1.0f;
     if (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL]) {
       float an = o_normal_absorptance(D, R->live, row, ph->lam, ml.n, q.normal);
@@ -779,10 +786,11 @@ typedef struct OGroupCtx {
 } OGroupCtx;
 
 /* one photon's loop (run.py:307 item): begin, steps until it ends or reaches the vertex guard */
+template <class NF>
 static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTally* T, int32_t* rec_i,
                      float* rec_f, OGroupCtx* gc, float* truth) {
   const OScene* S = &R->S;
-  OPhoton ph;
+  OPhotonT<NF> ph;
   memset(&ph, 0, sizeof(ph));
   for (int a = 0; a < 3; ++a) { ph.x[a] = row->x[a]; ph.d[a] = row->d[a]; ph.er[a] = row->er[a]; ph.ei[a] = row->ei[a]; }
   ph.t = row->t;
@@ -791,7 +799,7 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
   ph.wr = 1.0f;
   ph.alive = 1;
   ph.vertex = 0;
-  ph.vol = o_locate(S, ph.x);
+  ph.vol = onav_locate(S, ph.x);
   ph.cls = o_cls(S, ph.vol);
   ph.srf = -1;
   ph.nz = 0;
@@ -907,6 +915,8 @@ static int o_scene(const LumenSceneDesc* D, OScene* S) {
     }
   }
   S->SU = D->n_vol + 1;
+  S->nav64 = D->precision == LUMEN_PREC_FLOAT64;
+  if (S->nav64 && (!D->vol_f64 || !D->leaf_f64 || (D->n_plane > 0 && !D->plane_f64))) return LUMEN_ERR_ARG;
   return LUMEN_OK;
 }
 
@@ -1138,7 +1148,41 @@ int32_t lumen_oracle_locate(const LumenSceneDesc* D, const float* pts, int64_t n
   int st = o_scene(D, &S);
   if (st) return st;
 #pragma omp parallel for schedule(dynamic, 64)
-  for (int64_t i = 0; i < n; ++i) vol[i] = o_locate(&S, pts + 3 * i);
+  for (int64_t i = 0; i < n; ++i) vol[i] = onav32::o_locate(&S, pts + 3 * i);
+  return 0;
+}
+
+/* locate and query in float64 (a float64 scene: LUMEN_PREC_FLOAT64), the layout of lumen_b200_locate64 / query64 */
+int32_t lumen_oracle_locate64(const LumenSceneDesc* D, const double* pts, int64_t n, int32_t* vol) {
+  OScene S;
+  int st = o_scene(D, &S);
+  if (st) return st;
+  if (!S.nav64) return LUMEN_ERR_ARG;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) vol[i] = onav64::o_locate(&S, pts + 3 * i);
+  return 0;
+}
+
+int32_t lumen_oracle_query64(const LumenSceneDesc* D, const double* ray, const int32_t* vol, const int32_t* srf,
+                             double t_max, int64_t n, int32_t* out_i, double* out_f) {
+  OScene S;
+  int st = o_scene(D, &S);
+  if (st) return st;
+  if (!S.nav64) return LUMEN_ERR_ARG;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    const double* o = ray + 6 * i;
+    const double* d = ray + 6 * i + 3;
+    int v = vol[i] >= 0 ? vol[i] : onav64::o_locate(&S, o);
+    int last = vol[i] >= 0 ? srf[i] : -1;
+    OQueryT<double> q = onav64::o_query(&S, o, d, v, t_max, last, 0, 1e30);
+    int32_t* oi = out_i + 8 * i;
+    oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
+    oi[5] = q.srf; oi[6] = q.zero;
+    oi[7] = q.hit ? D->vol_i[(size_t)q.vol_after * LUMEN_VOL_I + LUMEN_VI_SENSOR] : -1;
+    double* of = out_f + 4 * i;
+    of[0] = q.t; of[1] = q.normal[0]; of[2] = q.normal[1]; of[3] = q.normal[2];
+  }
   return 0;
 }
 
@@ -1152,9 +1196,9 @@ int32_t lumen_oracle_query(const LumenSceneDesc* D, const float* ray, const int3
   for (int64_t i = 0; i < n; ++i) {
     const float* o = ray + 6 * i;
     const float* d = ray + 6 * i + 3;
-    int v = vol[i] >= 0 ? vol[i] : o_locate(&S, o);
+    int v = vol[i] >= 0 ? vol[i] : onav32::o_locate(&S, o);
     int last = vol[i] >= 0 ? srf[i] : -1;
-    OQuery q = o_query(&S, o, d, v, t_max, last, 0, O_HUGE);
+    OQuery q = onav32::o_query(&S, o, d, v, t_max, last, 0, O_HUGE);
     int32_t* oi = out_i + 8 * i;
     oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
     oi[5] = q.srf; oi[6] = q.zero;
@@ -1203,9 +1247,13 @@ int32_t lumen_oracle_trace(const LumenSceneDesc* D, const float* pool_live, cons
   for (int64_t i = 0; i < n; ++i) {
     ORow r;
     o_row_of(&R, rows, src, key, first_id, i, &r);
-    o_photon(&R, &r, key, first_id + i, &parts[omp_get_thread_num()], rec_i ? rec_i + 5 * i : 0,
-             rec_f ? rec_f + 4 * i : 0, groups ? &gparts[omp_get_thread_num()] : 0,
-             (R.analog && out->truth) ? out->truth + (size_t)LUMEN_TRUTH_WORDS * i : 0);
+    OTally* Tp = &parts[omp_get_thread_num()];
+    OGroupCtx* gp = groups ? &gparts[omp_get_thread_num()] : 0;
+    float* tr = (R.analog && out->truth) ? out->truth + (size_t)LUMEN_TRUTH_WORDS * i : 0;
+    if (R.S.nav64)
+      o_photon<double>(&R, &r, key, first_id + i, Tp, rec_i ? rec_i + 5 * i : 0, rec_f ? rec_f + 4 * i : 0, gp, tr);
+    else
+      o_photon<float>(&R, &r, key, first_id + i, Tp, rec_i ? rec_i + 5 * i : 0, rec_f ? rec_f + 4 * i : 0, gp, tr);
   }
   if (groups) { /* the threads' cells, and the records in photon order (the engine's layout, LUMEN_REC_WORDS each) */
     for (auto& G : gparts) {

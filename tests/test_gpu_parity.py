@@ -462,3 +462,66 @@ def test_simulate_truth_rows(toy, built):
     with pytest.raises(ValueError):
         api.simulate(toy, sources.Point(position=(0.0, 0.0, 0.1), n_photons=2.0 * n, lam=400.0), samples=n,
                      truth=TR.Truth())  # fmt: skip
+
+
+def _float64_det(which, toy, solids):
+    if which == "coated":
+        return detectors.coated_panel(precision="float64")
+    return {"toy": toy, "solids": solids}[which].with_precision("float64")
+
+
+@pytest.mark.parametrize("which", ["toy", "solids", "coated"])
+def test_float64_query_and_locate_bit_exact(which, toy, solids, built):
+    """The float64 navigator (lumen_b200_query64 / locate64): every query's integers and float64 t (and the float32
+    normal, widened) are the checker's bit for bit."""
+    det = _float64_det(which, toy, solids)
+    rng = np.random.default_rng(7)
+    n = 20000
+    lo, hi = det.arrays["vol_f64"][0, 12:15], det.arrays["vol_f64"][0, 15:18]
+    o = rng.uniform(lo, hi, (n, 3))
+    d = rng.normal(size=(n, 3))
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    eng = _engine(det)
+    gi, gf = eng.query(o, d)
+    oi, of = oracle.query(det, o, d)
+    gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+    assert gf.dtype == np.float64 and of.dtype == np.float64
+    assert (gi == oi).all(), np.flatnonzero((gi != oi).any(1))[:10]
+    assert (gf.view(np.uint64) == of.view(np.uint64)).all()
+    gv = eng.locate(o).cpu().numpy()
+    assert (gv == oracle.locate(det, o)).all()
+
+
+@pytest.mark.parametrize("which", ["toy", "solids", "coated"])
+def test_float64_photons_bit_exact(which, toy, solids, built):
+    """Photons traced with the float64 navigator and position (the NAV64 instantiation): every record is the
+    checker's, through the coating float32 steps over too."""
+    det = _float64_det(which, toy, solids)
+    pos = {"toy": (0.0, 0.0, 0.1), "solids": (0.05, 0.02, -0.6), "coated": (0.0, 0.0, 0.0)}[which]
+    src = sources.Point(position=pos, n_photons=1.0, lam=420.0)
+    bad, gi, oi, gf, of = _records_match(det, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+def test_float64_tallies_gradients_and_truth(tank, toy, built):
+    """The float64 instantiations with tangents (G = 8) and with truth rows (ANALOG): tallies, Jacobian and analog
+    records are the checker's."""
+    det = tank.with_precision("float64")
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    grads = [det.params_index[k] for k in ("media/Water/absorption", "media/Water/rayleigh")]
+    c = A.controls(grad_tabs=grads, variant=3)  # a wavefront request runs the persistent loop in float64
+    T, O = _tallies(det, src, 1 << 15, controls=c)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+    np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+    det = toy.with_precision("float64")
+    n = 1 << 14
+    src = sources.Point(position=(0.1, 0.0, 0.05), n_photons=float(n), lam_range=(330.0, 480.0))
+    eng = _engine(det)
+    ds = DeviceSource(src, n)
+    c = A.controls(roulette=0.05, flags=A.F_TRUTH)
+    Tt = DeviceTallies(det.n_sensor, 1, 0, 0.0, 1.0, 0).attach_truth(n)
+    eng.trace(KEY, n, source=ds, controls=c, tallies=Tt)
+    Ot, _ = oracle.trace(det, KEY, n, source=src, samples=n, controls=c, truth=True)
+    g = Tt.truth.cpu().numpy()
+    assert (g.view(np.uint32) == Ot.truth.view(np.uint32)).all()
+    np.testing.assert_allclose(Tt.arrival.cpu().numpy(), Ot.arrival, rtol=RTOL, atol=1e-15)
