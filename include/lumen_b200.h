@@ -38,7 +38,9 @@ typedef enum LumenStatus {
 } LumenStatus;
 
 /* ---------------------------------------------------------------------------------------------- array layouts */
-/* Per volume v (0..n_vol-1; index n_vol is the outside), int record of LUMEN_VOL_I int32: */
+/* Per volume v (0..n_vol-1; index n_vol is the outside; then, with meshes, mesh k's pseudo-volume at n_vol + 1 + k and
+   mesh chunk c at LUMEN's CH0 + c, CH0 = n_vol + 1 + n_mesh: their kind is -1, their parent the mesh's mother, their
+   class and order the mesh's, no candidates, no BVH), int record of LUMEN_VOL_I int32: */
 enum {
   LUMEN_VI_KIND = 0,   /* the solid (kind) of the volume; -1 for the outside */
   LUMEN_VI_PARENT = 1, /* the mother volume (n_vol for a top volume; -1 for the outside) */
@@ -118,7 +120,7 @@ enum { LUMEN_JUMP_F = 4, LUMEN_JUMP_I = 8 };
 typedef struct LumenSceneDesc {
   /* geometry (the navigator's arrays, src/lumen/geometry/navigator_build.py:51, csg_build.py:30) */
   int32_t n_vol, n_kind, n_leaf, n_plane, n_prog, n_node, n_item, n_cand;
-  const int32_t* vol_i;   /* host, (n_vol + 1) * LUMEN_VOL_I */
+  const int32_t* vol_i;   /* host, (n_vol + 1 + n_mesh + n_chunk) * LUMEN_VOL_I */
   const float* vol_f;     /* host, n_vol * LUMEN_VOL_F */
   const int32_t* cand;    /* host, n_cand: daughters per volume (and the outside's top volumes) */
   const float* node_f;    /* host, n_node * LUMEN_NODE_F */
@@ -167,7 +169,20 @@ typedef struct LumenSceneDesc {
   const double* node_f64;    /* host, n_node * LUMEN_NODE_F */
   const double* leaf_f64;    /* host, n_leaf * LUMEN_LEAF_F */
   const double* plane_f64;   /* host, n_plane * LUMEN_PLANE_F */
+  /* tessellated meshes (G4TessellatedSolid; src/lumen/geometry/scene.py:33 Mesh, navigator_build.py:266
+     _mesh_chunks): opaque parts of closed triangle surfaces. Triangles (world, each LUMEN_TRI_F: V0, V1, V2 and the
+     unit normal (V1 - V0) x (V2 - V0), outward) in chunks of at most LUMEN_MESH_CHUNK consecutive triangles; each chunk
+     is a BVH item (navigator id CH0 + c) of its mesh's mother. A facet met from either side is an entry into the mesh
+     (navigate.py:303 the facet rule); the mesh's class is that of its pseudo-volume. 0 / null: no mesh. */
+  int32_t n_mesh, n_chunk, n_tri;
+  const float* mesh_tri;     /* host, n_tri * LUMEN_TRI_F */
+  const double* mesh_tri64;  /* host, n_tri * LUMEN_TRI_F: the float64 navigator's (LUMEN_PREC_FLOAT64) */
+  const int32_t* mesh_chunk; /* host, n_chunk * LUMEN_CHUNK_I: first triangle, count, mesh, 0 */
+  const float* chunk_box;    /* host, n_chunk * 6: each chunk's padded world box (lo, hi), its BVH leaf's */
+  const double* chunk_box64; /* host, n_chunk * 6: the same in float64 */
 } LumenSceneDesc;
+
+enum { LUMEN_TRI_F = 12, LUMEN_CHUNK_I = 4, LUMEN_MESH_CHUNK = 8 };
 
 enum { LUMEN_PREC_FLOAT32 = 0, LUMEN_PREC_FLOAT64 = 1 };
 

@@ -65,6 +65,8 @@ class LumenSceneDesc(ctypes.Structure):
         ("clear", c_f32p),
         ("precision", ctypes.c_int32), ("vol_f64", c_f64p), ("node_f64", c_f64p), ("leaf_f64", c_f64p),
         ("plane_f64", c_f64p),
+        ("n_mesh", ctypes.c_int32), ("n_chunk", ctypes.c_int32), ("n_tri", ctypes.c_int32), ("mesh_tri", c_f32p),
+        ("mesh_tri64", c_f64p), ("mesh_chunk", c_i32p), ("chunk_box", c_f32p), ("chunk_box64", c_f64p),
     ]  # fmt: skip
 
 

@@ -44,7 +44,7 @@ struct DScene {
   float reach;
   const int32_t* __restrict__ vol_i;
   const float* __restrict__ vol_f;  // vol_f, node_f, leaf_f, plane_f: float64 data on a float64 scene (nav64)
-  const int32_t* __restrict__ cand;
+  const int32_t* __restrict__ mesh;  // the meshes' block (dnav.cuh: header, chunks, triangle chunks), null: none
   const float* __restrict__ node_f;
   const int32_t* __restrict__ node_i;
   const int32_t* __restrict__ items;

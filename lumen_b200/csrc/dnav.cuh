@@ -716,11 +716,131 @@ L_DEV void d_slab(const A* __restrict__ node_f, int node, const NF* o, const V* 
   *tout = hi_t;
 }
 
+
+// ------------------------------------------------------------------------------------------------- meshes
+// Tessellated meshes (navigate.py:283-332, surface_id.py:120): a mesh chunk (navigator id >= CH0) is visited by the
+// watertight ray-triangle test (Woop, Benthin and Wald, JCGT 2013: the ray's axes sheared so that it runs along +z,
+// each triangle's edge functions in the sheared xy plane) for inside / outside only; t comes from the triangle's
+// plane. The block S.mesh: n_mesh, n_chunk, n_tri, the triangles' offset in the leaf array (elements), SM (the
+// first mesh surface code), CH0, 0, 0; per chunk (first triangle, count, mesh, 0); per triangle its chunk. A triangle
+// is LUMEN_TRI_F values of the navigator's precision: V0, V1, V2, the unit normal.
+constexpr int MESH_HDR = 8;
+constexpr NF N_FACET_BEHIND_BANDS = 0.25f;  // a start behind a facet's plane by at most this many bands is on it
+constexpr NF N_FACET_SHORT_ULPS = 2.0f;     // a mesh hit's t from its plane, this many ulps short of it
+constexpr NF N_MESH_PARALLEL = NK(1e-6);    // a mesh hit's plane is used where |n . d| is above this
+
+L_DEV int m_ch0(const DScene& S) { return S.mesh ? __ldg(S.mesh + 5) : 0x7fffffff; }
+L_DEV int m_sm(const DScene& S) { return S.mesh ? __ldg(S.mesh + 4) : 0x7fffffff; }
+L_DEV const NF* m_tri(const DScene& S, int k) { return NAV_LEAF(S) + __ldg(S.mesh + 3) + (size_t)k * LUMEN_TRI_F; }
+L_DEV NF m_pick(const NF* v, int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+
+struct Shear { int kx, ky, kz; NF sx, sy, sz; };
+// the watertight test's shear of the direction (navigate.py:80 _shear)
+L_DEV Shear d_shear(const NF* dd) {
+  NF a0 = n_abs(dd[0]), a1 = n_abs(dd[1]), a2 = n_abs(dd[2]);
+  int kz = (a0 >= a1 && a0 >= a2) ? 0 : (a1 >= a2 ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1;
+  int ky = kx == 2 ? 0 : kx + 1;
+  NF dz = m_pick(dd, kz);
+  if (dz < 0.0f) { int s = kx; kx = ky; ky = s; }
+  Shear h = {kx, ky, kz, m_pick(dd, kx) / dz, m_pick(dd, ky) / dz, (NF)1.0f / dz};
+  return h;
+}
+
+// whether the ray crosses triangle k, its t from the plane, n . d and the start's height over the plane
+// (navigate.py:283 _crossing)
+L_DEV int d_crossing(const DScene& S, const Ctx& c, const Shear& h, int k, NF* t_k, NF* nd, NF* s0) {
+  const NF* T = m_tri(S, k);
+  NF A[3], B[3], C[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    A[a] = __ldg(T + a) - c.od[a];
+    B[a] = __ldg(T + 3 + a) - c.od[a];
+    C[a] = __ldg(T + 6 + a) - c.od[a];
+  }
+  NF Ax = m_pick(A, h.kx) - h.sx * m_pick(A, h.kz), Ay = m_pick(A, h.ky) - h.sy * m_pick(A, h.kz);
+  NF Bx = m_pick(B, h.kx) - h.sx * m_pick(B, h.kz), By = m_pick(B, h.ky) - h.sy * m_pick(B, h.kz);
+  NF Cx = m_pick(C, h.kx) - h.sx * m_pick(C, h.kz), Cy = m_pick(C, h.ky) - h.sy * m_pick(C, h.kz);
+  NF U = Cx * By - Cy * Bx;
+  NF V = Ax * Cy - Ay * Cx;
+  NF W = Bx * Ay - By * Ax;
+  int inside = (U >= 0.0f && V >= 0.0f && W >= 0.0f) || (U <= 0.0f && V <= 0.0f && W <= 0.0f);
+  NF det = U + V + W;
+  NF N[3] = {__ldg(T + 9), __ldg(T + 10), __ldg(T + 11)};
+  NF w[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) w[a] = (c.od[a] + c.t_lo * c.dd[a]) - __ldg(T + a);
+  *s0 = d_dot(N, w);
+  *nd = d_dot(N, c.dd);
+  *t_k = c.t_lo - *s0 / (*nd != 0.0f ? *nd : (NF)-1.0f);
+  return inside && det != 0.0f;
+}
+
+// the best event after mesh chunk i (navigate.py:320 _mesh_visit, :303 _triangle: the facet rule): the triangle the
+// photon sits on, heading into it, is a zero-length re-hit; else a facet is met entering it (n . d < 0, the start
+// behind its plane within the tolerance) or from clearly behind (the start inside the closed surface): both entries
+L_CALL Best d_mesh_visit(const DScene& S, const Ctx& c, int ch0, int i, Best b) {
+  const int* cr = S.mesh + MESH_HDR + 4 * (i - ch0);
+  const int k0 = __ldg(cr), kn = __ldg(cr + 1);
+  const NF hi_t = d_min(b.t, c.t_bound);
+  const Side& sd = c.sd;
+  int re = sd.known && i == c.last && sd.s < 0.0f && (c.t_lo < b.t || (c.t_lo == b.t && b.own));
+  if (re) {
+    Best nb = {c.t_lo, i, sd.leaf, -1, 1, 0};
+    b = nb;
+  }
+  const Shear h = d_shear(c.dd);
+  const NF tol = N_FACET_BEHIND_BANDS * c.band;
+  for (int q = 0; q < kn; ++q) {
+    NF t_k, nd, s0;
+    int ok = d_crossing(S, c, h, k0 + q, &t_k, &nd, &s0);
+    int front = ok && nd < 0.0f && s0 > -tol && (c.t_lo - t_k <= c.band);
+    int back = ok && nd > 0.0f && s0 < -tol && t_k > c.t_lo;
+    NF t_c = d_max(t_k, c.t_lo);
+    if ((front || back) && t_c < hi_t && (t_c < b.t || (t_c == b.t && b.own))) {
+      Best nb = {t_c, i, k0 + q, -1, t_k <= c.t_lo, 0};
+      b = nb;
+    }
+  }
+  return b;
+}
+
+// a surface code with the mesh codes (surface_id.py:33 srf_decode, :56 srf_pack: a mesh triangle k is SM + 4 k + 2 o
+// + e, its item the triangle's chunk)
+L_DEV Srf d_srf_decode_m(const DScene& S, int s) {
+  const int sm = m_sm(S);
+  if (s < sm) return d_srf_decode(S, s);
+  int km = s - sm;
+  Srf r;
+  r.e = km % 2; km /= 2;
+  r.o = km % 2; km /= 2;
+  r.item = m_ch0(S) + __ldg(S.mesh + MESH_HDR + 4 * __ldg(S.mesh + 1) + km);
+  r.leaf = km;
+  r.face = -1;
+  r.known = 1;
+  return r;
+}
+template <int EXT>
+L_DEV Srf d_decode(const DScene& S, int s) {
+  if constexpr (EXT) return d_srf_decode_m(S, s);
+  else return d_srf_decode(S, s);
+}
+// the winning surface's gradient: a mesh triangle's normal, else the volume's leaf (surface_id.py:67 hit_grad)
+L_DEV void d_hit_grad_m(const DScene& S, int ch0, int item, int leaf, int face, const NF* x, NF* g) {
+  if (item >= ch0) {
+    const NF* T = m_tri(S, leaf > 0 ? leaf : 0);
+    g[0] = __ldg(T + 9); g[1] = __ldg(T + 10); g[2] = __ldg(T + 11);
+  } else {
+    d_hit_grad(S, item, leaf, face, x, g);
+  }
+}
+
 // the next event in volume v: its own exit, then the first entry of every daughter the BVH does not prune. One
 // call site of the visit (the own solid is the first candidate, then the traversal yields one leaf item at a time).
 template <int TORUS>
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   Best b = {N_HUGE, -1, -1, -1, 0, 0};
+  const int ch0 = TORUS ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks among the items
   int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
   NF inv[3];
 #pragma unroll
@@ -784,7 +904,8 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
       }
       if (item < 0) break;
     }
-    b = d_unit_visit<TORUS>(S, c, item, b, is_own);
+    if (TORUS && item >= ch0 && !is_own) b = d_mesh_visit(S, c, ch0, item, b);
+    else b = d_unit_visit<TORUS>(S, c, item, b, is_own);
   }
   return b;
 }
@@ -804,9 +925,10 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   const NF* sn = sn_f;
 #endif
   const int OUT = S.n;
+  const int ch0 = TORUS ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks
   NF xa = d_maxabs3(o);
   int cls0 = d_cls(S, vol);
-  Srf l0 = d_srf_decode(S, last);
+  Srf l0 = d_decode<TORUS>(S, last);
   int kn0 = l0.known;
   NF t_lo = 0.0f;
   int v = vol, last_ = last, done = 0, it = 0;
@@ -820,7 +942,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
     NF band = d_band(xa + n_abs(t_lo));
     int vi = v < OUT - 1 ? v : OUT - 1;
     int has_own = v < OUT;
-    Srf ls = d_srf_decode(S, last_);
+    Srf ls = d_decode<TORUS>(S, last_);
     Side sd = {ls.known, ls.leaf, ls.face, 0.0f, 0};
     if (ls.known) {
       if (sn) {
@@ -829,7 +951,8 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       } else {
         NF x0[3] = {o[0] + t_lo * d[0], o[1] + t_lo * d[1], o[2] + t_lo * d[2]};
         NF g[3];
-        d_hit_grad(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
+        if constexpr (TORUS) d_hit_grad_m(S, ch0, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
+        else d_hit_grad(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
         NF gd = d_dot(g, d);
         sd.s = gd / d_safe_norm(g) * (ls.o ? 1.0f : -1.0f);
         sd.entry = gd < 0.0f;
@@ -852,7 +975,8 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       int up = d_parent(S, v < OUT ? v : OUT);
       int nx0 = go_in ? u_in : up;
       int unit_x = go_in ? u_in : vi;
-      int off = hit && l_in >= 0;
+      const int is_ch = TORUS && go_in && u_in >= ch0;  // a mesh chunk: entered, not relocated (navigate.py:531)
+      int off = hit && l_in >= 0 && !is_ch;
       NF od2[3] = {o[0], o[1], o[2]};
       if (off) {
         NF x[3] = {o[0] + t_c * d[0], o[1] + t_c * d[1], o[2] + t_c * d[2]};
@@ -868,7 +992,8 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
         for (int a = 0; a < 3; ++a) od2[a] = o[a] + m * sg * n_[a];
       }
       NF tr = off ? t_c : t_c + step;
-      if (hit) nxt = d_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
+      if (is_ch) { nxt = OUT + 1 + __ldg(S.mesh + MESH_HDR + 4 * (u_in - ch0) + 2); moved = 0; }
+      else if (hit) nxt = d_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
       else { nxt = nx0; moved = 0; }
     }
     int item = !is_own ? u_in : vi;
@@ -913,10 +1038,29 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   int vis_end = rec_vis;
   int cont = !vis_end && pz_hit && pz_zc >= D_ZSBP;
   int hit = (vis_end || cont) && bt < t_max;
+  if constexpr (TORUS) {  // a mesh hit's t from its plane, short of it (surface_id.py:120 mesh_plane_t)
+    if (hit && !zero && bl >= 0 && bi >= ch0) {
+      const NF* T = m_tri(S, bl);
+      NF nk[3] = {__ldg(T + 9), __ldg(T + 10), __ldg(T + 11)};
+      NF nd = d_dot(nk, d);
+      if (n_abs(nd) > N_MESH_PARALLEL) {
+        NF w0[3], w1[3], w2[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { w0[a] = __ldg(T + a) - o[a]; w1[a] = __ldg(T + 3 + a) - o[a]; w2[a] = __ldg(T + 6 + a) - o[a]; }
+        NF m0 = d_maxabs3(w0), m1 = d_maxabs3(w1), m2 = d_maxabs3(w2);
+        const NF* wn = (m0 <= m1 && m0 <= m2) ? w0 : (m1 <= m2 ? w1 : w2);
+        NF t_pl = d_dot(nk, wn) / nd;
+        NF ulp = N_EPS * (xa + n_abs(bt));
+        NF sh = N_FACET_SHORT_ULPS * ulp / n_abs(nd);
+        bt = d_max(t_pl - sh, 0.0f);
+      }
+    }
+  }
   NF px = bt < N_HUGE ? bt : 0.0f;
   NF xh[3] = {o[0] + px * d[0], o[1] + px * d[1], o[2] + px * d[2]};
   NF g[3];
-  d_hit_grad(S, bi, bl > 0 ? bl : 0, bf, xh, g);
+  if constexpr (TORUS) d_hit_grad_m(S, ch0, bi, bl > 0 ? bl : 0, bf, xh, g);
+  else d_hit_grad(S, bi, bl > 0 ? bl : 0, bf, xh, g);
   NF gn = d_safe_norm(g);
   NF nrm[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
   NF fb[3] = {-d[0], -d[1], -d[2]};
@@ -930,7 +1074,9 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   if (!(hit && bl >= 0)) { nrm[0] = fb[0]; nrm[1] = fb[1]; nrm[2] = fb[2]; }
   NF gd = d_dot(g, d);
   int entry = bi != vb;
-  q.srf = hit ? d_srf_pack(S, bi, bl, bf, entry ? gd < 0.0f : gd > 0.0f, entry) : -1;
+  int o_ = entry ? gd < 0.0f : gd > 0.0f;
+  if (TORUS && bi >= ch0 && bl >= 0) q.srf = hit ? m_sm(S) + 4 * bl + 2 * o_ + entry : -1;  // a mesh triangle
+  else q.srf = hit ? d_srf_pack(S, bi, bl, bf, o_, entry) : -1;
   if (nrm[0] * d[0] + nrm[1] * d[1] + nrm[2] * d[2] > 0.0f) { nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2]; }
   vb = hit ? vb : pz_vend;
   q.t = hit ? bt : t_max;

@@ -15,6 +15,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -189,8 +190,9 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
 // Launch shapes (LumenControls.variant): 0 = 256 threads x 4 blocks per SM (64 registers, 32 warps an SM: the
 // measured best of 128 / 256 threads at 1-8 blocks on the tank: the loop is latency- and divergence-bound, so warps
 // to switch between beat registers), 1 = 128 x 8 (64 registers), 2 = 256 x 3 (85 registers). The autotuner
-// (lumen_b200/autotune.py) picks one per workload. TORUS: the instantiation with the torus leaf code, run for scenes
-// with a torus (shape 0 only); the others are compiled without it, so a scene without one pays nothing for it.
+// (lumen_b200/autotune.py) picks one per workload. TORUS: the extended-geometry instantiation (torus
+// leaves and mesh chunks), run for scenes with either (shape 0 only); the others are compiled without that code, so a
+// scene of quadric and plane leaves pays nothing for it.
 // ANALOG: each photon carries its analog photon and writes its record (truth rows: LUMEN_F_TRUTH; G = 0, shape 0).
 // NAV64: the float64 navigator and position (a LUMEN_PREC_FLOAT64 scene; shape 0, with the torus code).
 template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0, int NAV64 = 0>
@@ -577,8 +579,16 @@ static int check_desc(const LumenSceneDesc* d) {
   if (d->precision != LUMEN_PREC_FLOAT32 && d->precision != LUMEN_PREC_FLOAT64)
     return set_err(LUMEN_ERR_ARG, "scene_create: precision is LUMEN_PREC_FLOAT32 or LUMEN_PREC_FLOAT64");
   if (d->precision == LUMEN_PREC_FLOAT64 && (!d->vol_f64 || !d->leaf_f64 || (d->n_node > 0 && !d->node_f64) ||
-                                             (d->n_plane > 0 && !d->plane_f64)))
+                                             (d->n_plane > 0 && !d->plane_f64) || (d->n_tri > 0 && !d->mesh_tri64)))
     return set_err(LUMEN_ERR_ARG, "scene_create: a float64 scene without its float64 geometry arrays");
+  if (d->n_mesh < 0 || d->n_chunk < 0 || d->n_tri < 0 || (d->n_mesh > 0) != (d->n_chunk > 0) ||
+      (d->n_chunk > 0 && (!d->mesh_tri || !d->mesh_chunk)))
+    return set_err(LUMEN_ERR_ARG, "scene_create: meshes without their triangles or chunks");
+  for (int c = 0; c < d->n_chunk; ++c) {
+    const int32_t* cr = d->mesh_chunk + 4 * (size_t)c;
+    if (cr[0] < 0 || cr[1] < 1 || cr[1] > LUMEN_MESH_CHUNK || cr[0] + cr[1] > d->n_tri || cr[2] < 0 || cr[2] >= d->n_mesh)
+      return set_err(LUMEN_ERR_ARG, "scene_create: a mesh chunk out of range");
+  }
   for (int k = 0; k < d->n_kind; ++k) {
     int nl = d->kind_i[k * LUMEN_KIND_I + 1];
     if (nl < 1 || nl > LUMEN_MAX_LEAVES) return set_err(LUMEN_ERR_SCENE, "scene_create: a solid has too many leaves");
@@ -1112,19 +1122,43 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
       if (np_ + 1 > S.FM) S.FM = np_ + 1;
     }
   }
-  S.SU = d->n_vol + 1;
+  const int ch0 = d->n_vol + 1 + d->n_mesh;  // the first mesh chunk's id; plain items end after the chunks
+  S.SU = ch0 + d->n_chunk;
   S.n_cls = d->n_cls;
   S.n_sensor = d->n_sensor;
   S.reach = d->reach;
   int e = 0;
-  UPLOAD(S.vol_i, d->vol_i, (size_t)(d->n_vol + 1) * LUMEN_VOL_I);
+  UPLOAD(S.vol_i, d->vol_i, (size_t)(ch0 + d->n_chunk) * LUMEN_VOL_I);
   UPLOAD(S.vol_f, d->vol_f, (size_t)d->n_vol * LUMEN_VOL_F);
-  UPLOAD(S.cand, d->cand, (size_t)d->n_cand);
+  S.mesh = nullptr;  // the candidate lists are the checker's: the engine walks the BVH
+  if (d->n_mesh > 0) {  // the meshes' block: header, chunks, each triangle's chunk (dnav.cuh)
+    const long long sm = (long long)S.SU + (long long)d->n_vol * S.LM * S.FM * 4;
+    if (sm + 4LL * d->n_tri >= (1LL << 31)) {
+      for (void* p : sc->allocs) cudaFree(p);
+      delete sc;
+      return set_err(LUMEN_ERR_SCENE, "scene_create: the surface codes of the volumes and mesh triangles exceed int32");
+    }
+    std::vector<int32_t> blk(8 + 4 * (size_t)d->n_chunk + d->n_tri, 0);
+    blk[0] = d->n_mesh; blk[1] = d->n_chunk; blk[2] = d->n_tri; blk[3] = d->n_leaf * LUMEN_LEAF_F;
+    blk[4] = (int32_t)sm; blk[5] = ch0;
+    for (int c = 0; c < d->n_chunk; ++c) {
+      for (int j = 0; j < 4; ++j) blk[8 + 4 * c + j] = d->mesh_chunk[4 * c + j];
+      for (int k = 0; k < d->mesh_chunk[4 * c + 1]; ++k) blk[8 + 4 * (size_t)d->n_chunk + d->mesh_chunk[4 * c] + k] = c;
+    }
+    UPLOAD(S.mesh, blk.data(), blk.size());
+  }
   UPLOAD(S.node_f, d->node_f, (size_t)d->n_node * LUMEN_NODE_F);
   UPLOAD(S.node_i, d->node_i, (size_t)d->n_node * LUMEN_NODE_I);
   UPLOAD(S.items, d->items, (size_t)d->n_item);
   UPLOAD(S.kind_i, d->kind_i, (size_t)d->n_kind * LUMEN_KIND_I);
-  UPLOAD(S.leaf_f, d->leaf_f, (size_t)d->n_leaf * LUMEN_LEAF_F);
+  if (d->n_tri > 0) {  // the meshes' triangles after the leaves (one allocation: the navigator reads both)
+    std::vector<float> lt((size_t)d->n_leaf * LUMEN_LEAF_F + (size_t)d->n_tri * LUMEN_TRI_F);
+    std::copy(d->leaf_f, d->leaf_f + (size_t)d->n_leaf * LUMEN_LEAF_F, lt.begin());
+    std::copy(d->mesh_tri, d->mesh_tri + (size_t)d->n_tri * LUMEN_TRI_F, lt.begin() + (size_t)d->n_leaf * LUMEN_LEAF_F);
+    UPLOAD(S.leaf_f, lt.data(), lt.size());
+  } else {
+    UPLOAD(S.leaf_f, d->leaf_f, (size_t)d->n_leaf * LUMEN_LEAF_F);
+  }
   UPLOAD(S.leaf_i, d->leaf_i, (size_t)d->n_leaf * LUMEN_LEAF_I);
   UPLOAD(S.plane_f, d->plane_f, (size_t)d->n_plane * LUMEN_PLANE_F);
   UPLOAD(S.prog_i, d->prog_i, (size_t)d->n_prog * LUMEN_PROG_I);
@@ -1134,7 +1168,11 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
     const double *vd = nullptr, *nd = nullptr, *ld = nullptr, *pd = nullptr;
     UPLOAD(vd, d->vol_f64, (size_t)d->n_vol * LUMEN_VOL_F);
     UPLOAD(nd, d->node_f64, (size_t)d->n_node * LUMEN_NODE_F);
-    UPLOAD(ld, d->leaf_f64, (size_t)d->n_leaf * LUMEN_LEAF_F);
+    std::vector<double> lt((size_t)d->n_leaf * LUMEN_LEAF_F + (size_t)d->n_tri * LUMEN_TRI_F);
+    std::copy(d->leaf_f64, d->leaf_f64 + (size_t)d->n_leaf * LUMEN_LEAF_F, lt.begin());
+    if (d->n_tri > 0)
+      std::copy(d->mesh_tri64, d->mesh_tri64 + (size_t)d->n_tri * LUMEN_TRI_F, lt.begin() + (size_t)d->n_leaf * LUMEN_LEAF_F);
+    UPLOAD(ld, lt.data(), lt.size());
     UPLOAD(pd, d->plane_f64, (size_t)d->n_plane * LUMEN_PLANE_F);
     S.vol_f = reinterpret_cast<const float*>(vd);
     S.node_f = reinterpret_cast<const float*>(nd);
@@ -1186,7 +1224,7 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
       sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
   }
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
-  sc->has_torus = 0;
+  sc->has_torus = d->n_mesh > 0;  // the extended instantiation: torus leaves or mesh chunks
   for (int l = 0; l < d->n_leaf; ++l) sc->has_torus = sc->has_torus || d->leaf_i[(size_t)l * LUMEN_LEAF_I] == 2;
   for (int m = 0; m < d->n_med; ++m) {
     const int32_t* mr = d->med_i + (size_t)m * LUMEN_MED_I;

@@ -97,6 +97,10 @@ class Detector:
         d.node_f, d.node_i, d.items = fptr(keep["node_f"]), iptr(keep["node_i"]), iptr(keep["items"])
         d.kind_i, d.leaf_f, d.leaf_i = iptr(keep["kind_i"]), fptr(keep["leaf_f"]), iptr(keep["leaf_i"])
         d.plane_f, d.prog_i = fptr(keep["plane_f"]), iptr(keep["prog_i"])
+        if a.get("n_mesh", 0):  # tessellated meshes: triangles, chunks and the chunks' boxes
+            d.n_mesh, d.n_chunk, d.n_tri = a["n_mesh"], len(keep["mesh_chunk"]), len(keep["mesh_tri"])
+            d.mesh_tri, d.mesh_tri64 = fptr(keep["mesh_tri"]), dptr(keep["mesh_tri64"])
+            d.mesh_chunk, d.chunk_box, d.chunk_box64 = iptr(keep["mesh_chunk"]), fptr(keep["chunk_box"]), dptr(keep["chunk_box64"])
         if self.precision == "float64":  # the float64 navigator's arrays
             d.precision = 1
             d.vol_f64, d.node_f64 = dptr(keep["vol_f64"]), dptr(keep["node_f64"])
@@ -141,24 +145,45 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     """
     skins = skins or {}
     sensors = sensors or {}
-    placed = G.flatten(top)
+    sensor_lv = {lv: g for g, lv in sensors.items()}
+    # the volumes, then the meshes (G4TessellatedSolid placements: navigator pseudo-volumes after the outside)
+    flat = G.flatten(top)
+    is_mesh = [isinstance(p.lv.solid, G.Mesh) for p in flat]
+    vol_idx = [i for i, m in enumerate(is_mesh) if not m]
+    mesh_idx = [i for i, m in enumerate(is_mesh) if m]
+    new_of = {old: new for new, old in enumerate(vol_idx)}
+    for i in mesh_idx:
+        p = flat[i]
+        if p.lv.daughters:
+            raise ValueError(f"mesh {p.name!r} has daughters: a mesh holds no point (src/lumen/geometry/navigator_build.py:131)")
+        if p.lv.name in sensor_lv:
+            raise ValueError(f"mesh {p.name!r} is a sensor: a mesh reports only its first hit")
+        if materials[p.lv.material].rindex is not None:
+            raise ValueError(f"mesh {p.name!r}: its material {p.lv.material!r} has a RINDEX; the navigator does not track "
+                             "inside a mesh (an opaque part: no RINDEX, its surfaces reflect or absorb)")
+        if p.parent < 0:
+            raise ValueError("the top volume is a mesh")
+    placed = [dataclasses.replace(flat[i], parent=new_of.get(flat[i].parent, -1)) for i in vol_idx]
+    meshes = [(np.einsum("ij,nkj->nki", flat[i].R, flat[i].lv.solid.tris) + flat[i].t, new_of[flat[i].parent])
+              for i in mesh_idx]  # fmt: skip
+    everything = placed + [flat[i] for i in mesh_idx]
+    n = len(placed)
     names = [p.name for p in placed]
-    by_name = {p.name: i for i, p in enumerate(placed)}
+    by_name = {p.name: i for i, p in enumerate(everything)}
     # optical roles -> classes (the outside is class 0's neighbour: its own class)
-    roles = [set() for _ in placed]
+    roles = [set() for _ in everything]
     for a, b, s in borders:
         roles[by_name[a]].add((s.name, "from"))
         roles[by_name[b]].add((s.name, "to"))
-    sensor_lv = {lv: g for g, lv in sensors.items()}
     keys = []
-    for i, p in enumerate(placed):
+    for i, p in enumerate(everything):
         keys.append((p.lv.name, p.lv.material, tuple(sorted(roles[i])), p.lv.name in skins, p.lv.name in sensor_lv))
     cls_of_key, vol_cls, cls_lv, cls_mat = {}, [], [], []
     for i, k in enumerate(keys):
         if k not in cls_of_key:
             cls_of_key[k] = len(cls_of_key)
-            cls_lv.append(placed[i].lv)
-            cls_mat.append(placed[i].lv.material)
+            cls_lv.append(everything[i].lv)
+            cls_mat.append(everything[i].lv.material)
         vol_cls.append(cls_of_key[k])
     out_cls = len(cls_of_key)
     n_cls = out_cls + 1
@@ -174,7 +199,9 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             s_group.append(g)
             s_pos.append(p.t)
             s_axis.append(p.R[:, 2])
-    nav = G.navigator_arrays(placed, vol_cls, out_cls, vol_sensor, prio)
+    if prio is not None:  # the rule's order given per placement of the walk (and the outside last)
+        prio = np.asarray([prio[i] for i in vol_idx] + [prio[len(flat)]])
+    nav = G.navigator_arrays(placed, vol_cls[:n], out_cls, vol_sensor, prio, meshes=meshes, mesh_cls=vol_cls[n:])
     # media
     pool = O.Pool()
     med_names = sorted(set(cls_mat))
@@ -276,7 +303,7 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             off, k = tab[med_i[m, 2]]
             lam = float(np.min(data[off + k:off + 2 * k].astype(np.float64)))
         media.append((ok, lam))
-    jp = J.prepare(arrays, cls_medium[np.asarray(vol_cls, np.int64)], media)
+    jp = J.prepare(arrays, cls_medium[np.asarray(vol_cls[:n], np.int64)], media)
     arrays.update(jump_f=jp["jump_f"], jump_i=jp["jump_i"], clear=jp["clear"], jump_report=jp["report"])
     st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
     cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}

@@ -125,6 +125,33 @@ def solids_box() -> D.Detector:
                    skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def mesh_tank() -> D.Detector:
+    """Return a 3 m water box holding two opaque tessellated parts (G4TessellatedSolid): a polished steel icosphere
+    (r 0.4 m, 320 triangles, reflectivity 0.8) and a rotated black box mesh (12 triangles), beside a glass orb, and 8
+    sensor discs on two walls."""  # noqa: D205
+    water = O.Material("Water", rindex=1.33, abslength=30.0, rayleigh=10.0)
+    glass = O.Material("Glass", rindex=1.5, abslength=5.0)
+    steel = O.Material("Steel")
+    black = O.Material("Black")
+    cathode = O.Material("Photocathode")
+    box = G.Volume("Box", G.Box(1.5, 1.5, 1.5), "Water")
+    box.place(G.Volume("Ball", G.Mesh(G.icosphere(0.4, 2)), "Steel"), (-0.5, 0.2, 0.1), G.rotation("x", 20.0),
+              name="Ball")  # fmt: skip
+    box.place(G.Volume("Block", G.Mesh(G.box_mesh(0.3, 0.2, 0.25)), "Black"), (0.6, -0.3, -0.2),
+              G.rotation("z", 30.0) @ G.rotation("y", 15.0), name="Block")  # fmt: skip
+    box.place(G.Volume("Orb", G.Orb(0.25), "Glass"), (0.3, 0.6, 0.4), None, name="Orb")
+    pmt = G.Volume("PMT", G.Tube(rmax=0.15, dz=0.01), "Photocathode")
+    for i in range(4):
+        box.place(pmt, (-0.75 + 0.5 * i, 0.0, -1.48), None, name=f"PMT_{i}", copy=i)
+        box.place(pmt, (-0.75 + 0.5 * i, 0.0, 1.48), None, name=f"PMT_{4 + i}", copy=4 + i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    shiny = O.OpticalSurface("Shiny", "dielectric_metal", "polished", reflectivity=0.8)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.6, sigma_alpha=0.2, specularlobe=0.5)
+    borders = [("Box", f"PMT_{i}", surf) for i in range(8)]
+    return D.build(box, {"Water": water, "Glass": glass, "Steel": steel, "Black": black, "Photocathode": cathode},
+                   borders=borders, skins={"Box": wall, "Ball": shiny}, sensors={"pmt": "PMT"})  # fmt: skip
+
+
 def coated_panel(thickness=3e-6, distance=5.0, precision="float32") -> D.Detector:
     """Return a 12 m water box with a 2 x 2 m acrylic backing 20 cm thick at x = ``distance`` m, coated on its front
     face with a TPB-like layer ``thickness`` m thick (rindex 1.6), and 4 photocathode discs (r 0.3 m) behind it: the

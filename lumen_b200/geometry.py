@@ -687,6 +687,95 @@ def gdml_rotation(x=0.0, y=0.0, z=0.0) -> np.ndarray:
 
 
 # ------------------------------------------------------------------------------------------------------ volumes
+class Mesh(Solid):
+    """G4TessellatedSolid (src/lumen/geometry/scene.py:33 Mesh): a closed triangle surface, ``tris`` (n, 3, 3) m in its
+    definition frame, each triangle's normal (V1 - V0) x (V2 - V0) outward. An opaque free-form part: the navigator
+    uses only its first facet hit and that facet's normal (a facet met from either side is an entry into it; no point
+    is inside it), so its material holds no photon (no RINDEX) and it has no daughters and is no sensor."""  # noqa: D205
+
+    def __init__(self, tris):
+        self.tris = np.asarray(tris, float).reshape(-1, 3, 3)
+        if not len(self.tris):
+            raise ValueError("Mesh: no triangles")
+
+    def lower(self):
+        raise ValueError("a Mesh is not a CSG solid: it is placed as triangle chunks (navigator_arrays)")
+
+
+def icosphere(radius: float, subdiv: int = 2) -> np.ndarray:
+    """Return the triangles (n, 3, 3) of a sphere of ``radius`` tessellated from an icosahedron by ``subdiv`` 4-way
+    splits (20 x 4^subdiv triangles, vertices on the sphere), wound so that (V1 - V0) x (V2 - V0) points out."""  # noqa: D205
+    p = (1.0 + math.sqrt(5.0)) / 2.0
+    V = [(-1, p, 0), (1, p, 0), (-1, -p, 0), (1, -p, 0), (0, -1, p), (0, 1, p), (0, -1, -p), (0, 1, -p),
+         (p, 0, -1), (p, 0, 1), (-p, 0, -1), (-p, 0, 1)]  # fmt: skip
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]  # fmt: skip
+    T = np.asarray([[V[i] for i in f] for f in F], np.float64)
+    T /= np.linalg.norm(T, axis=2, keepdims=True)
+    for _ in range(subdiv):
+        a, b, c = T[:, 0], T[:, 1], T[:, 2]
+        ab, bc, ca = [x / np.linalg.norm(x, axis=1, keepdims=True) for x in (a + b, b + c, c + a)]
+        T = np.concatenate([np.stack(s, 1) for s in ((a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca))])
+    n = np.cross(T[:, 1] - T[:, 0], T[:, 2] - T[:, 0])
+    flip = np.einsum("ij,ij->i", n, T.mean(1)) < 0
+    T[flip] = T[flip][:, ::-1]
+    return radius * T
+
+
+def box_mesh(hx: float, hy: float, hz: float) -> np.ndarray:
+    """Return the 12 triangles of a box of half lengths (hx, hy, hz), wound outward."""
+    c = np.array([[sx * hx, sy * hy, sz * hz] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)])
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    T = np.asarray([[c[q[0]], c[q[1]], c[q[2]]] for q in quads] + [[c[q[0]], c[q[2]], c[q[3]]] for q in quads])
+    n = np.cross(T[:, 1] - T[:, 0], T[:, 2] - T[:, 0])
+    flip = np.einsum("ij,ij->i", n, T.mean(1)) < 0
+    T[flip] = T[flip][:, ::-1]
+    return T
+
+
+MESH_CHUNK = 8  # triangles per chunk (one BVH item: src/lumen/geometry/navigator_build.py:46)
+MORTON_BITS = 10  # the chunks' order: triangles sorted along a Morton curve of this many bits per axis
+MESH_PARALLEL = 1e-6  # a mesh hit's t comes from its plane where |n . d| is above this (tolerances.py:135)
+
+
+def morton(c) -> np.ndarray:
+    """Return the Morton codes (MORTON_BITS bits per axis, interleaved z y x from the top bit) of points c (n, 3),
+    quantised in their own bounding box."""  # noqa: D205, D209
+    c = np.asarray(c, np.float64)
+    lo, hi = c.min(0), c.max(0)
+    q = np.clip(((c - lo) / np.maximum(hi - lo, 1e-300) * (1 << MORTON_BITS)).astype(np.int64), 0, (1 << MORTON_BITS) - 1)
+    code = np.zeros(len(c), np.int64)
+    for b in range(MORTON_BITS - 1, -1, -1):
+        for a in range(3):
+            code = (code << 1) | ((q[:, a] >> b) & 1)
+    return code
+
+
+def mesh_chunks(meshes):
+    """Return the chunk arrays of placed meshes [(world triangles (n, 3, 3), mother)]: the triangles Morton-ordered
+    per mesh (its centroids), cut into chunks of MESH_CHUNK consecutive triangles; per triangle V0, V1, V2 and the unit
+    normal (float64), per chunk (first triangle, count, mesh) and its box padded as the reference's chunks
+    (navigator_build.py:346: WORLD_BOX_PAD_REL (|lo| + |hi|) + WORLD_BOX_PAD_ABS)."""  # noqa: D205, D209
+    tri, chunk, mother = [], [], []
+    for m, (T, mo) in enumerate(meshes):
+        T = np.asarray(T, np.float64)[np.argsort(morton(T.mean(1)), kind="stable")]
+        k0 = sum(len(x) for x in tri)
+        for s in range(0, len(T), MESH_CHUNK):
+            chunk.append([k0 + s, min(MESH_CHUNK, len(T) - s), m, 0])
+            mother.append(mo)
+        tri.append(T)
+    V = np.concatenate(tri) if tri else np.zeros((0, 3, 3))
+    nrm = np.cross(V[:, 1] - V[:, 0], V[:, 2] - V[:, 0])
+    nrm = nrm / np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-30)
+    ch = np.asarray(chunk, np.int64).reshape(-1, 4)
+    lo = np.asarray([V[s:s + c].reshape(-1, 3).min(0) for s, c, _, _ in ch]).reshape(-1, 3)
+    hi = np.asarray([V[s:s + c].reshape(-1, 3).max(0) for s, c, _, _ in ch]).reshape(-1, 3)
+    pad = WORLD_BOX_PAD_REL * (np.abs(lo) + np.abs(hi)) + WORLD_BOX_PAD_ABS
+    tri_f = np.concatenate([V.reshape(-1, 9), nrm], 1) if len(V) else np.zeros((0, 12))
+    return dict(tri=tri_f, chunk=ch, mother=np.asarray(mother, np.int64), lo=lo - pad, hi=hi + pad)
+
+
 @dataclass
 class Volume:
     """A logical volume: a solid of a material, with placed daughters."""
@@ -822,6 +911,10 @@ def reach_arrays(arrays) -> dict:
     np.maximum.at(c_hi, comp, hi_w)
     sv = np.flatnonzero(sensor >= 0)
     f_lo, f_hi = lo_w - pad, hi_w + pad
+    cb = np.asarray(arrays.get("chunk_box64", np.zeros((0, 6))), np.float64)
+    if len(cb):  # a mesh chunk's box bounds the query like a sensor's (reach.py:102: a mesh box on the segment)
+        sv = np.concatenate([sv, n + np.arange(len(cb))])
+        f_lo, f_hi = np.concatenate([f_lo, cb[:, :3] - pad]), np.concatenate([f_hi, cb[:, 3:] + pad])
     nodes, _ = _bvh(sv.astype(np.int64), f_lo, f_hi)
     fnode_f = np.asarray([[*nd[0], *nd[1]] for nd in nodes], np.float32).reshape(-1, 6)
     fnode_i = np.asarray([[nd[2], nd[3], 0, 0] for nd in nodes], np.int32).reshape(-1, 4)
@@ -856,8 +949,11 @@ def _node_boxes64(node_i, items, lo, hi) -> np.ndarray:
     return out
 
 
-def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=None) -> dict:
-    """Return the navigator's flat arrays (include/lumen_b200.h layouts) of the placed volumes."""
+def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=None, meshes=(), mesh_cls=()) -> dict:
+    """Return the navigator's flat arrays (include/lumen_b200.h layouts) of the placed volumes and ``meshes``
+    [(world triangles, mother)] of classes ``mesh_cls``: navigator ids 0 .. n - 1 the volumes, n the outside, n + 1 + k
+    mesh k's pseudo-volume, CH0 + c (CH0 = n + 1 + meshes) chunk c, an item of its mesh's mother; every id has a
+    vol_i row (a mesh's and its chunks' carry its class, mother and rank)."""  # noqa: D205, D209
     n = len(placed)
     kinds, kind_of = [], {}
     for p in placed:
@@ -896,12 +992,29 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         vol_f[i, 9:12] = p.t
         vol_f[i, 12:15] = blo
         vol_f[i, 15:18] = bhi
+    nm = len(meshes)
+    mc = mesh_chunks(meshes)
+    nch = len(mc["chunk"])
+    ch0 = n + 1 + nm
     kids = [[] for _ in range(n + 1)]
     for i, p in enumerate(placed):
         kids[p.parent if p.parent >= 0 else n].append(i)
+    for c in range(nch):  # each chunk: an item of its mesh's mother (Geant4: not of the volumes below it)
+        kids[int(mc["mother"][c])].append(ch0 + c)
     prio = np.arange(n + 1) if prio is None else np.asarray(prio)
-    vol_i = np.zeros((n + 1, 10), np.int32)
+    prio = np.concatenate([prio[:n + 1], n + 1 + np.arange(nm)])
+    # boxes per navigator id (the volumes', then zero for the outside and the meshes, then the chunks')
+    lo_w = np.concatenate([lo_w, np.zeros((1 + nm, 3)), mc["lo"]])
+    hi_w = np.concatenate([hi_w, np.zeros((1 + nm, 3)), mc["hi"]])
+    vol_i = np.zeros((ch0 + nch, 10), np.int32)
     cand, node_f, node_i, items = [], [], [], []
+    for v in range(n + 1, ch0 + nch):  # the meshes' and their chunks' rows: class, mother, rank; no solid, no BVH
+        k = v - n - 1 if v < ch0 else int(mc["chunk"][v - ch0, 2])
+        vol_i[v, 0] = -1
+        vol_i[v, 1] = int(meshes[k][1]) if int(meshes[k][1]) >= 0 else n
+        vol_i[v, 2] = mesh_cls[k]
+        vol_i[v, 3] = -1
+        vol_i[v, 4] = prio[n + 1 + k]
     for v in range(n + 1):
         ks = kids[v]
         vol_i[v, 0] = kind_of[id(placed[v].lv.solid)] if v < n else -1
@@ -926,7 +1039,9 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
     for v in range(n + 1):
         if bvh_depth(ni_arr, vol_i[v, 7], vol_i[v, 8]) > MAX_BVH_DEPTH:
             raise ValueError(f"volume {v}: a daughter BVH deeper than {MAX_BVH_DEPTH} levels")
-    allp = np.concatenate([lo_w, hi_w]) if n else np.zeros((1, 3))
+    for v in range(n + 1, ch0 + nch):
+        vol_i[v, 5], vol_i[v, 7], vol_i[v, 8] = len(cand), len(node_f), len(node_f)
+    allp = np.concatenate([lo_w[:n], hi_w[:n], mc["lo"], mc["hi"]]) if n else np.zeros((1, 3))
     reach = float(np.linalg.norm(allp.max(0) - allp.min(0)))
     items_a = np.asarray(items, np.int64)
     return dict(
@@ -940,4 +1055,8 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         leaf_f=np.asarray(leaf_f, np.float32).reshape(-1, 20), leaf_i=np.asarray(leaf_i, np.int32).reshape(-1, 4),
         plane_f=np.asarray(plane_f, np.float32).reshape(-1, 4), prog_i=np.asarray(prog_i, np.int32).reshape(-1, 2),
         reach=reach, names=[p.name for p in placed],
+        # the meshes: triangles (V0, V1, V2, unit normal), chunks (first triangle, count, mesh, 0) and their boxes
+        n_mesh=nm, ch0=ch0, mesh_tri=mc["tri"].astype(np.float32), mesh_tri64=mc["tri"].copy(),
+        mesh_chunk=mc["chunk"].astype(np.int32), chunk_box=np.concatenate([mc["lo"], mc["hi"]], 1).astype(np.float32),
+        chunk_box64=np.concatenate([mc["lo"], mc["hi"]], 1),
     )  # fmt: skip

@@ -90,6 +90,18 @@ def clearance(arrays, lo, h, n, cap) -> np.ndarray:
         for g in range(l0, l0 + nl):
             cv = np.minimum(cv, _leaf_bound(arrays, g, xl))
         out[inside] = np.minimum(out[inside], cv)
+    tri = np.asarray(arrays.get("mesh_tri64", np.zeros((0, 12))), np.float64)
+    for s, c, _, _ in np.asarray(arrays.get("mesh_chunk", np.zeros((0, 4))), np.int64):
+        # a mesh chunk: the distance to its box outside it, to its triangles' planes (a lower bound) inside it
+        T = tri[s:s + c]
+        blo, bhi = T[:, 0:9].reshape(-1, 3).min(0), T[:, 0:9].reshape(-1, 3).max(0)
+        o = np.maximum(np.maximum(blo - x, x - bhi), 0.0)
+        d = np.sqrt(np.sum(o * o, 1))
+        inside = np.flatnonzero(d == 0.0)
+        out = np.minimum(out, np.where(d > 0.0, d, np.inf))
+        if len(inside):
+            pl = np.abs(np.einsum("nki,ki->nk", x[inside, None, :] - T[None, :, 0:3], T[:, 9:12]))
+            out[inside] = np.minimum(out[inside], pl.min(1))
     scale = float(np.max(np.abs(np.concatenate([lo, np.asarray(lo) + h * (n - 1)])))) + float(cap)
     band = G.BAND_ULPS_EPS * scale + G.BAND_FLOOR
     c = np.maximum(out - band, 0.0)

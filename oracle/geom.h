@@ -44,6 +44,7 @@ typedef struct OScene {
   int LM, FM; /* most leaves of a kind, most faces of a leaf (1 + planes) */
   int SU;     /* first face code: a code below it is a plain item */
   int nav64;  /* LUMEN_PREC_FLOAT64: the navigator reads the desc's float64 arrays */
+  int n_chunk, ch0, sm; /* mesh chunks, the first chunk id, the first mesh surface code (INT_MAX: no mesh) */
 } OScene;
 
 /* ------------------------------------------------------------------------------------------- small vector math */
@@ -101,10 +102,14 @@ typedef float NF;
 #define O_NAV_VOL(S) (S)->D->vol_f
 #define O_NAV_LEAF(S) (S)->D->leaf_f
 #define O_NAV_PLANE(S) (S)->D->plane_f
+#define O_NAV_TRI(S) (S)->D->mesh_tri
+#define O_NAV_CBOX(S) (S)->D->chunk_box
 #include "geom_nav.h"
 #undef O_NAV_VOL
 #undef O_NAV_LEAF
 #undef O_NAV_PLANE
+#undef O_NAV_TRI
+#undef O_NAV_CBOX
 }  // namespace onav32
 
 namespace onav64 {
@@ -112,10 +117,14 @@ typedef double NF;
 #define O_NAV_VOL(S) (S)->D->vol_f64
 #define O_NAV_LEAF(S) (S)->D->leaf_f64
 #define O_NAV_PLANE(S) (S)->D->plane_f64
+#define O_NAV_TRI(S) (S)->D->mesh_tri64
+#define O_NAV_CBOX(S) (S)->D->chunk_box64
 #include "geom_nav.h"
 #undef O_NAV_VOL
 #undef O_NAV_LEAF
 #undef O_NAV_PLANE
+#undef O_NAV_TRI
+#undef O_NAV_CBOX
 }  // namespace onav64
 
 typedef OQueryT<float> OQuery;

@@ -690,15 +690,113 @@ static inline OBest o_unit_visit(const OScene* S, const OCtx* c, int i, OBest b,
 
 /* the ray's slab test against volume i's padded world box (bvh.py:258 slab; navigate.py:424 _meets) */
 static inline int o_meets_box(const OScene* S, const OCtx* c, int i, const NF* inv) {
-  const NF* f = o_vfn(S, i);
+  /* a volume's padded world box, or a mesh chunk's (its BVH leaf box) */
+  const NF* lo = i >= S->ch0 ? O_NAV_CBOX(S) + (size_t)6 * (i - S->ch0) : o_vfn(S, i) + LUMEN_VF_LO;
+  const NF* hi = i >= S->ch0 ? lo + 3 : o_vfn(S, i) + LUMEN_VF_HI;
   NF lo_t = -N_HUGE * 10.0f, hi_t = N_HUGE * 10.0f;
   for (int a = 0; a < 3; ++a) {
-    NF ta = (f[LUMEN_VF_LO + a] - c->od[a]) * inv[a];
-    NF tb = (f[LUMEN_VF_HI + a] - c->od[a]) * inv[a];
+    NF ta = (lo[a] - c->od[a]) * inv[a];
+    NF tb = (hi[a] - c->od[a]) * inv[a];
     lo_t = o_max(lo_t, o_min(ta, tb));
     hi_t = o_min(hi_t, o_max(ta, tb));
   }
   return lo_t <= hi_t && hi_t >= c->t_lo && lo_t <= c->t_bound + c->band;
+}
+
+/* ----------------------------------------------------------------------------------------------- meshes */
+/* tessellated meshes (navigate.py:80 _shear, :283 _crossing, :303 _triangle, :320 _mesh_visit; surface_id.py:33,
+   :56, :67, :120): the watertight ray-triangle test (Woop, Benthin and Wald, JCGT 2013) decides inside / outside,
+   t comes from the triangle's plane; a facet met from either side is an entry into the mesh */
+static const NF N_FACET_BEHIND_BANDS = 0.25f;
+static const NF N_FACET_SHORT_ULPS = 2.0f;
+static const NF N_MESH_PARALLEL = NK(1e-6);
+
+static inline const NF* o_tri(const OScene* S, int k) { return O_NAV_TRI(S) + (size_t)k * LUMEN_TRI_F; }
+static inline NF o_pick(const NF* v, int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+/* the chunk holding triangle k (chunks are consecutive triangles, in order) */
+static inline int o_tri_chunk(const OScene* S, int k) {
+  int lo = 0, hi = S->n_chunk - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) / 2;
+    if (S->D->mesh_chunk[4 * mid] <= k) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+typedef struct OShear { int kx, ky, kz; NF sx, sy, sz; } OShear;
+static inline OShear o_shear(const NF* dd) {
+  NF a0 = n_abs(dd[0]), a1 = n_abs(dd[1]), a2 = n_abs(dd[2]);
+  int kz = (a0 >= a1 && a0 >= a2) ? 0 : (a1 >= a2 ? 1 : 2);
+  int kx = (kz + 1) % 3, ky = (kx + 1) % 3;
+  NF dz = o_pick(dd, kz);
+  if (dz < 0.0f) { int s = kx; kx = ky; ky = s; }
+  OShear h = {kx, ky, kz, o_pick(dd, kx) / dz, o_pick(dd, ky) / dz, (NF)1.0f / dz};
+  return h;
+}
+
+static inline int o_crossing(const OScene* S, const OCtx* c, const OShear* h, int k, NF* t_k, NF* nd, NF* s0) {
+  const NF* T = o_tri(S, k);
+  NF A[3], B[3], C[3];
+  for (int a = 0; a < 3; ++a) { A[a] = T[a] - c->od[a]; B[a] = T[3 + a] - c->od[a]; C[a] = T[6 + a] - c->od[a]; }
+  NF Ax = o_pick(A, h->kx) - h->sx * o_pick(A, h->kz), Ay = o_pick(A, h->ky) - h->sy * o_pick(A, h->kz);
+  NF Bx = o_pick(B, h->kx) - h->sx * o_pick(B, h->kz), By = o_pick(B, h->ky) - h->sy * o_pick(B, h->kz);
+  NF Cx = o_pick(C, h->kx) - h->sx * o_pick(C, h->kz), Cy = o_pick(C, h->ky) - h->sy * o_pick(C, h->kz);
+  NF U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+  int inside = (U >= 0.0f && V >= 0.0f && W >= 0.0f) || (U <= 0.0f && V <= 0.0f && W <= 0.0f);
+  NF det = U + V + W;
+  NF w[3];
+  for (int a = 0; a < 3; ++a) w[a] = (c->od[a] + c->t_lo * c->dd[a]) - T[a];
+  *s0 = o_dot(T + 9, w);
+  *nd = o_dot(T + 9, c->dd);
+  *t_k = c->t_lo - *s0 / (*nd != 0.0f ? *nd : (NF)-1.0f);
+  return inside && det != 0.0f;
+}
+
+static inline OBest o_mesh_visit(const OScene* S, const OCtx* c, int i, OBest b) {
+  const int32_t* cr = S->D->mesh_chunk + 4 * (size_t)(i - S->ch0);
+  const int k0 = cr[0], kn = cr[1];
+  const NF hi_t = o_min(b.t, c->t_bound);
+  const OSide* sd = &c->sd;
+  if (sd->known && i == c->last && sd->s < 0.0f && (c->t_lo < b.t || (c->t_lo == b.t && b.own))) {
+    OBest nb = {c->t_lo, i, sd->leaf, -1, 1, 0};
+    b = nb;
+  }
+  const OShear h = o_shear(c->dd);
+  const NF tol = N_FACET_BEHIND_BANDS * c->band;
+  for (int q = 0; q < kn; ++q) {
+    NF t_k, nd, s0;
+    int ok = o_crossing(S, c, &h, k0 + q, &t_k, &nd, &s0);
+    int front = ok && nd < 0.0f && s0 > -tol && (c->t_lo - t_k <= c->band);
+    int back = ok && nd > 0.0f && s0 < -tol && t_k > c->t_lo;
+    NF t_c = o_max(t_k, c->t_lo);
+    if ((front || back) && t_c < hi_t && (t_c < b.t || (t_c == b.t && b.own))) {
+      OBest nb = {t_c, i, k0 + q, -1, t_k <= c->t_lo, 0};
+      b = nb;
+    }
+  }
+  return b;
+}
+
+static inline OSrf o_srf_decode_m(const OScene* S, int s) {
+  if (s < S->sm) return o_srf_decode(S, s);
+  int km = s - S->sm;
+  OSrf r;
+  r.e = km % 2; km /= 2;
+  r.o = km % 2; km /= 2;
+  r.item = S->ch0 + o_tri_chunk(S, km);
+  r.leaf = km;
+  r.face = -1;
+  r.known = 1;
+  return r;
+}
+static inline void o_hit_grad_m(const OScene* S, int item, int leaf, int face, const NF* x, NF* g) {
+  if (item >= S->ch0) {
+    const NF* T = o_tri(S, leaf > 0 ? leaf : 0);
+    g[0] = T[9]; g[1] = T[10]; g[2] = T[11];
+  } else {
+    o_hit_grad(S, item, leaf, face, x, g);
+  }
 }
 
 /* the photon's next event in volume v: its own exit, then the first entry of every daughter whose box the ray meets
@@ -714,7 +812,8 @@ static inline OBest o_enter(const OScene* S, const OCtx* c, int has_own, int vi)
   const int32_t* vr = o_vi(S, c->v);
   for (int k = 0; k < vr[LUMEN_VI_CN]; ++k) {
     int i = S->D->cand[vr[LUMEN_VI_C0] + k];
-    if (o_meets_box(S, c, i, inv)) b = o_unit_visit(S, c, i, b, 0);
+    if (!o_meets_box(S, c, i, inv)) continue;
+    b = i >= S->ch0 ? o_mesh_visit(S, c, i, b) : o_unit_visit(S, c, i, b, 0);
   }
   return b;
 }
@@ -733,7 +832,7 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
   const int OUT = S->n;
   NF xa = o_maxabs3(o);
   int cls0 = o_cls(S, vol);
-  OSrf l0 = o_srf_decode(S, last);
+  OSrf l0 = o_srf_decode_m(S, last);
   int kn0 = l0.known;
   /* the round loop's carry */
   NF t_lo = 0.0f;
@@ -749,7 +848,7 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
     int vi = v < OUT - 1 ? v : OUT - 1;
     int has_own = v < OUT;
     /* _side */
-    OSrf ls = o_srf_decode(S, last_);
+    OSrf ls = o_srf_decode_m(S, last_);
     OSide sd = {ls.known, ls.leaf, ls.face, 0.0f, 0};
     if (ls.known) {
       if (sn) {
@@ -758,7 +857,7 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
       } else {
         NF x0[3] = {o[0] + t_lo * d[0], o[1] + t_lo * d[1], o[2] + t_lo * d[2]};
         NF g[3];
-        o_hit_grad(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
+        o_hit_grad_m(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
         NF gd = o_dot(g, d);
         sd.s = gd / o_safe_norm(g) * (ls.o ? 1.0f : -1.0f);
         sd.entry = gd < 0.0f;
@@ -778,7 +877,8 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
       int up = o_parent(S, v < OUT ? v : OUT);
       int nx0 = go_in ? u_in : up;
       int unit_x = go_in ? u_in : vi;
-      int off = hit && l_in >= 0;
+      const int is_ch = go_in && u_in >= S->ch0; /* a mesh chunk: entered, not relocated (navigate.py:531) */
+      int off = hit && l_in >= 0 && !is_ch;
       NF od2[3] = {o[0], o[1], o[2]};
       if (off) {
         NF x[3] = {o[0] + t_c * d[0], o[1] + t_c * d[1], o[2] + t_c * d[2]};
@@ -793,7 +893,8 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
         for (int a = 0; a < 3; ++a) od2[a] = o[a] + m * sg * n_[a];
       }
       NF tr = off ? t_c : t_c + step;
-      if (hit) nxt = o_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
+      if (is_ch) nxt = OUT + 1 + S->D->mesh_chunk[4 * (size_t)(u_in - S->ch0) + 2], moved = 0;
+      else if (hit) nxt = o_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
       else nxt = nx0, moved = 0;
     }
     int item = !is_own ? u_in : vi;
@@ -838,10 +939,24 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
   int vis_end = rec_vis;
   int cont = !vis_end && pz_hit && pz_zc >= O_ZSBP;
   int hit = (vis_end || cont) && bt < t_max;
+  if (hit && !zero && bl >= 0 && bi >= S->ch0) { /* a mesh hit's t from its plane, short of it (mesh_plane_t) */
+    const NF* T = o_tri(S, bl);
+    NF nd = o_dot(T + 9, d);
+    if (n_abs(nd) > N_MESH_PARALLEL) {
+      NF w0[3], w1[3], w2[3];
+      for (int a = 0; a < 3; ++a) { w0[a] = T[a] - o[a]; w1[a] = T[3 + a] - o[a]; w2[a] = T[6 + a] - o[a]; }
+      NF m0 = o_maxabs3(w0), m1 = o_maxabs3(w1), m2 = o_maxabs3(w2);
+      const NF* wn = (m0 <= m1 && m0 <= m2) ? w0 : (m1 <= m2 ? w1 : w2);
+      NF t_pl = o_dot(T + 9, wn) / nd;
+      NF ulp = N_EPS * (xa + n_abs(bt));
+      NF sh = N_FACET_SHORT_ULPS * ulp / n_abs(nd);
+      bt = o_max(t_pl - sh, 0.0f);
+    }
+  }
   NF px = bt < N_HUGE ? bt : 0.0f;
   NF xh[3] = {o[0] + px * d[0], o[1] + px * d[1], o[2] + px * d[2]};
   NF g[3];
-  o_hit_grad(S, bi, bl > 0 ? bl : 0, bf, xh, g);
+  o_hit_grad_m(S, bi, bl > 0 ? bl : 0, bf, xh, g);
   NF gn = o_safe_norm(g);
   NF nrm[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
   NF fb[3] = {-d[0], -d[1], -d[2]};
@@ -855,7 +970,9 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
   if (!(hit && bl >= 0)) { nrm[0] = fb[0]; nrm[1] = fb[1]; nrm[2] = fb[2]; }
   NF gd = o_dot(g, d);
   int entry = bi != vb;
-  q.srf = hit ? o_srf_pack(S, bi, bl, bf, entry ? gd < 0.0f : gd > 0.0f, entry) : -1;
+  int o_ = entry ? gd < 0.0f : gd > 0.0f;
+  if (bi >= S->ch0 && bl >= 0) q.srf = hit ? S->sm + 4 * bl + 2 * o_ + entry : -1; /* a mesh triangle */
+  else q.srf = hit ? o_srf_pack(S, bi, bl, bf, o_, entry) : -1;
   if (nrm[0] * d[0] + nrm[1] * d[1] + nrm[2] * d[2] > 0.0f) { nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2]; }
   vb = hit ? vb : pz_vend;
   q.t = hit ? bt : t_max;

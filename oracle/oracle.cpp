@@ -914,7 +914,10 @@ static int o_scene(const LumenSceneDesc* D, OScene* S) {
       if (np + 1 > S->FM) S->FM = np + 1;
     }
   }
-  S->SU = D->n_vol + 1;
+  S->n_chunk = D->n_mesh > 0 ? D->n_chunk : 0;
+  S->ch0 = D->n_mesh > 0 ? D->n_vol + 1 + D->n_mesh : 0x7fffffff;
+  S->SU = D->n_vol + 1 + (D->n_mesh > 0 ? D->n_mesh + D->n_chunk : 0);
+  S->sm = D->n_mesh > 0 ? S->SU + D->n_vol * S->LM * S->FM * 4 : 0x7fffffff;
   S->nav64 = D->precision == LUMEN_PREC_FLOAT64;
   if (S->nav64 && (!D->vol_f64 || !D->leaf_f64 || (D->n_plane > 0 && !D->plane_f64))) return LUMEN_ERR_ARG;
   return LUMEN_OK;

@@ -525,3 +525,27 @@ def test_float64_tallies_gradients_and_truth(tank, toy, built):
     g = Tt.truth.cpu().numpy()
     assert (g.view(np.uint32) == Ot.truth.view(np.uint32)).all()
     np.testing.assert_allclose(Tt.arrival.cpu().numpy(), Ot.arrival, rtol=RTOL, atol=1e-15)
+
+
+@pytest.mark.parametrize("prec", ["float32", "float64"])
+def test_mesh_tank_bit_exact(prec, built):
+    """Tessellated meshes (the extended instantiation: chunk items, the watertight test, the facet rule, mesh surface
+    codes): queries, locates and photons reflecting off the steel icosphere are the checker's bit for bit."""
+    det = detectors.mesh_tank().with_precision(prec)
+    dt, ut = (np.float64, np.uint64) if prec == "float64" else (np.float32, np.uint32)
+    rng = np.random.default_rng(11)
+    n = 20000
+    o = rng.uniform(-1.45, 1.45, (n, 3)).astype(dt)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(dt)
+    eng = _engine(det)
+    gi, gf = eng.query(o, d)
+    oi, of = oracle.query(det, o, d)
+    gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+    assert ((oi[:, 2] > det.arrays["n_vol"])).sum() > 500  # rays that enter a mesh
+    assert (gi == oi).all(), np.flatnonzero((gi != oi).any(1))[:10]
+    assert (gf.view(ut) == of.view(ut)).all()
+    assert (eng.locate(o).cpu().numpy() == oracle.locate(det, o)).all()
+    src = sources.Point(position=(0.0, 0.5, -0.6), n_photons=1.0, lam=400.0)
+    bad, gi, oi, gf, of = _records_match(det, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
