@@ -349,9 +349,11 @@ L_DEV int d_inside_kind(const DScene& S, int kind, const NF* x) {
 }
 
 // ----------------------------------------------------------------------------------------- first_change
-struct Scan {
+// NLMAX: the leaves a kind can have (LUMEN_MAX_LEAVES; 1 in the instantiation for scenes of single-leaf solids)
+template <int NLMAX>
+struct ScanT {
   int kind, nl;
-  Iv iv[LUMEN_MAX_LEAVES];
+  Iv iv[NLMAX];
   NF xa, t1;
   int want;
   int has_init, init_known, init_inside;
@@ -361,10 +363,20 @@ struct Scan {
   NF on_tend, hend;
 };
 
-L_DEV NF d_scan_band(const Scan& s, NF t) { return d_band(s.xa + n_abs(t)); }
+using Scan = ScanT<LUMEN_MAX_LEAVES>;
 
-L_DEV int d_mem_at(const DScene& S, const Scan& s, NF t, int use_on) {
+template <int NLMAX>
+L_DEV NF d_scan_band(const ScanT<NLMAX>& s, NF t) { return d_band(s.xa + n_abs(t)); }
+
+template <int NLMAX>
+L_DEV int d_mem_at(const DScene& S, const ScanT<NLMAX>& s, NF t, int use_on) {
   int on = s.has_on && use_on;
+  if constexpr (NLMAX == 1) {  // a single-leaf solid: its program is the leaf itself
+    const Iv& v = s.iv[0];
+    int m = (v.lo0 <= t && t < v.hi0) || (v.lo1 <= t && t < v.hi1);
+    if (on && s.on_leaf == 0 && t < s.hend) m = s.on_inside;
+    return m;
+  }
   return d_program(S, s.kind, [&](int l) {
     const Iv& v = s.iv[l];
     int m = (v.lo0 <= t && t < v.hi0) || (v.lo1 <= t && t < v.hi1);
@@ -373,15 +385,16 @@ L_DEV int d_mem_at(const DScene& S, const Scan& s, NF t, int use_on) {
   });
 }
 
-// TORUS: the instantiation reads torus leaves (scenes without one run the instantiation without their code)
-template <int TORUS>
-L_DEV void d_scan_init(const DScene& S, Scan& s, int kind, const NF* o, const NF* d, NF t1) {
+// TORUS: the geometry instantiation: 1 reads torus leaves and mesh chunks (scenes without either run one without
+// their code), 2 is for scenes whose solids are single quadric / plane leaves, 0 the rest
+template <int TORUS, int NLMAX>
+L_DEV void d_scan_init(const DScene& S, ScanT<NLMAX>& s, int kind, const NF* o, const NF* d, NF t1) {
   s.kind = kind;
   const int32_t* k = S.kind_i + (size_t)kind * LUMEN_KIND_I;
-  s.nl = __ldg(k + 1);
+  s.nl = NLMAX == 1 ? 1 : __ldg(k + 1);
   int l0 = __ldg(k);
-  for (int l = 0; l < s.nl; ++l) {
-    if (TORUS && __ldg(S.leaf_i + (size_t)(l0 + l) * LUMEN_LEAF_I) == 2)
+  for (int l = 0; l < (NLMAX == 1 ? 1 : s.nl); ++l) {
+    if (TORUS == 1 && __ldg(S.leaf_i + (size_t)(l0 + l) * LUMEN_LEAF_I) == 2)
       s.iv[l] = d_torus_iv(NAV_LEAF(S) + (size_t)(l0 + l) * LUMEN_LEAF_F, NF3{o[0], o[1], o[2]},
                            NF3{d[0], d[1], d[2]});
     else
@@ -397,10 +410,11 @@ L_DEV void d_scan_init(const DScene& S, Scan& s, int kind, const NF* o, const NF
 struct First { int hit; NF t; int inside, leaf, face; };
 struct Fc { int hit; NF t; int inside, leaf, face, inside0; First first; };
 
-L_DEV void d_nearest(const Scan& s, NF t_cur, NF* e1o, int* lbo, int* fco, int* eko) {
+template <int NLMAX>
+L_DEV void d_nearest(const ScanT<NLMAX>& s, NF t_cur, NF* e1o, int* lbo, int* fco, int* eko) {
   NF e1 = N_HUGE;
   int lb = -1, fc = -1, ek = 0;
-  for (int l = 0; l < s.nl; ++l) {
+  for (int l = 0; l < (NLMAX == 1 ? 1 : s.nl); ++l) {
     const Iv& v = s.iv[l];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -415,7 +429,8 @@ L_DEV void d_nearest(const Scan& s, NF t_cur, NF* e1o, int* lbo, int* fco, int* 
   *e1o = e1; *lbo = lb; *fco = fc; *eko = ek;
 }
 
-L_DEV Fc d_first_change(const DScene& S, Scan& s, NF t0) {
+template <int NLMAX>
+L_DEV Fc d_first_change(const DScene& S, ScanT<NLMAX>& s, NF t0) {
   NF t_cur = t0;
   int done = 0, now = 0, lb_h = -1, fc_h = -1, now0 = 0, it = 0;
   First fs = {0, N_HUGE, 0, -1, -1};
@@ -665,7 +680,7 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   int kn_i = sd.known && i == c.last;
   NF t_on = c.t_lo + D_K_ON * c.band / d_max(n_abs(sd.s), 1.0f / D_GRAZE);
   int lf_on = kn_i ? sd.leaf : -2;
-  Scan s;
+  ScanT<TORUS == 2 ? 1 : LUMEN_MAX_LEAVES> s;
   d_scan_init<TORUS>(S, s, vI(S, i, LUMEN_VI_KIND), ol, dl, bnd);
   s.want = is_own ? 0 : 1;
   s.has_init = 1; s.init_known = kn_i; s.init_inside = is_own;
@@ -840,7 +855,7 @@ L_DEV void d_hit_grad_m(const DScene& S, int ch0, int item, int leaf, int face, 
 template <int TORUS>
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   Best b = {N_HUGE, -1, -1, -1, 0, 0};
-  const int ch0 = TORUS ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks among the items
+  const int ch0 = TORUS == 1 ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks among the items
   int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
   NF inv[3];
 #pragma unroll
@@ -904,7 +919,7 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
       }
       if (item < 0) break;
     }
-    if (TORUS && item >= ch0 && !is_own) b = d_mesh_visit(S, c, ch0, item, b);
+    if (TORUS == 1 && item >= ch0 && !is_own) b = d_mesh_visit(S, c, ch0, item, b);
     else b = d_unit_visit<TORUS>(S, c, item, b, is_own);
   }
   return b;
@@ -925,10 +940,10 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   const NF* sn = sn_f;
 #endif
   const int OUT = S.n;
-  const int ch0 = TORUS ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks
+  const int ch0 = TORUS == 1 ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks
   NF xa = d_maxabs3(o);
   int cls0 = d_cls(S, vol);
-  Srf l0 = d_decode<TORUS>(S, last);
+  Srf l0 = d_decode<TORUS == 1>(S, last);
   int kn0 = l0.known;
   NF t_lo = 0.0f;
   int v = vol, last_ = last, done = 0, it = 0;
@@ -942,7 +957,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
     NF band = d_band(xa + n_abs(t_lo));
     int vi = v < OUT - 1 ? v : OUT - 1;
     int has_own = v < OUT;
-    Srf ls = d_decode<TORUS>(S, last_);
+    Srf ls = d_decode<TORUS == 1>(S, last_);
     Side sd = {ls.known, ls.leaf, ls.face, 0.0f, 0};
     if (ls.known) {
       if (sn) {
@@ -951,7 +966,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       } else {
         NF x0[3] = {o[0] + t_lo * d[0], o[1] + t_lo * d[1], o[2] + t_lo * d[2]};
         NF g[3];
-        if constexpr (TORUS) d_hit_grad_m(S, ch0, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
+        if constexpr (TORUS == 1) d_hit_grad_m(S, ch0, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
         else d_hit_grad(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
         NF gd = d_dot(g, d);
         sd.s = gd / d_safe_norm(g) * (ls.o ? 1.0f : -1.0f);
@@ -975,7 +990,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       int up = d_parent(S, v < OUT ? v : OUT);
       int nx0 = go_in ? u_in : up;
       int unit_x = go_in ? u_in : vi;
-      const int is_ch = TORUS && go_in && u_in >= ch0;  // a mesh chunk: entered, not relocated (navigate.py:531)
+      const int is_ch = TORUS == 1 && go_in && u_in >= ch0;  // a mesh chunk: entered, not relocated (navigate.py:531)
       int off = hit && l_in >= 0 && !is_ch;
       NF od2[3] = {o[0], o[1], o[2]};
       if (off) {
@@ -1038,7 +1053,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   int vis_end = rec_vis;
   int cont = !vis_end && pz_hit && pz_zc >= D_ZSBP;
   int hit = (vis_end || cont) && bt < t_max;
-  if constexpr (TORUS) {  // a mesh hit's t from its plane, short of it (surface_id.py:120 mesh_plane_t)
+  if constexpr (TORUS == 1) {  // a mesh hit's t from its plane, short of it (surface_id.py:120 mesh_plane_t)
     if (hit && !zero && bl >= 0 && bi >= ch0) {
       const NF* T = m_tri(S, bl);
       NF nk[3] = {__ldg(T + 9), __ldg(T + 10), __ldg(T + 11)};
@@ -1059,7 +1074,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   NF px = bt < N_HUGE ? bt : 0.0f;
   NF xh[3] = {o[0] + px * d[0], o[1] + px * d[1], o[2] + px * d[2]};
   NF g[3];
-  if constexpr (TORUS) d_hit_grad_m(S, ch0, bi, bl > 0 ? bl : 0, bf, xh, g);
+  if constexpr (TORUS == 1) d_hit_grad_m(S, ch0, bi, bl > 0 ? bl : 0, bf, xh, g);
   else d_hit_grad(S, bi, bl > 0 ? bl : 0, bf, xh, g);
   NF gn = d_safe_norm(g);
   NF nrm[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
@@ -1075,7 +1090,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   NF gd = d_dot(g, d);
   int entry = bi != vb;
   int o_ = entry ? gd < 0.0f : gd > 0.0f;
-  if (TORUS && bi >= ch0 && bl >= 0) q.srf = hit ? m_sm(S) + 4 * bl + 2 * o_ + entry : -1;  // a mesh triangle
+  if (TORUS == 1 && bi >= ch0 && bl >= 0) q.srf = hit ? m_sm(S) + 4 * bl + 2 * o_ + entry : -1;  // a mesh triangle
   else q.srf = hit ? d_srf_pack(S, bi, bl, bf, o_, entry) : -1;
   if (nrm[0] * d[0] + nrm[1] * d[1] + nrm[2] * d[2] > 0.0f) { nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2]; }
   vb = hit ? vb : pz_vend;

@@ -49,6 +49,7 @@ struct LumenScene {
   std::vector<int32_t> tab;         // host copy of the (offset, knots) table index
   std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
   int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
+  int single;                          // every solid one quadric / plane leaf: the single-leaf instantiation
   int nav64;                           // LUMEN_PREC_FLOAT64: S's vol_f, node_f, leaf_f, plane_f hold float64 data
   const float* vol_f32;                // the float32 frames (the readout groups' binning reads them in either precision)
 };
@@ -85,6 +86,7 @@ struct Launch {
 // what picks a launch's instantiation, host side: the scene has a torus leaf; the run keeps truth rows
 struct Pick {
   int torus;
+  int single;              // every solid a single quadric / plane leaf
   int analog;
   int nav64;               // the scene's navigator is float64
   const float* vol_f32;    // the scene's float32 frames (the readout binning)
@@ -764,6 +766,7 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   L.n = n;
   L.step_budget = c->step_budget;
   pk.torus = sc->has_torus;
+  pk.single = sc->single;
   pk.nav64 = sc->nav64;
   pk.vol_f32 = sc->vol_f32;
   pk.analog = (c->flags & LUMEN_F_TRUTH) != 0;
@@ -809,6 +812,11 @@ static int launch_trace(const Launch& L, const Pick& pk, int variant, int bps, c
       return pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream) : launch_shape<0, 256, 4, 0, 1>(L, bps, stream);
   }
   if (pk.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream);  // tori: shape 0 whatever the variant
+  if (pk.single) switch (variant) {  // single-leaf solids: the scan of one leaf, no postfix program
+      case 1: return launch_shape<G, 128, 8, 2>(L, bps, stream);
+      case 2: return launch_shape<G, 256, 3, 2>(L, bps, stream);
+      default: return launch_shape<G, 256, 4, 2>(L, bps, stream);
+    }
   switch (variant) {
     case 1: return launch_shape<G, 128, 8, 0>(L, bps, stream);
     case 2: return launch_shape<G, 256, 3, 0>(L, bps, stream);
@@ -1226,6 +1234,9 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
   sc->has_torus = d->n_mesh > 0;  // the extended instantiation: torus leaves or mesh chunks
   for (int l = 0; l < d->n_leaf; ++l) sc->has_torus = sc->has_torus || d->leaf_i[(size_t)l * LUMEN_LEAF_I] == 2;
+  sc->single = !sc->has_torus;  // every kind one leaf (a quadric and / or planes) whose program is that leaf
+  for (int k = 0; k < d->n_kind; ++k)
+    sc->single = sc->single && d->kind_i[(size_t)k * LUMEN_KIND_I + 1] == 1 && d->kind_i[(size_t)k * LUMEN_KIND_I + 3] == 1;
   for (int m = 0; m < d->n_med; ++m) {
     const int32_t* mr = d->med_i + (size_t)m * LUMEN_MED_I;
     if (mr[LUMEN_MI_WLS] >= 0) sc->spectrum_tabs.push_back(mr[LUMEN_MI_WLS_SPEC]);
