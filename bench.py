@@ -39,7 +39,7 @@ L2_FLUSH_BYTES = 256 << 20
 
 # DRAM bytes per photon of k_trace<0,256,4> on the tank workload: ncu's dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch of 2^20 photons (2.556 GB + 3.611 GB), almost all of it local memory; it grows with the photons
-TRAFFIC_PER_PHOTON = (2.556263e9 + 3.611490e9) / 1048576
+TRAFFIC_PER_PHOTON = (2.712409e9 + 3.530416e9) / 1048576
 
 
 def workload_point(seed=12345):
@@ -420,7 +420,7 @@ def main():
                          "traffic": TRAFFIC_PER_PHOTON * n if args.variant == 0 else None, "peak_kind": pk_kind,
                          "algorithmic_bytes": alg,
                          "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-photon launch "
-                                         "of k_trace<0,256,4> on this workload (6.17 GB), scaled by photons"},
+                                         "of k_trace<0,256,4,2,0,0> on this workload (6.24 GB), scaled by photons"},
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             # one launch of the persistent loop per step (the wavefront's rounds are counted by no host-side number)
             "gpu_launches": args.steps if args.variant != 3 else None, "launch_variant": args.variant,
