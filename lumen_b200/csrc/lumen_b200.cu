@@ -852,6 +852,7 @@ static int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, c
   int st = 0;
   for (long long r = 0;; ++r) {
     if (pk.torus) k_wave_query<G, 1><<<grid, 256, 0, stream>>>(L, V);
+    else if (pk.single) k_wave_query<G, 2><<<grid, 256, 0, stream>>>(L, V);
     else k_wave_query<G, 0><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaMemsetAsync(V.live, 0, sizeof(unsigned long long), stream));
     k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
