@@ -152,6 +152,31 @@ def mesh_tank() -> D.Detector:
                    borders=borders, skins={"Box": wall, "Ball": shiny}, sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def overlap_box() -> D.Detector:
+    """Return a 2 m water box with overlapping siblings, resolved as the reference's ownership rule does (one owner per
+    point): an argon-like "Active" box with a glass "Plane" placed after it inside it (proved inside, so ahead of it:
+    the plane owns its region, as a wire plane lying in its active volume), and two partly overlapping glass-like boxes
+    "A" and "B" (A placed first owns the shared part); 4 sensor discs on one wall."""  # noqa: D205
+    water = O.Material("Water", rindex=1.33, abslength=30.0, rayleigh=10.0)
+    active = O.Material("Active", rindex=1.25, abslength=20.0)
+    glass = O.Material("Glass", rindex=1.5, abslength=5.0)
+    acryl = O.Material("Acrylic", rindex=1.45, abslength=5.0)
+    cathode = O.Material("Photocathode")
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "Water")
+    box.place(G.Volume("Active", G.Box(0.5, 0.5, 0.4), "Active"), (0.0, 0.0, 0.45), None, name="Active")
+    box.place(G.Volume("Plane", G.Box(0.02, 0.4, 0.3), "Glass"), (0.1, 0.0, 0.45), G.rotation("z", 10.0), name="Plane")
+    box.place(G.Volume("A", G.Box(0.25, 0.25, 0.2), "Glass"), (-0.2, 0.0, -0.5), None, name="A")
+    box.place(G.Volume("B", G.Tube(rmax=0.25, dz=0.2), "Acrylic"), (0.15, 0.05, -0.5), None, name="B")
+    pmt = G.Volume("PMT", G.Tube(rmax=0.15, dz=0.01), "Photocathode")
+    for i in range(4):
+        box.place(pmt, (-0.6 + 0.4 * i, 0.0, -0.98), None, name=f"PMT_{i}", copy=i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.6, sigma_alpha=0.2, specularlobe=0.5)
+    borders = [("Box", f"PMT_{i}", surf) for i in range(4)]
+    return D.build(box, {"Water": water, "Active": active, "Glass": glass, "Acrylic": acryl, "Photocathode": cathode},
+                   borders=borders, skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
+
+
 def coated_panel(thickness=3e-6, distance=5.0, precision="float32") -> D.Detector:
     """Return a 12 m water box with a 2 x 2 m acrylic backing 20 cm thick at x = ``distance`` m, coated on its front
     face with a TPB-like layer ``thickness`` m thick (rindex 1.6), and 4 photocathode discs (r 0.3 m) behind it: the

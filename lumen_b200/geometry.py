@@ -949,6 +949,181 @@ def _node_boxes64(node_i, items, lo, hi) -> np.ndarray:
     return out
 
 
+def _convex_leaf(low: Lowered) -> bool:
+    """Whether a lowered solid is one convex leaf (planes, and a quadric whose matrix is positive semidefinite)."""
+    if len(low.leaves) != 1 or len(low.program) != 1 or low.leaves[0].torus is not None:
+        return False
+    lf = low.leaves[0]
+    return (not lf.has_q) or float(np.min(np.linalg.eigvalsh(0.5 * (lf.A + lf.A.T)))) >= -1e-12
+
+
+def _leaf_holds(lf: Leaf, x: np.ndarray) -> np.ndarray:
+    """Whether points x (n, 3; the solid's frame) lie in leaf lf (float64)."""
+    ok = np.all((x - lf.og) @ lf.N.T <= lf.H, axis=1) if len(lf.N) else np.ones(len(x), bool)
+    if lf.has_q:
+        y = x - lf.oq
+        ok &= np.einsum("ni,ij,nj->n", y, lf.A, y) + 2.0 * (y @ lf.b) + lf.c <= 0.0
+    return ok
+
+
+def _proved_inside(inner: Placed, outer: Placed, low_in: Lowered, low_out: Lowered, tol: float) -> bool:
+    """Whether ``inner``'s solid is proved to lie inside ``outer``'s: its box shrunk by ``tol`` has every corner in
+    ``outer``'s solid and that solid is one convex leaf (so the corners' hull, the box, is inside it). No sampling: what
+    is not proved is not assumed (src/lumen/geometry/ownership.py:11)."""  # noqa: D205, D209
+    if not _convex_leaf(low_out):
+        return False
+    lo, hi = np.minimum(low_in.lo + tol, low_in.hi - tol), np.maximum(low_in.hi - tol, low_in.lo + tol)
+    c = np.array([[(hi if (k >> a) & 1 else lo)[a] for a in range(3)] for k in range(8)])
+    w = c @ inner.R.T + inner.t
+    return bool(_leaf_holds(low_out.leaves[0], (w - outer.t) @ outer.R).all())
+
+
+def _leaf_interval(lf: Leaf, lo, hi) -> int:
+    """Return leaf lf's membership over the box [lo, hi] (its solid's frame) by interval bounds: -1 out everywhere,
+    1 in everywhere, 0 not proved either way (a torus is never proved)."""
+    if lf.torus is not None:
+        return 0
+    c, r = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    ins = True
+    for nn, hh in zip(lf.N, lf.H, strict=True):  # n . (x - og) <= h: exact bounds of a linear form
+        m, s = float(nn @ (c - lf.og)) - hh, float(np.abs(nn) @ r)
+        if m - s > 0.0:
+            return -1
+        ins = ins and m + s <= 0.0
+    if lf.has_q:  # y^T A y + 2 b . y + c over y in [lo - oq, hi - oq]: interval arithmetic, term by term
+        ylo, yhi = lo - lf.oq, hi - lf.oq
+        fl, fh = float(lf.c), float(lf.c)
+        for i in range(3):
+            for j in range(3):
+                a = float(lf.A[i, j])
+                if a == 0.0:
+                    continue
+                if i == j:
+                    sq = [ylo[i] * ylo[i], yhi[i] * yhi[i]]
+                    pl, ph = (0.0 if ylo[i] <= 0.0 <= yhi[i] else min(sq)), max(sq)
+                else:
+                    pr = [ylo[i] * ylo[j], ylo[i] * yhi[j], yhi[i] * ylo[j], yhi[i] * yhi[j]]
+                    pl, ph = min(pr), max(pr)
+                fl += min(a * pl, a * ph)
+                fh += max(a * pl, a * ph)
+            bl, bh = 2.0 * float(lf.b[i]) * ylo[i], 2.0 * float(lf.b[i]) * yhi[i]
+            fl += min(bl, bh)
+            fh += max(bl, bh)
+        if fl > 0.0:
+            return -1
+        ins = ins and fh <= 0.0
+    return 1 if ins else 0
+
+
+def _solid_interval(low: Lowered, lo, hi) -> int:
+    """Return a lowered solid's membership over the box [lo, hi] (its frame): its program in three-valued logic."""
+    st = []
+    for op, arg in low.program:
+        if op == 0:
+            st.append(_leaf_interval(low.leaves[arg], lo, hi))
+            continue
+        b, a = st.pop(), st.pop()
+        if op == 1:  # union
+            st.append(1 if (a == 1 or b == 1) else (-1 if (a == -1 and b == -1) else 0))
+        elif op == 2:  # intersection
+            st.append(-1 if (a == -1 or b == -1) else (1 if (a == 1 and b == 1) else 0))
+        else:  # subtraction a - b
+            st.append(-1 if (a == -1 or b == 1) else (1 if (a == 1 and b == -1) else 0))
+    return st[-1]
+
+
+def _local_box(p: Placed, lo, hi):
+    """Return the box (in placement p's frame) enclosing the world box [lo, hi]."""
+    c, r = 0.5 * (lo + hi) - p.t, 0.5 * (hi - lo)
+    cl, rl = c @ p.R, r @ np.abs(p.R)
+    return cl - rl, cl + rl
+
+
+def _proved_apart(pa: Placed, pb: Placed, la: Lowered, lb: Lowered, lo, hi, depth: int = 7) -> bool:
+    """Whether solids a and b share no point of the world box [lo, hi] (the overlap of their boxes): every cell of its
+    bisection (down to ``depth`` levels) is proved outside one of them by interval bounds (``relation`` in
+    src/lumen/geometry/ownership.py: interval bounds over bisected boxes, never sampling)."""  # noqa: D205, D209
+    todo = [(np.asarray(lo, float), np.asarray(hi, float), 0)]
+    while todo:
+        clo, chi, dp = todo.pop()
+        if _solid_interval(la, *_local_box(pa, clo, chi)) == -1 or _solid_interval(lb, *_local_box(pb, clo, chi)) == -1:
+            continue
+        if dp >= depth:
+            return False
+        ax = int(np.argmax(chi - clo))
+        mid = 0.5 * (clo[ax] + chi[ax])
+        h1, l2 = chi.copy(), clo.copy()
+        h1[ax], l2[ax] = mid, mid
+        todo += [(clo, h1, dp + 1), (l2, chi, dp + 1)]
+    return True
+
+
+def ownership(placed: list, kinds: list, kind_of: dict, lo_w, hi_w, tol: float):
+    """Return (prio, owners) of the placed volumes (src/lumen/geometry/ownership.py:744 resolve, without protrusion
+    clips): one owner per point, level by level. Among siblings the rule's order puts a volume proved inside a sibling
+    ahead of it, else keeps the placement order; ``prio`` is the depth-first order of the tree with each mother's
+    daughters in that order (lower first). ``owners[v]``: the siblings ahead of v whose world boxes meet v's deeper
+    than the contact tolerance, and those of v's ancestors' siblings ahead of them that meet v (a candidate entered as a
+    daughter: where it holds a point, the point is not v's)."""  # noqa: D205, D209
+    n = len(placed)
+    kids = [[] for _ in range(n + 1)]
+    for i, p in enumerate(placed):
+        kids[p.parent if p.parent >= 0 else n].append(i)
+    low = [kinds[kind_of[id(p.lv.solid)]] for p in placed]
+    lo_w, hi_w = np.asarray(lo_w, np.float64), np.asarray(hi_w, np.float64)
+
+    def meets(a, bs):  # the siblings bs whose boxes meet a's deeper than the contact tolerance
+        bs = np.asarray(bs, np.int64)
+        if not len(bs):
+            return bs
+        d = np.minimum(hi_w[bs], hi_w[a]) - np.maximum(lo_w[bs], lo_w[a])
+        return bs[(d > tol).all(1)]
+
+    linked = {}  # (a, b) -> the solids may share a point (boxes meet, not proved apart)
+
+    def link(a, b):
+        k = (min(a, b), max(a, b))
+        if k not in linked:
+            lo, hi = np.maximum(lo_w[a], lo_w[b]), np.minimum(hi_w[a], hi_w[b])
+            linked[k] = not _proved_apart(placed[a], placed[b], low[a], low[b], lo, hi)
+        return linked[k]
+
+    order_of = {}
+    for ks in kids:
+        n_in = {a: 0 for a in ks}
+        for a in ks:  # how many siblings a is proved inside (only a sibling whose box meets a's can hold it)
+            for b in meets(a, [b for b in ks if b != a]):
+                n_in[a] += _proved_inside(placed[a], placed[int(b)], low[a], low[int(b)], tol)
+        for r, a in enumerate(sorted(ks, key=lambda a: (-n_in[a], a))):
+            order_of[a] = r
+    prio = np.zeros(n + 1, np.int64)
+    count = 0
+
+    def walk(v):
+        nonlocal count
+        for a in sorted(kids[v], key=lambda a: order_of[a]):
+            prio[a] = count
+            count += 1
+            walk(a)
+
+    walk(n)
+    prio[n] = count
+    owners = [[] for _ in range(n)]
+    for ks in kids:
+        for a in ks:
+            for b in meets(a, [b for b in ks if b != a and order_of[b] < order_of[a]]):
+                if link(a, int(b)):
+                    owners[a].append(int(b))
+    for v in range(n):  # below a non-owner: the owners of an ancestor that may meet v too
+        u = placed[v].parent
+        while u >= 0:
+            for b in meets(v, [b for b in owners[u] if b not in owners[v]]):
+                if link(v, int(b)):
+                    owners[v].append(int(b))
+            u = placed[u].parent
+    return prio, owners
+
+
 def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=None, meshes=(), mesh_cls=()) -> dict:
     """Return the navigator's flat arrays (include/lumen_b200.h layouts) of the placed volumes and ``meshes``
     [(world triangles, mother)] of classes ``mesh_cls``: navigator ids 0 .. n - 1 the volumes, n the outside, n + 1 + k
@@ -1001,7 +1176,12 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         kids[p.parent if p.parent >= 0 else n].append(i)
     for c in range(nch):  # each chunk: an item of its mesh's mother (Geant4: not of the volumes below it)
         kids[int(mc["mother"][c])].append(ch0 + c)
-    prio = np.arange(n + 1) if prio is None else np.asarray(prio)
+    scale = float(np.max(np.abs(np.concatenate([lo_w, hi_w])))) if n else 1.0
+    tol = K_ON * (BAND_ULPS_EPS * scale + BAND_FLOOR)  # the contact tolerance: a contact is no overlap
+    own_prio, owners = ownership(placed, kinds, kind_of, lo_w, hi_w, tol)
+    for v in range(n):  # an owner is a candidate of its non-owner (src/lumen/geometry/navigator_build.py:442)
+        kids[v].extend(owners[v])
+    prio = own_prio if prio is None else np.asarray(prio)
     prio = np.concatenate([prio[:n + 1], n + 1 + np.arange(nm)])
     # boxes per navigator id (the volumes', then zero for the outside and the meshes, then the chunks')
     lo_w = np.concatenate([lo_w, np.zeros((1 + nm, 3)), mc["lo"]])
