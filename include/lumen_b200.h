@@ -51,6 +51,9 @@ enum {
   LUMEN_VI_CN = 6,     /* number of candidates */
   LUMEN_VI_NODE0 = 7,  /* first BVH node of the volume's daughter BVH (world frame) */
   LUMEN_VI_NODE1 = 8,  /* one past its last node (NODE0 == NODE1: no daughters) */
+  LUMEN_VI_SIZE = 9,   /* the volumes of its subtree, itself included (the walk is depth first: an ancestor of w is a
+                          v < w < v + size); a candidate that is an ancestor is one the volume reaches out of (a
+                          protrusion clip, src/lumen/geometry/ownership.py:679): its face is an exit */
   LUMEN_VOL_I = 10
 };
 /* Per volume, float record of LUMEN_VOL_F float32: R (3x3 row-major, world = R local + t), t (3), padded world box */

@@ -153,8 +153,17 @@ L_DEV float nav_band(float scale) { return nav32::d_band(scale); }
 L_DEV double nav_band(double scale) { return nav64::d_band(scale); }
 L_DEV float nav_maxabs3(const float* x) { return nav32::d_maxabs3(x); }
 L_DEV double nav_maxabs3(const double* x) { return nav64::d_maxabs3(x); }
-L_DEV int nav_locate(const DScene& S, const float* x) { return nav32::d_locate(S, x); }
-L_DEV int nav_locate(const DScene& S, const double* x) { return nav64::d_locate(S, x); }
+// EXT: the extended instantiation's locate (skips ancestors among the candidates: protrusion clips)
+template <int EXT = 0>
+L_DEV int nav_locate(const DScene& S, const float* x) {
+  if constexpr (EXT) return nav32::d_locate_x(S, x);
+  else return nav32::d_locate(S, x);
+}
+template <int EXT = 0>
+L_DEV int nav_locate(const DScene& S, const double* x) {
+  if constexpr (EXT) return nav64::d_locate_x(S, x);
+  else return nav64::d_locate(S, x);
+}
 template <int TORUS>
 L_DEV QueryT<float> nav_query(const DScene& S, const float* o, const float* d, int vol, float t_max, int last,
                               const float* sn, float s_at) {

@@ -596,6 +596,11 @@ L_DEV void d_point_scan(const DScene& S, int v, const NF* x, NF pad, F visit) {
   }
 }
 
+// whether volume i is an ancestor of volume v (navigate.py:199 is_ancestor: the walk is depth first, a subtree is its
+// root and the LUMEN_VI_SIZE - 1 volumes after it): an ancestor among v's candidates is one v reaches out of, whose
+// face is v's exit (a protrusion clip). Daughters come after v, so for them the first test ends it without a load.
+L_DEV int d_is_anc(const DScene& S, int i, int v) { return i >= 0 && i < v && v < S.n && v < i + vI(S, i, LUMEN_VI_SIZE); }
+
 L_DEV int d_find(const DScene& S, int v, const NF* x) {
   int g = -1;
   d_point_scan(S, v, x, 0.0f, [&](int i) {
@@ -627,6 +632,47 @@ L_CALL int d_settle(const DScene& S, int v, const NF* od, const NF* dd, NF t, in
     int test = !held && v_ < S.n && v_ != crossed;
     int ins = !test || d_ray_holds(S, vi, od, dd, t);
     int f = ins ? d_find_ray(S, v_, od, dd, t, crossed, pad) : -1;
+    int nv = ins ? (f >= 0 ? f : v_) : d_parent(S, v_ < S.n ? v_ : S.n);
+    held = ins && f >= 0;
+    if (f < 0 && ins) break;
+    v_ = nv;
+  }
+  *moved = v_ != v;
+  return v_;
+}
+// the same for the extended instantiation (a scene with protrusion clips): an ancestor among the candidates is one
+// the volume reaches out of, never a volume to descend into
+L_DEV int d_find_x(const DScene& S, int v, const NF* x) {
+  int g = -1;
+  d_point_scan(S, v, x, 0.0f, [&](int i) {
+    if (d_level_wins(S, i, g, -1) && !d_is_anc(S, i, v) && d_holds_point(S, i, x)) g = i;
+  });
+  return g;
+}
+L_CALL int d_locate_x(const DScene& S, const NF* x) {
+  int v = S.n;
+  for (int guard = 0; guard < 64; ++guard) {
+    int f = d_find_x(S, v, x);
+    if (f < 0) return v;
+    v = f;
+  }
+  return v;
+}
+L_DEV int d_find_ray_x(const DScene& S, int v, const NF* od, const NF* dd, NF t, int excl, NF pad) {
+  NF x[3] = {od[0] + t * dd[0], od[1] + t * dd[1], od[2] + t * dd[2]};
+  int g = -1;
+  d_point_scan(S, v, x, pad, [&](int i) {
+    if (d_level_wins(S, i, g, excl) && !d_is_anc(S, i, v) && d_ray_holds(S, i, od, dd, t)) g = i;
+  });
+  return g;
+}
+L_CALL int d_settle_x(const DScene& S, int v, const NF* od, const NF* dd, NF t, int crossed, NF pad, int* moved) {
+  int v_ = v, held = 0;
+  for (int guard = 0; guard < 256; ++guard) {
+    int vi = v_ < S.n - 1 ? v_ : S.n - 1;
+    int test = !held && v_ < S.n && v_ != crossed;
+    int ins = !test || d_ray_holds(S, vi, od, dd, t);
+    int f = ins ? d_find_ray_x(S, v_, od, dd, t, crossed, pad) : -1;
     int nv = ins ? (f >= 0 ? f : v_) : d_parent(S, v_ < S.n ? v_ : S.n);
     held = ins && f >= 0;
     if (f < 0 && ins) break;
@@ -672,6 +718,12 @@ L_DEV int d_entry_wins(const DScene& S, NF t, int item, const Best& b) {
 
 template <int TORUS>
 L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own) {
+  // an ancestor the volume is not proved inside (the extended instantiation): its first exit from a start inside it,
+  // when earlier than every other event (navigate.py:376 _unit_visit, clip)
+  int clip = 0;
+  if constexpr (TORUS == 1) clip = !is_own && d_is_anc(S, i, c.v);
+  const int own = is_own;
+  if constexpr (TORUS == 1) is_own = is_own || clip;
   const Side& sd = c.sd;
   NF bnd = c.t_bound + c.band;
   NF ol[3], dl[3];
@@ -693,7 +745,9 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   int by_s = kn_i && (is_own ? sd.s > 0.0f : sd.s < 0.0f);
   int ins = kn_i ? (is_own ? (sd.s <= 0.0f && h) : sd.s < 0.0f) : (on ? r.first.inside : r.inside0);
   h = h && (is_own || !ins);
+  if constexpr (TORUS == 1) h = h && (!clip || ins);
   int zero = is_own ? !ins : (ins && (i != c.last || kn_i));
+  if constexpr (TORUS == 1) zero = zero && !clip;
   if (zero) {
     lf = by_s ? sd.leaf : (on ? r.first.leaf : -1);
     f = by_s ? sd.face : (on ? r.first.face : -1);
@@ -707,8 +761,9 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   NF te = apart ? r.first.t : (zero ? c.t_lo : (h ? t : N_HUGE));
   int wins = d_entry_wins(S, te, i, b);
   int better = is_own || (!is_own && (zero || h) && wins);
+  if constexpr (TORUS == 1) better = own || (clip && h && te < b.t) || (!is_own && (zero || h) && wins);
   if (better) {
-    Best nb = {te, i, lf, f, zero && !apart, is_own};
+    Best nb = {te, i, lf, f, zero && !apart, own};
     return nb;
   }
   return b;
@@ -985,9 +1040,10 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
     NF step = d_band(xa + n_abs(hit ? t_c : t_lo));
     int nxt = v, moved = 0;
     {
-      int go_in = !is_own;
+      const int clip = TORUS == 1 && !is_own && d_is_anc(S, u_in, v);  // out through an ancestor's face
+      int go_in = !is_own && !clip;
       int uc = u_in < 0 ? 0 : (u_in > OUT - 1 ? OUT - 1 : u_in);
-      int up = d_parent(S, v < OUT ? v : OUT);
+      int up = clip ? d_parent(S, uc) : d_parent(S, v < OUT ? v : OUT);
       int nx0 = go_in ? u_in : up;
       int unit_x = go_in ? u_in : vi;
       const int is_ch = TORUS == 1 && go_in && u_in >= ch0;  // a mesh chunk: entered, not relocated (navigate.py:531)
@@ -1008,7 +1064,10 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       }
       NF tr = off ? t_c : t_c + step;
       if (is_ch) { nxt = OUT + 1 + __ldg(S.mesh + MESH_HDR + 4 * (u_in - ch0) + 2); moved = 0; }
-      else if (hit) nxt = d_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
+      else if (hit) {
+        if constexpr (TORUS == 1) nxt = d_settle_x(S, nx0, od2, d, tr, unit_x, step + step, &moved);
+        else nxt = d_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
+      }
       else { nxt = nx0; moved = 0; }
     }
     int item = !is_own ? u_in : vi;
@@ -1088,7 +1147,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   }
   if (!(hit && bl >= 0)) { nrm[0] = fb[0]; nrm[1] = fb[1]; nrm[2] = fb[2]; }
   NF gd = d_dot(g, d);
-  int entry = bi != vb;
+  int entry = bi != vb && !(TORUS == 1 && d_is_anc(S, bi, vb));  // an ancestor's face reached out of: an exit
   int o_ = entry ? gd < 0.0f : gd > 0.0f;
   if (TORUS == 1 && bi >= ch0 && bl >= 0) q.srf = hit ? m_sm(S) + 4 * bl + 2 * o_ + entry : -1;  // a mesh triangle
   else q.srf = hit ? d_srf_pack(S, bi, bl, bf, o_, entry) : -1;

@@ -181,7 +181,7 @@ using Pre = PreT<float>;
 
 // the step up to its query: the stuck push, the vertex key, the polarisation fill, the media, the free path
 // (step.py:318 _step_context, :245 _recover)
-template <class NF>
+template <int EXT = 0, class NF>
 L_DEV void d_pre(const Run& R, PhotonT<NF>& ph, Key pkey, PreT<NF>& pr) {
   const DScene& S = R.S;
   pr.b0 = nav_band(nav_maxabs3(ph.x));
@@ -190,7 +190,7 @@ L_DEV void d_pre(const Run& R, PhotonT<NF>& ph, Key pkey, PreT<NF>& pr) {
     NF pb = D_PUSH_BANDS * pr.b0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) ph.x[a] = ph.x[a] + pb * ph.d[a];
-    ph.vol = nav_locate(S, ph.x);
+    ph.vol = nav_locate<EXT>(S, ph.x);
     ph.cls = d_cls(S, ph.vol);
     ph.srf = -1;
   }
@@ -675,7 +675,7 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
 template <int G, int TORUS, int ANALOG = 0, class NF = float>
 L_DEV void d_step(const Run& R, PhotonT<NF>& ph, float* dw, Key pkey, Dep& dep, float* dq, Ana& an) {
   PreT<NF> pr;
-  d_pre(R, ph, pkey, pr);
+  d_pre<TORUS == 1>(R, ph, pkey, pr);
   QueryT<NF> q = d_step_query<TORUS>(R, ph, pr);
   d_post<G, ANALOG>(R, ph, dw, pr, q, dep, dq, an);
 }
@@ -888,7 +888,7 @@ L_DEV void d_rows_row(const LumenRows& rows, int64_t i, Row& r) {
   r.event = rows.event ? __ldg(rows.event + i) : 0;
 }
 
-template <class NF>
+template <int EXT = 0, class NF>
 L_DEV void d_start(const DScene& S, const Row& r, PhotonT<NF>& ph) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) { ph.x[a] = r.x[a]; ph.d[a] = r.d[a]; ph.er[a] = r.er[a]; ph.ei[a] = r.ei[a]; ph.sn[a] = 0.0f; }
@@ -898,7 +898,7 @@ L_DEV void d_start(const DScene& S, const Row& r, PhotonT<NF>& ph) {
   ph.wr = 1.0f;
   ph.alive = 1;
   ph.vertex = 0;
-  ph.vol = nav_locate(S, ph.x);
+  ph.vol = nav_locate<EXT>(S, ph.x);
   ph.cls = d_cls(S, ph.vol);
   ph.srf = -1;
   ph.nz = 0;

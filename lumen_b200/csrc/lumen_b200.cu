@@ -50,6 +50,7 @@ struct LumenScene {
   std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
   int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
   int single;                          // every solid one quadric / plane leaf: the single-leaf instantiation
+  int clip;                            // a volume has an ancestor among its candidates (a protrusion clip)
   int nav64;                           // LUMEN_PREC_FLOAT64: S's vol_f, node_f, leaf_f, plane_f hold float64 data
   const float* vol_f32;                // the float32 frames (the readout groups' binning reads them in either precision)
 };
@@ -87,6 +88,7 @@ struct Launch {
 struct Pick {
   int torus;
   int single;              // every solid a single quadric / plane leaf
+  int clip;                // a protrusion clip (the wavefront's fill locates without the extended rule)
   int analog;
   int nav64;               // the scene's navigator is float64
   const float* vol_f32;    // the scene's float32 frames (the readout binning)
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
         if (g < (unsigned long long)L.n) {
           Row r;
           get_row(L, (int64_t)g, r);
-          d_start(L.R.S, r, ph);
+          d_start<TORUS == 1>(L.R.S, r, ph);
           pkey = fold_in(L.key, (uint32_t)(L.first_id + (int64_t)g));
           w0 = (double)r.w0;
           ev = r.event;
@@ -372,7 +374,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   wv_ld(V.ph, V.W, i, ph);
   wv_ld(V.ex, V.W, i, ex);
   Pre pr;
-  d_pre(L.R, ph, ex.pkey, pr);
+  d_pre<TORUS == 1>(L.R, ph, ex.pkey, pr);
   Query q = d_step_query<TORUS>(L.R, ph, pr);
   wv_st(V.ph, V.W, i, ph);
   wv_st(V.pre, V.W, i, pr);
@@ -502,7 +504,7 @@ __global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
   Row r;
   get_row(L, i, r);
   PhotonT<typename NavOf<NAV64>::F> ph;
-  d_start(L.R.S, r, ph);
+  d_start<1>(L.R.S, r, ph);
   Key pkey = fold_in(L.key, (uint32_t)(L.first_id + i));
   float dw[1], dq[1];
   int n_dep = 0, first_sensor = -1;
@@ -537,7 +539,7 @@ __global__ void k_query(DScene S, const NF* ray, const int32_t* vol, const int32
   NF o[3] = {ray[6 * i], ray[6 * i + 1], ray[6 * i + 2]};
   NF d[3] = {ray[6 * i + 3], ray[6 * i + 4], ray[6 * i + 5]};
   int known = vol[i] >= 0 && vol[i] <= S.n;
-  int v = known ? vol[i] : nav_locate(S, o);
+  int v = known ? vol[i] : nav_locate<1>(S, o);
   int last = known ? srf[i] : -1;
   QueryT<NF> q = nav_query<1>(S, o, d, v, t_max, last, nullptr, sizeof(NF) == 4 ? (NF)D_HUGE : (NF)1e30);
   int32_t* oi = out_i + 8 * i;
@@ -553,7 +555,7 @@ __global__ void k_locate(DScene S, const NF* pts, int64_t n, int32_t* vol) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   NF x[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
-  vol[i] = nav_locate(S, x);
+  vol[i] = nav_locate<1>(S, x);
 }
 
 // ------------------------------------------------------------------------------------------- host helpers
@@ -767,6 +769,7 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   L.step_budget = c->step_budget;
   pk.torus = sc->has_torus;
   pk.single = sc->single;
+  pk.clip = sc->clip;
   pk.nav64 = sc->nav64;
   pk.vol_f32 = sc->vol_f32;
   pk.analog = (c->flags & LUMEN_F_TRUTH) != 0;
@@ -929,7 +932,7 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
     L.truth = out->truth;
     if (variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;
   }
-  if (pk.nav64 && variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;  // the wavefront's slots hold float32 positions
+  if ((pk.nav64 || pk.clip) && variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;  // the wavefront's slots hold float32 positions
   T.grads = grads;
   // scratch: the photon counter, the abort flag, the steps used, the wavefront's live slots and the record count (one
   // small allocation per call)
@@ -1235,6 +1238,13 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
   sc->has_torus = d->n_mesh > 0;  // the extended instantiation: torus leaves or mesh chunks
   for (int l = 0; l < d->n_leaf; ++l) sc->has_torus = sc->has_torus || d->leaf_i[(size_t)l * LUMEN_LEAF_I] == 2;
+  for (int v = 0; v < d->n_vol && !sc->has_torus; ++v) {  // a protrusion clip: the extended instantiation
+    const int32_t* vr = d->vol_i + (size_t)v * LUMEN_VOL_I;
+    for (int k = 0; k < vr[LUMEN_VI_CN]; ++k) {
+      int i = d->cand[vr[LUMEN_VI_C0] + k];
+      if (i >= 0 && i < v && v < i + d->vol_i[(size_t)i * LUMEN_VOL_I + LUMEN_VI_SIZE]) sc->has_torus = sc->clip = 1;
+    }
+  }
   sc->single = !sc->has_torus;  // every kind one leaf (a quadric and / or planes) whose program is that leaf
   for (int k = 0; k < d->n_kind; ++k)
     sc->single = sc->single && d->kind_i[(size_t)k * LUMEN_KIND_I + 1] == 1 && d->kind_i[(size_t)k * LUMEN_KIND_I + 3] == 1;

@@ -177,6 +177,28 @@ def overlap_box() -> D.Detector:
                    borders=borders, skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def protrusion_box() -> D.Detector:
+    """Return a 2 m water box holding an acrylic block with a glass rod placed in it that sticks out through the
+    block's top face (the reference's protrusion: the rod holds only what lies inside the block; a photon in the rod
+    leaves it at the block's face), and 4 sensor discs above."""  # noqa: D205
+    water = O.Material("Water", rindex=1.33, abslength=30.0, rayleigh=10.0)
+    acryl = O.Material("Acrylic", rindex=1.45, abslength=5.0)
+    glass = O.Material("Glass", rindex=1.6, abslength=5.0)
+    cathode = O.Material("Photocathode")
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "Water")
+    block = G.Volume("Block", G.Box(0.4, 0.4, 0.3), "Acrylic")
+    block.place(G.Volume("Rod", G.Tube(rmax=0.08, dz=0.25), "Glass"), (0.1, -0.05, 0.2), None, name="Rod")
+    box.place(block, (0.0, 0.0, -0.2), None, name="Block")
+    pmt = G.Volume("PMT", G.Tube(rmax=0.15, dz=0.01), "Photocathode")
+    for i in range(4):
+        box.place(pmt, (-0.6 + 0.4 * i, 0.0, 0.98), None, name=f"PMT_{i}", copy=i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.6, sigma_alpha=0.2, specularlobe=0.5)
+    borders = [("Box", f"PMT_{i}", surf) for i in range(4)]
+    return D.build(box, {"Water": water, "Acrylic": acryl, "Glass": glass, "Photocathode": cathode}, borders=borders,
+                   skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
+
+
 def coated_panel(thickness=3e-6, distance=5.0, precision="float32") -> D.Detector:
     """Return a 12 m water box with a 2 x 2 m acrylic backing 20 cm thick at x = ``distance`` m, coated on its front
     face with a TPB-like layer ``thickness`` m thick (rindex 1.6), and 4 photocathode discs (r 0.3 m) behind it: the

@@ -1058,6 +1058,48 @@ def _proved_apart(pa: Placed, pb: Placed, la: Lowered, lb: Lowered, lo, hi, dept
     return True
 
 
+def _world_box(p: Placed, lo, hi):
+    """Return the world box enclosing the box [lo, hi] of placement p's frame."""
+    c, r = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    return p.R @ c + p.t - np.abs(p.R) @ r, p.R @ c + p.t + np.abs(p.R) @ r
+
+
+def _proved_within(pv: Placed, pm: Placed, lv: Lowered, lm: Lowered, tol: float, depth: int = 7) -> bool:
+    """Whether solid v (its box shrunk by ``tol``) lies inside solid m: the corner proof for a convex m, else every
+    cell of a bisection of v's box is proved outside v or inside m by interval bounds (src/lumen/geometry/ownership.py
+    :679 _clips: the unit's box shrunk by the contact tolerance, then the containment proof)."""  # noqa: D205, D209
+    if _proved_inside(pv, pm, lv, lm, tol):
+        return True
+    lo, hi = np.minimum(lv.lo + tol, lv.hi - tol), np.maximum(lv.hi - tol, lv.lo + tol)
+    todo = [(lo, hi, 0)]
+    while todo:
+        clo, chi, dp = todo.pop()
+        if _solid_interval(lv, clo, chi) == -1 or _solid_interval(lm, *_local_box(pm, *_world_box(pv, clo, chi))) == 1:
+            continue
+        if dp >= depth:
+            return False
+        ax = int(np.argmax(chi - clo))
+        mid = 0.5 * (clo[ax] + chi[ax])
+        h1, l2 = chi.copy(), clo.copy()
+        h1[ax], l2[ax] = mid, mid
+        todo += [(clo, h1, dp + 1), (l2, chi, dp + 1)]
+    return True
+
+
+def clips_of(placed: list, kinds: list, kind_of: dict, tol: float) -> list:
+    """Return per volume the ancestors it is not proved to lie inside (src/lumen/geometry/ownership.py:679 _clips):
+    its mother and those of its mother's clips, each a candidate whose face is the volume's exit."""  # noqa: D205, D209
+    low = [kinds[kind_of[id(p.lv.solid)]] for p in placed]
+    clips = [[] for _ in placed]
+    for v, p in enumerate(placed):  # parents first (the walk's order)
+        if p.parent < 0:
+            continue
+        for m in [p.parent, *clips[p.parent]]:
+            if not _proved_within(p, placed[m], low[v], low[m], tol):
+                clips[v].append(m)
+    return clips
+
+
 def ownership(placed: list, kinds: list, kind_of: dict, lo_w, hi_w, tol: float):
     """Return (prio, owners) of the placed volumes (src/lumen/geometry/ownership.py:744 resolve, without protrusion
     clips): one owner per point, level by level. Among siblings the rule's order puts a volume proved inside a sibling
@@ -1178,9 +1220,15 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         kids[int(mc["mother"][c])].append(ch0 + c)
     scale = float(np.max(np.abs(np.concatenate([lo_w, hi_w])))) if n else 1.0
     tol = K_ON * (BAND_ULPS_EPS * scale + BAND_FLOOR)  # the contact tolerance: a contact is no overlap
+    size = np.ones(n, np.int64)
+    for v in range(n - 1, -1, -1):  # the walk is depth first: a subtree is its root and the size - 1 volumes after it
+        if placed[v].parent >= 0:
+            size[placed[v].parent] += size[v]
     own_prio, owners = ownership(placed, kinds, kind_of, lo_w, hi_w, tol)
-    for v in range(n):  # an owner is a candidate of its non-owner (src/lumen/geometry/navigator_build.py:442)
-        kids[v].extend(owners[v])
+    clips = clips_of(placed, kinds, kind_of, tol)
+    for v in range(n):  # an owner is a candidate of its non-owner, an ancestor v reaches out of too (its face an
+        kids[v].extend(owners[v])  # exit: src/lumen/geometry/navigator_build.py:442)
+        kids[v].extend(clips[v])
     prio = own_prio if prio is None else np.asarray(prio)
     prio = np.concatenate([prio[:n + 1], n + 1 + np.arange(nm)])
     # boxes per navigator id (the volumes', then zero for the outside and the meshes, then the chunks')
@@ -1203,6 +1251,7 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         vol_i[v, 3] = vol_sensor[v] if v < n else -1
         vol_i[v, 4] = prio[v]
         vol_i[v, 5], vol_i[v, 6] = len(cand), len(ks)
+        vol_i[v, 9] = size[v] if v < n else 1  # the volumes of its subtree (an ancestor of w: v < w < v + size)
         cand.extend(ks)
         # the daughters' BVH, in the float32 boxes the engine reads
         lo32 = lo_w.astype(np.float32).astype(np.float64)

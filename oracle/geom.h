@@ -70,6 +70,10 @@ static inline const int32_t* o_li(const OScene* S, int g) { return S->D->leaf_i 
 static inline const float* o_pl(const OScene* S, int q) { return S->D->plane_f + (size_t)q * LUMEN_PLANE_F; }
 static inline int o_cls(const OScene* S, int v) { return o_vi(S, v)[LUMEN_VI_CLS]; }
 static inline int o_parent(const OScene* S, int v) { return o_vi(S, v)[LUMEN_VI_PARENT]; }
+/* whether volume i is an ancestor of volume v (navigate.py:199 is_ancestor; the walk is depth first) */
+static inline int o_is_anc(const OScene* S, int i, int v) {
+  return i >= 0 && i < v && v < S->n && v < i + o_vi(S, i)[LUMEN_VI_SIZE];
+}
 /* rank of a candidate: minus its place in the rule's order (navigate.py:208) */
 static inline int o_rank(const OScene* S, int i) { return i >= 0 ? -o_vi(S, i)[LUMEN_VI_PRIO] : 0; }
 

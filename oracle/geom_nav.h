@@ -566,7 +566,7 @@ static inline int o_find(const OScene* S, int v, const NF* x) {
   for (int k = 0; k < vi[LUMEN_VI_CN]; ++k) {
     int i = S->D->cand[vi[LUMEN_VI_C0] + k];
     if (!o_box_holds(S, i, x, 0.0f)) continue;
-    if (o_level_wins(S, i, g, -1) && o_holds_point(S, i, x)) g = i;
+    if (o_level_wins(S, i, g, -1) && !o_is_anc(S, i, v) && o_holds_point(S, i, x)) g = i;
   }
   return g;
 }
@@ -587,7 +587,7 @@ static inline int o_find_ray(const OScene* S, int v, const NF* od, const NF* dd,
   for (int k = 0; k < vi[LUMEN_VI_CN]; ++k) {
     int i = S->D->cand[vi[LUMEN_VI_C0] + k];
     if (!o_box_holds(S, i, x, pad)) continue;
-    if (o_level_wins(S, i, g, excl) && o_ray_holds(S, i, od, dd, t)) g = i;
+    if (o_level_wins(S, i, g, excl) && !o_is_anc(S, i, v) && o_ray_holds(S, i, od, dd, t)) g = i;
   }
   return g;
 }
@@ -646,6 +646,11 @@ static inline int o_entry_wins(const OScene* S, NF t, int item, const OBest* b) 
 
 /* the best event after volume i: own its first exit, a daughter its first entry (navigate.py:357-416) */
 static inline OBest o_unit_visit(const OScene* S, const OCtx* c, int i, OBest b, int is_own) {
+  /* an ancestor the volume is not proved inside (a protrusion clip): its first exit from a start inside it, when
+     earlier than every other event (navigate.py:376 _unit_visit) */
+  const int clip = !is_own && o_is_anc(S, i, c->v);
+  const int own = is_own;
+  is_own = is_own || clip;
   const OSide* sd = &c->sd;
   NF bnd = c->t_bound + c->band; /* the scan's window: the query's bound (order-independent) */
   NF ol[3], dl[3];
@@ -666,8 +671,8 @@ static inline OBest o_unit_visit(const OScene* S, const OCtx* c, int i, OBest b,
   int on = o_on_face(S, c, i, &r.first, kn_i);
   int by_s = kn_i && (is_own ? sd->s > 0.0f : sd->s < 0.0f);
   int ins = kn_i ? (is_own ? (sd->s <= 0.0f && h) : sd->s < 0.0f) : (on ? r.first.inside : r.inside0);
-  h = h && (is_own || !ins);
-  int zero = is_own ? !ins : (ins && (i != c->last || kn_i));
+  h = h && (is_own || !ins) && (!clip || ins);
+  int zero = is_own ? (!ins && !clip) : (ins && (i != c->last || kn_i));
   if (zero) {
     lf = by_s ? sd->leaf : (on ? r.first.leaf : -1);
     f = by_s ? sd->face : (on ? r.first.face : -1);
@@ -680,9 +685,9 @@ static inline OBest o_unit_visit(const OScene* S, const OCtx* c, int i, OBest b,
   }
   NF te = apart ? r.first.t : (zero ? c->t_lo : (h ? t : N_HUGE));
   int wins = o_entry_wins(S, te, i, &b);
-  int better = is_own || (!is_own && (zero || h) && wins);
+  int better = own || (clip && h && te < b.t) || (!is_own && (zero || h) && wins);
   if (better) {
-    OBest nb = {te, i, lf, f, zero && !apart, is_own};
+    OBest nb = {te, i, lf, f, zero && !apart, own};
     return nb;
   }
   return b;
@@ -872,9 +877,10 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
     /* _next_volume */
     int nxt = v, moved = 0;
     {
-      int go_in = !is_own;
+      const int clip = !is_own && o_is_anc(S, u_in, v); /* out through an ancestor's face */
+      int go_in = !is_own && !clip;
       int uc = u_in < 0 ? 0 : (u_in > OUT - 1 ? OUT - 1 : u_in);
-      int up = o_parent(S, v < OUT ? v : OUT);
+      int up = clip ? o_parent(S, uc) : o_parent(S, v < OUT ? v : OUT);
       int nx0 = go_in ? u_in : up;
       int unit_x = go_in ? u_in : vi;
       const int is_ch = go_in && u_in >= S->ch0; /* a mesh chunk: entered, not relocated (navigate.py:531) */
@@ -969,7 +975,7 @@ static inline OQuery o_query(const OScene* S, const NF* o, const NF* d, int vol,
   }
   if (!(hit && bl >= 0)) { nrm[0] = fb[0]; nrm[1] = fb[1]; nrm[2] = fb[2]; }
   NF gd = o_dot(g, d);
-  int entry = bi != vb;
+  int entry = bi != vb && !o_is_anc(S, bi, vb); /* an ancestor's face reached out of: an exit */
   int o_ = entry ? gd < 0.0f : gd > 0.0f;
   if (bi >= S->ch0 && bl >= 0) q.srf = hit ? S->sm + 4 * bl + 2 * o_ + entry : -1; /* a mesh triangle */
   else q.srf = hit ? o_srf_pack(S, bi, bl, bf, o_, entry) : -1;

@@ -551,10 +551,12 @@ def test_mesh_tank_bit_exact(prec, built):
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
 
 
-def test_overlapping_siblings_bit_exact(built):
+@pytest.mark.parametrize("which", ["overlap", "protrusion"])
+def test_overlapping_siblings_bit_exact(which, built):
     """Overlapping siblings resolved by the ownership rule (an owner a candidate entered as a daughter, the rule's
-    order in every locate): queries, locates and photons on the overlap box are the checker's bit for bit."""
-    det = detectors.overlap_box()
+    order in every locate) and a daughter sticking out of its mother (the mother a candidate whose face is an exit,
+    in the extended instantiation): queries, locates and photons are the checker's bit for bit."""
+    det = detectors.overlap_box() if which == "overlap" else detectors.protrusion_box()
     rng = np.random.default_rng(13)
     n = 20000
     o = rng.uniform(-0.99, 0.99, (n, 3)).astype(np.float32)

@@ -77,3 +77,28 @@ def test_photons_conserve_their_weight(det):
                      controls=A.controls())[0]  # fmt: skip
     assert abs(T.health[:10].sum() - T.health[10]) < 1e-6 * T.health[10]
     assert T.arrival[0].sum() > 0
+
+
+def test_a_protruding_daughter_is_clipped_by_its_mother():
+    """A rod placed in a block and sticking out of its top face (src/lumen/geometry/ownership.py:679 clips): the block
+    is a candidate of the rod whose face is its exit; the part outside the block is the water's."""
+    det = detectors.protrusion_box()
+    ib, ir, iw = _ids(det, "Block", "Rod", "Box")
+    vi = det.arrays["vol_i"]
+    cand = det.arrays["cand"]
+    assert ib in cand[vi[ir, 5]:vi[ir, 5] + vi[ir, 6]]  # the clip
+    assert vi[ib, 9] == 2 and vi[ir, 9] == 1  # the subtree sizes
+    rng = np.random.default_rng(4)
+    n = 300
+    xy = np.stack([0.1 + rng.uniform(-0.05, 0.05, n), -0.05 + rng.uniform(-0.05, 0.05, n)], 1)
+    v_in = oracle.locate(det, np.c_[xy, np.full(n, -0.1)])
+    v_out = oracle.locate(det, np.c_[xy, np.full(n, 0.2)])  # in the rod's solid, above the block (top z = 0.1)
+    assert (v_in == ir).all() and (v_out == iw).all()
+    o = np.c_[xy, rng.uniform(-0.2, 0.0, n)]
+    d = np.tile([0.0, 0.0, 1.0], (n, 1))
+    oi, of = oracle.query(det, o, d)
+    assert (oi[:, 1] == ir).all() and (oi[:, 2] == iw).all()  # out of the rod through the block's top face
+    np.testing.assert_allclose(of[:, 0], 0.1 - o[:, 2], atol=2e-6)
+    T = oracle.trace(det, A.key_of_seed(2), 1 << 14, source=sources.Point((0.1, -0.05, -0.1), 1.0, lam=400.0),
+                     samples=1 << 14, controls=A.controls())[0]  # fmt: skip
+    assert abs(T.health[:10].sum() - T.health[10]) < 1e-6 * T.health[10]
