@@ -183,9 +183,17 @@ typedef struct LumenSceneDesc {
   const int32_t* mesh_chunk; /* host, n_chunk * LUMEN_CHUNK_I: first triangle, count, mesh, 0 */
   const float* chunk_box;    /* host, n_chunk * 6: each chunk's padded world box (lo, hi), its BVH leaf's */
   const double* chunk_box64; /* host, n_chunk * 6: the same in float64 */
+  /* frame groups (src/lumen/geometry/navigator_build.py:11, bvh.py:20): a volume's daughters sharing a rotation R
+     whose world boxes are much larger than their own (diagonal wire planes) get a BVH of their own in R's frame
+     (x_g = R^T x_w), nodes in node_f / node_i after the volume's world-frame BVH; its members are not in that one.
+     0 / null: none. */
+  int32_t n_group;           /* at most LUMEN_MAX_GROUPS_PER_VOLUME in one volume */
+  const int32_t* group_i;    /* host, n_group * 4: the volume, first node, end node, 0 */
+  const float* group_r;      /* host, n_group * 9: R row-major */
+  const double* group_r64;   /* host, n_group * 9: the float64 navigator's */
 } LumenSceneDesc;
 
-enum { LUMEN_TRI_F = 12, LUMEN_CHUNK_I = 4, LUMEN_MESH_CHUNK = 8 };
+enum { LUMEN_TRI_F = 12, LUMEN_CHUNK_I = 4, LUMEN_MESH_CHUNK = 8, LUMEN_MAX_GROUPS_PER_VOLUME = 64 };
 
 enum { LUMEN_PREC_FLOAT32 = 0, LUMEN_PREC_FLOAT64 = 1 };
 

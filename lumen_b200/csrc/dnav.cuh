@@ -596,6 +596,44 @@ L_DEV void d_point_scan(const DScene& S, int v, const NF* x, NF pad, F visit) {
   }
 }
 
+// the same over the extended instantiation's frame groups too: each group's nodes with the point in its frame
+// (x_g = R^T x; the group tables and frames as d_enter_x reads them)
+template <class F>
+L_DEV void d_point_scan_x(const DScene& S, int v, const NF* x, NF pad, F visit) {
+  int n0 = vI(S, v, LUMEN_VI_NODE0), n1 = vI(S, v, LUMEN_VI_NODE1);
+  int g = 0, g_end = 0;
+  const int* gt = (S.mesh && __ldg(S.mesh + 7) > 0) ? S.mesh + __ldg(S.mesh + 7) : nullptr;
+  if (gt) {
+    g = __ldg(gt + 2 * v);
+    g_end = g + __ldg(gt + 2 * v + 1);
+  }
+  NF xs[3] = {x[0], x[1], x[2]};
+  for (int guard = 0; guard <= LUMEN_MAX_GROUPS_PER_VOLUME; ++guard) {
+    int node = n0;
+    while (node < n1) {
+      const NF* nf = NAV_NODE(S) + (size_t)node * LUMEN_NODE_F;
+      int inside = (__ldg(nf) - pad <= xs[0] && xs[0] <= __ldg(nf + 3) + pad) &&
+                   (__ldg(nf + 1) - pad <= xs[1] && xs[1] <= __ldg(nf + 4) + pad) &&
+                   (__ldg(nf + 2) - pad <= xs[2] && xs[2] <= __ldg(nf + 5) + pad);
+      const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
+      int cnt = __ldg(ni + 1);
+      if (inside && cnt > 0) {
+        int st = __ldg(ni + 2);
+        for (int k = 0; k < cnt; ++k) visit(__ldg(S.items + st + k));
+      }
+      node = (inside && cnt == 0) ? node + 1 : __ldg(ni);
+    }
+    if (g >= g_end) break;
+    const int* gr = gt + 2 * (S.n + 1) + 2 * g;
+    n0 = __ldg(gr);
+    n1 = __ldg(gr + 1);
+    const NF* R = NAV_LEAF(S) + __ldg(S.mesh + 6) + (size_t)9 * g;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) xs[a] = (__ldg(R + a) * x[0] + __ldg(R + 3 + a) * x[1]) + __ldg(R + 6 + a) * x[2];
+    g++;
+  }
+}
+
 // whether volume i is an ancestor of volume v (navigate.py:199 is_ancestor: the walk is depth first, a subtree is its
 // root and the LUMEN_VI_SIZE - 1 volumes after it): an ancestor among v's candidates is one v reaches out of, whose
 // face is v's exit (a protrusion clip). Daughters come after v, so for them the first test ends it without a load.
@@ -644,7 +682,7 @@ L_CALL int d_settle(const DScene& S, int v, const NF* od, const NF* dd, NF t, in
 // the volume reaches out of, never a volume to descend into
 L_DEV int d_find_x(const DScene& S, int v, const NF* x) {
   int g = -1;
-  d_point_scan(S, v, x, 0.0f, [&](int i) {
+  d_point_scan_x(S, v, x, 0.0f, [&](int i) {
     if (d_level_wins(S, i, g, -1) && !d_is_anc(S, i, v) && d_holds_point(S, i, x)) g = i;
   });
   return g;
@@ -661,7 +699,7 @@ L_CALL int d_locate_x(const DScene& S, const NF* x) {
 L_DEV int d_find_ray_x(const DScene& S, int v, const NF* od, const NF* dd, NF t, int excl, NF pad) {
   NF x[3] = {od[0] + t * dd[0], od[1] + t * dd[1], od[2] + t * dd[2]};
   int g = -1;
-  d_point_scan(S, v, x, pad, [&](int i) {
+  d_point_scan_x(S, v, x, pad, [&](int i) {
     if (d_level_wins(S, i, g, excl) && !d_is_anc(S, i, v) && d_ray_holds(S, i, od, dd, t)) g = i;
   });
   return g;
@@ -907,8 +945,112 @@ L_DEV void d_hit_grad_m(const DScene& S, int ch0, int item, int leaf, int face, 
 
 // the next event in volume v: its own exit, then the first entry of every daughter the BVH does not prune. One
 // call site of the visit (the own solid is the first candidate, then the traversal yields one leaf item at a time).
+// the extended instantiation's next event in volume v: the world-frame BVH, then each frame group's BVH with the ray
+// in the group's frame (x_g = R^T x_w: the boxes there are the members' own, tight for rotated wire planes); the
+// visits are the world ray's, so the winner is the same as one BVH over every candidate
+L_DEV Best d_enter_x(const DScene& S, const Ctx& c, int has_own, int vi) {
+  Best b = {N_HUGE, -1, -1, -1, 0, 0};
+  const int ch0 = m_ch0(S);
+  int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
+  int g = 0, g_end = 0;  // the volume's frame groups still to walk
+  const int* gt = (S.mesh && __ldg(S.mesh + 7) > 0) ? S.mesh + __ldg(S.mesh + 7) : nullptr;
+  if (gt) {
+    g = __ldg(gt + 2 * c.v);
+    g_end = g + __ldg(gt + 2 * c.v + 1);
+  }
+  NF os[3] = {c.od[0], c.od[1], c.od[2]}, ds[3] = {c.dd[0], c.dd[1], c.dd[2]};
+  NF inv[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    NF dv = ds[a];
+    inv[a] = 1.0f / (n_abs(dv) < N_TINY_DIR ? (dv < 0.0f ? -N_TINY_DIR : N_TINY_DIR) : dv);
+  }
+  int stack[D_STACK];
+  NF tins[D_STACK];
+  int sp = 0;
+  int node = -1;
+  int started = 0;
+  int pending = has_own;
+  for (;;) {
+    int item = -1, is_own = 0;
+    if (pending) {
+      item = vi;
+      is_own = 1;
+      pending = 0;
+    } else {
+      if (!started) {
+        started = 1;
+        node = -1;
+        if (n0 < n1) {
+          NF tin, tout;
+          d_slab(NAV_NODE(S), n0, os, inv, &tin, &tout);
+          node = (tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band) ? n0 : -1;
+        }
+      }
+      while (item < 0) {
+        if (node < 0) {
+          NF lim = d_min(b.t, c.t_bound) + c.band;
+          while (sp > 0 && tins[sp - 1] > lim) sp--;
+          if (sp == 0) break;
+          sp--;
+          node = stack[sp];
+        }
+        const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
+        int cnt = __ldg(ni + 1);
+        if (cnt > 0) {
+          item = __ldg(S.items + __ldg(ni + 2));
+          node = -1;
+          break;
+        }
+        int lc = node + 1;
+        int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
+        NF tl, tlo, tr, tro;
+        d_slab(NAV_NODE(S), lc, os, inv, &tl, &tlo);
+        d_slab(NAV_NODE(S), rc, os, inv, &tr, &tro);
+        NF lim = d_min(b.t, c.t_bound) + c.band;
+        int hl = tl <= tlo && tlo >= c.t_lo && tl <= lim;
+        int hr = tr <= tro && tro >= c.t_lo && tr <= lim;
+        int first = tl <= tr;
+        int near_ = first ? lc : rc, far_ = first ? rc : lc;
+        int h_near = first ? hl : hr, h_far = first ? hr : hl;
+        if (h_near && h_far && sp < D_STACK) {
+          stack[sp] = far_;
+          tins[sp] = first ? tr : tl;
+          sp++;
+        }
+        node = h_near ? near_ : (h_far ? far_ : -1);
+      }
+      if (item < 0) {  // this BVH is done: the next frame group's, the ray in its frame
+        if (g >= g_end) break;
+        const int* gr = gt + 2 * (S.n + 1) + 2 * g;
+        n0 = __ldg(gr);
+        n1 = __ldg(gr + 1);
+        const NF* R = NAV_LEAF(S) + __ldg(S.mesh + 6) + (size_t)9 * g;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          os[a] = (__ldg(R + a) * c.od[0] + __ldg(R + 3 + a) * c.od[1]) + __ldg(R + 6 + a) * c.od[2];
+          ds[a] = (__ldg(R + a) * c.dd[0] + __ldg(R + 3 + a) * c.dd[1]) + __ldg(R + 6 + a) * c.dd[2];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          NF dv = ds[a];
+          inv[a] = 1.0f / (n_abs(dv) < N_TINY_DIR ? (dv < 0.0f ? -N_TINY_DIR : N_TINY_DIR) : dv);
+        }
+        g++;
+        started = 0;
+        sp = 0;
+        continue;
+      }
+    }
+    if (item >= ch0 && !is_own) b = d_mesh_visit(S, c, ch0, item, b);
+    else b = d_unit_visit<1>(S, c, item, b, is_own);
+  }
+  return b;
+}
+
 template <int TORUS>
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
+  if constexpr (TORUS == 1) return d_enter_x(S, c, has_own, vi);
   Best b = {N_HUGE, -1, -1, -1, 0, 0};
   const int ch0 = TORUS == 1 ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks among the items
   int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);

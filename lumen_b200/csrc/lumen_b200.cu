@@ -50,7 +50,7 @@ struct LumenScene {
   std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
   int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
   int single;                          // every solid one quadric / plane leaf: the single-leaf instantiation
-  int clip;                            // a volume has an ancestor among its candidates (a protrusion clip)
+  int clip;                            // the extended locate is needed: a protrusion clip or frame groups
   int nav64;                           // LUMEN_PREC_FLOAT64: S's vol_f, node_f, leaf_f, plane_f hold float64 data
   const float* vol_f32;                // the float32 frames (the readout groups' binning reads them in either precision)
 };
@@ -585,6 +585,16 @@ static int check_desc(const LumenSceneDesc* d) {
   if (d->precision == LUMEN_PREC_FLOAT64 && (!d->vol_f64 || !d->leaf_f64 || (d->n_node > 0 && !d->node_f64) ||
                                              (d->n_plane > 0 && !d->plane_f64) || (d->n_tri > 0 && !d->mesh_tri64)))
     return set_err(LUMEN_ERR_ARG, "scene_create: a float64 scene without its float64 geometry arrays");
+  if (d->n_group < 0 || (d->n_group > 0 && (!d->group_i || !d->group_r || (d->precision == LUMEN_PREC_FLOAT64 && !d->group_r64))))
+    return set_err(LUMEN_ERR_ARG, "scene_create: frame groups without their tables");
+  for (int g = 0; g < d->n_group; ++g) {
+    const int32_t* gr = d->group_i + 4 * (size_t)g;
+    if (gr[0] < 0 || gr[0] > d->n_vol || gr[1] < 0 || gr[2] < gr[1] || gr[2] > d->n_node || (g > 0 && gr[0] < gr[-4]))
+      return set_err(LUMEN_ERR_ARG, "scene_create: a frame group out of range (groups in volume order)");
+    int same = 1;
+    for (int h = g - 1; h >= 0 && d->group_i[4 * (size_t)h] == gr[0]; --h) same++;
+    if (same > LUMEN_MAX_GROUPS_PER_VOLUME) return set_err(LUMEN_ERR_SCENE, "scene_create: too many frame groups in a volume");
+  }
   if (d->n_mesh < 0 || d->n_chunk < 0 || d->n_tri < 0 || (d->n_mesh > 0) != (d->n_chunk > 0) ||
       (d->n_chunk > 0 && (!d->mesh_tri || !d->mesh_chunk)))
     return set_err(LUMEN_ERR_ARG, "scene_create: meshes without their triangles or chunks");
@@ -1143,16 +1153,26 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   UPLOAD(S.vol_i, d->vol_i, (size_t)(ch0 + d->n_chunk) * LUMEN_VOL_I);
   UPLOAD(S.vol_f, d->vol_f, (size_t)d->n_vol * LUMEN_VOL_F);
   S.mesh = nullptr;  // the candidate lists are the checker's: the engine walks the BVH
-  if (d->n_mesh > 0) {  // the meshes' block: header, chunks, each triangle's chunk (dnav.cuh)
+  if (d->n_mesh > 0 || d->n_group > 0) {  // the extended block: header, chunks, each triangle's chunk, frame groups
     const long long sm = (long long)S.SU + (long long)d->n_vol * S.LM * S.FM * 4;
     if (sm + 4LL * d->n_tri >= (1LL << 31)) {
       for (void* p : sc->allocs) cudaFree(p);
       delete sc;
       return set_err(LUMEN_ERR_SCENE, "scene_create: the surface codes of the volumes and mesh triangles exceed int32");
     }
-    std::vector<int32_t> blk(8 + 4 * (size_t)d->n_chunk + d->n_tri, 0);
+    const size_t gto = 8 + 4 * (size_t)d->n_chunk + d->n_tri;  // the frame groups' table
+    std::vector<int32_t> blk(gto + 2 * (size_t)(d->n_vol + 1) + 2 * (size_t)d->n_group, 0);
     blk[0] = d->n_mesh; blk[1] = d->n_chunk; blk[2] = d->n_tri; blk[3] = d->n_leaf * LUMEN_LEAF_F;
     blk[4] = (int32_t)sm; blk[5] = ch0;
+    blk[6] = d->n_leaf * LUMEN_LEAF_F + d->n_tri * LUMEN_TRI_F;  // the groups' frames in the leaf array
+    blk[7] = d->n_group > 0 ? (int32_t)gto : 0;
+    for (int g = 0; g < d->n_group; ++g) {  // per volume its first group and count; per group its node range
+      int v = d->group_i[4 * g];
+      if (blk[gto + 2 * v + 1] == 0) blk[gto + 2 * v] = g;
+      blk[gto + 2 * v + 1] += 1;
+      blk[gto + 2 * (size_t)(d->n_vol + 1) + 2 * g] = d->group_i[4 * g + 1];
+      blk[gto + 2 * (size_t)(d->n_vol + 1) + 2 * g + 1] = d->group_i[4 * g + 2];
+    }
     for (int c = 0; c < d->n_chunk; ++c) {
       for (int j = 0; j < 4; ++j) blk[8 + 4 * c + j] = d->mesh_chunk[4 * c + j];
       for (int k = 0; k < d->mesh_chunk[4 * c + 1]; ++k) blk[8 + 4 * (size_t)d->n_chunk + d->mesh_chunk[4 * c] + k] = c;
@@ -1163,10 +1183,12 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   UPLOAD(S.node_i, d->node_i, (size_t)d->n_node * LUMEN_NODE_I);
   UPLOAD(S.items, d->items, (size_t)d->n_item);
   UPLOAD(S.kind_i, d->kind_i, (size_t)d->n_kind * LUMEN_KIND_I);
-  if (d->n_tri > 0) {  // the meshes' triangles after the leaves (one allocation: the navigator reads both)
-    std::vector<float> lt((size_t)d->n_leaf * LUMEN_LEAF_F + (size_t)d->n_tri * LUMEN_TRI_F);
-    std::copy(d->leaf_f, d->leaf_f + (size_t)d->n_leaf * LUMEN_LEAF_F, lt.begin());
-    std::copy(d->mesh_tri, d->mesh_tri + (size_t)d->n_tri * LUMEN_TRI_F, lt.begin() + (size_t)d->n_leaf * LUMEN_LEAF_F);
+  if (d->n_tri > 0 || d->n_group > 0) {  // the triangles and the groups' frames after the leaves (one allocation)
+    const size_t nl = (size_t)d->n_leaf * LUMEN_LEAF_F, nt = (size_t)d->n_tri * LUMEN_TRI_F;
+    std::vector<float> lt(nl + nt + 9 * (size_t)d->n_group);
+    std::copy(d->leaf_f, d->leaf_f + nl, lt.begin());
+    if (nt) std::copy(d->mesh_tri, d->mesh_tri + nt, lt.begin() + nl);
+    if (d->n_group) std::copy(d->group_r, d->group_r + 9 * (size_t)d->n_group, lt.begin() + nl + nt);
     UPLOAD(S.leaf_f, lt.data(), lt.size());
   } else {
     UPLOAD(S.leaf_f, d->leaf_f, (size_t)d->n_leaf * LUMEN_LEAF_F);
@@ -1180,10 +1202,11 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
     const double *vd = nullptr, *nd = nullptr, *ld = nullptr, *pd = nullptr;
     UPLOAD(vd, d->vol_f64, (size_t)d->n_vol * LUMEN_VOL_F);
     UPLOAD(nd, d->node_f64, (size_t)d->n_node * LUMEN_NODE_F);
-    std::vector<double> lt((size_t)d->n_leaf * LUMEN_LEAF_F + (size_t)d->n_tri * LUMEN_TRI_F);
-    std::copy(d->leaf_f64, d->leaf_f64 + (size_t)d->n_leaf * LUMEN_LEAF_F, lt.begin());
-    if (d->n_tri > 0)
-      std::copy(d->mesh_tri64, d->mesh_tri64 + (size_t)d->n_tri * LUMEN_TRI_F, lt.begin() + (size_t)d->n_leaf * LUMEN_LEAF_F);
+    const size_t nl = (size_t)d->n_leaf * LUMEN_LEAF_F, nt = (size_t)d->n_tri * LUMEN_TRI_F;
+    std::vector<double> lt(nl + nt + 9 * (size_t)d->n_group);
+    std::copy(d->leaf_f64, d->leaf_f64 + nl, lt.begin());
+    if (nt) std::copy(d->mesh_tri64, d->mesh_tri64 + nt, lt.begin() + nl);
+    if (d->n_group) std::copy(d->group_r64, d->group_r64 + 9 * (size_t)d->n_group, lt.begin() + nl + nt);
     UPLOAD(ld, lt.data(), lt.size());
     UPLOAD(pd, d->plane_f64, (size_t)d->n_plane * LUMEN_PLANE_F);
     S.vol_f = reinterpret_cast<const float*>(vd);
@@ -1236,9 +1259,10 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
       sc->sigma_tabs.push_back(ri[LUMEN_RI_COL + LUMEN_COL_SIGMA]);
   }
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
-  sc->has_torus = d->n_mesh > 0;  // the extended instantiation: torus leaves or mesh chunks
+  sc->has_torus = d->n_mesh > 0 || d->n_group > 0;  // the extended instantiation: tori, meshes, frame groups
+  sc->clip = d->n_group > 0;  // the extended locate (frame groups, protrusion clips): no wavefront (its fill's locate)
   for (int l = 0; l < d->n_leaf; ++l) sc->has_torus = sc->has_torus || d->leaf_i[(size_t)l * LUMEN_LEAF_I] == 2;
-  for (int v = 0; v < d->n_vol && !sc->has_torus; ++v) {  // a protrusion clip: the extended instantiation
+  for (int v = 0; v < d->n_vol && !sc->clip; ++v) {  // a protrusion clip: the extended instantiation
     const int32_t* vr = d->vol_i + (size_t)v * LUMEN_VOL_I;
     for (int k = 0; k < vr[LUMEN_VI_CN]; ++k) {
       int i = d->cand[vr[LUMEN_VI_C0] + k];

@@ -101,6 +101,9 @@ class Detector:
             d.n_mesh, d.n_chunk, d.n_tri = a["n_mesh"], len(keep["mesh_chunk"]), len(keep["mesh_tri"])
             d.mesh_tri, d.mesh_tri64 = fptr(keep["mesh_tri"]), dptr(keep["mesh_tri64"])
             d.mesh_chunk, d.chunk_box, d.chunk_box64 = iptr(keep["mesh_chunk"]), fptr(keep["chunk_box"]), dptr(keep["chunk_box64"])
+        if a.get("n_group", 0):  # frame groups: their node ranges and frames
+            d.n_group = a["n_group"]
+            d.group_i, d.group_r, d.group_r64 = iptr(keep["group_i"]), fptr(keep["group_r"]), dptr(keep["group_r64"])
         if self.precision == "float64":  # the float64 navigator's arrays
             d.precision = 1
             d.vol_f64, d.node_f64 = dptr(keep["vol_f64"]), dptr(keep["node_f64"])
@@ -131,7 +134,7 @@ class Detector:
 
 
 def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None,
-          after_tracking=(), precision="float32") -> Detector:
+          after_tracking=(), precision="float32", frame_groups=True) -> Detector:
     """Return the Detector of the volume tree ``top`` (the detector volume, placed at the origin).
 
     ``materials``: {name: Material}. ``borders``: [(pv from, pv to, OpticalSurface)] (Geant4 border surfaces, ordered);
@@ -141,7 +144,8 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     ``after_tracking``: sensor groups whose sensor model applies its QE after tracking: their rows detect every
     absorption (eff 1) and are read per normal incidence (types.py:576 per_normal: a deposit carries 1 / A_n, by
     which a normalising readout grid divides it). ``precision``: the navigator's ("float32", or "float64":
-    ``Detector.with_precision``).
+    ``Detector.with_precision``). ``frame_groups``: daughters sharing a rotation get a BVH in its frame where that
+    pays (the navigator's speed only; the same results).
     """
     skins = skins or {}
     sensors = sensors or {}
@@ -201,7 +205,8 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             s_axis.append(p.R[:, 2])
     if prio is not None:  # the rule's order given per placement of the walk (and the outside last)
         prio = np.asarray([prio[i] for i in vol_idx] + [prio[len(flat)]])
-    nav = G.navigator_arrays(placed, vol_cls[:n], out_cls, vol_sensor, prio, meshes=meshes, mesh_cls=vol_cls[n:])
+    nav = G.navigator_arrays(placed, vol_cls[:n], out_cls, vol_sensor, prio, meshes=meshes, mesh_cls=vol_cls[n:],
+                             use_frame_groups=frame_groups)  # fmt: skip
     # media
     pool = O.Pool()
     med_names = sorted(set(cls_mat))

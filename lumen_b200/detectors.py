@@ -199,6 +199,30 @@ def protrusion_box() -> D.Detector:
                    skins={"Box": wall}, sensors={"pmt": "PMT"})  # fmt: skip
 
 
+def wire_planes(n_wires=48, frame_groups=True) -> D.Detector:
+    """Return a 2 m argon-like box with two planes of ``n_wires`` thin steel wires (r 1.5 mm) at +60 and -60 degrees
+    about x (the induction planes of a wire chamber), a collection plane of vertical wires, and 8 sensor discs on one
+    wall: daughters sharing a rotation whose world boxes are much larger than their own (frame groups)."""  # noqa: D205
+    lar = O.Material("LAr", rindex=1.38, abslength=20.0, rayleigh=0.9)
+    steel = O.Material("Steel")
+    cathode = O.Material("Photocathode")
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "LAr")
+    wire = G.Volume("Wire", G.Tube(rmax=0.0015, dz=0.55), "Steel")
+    for p_, (x, ang) in enumerate(((0.3, 60.0), (0.4, -60.0), (0.5, 0.0))):
+        for k in range(n_wires):
+            y = -0.45 + 0.9 * k / (n_wires - 1)
+            box.place(wire, (x, y, 0.0), G.rotation("x", ang), name=f"W{p_}_{k}", copy=p_ * n_wires + k)
+    pmt = G.Volume("PMT", G.Tube(rmax=0.12, dz=0.01), "Photocathode")
+    rot = G.rotation("y", 90.0)
+    for i in range(8):
+        box.place(pmt, (0.98, -0.6 + 0.4 * (i % 4), -0.3 + 0.6 * (i // 4)), rot, name=f"PMT_{i}", copy=i)
+    surf = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    shiny = O.OpticalSurface("WireSurface", "dielectric_metal", "polished", reflectivity=0.5)
+    borders = [("Box", f"PMT_{i}", surf) for i in range(8)]
+    return D.build(box, {"LAr": lar, "Steel": steel, "Photocathode": cathode}, borders=borders,
+                   skins={"Wire": shiny}, sensors={"pmt": "PMT"}, frame_groups=frame_groups)  # fmt: skip
+
+
 def coated_panel(thickness=3e-6, distance=5.0, precision="float32") -> D.Detector:
     """Return a 12 m water box with a 2 x 2 m acrylic backing 20 cm thick at x = ``distance`` m, coated on its front
     face with a TPB-like layer ``thickness`` m thick (rindex 1.6), and 4 photocathode discs (r 0.3 m) behind it: the

@@ -931,12 +931,56 @@ def pad_box(lo, hi):
     return lo - pad, hi + pad
 
 
-def _node_boxes64(node_i, items, lo, hi) -> np.ndarray:
+MIN_GROUP = 8  # a rotation shared by at least this many daughters (or by all) may be a frame group (bvh.py:20)
+GROUP_GAIN = 4.0  # ... when their world boxes' surface areas are at least this times their own boxes' (bvh.py:21)
+MAX_GROUPS_PER_VOLUME = 64  # frame groups in one volume (the engine walks them in turn)
+
+
+def _area(lo, hi):
+    d = np.maximum(np.asarray(hi) - np.asarray(lo), 0.0)
+    return 2.0 * (d[..., 0] * d[..., 1] + d[..., 1] * d[..., 2] + d[..., 0] * d[..., 2])
+
+
+def frame_groups(ks, placed, low, lo_w, hi_w, n):
+    """Return (the candidates left to the world-frame BVH, [(R, members)]): the daughters of one volume sharing a
+    rotation R other than the identity, at least MIN_GROUP of them (or all its daughters), whose world boxes' summed
+    surface area is at least GROUP_GAIN times their own boxes' (src/lumen/geometry/navigator_build.py:11, bvh.py
+    frame_groups_all): each such set gets a BVH in R's frame (diagonal wire planes)."""  # noqa: D205, D209
+    units = [k for k in ks if k < n]
+    by = {}
+    for k in units:
+        by.setdefault(tuple(np.round(placed[k].R.ravel(), 12)), []).append(k)
+    groups, taken = [], set()
+    for mem in by.values():
+        R = placed[mem[0]].R
+        if np.allclose(R, np.eye(3), atol=1e-12) or not (len(mem) >= MIN_GROUP or len(mem) == len(units)):
+            continue
+        own = sum(float(_area(low[k].lo, low[k].hi)) for k in mem)
+        if float(_area(lo_w[mem], hi_w[mem]).sum()) < GROUP_GAIN * own:
+            continue
+        groups.append((R, mem))
+        taken.update(mem)
+        if len(groups) == MAX_GROUPS_PER_VOLUME:  # the engine's bound (LUMEN_MAX_GROUPS_PER_VOLUME)
+            break
+    return [k for k in ks if k not in taken], groups
+
+
+def group_boxes(R, mem, placed, low):
+    """Return the members' boxes (lo, hi) in the group frame x_g = R^T x_w, padded as the world boxes."""
+    lo, hi = np.zeros((len(mem), 3)), np.zeros((len(mem), 3))
+    for j, k in enumerate(mem):
+        M, tt = R.T @ placed[k].R, R.T @ placed[k].t
+        c = np.array([[(low[k].hi if (q >> a) & 1 else low[k].lo)[a] for a in range(3)] for q in range(8)]) @ M.T + tt
+        lo[j], hi[j] = pad_box(c.min(0), c.max(0))
+    return lo, hi
+
+
+def _node_boxes64(node_i, items, lo, hi, n0=0, n1=None, out=None) -> np.ndarray:
     """Return the BVH nodes' boxes in float64 over the float32 BVH's topology (depth-first with skips: a node's left
     child follows it, its right child is the left child's skip): a leaf the union of its items' float64 boxes, an inner
     node the union of its children's, bottom-up."""
-    out = np.zeros((len(node_i), 6))
-    for k in range(len(node_i) - 1, -1, -1):
+    out = np.zeros((len(node_i), 6)) if out is None else out
+    for k in range((len(node_i) if n1 is None else n1) - 1, n0 - 1, -1):
         cnt, st = int(node_i[k, 1]), int(node_i[k, 2])
         if cnt > 0:
             it = items[st:st + cnt]
@@ -1039,14 +1083,20 @@ def _local_box(p: Placed, lo, hi):
     return cl - rl, cl + rl
 
 
-def _proved_apart(pa: Placed, pb: Placed, la: Lowered, lb: Lowered, lo, hi, depth: int = 7) -> bool:
-    """Whether solids a and b share no point of the world box [lo, hi] (the overlap of their boxes): every cell of its
-    bisection (down to ``depth`` levels) is proved outside one of them by interval bounds (``relation`` in
-    src/lumen/geometry/ownership.py: interval bounds over bisected boxes, never sampling)."""  # noqa: D205, D209
-    todo = [(np.asarray(lo, float), np.asarray(hi, float), 0)]
+def _proved_apart(pa: Placed, pb: Placed, la: Lowered, lb: Lowered, lo=None, hi=None, depth: int = 7) -> bool:
+    """Whether solids a and b share no point: in a's frame, the region a's box shares with the box of b's box
+    corners is empty, or every cell of its bisection (down to ``depth`` levels) is proved outside one of them by
+    interval bounds (``relation`` in src/lumen/geometry/ownership.py: interval bounds over bisected boxes, never
+    sampling)."""  # noqa: D205, D209
+    cb = np.array([[(lb.hi if (q >> a) & 1 else lb.lo)[a] for a in range(3)] for q in range(8)]) @ pb.R.T + pb.t
+    ca = (cb - pa.t) @ pa.R  # b's box corners in a's frame
+    rlo, rhi = np.maximum(la.lo, ca.min(0)), np.minimum(la.hi, ca.max(0))
+    if np.any(rlo >= rhi):
+        return True
+    todo = [(rlo, rhi, 0)]
     while todo:
         clo, chi, dp = todo.pop()
-        if _solid_interval(la, *_local_box(pa, clo, chi)) == -1 or _solid_interval(lb, *_local_box(pb, clo, chi)) == -1:
+        if _solid_interval(la, clo, chi) == -1 or _solid_interval(lb, *_local_box(pb, *_world_box(pa, clo, chi))) == -1:
             continue
         if dp >= depth:
             return False
@@ -1166,7 +1216,8 @@ def ownership(placed: list, kinds: list, kind_of: dict, lo_w, hi_w, tol: float):
     return prio, owners
 
 
-def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=None, meshes=(), mesh_cls=()) -> dict:
+def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=None, meshes=(), mesh_cls=(),
+                     use_frame_groups=True) -> dict:
     """Return the navigator's flat arrays (include/lumen_b200.h layouts) of the placed volumes and ``meshes``
     [(world triangles, mother)] of classes ``mesh_cls``: navigator ids 0 .. n - 1 the volumes, n the outside, n + 1 + k
     mesh k's pseudo-volume, CH0 + c (CH0 = n + 1 + meshes) chunk c, an item of its mesh's mother; every id has a
@@ -1236,6 +1287,8 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
     hi_w = np.concatenate([hi_w, np.zeros((1 + nm, 3)), mc["hi"]])
     vol_i = np.zeros((ch0 + nch, 10), np.int32)
     cand, node_f, node_i, items = [], [], [], []
+    fgroups = []  # (volume, first node, end node, R, members' group-frame boxes lo, hi)
+    low_all = [kinds[kind_of[id(p.lv.solid)]] for p in placed]
     for v in range(n + 1, ch0 + nch):  # the meshes' and their chunks' rows: class, mother, rank; no solid, no BVH
         k = v - n - 1 if v < ch0 else int(mc["chunk"][v - ch0, 2])
         vol_i[v, 0] = -1
@@ -1253,10 +1306,11 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
         vol_i[v, 5], vol_i[v, 6] = len(cand), len(ks)
         vol_i[v, 9] = size[v] if v < n else 1  # the volumes of its subtree (an ancestor of w: v < w < v + size)
         cand.extend(ks)
-        # the daughters' BVH, in the float32 boxes the engine reads
+        # the daughters' BVH, in the float32 boxes the engine reads (the frame groups' own BVHs after it)
         lo32 = lo_w.astype(np.float32).astype(np.float64)
         hi32 = hi_w.astype(np.float32).astype(np.float64)
-        nodes, order = _bvh(np.asarray(ks, np.int64), lo32, hi32)
+        wks, grp = frame_groups(ks, placed, low_all, lo_w, hi_w, n) if use_frame_groups and v < n + 1 else (ks, [])
+        nodes, order = _bvh(np.asarray(wks, np.int64), lo32, hi32)
         base, ibase = len(node_f), len(items)
         vol_i[v, 7] = base
         for nd in nodes:
@@ -1264,7 +1318,22 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
             node_i.append([base + nd[2], nd[3], ibase + nd[4] if nd[3] else 0, 0])
         items.extend(order)
         vol_i[v, 8] = len(node_f)
+        for R, mem in grp:  # a frame group: its BVH over the members' boxes in the group frame
+            glo, ghi = group_boxes(R, mem, placed, low_all)
+            gl, gh = np.zeros_like(lo_w), np.zeros_like(hi_w)
+            gl[mem], gh[mem] = glo, ghi
+            gnodes, gorder = _bvh(np.asarray(mem, np.int64), gl.astype(np.float32).astype(np.float64),
+                                  gh.astype(np.float32).astype(np.float64))  # fmt: skip
+            gb, gib = len(node_f), len(items)
+            for nd in gnodes:
+                node_f.append([*nd[0], *nd[1]])
+                node_i.append([gb + nd[2], nd[3], gib + nd[4] if nd[3] else 0, 0])
+            items.extend(gorder)
+            fgroups.append((v, gb, len(node_f), R, gl, gh))
     ni_arr = np.asarray(node_i, np.int32).reshape(-1, 4)
+    for _, g0, g1, _, _, _ in fgroups:
+        if bvh_depth(ni_arr, g0, g1) > MAX_BVH_DEPTH:
+            raise ValueError(f"a frame group's BVH deeper than {MAX_BVH_DEPTH} levels")
     for v in range(n + 1):
         if bvh_depth(ni_arr, vol_i[v, 7], vol_i[v, 8]) > MAX_BVH_DEPTH:
             raise ValueError(f"volume {v}: a daughter BVH deeper than {MAX_BVH_DEPTH} levels")
@@ -1273,12 +1342,19 @@ def navigator_arrays(placed: list, vol_cls, outside_cls: int, vol_sensor, prio=N
     allp = np.concatenate([lo_w[:n], hi_w[:n], mc["lo"], mc["hi"]]) if n else np.zeros((1, 3))
     reach = float(np.linalg.norm(allp.max(0) - allp.min(0)))
     items_a = np.asarray(items, np.int64)
+    node64 = _node_boxes64(ni_arr, items_a, lo_w, hi_w)
+    for _, g0, g1, _, gl, gh in fgroups:  # a group's nodes over its members' group-frame boxes
+        _node_boxes64(ni_arr, items_a, gl, gh, g0, g1, node64)
     return dict(
         n_vol=n, vol_i=vol_i, vol_f=vol_f.astype(np.float32), cand=np.asarray(cand, np.int32),
         # the float64 navigator's arrays (LUMEN_PREC_FLOAT64): the same geometry in float64, the BVH's topology shared
         vol_f64=vol_f.copy(), leaf_f64=np.asarray(leaf_f, np.float64).reshape(-1, 20),
         plane_f64=np.asarray(plane_f, np.float64).reshape(-1, 4),
-        node_f64=_node_boxes64(ni_arr, items_a, lo_w, hi_w),
+        node_f64=node64,
+        # frame groups: per group (volume, first node, end node, 0) and its frame R (row-major, x_g = R^T x_w)
+        n_group=len(fgroups), group_i=np.asarray([[g[0], g[1], g[2], 0] for g in fgroups], np.int32).reshape(-1, 4),
+        group_r=np.asarray([g[3].ravel() for g in fgroups], np.float32).reshape(-1, 9),
+        group_r64=np.asarray([g[3].ravel() for g in fgroups], np.float64).reshape(-1, 9),
         node_f=np.asarray(node_f, np.float32).reshape(-1, 6), node_i=np.asarray(node_i, np.int32).reshape(-1, 4),
         items=np.asarray(items, np.int32), kind_i=np.asarray(kind_i, np.int32).reshape(-1, 4),
         leaf_f=np.asarray(leaf_f, np.float32).reshape(-1, 20), leaf_i=np.asarray(leaf_i, np.int32).reshape(-1, 4),

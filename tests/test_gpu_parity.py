@@ -572,3 +572,27 @@ def test_overlapping_siblings_bit_exact(which, built):
     src = sources.Point(position=(0.0, 0.0, 0.0), n_photons=1.0, lam=400.0)
     bad, gi, oi, gf, of = _records_match(det, src, 1 << 14)
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+def test_wire_planes_with_frame_groups_bit_exact(built):
+    """Frame groups (the +-60 degree wire planes walked in their own frame by the extended instantiation): queries,
+    locates and photons are the checker's bit for bit (the checker scans every candidate: the winner does not depend
+    on the traversal)."""
+    det = detectors.wire_planes()
+    assert det.arrays["n_group"] == 2
+    rng = np.random.default_rng(17)
+    n = 20000
+    o = rng.uniform(-0.99, 0.99, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    eng = _engine(det)
+    gi, gf = eng.query(o, d)
+    oi, of = oracle.query(det, o, d)
+    gi, gf = gi.cpu().numpy(), gf.cpu().numpy()
+    assert ((oi[:, 2] > 0) & (oi[:, 2] <= 144)).sum() > 200  # rays that meet a wire
+    assert (gi == oi).all(), np.flatnonzero((gi != oi).any(1))[:10]
+    assert (gf.view(np.uint32) == of.view(np.uint32)).all()
+    assert (eng.locate(o).cpu().numpy() == oracle.locate(det, o)).all()
+    src = sources.Point(position=(-0.5, 0.0, 0.0), n_photons=1.0, lam=128.0)
+    bad, gi, oi, gf, of = _records_match(det, src, 1 << 14)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"

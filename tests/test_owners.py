@@ -102,3 +102,23 @@ def test_a_protruding_daughter_is_clipped_by_its_mother():
     T = oracle.trace(det, A.key_of_seed(2), 1 << 14, source=sources.Point((0.1, -0.05, -0.1), 1.0, lam=400.0),
                      samples=1 << 14, controls=A.controls())[0]  # fmt: skip
     assert abs(T.health[:10].sum() - T.health[10]) < 1e-6 * T.health[10]
+
+
+def test_frame_groups():
+    """Daughters sharing a rotation whose world boxes are much larger than their own (the wire planes at +-60
+    degrees) get a BVH in their frame; the vertical plane and the sensors stay in the world-frame BVH; parallel wires
+    are proved apart (no owners among them)."""
+    det = detectors.wire_planes()
+    a = det.arrays
+    assert a["n_group"] == 2 and (a["group_i"][:, 0] == 0).all()
+    vi, n, cand = a["vol_i"], a["n_vol"], a["cand"]
+    for v in range(1, n):
+        ks = cand[vi[v, 5]:vi[v, 5] + vi[v, 6]]
+        assert not [k for k in ks if k < n and vi[k, 1] != v]  # no owner: the wires are apart
+    R = a["group_r64"].reshape(-1, 3, 3)
+    ang = np.degrees(np.arctan2(R[:, 2, 1], R[:, 1, 1]))
+    assert sorted(np.round(ang).tolist()) == [-60.0, 60.0]
+    items = [set(a["items"][a["node_i"][g1:g2][:, 2][a["node_i"][g1:g2][:, 1] > 0]].tolist()) for _, g1, g2, _ in a["group_i"]]
+    assert all(len(s) == 48 for s in items) and not (items[0] & items[1])
+    world = a["items"][a["node_i"][vi[0, 7]:vi[0, 8]][:, 2][a["node_i"][vi[0, 7]:vi[0, 8]][:, 1] > 0]]
+    assert len(world) == 48 + 8 and not (set(world.tolist()) & (items[0] | items[1]))
