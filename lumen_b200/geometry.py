@@ -1083,7 +1083,7 @@ def _local_box(p: Placed, lo, hi):
     return cl - rl, cl + rl
 
 
-def _proved_apart(pa: Placed, pb: Placed, la: Lowered, lb: Lowered, lo=None, hi=None, depth: int = 7) -> bool:
+def _proved_apart(pa: Placed, pb: Placed, la: Lowered, lb: Lowered, depth: int = 7) -> bool:
     """Whether solids a and b share no point: in a's frame, the region a's box shares with the box of b's box
     corners is empty, or every cell of its bisection (down to ``depth`` levels) is proved outside one of them by
     interval bounds (``relation`` in src/lumen/geometry/ownership.py: interval bounds over bisected boxes, never
@@ -1176,8 +1176,7 @@ def ownership(placed: list, kinds: list, kind_of: dict, lo_w, hi_w, tol: float):
     def link(a, b):
         k = (min(a, b), max(a, b))
         if k not in linked:
-            lo, hi = np.maximum(lo_w[a], lo_w[b]), np.minimum(hi_w[a], hi_w[b])
-            linked[k] = not _proved_apart(placed[a], placed[b], low[a], low[b], lo, hi)
+            linked[k] = not _proved_apart(placed[a], placed[b], low[a], low[b])
         return linked[k]
 
     order_of = {}
