@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 10
+#define LUMEN_B200_ABI_VERSION 11
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
