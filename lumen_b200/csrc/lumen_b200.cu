@@ -815,9 +815,10 @@ static int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
 
 template <int G>
 static int launch_trace(const Launch& L, const Pick& pk, int variant, int bps, cudaStream_t stream) {
-  if (pk.nav64) {  // the float64 navigator: shape 0 with the torus code, whatever the variant
+  if (pk.nav64) {  // the float64 navigator: shape 0, extended or single-leaf geometry, whatever the variant
     if constexpr (G == 0)
       if (L.truth) return launch_shape<0, 256, 4, 1, 1, 1>(L, bps, stream);
+    if (pk.single) return launch_shape<G, 256, 4, 2, 0, 1>(L, bps, stream);
     return launch_shape<G, 256, 4, 1, 0, 1>(L, bps, stream);
   }
   if constexpr (G == 0) {
