@@ -385,8 +385,9 @@ L_DEV int d_mem_at(const DScene& S, const ScanT<NLMAX>& s, NF t, int use_on) {
   });
 }
 
-// TORUS: the geometry instantiation: 1 reads torus leaves and mesh chunks (scenes without either run one without
-// their code), 2 is for scenes whose solids are single quadric / plane leaves, 0 the rest
+// TORUS: the geometry instantiation: 1 reads torus leaves, mesh chunks and protrusion clips (scenes without them run
+// one without their code), 3 the same with frame groups, 2 is for scenes whose solids are single quadric / plane
+// leaves, 0 the rest
 template <int TORUS, int NLMAX>
 L_DEV void d_scan_init(const DScene& S, ScanT<NLMAX>& s, int kind, const NF* o, const NF* d, NF t1) {
   s.kind = kind;
@@ -394,7 +395,7 @@ L_DEV void d_scan_init(const DScene& S, ScanT<NLMAX>& s, int kind, const NF* o, 
   s.nl = NLMAX == 1 ? 1 : __ldg(k + 1);
   int l0 = __ldg(k);
   for (int l = 0; l < (NLMAX == 1 ? 1 : s.nl); ++l) {
-    if (TORUS == 1 && __ldg(S.leaf_i + (size_t)(l0 + l) * LUMEN_LEAF_I) == 2)
+    if ((TORUS & 1) && __ldg(S.leaf_i + (size_t)(l0 + l) * LUMEN_LEAF_I) == 2)
       s.iv[l] = d_torus_iv(NAV_LEAF(S) + (size_t)(l0 + l) * LUMEN_LEAF_F, NF3{o[0], o[1], o[2]},
                            NF3{d[0], d[1], d[2]});
     else
@@ -759,9 +760,9 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   // an ancestor the volume is not proved inside (the extended instantiation): its first exit from a start inside it,
   // when earlier than every other event (navigate.py:376 _unit_visit, clip)
   int clip = 0;
-  if constexpr (TORUS == 1) clip = !is_own && d_is_anc(S, i, c.v);
+  if constexpr ((TORUS & 1)) clip = !is_own && d_is_anc(S, i, c.v);
   const int own = is_own;
-  if constexpr (TORUS == 1) is_own = is_own || clip;
+  if constexpr ((TORUS & 1)) is_own = is_own || clip;
   const Side& sd = c.sd;
   NF bnd = c.t_bound + c.band;
   NF ol[3], dl[3];
@@ -783,9 +784,9 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   int by_s = kn_i && (is_own ? sd.s > 0.0f : sd.s < 0.0f);
   int ins = kn_i ? (is_own ? (sd.s <= 0.0f && h) : sd.s < 0.0f) : (on ? r.first.inside : r.inside0);
   h = h && (is_own || !ins);
-  if constexpr (TORUS == 1) h = h && (!clip || ins);
+  if constexpr ((TORUS & 1)) h = h && (!clip || ins);
   int zero = is_own ? !ins : (ins && (i != c.last || kn_i));
-  if constexpr (TORUS == 1) zero = zero && !clip;
+  if constexpr ((TORUS & 1)) zero = zero && !clip;
   if (zero) {
     lf = by_s ? sd.leaf : (on ? r.first.leaf : -1);
     f = by_s ? sd.face : (on ? r.first.face : -1);
@@ -799,7 +800,7 @@ L_DEV Best d_unit_visit(const DScene& S, const Ctx& c, int i, Best b, int is_own
   NF te = apart ? r.first.t : (zero ? c.t_lo : (h ? t : N_HUGE));
   int wins = d_entry_wins(S, te, i, b);
   int better = is_own || (!is_own && (zero || h) && wins);
-  if constexpr (TORUS == 1) better = own || (clip && h && te < b.t) || (!is_own && (zero || h) && wins);
+  if constexpr ((TORUS & 1)) better = own || (clip && h && te < b.t) || (!is_own && (zero || h) && wins);
   if (better) {
     Best nb = {te, i, lf, f, zero && !apart, own};
     return nb;
@@ -1050,9 +1051,9 @@ L_DEV Best d_enter_x(const DScene& S, const Ctx& c, int has_own, int vi) {
 
 template <int TORUS>
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
-  if constexpr (TORUS == 1) return d_enter_x(S, c, has_own, vi);
+  if constexpr (TORUS == 3) return d_enter_x(S, c, has_own, vi);
   Best b = {N_HUGE, -1, -1, -1, 0, 0};
-  const int ch0 = TORUS == 1 ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks among the items
+  const int ch0 = (TORUS & 1) ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks among the items
   int n0 = vI(S, c.v, LUMEN_VI_NODE0), n1 = vI(S, c.v, LUMEN_VI_NODE1);
   NF inv[3];
 #pragma unroll
@@ -1116,7 +1117,7 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
       }
       if (item < 0) break;
     }
-    if (TORUS == 1 && item >= ch0 && !is_own) b = d_mesh_visit(S, c, ch0, item, b);
+    if ((TORUS & 1) && item >= ch0 && !is_own) b = d_mesh_visit(S, c, ch0, item, b);
     else b = d_unit_visit<TORUS>(S, c, item, b, is_own);
   }
   return b;
@@ -1137,10 +1138,10 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   const NF* sn = sn_f;
 #endif
   const int OUT = S.n;
-  const int ch0 = TORUS == 1 ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks
+  const int ch0 = (TORUS & 1) ? m_ch0(S) : 0x7fffffff;  // the extended instantiation: mesh chunks
   NF xa = d_maxabs3(o);
   int cls0 = d_cls(S, vol);
-  Srf l0 = d_decode<TORUS == 1>(S, last);
+  Srf l0 = d_decode<(TORUS & 1)>(S, last);
   int kn0 = l0.known;
   NF t_lo = 0.0f;
   int v = vol, last_ = last, done = 0, it = 0;
@@ -1154,7 +1155,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
     NF band = d_band(xa + n_abs(t_lo));
     int vi = v < OUT - 1 ? v : OUT - 1;
     int has_own = v < OUT;
-    Srf ls = d_decode<TORUS == 1>(S, last_);
+    Srf ls = d_decode<(TORUS & 1)>(S, last_);
     Side sd = {ls.known, ls.leaf, ls.face, 0.0f, 0};
     if (ls.known) {
       if (sn) {
@@ -1163,7 +1164,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       } else {
         NF x0[3] = {o[0] + t_lo * d[0], o[1] + t_lo * d[1], o[2] + t_lo * d[2]};
         NF g[3];
-        if constexpr (TORUS == 1) d_hit_grad_m(S, ch0, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
+        if constexpr ((TORUS & 1)) d_hit_grad_m(S, ch0, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
         else d_hit_grad(S, ls.item, ls.leaf > 0 ? ls.leaf : 0, ls.face, x0, g);
         NF gd = d_dot(g, d);
         sd.s = gd / d_safe_norm(g) * (ls.o ? 1.0f : -1.0f);
@@ -1182,13 +1183,13 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
     NF step = d_band(xa + n_abs(hit ? t_c : t_lo));
     int nxt = v, moved = 0;
     {
-      const int clip = TORUS == 1 && !is_own && d_is_anc(S, u_in, v);  // out through an ancestor's face
+      const int clip = (TORUS & 1) && !is_own && d_is_anc(S, u_in, v);  // out through an ancestor's face
       int go_in = !is_own && !clip;
       int uc = u_in < 0 ? 0 : (u_in > OUT - 1 ? OUT - 1 : u_in);
       int up = clip ? d_parent(S, uc) : d_parent(S, v < OUT ? v : OUT);
       int nx0 = go_in ? u_in : up;
       int unit_x = go_in ? u_in : vi;
-      const int is_ch = TORUS == 1 && go_in && u_in >= ch0;  // a mesh chunk: entered, not relocated (navigate.py:531)
+      const int is_ch = (TORUS & 1) && go_in && u_in >= ch0;  // a mesh chunk: entered, not relocated (navigate.py:531)
       int off = hit && l_in >= 0 && !is_ch;
       NF od2[3] = {o[0], o[1], o[2]};
       if (off) {
@@ -1207,7 +1208,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
       NF tr = off ? t_c : t_c + step;
       if (is_ch) { nxt = OUT + 1 + __ldg(S.mesh + MESH_HDR + 4 * (u_in - ch0) + 2); moved = 0; }
       else if (hit) {
-        if constexpr (TORUS == 1) nxt = d_settle_x(S, nx0, od2, d, tr, unit_x, step + step, &moved);
+        if constexpr ((TORUS & 1)) nxt = d_settle_x(S, nx0, od2, d, tr, unit_x, step + step, &moved);
         else nxt = d_settle(S, nx0, od2, d, tr, unit_x, step + step, &moved);
       }
       else { nxt = nx0; moved = 0; }
@@ -1254,7 +1255,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   int vis_end = rec_vis;
   int cont = !vis_end && pz_hit && pz_zc >= D_ZSBP;
   int hit = (vis_end || cont) && bt < t_max;
-  if constexpr (TORUS == 1) {  // a mesh hit's t from its plane, short of it (surface_id.py:120 mesh_plane_t)
+  if constexpr ((TORUS & 1)) {  // a mesh hit's t from its plane, short of it (surface_id.py:120 mesh_plane_t)
     if (hit && !zero && bl >= 0 && bi >= ch0) {
       const NF* T = m_tri(S, bl);
       NF nk[3] = {__ldg(T + 9), __ldg(T + 10), __ldg(T + 11)};
@@ -1275,7 +1276,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   NF px = bt < N_HUGE ? bt : 0.0f;
   NF xh[3] = {o[0] + px * d[0], o[1] + px * d[1], o[2] + px * d[2]};
   NF g[3];
-  if constexpr (TORUS == 1) d_hit_grad_m(S, ch0, bi, bl > 0 ? bl : 0, bf, xh, g);
+  if constexpr ((TORUS & 1)) d_hit_grad_m(S, ch0, bi, bl > 0 ? bl : 0, bf, xh, g);
   else d_hit_grad(S, bi, bl > 0 ? bl : 0, bf, xh, g);
   NF gn = d_safe_norm(g);
   NF nrm[3] = {g[0] / gn, g[1] / gn, g[2] / gn};
@@ -1289,9 +1290,9 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
   }
   if (!(hit && bl >= 0)) { nrm[0] = fb[0]; nrm[1] = fb[1]; nrm[2] = fb[2]; }
   NF gd = d_dot(g, d);
-  int entry = bi != vb && !(TORUS == 1 && d_is_anc(S, bi, vb));  // an ancestor's face reached out of: an exit
+  int entry = bi != vb && !((TORUS & 1) && d_is_anc(S, bi, vb));  // an ancestor's face reached out of: an exit
   int o_ = entry ? gd < 0.0f : gd > 0.0f;
-  if (TORUS == 1 && bi >= ch0 && bl >= 0) q.srf = hit ? m_sm(S) + 4 * bl + 2 * o_ + entry : -1;  // a mesh triangle
+  if ((TORUS & 1) && bi >= ch0 && bl >= 0) q.srf = hit ? m_sm(S) + 4 * bl + 2 * o_ + entry : -1;  // a mesh triangle
   else q.srf = hit ? d_srf_pack(S, bi, bl, bf, o_, entry) : -1;
   if (nrm[0] * d[0] + nrm[1] * d[1] + nrm[2] * d[2] > 0.0f) { nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2]; }
   vb = hit ? vb : pz_vend;

@@ -675,7 +675,7 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
 template <int G, int TORUS, int ANALOG = 0, class NF = float>
 L_DEV void d_step(const Run& R, PhotonT<NF>& ph, float* dw, Key pkey, Dep& dep, float* dq, Ana& an) {
   PreT<NF> pr;
-  d_pre<TORUS == 1>(R, ph, pkey, pr);
+  d_pre<(TORUS & 1)>(R, ph, pkey, pr);
   QueryT<NF> q = d_step_query<TORUS>(R, ph, pr);
   d_post<G, ANALOG>(R, ph, dw, pr, q, dep, dq, an);
 }

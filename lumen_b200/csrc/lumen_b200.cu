@@ -51,6 +51,7 @@ struct LumenScene {
   int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
   int single;                          // every solid one quadric / plane leaf: the single-leaf instantiation
   int clip;                            // the extended locate is needed: a protrusion clip or frame groups
+  int groups;                          // frame groups (the instantiation walking them)
   int nav64;                           // LUMEN_PREC_FLOAT64: S's vol_f, node_f, leaf_f, plane_f hold float64 data
   const float* vol_f32;                // the float32 frames (the readout groups' binning reads them in either precision)
 };
@@ -89,6 +90,7 @@ struct Pick {
   int torus;
   int single;              // every solid a single quadric / plane leaf
   int clip;                // a protrusion clip (the wavefront's fill locates without the extended rule)
+  int groups;              // frame groups: the extended instantiation with their traversal
   int analog;
   int nav64;               // the scene's navigator is float64
   const float* vol_f32;    // the scene's float32 frames (the readout binning)
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
         if (g < (unsigned long long)L.n) {
           Row r;
           get_row(L, (int64_t)g, r);
-          d_start<TORUS == 1>(L.R.S, r, ph);
+          d_start<(TORUS & 1)>(L.R.S, r, ph);
           pkey = fold_in(L.key, (uint32_t)(L.first_id + (int64_t)g));
           w0 = (double)r.w0;
           ev = r.event;
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   wv_ld(V.ph, V.W, i, ph);
   wv_ld(V.ex, V.W, i, ex);
   Pre pr;
-  d_pre<TORUS == 1>(L.R, ph, ex.pkey, pr);
+  d_pre<(TORUS & 1)>(L.R, ph, ex.pkey, pr);
   Query q = d_step_query<TORUS>(L.R, ph, pr);
   wv_st(V.ph, V.W, i, ph);
   wv_st(V.pre, V.W, i, pr);
@@ -512,7 +514,7 @@ __global__ void k_trace_photons(Launch L, int32_t* out_i, float* out_f) {
   while (ph.alive && ph.vertex < L.R.max_vertices) {
     Dep dep;
     Ana an;
-    d_step<0, 1>(L.R, ph, dw, pkey, dep, dq, an);
+    d_step<0, 3>(L.R, ph, dw, pkey, dep, dq, an);  // every geometry: tori, meshes, clips, frame groups
     if (dep.sensor >= 0) {
       n_dep++;
       if (first_sensor < 0) first_sensor = dep.sensor;
@@ -541,7 +543,7 @@ __global__ void k_query(DScene S, const NF* ray, const int32_t* vol, const int32
   int known = vol[i] >= 0 && vol[i] <= S.n;
   int v = known ? vol[i] : nav_locate<1>(S, o);
   int last = known ? srf[i] : -1;
-  QueryT<NF> q = nav_query<1>(S, o, d, v, t_max, last, nullptr, sizeof(NF) == 4 ? (NF)D_HUGE : (NF)1e30);
+  QueryT<NF> q = nav_query<3>(S, o, d, v, t_max, last, nullptr, sizeof(NF) == 4 ? (NF)D_HUGE : (NF)1e30);
   int32_t* oi = out_i + 8 * i;
   oi[0] = q.hit; oi[1] = q.vol_before; oi[2] = q.vol_after; oi[3] = q.cls_before; oi[4] = q.cls_after;
   oi[5] = q.srf; oi[6] = q.zero;
@@ -780,6 +782,7 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   pk.torus = sc->has_torus;
   pk.single = sc->single;
   pk.clip = sc->clip;
+  pk.groups = sc->groups;
   pk.nav64 = sc->nav64;
   pk.vol_f32 = sc->vol_f32;
   pk.analog = (c->flags & LUMEN_F_TRUTH) != 0;
@@ -815,16 +818,21 @@ static int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
 
 template <int G>
 static int launch_trace(const Launch& L, const Pick& pk, int variant, int bps, cudaStream_t stream) {
-  if (pk.nav64) {  // the float64 navigator: shape 0, extended or single-leaf geometry, whatever the variant
+  if (pk.nav64) {  // the float64 navigator: shape 0, extended (with frame groups or not) or single-leaf geometry
     if constexpr (G == 0)
-      if (L.truth) return launch_shape<0, 256, 4, 1, 1, 1>(L, bps, stream);
+      if (L.truth) return pk.groups ? launch_shape<0, 256, 4, 3, 1, 1>(L, bps, stream)
+                                    : launch_shape<0, 256, 4, 1, 1, 1>(L, bps, stream);  // fmt: skip
     if (pk.single) return launch_shape<G, 256, 4, 2, 0, 1>(L, bps, stream);
+    if (pk.groups) return launch_shape<G, 256, 4, 3, 0, 1>(L, bps, stream);
     return launch_shape<G, 256, 4, 1, 0, 1>(L, bps, stream);
   }
   if constexpr (G == 0) {
     if (L.truth)  // truth rows: the analog instantiation of shape 0
-      return pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream) : launch_shape<0, 256, 4, 0, 1>(L, bps, stream);
+      return pk.groups ? launch_shape<0, 256, 4, 3, 1>(L, bps, stream)
+                       : (pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream)
+                                   : launch_shape<0, 256, 4, 0, 1>(L, bps, stream));  // fmt: skip
   }
+  if (pk.groups) return launch_shape<G, 256, 4, 3>(L, bps, stream);  // frame groups: shape 0 whatever the variant
   if (pk.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream);  // tori: shape 0 whatever the variant
   if (pk.single) switch (variant) {  // single-leaf solids: the scan of one leaf, no postfix program
       case 1: return launch_shape<G, 128, 8, 2>(L, bps, stream);
@@ -1262,6 +1270,7 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   sc->tab.assign(d->tab, d->tab + 2 * (size_t)d->n_tab);
   sc->has_torus = d->n_mesh > 0 || d->n_group > 0;  // the extended instantiation: tori, meshes, frame groups
   sc->clip = d->n_group > 0;  // the extended locate (frame groups, protrusion clips): no wavefront (its fill's locate)
+  sc->groups = d->n_group > 0;
   for (int l = 0; l < d->n_leaf; ++l) sc->has_torus = sc->has_torus || d->leaf_i[(size_t)l * LUMEN_LEAF_I] == 2;
   for (int v = 0; v < d->n_vol && !sc->clip; ++v) {  // a protrusion clip: the extended instantiation
     const int32_t* vr = d->vol_i + (size_t)v * LUMEN_VOL_I;
