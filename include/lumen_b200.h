@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 11
+#define LUMEN_B200_ABI_VERSION 12
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -76,11 +76,18 @@ enum { LUMEN_PROG_I = 2 };
 
 /* Surface table: row ints of LUMEN_ROW_I: model (0 reflect, 1 dielectric, 2 complex index), normal, glisur (the
    GLOSSY lobe: 0 the unified facet path, 1 GLISUR's on a metal, 2 GLISUR's reflecting or refracting facets),
-   far_opaque, per_normal, then one table index per column (LUMEN_COL_*) read at the photon energy */
+   far_opaque, per_normal, cover, then one table index per column (LUMEN_COL_*) read at the photon energy.
+   cover: the defensive mixture's outcomes of an edge row (src/lumen/transport/estimator.py:146 edge_floor): bit o set
+   for each outcome o (LUMEN_OUT_*) of the row type's support (src/lumen/build/lookup.py:999) when the row reads a
+   parameter with a defensive role (src/lumen/api.py:797 _edge_rows); 0 for every other row. At a crossing of such a
+   row each covered outcome whose reference probability is 0 is drawn at e / (1 - e) / n, e = 0.01
+   (src/lumen/transport/estimator.py:83 defensive). */
+enum { LUMEN_OUT_STRAIGHT = 0, LUMEN_OUT_REFRACT, LUMEN_OUT_SPECULAR, LUMEN_OUT_BACKSCATTER, LUMEN_OUT_GLOSSY,
+       LUMEN_OUT_DIFFUSE, LUMEN_N_OUT };
 enum { LUMEN_COL_R = 0, LUMEN_COL_T, LUMEN_COL_EFF, LUMEN_COL_PSPIKE, LUMEN_COL_PLOBE, LUMEN_COL_PBACK,
        LUMEN_COL_SIGMA, LUMEN_COL_POLISH, LUMEN_COL_NR, LUMEN_COL_NK, LUMEN_N_COL };
 enum { LUMEN_RI_MODEL = 0, LUMEN_RI_NORMAL = 1, LUMEN_RI_GLISUR = 2, LUMEN_RI_FAR_OPAQUE = 3,
-       LUMEN_RI_PER_NORMAL = 4, LUMEN_RI_COL = 6, LUMEN_ROW_I = 16 };
+       LUMEN_RI_PER_NORMAL = 4, LUMEN_RI_COVER = 5, LUMEN_RI_COL = 6, LUMEN_ROW_I = 16 };
 /* Medium ints, one table index each (-1: none), src/lumen/media/bulk.py:45 Medium with its channels in Geant4's order
    (bulk.py:21 CHANNEL_ORDER): the index (-1: opaque), the absorption length, the Rayleigh length; the Mie (G4OpMieHG)
    length and its lobe constants g_forward, g_backward, forward_ratio (MIEHG, MIEHG_FORWARD, MIEHG_BACKWARD,
@@ -282,8 +289,13 @@ typedef struct LumenControls {
 enum { LUMEN_H_LOST = 0, LUMEN_H_ABANDONED, LUMEN_H_ESCAPED, LUMEN_H_DISTANCE_CUT, LUMEN_H_ABSORBED_BULK,
        LUMEN_H_ABSORBED_SURFACE, LUMEN_H_ROULETTED, LUMEN_H_REWEIGHTED, LUMEN_H_TRUNCATED, LUMEN_H_PUSHED,
        LUMEN_H_START, LUMEN_N_HEALTH };
+/* Counts: photons ended, steps, deposits (records), photons cut at the vertex guard, MULTI the per-photon sensor sums
+   past a photon's first four (each photon's sum per sensor is exact whatever their number: the first four are kept in
+   registers, the rest in the call's moment table), ABORTED (the step budget ran out), RECORDS (the readout groups'
+   record count), MOMENT_LOST the sums that found the moment table full (each squared alone: the second moment is
+   then not exact; 0 in every call whose table is large enough). */
 enum { LUMEN_C_PHOTONS = 0, LUMEN_C_STEPS, LUMEN_C_DEPOSITS, LUMEN_C_TRUNCATED, LUMEN_C_MULTI, LUMEN_C_ABORTED,
-       LUMEN_C_RECORDS, LUMEN_N_COUNT };
+       LUMEN_C_RECORDS, LUMEN_C_MOMENT_LOST, LUMEN_N_COUNT };
 
 /* ------------------------------------------------------------------------------------ the readout groups */
 /* The histograms of src/lumen/readout/grid.py filled from the deposit records (src/lumen/readout/fill.py:88
@@ -378,18 +390,26 @@ int32_t lumen_b200_adjoint(const LumenScene* scene, const LumenRows* rows, const
 
 /* The words of the fixed device array lumen_b200_trace_static takes its scratch from (64 x 8 bytes). */
 #define LUMEN_STATIC_SCRATCH_WORDS 64
+/* The slots of its fixed moment table (16 bytes each: 1 MiB): the photons' per-sensor sums past their first four. */
+#define LUMEN_STATIC_MOMENT_SLOTS 65536
 
 /* lumen_b200_trace for callers that cannot allocate device memory during a call. Such callers include a framework
    whose pool owns all of the device's memory and forbids other allocations while it runs a step, and a loop that
    must not wait on the allocator. No counterpart in the reference: lumen's loop allocates through JAX.
    Same arguments, outputs and results as lumen_b200_trace; the caller still passes every input and output. The
-   call's own scratch (the photon counter, the abort flag and the step count: 3 of LUMEN_STATIC_SCRATCH_WORDS words)
-   comes from one fixed array in the library's device memory instead of an allocation, and a call whose scratch
-   would not fit that array is refused with LUMEN_ERR_ARG. Every GPU that loads the library holds the array until the
-   process exits. The first call on a device looks up the array's address there, with that device current, so make
-   that first call before any stream capture. All calls share the one array and leave their counts in it; each call
-   clears what must start at zero. Calls that overlap on the GPU (other streams, other host threads) race on the
-   array: run them one after another. */
+   controls' variant and blocks_per_sm pick the launch as there, except that the wavefront (whose slot pool is an
+   allocation) runs as the persistent shape 0. With LUMEN_F_ASYNC the call returns once its work is enqueued, and a
+   step budget that ran out shows in counts[LUMEN_C_ABORTED]; without it the call waits for the stream and reads
+   back the abort flag and the record count. The call's own scratch (4 of LUMEN_STATIC_SCRATCH_WORDS words: the
+   photon counter, the abort flag, the step count and the readout groups' record count) comes from one fixed array
+   in the library's device memory instead of an allocation, and a call whose scratch would not fit that array is
+   refused with LUMEN_ERR_ARG. The photons' sums past their first four sensors go to a fixed moment table of
+   LUMEN_STATIC_MOMENT_SLOTS slots; a sum that finds it full is squared alone and counted in
+   counts[LUMEN_C_MOMENT_LOST]. Every GPU that loads the library holds both arrays until the process exits. The
+   first call on a device looks up the arrays' addresses there, with that device current, so make that first call
+   before any stream capture. All calls share the arrays and leave their contents in them; each call clears what
+   must start at zero. Calls that overlap on the GPU (other streams, other host threads) race on the arrays: run
+   them one after another. */
 int32_t lumen_b200_trace_static(const LumenScene* scene, const LumenRows* rows, const LumenSource* source,
                                 uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
                                 const LumenControls* controls, LumenTallies* out, void* stream);

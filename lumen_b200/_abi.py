@@ -23,8 +23,8 @@ c_u64p = ctypes.POINTER(ctypes.c_uint64)
 MAX_GRAD = 8
 N_COL = 10
 N_HEALTH = 11
-N_COUNT = 7
-C_RECORDS = 6
+N_COUNT = 8
+C_PHOTONS, C_STEPS, C_DEPOSITS, C_TRUNCATED, C_MULTI, C_ABORTED, C_RECORDS, C_MOMENT_LOST = range(8)  # LUMEN_C_*
 ERR_RECORDS = 7
 MAX_AXES = 4
 MAX_GROUPS = 8
@@ -40,7 +40,7 @@ UNI_NX, UNI_NY = 257, 69
 UNI_WORDS = 4 * UNI_NX * UNI_NY + 2 * UNI_NY
 HEALTH = ("lost", "abandoned", "escaped", "distance_cut", "absorbed_bulk", "absorbed_surface", "rouletted",
           "reweighted", "truncated", "pushed", "start")  # fmt: skip
-COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted", "records")
+COUNTS = ("photons", "steps", "deposits", "truncated", "multi", "aborted", "records", "moment_lost")
 FEATURES = ("wavelength", "theta", "cos_incidence", "generation", "x", "y", "z", "rho")  # LUMEN_FEAT_* order
 SRC_POINT, SRC_TRACK, SRC_SCINT, SRC_CHERENKOV, SRC_SCINT_MATERIAL = 0, 1, 2, 3, 4
 SM_N, SM_SEGMENT, SM_RISES, SM_YIELD, SM_SPEC, SM_TAU, SM_RISE, SM_SHARE, SM_WORDS = 0, 1, 2, 3, 4, 7, 10, 13, 16

@@ -12,6 +12,7 @@ reference held, runs at nearby values share their random numbers (common random 
 from __future__ import annotations
 
 import math
+import warnings
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -231,7 +232,13 @@ def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):
     if gnames:
         jac = T.jac.cpu().numpy()
         grads = {k: (jac[..., i] if n_ev > 1 else jac[0, :, i]) for i, k in enumerate(gnames)}
-    prov = dict(seed=seed, samples=samples, engine="lumen_b200", steps_per_photon=cnt[1] / max(cnt[0], 1))
+    prov = dict(seed=seed, samples=samples, engine="lumen_b200", steps_per_photon=cnt[1] / max(cnt[0], 1),
+                moment_table_sums=int(cnt[A.C_MULTI]))  # fmt: skip
+    if cnt[A.C_MOMENT_LOST]:  # sums that found the moment table full were squared alone: the errors are not exact
+        warnings.warn(f"simulate: {int(cnt[A.C_MOMENT_LOST])} per-photon sensor sums found the moment table full; "
+                      "arrivals_error is approximate (run fewer photons per launch: chunk=)", RuntimeWarning,
+                      stacklevel=3)  # fmt: skip
+        prov["moment_lost"] = int(cnt[A.C_MOMENT_LOST])
     return Light(arr, err, mt, health, prov, groups, grads, diag)
 
 

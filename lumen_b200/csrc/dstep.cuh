@@ -346,6 +346,23 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
         ddet[p] = 0.0f;
       }
   }
+  // the one defensive mixture at an edge row (estimator.py:146 edge_floor, :83 defensive): each outcome of the row's
+  // support whose reference probability is 0 is drawn at e / (1 - e) / n (n of them), the stand-in row of a continue
+  // event included; re.probs holds the draw's probabilities from here on (a bulk step draws no outcome)
+  if (!scatter && row >= 0) {
+    const int cover = __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_COVER);
+    if (cover) {
+      int n_fl = 0;
+#pragma unroll
+      for (int o = 0; o < N_OUT; ++o) n_fl += ((cover >> o) & 1) && re.probs[o] <= 0.0f;
+      if (n_fl) {
+        const float eps = D_EDGE_SHARE / (float)n_fl;
+#pragma unroll
+        for (int o = 0; o < N_OUT; ++o)
+          if (((cover >> o) & 1) && re.probs[o] <= 0.0f) re.probs[o] = eps;
+      }
+    }
+  }
   float p_prop[N_OUT];
   float tot = 0.0f;
 #pragma unroll

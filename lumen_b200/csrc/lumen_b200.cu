@@ -6,7 +6,9 @@
 // next photon id from a global counter (one atomic per warp, ballot-compacted), so lanes stay busy as paths end at
 // different steps. Deposits go straight into FP64 per-sensor tallies (arrival, arrival x time, time histograms,
 // Jacobian); the per-photon second moment is formed from a four-entry per-thread cache of the photon's per-sensor
-// sums, squared when the photon ends; health fates and counters are reduced per block before their atomics.
+// sums, squared when the photon ends; a photon's sums past its first four sensors go to the call's moment table (a
+// hash of (photon, event x sensor) to its sum in HBM), squared by a pass after the launch, so the moment is exact for
+// any number of sensors; health fates and counters are reduced per block before their atomics.
 //
 // Numerics: compiled with -fmad=false; every fused multiply-add is an explicit fmaf, every elementary function the
 // library's own (dmath.cuh), so a photon's path is the CPU checker's bit for bit.
@@ -68,7 +70,42 @@ struct Tally {
   unsigned long long* counts;
   const double* cot;  // the adjoint's cotangent (E * S_) or null
   double* grads;      // the adjoint's output (P) or null
+  unsigned long long* mt_key;  // the moment table: keys (photon << 32 | event x sensor cell), MT_EMPTY when free
+  double* mt_sum;              // the photon's sum on that cell
+  unsigned mt_mask;            // slots - 1 (a power of two)
 };
+
+// The moment table. The second moment (run.py:483 _moment_adds) squares each photon's own sum per cell; a photon keeps
+// its first four sums in registers (PhotonTally) and the rest here: one slot per (photon, cell), claimed by a CAS and
+// then written only by the photon's own thread (its sum is the sequential sum of its deposits, as in registers).
+// k_moment_flush squares every slot into arrival2 and frees it after the launch. A slot is found within MT_PROBES
+// linear probes or the sum is lost (squared alone, counts[LUMEN_C_MOMENT_LOST]).
+#define MT_EMPTY 0xffffffffffffffffull
+#define MT_PROBES 64
+
+__device__ __forceinline__ int mt_add(const Tally& T, unsigned pid, unsigned cell, double v) {
+  const unsigned long long k = ((unsigned long long)pid << 32) | cell;
+  unsigned h = (unsigned)((k * 0x9E3779B97F4A7C15ull) >> 32) & T.mt_mask;
+  for (int p = 0; p < MT_PROBES; ++p) {
+    unsigned long long old = T.mt_key[h];  // a key once written stays for the launch: a non-empty read is final
+    if (old == MT_EMPTY) old = atomicCAS(T.mt_key + h, MT_EMPTY, k);
+    if (old == MT_EMPTY) { T.mt_sum[h] = v; return 1; }
+    if (old == k) { T.mt_sum[h] += v; return 1; }
+    h = (h + 1) & T.mt_mask;
+  }
+  return 0;
+}
+
+// squares every held sum into arrival2 and frees its slot (grid-stride over the table)
+__global__ void k_moment_flush(Tally T) {
+  for (size_t h = (size_t)blockIdx.x * blockDim.x + threadIdx.x; h <= T.mt_mask; h += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long k = T.mt_key[h];
+    if (k == MT_EMPTY) continue;
+    const double v = T.mt_sum[h];
+    atomicAdd(T.arrival2 + (unsigned)(k & 0xffffffffull), v * v);
+    T.mt_key[h] = MT_EMPTY;
+  }
+}
 
 struct Launch {
   Run R;
@@ -98,12 +135,14 @@ struct Pick {
 
 #define CACHE 4
 
-// the current photon's per-sensor sums (the second moment squares each at the photon's end); four entries, read and
-// written by constant index only, so they stay in registers
+// the current photon's first four per-sensor sums (the second moment squares each at the photon's end); read and
+// written by constant index only, so they stay in registers; pid is the photon's index in the call (the moment
+// table's key for its further sums)
 struct PhotonTally {
   int sensor[CACHE];
   double sum[CACHE];
   int n;
+  unsigned pid;
 };
 
 __device__ __forceinline__ void flush2(const Tally& T, int e, int s, double v) {
@@ -117,7 +156,6 @@ __device__ __forceinline__ void flush_all(const Tally& T, int e, PhotonTally& pt
     if (j < pt.n) flush2(T, e, pt.sensor[j], pt.sum[j]);
 }
 
-// adds one deposit to the tallies; returns 1 where the photon's sensor-sum cache was full (its oldest sum flushed)
 // adds every lane's non-zero health fates (times its row weight) to the block's shared sums: a warp sum first, then
 // one shared atomic per fate and warp (lanes with nothing to add pass zeros; every lane of the warp must call it)
 __device__ __forceinline__ void health_add(double* sh, const Dep& dep, double w0, int on) {
@@ -143,6 +181,8 @@ __device__ __forceinline__ void warp_add(double* sh, double v) {
   if ((threadIdx.x & 31) == 0) atomicAdd(sh, v);
 }
 
+// adds one deposit to the tallies; returns 0, or 1 where its sum went to the moment table (a sensor past the photon's
+// first four), or 2 where the table had no room (the deposit squared alone)
 template <int G>
 __device__ __forceinline__ int deposit(const Tally& T, int e, const Dep& dep, const float* dq, double w0,
                                        PhotonTally& pt) {
@@ -167,24 +207,22 @@ __device__ __forceinline__ int deposit(const Tally& T, int e, const Dep& dep, co
         for (int p = 0; p < T.P; ++p) atomicAdd(T.grads + p, c * (double)dq[p] * w0);
     }
   }
-  int found = 0, evicted = 0;
+  if (v == 0.0 || !T.arrival2) return 0;  // a deposit of 0 (a photon of weight 0) adds nothing to any sum
+  int found = 0;
 #pragma unroll
   for (int j = 0; j < CACHE; ++j)
     if (j < pt.n && pt.sensor[j] == s) { pt.sum[j] += v; found = 1; }
-  if (!found) {
-    if (pt.n == CACHE) {  // the oldest entry's sum is final: flush it and shift
-      flush2(T, e, pt.sensor[0], pt.sum[0]);
-#pragma unroll
-      for (int k = 1; k < CACHE; ++k) { pt.sensor[k - 1] = pt.sensor[k]; pt.sum[k - 1] = pt.sum[k]; }
-      pt.n = CACHE - 1;
-      evicted = 1;
-    }
+  if (found) return 0;
+  if (pt.n < CACHE) {
 #pragma unroll
     for (int j = 0; j < CACHE; ++j)
       if (j == pt.n) { pt.sensor[j] = s; pt.sum[j] = v; }
     pt.n += 1;
+    return 0;
   }
-  return evicted;
+  if (T.mt_key && mt_add(T, pt.pid, (unsigned)ix, v)) return 1;
+  atomicAdd(T.arrival2 + ix, v * v);
+  return 2;
 }
 
 __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
@@ -219,7 +257,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   __shared__ double sh_health[LUMEN_N_HEALTH];
   if (threadIdx.x < LUMEN_N_HEALTH) sh_health[threadIdx.x] = 0.0;
   __syncthreads();
-  unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0;
+  unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0, c_lost = 0;
   int budget_chunk = 0;
   for (;;) {
     unsigned need = __ballot_sync(FULL, !active);
@@ -243,6 +281,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
           ev = r.event;
           active = 1;
           pt.n = 0;
+          pt.pid = (unsigned)g;
           if (G > 0)
             for (int p = 0; p < L.R.P; ++p) dw[p] = 0.0f;
           if (ANALOG) {  // run.py:319: one uniform of its own stream, open with probability k (state.py:58)
@@ -267,7 +306,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
     if (active) {
       c_steps++;
       if (dep.sensor >= 0) {
-        c_multi += deposit<G>(L.T, ev, dep, dq, w0, pt);
+        const int m = deposit<G>(L.T, ev, dep, dq, w0, pt);
+        c_multi += m != 0;
+        c_lost += m == 2;
         c_dep++;
       }
       if (!ph.alive || ph.vertex >= L.R.max_vertices) {
@@ -309,6 +350,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   cv[LUMEN_C_DEPOSITS] = c_dep;
   cv[LUMEN_C_TRUNCATED] = c_trunc;
   cv[LUMEN_C_MULTI] = c_multi;
+  cv[LUMEN_C_MOMENT_LOST] = c_lost;
   if (threadIdx.x == 0 && L.abort_flag && *(volatile int*)L.abort_flag) cv[LUMEN_C_ABORTED] = 1ull;
 #pragma unroll
   for (int k = 0; k < LUMEN_N_COUNT; ++k) {
@@ -395,7 +437,7 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
   int in = i < V.W;
   int aborted = L.abort_flag && *(volatile int*)L.abort_flag;
   int act = in && !aborted && V.act[i];
-  unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0;
+  unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0, c_lost = 0;
   Photon ph;
   WaveExtra ex;
   float dw[G > 0 ? G : 1], dq[G > 0 ? G : 1];
@@ -415,7 +457,9 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
     d_post<G>(L.R, ph, dw, pr, q, dep, dq, an);
     c_steps++;
     if (dep.sensor >= 0) {
-      c_multi += deposit<G>(L.T, ex.ev, dep, dq, ex.w0, ex.pt);
+      const int m = deposit<G>(L.T, ex.ev, dep, dq, ex.w0, ex.pt);
+      c_multi += m != 0;
+      c_lost += m == 2;
       c_dep++;
     }
     if (!ph.alive || ph.vertex >= L.R.max_vertices) {
@@ -452,6 +496,7 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
         ex.ev = r.event;
         ex.pad = 0;
         ex.pt.n = 0;
+        ex.pt.pid = (unsigned)g;
         if (G > 0)
           for (int p = 0; p < L.R.P; ++p) dw[p] = 0.0f;
         act = 1;
@@ -475,6 +520,7 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
   cv[LUMEN_C_DEPOSITS] = c_dep;
   cv[LUMEN_C_TRUNCATED] = c_trunc;
   cv[LUMEN_C_MULTI] = c_multi;
+  cv[LUMEN_C_MOMENT_LOST] = c_lost;
   cv[LUMEN_N_COUNT] = (unsigned long long)act;  // the live slots
 #pragma unroll
   for (int k = 0; k < LUMEN_N_COUNT + 1; ++k) {
@@ -937,6 +983,29 @@ static int launch_bin(const Launch& L, const Pick& pk, const LumenTallies* out, 
   return 0;
 }
 
+// the moment table's slots for n photons: n / 8 rounded up to a power of two, at least 2^16 (16 bytes a slot); the
+// photons of the benchmark's LAr box hold about 0.03 sums each past their first four, the tank's none
+static size_t moment_slots(int64_t n) {
+  size_t want = (size_t)(n / 8), s = (size_t)1 << 16;
+  while (s < want) s <<= 1;
+  return s;
+}
+
+static int launch_moment_flush(const Tally& T, cudaStream_t stream) {
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  k_moment_flush<<<sms * 8, 256, 0, stream>>>(T);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int check_cells(const Tally& T) {
+  if ((unsigned long long)T.E * (unsigned long long)T.S_ >= (1ull << 32))
+    return set_err(LUMEN_ERR_ARG, "tallies: events x sensors must stay below 2^32");
+  return 0;
+}
+
 static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
                      cudaStream_t stream, int variant = 0, int bps = 0, int async = 0) {
   if (variant == LUMEN_VARIANT_WAVEFRONT && async)
@@ -956,10 +1025,9 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
   // scratch: the photon counter, the abort flag, the steps used, the wavefront's live slots and the record count (one
   // small allocation per call)
   const int groups = out && out->n_groups > 0;
-  if (groups) {
-    int gs = check_groups(L.R.S.n_sensor, out);
-    if (gs) return gs;
-  }
+  int st0 = 0;
+  if (groups && (st0 = check_groups(L.R.S.n_sensor, out))) return st0;
+  if ((st0 = check_cells(T))) return st0;
   unsigned long long* scratch = nullptr;
   CK(cudaMallocAsync((void**)&scratch, 5 * sizeof(unsigned long long), stream));
   CK(cudaMemsetAsync(scratch, 0, 5 * sizeof(unsigned long long), stream));
@@ -990,6 +1058,16 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
     T.health = out->health;
     T.counts = out->counts;
   }
+  // the moment table (the photons' sums past their first four sensors), every key free
+  unsigned long long* mt = nullptr;
+  if (T.arrival2 && L.n > 0) {
+    const size_t slots = moment_slots(L.n);
+    CK(cudaMallocAsync((void**)&mt, slots * 16, stream));
+    CK(cudaMemsetAsync(mt, 0xff, slots * 8, stream));
+    T.mt_key = mt;
+    T.mt_sum = (double*)(mt + slots);
+    T.mt_mask = (unsigned)(slots - 1);
+  }
   int st = 0;
   if (L.n > 0) {
     if (L.R.P > 0 || cot) {
@@ -1006,6 +1084,10 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
                                               : launch_trace<0>(L, pk, variant, bps, stream);
       if (st) return st;
     }
+  }
+  if (mt) {
+    if ((st = launch_moment_flush(T, stream))) return st;
+    CK(cudaFreeAsync(mt, stream));
   }
   if (groups && (st = launch_bin(L, pk, out, stream))) return st;
   if (async) {  // enqueue only: the abort flag reaches counts[LUMEN_C_ABORTED] on the device
@@ -1033,30 +1115,38 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
 // array's name as an address (it names a host-side stand-in); each device's address is looked up once, with that
 // device current, by cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned long long g_static_scratch[LUMEN_STATIC_SCRATCH_WORDS];
+// its moment table: keys, then sums (LUMEN_STATIC_MOMENT_SLOTS each, 16 bytes a slot)
+static __device__ __align__(256) unsigned long long g_static_moment[2 * LUMEN_STATIC_MOMENT_SLOTS];
 static const int STATIC_SCRATCH_NEED = 4;  // photon counter, abort flag, steps used, record count
 static std::mutex g_static_mu;
-static void* g_static_addr[256];
+static void* g_static_addr[256][2];
 
-static int static_scratch(unsigned long long** out) {
+static int static_scratch(unsigned long long** out, unsigned long long** moment) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 256) return set_err(LUMEN_ERR_NO_DEVICE, "trace_static: device index out of range");
   std::lock_guard<std::mutex> lock(g_static_mu);
-  if (!g_static_addr[dev]) {
-    void* p = nullptr;
+  if (!g_static_addr[dev][0]) {
+    void *p = nullptr, *m = nullptr;
     CK(cudaGetSymbolAddress(&p, g_static_scratch));
-    g_static_addr[dev] = p;
+    CK(cudaGetSymbolAddress(&m, g_static_moment));
+    g_static_addr[dev][0] = p;
+    g_static_addr[dev][1] = m;
   }
-  *out = (unsigned long long*)g_static_addr[dev];
+  *out = (unsigned long long*)g_static_addr[dev][0];
+  *moment = (unsigned long long*)g_static_addr[dev][1];
   return 0;
 }
 
-// run_trace with the scratch of the fixed array (no allocation, no free)
-static int run_trace_static(Launch& L, Pick pk, const LumenTallies* out, cudaStream_t stream) {
+// run_trace with the scratch and moment table of the fixed arrays (no allocation, no free); variant and bps as in
+// run_trace (the wavefront, whose slot pool is an allocation, runs as the persistent shape 0); async: enqueue only
+static int run_trace_static(Launch& L, Pick pk, const LumenTallies* out, cudaStream_t stream, int variant, int bps,
+                            int async) {
   if (STATIC_SCRATCH_NEED > LUMEN_STATIC_SCRATCH_WORDS)
     return set_err(LUMEN_ERR_ARG, "trace_static: the call needs more scratch than LUMEN_STATIC_SCRATCH_WORDS");
-  unsigned long long* scratch = nullptr;
-  int st = static_scratch(&scratch);
+  if (variant == LUMEN_VARIANT_WAVEFRONT) variant = 0;
+  unsigned long long *scratch = nullptr, *moment = nullptr;
+  int st = static_scratch(&scratch, &moment);
   if (st) return st;
   Tally& T = L.T;
   T.E = out->n_events > 0 ? out->n_events : 1;
@@ -1080,8 +1170,14 @@ static int run_trace_static(Launch& L, Pick pk, const LumenTallies* out, cudaStr
   T.counts = out->counts;
   const int groups = out->n_groups > 0;
   if (groups && (st = check_groups(L.R.S.n_sensor, out))) return st;
-  // the array keeps the previous call's counts: clear the words this call reads before they are written
+  if ((st = check_cells(T))) return st;
+  // the arrays keep the previous call's contents: clear the words this call reads before they are written, and free
+  // every slot of the moment table
   CK(cudaMemsetAsync(scratch, 0, STATIC_SCRATCH_NEED * sizeof(unsigned long long), stream));
+  CK(cudaMemsetAsync(moment, 0xff, LUMEN_STATIC_MOMENT_SLOTS * sizeof(unsigned long long), stream));
+  T.mt_key = moment;
+  T.mt_sum = (double*)(moment + LUMEN_STATIC_MOMENT_SLOTS);
+  T.mt_mask = LUMEN_STATIC_MOMENT_SLOTS - 1;
   L.next = scratch;
   L.abort_flag = (int*)(scratch + 1);
   L.steps_used = scratch + 2;
@@ -1091,11 +1187,13 @@ static int run_trace_static(Launch& L, Pick pk, const LumenTallies* out, cudaStr
     L.R.rec_n = scratch + 3;
   }
   if (L.n > 0) {
-    if (L.R.P > 0) st = launch_trace<LUMEN_MAX_GRAD>(L, pk, 0, 0, stream);
-    else st = launch_trace<0>(L, pk, 0, 0, stream);
+    if (L.R.P > 0) st = launch_trace<LUMEN_MAX_GRAD>(L, pk, variant, bps, stream);
+    else st = launch_trace<0>(L, pk, variant, bps, stream);
     if (st) return st;
+    if ((st = launch_moment_flush(T, stream))) return st;
   }
   if (groups && (st = launch_bin(L, pk, out, stream))) return st;
+  if (async) return 0;  // enqueue only: the abort flag reaches counts[LUMEN_C_ABORTED] on the device
   int flag = 0;
   unsigned long long n_rec = 0;
   CK(cudaMemcpyAsync(&flag, L.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -1124,7 +1222,8 @@ int32_t lumen_b200_trace_static(const LumenScene* sc, const LumenRows* rows, con
   Pick pk;
   int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
-  return run_trace_static(L, pk, out, (cudaStream_t)stream);
+  return run_trace_static(L, pk, out, (cudaStream_t)stream, c ? c->variant : 0, c ? c->blocks_per_sm : 0,
+                          c ? (c->flags & LUMEN_F_ASYNC) != 0 : 0);
 }
 
 int32_t lumen_b200_abi_version(void) { return LUMEN_B200_ABI_VERSION; }

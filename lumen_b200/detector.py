@@ -276,13 +276,15 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
                 row = O.surface_row(surf, is_sensor, far_opq, 1.0 if per_normal else None)
                 row.sensor = is_sensor
                 row.per_normal = per_normal
+                if surf is O.ABSORBER:  # the reference's ABSORBER type: no outcome, no parameter (types.py:441)
+                    row.cover = 0
                 row_key[key] = len(rows)
                 rows.append(row)
             row_of[ca, cb] = row_key[key]
     row_i = np.zeros((len(rows), 16), np.int32)
     col_tab = {}  # one table per (surface, column): every row of a surface reads (and moves with) the same values
     for r, row in enumerate(rows):
-        row_i[r, 0:5] = [row.model, row.normal, row.glisur, row.far_opaque, row.per_normal]
+        row_i[r, 0:6] = [row.model, row.normal, row.glisur, row.far_opaque, row.per_normal, row.cover]
         for c, col in enumerate(O.COLUMNS):
             if col not in row.cols or (col == "eff" and not row.sensor):
                 row_i[r, 6 + c] = neutral[col]

@@ -34,6 +34,8 @@ COLUMNS = ("R", "T", "eff", "p_spike", "p_lobe", "p_back", "sigma_alpha", "polis
 NEUTRAL = {"R": 0.0, "T": 0.0, "eff": 0.0, "p_spike": 0.0, "p_lobe": 0.0, "p_back": 0.0, "sigma_alpha": 0.1,
            "polish": 0.0, "nr": 1.0, "nk": 0.0}  # fmt: skip
 MODEL_REFLECT, MODEL_DIELECTRIC, MODEL_COMPLEX = 0, 1, 2
+# the outcomes, in the reference's order (src/lumen/surfaces/outcomes.py:30 NAMES)
+STRAIGHT, REFRACT, SPECULAR, BACKSCATTER, GLOSSY, DIFFUSE = range(6)
 
 
 def table(v, energy=None):
@@ -166,6 +168,29 @@ class Row:
     name: str = ""
     sensor: bool = False
     per_normal: int = 0  # read for a sensor model applying its QE after tracking: eff 1, deposits carry 1 / A_n
+    cover: int = 0  # the defensive mixture's outcomes (bit per outcome) of an edge row, else 0 (``edge_cover``)
+
+
+def edge_cover(surf: OpticalSurface, sensor: bool, support) -> int:
+    """Return the cover mask of a surface row: the bits of ``support`` (the row type's possible outcomes,
+    src/lumen/surfaces/types.py:413-513 and their ``fixed`` / ``transmitting`` rules) when the row reads a parameter
+    with a defensive role, else 0.
+
+    The reference decides edge rows by structure (src/lumen/api.py:797 ``_edge_rows``): a row is one when a property
+    the detector gives (a parameter key; an omitted Geant4 default is no key) is read through a column whose role is
+    "zero" (R, T, eff, the unified constants; types.py:329-336) or "support" (GLISUR's polish, read wherever a facet
+    path is). EFFICIENCY is read on a sensor only (types.py:557 ``no_detection``).
+    """
+    keyed = (surf.reflectivity is not None or surf.transmittance is not None
+             or (sensor and surf.efficiency is not None)
+             or any(v is not None for v in (surf.specularspike, surf.specularlobe, surf.backscatter)))  # fmt: skip
+    glisur_path = surf.model == "glisur" and surf.finish != "polished" and surf.polish < 1.0
+    if not (keyed or glisur_path):
+        return 0
+    m = 0
+    for o in support:
+        m |= 1 << o
+    return m
 
 
 def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=None) -> Row:
@@ -180,14 +205,19 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
         cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
                 "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff,
                 "p_spike": 1.0 if surf.finish == "polishedfrontpainted" else 0.0, "p_lobe": 0.0, "p_back": 0.0}  # fmt: skip
-        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+        # support: the straight share (T is read at its default), and the finish's half of the split (types.py:425)
+        sup = (STRAIGHT, SPECULAR if surf.finish == "polishedfrontpainted" else DIFFUSE)
+        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+                   cover=edge_cover(surf, sensor, sup))  # fmt: skip
     if surf.type == "dielectric_metal" and (surf.rindex is not None or surf.kindex is not None):
         # PHOTOCATHODE (types.py:455): the complex index's Fresnel reflectance, specular; the rest detected with eff
         if surf.rindex is None or surf.kindex is None or surf.finish != "polished":
             raise NotImplementedError(f"surface {surf.name}: a complex index needs RINDEX and KINDEX, polished")
         cols = {"nr": surf.rindex, "nk": surf.kindex, "eff": eff,
                 "T": 0.0 if surf.transmittance is None else surf.transmittance}  # fmt: skip
-        return Row(MODEL_COMPLEX, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+        sup = (SPECULAR,) + ((STRAIGHT,) if surf.transmittance is not None else ())  # types.py:455, :494
+        return Row(MODEL_COMPLEX, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+                   cover=edge_cover(surf, sensor, sup))  # fmt: skip
     if surf.type == "dielectric_dielectric":
         if surf.finish != "polished" and surf.model == "glisur" and surf.polish < 1.0:
             # GLISUR_DIELECTRIC (types.py:463): the cuts, then below R the GLISUR facet path that reflects or refracts
@@ -195,22 +225,28 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
             cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
                     "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff, "p_spike": 0.0,
                     "p_lobe": 1.0, "p_back": 0.0, "polish": float(surf.polish)}  # fmt: skip
-            return Row(MODEL_REFLECT, glisur=2, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+            return Row(MODEL_REFLECT, glisur=2, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+                       cover=edge_cover(surf, sensor, (GLOSSY, STRAIGHT)))  # fmt: skip
         if surf.finish != "polished" and not (surf.model == "glisur" and surf.polish >= 1.0):
             raise NotImplementedError("dielectric_dielectric ground with the unified model is not built")
         cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
                 "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff}  # fmt: skip
-        return Row(MODEL_DIELECTRIC, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+        # DIELECTRIC_RT (types.py:444): refract, specular, straight
+        return Row(MODEL_DIELECTRIC, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+                   cover=edge_cover(surf, sensor, (REFRACT, SPECULAR, STRAIGHT)))  # fmt: skip
     # dielectric_metal
     R = 1.0 if surf.reflectivity is None else surf.reflectivity
     cols = {"R": R, "eff": eff, "T": 0.0 if surf.transmittance is None else surf.transmittance}
+    tr = (STRAIGHT,) if surf.transmittance is not None else ()  # types.transmitting (types.py:494)
     if surf.model == "glisur" and surf.finish != "polished" and surf.polish < 1.0:
         # GLISUR_METAL (types.py:459): R into the GLISUR facet path of radius 1 - polish
         cols.update({"p_spike": 0.0, "p_lobe": 1.0, "p_back": 0.0, "polish": float(surf.polish)})
-        return Row(MODEL_REFLECT, glisur=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+        return Row(MODEL_REFLECT, glisur=1, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+                   cover=edge_cover(surf, sensor, (GLOSSY, *tr)))  # fmt: skip
     if surf.finish == "polished" or surf.model == "glisur":
         cols["p_spike"] = 1.0  # polished, or GLISUR at polish 1: the mirror (types.py:573 SPECULAR_METAL)
-        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+                   cover=edge_cover(surf, sensor, (SPECULAR, *tr)))  # fmt: skip
     ss = 0.0 if surf.specularspike is None else surf.specularspike
     sl = 0.0 if surf.specularlobe is None else surf.specularlobe
     bs = 0.0 if surf.backscatter is None else surf.backscatter
@@ -219,7 +255,11 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
     if not normal and not (facets.SIGMA_MIN <= surf.sigma_alpha <= facets.SIGMA_MAX):
         raise ValueError(f"surface {surf.name}: sigma_alpha {surf.sigma_alpha} outside the unified tables' span "
                          f"[{facets.SIGMA_MIN:.5f}, {facets.SIGMA_MAX}] rad (or exactly 0)")  # fmt: skip
-    return Row(MODEL_REFLECT, normal=normal, far_opaque=int(far_opaque), cols=cols, name=surf.name)
+    # UNIFIED_METAL_NORMAL (types.py:471: its support rule reads fixed constants only, and these are read values)
+    # or UNIFIED_METAL (types.py:467)
+    sup = (SPECULAR, BACKSCATTER, DIFFUSE) if normal else (SPECULAR, BACKSCATTER, GLOSSY, DIFFUSE)
+    return Row(MODEL_REFLECT, normal=normal, far_opaque=int(far_opaque), cols=cols, name=surf.name,
+               cover=edge_cover(surf, sensor, (*sup, *tr)))  # fmt: skip
 
 
 class Pool:

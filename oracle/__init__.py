@@ -45,6 +45,7 @@ def lib():
                                             ctypes.c_int32, ctypes.c_int32, A.c_f32p]
         L.lumen_oracle_threefry.argtypes = [ctypes.c_uint32] * 4 + [P(ctypes.c_uint32)]
         L.lumen_oracle_math.argtypes = [ctypes.c_int32, A.c_f32p, ctypes.c_int64, A.c_f32p]
+        L.lumen_oracle_set_rule_020.argtypes = [ctypes.c_int32]
         L.lumen_oracle_fresnel.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_basis.argtypes = [A.c_f32p, ctypes.c_int64, A.c_f32p]
         L.lumen_oracle_facet_path.argtypes = [ctypes.c_float, A.c_f32p, ctypes.c_uint32, ctypes.c_uint32,
@@ -83,6 +84,19 @@ def uniforms(key, ids, vertex, n):
 
 MATH = {"exp": 0, "log": 1, "sin2pi": 2, "cos2pi": 3, "acos": 4, "cbrt": 5, "erfinv": 6, "sin": 7, "cos": 8,
         "dipole_cos": 9, "gaussian": 10}  # fmt: skip
+
+
+class rule_020:
+    """Within the block the checker runs lumen 0.2.0's reference weight at a covered draw of a surface that absorbs
+    every photon at the reference (kept as it was; lumen 0.2.1 multiplies it by e / (1 - e)): the rule of the
+    reference's published tutorial run."""  # noqa: D205, N801
+
+    def __enter__(self):
+        self.was = lib().lumen_oracle_set_rule_020(1)
+        return self
+
+    def __exit__(self, *exc):
+        lib().lumen_oracle_set_rule_020(self.was)
 
 
 def math(fn, x):

@@ -9,6 +9,8 @@
 
 #define O_FOUR_PI 12.5663706143591729539f
 #define O_DEFENSIVE 0.01f      /* the defensive mixture's share (src/lumen/rules/choices.py:113) */
+/* its covering weight e / (1 - e), formed in double and rounded once to float32 (estimator.py:106) */
+#define O_EDGE_SHARE ((float)(0.01 / (1.0 - 0.01)))
 #define O_EPS32 1.1920928955078125e-7f
 #define O_WLS_TRIES 100.0f     /* G4OpWLS's redraws of an energy below the absorbed one (spectra.py:22) */
 

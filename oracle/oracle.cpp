@@ -161,6 +161,10 @@ static inline void o_dmed(const ORun* R, int mi, float lam, const OMed* m, float
   }
 }
 
+/* lumen 0.2.0's reference weight at a covered draw (lumen_oracle_set_rule_020): checker-only, so that the published
+   run of that version can be reproduced; every engine path runs the current rule */
+static int g_rule_020 = 0;
+
 /* one step (step.py:516); NF the navigator's precision */
 template <class NF>
 static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
@@ -221,8 +225,22 @@ static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
     for (int p = 0; p < P; ++p) { for (int o = 0; o < O_N_OUT; ++o) dprobs[p * O_N_OUT + o] = 0.0f; ddet[p] = 0.0f; }
   }
   float p_draw[O_N_OUT], p_prop[O_N_OUT];
+  for (int o = 0; o < O_N_OUT; ++o) p_draw[o] = re.probs[o];
+  /* the one defensive mixture at an edge row (estimator.py:146 edge_floor, :83 defensive): each outcome of the row's
+     support whose reference probability is 0 is drawn at e / (1 - e) / n (n of them); the stand-in row of a continue
+     event included, as the reference reads it */
+  const int cover = row >= 0 ? D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_COVER] : 0;
+  if (cover) {
+    int n_fl = 0;
+    for (int o = 0; o < O_N_OUT; ++o) n_fl += ((cover >> o) & 1) && p_draw[o] <= 0.0f;
+    if (n_fl) {
+      const float eps = O_EDGE_SHARE / (float)n_fl;
+      for (int o = 0; o < O_N_OUT; ++o)
+        if (((cover >> o) & 1) && p_draw[o] <= 0.0f) p_draw[o] = eps;
+    }
+  }
   float tot = 0.0f;
-  for (int o = 0; o < O_N_OUT; ++o) { p_draw[o] = re.probs[o]; tot = o == 0 ? p_draw[0] : tot + p_draw[o]; }
+  for (int o = 0; o < O_N_OUT; ++o) tot = o == 0 ? p_draw[0] : tot + p_draw[o];
   for (int o = 0; o < O_N_OUT; ++o) p_prop[o] = tot > 0.0f ? p_draw[o] / tot : 0.0f;
   int oc_ = o_choose(p_prop, O_N_OUT, o_uniform(vkey, 2));
   int os_ = oc_ > 0 ? oc_ : 0;
@@ -444,6 +462,12 @@ static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
     int ok = q.hit && drawn && row >= 0;
     for (int a = 0; a < 3; ++a) nx_x[a] = ph->x[a] + q.t * ph->d[a];
     float r_o = drawn ? (p_prop[os_] != 0.0f ? p_draw[os_] / p_prop[os_] : 0.0f) : 0.0f;
+    if (g_rule_020 && drawn && cover) { /* lumen 0.2.0: a covered draw at a surface absorbing every photon at the
+                                           reference left the reference weight as it was (CHANGELOG.md, 0.2.1) */
+      float s0 = 0.0f;
+      for (int o = 0; o < O_N_OUT; ++o) s0 += re.probs[o];
+      if (s0 <= 0.0f) r_o = 1.0f;
+    }
     wr = ph->wr * (reach_ref != 0.0f ? 1.0f : 0.0f) * att_r * r_o * out_wd;
     float w_at = ph->w * rr;
     float s_cont = 0.0f;
@@ -767,12 +791,11 @@ typedef struct OTally {
   std::vector<long long> counts;
 } OTally;
 
-#define O_CACHE 4
-typedef struct OPhotonSums { int sensor[O_CACHE]; double sum[O_CACHE]; int n; } OPhotonSums;
+static inline int s_out_of(const OTally* T, int s) { return s < 0 || s >= T->S_; }
 
-static void o_flush2(OTally* T, int e, OPhotonSums* ps, int j) {
-  T->arrival2[(size_t)e * T->S_ + ps->sensor[j]] += ps->sum[j] * ps->sum[j];
-}
+/* a photon's per-sensor sums, in the order its sensors first took light: the second moment adds the square of each at
+   the photon's end (run.py:483 _moment_adds: the photon's own cell total squared, exact over any number of sensors) */
+typedef std::vector<std::pair<int, double>> OPhotonSums;
 
 /* a thread's readout groups: the cells, and the photons' records when the caller asks for them (photon id, record,
    the photon's row weight and event) */
@@ -817,7 +840,6 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double pushed = 0.0;
   OPhotonSums ps;
-  ps.n = 0;
   int n_dep = 0, first_sensor = -1;
   double sum_q = 0.0, sum_qt = 0.0;
   long long steps = 0;
@@ -828,7 +850,15 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
     steps++;
     for (int k = 0; k < 8; ++k) acc[k] += (double)dep.fates[k];
     pushed += (double)dep.pushed * w0;
-    if (dep.sensor >= 0) {
+    if (dep.sensor >= 0 && (e < 0 || e >= T->E || s_out_of(T, dep.sensor))) { /* an event or sensor out of range:
+                                                                                  counted, not tallied (the engine's rule) */
+      n_dep++;
+      T->counts[LUMEN_C_DEPOSITS] += 1;
+      if (gc) recs.push_back(dep.rec);
+      if (first_sensor < 0) first_sensor = dep.sensor;
+      sum_q += (double)dep.q;
+      sum_qt += (double)dep.q * (double)dep.time;
+    } else if (dep.sensor >= 0) {
       int s = dep.sensor;
       double v = (double)dep.q * w0;
       size_t ix = (size_t)e * T->S_ + s;
@@ -839,20 +869,12 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
         if (b >= 0.0f && b < (float)T->nb) T->hist[ix * T->nb + (size_t)b] += v;
       }
       for (int p = 0; p < R->P; ++p) T->jac[ix * R->P + p] += (double)dep.dq[p] * w0;
-      int j = 0;
-      while (j < ps.n && ps.sensor[j] != s) ++j;
-      if (j == ps.n) {
-        if (ps.n == O_CACHE) { /* the oldest entry's sum is final: flush it */
-          o_flush2(T, e, &ps, 0);
-          for (int k = 1; k < O_CACHE; ++k) { ps.sensor[k - 1] = ps.sensor[k]; ps.sum[k - 1] = ps.sum[k]; }
-          ps.n -= 1;
-          T->counts[LUMEN_C_MULTI] += 1;
-        }
-        j = ps.n++;
-        ps.sensor[j] = s;
-        ps.sum[j] = 0.0;
+      if (v != 0.0) { /* a deposit of 0 (a photon of weight 0) adds nothing to any sum */
+        size_t j = 0;
+        while (j < ps.size() && ps[j].first != s) ++j;
+        if (j == ps.size()) ps.push_back({s, 0.0});
+        ps[j].second += v;
       }
-      ps.sum[j] += v;
       n_dep++;
       if (gc) recs.push_back(dep.rec);
       if (first_sensor < 0) first_sensor = s;
@@ -861,7 +883,8 @@ static void o_photon(const ORun* R, const ORow* row, OKey key, int64_t gid, OTal
       T->counts[LUMEN_C_DEPOSITS] += 1;
     }
   }
-  for (int j = 0; j < ps.n; ++j) o_flush2(T, e, &ps, j);
+  if (ps.size() > 4) T->counts[LUMEN_C_MULTI] += (long long)ps.size() - 4; /* the sums past the photon's first four */
+  for (const auto& sv : ps) T->arrival2[(size_t)e * T->S_ + sv.first] += sv.second * sv.second;
   if (gc && !recs.empty()) {
     if (e >= 0 && e < T->E) o_bin_photon(R->S.D, gc->out, recs, w0, e, T->S_, &gc->T);
     if (gc->keep)
@@ -976,6 +999,15 @@ int32_t lumen_oracle_uniforms(uint32_t k0, uint32_t k1, const int64_t* ids, int6
 
 /* elementwise math for the golden checks: fn 0 exp, 1 log, 2 sin 2 pi x, 3 cos 2 pi x, 4 acos, 5 cbrt, 6 erfinv,
    7 sin, 8 cos, 9 dipole_cos, 10 gaussian */
+/* 1: run lumen 0.2.0's rule for the reference weight after a covered draw at a surface whose reference probabilities
+   are all 0 (the weight kept; 0.2.1 multiplies it by e / (1 - e) / n, src/lumen/transport/estimator.py:83); 0: the
+   current rule. Returns the previous setting. Not thread-safe: set it before a trace. */
+int32_t lumen_oracle_set_rule_020(int32_t on) {
+  int32_t was = g_rule_020;
+  g_rule_020 = on != 0;
+  return was;
+}
+
 int32_t lumen_oracle_math(int32_t fn, const float* x, int64_t n, float* out) {
   for (int64_t i = 0; i < n; ++i) {
     float s, c;

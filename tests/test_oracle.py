@@ -91,6 +91,25 @@ def test_toy_tank_matches_the_published_run(toy_run):
     np.testing.assert_allclose(T.arrival_t[0] / arr, PUB_TIMES, atol=0.0006)
     q = np.interp(400.0, *TOY_QE)
     np.testing.assert_allclose(arr * q, PUB_PE, atol=0.051)
+    # the current rule's deposit records: every cathode crossing draws its covered specular outcome (an edge row,
+    # estimator.py:146), and that photon goes on with weight 0 and its reference weight times e / (1 - e), so some
+    # reach a second cathode (a record of q = 0) before the roulette ends them
+    assert T.counts[A.C_DEPOSITS] == 5735
+
+
+def test_toy_tank_published_record_count_under_the_rule_of_its_version():
+    """The published run reports 'records': 5921 (docs/tutorial/first-hour.md:111). It was made by lumen 0.2.0, whose
+    covered draw at a surface absorbing every photon at the reference kept the photon's reference weight
+    (CHANGELOG.md, 0.2.1 "A photon in a closed cavity of absorbing walls now ends"): its zero-weight photons bounce on
+    between facing cathodes until the water or the tank's wall ends them. Run under that rule the checker makes
+    exactly the published count, and the arrivals do not move (those photons carry weight 0)."""
+    det = detectors.toy_tank()
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    n = 1 << 18
+    with oracle.rule_020():
+        T, _ = oracle.trace(det, KEY0, n, source=src, samples=n)
+    assert T.counts[A.C_DEPOSITS] == 5921
+    np.testing.assert_allclose(T.arrival[0], PUB_ARRIVALS, atol=0.0051)
 
 
 def test_weight_balance(toy_run):
