@@ -25,7 +25,7 @@ N_COL = 10
 N_HEALTH = 11
 N_COUNT = 8
 C_PHOTONS, C_STEPS, C_DEPOSITS, C_TRUNCATED, C_MULTI, C_ABORTED, C_RECORDS, C_MOMENT_LOST = range(8)  # LUMEN_C_*
-ERR_RECORDS = 7
+ERR_ARG, ERR_CUDA, ERR_SCENE, ERR_STEP_BUDGET, ERR_NO_DEVICE, ERR_NOT_SUPPORTED, ERR_RECORDS = range(1, 8)
 MAX_AXES = 4
 MAX_GROUPS = 8
 REC_WORDS = 20
@@ -198,11 +198,17 @@ class RecordsOverflow(EngineError):
     """The deposit records outgrew the scratch (LUMEN_ERR_RECORDS; src/lumen/run.py:236 RecordsOverflow)."""
 
 
+class StepBudgetExhausted(EngineError):
+    """The call's device step budget ran out before every photon ended (LUMEN_ERR_STEP_BUDGET): the kernel stopped
+    handing out photons and returned; the tallies hold the photons that ended before it."""  # noqa: D205, D209
+
+
 def check(status: int):
     """Raise the engine's error for a non-zero status."""
     if status != 0:
         msg = engine().lumen_b200_last_error().decode(errors="replace")
-        raise (RecordsOverflow if status == ERR_RECORDS else EngineError)(status, msg)
+        cls = {ERR_RECORDS: RecordsOverflow, ERR_STEP_BUDGET: StepBudgetExhausted}.get(status, EngineError)
+        raise cls(status, msg)
 
 
 def key_of_seed(seed: int):

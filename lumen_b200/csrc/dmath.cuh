@@ -14,7 +14,7 @@
 #include <stdint.h>
 
 #define L_DEV __device__ __forceinline__
-#define L_CALL __device__ __noinline__  // large functions: one copy shared by every call site (instruction cache)
+#define L_CALL static __device__ __noinline__  // large functions: one copy shared by every call site (instruction cache)
 
 namespace lb {
 

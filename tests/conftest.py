@@ -29,3 +29,11 @@ def built():
     from lumen_b200 import make as build
 
     return build.build()
+
+
+@pytest.fixture(scope="session", autouse=True)
+def checker_built():
+    """The CPU checker (oracle/), rebuilt by make when a source is newer than its library."""
+    import oracle
+
+    oracle.build()

@@ -240,6 +240,30 @@ def test_wavefront_tallies_match(which, tank, facet_lar, built):
         assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
 
 
+@pytest.mark.parametrize("variant", [0, A.VARIANT_WAVEFRONT])
+def test_second_moment_past_four_sensors_matches(variant, lar, built):
+    """The LAr box's photons deposit on many sensors: the sums past a photon's first four go to the moment table, and
+    arrival2 (each photon's per-sensor sum squared) is the checker's exact one; the table never fills."""
+    src = sources.Scintillation(position=[(0.3, 0.2, -0.4), (-1.0, 1.0, 0.5)], lam=128.0, tau=(6.0, 1500.0),
+                                fraction=0.25)  # fmt: skip
+    T, O = _tallies(lar, src, 1 << 14, controls=A.controls(variant=variant))
+    np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL, atol=1e-15)
+    cnt = T.counts.cpu().numpy()
+    assert cnt[A.C_MULTI] == int(O.counts[A.C_MULTI]) > 0
+    assert cnt[A.C_MOMENT_LOST] == 0
+
+
+def test_cathode_reflectivity_derivative_at_zero_matches(toy, built):
+    """The toy tank's cathodes (R = 0, an edge row): the covered specular draw carries d/dR; the checker's Jacobian."""
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    c = A.controls(grad_tabs=[toy.params_index["surfaces/CathodeSurface/R"]])
+    for variant in (0, A.VARIANT_WAVEFRONT):
+        c.variant = variant
+        T, O = _tallies(toy, src, 1 << 16, controls=c)
+        np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+        assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+
+
 def test_wavefront_refuses_asynchronous_calls(tank, built):
     eng = _engine(tank)
     src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam=400.0)

@@ -174,3 +174,56 @@ def test_enclosing_sensor_counts_everything_whatever_the_scattering():
     assert abs(T.arrival[0, 0] - 1.0) < 4 * err, (T.arrival[0, 0], err)
     assert abs(T.health[5] - 1.0) < 1e-6  # every photon's weight ends absorbed at the cathode
     assert T.counts[1] / T.counts[0] > 3  # it scattered
+
+
+def test_second_moment_is_exact_past_four_sensors():
+    """arrival2 is the sum over photons of each photon's own per-sensor sum squared (run.py:483 _moment_adds), for
+    any number of sensors a photon deposits on: the LAr box's photons scatter often and deposit their expected
+    detection on many of its 120 sensors. Restated here in float64 from the checker's deposit records (photon order,
+    each photon's chain ending at its head), and the count of sums past each photon's first four."""
+    from lumen_b200.readout import Grid
+
+    det = detectors.lar_box()
+    src = sources.Scintillation(position=[(0.3, 0.2, -0.4)], lam=128.0, tau=(6.0, 1500.0), fraction=0.25)
+    n = 1 << 12
+    T, _ = oracle.trace(det, KEY0, n, source=src, samples=n,
+                        groups={"sensor": Grid.bands((100.0, 200.0), nt=2, t0=0.0, dt=1.0)}, deposits=1 << 18)
+    nrec = int(T.counts[A.C_RECORDS])
+    assert 0 < nrec <= len(T.deposits)
+    d = T.deposits[:nrec]
+    head = d[:, 17] == 1
+    photon = np.concatenate([[0], np.cumsum(head)[:-1]])  # records are in photon order, a head closes a photon
+    w0 = d[head, 18].view(np.float32).astype(np.float64)[photon]
+    sensor = d[:, 1].view(np.int32).astype(np.int64)
+    v = d[:, 2].view(np.float32).astype(np.float64) * w0
+    keys, inv = np.unique(photon * det.n_sensor + sensor, return_inverse=True)
+    sums = np.zeros(len(keys))
+    np.add.at(sums, inv, v)
+    want = np.zeros(det.n_sensor)
+    np.add.at(want, keys % det.n_sensor, sums**2)
+    np.testing.assert_allclose(T.arrival2[0], want, rtol=1e-10, atol=1e-300)
+    live = np.unique(keys[sums != 0.0] // det.n_sensor, return_counts=True)[1]
+    assert live.max() > 4  # photons with more than four sensors: the register sums alone would not hold them
+    assert int(T.counts[A.C_MULTI]) == int(np.maximum(live - 4, 0).sum())
+
+
+def test_cathode_reflectivity_derivative_at_zero():
+    """At a cathode of reflectivity 0 the reference draws its specular outcome from the defensive cover (an edge row,
+    estimator.py:146): the photon goes on with weight 0 and the derivative of its weight in R, so the arrivals'
+    derivative in R at R = 0 counts the light a reflection would send to the other PMTs. It matches the one-sided
+    difference at the reference held at R = 0 (the same paths, weights moving with R)."""
+    det = detectors.toy_tank()
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    n = 1 << 16
+    key = "surfaces/CathodeSurface/R"
+    c = A.controls(grad_tabs=[det.params_index[key]])
+    T, _ = oracle.trace(det, KEY0, n, source=src, samples=n, controls=c)
+    h = 1e-3
+    hi, _ = oracle.trace(det, KEY0, n, source=src, samples=n, pool_live=det.pool_with({key: h}), pool_ref=det.pool)
+    lo, _ = oracle.trace(det, KEY0, n, source=src, samples=n)
+    jac = T.jac[0, :, 0]
+    fd = (hi.arrival[0] - lo.arrival[0]) / h
+    # d/dR of (1 - R) eff at the cathode is -1 per arrival; the reflections a cathode sends to the others add to it
+    refl = jac + lo.arrival[0]
+    assert (refl > -1e-9 * lo.arrival[0]).all() and refl[0] > 0 and refl[1] > 0  # PMTs 0 and 1 face each other
+    np.testing.assert_allclose(fd, jac, rtol=2e-3)
