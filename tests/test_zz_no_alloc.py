@@ -87,9 +87,10 @@ def _pool_high():
 
 
 def _pool_reset(pool):
+    from cuda.bindings import driver
     from cuda.bindings import runtime as rt
 
-    err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh, rt.cuuint64_t(0))
+    err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh, driver.cuuint64_t(0))
     assert err == rt.cudaError_t.cudaSuccess
 
 
