@@ -220,21 +220,25 @@ def _planes_leaf(planes, origin=(0.0, 0.0, 0.0)) -> Leaf:
     return Leaf(False, og=o.copy(), oq=o.copy(), N=N, H=H)
 
 
-def _frustum(z1, r1, z2, r2, caps=True, selector=True) -> Leaf:
-    """rho <= r(z), r linear from r1 at z1 to r2 at z2 (z1 < z2), origin at the section's middle: the quadric
-    rho^2 - (r0 + k z)^2 <= 0 with the nappe r0 + k z >= 0 (solids.py:253 q_frustum)."""  # noqa: D205
-    zm = 0.5 * (z1 + z2)
-    o = np.array([0.0, 0.0, zm])
-    N, H = ([[0, 0, 1.0], [0, 0, -1.0]], [z2 - zm, -(z1 - zm)]) if caps else ([], [])
-    if abs(r2 - r1) < CYLINDER_REL * max(1.0, abs(r1)):
-        return Leaf(True, A=np.diag([1.0, 1.0, 0.0]), c=-r1 * r1, oq=o, og=o.copy(),
-                    N=np.asarray(N, float).reshape(-1, 3), H=np.asarray(H, float))  # fmt: skip
-    k = (r2 - r1) / (z2 - z1)
-    r0 = 0.5 * (r1 + r2)
-    if selector:
-        N, H = [*N, [0.0, 0.0, -k]], [*H, r0]
-    return Leaf(True, A=np.diag([1.0, 1.0, -k * k]), b=np.array([0.0, 0.0, -r0 * k]), c=-r0 * r0, oq=o,
-                og=o.copy(), N=np.asarray(N, float).reshape(-1, 3), H=np.asarray(H, float))  # fmt: skip
+def _frustum(z_lo, r_lo, z_hi, r_hi, caps=True, one_nappe=True) -> Leaf:
+    """The solid of revolution about z whose radius runs affinely from r_lo at z_lo to r_hi at z_hi (z_lo < z_hi):
+    a G4Cons, or one section of a G4Polycone. Taken about the slab's middle m, with the slope s and the middle
+    radius r_m, its surface is x^2 + y^2 = (r_m + s z)^2: the quadric x^2 + y^2 - s^2 z^2 - 2 r_m s z - r_m^2 <= 0,
+    which holds two nappes meeting at the apex; ``one_nappe`` keeps the one of positive radius (the plane
+    r_m + s z >= 0). Equal radii make it the cylinder x^2 + y^2 <= r^2. ``caps``: the slab's planes."""  # noqa: D205
+    half = 0.5 * (z_hi - z_lo)
+    centre = np.array([0.0, 0.0, 0.5 * (z_lo + z_hi)])
+    normals, offsets = ([(0.0, 0.0, 1.0), (0.0, 0.0, -1.0)], [half, half]) if caps else ([], [])
+    if abs(r_hi - r_lo) < CYLINDER_REL * max(1.0, abs(r_lo)):
+        quad = dict(A=np.diag([1.0, 1.0, 0.0]), c=-(r_lo * r_lo))
+    else:
+        slope, r_m = (r_hi - r_lo) / (z_hi - z_lo), 0.5 * (r_lo + r_hi)
+        quad = dict(A=np.diag([1.0, 1.0, -(slope * slope)]), b=np.array([0.0, 0.0, -(r_m * slope)]), c=-(r_m * r_m))
+        if one_nappe:
+            normals.append((0.0, 0.0, -slope))
+            offsets.append(r_m)
+    return Leaf(True, oq=centre, og=centre.copy(), N=np.asarray(normals, float).reshape(-1, 3),
+                H=np.asarray(offsets, float), **quad)  # fmt: skip
 
 
 def _cone_theta(theta, up=True) -> Leaf:
@@ -439,29 +443,36 @@ class Hype(Solid):
         return low
 
 
-def _merge_affine(zs, rel=1e-12):
-    """[(z, rmin, rmax)] without the interior z-planes across which both radii stay affine in z (one straight
-    section: Geant4's RemoveRedundantVertices; solids.py:528 merge_affine)."""  # noqa: D205
-    out = list(zs[:1])
-    for k in range(1, len(zs)):
-        if k + 1 < len(zs):
-            (za, ia, oa), (zb, ib, ob), (zc, ic, oc) = out[-1], zs[k], zs[k + 1]
-            if (zb - za) * (zc - zb) > 0:
-                f = (zb - za) / (zc - za)
-                tol = rel * max(1.0, abs(za), abs(zc), abs(oa), abs(oc))
-                if abs(ia + f * (ic - ia) - ib) <= tol and abs(oa + f * (oc - oa) - ob) <= tol:
-                    continue
-        out.append(zs[k])
-    return out
+def _profile(zplanes, rel=1e-12):
+    """A G4Polycone / G4Polyhedra profile as arrays (z, inner, outer) from its z-planes [(rmin, rmax, z)], with every
+    interior plane dropped that lies on the straight line of its kept neighbours for both radii, z strictly between
+    them: Geant4 builds the solid from G4ReduciblePolygon after RemoveRedundantVertices, so such a plane is no
+    section boundary (the tolerance is ``rel`` of the profile's scale there)."""  # noqa: D205
+    arr = np.asarray(zplanes, float).reshape(-1, 3)
+    inner, outer, z = arr[:, 0], arr[:, 1], arr[:, 2]
+    kept = [0]
+    for i in range(1, len(z) - 1):
+        a, c = kept[-1], i + 1
+        between = (z[i] - z[a]) * (z[c] - z[i]) > 0
+        if between:
+            t = (z[i] - z[a]) / (z[c] - z[a])
+            scale = rel * max(1.0, abs(z[a]), abs(z[c]), abs(outer[a]), abs(outer[c]))
+            if all(abs(r[a] + t * (r[c] - r[a]) - r[i]) <= scale for r in (inner, outer)):
+                continue
+        kept.append(i)
+    if len(z) > 1:
+        kept.append(len(z) - 1)
+    return z[kept], inner[kept], outer[kept]
 
 
-def _sections(zs):
-    for (za, ia, oa), (zb, ib, ob) in zip(zs[:-1], zs[1:], strict=True):
-        if abs(zb - za) < Z_TOL:
+def _slabs(z, inner, outer):
+    """The profile's sections between consecutive z-planes, each as (z_lo, z_hi, inner_lo, inner_hi, outer_lo,
+    outer_hi) with z_lo below z_hi; a section thinner than Z_TOL (a radius step at one z) bounds nothing."""  # noqa: D205
+    for i in range(len(z) - 1):
+        lo, hi = (i, i + 1) if z[i] <= z[i + 1] else (i + 1, i)
+        if z[hi] - z[lo] < Z_TOL:
             continue
-        if zb < za:
-            za, ia, oa, zb, ib, ob = zb, ib, ob, za, ia, oa
-        yield za, ia, oa, zb, ib, ob
+        yield z[lo], z[hi], inner[lo], inner[hi], outer[lo], outer[hi]
 
 
 def _union_all(parts, lo, hi) -> Lowered:
@@ -482,16 +493,16 @@ class Polycone(Solid):
     dphi: float = FULL
 
     def lower(self):
-        zs = _merge_affine([(z, rmin, rmax) for rmin, rmax, z in self.zplanes])
-        big = max(z[2] for z in zs)
-        lo, hi = (-big, -big, min(z[0] for z in zs)), (big, big, max(z[0] for z in zs))
-        secs = []
-        for za, ia, oa, zb, ib, ob in _sections(zs):
-            s = _one(_frustum(za, oa, zb, ob), lo, hi)
-            if ia > 0 or ib > 0:
-                s = _combine(3, s, _unbounded(_frustum(za, ia, zb, ib, caps=False)), lo, hi)
-            secs.append(s)
-        return with_phi(_union_all(secs, lo, hi), self.sphi, FULL if self.dphi <= 0.0 else self.dphi)
+        z, inner, outer = _profile(self.zplanes)
+        r = float(outer.max())
+        lo, hi = (-r, -r, float(z.min())), (r, r, float(z.max()))
+        parts = []
+        for z0, z1, i0, i1, o0, o1 in _slabs(z, inner, outer):
+            part = _one(_frustum(z0, o0, z1, o1), lo, hi)
+            if i0 > 0 or i1 > 0:  # the bore: the inner frustum taken out, unbounded across the slab's planes
+                part = _combine(3, part, _unbounded(_frustum(z0, i0, z1, i1, caps=False)), lo, hi)
+            parts.append(part)
+        return with_phi(_union_all(parts, lo, hi), self.sphi, FULL if self.dphi <= 0.0 else self.dphi)
 
 
 @dataclass
@@ -504,30 +515,31 @@ class Polyhedra(Solid):
     sphi: float = 0.0
     dphi: float = FULL
 
-    def _section(self, za, aa, zb, ab, caps):
-        dphi = FULL if self.dphi <= 0.0 else self.dphi
-        k = (ab - aa) / (zb - za)
-        planes = []
-        for i in range(self.nsides):
-            ph = self.sphi + (i + 0.5) * dphi / self.nsides
-            planes.append((np.array([math.cos(ph), math.sin(ph), -k]), aa - k * za))
+    def _section(self, z_lo, a_lo, z_hi, a_hi, caps):
+        """One section as a plane leaf: side k (its outward normal at the middle of its phi step) keeps the points
+        whose distance from the axis along that normal is within the apothem, affine in z from a_lo to a_hi."""  # noqa: D205
+        span = FULL if self.dphi <= 0.0 else self.dphi
+        slope = (a_hi - a_lo) / (z_hi - z_lo)
+        mids = self.sphi + (np.arange(self.nsides) + 0.5) * (span / self.nsides)
+        normals = np.column_stack([np.cos(mids), np.sin(mids), np.full(self.nsides, -slope)])
+        planes = [(nv, a_lo - slope * z_lo) for nv in normals]
         if caps:
-            planes += [((0, 0, 1.0), zb), ((0, 0, -1.0), -za)]
-        return _planes_leaf(planes, (0.0, 0.0, 0.5 * (za + zb)))
+            planes += [((0.0, 0.0, 1.0), z_hi), ((0.0, 0.0, -1.0), -z_lo)]
+        return _planes_leaf(planes, (0.0, 0.0, 0.5 * (z_lo + z_hi)))
 
     def lower(self):
-        zs = _merge_affine([(z, rmin, rmax) for rmin, rmax, z in self.zplanes])
+        z, inner, outer = _profile(self.zplanes)
         full = self.dphi >= FULL - FULL_PHI_TOL or self.dphi <= 0.0
-        dph = (FULL if self.dphi <= 0 else self.dphi) / self.nsides
-        big = max(z[2] for z in zs) / math.cos(0.5 * min(dph, math.pi - 1e-6))
-        lo, hi = (-big, -big, min(z[0] for z in zs)), (big, big, max(z[0] for z in zs))
-        secs = []
-        for za, ia, oa, zb, ib, ob in _sections(zs):
-            s = _one(self._section(za, oa, zb, ob, True), lo, hi)
-            if ia > 0 or ib > 0:
-                s = _combine(3, s, _unbounded(self._section(za, ia, zb, ib, False)), lo, hi)
-            secs.append(s)
-        low = _union_all(secs, lo, hi)
+        step = (FULL if self.dphi <= 0 else self.dphi) / self.nsides
+        r = float(outer.max()) / math.cos(0.5 * min(step, math.pi - 1e-6))  # the corners lie beyond the apothem
+        lo, hi = (-r, -r, float(z.min())), (r, r, float(z.max()))
+        parts = []
+        for z0, z1, i0, i1, o0, o1 in _slabs(z, inner, outer):
+            part = _one(self._section(z0, o0, z1, o1, True), lo, hi)
+            if i0 > 0 or i1 > 0:
+                part = _combine(3, part, _unbounded(self._section(z0, i0, z1, i1, False)), lo, hi)
+            parts.append(part)
+        low = _union_all(parts, lo, hi)
         return low if full else _combine(2, low, phi_wedge(self.sphi, self.dphi), lo, hi)
 
 
@@ -620,14 +632,20 @@ class GenericTrap(Solid):
     dz: float
 
     def lower(self):
-        V = np.asarray([(x, y, -self.dz) for x, y in self.verts_xy[:4]] + [(x, y, self.dz) for x, y in self.verts_xy[4:]])
-        for i in range(4):
-            j = (i + 1) % 4
-            P = V[[i, j, j + 4, i + 4]]
-            nrm = np.cross(P[2] - P[0], P[3] - P[1])
-            if np.linalg.norm(nrm) > 0 and abs(np.dot(nrm / np.linalg.norm(nrm), P[1] - P[0])) > 1e-9:
+        xy = np.asarray(self.verts_xy, float).reshape(8, 2)
+        zcol = np.repeat([-self.dz, self.dz], 4)[:, None]
+        V = np.hstack([xy, zcol])  # rows 0..3 the -dz face, 4..7 the +dz face, in the same order
+        low_ring = np.arange(4)
+        nxt = np.roll(low_ring, -1)
+        sides = np.stack([low_ring, nxt, nxt + 4, low_ring + 4], 1)  # each side: an edge below and the one above it
+        for quad in sides:
+            p = V[quad]
+            # four points are coplanar when the volume they span is 0: a twisted side is a hyperbolic paraboloid
+            vol = abs(np.linalg.det(np.stack([p[1] - p[0], p[2] - p[0], p[3] - p[0]])))
+            scale = max(np.linalg.norm(p - p[0], axis=1).max(), 1e-300) ** 3
+            if vol > 1e-9 * scale:
                 raise NotImplementedError("GenericTrap with a twisted (non-planar) face")
-        return convex_polytope(V, [(0, 1, 2, 3), (4, 5, 6, 7)] + [(i, (i + 1) % 4, (i + 1) % 4 + 4, i + 4) for i in range(4)])
+        return convex_polytope(V, [tuple(low_ring), tuple(low_ring + 4), *map(tuple, sides)])
 
 
 @dataclass
