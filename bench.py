@@ -95,6 +95,15 @@ class Clocks:
             self.p.wait(timeout=10)
             self.t.join(timeout=10)
 
+    def per_step(self, bounds):
+        """The median SM clock (MHz) sampled inside each (start, end) host-time interval of ``bounds`` (None: no
+        sample fell in it: a step shorter than the 200 ms sampling period)."""  # noqa: D205, D209
+        out = []
+        for a, b in bounds:
+            v = [float(r[0]) for t, r in self.rows if a <= t <= b and len(r) >= 6 and r[0].replace(".", "").isdigit()]
+            out.append(float(np.median(v)) if v else None)
+        return out
+
     def summary(self):
         t0, t1 = self.t0 or 0.0, (self.t1 or time.monotonic()) + 0.25
         rows = [r for t, r in self.rows if t0 <= t <= t1 and len(r) >= 6]
@@ -162,7 +171,105 @@ def batched_events(seed=2024, n_events=256):
     return np.asarray(st), np.asarray(dr), np.asarray(ln), counts
 
 
-def run_batched(dev, det, reps=3):
+def per_sensor(arrival, arrival2, photons_per_event):
+    """Per-sensor arrivals summed over events and their MC errors (each event's moment error, src/lumen/readout/
+    grid.py:48, added in quadrature)."""  # noqa: D205, D209
+    from lumen_b200.api import moment_error
+
+    n = np.asarray(photons_per_event, np.float64).reshape(-1, 1)
+    err = moment_error(arrival2, arrival, n)
+    return arrival.sum(0), np.sqrt((err**2).sum(0))
+
+
+def chi2_vs_checker(eng, det, src, n_ev, gt=(), m=1 << 17, flags=0):
+    """The GPU's arrivals of photon ids 0 .. m - 1 (seed 0) against the checker's of the same ids drawn with seed 1:
+    two independent samples of the same photons' law. Returns chi^2 / ndf over the sensors that see light (per-sensor
+    sums over events, combined MC errors), ndf, and the largest relative difference of the GPU and the checker on the
+    SAME photons (seed 0), which parity makes ~1e-12."""  # noqa: D205, D209
+    import torch
+
+    import oracle
+    from lumen_b200 import _abi as A
+    from lumen_b200.engine import DeviceSource, DeviceTallies
+
+    ds = DeviceSource(src, m, eng.device, det)
+    c = A.controls(grad_tabs=list(gt), flags=flags)
+    T = DeviceTallies(det.n_sensor, n_ev, 0, 0.0, 1.0, len(gt), eng.device)
+    eng.trace(A.key_of_seed(0), m, source=ds, controls=c, tallies=T)
+    torch.cuda.synchronize(eng.device)
+    ev_first = ds.ev_first.cpu().numpy()
+    per_ev = np.diff(np.clip(ev_first, 0, m))
+    threads = os.cpu_count() or 1
+    a0, e0 = per_sensor(T.arrival.cpu().numpy(), T.arrival2.cpu().numpy(), per_ev)
+    O1, _ = oracle.trace(det, A.key_of_seed(1), m, source=src, samples=m, controls=c, n_events=n_ev, threads=threads)
+    a1, e1 = per_sensor(O1.arrival, O1.arrival2, per_ev)
+    O0, _ = oracle.trace(det, A.key_of_seed(0), m, source=src, samples=m, controls=c, n_events=n_ev, threads=threads)
+    var = e0**2 + e1**2
+    ok = var > 0
+    chi2 = float(((a0 - a1)[ok] ** 2 / var[ok]).sum())
+    ndf = int(ok.sum())
+    same = float(np.max(np.abs(T.arrival.cpu().numpy() - O0.arrival) / np.maximum(np.abs(O0.arrival), 1e-300)))
+    return {"chi2_ndf": chi2 / max(ndf, 1), "ndf": ndf, "photons": m, "checker_seed": 1,
+            "same_photons_max_rel_diff": same}
+
+
+def mc_error(arrival, arrival2, per_ev):
+    """The median relative per-PMT MC error over the sensors that see light (per-sensor sums over events)."""
+    a, e = per_sensor(arrival, arrival2, per_ev)
+    ok = a > 0
+    return float(np.median(e[ok] / a[ok])) if ok.any() else None
+
+
+# the reference's published run of the tutorial tank (docs/tutorial/first-hour.md:101-111): arrivals and their errors
+PUBLISHED_TOY = ([394.54, 913.75, 547.76, 501.74, 515.31, 528.14, 320.36, 340.68],
+                 [17.22, 26.23, 20.30, 19.43, 19.69, 19.94, 15.51, 16.03])  # fmt: skip
+
+
+def run_toy(dev, reps=10, with_cpu=True):
+    """The shipped toy tank (8 PMTs): one isotropic 400 nm point at (0, 0, 0.1) m, n_photons 2e5, 2^18 photons, seed 0,
+    plain forward; arrivals +- MC error per PMT and their chi^2 / ndf against the reference's published table."""  # noqa: D205
+    import torch
+
+    from lumen_b200 import _abi as A
+    from lumen_b200 import detectors, sources
+    from lumen_b200.api import moment_error
+    from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
+
+    det = detectors.toy_tank()
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+    n = 1 << 18
+    eng = Engine(det, dev)
+    ds = DeviceSource(src, n, dev)
+    c = A.controls()
+    T = DeviceTallies(det.n_sensor, 1, 0, 0.0, 1.0, 0, dev)
+    eng.trace(A.key_of_seed(0), n, source=ds, controls=c, tallies=T)
+    ms = []
+    for _ in range(reps):
+        T.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.trace(A.key_of_seed(0), n, source=ds, controls=c, tallies=T)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    arr = T.arrival.cpu().numpy()[0]
+    err = moment_error(T.arrival2.cpu().numpy()[0], arr, n)
+    cnt = T.counts.cpu().numpy()
+    pa, pe = np.asarray(PUBLISHED_TOY[0]), np.asarray(PUBLISHED_TOY[1])
+    m = float(np.median(ms))
+    out = {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
+           "steps_per_photon": float(cnt[1] / cnt[0]), "records": int(cnt[2]),
+           "arrivals": [round(float(x), 2) for x in arr], "arrivals_error": [round(float(x), 2) for x in err],
+           "mc_error": float(np.median(err / arr)),
+           "chi2_ndf_vs_published": float((((arr - pa) ** 2) / (err**2 + pe**2)).sum() / len(pa)),
+           "published": "docs/tutorial/first-hour.md:101-111 (lumen 0.2.0)"}  # fmt: skip
+    if with_cpu:
+        out["vs_checker"] = chi2_vs_checker(eng, det, src, 1, m=n)
+    eng.close()
+    return out
+
+
+def run_batched(dev, det, reps=3, with_cpu=True):
     """The batched forward + adjoint: one fused launch (arrivals and their Jacobian per event) under a CUDA graph."""
     import torch
 
@@ -204,15 +311,20 @@ def run_batched(dev, det, reps=3):
     cnt = T.counts.cpu().numpy()
     jac = T.jac.cpu().numpy()
     m = float(np.median(ms))
+    per_ev = np.diff(ds.ev_first.cpu().numpy())
+    err = mc_error(T.arrival.cpu().numpy(), T.arrival2.cpu().numpy(), per_ev)
+    vs = chi2_vs_checker(eng, det, src, ds.n_events, gt) if with_cpu else None
+    del g
     eng.close()
     return {"value": n / (m * 1e-3), "unit": "photons/s", "events": int(ds.n_events), "photons_per_launch": n,
+            "mc_error": err, "vs_checker": vs,
             "ms_per_launch": m, "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "gradients": names,
             "graph": True, "autotune": {"variant": variant, "blocks_per_sm": bps,
                                         "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}},
             "jacobian_norm": float(np.abs(jac).sum()), "aborted": int(cnt[5])}  # fmt: skip
 
 
-def run_tank_adjoint(dev, src, n, reps=2):
+def run_tank_adjoint(dev, src, n, reps=2, with_cpu=True):
     """The tank forward + Jacobian with its wall switched to ground unified, sigma_alpha 0.1: derivatives in the
     absorption and Rayleigh lengths, the wall reflectivity and its sigma_alpha (the facet path's score) in the same
     launch (the 2000 PMT efficiencies' derivatives are the arrivals: after tracking)."""  # noqa: D205
@@ -247,16 +359,18 @@ def run_tank_adjoint(dev, src, n, reps=2):
     cnt = T.counts.cpu().numpy()
     m = float(np.median(ms))
     jac = T.jac.cpu().numpy()[0]
+    err = mc_error(T.arrival.cpu().numpy(), T.arrival2.cpu().numpy(), [n])
+    vs = chi2_vs_checker(eng, det, src, 1, gt) if with_cpu else None
     eng.close()
     return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
-            "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
+            "mc_error": err, "vs_checker": vs, "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
             "autotune": {"variant": variant, "blocks_per_sm": bps,
                          "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}},
             "jacobian_abs_sum": [float(x) for x in np.abs(jac).sum(0)]}  # fmt: skip
 
 
-def run_lar(dev, n, reps=2):
+def run_lar(dev, n, reps=1, with_cpu=True):
     """The liquid-argon box: 10^4 scintillation points, forward + Jacobian over the cage reflectivity and the
     Rayleigh length (the sensor efficiencies' derivatives are the arrivals: after tracking). The cage and cathode are
     ground unified with sigma_alpha 0.1."""  # noqa: D205
@@ -290,9 +404,12 @@ def run_lar(dev, n, reps=2):
         ms.append(e0.elapsed_time(e1))
     cnt = T.counts.cpu().numpy()
     m = float(np.median(ms))
+    err = mc_error(T.arrival.cpu().numpy(), T.arrival2.cpu().numpy(), np.diff(ds.ev_first.cpu().numpy()))
+    vs = chi2_vs_checker(eng, det, src, ds.n_events, gt) if with_cpu else None
     eng.close()
     return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
+            "mc_error": err, "vs_checker": vs, "moment_table_sums": int(cnt[4]), "moment_lost": int(cnt[7]),
             "points": 10000, "gradients": names, "arrivals_sum": float(T.arrival.sum().item()),
             "autotune": {"variant": variant, "blocks_per_sm": bps,
                          "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}}}  # fmt: skip
@@ -309,7 +426,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched and liquid-argon workloads")
-    ap.add_argument("--lar-photons", type=int, default=1 << 24)
+    ap.add_argument("--lar-photons", type=int, default=1 << 26)
     ap.add_argument("--variant", type=int, default=0, help="the headline workload's launch variant (3: wavefront)")
     args = ap.parse_args()
 
@@ -341,7 +458,7 @@ def main():
     import torch
 
     from lumen_b200 import _abi as A
-    from lumen_b200 import api
+    from lumen_b200 import api, distributed
     from lumen_b200 import make as engine_build
     from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
 
@@ -350,7 +467,7 @@ def main():
     dev = torch.device("cuda", local)
     eng = Engine(det, dev)
     key = A.key_of_seed(0)
-    first = rank * n  # this rank's photon ids
+    first, n_rank = distributed.shard_range(n * world, rank, world)  # this rank's contiguous photon ids
     ds = DeviceSource(src, n * world, dev)
     T = DeviceTallies(det.n_sensor, 1, 200, 0.0, 1.0, 0, dev)
     c = A.controls(variant=args.variant)
@@ -359,12 +476,8 @@ def main():
 
     def one_step():
         T.zero_()
-        eng.trace(key, n, source=ds, first_id=first, controls=c, tallies=T, stream=stream)
-        if world > 1:
-            import torch.distributed as dist
-
-            for t in (T.arrival, T.arrival_t, T.arrival2, T.hist, T.health):
-                dist.all_reduce(t)
+        distributed.trace_shard(eng, key, first, n_rank, source=ds, controls=c, tallies=T, stream=stream)
+        distributed.all_reduce_tallies(T)  # one NCCL all-reduce of every tally (nothing with one rank)
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     # the clock sampler starts before the warm-up and samples on through the timed steps
@@ -379,11 +492,15 @@ def main():
 
             dist.barrier()
         torch.cuda.synchronize(dev)
+        bounds = []  # each step's host-time interval (the device is idle between steps: a sync after each)
         for k in range(args.steps):
             flush.fill_(float(k))
+            t_a = time.monotonic()
             ev[k][0].record(stream)
             one_step()
             ev[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+            bounds.append((t_a, time.monotonic()))
         torch.cuda.synchronize(dev)
     ms = [a.elapsed_time(b) for a, b in ev]
     cnt = T.counts.cpu().numpy()
@@ -422,14 +539,21 @@ def main():
                          "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-photon launch "
                                          "of k_trace<0,256,4,2,0,0> on this workload (6.24 GB), scaled by photons"},
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            # one launch of the persistent loop per step (the wavefront's rounds are counted by no host-side number)
-            "gpu_launches": args.steps if args.variant != 3 else None, "launch_variant": args.variant,
+            # per step: the persistent loop and the moment table's pass (the wavefront's rounds are counted by no
+            # host-side number)
+            "gpu_launches": 2 * args.steps if args.variant != 3 else None, "launch_variant": args.variant,
             "clocks": clk.summary(), "ms_steps": [round(x, 3) for x in ms],
+            "sm_mhz_steps": clk.per_step(bounds), "mc_error": mc_error(T.arrival.cpu().numpy(),
+                                                                       T.arrival2.cpu().numpy(), [n * world]),
             "arrivals_sum": float(light.arrivals.sum())}  # fmt: skip
+    if rank == 0 and not args.no_cpu:
+        line["vs_checker"] = chi2_vs_checker(eng, det, src, 1)
     if rank == 0 and not args.no_extra:
-        line["tank_fwd_adjoint"] = run_tank_adjoint(dev, src, n)
-        line["batched_fwd_adjoint"] = run_batched(dev, det)
-        line["lar_fwd_adjoint"] = run_lar(dev, args.lar_photons)
+        cpu = not args.no_cpu
+        line["toy_tank"] = run_toy(dev, with_cpu=cpu)
+        line["tank_fwd_adjoint"] = run_tank_adjoint(dev, src, n, with_cpu=cpu)
+        line["batched_fwd_adjoint"] = run_batched(dev, det, with_cpu=cpu)
+        line["lar_fwd_adjoint"] = run_lar(dev, args.lar_photons, with_cpu=cpu)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_reference(args, det, src, n)
     if world > 1:

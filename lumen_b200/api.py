@@ -115,9 +115,12 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     analog record thinned by detection at the groups' efficiency and acceptance). Not differentiable; at one set of
     values (no ``reference``); each source row at most one photon (samples >= the photons emitted).
     """
-    eng = _engine(det, device)
     live = det.pool_with(params)
     ref = None if reference is None else det.pool_with({**(params or {}), **reference})
+    det.check_values(live, "simulate")  # a concrete value outside its range is refused (build/values.py:203)
+    if ref is not None:
+        det.check_values(ref, "simulate: reference")
+    eng = _engine(det, device)
     eng.set_pools(live, ref)
     ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22, variant=None, jump=True) | (controls or {})
     gnames = list(gradients)
@@ -220,9 +223,13 @@ def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):
     err = moment_error(arr2, arr, nn)
     with np.errstate(invalid="ignore", divide="ignore"):
         mt = np.where(arr > 0, arr_t / np.where(arr > 0, arr, 1.0), np.nan)
+    # the output cells that are not finite (the reference's exact-sum cells that are NaN, src/lumen/api.py:469)
+    cells = [arr, arr_t, arr2] + [x.cpu().numpy() for x in (T.hist, T.jac) if x is not None]
+    nonfinite = int(sum(np.count_nonzero(~np.isfinite(c)) for c in cells))
     health = Health(lost=h[0], abandoned=h[1], escaped=h[2], distance_cut=h[3], absorbed_bulk=h[4],
                     absorbed_surface=h[5], rouletted=h[6], reweighted=h[7], truncated=h[8], pushed=h[9],
-                    start=h[10], records=int(cnt[2]), photons=int(cnt[0]), steps=int(cnt[1]))  # fmt: skip
+                    start=h[10], records=int(cnt[2]), photons=int(cnt[0]), steps=int(cnt[1]),
+                    nonfinite=nonfinite)  # fmt: skip
     diag = None
     if bins[0]:
         hist = T.hist.cpu().numpy()

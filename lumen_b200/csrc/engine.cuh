@@ -40,6 +40,7 @@ struct LumenScene {
   std::vector<int32_t> sigma_tabs;  // the sigma_alpha tables of the unified facet rows
   std::vector<int32_t> tab;         // host copy of the (offset, knots) table index
   std::vector<int32_t> spectrum_tabs;  // the WLS emission spectra's tables
+  std::vector<std::pair<int, int>> roles;  // (table, admissible range) of every table a run reads
   int has_torus;                       // a leaf of typ 2: the launches run the kernels with the torus code
   int single;                          // every solid one quadric / plane leaf: the single-leaf instantiation
   int clip;                            // the extended locate is needed: a protrusion clip or frame groups

@@ -65,6 +65,9 @@ static int upload_raw(LumenScene* sc, const void* h, size_t bytes, void** out) {
     field = (decltype(field))p_;                                                    \
   } while (0)
 
+static void value_roles(const LumenSceneDesc* d, std::vector<std::pair<int, int>>& out);
+static int check_values(const std::vector<std::pair<int, int>>& roles, const int32_t* tab, int n_tab, const float* pool);
+
 static int check_desc(const LumenSceneDesc* d) {
   if (!d || d->n_vol <= 0 || !d->vol_i || !d->vol_f || !d->kind_i || !d->leaf_f || !d->leaf_i || !d->prog_i ||
       !d->cls_medium || !d->row_of || !d->med_i || !d->tab || !d->pool || d->n_cls <= 0 || d->n_pool <= 0)
@@ -143,6 +146,17 @@ static int check_desc(const LumenSceneDesc* d) {
       }
     }
   }
+  {  // every BVH item a volume or a mesh chunk (CH0 + c), every candidate one of the navigator's ids
+    const int ch0 = d->n_vol + 1 + d->n_mesh;
+    for (int i = 0; i < d->n_item; ++i) {
+      const int it = d->items[i];
+      if (!((it >= 0 && it < d->n_vol) || (it >= ch0 && it < ch0 + d->n_chunk)))
+        return set_err(LUMEN_ERR_ARG, "scene_create: a BVH item is neither a volume nor a mesh chunk");
+    }
+    for (int i = 0; i < d->n_cand; ++i)
+      if (d->cand[i] < 0 || d->cand[i] >= ch0 + d->n_chunk)
+        return set_err(LUMEN_ERR_ARG, "scene_create: a candidate is not a volume, a mesh or a mesh chunk");
+  }
   for (int c = 0; c < d->n_cls; ++c)
     if (d->cls_medium[c] < 0 || d->cls_medium[c] >= d->n_med) return set_err(LUMEN_ERR_ARG, "scene_create: a medium is out of range");
   for (int r = 0; r < d->n_row; ++r) {
@@ -176,10 +190,64 @@ static int check_desc(const LumenSceneDesc* d) {
       if (sk <= k || sk > d->n_fnode) return set_err(LUMEN_ERR_ARG, "scene_create: a sensor-box tree skip is out of order");
     }
   }
-  return 0;
+  std::vector<std::pair<int, int>> roles;  // the values of every table a run reads, inside their ranges
+  value_roles(d, roles);
+  return check_values(roles, d->tab, d->n_tab, d->pool);
 }
 
 // sigma_alpha of every unified facet row within the tables' span (src/lumen/rules/choices.py:103 SIGMA_MIN/MAX)
+// The admissible values of the tables a run reads, by their role (src/lumen/_core/domains.py: a range with both ends
+// included, never a value that is not finite; src/lumen/build/values.py:235 _check_params refuses a concrete value
+// outside it): the knots of every such table strictly ascending and finite, its values inside the role's range.
+enum { DOM_FRACTION = 0, DOM_POSITIVE, DOM_INDEX, DOM_MIE_G };
+static void value_roles(const LumenSceneDesc* d, std::vector<std::pair<int, int>>& out) {
+  out.clear();
+  static const int med_role[][2] = {{LUMEN_MI_INDEX, DOM_INDEX}, {LUMEN_MI_ABS, DOM_POSITIVE}, {LUMEN_MI_RAY, DOM_POSITIVE},
+                                    {LUMEN_MI_MIE, DOM_POSITIVE}, {LUMEN_MI_MIE_GF, DOM_MIE_G}, {LUMEN_MI_MIE_GB, DOM_MIE_G},
+                                    {LUMEN_MI_MIE_R, DOM_FRACTION}, {LUMEN_MI_WLS, DOM_POSITIVE},
+                                    {LUMEN_MI_WLS_YIELD, DOM_POSITIVE}, {LUMEN_MI_WLS_TAU, DOM_POSITIVE},
+                                    {LUMEN_MI_WLS_SPEC, DOM_POSITIVE}};  // fmt: skip
+  for (int m = 0; m < d->n_med; ++m)
+    for (const auto& mr : med_role) {
+      const int t = d->med_i[(size_t)m * LUMEN_MED_I + mr[0]];
+      if (t >= 0) out.push_back({t, mr[1]});
+    }
+  static const int col_role[LUMEN_N_COL] = {DOM_FRACTION, DOM_FRACTION, DOM_FRACTION, DOM_FRACTION, DOM_FRACTION,
+                                            DOM_FRACTION, DOM_POSITIVE, DOM_FRACTION, DOM_INDEX, DOM_POSITIVE};
+  for (int r = 0; r < d->n_row; ++r)
+    for (int c = 0; c < LUMEN_N_COL; ++c) {
+      const int t = d->row_i[(size_t)r * LUMEN_ROW_I + LUMEN_RI_COL + c];
+      if (t >= 0) out.push_back({t, col_role[c]});
+    }
+}
+
+static int check_values(const std::vector<std::pair<int, int>>& roles, const int32_t* tab, int n_tab, const float* pool) {
+  static const char* what[] = {"a fraction outside [0, 1]", "a negative length, yield, time or intensity",
+                               "a refractive index below 1", "a Mie asymmetry |g| above 0.999"};
+  for (const auto& tr : roles) {
+    const int t = tr.first;
+    if (t < 0 || t >= n_tab) continue;  // the table index itself is checked with the arrays
+    const int off = tab[2 * t], k = tab[2 * t + 1];
+    for (int j = 0; j < k; ++j) {
+      const float e = pool[off + j], v = pool[off + k + j];
+      if (!std::isfinite(e) || (j > 0 && !(e > pool[off + j - 1])))
+        return set_err(LUMEN_ERR_ARG, "table " + std::to_string(t) + ": its knot energies must be finite and strictly "
+                                      "ascending");
+      bool ok = std::isfinite(v);
+      switch (tr.second) {
+        case DOM_FRACTION: ok = ok && v >= 0.0f && v <= 1.0f; break;
+        case DOM_POSITIVE: ok = ok && v >= 0.0f; break;
+        case DOM_INDEX: ok = ok && v >= 1.0f; break;
+        default: ok = ok && fabsf(v) <= 0.999f; break;
+      }
+      if (!ok)
+        return set_err(LUMEN_ERR_ARG, "table " + std::to_string(t) + " holds " + what[tr.second] +
+                                          " or a value that is not finite (" + std::to_string(v) + ")");
+    }
+  }
+  return 0;
+}
+
 static int check_widths(const LumenScene* sc, const float* pool) {
   const double lo = exp(LUMEN_UNI_Y0 + LUMEN_UNI_DY * LUMEN_UNI_J_LO);
   const double hi = exp(LUMEN_UNI_Y0 + LUMEN_UNI_DY * (LUMEN_UNI_J_LO + LUMEN_UNI_NY - 1));
@@ -613,6 +681,13 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(LUMEN_ERR_NO_DEVICE, "no CUDA device");
   LumenScene* sc = new LumenScene();
   CK(cudaGetDevice(&sc->dev));
+  {  // the calls' scratch and moment tables come from the device's default pool (cudaMallocAsync): the pool keeps
+     // what it has once held in this process, so a later call reuses it without mapping memory again
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, sc->dev));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   DScene& S = sc->S;
   S.n = d->n_vol;
   S.LM = 1;
@@ -758,6 +833,7 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
     const int32_t* mr = d->med_i + (size_t)m * LUMEN_MED_I;
     if (mr[LUMEN_MI_WLS] >= 0) sc->spectrum_tabs.push_back(mr[LUMEN_MI_WLS_SPEC]);
   }
+  value_roles(d, sc->roles);
   if (check_widths(sc, d->pool)) {
     for (void* p : sc->allocs) cudaFree(p);
     delete sc;
@@ -774,6 +850,10 @@ int32_t lumen_b200_scene_set_pools(LumenScene* sc, const float* live, const floa
   g_err.clear();
   if (!sc || !live) return set_err(LUMEN_ERR_ARG, "scene or live pool is null");
   if (check_widths(sc, live) || (ref && check_widths(sc, ref))) return LUMEN_ERR_ARG;
+  const int n_tab = (int)(sc->tab.size() / 2);
+  int sv = check_values(sc->roles, sc->tab.data(), n_tab, live);
+  if (!sv && ref) sv = check_values(sc->roles, sc->tab.data(), n_tab, ref);
+  if (sv) return sv;
   CK(cudaMemcpy(sc->pool_live, live, sc->n_pool * sizeof(float), cudaMemcpyHostToDevice));
   if (ref && ref != live) {
     if (sc->pool_ref == sc->pool_live) {

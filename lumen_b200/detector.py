@@ -36,6 +36,20 @@ class SensorTable:
     axis: np.ndarray
 
 
+class InvalidValue(ValueError):  # noqa: N818 (the reference's name, src/lumen/build/values.py:52)
+    """A parameter value outside what the detector's structure holds: outside its range, or not finite."""
+
+
+# the admissible ranges of the values a run reads (src/lumen/_core/domains.py: FRACTION, POSITIVE / LENGTH, INDEX;
+# a Mie asymmetry within MIE_G_MAX, src/lumen/rules/choices.py:99), by the table's role: a medium's tables (LUMEN_MI_*)
+# and a surface row's columns (LUMEN_COL_*)
+_DOMAINS = {"fraction": (0.0, 1.0), "positive": (0.0, np.inf), "index": (1.0, np.inf), "mie_g": (-0.999, 0.999)}
+_MED_ROLES = {0: "index", 1: "positive", 2: "positive", 3: "positive", 4: "mie_g", 5: "mie_g", 6: "fraction",
+              7: "positive", 8: "positive", 9: "positive", 10: "positive"}  # fmt: skip
+_COL_ROLES = ("fraction", "fraction", "fraction", "fraction", "fraction", "fraction", "positive", "fraction", "index",
+              "positive")  # fmt: skip
+
+
 @dataclass
 class Detector:
     """The flattened detector (see the module docstring)."""
@@ -68,6 +82,30 @@ class Detector:
             off, n = self.arrays["tab"][t]
             out[k] = (self.pool[off:off + n].copy(), self.pool[off + n:off + 2 * n].copy())
         return out
+
+    def check_values(self, pool: np.ndarray, what: str = "values") -> None:
+        """Raise ``InvalidValue`` naming the first parameter of ``pool`` outside its admissible range, or not finite
+        (src/lumen/build/values.py:235 ``_check_params``: a concrete value is refused; the ranges of
+        src/lumen/_core/domains.py, both ends included). The C ABI refuses the same values (LUMEN_ERR_ARG)."""  # noqa: D205
+        a = self.arrays
+        tab = np.asarray(a["tab"]).reshape(-1, 2)
+        med = np.asarray(a["med_i"]).reshape(-1, 16)
+        rows = np.asarray(a["row_i"]).reshape(-1, 16)
+        name = {t: k for k, t in self.params_index.items()}
+        roles = [(t, r) for m in med for t, r in zip(m[list(_MED_ROLES)], _MED_ROLES.values(), strict=True)]
+        roles += [(t, r) for ri in rows for t, r in zip(ri[6:6 + len(_COL_ROLES)], _COL_ROLES, strict=True)]
+        for t, role in roles:
+            if t < 0:
+                continue
+            off, k = tab[t]
+            e, v = pool[off:off + k], pool[off + k:off + 2 * k]
+            label = name.get(int(t), f"table {int(t)}")
+            if not (np.all(np.isfinite(e)) and np.all(np.diff(e) > 0)):
+                raise InvalidValue(f"{what}: {label}: its knot energies must be finite and strictly ascending")
+            lo, hi = _DOMAINS[role]
+            if not np.all(np.isfinite(v) & (v >= lo) & (v <= hi)):
+                bad = v[~(np.isfinite(v) & (v >= lo) & (v <= hi))][0]
+                raise InvalidValue(f"{what}: {label} has a value outside [{lo}, {hi}] or not finite ({bad})")
 
     def pool_with(self, values: dict | None) -> np.ndarray:
         """Return the pool with some parameters replaced: {name: constant or values array (same knots)}."""

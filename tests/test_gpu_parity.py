@@ -620,3 +620,61 @@ def test_wire_planes_with_frame_groups_bit_exact(built):
     src = sources.Point(position=(-0.5, 0.0, 0.0), n_photons=1.0, lam=128.0)
     bad, gi, oi, gf, of = _records_match(det, src, 1 << 14)
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+
+
+def test_batched_events_in_a_captured_graph_match(tank, built):
+    """256 uneven track events (the batched workload's shape, its counts log-uniform over 3 .. 300 photons instead of
+    1e3 .. 1e6) in one LUMEN_F_ASYNC launch captured in a CUDA graph with its tallies' zeroing, replayed twice: the
+    arrivals and the Jacobian per event are the checker's, on both replays."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    e = 256
+    u = rng.normal(size=(e, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    start = np.column_stack([rng.uniform(-3.3, 3.3, (e, 2)), rng.uniform(-4.0, 4.0, e)])
+    counts = np.exp(rng.uniform(np.log(3.0), np.log(300.0), e)).astype(np.int64)
+    src = sources.Tracks(start=start, direction=u, length=rng.uniform(0.5, 3.0, e), cone_angle=np.radians(42.0),
+                         n_photons=counts.astype(float), lam_range=(300.0, 600.0), counts_=counts)  # fmt: skip
+    n = int(counts.sum())
+    names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R"]
+    gt = [tank.params_index[k] for k in names]
+    eng = _engine(tank)
+    ds = DeviceSource(src, n)
+    c = A.controls(grad_tabs=gt, flags=A.F_ASYNC)
+    T = DeviceTallies(tank.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt))
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):  # the first call on the side stream, before the capture
+        eng.trace(KEY, n, source=ds, controls=c, tallies=T, stream=stream)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        T.zero_()
+        eng.trace(KEY, n, source=ds, controls=c, tallies=T, stream=stream)
+    O, _ = oracle.trace(tank, KEY, n, source=src, samples=n, controls=A.controls(grad_tabs=gt), n_events=ds.n_events)
+    assert O.arrival.shape[0] == e
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+        assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+    del g
+
+
+def test_step_budget_ends_the_launch_with_an_error(tank, built):
+    """A device step budget that runs out (LumenControls.step_budget): the kernel stops handing out photons and
+    returns, the call raises StepBudgetExhausted, counts[LUMEN_C_ABORTED] is 1, and the engine serves the next call."""
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    eng = _engine(tank)
+    n = 1 << 16
+    ds = DeviceSource(src, n)
+    for variant in (0, A.VARIANT_WAVEFRONT):
+        T = DeviceTallies(tank.n_sensor, 1, 0, 0.0, 1.0)
+        with pytest.raises(A.StepBudgetExhausted):
+            eng.trace(KEY, n, source=ds, controls=A.controls(step_budget=1024, variant=variant), tallies=T)
+        cnt = T.counts.cpu().numpy()
+        assert cnt[A.C_ABORTED] == 1 and cnt[A.C_PHOTONS] < n
+    T, O = _tallies(tank, src, n)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
