@@ -285,8 +285,8 @@ def run_batched(dev, det, reps=3, with_cpu=True):
     ds = DeviceSource(src, n, dev)
     names = ["media/Water/absorption", "media/Water/rayleigh", "surfaces/BlackSheet/R"]
     gt = [det.params_index[k] for k in names]
-    (variant, bps), times = autotune.tune(eng, ds, 1 << 20, gt, ds.n_events, A.key_of_seed(0), asynchronous=True)
-    c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps, flags=A.F_ASYNC)
+    shape, times = autotune.tune(eng, ds, 1 << 20, gt, ds.n_events, A.key_of_seed(0), asynchronous=True)
+    c = shape.controls(n, gt, A.F_ASYNC)
     T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
     stream = torch.cuda.Stream(dev)
@@ -319,8 +319,7 @@ def run_batched(dev, det, reps=3, with_cpu=True):
     return {"value": n / (m * 1e-3), "unit": "photons/s", "events": int(ds.n_events), "photons_per_launch": n,
             "mc_error": err, "vs_checker": vs,
             "ms_per_launch": m, "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "gradients": names,
-            "graph": True, "autotune": {"variant": variant, "blocks_per_sm": bps,
-                                        "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}},
+            "graph": True, "autotune": {"shape": shape.label(), "ms_sample": {k: round(v, 3) for k, v in times.items()}},
             "jacobian_norm": float(np.abs(jac).sum()), "aborted": int(cnt[5])}  # fmt: skip
 
 
@@ -341,8 +340,8 @@ def run_tank_adjoint(dev, src, n, reps=2, with_cpu=True):
              "surfaces/BlackSheet/sigma_alpha"]  # fmt: skip
     gt = [det.params_index[k] for k in names]
     # a sample of several pool fills: the wavefront's last rounds run few photons, a cost a one-fill sample overstates
-    (variant, bps), times = autotune.tune(eng, ds, min(n, 1 << 23), gt, ds.n_events, A.key_of_seed(0), reps=1)
-    c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps)
+    shape, times = autotune.tune(eng, ds, min(n, 1 << 23), gt, ds.n_events, A.key_of_seed(0), reps=1)
+    c = shape.controls(n, gt)
     T = DeviceTallies(det.n_sensor, ds.n_events, 200, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
     eng.trace(key, min(n, 1 << 20), source=ds, controls=c, tallies=T)
@@ -365,8 +364,7 @@ def run_tank_adjoint(dev, src, n, reps=2, with_cpu=True):
     return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
             "mc_error": err, "vs_checker": vs, "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
-            "autotune": {"variant": variant, "blocks_per_sm": bps,
-                         "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}},
+            "autotune": {"shape": shape.label(), "ms_sample": {k: round(v, 3) for k, v in times.items()}},
             "jacobian_abs_sum": [float(x) for x in np.abs(jac).sum(0)]}  # fmt: skip
 
 
@@ -387,8 +385,8 @@ def run_lar(dev, n, reps=1, with_cpu=True):
     ds = DeviceSource(src, n, dev)
     names = ["surfaces/CageSurface/R", "media/LAr/rayleigh"]
     gt = [det.params_index[k] for k in names]
-    (variant, bps), times = autotune.tune(eng, ds, min(n, 1 << 20), gt, ds.n_events, A.key_of_seed(0), reps=1)
-    c = A.controls(grad_tabs=gt, variant=variant, blocks_per_sm=bps)
+    shape, times = autotune.tune(eng, ds, min(n, 1 << 22), gt, ds.n_events, A.key_of_seed(0), reps=1)
+    c = shape.controls(n, gt)
     T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt), dev)
     key = A.key_of_seed(0)
     eng.trace(key, min(n, 1 << 18), source=ds, controls=c, tallies=T)
@@ -411,8 +409,7 @@ def run_lar(dev, n, reps=1, with_cpu=True):
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
             "mc_error": err, "vs_checker": vs, "moment_table_sums": int(cnt[4]), "moment_lost": int(cnt[7]),
             "points": 10000, "gradients": names, "arrivals_sum": float(T.arrival.sum().item()),
-            "autotune": {"variant": variant, "blocks_per_sm": bps,
-                         "ms_sample": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in times.items()}}}  # fmt: skip
+            "autotune": {"shape": shape.label(), "ms_sample": {k: round(v, 3) for k, v in times.items()}}}  # fmt: skip
 
 
 def main():
@@ -427,7 +424,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched and liquid-argon workloads")
     ap.add_argument("--lar-photons", type=int, default=1 << 26)
-    ap.add_argument("--variant", type=int, default=0, help="the headline workload's launch variant (3: wavefront)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="the headline's launch variant (3: wavefront; default: the autotuner's pick)")
     args = ap.parse_args()
 
     from lumen_b200 import detectors, sources
@@ -470,13 +468,22 @@ def main():
     first, n_rank = distributed.shard_range(n * world, rank, world)  # this rank's contiguous photon ids
     ds = DeviceSource(src, n * world, dev)
     T = DeviceTallies(det.n_sensor, 1, 200, 0.0, 1.0, 0, dev)
-    c = A.controls(variant=args.variant)
+    from lumen_b200 import autotune
+
+    if args.variant < 0:  # the autotuner's pick on a sample of this rank's photons (src: the same photon law)
+        shape, tune_ms = autotune.tune(eng, ds, min(n_rank, 1 << 22), (), 1, key)
+    else:
+        shape, tune_ms = autotune.Shape(args.variant), {}
+    c = shape.controls(n_rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+
+    launches = []
 
     def one_step():
         T.zero_()
         distributed.trace_shard(eng, key, first, n_rank, source=ds, controls=c, tallies=T, stream=stream)
+        launches.append(eng.launches)  # the library's own kernels this call launched
         distributed.all_reduce_tallies(T)  # one NCCL all-reduce of every tally (nothing with one rank)
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -503,6 +510,7 @@ def main():
             bounds.append((t_a, time.monotonic()))
         torch.cuda.synchronize(dev)
     ms = [a.elapsed_time(b) for a, b in ev]
+    timed_launches = int(sum(launches[args.warmup:]))
     cnt = T.counts.cpu().numpy()
     ms_step = float(np.mean(ms))
     if world > 1:
@@ -534,14 +542,15 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "photon_steps_per_s": world * float(cnt[1]) / (ms_step * 1e-3), "steps_per_photon": steps_pp,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
-                         "traffic": TRAFFIC_PER_PHOTON * n if args.variant == 0 else None, "peak_kind": pk_kind,
+                         "traffic": TRAFFIC_PER_PHOTON * n if shape.variant == 0 else None, "peak_kind": pk_kind,
                          "algorithmic_bytes": alg,
                          "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-photon launch "
                                          "of k_trace<0,256,4,2,0,0> on this workload (6.24 GB), scaled by photons"},
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            # per step: the persistent loop and the moment table's pass (the wavefront's rounds are counted by no
-            # host-side number)
-            "gpu_launches": 2 * args.steps if args.variant != 3 else None, "launch_variant": args.variant,
+            # the library's kernels launched in the timed steps (lumen_b200_last_launches: the trace's kernels or the
+            # wavefront's rounds, and the moment table's pass)
+            "gpu_launches": timed_launches, "launch_shape": shape.label(),
+            "autotune_ms": {k: round(v, 3) for k, v in tune_ms.items()},
             "clocks": clk.summary(), "ms_steps": [round(x, 3) for x in ms],
             "sm_mhz_steps": clk.per_step(bounds), "mc_error": mc_error(T.arrival.cpu().numpy(),
                                                                        T.arrival2.cpu().numpy(), [n * world]),

@@ -281,7 +281,8 @@ typedef struct LumenControls {
   int32_t flags;           /* LUMEN_F_* */
   int32_t variant;         /* launch variant (0 .. LUMEN_N_VARIANT - 1), from the autotuner */
   int32_t blocks_per_sm;   /* resident blocks per SM launched (<= 0: as many as fit) */
-  int32_t reserved;
+  int32_t wave_slots_log2; /* the wavefront's slots: 2^k photons in flight, k in 16 .. 23 (else 2^21), from the
+                              autotuner: each slot carries n / 2^k photons in turn */
 } LumenControls;
 
 /* --------------------------------------------------------------------------------------------- the tallies */
@@ -361,6 +362,11 @@ typedef struct LumenTallies {
 int32_t lumen_b200_abi_version(void);
 /* The last error message of this thread (static storage; "" after success). */
 const char* lumen_b200_last_error(void);
+
+/* The kernels the calling thread's last call of an entry point launched (its trace kernels, the wavefront's rounds,
+   the moment table's pass, the readout groups' binning): for a caller counting its GPU work. No counterpart in the
+   reference (tallymap launches its kernels itself). */
+int64_t lumen_b200_last_launches(void);
 
 /* Upload a detector to the current CUDA device; replaces the reference's Navigator.operands / pack.pack device put
    (src/lumen/geometry/navigate.py:140, src/lumen/api.py:842). Unified rows with sigma_alpha > 0 draw Geant4's facet

@@ -87,7 +87,7 @@ class LumenControls(ctypes.Structure):
     _fields_ = [("max_distance", ctypes.c_float), ("roulette", ctypes.c_float), ("max_vertices", ctypes.c_int32),
                 ("n_grad", ctypes.c_int32), ("grad_tab", ctypes.c_int32 * MAX_GRAD),
                 ("step_budget", ctypes.c_int64), ("flags", ctypes.c_int32), ("variant", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]  # fmt: skip
+                ("blocks_per_sm", ctypes.c_int32), ("wave_slots_log2", ctypes.c_int32)]  # fmt: skip
 
 
 class LumenAxis(ctypes.Structure):
@@ -125,9 +125,10 @@ def dptr(a):
 
 
 def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=(), step_budget=0, flags=0, variant=0,
-             blocks_per_sm=0):
+             blocks_per_sm=0, wave_slots_log2=0):
     c = LumenControls()
     c.flags, c.variant, c.blocks_per_sm = int(flags), int(variant), int(blocks_per_sm)
+    c.wave_slots_log2 = int(wave_slots_log2)
     c.max_distance = float(max_distance)
     c.roulette = float(roulette)
     c.max_vertices = int(max_vertices)
@@ -140,9 +141,9 @@ def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=()
     return c
 
 
-ENTRY_POINTS = ("lumen_b200_abi_version", "lumen_b200_last_error", "lumen_b200_scene_create",
-                "lumen_b200_scene_set_pools", "lumen_b200_scene_destroy", "lumen_b200_trace", "lumen_b200_adjoint",
-                "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate", "lumen_b200_trace_static",
+ENTRY_POINTS = ("lumen_b200_abi_version", "lumen_b200_last_error", "lumen_b200_last_launches",
+                "lumen_b200_scene_create", "lumen_b200_scene_set_pools", "lumen_b200_scene_destroy", "lumen_b200_trace",
+                "lumen_b200_adjoint", "lumen_b200_trace_photons", "lumen_b200_query", "lumen_b200_locate", "lumen_b200_trace_static",
                 "lumen_b200_query64", "lumen_b200_locate64")  # fmt: skip
 
 _lib = None
@@ -159,6 +160,7 @@ def engine():
         vp = ctypes.c_void_p
         lib.lumen_b200_abi_version.restype = ctypes.c_int32
         lib.lumen_b200_last_error.restype = ctypes.c_char_p
+        lib.lumen_b200_last_launches.restype = ctypes.c_int64
         lib.lumen_b200_scene_create.argtypes = [ctypes.POINTER(LumenSceneDesc), ctypes.POINTER(vp)]
         lib.lumen_b200_scene_set_pools.argtypes = [vp, c_f32p, c_f32p]
         lib.lumen_b200_scene_destroy.argtypes = [vp]
@@ -180,7 +182,7 @@ def engine():
         lib.lumen_b200_query64.argtypes = [vp, c_f64p, c_i32p, c_i32p, ctypes.c_double, ctypes.c_int64, c_i32p,
                                            c_f64p, vp]  # fmt: skip
         lib.lumen_b200_locate64.argtypes = [vp, c_f64p, ctypes.c_int64, c_i32p, vp]
-        for name in ENTRY_POINTS[2:]:
+        for name in ENTRY_POINTS[3:]:
             getattr(lib, name).restype = ctypes.c_int32
         _lib = lib
     return _lib

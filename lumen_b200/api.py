@@ -102,9 +102,9 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     ``params``: {parameter name: value} overriding the detector's values (``det.params()``); ``reference``: the
     values the draws are made at (default: ``params``). ``controls``: ``dict(roulette=0.01, max_distance=None,
     max_vertices=2**22, variant=None, jump=True)``; ``jump`` the diffusion jump (on, as lumen.simulate's default: where a
-    medium and volume allow it; the same estimator in law as the plain walk); ``variant`` picks the launch (``LumenControls.variant``; default: the
-    wavefront where derivatives are asked for, the persistent loop otherwise, the measured faster of the two on the
-    tank workloads). ``chunk``: photons per launch (default: all in one launch). ``gradients``: parameter names
+    medium and volume allow it; the same estimator in law as the plain walk); ``variant`` picks the launch
+    (``LumenControls.variant``; default: the wavefront, measured the faster on the tank and LAr workloads, forward and
+    with tangents; scenes it does not serve run the persistent loop). ``chunk``: photons per launch (default: all in one launch). ``gradients``: parameter names
     whose derivatives of the arrivals are returned (forward tangents of the reweighting estimator along each path).
     ``time_bins``: (bins, t0, width) ns of the per-sensor arrival-time histograms (``Light.diagnostics``).
     ``groups``: the readout groups' histograms to fill ({name: lumen_b200.readout.Grid or Group}: a Grid's sensors
@@ -125,7 +125,7 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22, variant=None, jump=True) | (controls or {})
     gnames = list(gradients)
     gt = [det.params_index[k] for k in gnames]
-    variant = ctl["variant"] if ctl["variant"] is not None else (A.VARIANT_WAVEFRONT if gt else 0)
+    variant = ctl["variant"] if ctl["variant"] is not None else A.VARIANT_WAVEFRONT
     flags = A.F_JUMP if ctl["jump"] else 0  # the diffusion jump on, as lumen.simulate (src/lumen/api.py:1157)
     if truth is not None:  # src/lumen/api.py:1296 _truth_setup
         if not isinstance(truth, TR.Truth):

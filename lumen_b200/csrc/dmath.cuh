@@ -14,7 +14,11 @@
 #include <stdint.h>
 
 #define L_DEV __device__ __forceinline__
-#define L_CALL static __device__ __noinline__  // large functions: one copy shared by every call site (instruction cache)
+// one copy shared by every call site: the threefry block (called for every draw) and the torus's root finders (their
+// 40-step bisections, in the extended geometry only). Every other device function is inlined: measured on B200, the
+// inlined step is 11 % faster on the tank's plain forward and 26 % faster on its wavefront with tangents than with the
+// surface kernel, the media and the navigator's helpers called (their frames and argument copies were local memory)
+#define L_CALL static __device__ __noinline__
 
 namespace lb {
 

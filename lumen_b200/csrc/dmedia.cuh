@@ -200,7 +200,7 @@ struct Bulk2 {
   float rlw, y_w, y_r, delay, lam;
   float dlob[LUMEN_MAX_GRAD], dyld[LUMEN_MAX_GRAD];
 };
-L_CALL void d_bulk_other(const DScene& S, const float* __restrict__ live, const float* __restrict__ ref, int shared,
+L_DEV void d_bulk_other(const DScene& S, const float* __restrict__ live, const float* __restrict__ ref, int shared,
                          int cs, int mi, float lam, const float* wi, const float* er0, const float* ei0, Key vkey,
                          int P, const int* gt, Bulk2& b) {
   const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;

@@ -528,14 +528,14 @@ L_DEV NF d_leaf_dist(const DScene& S, int kind, int leaf, int face, const NF* x)
 
 L_DEV int d_clampv(const DScene& S, int item) { return item < 0 ? 0 : (item > S.n - 1 ? S.n - 1 : item); }
 
-L_CALL void d_hit_grad(const DScene& S, int item, int leaf, int face, const NF* x, NF* gw) {
+L_DEV void d_hit_grad(const DScene& S, int item, int leaf, int face, const NF* x, NF* gw) {
   int i = d_clampv(S, item);
   NF xl[3], g[3];
   d_to_local_pt(S, i, x, xl);
   d_leaf_grad(S, vI(S, i, LUMEN_VI_KIND), leaf, face, xl, g);
   d_to_world_dir(S, i, g, gw);
 }
-L_CALL NF d_face_dist(const DScene& S, int item, int leaf, int face, const NF* x) {
+L_DEV NF d_face_dist(const DScene& S, int item, int leaf, int face, const NF* x) {
   int i = d_clampv(S, item);
   NF xl[3];
   d_to_local_pt(S, i, x, xl);
@@ -565,7 +565,7 @@ L_DEV int d_holds_point(const DScene& S, int i, const NF* x) {
   d_to_local_pt(S, i, x, xl);
   return d_inside_kind(S, vI(S, i, LUMEN_VI_KIND), xl);
 }
-L_CALL int d_ray_holds(const DScene& S, int i, const NF* od, const NF* dd, NF t) {
+L_DEV int d_ray_holds(const DScene& S, int i, const NF* od, const NF* dd, NF t) {
   NF ol[3], dl[3];
   d_to_local_pt(S, i, od, ol);
   d_to_local_dir(S, i, dd, dl);
@@ -647,7 +647,7 @@ L_DEV int d_find(const DScene& S, int v, const NF* x) {
   });
   return g;
 }
-L_CALL int d_locate(const DScene& S, const NF* x) {
+L_DEV int d_locate(const DScene& S, const NF* x) {
   int v = S.n;
   for (int guard = 0; guard < 64; ++guard) {
     int f = d_find(S, v, x);
@@ -664,7 +664,7 @@ L_DEV int d_find_ray(const DScene& S, int v, const NF* od, const NF* dd, NF t, i
   });
   return g;
 }
-L_CALL int d_settle(const DScene& S, int v, const NF* od, const NF* dd, NF t, int crossed, NF pad, int* moved) {
+L_DEV int d_settle(const DScene& S, int v, const NF* od, const NF* dd, NF t, int crossed, NF pad, int* moved) {
   int v_ = v, held = 0;
   for (int guard = 0; guard < 256; ++guard) {
     int vi = v_ < S.n - 1 ? v_ : S.n - 1;
@@ -688,7 +688,7 @@ L_DEV int d_find_x(const DScene& S, int v, const NF* x) {
   });
   return g;
 }
-L_CALL int d_locate_x(const DScene& S, const NF* x) {
+L_DEV int d_locate_x(const DScene& S, const NF* x) {
   int v = S.n;
   for (int guard = 0; guard < 64; ++guard) {
     int f = d_find_x(S, v, x);
@@ -705,7 +705,7 @@ L_DEV int d_find_ray_x(const DScene& S, int v, const NF* od, const NF* dd, NF t,
   });
   return g;
 }
-L_CALL int d_settle_x(const DScene& S, int v, const NF* od, const NF* dd, NF t, int crossed, NF pad, int* moved) {
+L_DEV int d_settle_x(const DScene& S, int v, const NF* od, const NF* dd, NF t, int crossed, NF pad, int* moved) {
   int v_ = v, held = 0;
   for (int guard = 0; guard < 256; ++guard) {
     int vi = v_ < S.n - 1 ? v_ : S.n - 1;
@@ -733,7 +733,7 @@ struct Ctx {
   Side sd;
 };
 
-L_CALL int d_on_face(const DScene& S, const Ctx& c, int i, const First& fr, int kn_i) {
+L_DEV int d_on_face(const DScene& S, const Ctx& c, int i, const First& fr, int kn_i) {
   NF dt = fr.t - c.t_lo;
   NF lim = D_K_ON * c.band;
   int far_ = 0;
@@ -888,7 +888,7 @@ L_DEV int d_crossing(const DScene& S, const Ctx& c, const Shear& h, int k, NF* t
 // the best event after mesh chunk i (navigate.py:320 _mesh_visit, :303 _triangle: the facet rule): the triangle the
 // photon sits on, heading into it, is a zero-length re-hit; else a facet is met entering it (n . d < 0, the start
 // behind its plane within the tolerance) or from clearly behind (the start inside the closed surface): both entries
-L_CALL Best d_mesh_visit(const DScene& S, const Ctx& c, int ch0, int i, Best b) {
+L_DEV Best d_mesh_visit(const DScene& S, const Ctx& c, int ch0, int i, Best b) {
   const int* cr = S.mesh + MESH_HDR + 4 * (i - ch0);
   const int k0 = __ldg(cr), kn = __ldg(cr + 1);
   const NF hi_t = d_min(b.t, c.t_bound);
@@ -1324,7 +1324,7 @@ L_DEV Query d_query(const DScene& S, const NF* o, const NF* d, int vol, NF t_max
 // meets no sensor box, every crossing it can deposit at lies beyond s, so the query may stop at s plus the
 // navigator's own look-ahead ((GRAZE K_ON + 2) bands): the same arithmetic for every round that starts before s
 // (the boxes, the direction and s float32 in either precision: reach.py:88, :216)
-L_CALL NF d_reach_bound(const DScene& S, const NF* x, const float* d, int vol, int srf, float s, NF t_max) {
+L_DEV NF d_reach_bound(const DScene& S, const NF* x, const float* d, int vol, int srf, float s, NF t_max) {
   if (!S.comp || srf >= 0 || vol < 0 || vol > S.n) return t_max;
   int c = __ldg(S.comp + vol);
   if (c < 0) return t_max;

@@ -48,7 +48,7 @@ L_DEV float d_eg(const float* e, int k, int j) {
   if (j == k) return __ldg(e + k);
   return 0.5f * (__ldg(e + j - 1) + __ldg(e + j));
 }
-L_CALL float d_group_index(const DScene& S, const float* __restrict__ pool, int t, float E) {
+L_DEV float d_group_index(const DScene& S, const float* __restrict__ pool, int t, float E) {
   int off = __ldg(S.tab + 2 * t), kk = __ldg(S.tab + 2 * t + 1);
   const float* e = pool + off;
   const float* n = pool + off + kk;
@@ -89,7 +89,7 @@ L_DEV void d_channel_rates(const DScene& S, const float* __restrict__ pool, floa
 
 // (n, n_g, mu_abs, the channels' rates summed) of medium mi at lam (medium.py:27, bulk.py:88 evaluate); a bulk event
 // reads the channels' own rates again (d_channel_rates: the same values)
-L_CALL Med d_medium_at(const DScene& S, const float* __restrict__ pool, float lam, int mi) {
+L_DEV Med d_medium_at(const DScene& S, const float* __restrict__ pool, float lam, int mi) {
   const int32_t* m = S.med_i + (size_t)mi * LUMEN_MED_I;
   float E = D_HC / lam;
   Med r = {1.0f, 1.0f, 0.0f, 0.0f};
@@ -166,7 +166,7 @@ L_DEV Cf c_decaying_sqrt(Cf z) {
   return q;
 }
 
-L_CALL void d_amplitudes(float cos_i, float n1, Cf n2, Cf* a) {
+L_DEV void d_amplitudes(float cos_i, float n1, Cf n2, Cf* a) {
   float c = cos_i < 0.0f ? 0.0f : (cos_i > 1.0f ? 1.0f : cos_i);
   Cf c1 = cf(c, 0.0f), n1c = cf(n1, 0.0f);
   Cf n22 = c_mul(n2, n2);
@@ -271,7 +271,7 @@ L_DEV void d_chained(const float* p, const float* dp, float* out, float* dout) {
 // the TypeEval of a surface row (types.py:352 kernel); with G > 0 gradient parameters, gt[p] the table each moves,
 // the tangents dprobs[p][o], ddet[p] (a column's value moves with its table)
 template <int G>
-L_CALL void d_type_eval(const DScene& S, const float* __restrict__ pool, int row, float lam, const float* wi,
+L_DEV void d_type_eval(const DScene& S, const float* __restrict__ pool, int row, float lam, const float* wi,
                        const float* n, float n1, float n2, const float* er, const float* ei, Eval& ev, int P,
                        const int* gt, float (*dprobs)[N_OUT], float* ddet) {
 #pragma unroll
@@ -384,7 +384,7 @@ L_DEV float d_dipole_cos(float rand) {
   float r = 2.0f * c;
   return r < -1.0f ? -1.0f : (r > 1.0f ? 1.0f : r);
 }
-L_CALL void d_rayleigh_sample(const float* er, const float* ei, float r0, float r1, float r2, float* wo) {
+L_DEV void d_rayleigh_sample(const float* er, const float* ei, float r0, float r1, float r2, float* wo) {
   float a2 = d_dot(er, er);
   float norm2 = d_dot(er, er) + d_dot(ei, ei);
   float axis[3];
@@ -423,7 +423,7 @@ L_DEV float d_front_arc(const float* V, float a) {
   float ratio = V[2] * ca / d_max(sv * sa, D_FLOOR32);
   return l_acos(-d_min(ratio, 1.0f));
 }
-L_CALL void d_unified_facet(float sigma, const float* V, Key key, float* m, int* capped) {
+L_DEV void d_unified_facet(float sigma, const float* V, Key key, float* m, int* capped) {
   float fmax = d_min(1.0f, 4.0f * sigma);
   float a = 0.0f, u2 = 0.5f;
   int ok = 0;
@@ -523,7 +523,7 @@ L_DEV float d_table_front(const float* __restrict__ U, float x, float y, float* 
 }
 // log p1(w1 | w0) of one unified facet reflection at width sigma and (want_d) its derivative in sigma
 // (facets.py:209 _unified_log_density, :248 _half_vector, :259 unified_facet_logpdf)
-L_CALL float d_unified_logpdf(const float* __restrict__ U, float sigma, const float* w0, const float* n,
+L_DEV float d_unified_logpdf(const float* __restrict__ U, float sigma, const float* w0, const float* n,
                               const float* w1, int want_d, float* dls) {
   float mw[3] = {-w0[0], -w0[1], -w0[2]};
   float V[3], W[3];
@@ -564,7 +564,7 @@ L_CALL float d_unified_logpdf(const float* __restrict__ U, float sigma, const fl
 // the facet path (facets.py:372 _path_of; the Jones vector mirrored about each facet's half vector,
 // surface_event.py:106 _facet_path_branch). With the tables U each facet's log density is summed: at the live width
 // into lp (with its derivative in sigma into dls where want_d), and where weigh is set at the drawn width into lr.
-L_CALL void d_facet_path(float sigma, const float* wi, const float* n, float r0, float r1, float r2, float* wo,
+L_DEV void d_facet_path(float sigma, const float* wi, const float* n, float r0, float r1, float r2, float* wo,
                          float* er, float* ei, int* capped, const float* __restrict__ U, float sig_live, int weigh,
                          int want_d, float* lp, float* lr, float* dls) {
   Key key = d_seed_key(r0, r1, r2);
@@ -617,7 +617,7 @@ L_DEV float l_expm1(float y) {
 
 // a GLISUR facet normal (local frame): M = e_z + r s, s uniform in the unit ball (on its sphere when the facet's
 // cover draw says so), redrawn until V . M > 0 (facets.py:341 glisur_facet)
-L_CALL void d_glisur_facet(float r, const float* V, Key key, float e, float* m, int* capped) {
+L_DEV void d_glisur_facet(float r, const float* V, Key key, float e, float* m, int* capped) {
   int shell = e > 0.0f && uniform(fold_in(key, D_SHELL_STREAM), 0) < e;
   float M[3] = {0.0f, 0.0f, 1.0f};
   int ok = 0;
@@ -675,7 +675,7 @@ L_DEV float d_glisur_log_proposal(float r, const float* V, const float* M, float
   float ls = l_log(2.0f * r) + l_log(c * c + q2) - 0.5f * l_log(q2) - d_glisur_log_area(r, V[2]);
   return d_logaddexp(l_log1p(-e) + lp, l_log(e) + ls);
 }
-L_CALL float d_glisur_logpdf(float r, const float* w0, const float* n, const float* w1, float e, float* dr) {
+L_DEV float d_glisur_logpdf(float r, const float* w0, const float* n, const float* w1, float e, float* dr) {
   float mw[3] = {-w0[0], -w0[1], -w0[2]};
   float V[3], W[3];
   d_to_local(mw, n, V);
@@ -695,7 +695,7 @@ L_CALL float d_glisur_logpdf(float r, const float* w0, const float* n, const flo
 }
 // the GLISUR metal facet path drawn from the cover at r_ref, weighted by its exact path density at r_live over the
 // cover's (surface_event.py:106 with the covered lobe); *on the drawn weight, *dlr d/dr_live of the log weight
-L_CALL float d_glisur_metal_path(float r_ref, float r_live, const float* wi, const float* n, float r0, float r1,
+L_DEV float d_glisur_metal_path(float r_ref, float r_live, const float* wi, const float* n, float r0, float r1,
                                  float r2, float e, float* wo, float* er, float* ei, int* capped, float* on_,
                                  float* dlr) {
   Key key = d_seed_key(r0, r1, r2);
@@ -751,7 +751,7 @@ L_DEV void d_refract_dir(const float* w, const float* m, float eta, float* wo) {
   for (int a = 0; a < 3; ++a) wo[a] = eta * w[a] + k * m[a];
   d_unit(wo);
 }
-L_CALL float d_dielectric_event_lp(float r, float n1, float n2, const float* n, const float* w0, const float* w1,
+L_DEV float d_dielectric_event_lp(float r, float n1, float n2, const float* n, const float* w0, const float* w1,
                                    int refracted, float side, float e, const float* er, const float* ei, float* er1,
                                    float* ei1, float* dr) {
   float na = side > 0.0f ? n1 : n2, nb = side > 0.0f ? n2 : n1;
@@ -795,7 +795,7 @@ L_CALL float d_dielectric_event_lp(float r, float n1, float n2, const float* n, 
 // the GLISUR dielectric facet path drawn from the cover at r_ref, at the live indices (n1 incident, n2 far) and state;
 // weighted by its exact path density at r_live over the cover's at r_ref, its Jones vector the live one
 // (surface_event.py:137 _dielectric_path_branch); *far: it ends beyond the surface
-L_CALL float d_glisur_dielectric_path(float r_ref, float r_live, float n1, float n2, const float* wi, const float* n,
+L_DEV float d_glisur_dielectric_path(float r_ref, float r_live, float n1, float n2, const float* wi, const float* n,
                                       float r0, float r1, float r2, float e, float* wo, float* er, float* ei,
                                       int* far_, int* capped, float* on_, float* dlr) {
   Key key = d_seed_key(r0, r1, r2);

@@ -38,7 +38,7 @@ struct Jmp {
 // the walk at a bulk Rayleigh event inside the proven clear ball at xs (fastpath.py:174 diffuse): free paths at the
 // reference rate, the polarised Rayleigh draw and projection, until a flight leaves the ball (the photon put at the
 // crossing) or the budget ceil((c mu_r)^2) of scatterings (at most LUMEN_JUMP_STEPS) is spent
-L_CALL void d_diffuse(const DScene& S, int mi, const float* xs, const float* d0, const float* er0, const float* ei0,
+L_DEV void d_diffuse(const DScene& S, int mi, const float* xs, const float* d0, const float* er0, const float* ei0,
                       float mu_r, int alive, Key vkey, Jmp& J) {
   J.ok = 0; J.n = 0; J.L = 0.0f;
   for (int a = 0; a < 3; ++a) { J.y[a] = 0.0f; J.d[a] = d0[a]; J.er[a] = er0[a]; }
@@ -131,7 +131,7 @@ L_DEV float d_normal_absorptance(const DScene& S, const float* __restrict__ pool
 // appends one deposit record (step.py:546 the deposit's local fields, before the sensor frame: the crossing point,
 // the direction and the normal in world coordinates, the volume entered, the re-emission count, 1 / A_n on a row
 // flagged per_normal) and returns its index (-1 past the scratch's capacity); prev links the photon's records
-L_CALL int d_record(const Run& R, int prev, int sensor, float q, float time, float lam, int gen, int row, float n1,
+L_DEV int d_record(const Run& R, int prev, int sensor, float q, float time, float lam, int gen, int row, float n1,
                     int vol, const float* x, const float* d, const float* nrm) {
   const DScene& S = R.S;
   float inv_an = 1.0f;
@@ -219,13 +219,13 @@ L_DEV QueryT<NF> d_step_query(const Run& R, const PhotonT<NF>& ph, const PreT<NF
 // The GLOSSY outcome's facet path by the row's lobe (surface_event.py:106 _facet_path_branch, :137
 // _dielectric_path_branch): the unified path drawn at the reference width and weighted live over reference, or GLISUR's
 // metal or dielectric path drawn from the cover at the reference width (1 - polish) and weighted exact over cover.
-// Out of line: a detector without glossy rows carries none of it in the step's registers.
+// Behind the outcome's branch: a detector without glossy rows never runs it.
 struct Glossy {
   float d[3];
   float w, wd, dls, sign;
   int far;
 };
-L_CALL void d_glossy(const Run& R, int row, float sig_r, float sig_l, float n1, float n2, const float* wi,
+L_DEV void d_glossy(const Run& R, int row, float sig_r, float sig_l, float n1, float n2, const float* wi,
                      const float* nrm, Key vkey, int want_d, float* er, float* ei, Glossy& g) {
   const DScene& S = R.S;
   int capped = 0;
@@ -738,7 +738,7 @@ L_DEV void d_scint_shares(const DScene& S, const float* __restrict__ pool, const
 // the one defensive mixture (estimator.py:101 defensive_q) and moved to one with light (_base.py:298 lit), its
 // wavelength drawn from its reference spectrum under the defensive cover and weighted to the live one (_base.py:337),
 // an isotropic direction, the component's decay (and rise) delay, a point or a place along the segment
-L_CALL void d_scint_row(const DScene& S, const float* __restrict__ live, const float* __restrict__ ref,
+L_DEV void d_scint_row(const DScene& S, const float* __restrict__ live, const float* __restrict__ ref,
                         const LumenSource& src, const float* f, Key rk, Row& r) {
   const int32_t* m = src.mat;
   const int nc = m[LUMEN_SM_N], seg = m[LUMEN_SM_SEGMENT], rises = m[LUMEN_SM_RISES];

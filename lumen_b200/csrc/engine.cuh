@@ -18,8 +18,9 @@
 using namespace lb;
 
 // ------------------------------------------------------------------------------------------- error handling
-// the calling thread's last error message (defined in lumen_b200.cu)
+// the calling thread's last error message, and the kernels its last call launched (defined in lumen_b200.cu)
 std::string& lumen_err();
+long long& lumen_launches();
 inline int set_err(int code, const std::string& m) {
   lumen_err() = m;
   return code;
@@ -618,6 +619,7 @@ int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
   LB.budget_chunk = (int)(per < 1 ? 1 : (per > 256 ? 256 : per));
   k_trace<G, BLOCK, MINB, TORUS, ANALOG, NAV64><<<grid, BLOCK, 0, stream>>>(LB);
   CK(cudaGetLastError());
+  ++lumen_launches();
   return 0;
 }
 
@@ -625,8 +627,9 @@ int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
 // pool holds up to LUMEN_WAVE_POOL slots (about 350 bytes each with gradients), allocated on the call's stream.
 #define LUMEN_WAVE_POOL (1 << 21)
 template <int G>
-int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStream_t stream) {
-  int64_t want = L.n < LUMEN_WAVE_POOL ? L.n : LUMEN_WAVE_POOL;
+int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStream_t stream, int slots_log2) {
+  const int64_t pool = slots_log2 >= 16 && slots_log2 <= 23 ? (int64_t)1 << slots_log2 : (int64_t)LUMEN_WAVE_POOL;
+  int64_t want = L.n < pool ? L.n : pool;
   int W = (int)((want + 255) / 256 * 256);
   const size_t nph = sizeof(Photon) / 4, nex = sizeof(WaveExtra) / 4, npre = sizeof(Pre) / 4, nq = sizeof(Query) / 4;
   const size_t ng = G > 0 ? LUMEN_MAX_GRAD : 0;
@@ -646,6 +649,7 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
   CK(cudaMemsetAsync(V.act, 0, (size_t)W * 4, stream));
   k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);  // the fill: every slot takes a photon
   CK(cudaGetLastError());
+  ++lumen_launches();
   int st = 0;
   for (long long r = 0;; ++r) {
     if (pk.torus) k_wave_query<G, 1><<<grid, 256, 0, stream>>>(L, V);
@@ -654,6 +658,7 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
     CK(cudaMemsetAsync(V.live, 0, sizeof(unsigned long long), stream));
     k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaGetLastError());
+    lumen_launches() += 2;
     if ((r & 3) == 3) {
       unsigned long long h = 0;
       CK(cudaMemcpyAsync(&h, V.live, sizeof(h), cudaMemcpyDeviceToHost, stream));
@@ -672,6 +677,7 @@ int launch_photons(const Launch& L, int32_t* out_i, float* out_f, cudaStream_t s
   const int64_t grid = (L.n + block - 1) / block;
   k_trace_photons<NAV64><<<(unsigned)grid, block, 0, stream>>>(L, out_i, out_f);
   CK(cudaGetLastError());
+  ++lumen_launches();
   return 0;
 }
 
@@ -681,6 +687,7 @@ int launch_query(const DScene& S, const NF* ray, const int32_t* vol, const int32
   const int block = 128;
   k_query<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(S, ray, vol, srf, t_max, n, out_i, out_f);
   CK(cudaGetLastError());
+  ++lumen_launches();
   return 0;
 }
 
@@ -689,6 +696,7 @@ int launch_locate(const DScene& S, const NF* pts, int64_t n, int32_t* vol, cudaS
   const int block = 128;
   k_locate<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(S, pts, n, vol);
   CK(cudaGetLastError());
+  ++lumen_launches();
   return 0;
 }
 

@@ -27,8 +27,8 @@ LUMEN_SHAPES_8(LUMEN_INST_SHAPE)
 #elif LUMEN_PART == 9
 LUMEN_SHAPES_9(LUMEN_INST_SHAPE)
 #elif LUMEN_PART == 10
-template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t);
-template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t);
+template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
+template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
 #elif LUMEN_PART == 11
 template int launch_photons<0>(const Launch&, int32_t*, float*, cudaStream_t);
 template int launch_photons<1>(const Launch&, int32_t*, float*, cudaStream_t);

@@ -20,13 +20,22 @@ std::string& lumen_err() {
   static thread_local std::string e;
   return e;
 }
+long long& lumen_launches() {
+  static thread_local long long n = 0;
+  return n;
+}
 #define g_err lumen_err()
+// every entry point starts here: no error yet, no kernel launched
+static void begin_call() {
+  lumen_err().clear();
+  lumen_launches() = 0;
+}
 
 // the launchers instantiated in the other parts of the build
 #define LUMEN_EXTERN_SHAPE(G, B, M, T, A, N) extern template LUMEN_SHAPE_DECL(G, B, M, T, A, N)
 LUMEN_SHAPES(LUMEN_EXTERN_SHAPE)
-extern template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t);
-extern template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t);
+extern template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
+extern template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
 extern template int launch_photons<0>(const Launch&, int32_t*, float*, cudaStream_t);
 extern template int launch_photons<1>(const Launch&, int32_t*, float*, cudaStream_t);
 extern template int launch_query<float>(const DScene&, const float*, const int32_t*, const int32_t*, float, int64_t,
@@ -421,6 +430,7 @@ static int launch_bin(const Launch& L, const Pick& pk, const LumenTallies* out, 
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   k_bin<<<sms * 8, 256, 0, stream>>>(B);
   CK(cudaGetLastError());
+  ++lumen_launches();
   return 0;
 }
 
@@ -438,6 +448,7 @@ static int launch_moment_flush(const Tally& T, cudaStream_t stream) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   k_moment_flush<<<sms * 8, 256, 0, stream>>>(T);
   CK(cudaGetLastError());
+  ++lumen_launches();
   return 0;
 }
 
@@ -448,7 +459,7 @@ static int check_cells(const Tally& T) {
 }
 
 static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
-                     cudaStream_t stream, int variant = 0, int bps = 0, int async = 0) {
+                     cudaStream_t stream, int variant = 0, int bps = 0, int async = 0, int slots_log2 = 0) {
   if (variant == LUMEN_VARIANT_WAVEFRONT && async)
     return set_err(LUMEN_ERR_ARG, "the wavefront variant reads its rounds back on the host: not with LUMEN_F_ASYNC");
   Tally& T = L.T;
@@ -517,11 +528,11 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
         L2.T.health = dummy;
         L2.T.counts = (unsigned long long*)(dummy + LUMEN_N_HEALTH);
       }
-      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<LUMEN_MAX_GRAD>(L2, pk, scratch + 3, stream)
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<LUMEN_MAX_GRAD>(L2, pk, scratch + 3, stream, slots_log2)
                                               : launch_trace<LUMEN_MAX_GRAD>(L2, pk, variant, bps, stream);
       if (st) return st;
     } else {
-      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, pk, scratch + 3, stream)
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, pk, scratch + 3, stream, slots_log2)
                                               : launch_trace<0>(L, pk, variant, bps, stream);
       if (st) return st;
     }
@@ -653,7 +664,7 @@ extern "C" {
 int32_t lumen_b200_trace_static(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
                                 uint32_t key1, int64_t first_id, int64_t n, const LumenControls* c, LumenTallies* out,
                                 void* stream) {
-  g_err.clear();
+  begin_call();
   if (!out || !out->arrival || !out->arrival_t || !out->arrival2 || !out->health || !out->counts)
     return set_err(LUMEN_ERR_ARG, "tallies: a required output is null");
   if (c && c->n_grad > 0 && !out->jac) return set_err(LUMEN_ERR_ARG, "tallies: jac is null with gradient parameters");
@@ -671,8 +682,10 @@ int32_t lumen_b200_abi_version(void) { return LUMEN_B200_ABI_VERSION; }
 
 const char* lumen_b200_last_error(void) { return g_err.c_str(); }
 
+int64_t lumen_b200_last_launches(void) { return lumen_launches(); }
+
 int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
-  g_err.clear();
+  begin_call();
   if (!out) return set_err(LUMEN_ERR_ARG, "out is null");
   *out = nullptr;
   int st = check_desc(d);
@@ -847,7 +860,7 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
 }
 
 int32_t lumen_b200_scene_set_pools(LumenScene* sc, const float* live, const float* ref) {
-  g_err.clear();
+  begin_call();
   if (!sc || !live) return set_err(LUMEN_ERR_ARG, "scene or live pool is null");
   if (check_widths(sc, live) || (ref && check_widths(sc, ref))) return LUMEN_ERR_ARG;
   const int n_tab = (int)(sc->tab.size() / 2);
@@ -870,7 +883,7 @@ int32_t lumen_b200_scene_set_pools(LumenScene* sc, const float* live, const floa
 }
 
 int32_t lumen_b200_scene_destroy(LumenScene* sc) {
-  g_err.clear();
+  begin_call();
   if (!sc) return 0;
   for (void* p : sc->allocs) cudaFree(p);
   delete sc;
@@ -880,7 +893,7 @@ int32_t lumen_b200_scene_destroy(LumenScene* sc) {
 int32_t lumen_b200_trace(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
                          uint32_t key1, int64_t first_id, int64_t n, const LumenControls* c, LumenTallies* out,
                          void* stream) {
-  g_err.clear();
+  begin_call();
   if (!out || !out->arrival || !out->arrival_t || !out->arrival2 || !out->health || !out->counts)
     return set_err(LUMEN_ERR_ARG, "tallies: a required output is null");
   if (c && c->n_grad > 0 && !out->jac) return set_err(LUMEN_ERR_ARG, "tallies: jac is null with gradient parameters");
@@ -891,13 +904,13 @@ int32_t lumen_b200_trace(const LumenScene* sc, const LumenRows* rows, const Lume
   int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
   return run_trace(L, pk, out, nullptr, 0, nullptr, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
-                   c->flags & LUMEN_F_ASYNC);
+                   c->flags & LUMEN_F_ASYNC, c->wave_slots_log2);
 }
 
 int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
                            uint32_t key1, int64_t first_id, int64_t n, const LumenControls* c,
                            const double* cotangent, int32_t n_events, double* grads, void* stream) {
-  g_err.clear();
+  begin_call();
   if (!cotangent || !grads) return set_err(LUMEN_ERR_ARG, "adjoint: cotangent and grads are required");
   if (!c || c->n_grad <= 0) return set_err(LUMEN_ERR_ARG, "adjoint: no gradient parameters");
   Launch L;
@@ -906,13 +919,13 @@ int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const Lu
   if (st) return st;
   if (pk.analog) return set_err(LUMEN_ERR_ARG, "the adjoint replays no truth rows");
   return run_trace(L, pk, nullptr, cotangent, n_events, grads, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
-                   c->flags & LUMEN_F_ASYNC);
+                   c->flags & LUMEN_F_ASYNC, c->wave_slots_log2);
 }
 
 int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, const LumenSource* source,
                                  uint32_t key0, uint32_t key1, int64_t first_id, int64_t n,
                                  const LumenControls* c, int32_t* out_i, float* out_f, void* stream) {
-  g_err.clear();
+  begin_call();
   if (!out_i || !out_f) return set_err(LUMEN_ERR_ARG, "trace_photons: outputs are null");
   Launch L;
   Pick pk;
@@ -928,7 +941,7 @@ int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, co
 
 int32_t lumen_b200_query(const LumenScene* sc, const float* ray, const int32_t* vol, const int32_t* srf, float t_max,
                          int64_t n, int32_t* out_i, float* out_f, void* stream) {
-  g_err.clear();
+  begin_call();
   if (!sc || !ray || !vol || !srf || !out_i || !out_f) return set_err(LUMEN_ERR_ARG, "query: a pointer is null");
   if (sc->nav64) return set_err(LUMEN_ERR_ARG, "query: a float64 scene: use lumen_b200_query64");
   if (n == 0) return 0;
@@ -939,7 +952,7 @@ int32_t lumen_b200_query(const LumenScene* sc, const float* ray, const int32_t* 
 }
 
 int32_t lumen_b200_locate(const LumenScene* sc, const float* pts, int64_t n, int32_t* vol, void* stream) {
-  g_err.clear();
+  begin_call();
   if (!sc || !pts || !vol) return set_err(LUMEN_ERR_ARG, "locate: a pointer is null");
   if (sc->nav64) return set_err(LUMEN_ERR_ARG, "locate: a float64 scene: use lumen_b200_locate64");
   if (n == 0) return 0;
@@ -951,7 +964,7 @@ int32_t lumen_b200_locate(const LumenScene* sc, const float* pts, int64_t n, int
 
 int32_t lumen_b200_query64(const LumenScene* sc, const double* ray, const int32_t* vol, const int32_t* srf,
                            double t_max, int64_t n, int32_t* out_i, double* out_f, void* stream) {
-  g_err.clear();
+  begin_call();
   if (!sc || !ray || !vol || !srf || !out_i || !out_f) return set_err(LUMEN_ERR_ARG, "query64: a pointer is null");
   if (!sc->nav64) return set_err(LUMEN_ERR_ARG, "query64: a float32 scene: use lumen_b200_query");
   if (n == 0) return 0;
@@ -962,7 +975,7 @@ int32_t lumen_b200_query64(const LumenScene* sc, const double* ray, const int32_
 }
 
 int32_t lumen_b200_locate64(const LumenScene* sc, const double* pts, int64_t n, int32_t* vol, void* stream) {
-  g_err.clear();
+  begin_call();
   if (!sc || !pts || !vol) return set_err(LUMEN_ERR_ARG, "locate64: a pointer is null");
   if (!sc->nav64) return set_err(LUMEN_ERR_ARG, "locate64: a float32 scene: use lumen_b200_locate");
   if (n == 0) return 0;

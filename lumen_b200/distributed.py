@@ -91,7 +91,7 @@ def simulate_sharded(det, source, params=None, *, samples=None, seed=0, referenc
     ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22, variant=None, jump=True) | (controls or {})
     gnames = list(gradients)
     gt = [det.params_index[k] for k in gnames]
-    variant = ctl["variant"] if ctl["variant"] is not None else (A.VARIANT_WAVEFRONT if gt else 0)
+    variant = ctl["variant"] if ctl["variant"] is not None else A.VARIANT_WAVEFRONT
     c = A.controls(ctl["max_distance"] or 0.0, ctl["roulette"], ctl["max_vertices"], gt, variant=variant,
                    flags=A.F_JUMP if ctl["jump"] else 0)  # fmt: skip
     nb, t0, tw = (0, 0.0, 1.0) if time_bins is None else time_bins

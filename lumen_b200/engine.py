@@ -165,8 +165,10 @@ class Engine:
         src = ctypes.byref(source.c) if source is not None else None
         rw = ctypes.byref(rows.c) if rows is not None else None
         with torch.cuda.device(self.device):
-            A.check(self.lib.lumen_b200_trace(self.h, rw, src, key[0], key[1], first_id, n, ctypes.byref(c),
-                                              ctypes.byref(tallies.c), self._stream(stream)))  # fmt: skip
+            st = self.lib.lumen_b200_trace(self.h, rw, src, key[0], key[1], first_id, n, ctypes.byref(c),
+                                           ctypes.byref(tallies.c), self._stream(stream))  # fmt: skip
+            self.launches = int(self.lib.lumen_b200_last_launches())  # the kernels the call launched
+            A.check(st)
         return tallies
 
     def adjoint(self, key, n, cotangent, *, source=None, rows=None, first_id=0, controls=None, stream=None):
