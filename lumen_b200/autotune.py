@@ -24,7 +24,7 @@ from lumen_b200 import _abi as A
 from lumen_b200.engine import DeviceTallies
 
 _cache: dict = {}
-PHOTONS_PER_SLOT = (1, 2, 4, 8)
+PHOTONS_PER_SLOT = (2, 4, 8, 16, 32)
 
 
 class Shape(NamedTuple):

@@ -678,3 +678,22 @@ def test_step_budget_ends_the_launch_with_an_error(tank, built):
         assert cnt[A.C_ABORTED] == 1 and cnt[A.C_PHOTONS] < n
     T, O = _tallies(tank, src, n)
     np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["cylinder_tank", "lar_box", "solids_box"])
+def test_engine_navigator_matches_the_reference_referee(name, built):
+    """The engine's locate and query kernels on the reference referee's data (tests/test_reference_oracle.py: the
+    reference's float64 Oracle on its own Scene of the detector), at the reference's thresholds."""
+    import test_reference_oracle as R
+
+    det = R.MAKERS[name]()
+    eng = _engine(det)
+    g = R.load(name)
+
+    def query(o, d, v, tm):
+        oi, of = eng.query(o, d, v, None, tm)
+        return oi.cpu().numpy(), of.cpu().numpy()
+
+    bad_pts, bad_rays, n = R.compare(det, g, lambda x: eng.locate(x).cpu().numpy(), query)
+    assert bad_pts <= 2 and bad_rays <= 0.002 * n, (name, bad_pts, bad_rays)
+    eng.close()
