@@ -37,9 +37,11 @@ METRIC = "photons/s on 1 B200 (fwd; batched fwd+adjoint) at matched per-PMT MC e
 L2_FLUSH_BYTES = 256 << 20
 
 
-# DRAM bytes per photon of k_trace<0,256,4> on the tank workload: ncu's dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch of 2^20 photons (2.556 GB + 3.611 GB), almost all of it local memory; it grows with the photons
-TRAFFIC_PER_PHOTON = (2.712409e9 + 3.530416e9) / 1048576
+# DRAM bytes per photon-step of the tank workload, from ncu's dram__bytes_read.sum + dram__bytes_write.sum: the
+# persistent loop k_trace<0,256,4,2,0,0> on one launch of 2^20 photons (2.57 steps each; local memory almost all of
+# it), and the wavefront's k_wave_query<0,2> + k_wave_step<0> summed over every round of seven calls of 2^20 photons
+# (2.76 steps each; 2.655 GB read + 2.101 GB written per call: the slots' state and the kernels' local memory)
+TRAFFIC_PER_STEP = {0: (2.712409e9 + 3.530416e9) / (1048576 * 2.57), 3: (2.655e9 + 2.101e9) / (1048576 * 2.761)}
 
 
 def workload_point(seed=12345):
@@ -542,10 +544,12 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "photon_steps_per_s": world * float(cnt[1]) / (ms_step * 1e-3), "steps_per_photon": steps_pp,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
-                         "traffic": TRAFFIC_PER_PHOTON * n if shape.variant == 0 else None, "peak_kind": pk_kind,
+                         "traffic": (TRAFFIC_PER_STEP[shape.variant] * float(cnt[1])
+                                     if shape.variant in TRAFFIC_PER_STEP else None), "peak_kind": pk_kind,
                          "algorithmic_bytes": alg,
-                         "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-photon launch "
-                                         "of k_trace<0,256,4,2,0,0> on this workload (6.24 GB), scaled by photons"},
+                         "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch shape on "
+                                         "2^20-photon calls of this workload (profiles/k_wave_cylinder_tank.md), per "
+                                         "photon-step, times this step's photon-steps"},
             "e2e": {"value": e2e_v, "unit": "photons/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             # the library's kernels launched in the timed steps (lumen_b200_last_launches: the trace's kernels or the
             # wavefront's rounds, and the moment table's pass)
