@@ -317,9 +317,22 @@ def run_batched(dev, det, reps=3, with_cpu=True):
     err = mc_error(T.arrival.cpu().numpy(), T.arrival2.cpu().numpy(), per_ev)
     vs = chi2_vs_checker(eng, det, src, ds.n_events, gt) if with_cpu else None
     del g
+    # the reverse mode over the same photons: one adjoint replay with a cotangent per event and sensor
+    cot = np.random.default_rng(10).normal(size=jac.shape[:2])
+    ca = A.controls(grad_tabs=gt)
+    eng.adjoint(key, n, cot, source=ds, controls=ca)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ga = eng.adjoint(key, n, cot, source=ds, controls=ca)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ma = e0.elapsed_time(e1)
+    want = np.einsum("es,esp->p", cot, jac)
+    adj = {"value": n / (ma * 1e-3), "unit": "photons/s", "ms_per_launch": ma,
+           "max_rel_diff_to_cot_jac": float(np.max(np.abs(ga.cpu().numpy() - want) / np.abs(want)))}  # fmt: skip
     eng.close()
     return {"value": n / (m * 1e-3), "unit": "photons/s", "events": int(ds.n_events), "photons_per_launch": n,
-            "mc_error": err, "vs_checker": vs,
+            "mc_error": err, "vs_checker": vs, "adjoint_replay": adj,
             "ms_per_launch": m, "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "gradients": names,
             "graph": True, "autotune": {"shape": shape.label(), "ms_sample": {k: round(v, 3) for k, v in times.items()}},
             "jacobian_norm": float(np.abs(jac).sum()), "aborted": int(cnt[5])}  # fmt: skip
@@ -362,12 +375,81 @@ def run_tank_adjoint(dev, src, n, reps=2, with_cpu=True):
     jac = T.jac.cpu().numpy()[0]
     err = mc_error(T.arrival.cpu().numpy(), T.arrival2.cpu().numpy(), [n])
     vs = chi2_vs_checker(eng, det, src, 1, gt) if with_cpu else None
+    adj = adjoint_replay(eng, ds, n, gt, jac, key, dev)
+    fd = fd_check(eng, det, ds, names, gt, key, dev)
     eng.close()
     return {"value": n / (m * 1e-3), "unit": "photons/s", "photons_per_launch": n, "ms_per_launch": m,
             "photon_steps_per_s": float(cnt[1]) / (m * 1e-3), "steps_per_photon": float(cnt[1] / max(cnt[0], 1)),
-            "mc_error": err, "vs_checker": vs, "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
+            "mc_error": err, "vs_checker": vs, "adjoint_replay": adj, "fd_check": fd,
+            "wall": "ground unified, sigma_alpha 0.1", "gradients": names,
             "autotune": {"shape": shape.label(), "ms_sample": {k: round(v, 3) for k, v in times.items()}},
             "jacobian_abs_sum": [float(x) for x in np.abs(jac).sum(0)]}  # fmt: skip
+
+
+def adjoint_replay(eng, ds, n, gt, jac, key, dev, reps=2):
+    """The reverse mode timed: lumen_b200_adjoint replays the run's photons from their keys and contracts every
+    deposit's tangent with a cotangent (one per sensor); the result must be cotangent @ the Jacobian the forward
+    tangents gave on the same photons."""  # noqa: D205, D209
+    import torch
+
+    from lumen_b200 import _abi as A
+
+    cot = np.random.default_rng(9).normal(size=(1, jac.shape[0]))
+    c = A.controls(grad_tabs=gt)
+    g = eng.adjoint(key, n, cot, source=ds, controls=c)
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g = eng.adjoint(key, n, cot, source=ds, controls=c)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    want = cot[0] @ jac
+    rel = float(np.max(np.abs(g.cpu().numpy() - want) / np.maximum(np.abs(want), 1e-300)))
+    m = float(np.median(ms))
+    return {"value": n / (m * 1e-3), "unit": "photons/s", "ms_per_launch": m, "max_rel_diff_to_cot_jac": rel}
+
+
+def fd_check(eng, det, ds, names, gt, key, dev, n=1 << 20, h=0.01, seeds=(0, 1, 2, 3)):
+    """Each parameter's derivative of the summed arrivals against central differences of +-1 % with the reference
+    held (common random numbers), over independent seeds: the mean difference in units of its standard error."""  # noqa: D205, D209
+    import torch
+
+    from lumen_b200 import _abi as A
+    from lumen_b200.engine import DeviceTallies
+
+    base = {k: float(det.params()[k][1][0]) for k in names}
+    c = A.controls(grad_tabs=gt)
+    c0 = A.controls()
+    rows = []
+    for seed in seeds:
+        k = A.key_of_seed(seed)
+        T = DeviceTallies(det.n_sensor, 1, 0, 0.0, 1.0, len(gt), dev)
+        eng.set_pools(det.pool, None)
+        eng.trace(k, n, source=ds, controls=c, tallies=T)
+        d = T.jac.cpu().numpy()[0].sum(0)
+        fd = []
+        for name in names:
+            s = []
+            for sgn in (1.0, -1.0):
+                Tp = DeviceTallies(det.n_sensor, 1, 0, 0.0, 1.0, 0, dev)
+                eng.set_pools(det.pool_with({name: base[name] * (1.0 + sgn * h)}), det.pool)
+                eng.trace(k, n, source=ds, controls=c0, tallies=Tp)
+                s.append(float(Tp.arrival.sum().item()))
+            fd.append((s[0] - s[1]) / (2.0 * h * base[name]))
+        rows.append((d, np.asarray(fd)))
+    eng.set_pools(det.pool, None)
+    torch.cuda.synchronize(dev)
+    D = np.array([r[0] for r in rows])
+    F = np.array([r[1] for r in rows])
+    diff = (D - F).mean(0)
+    se = np.sqrt(D.var(0, ddof=1) / len(seeds) + F.var(0, ddof=1) / len(seeds))
+    se_pair = (D - F).std(0, ddof=1) / np.sqrt(len(seeds))  # the same photons on both sides: the paired error
+    return {"photons": n, "seeds": len(seeds), "step": h, "derivative": [float(x) for x in D.mean(0)],
+            "central_difference": [float(x) for x in F.mean(0)],
+            "diff_in_standard_errors": [float(x) for x in diff / np.maximum(se, 1e-300)],
+            "diff_in_paired_standard_errors": [float(x) for x in diff / np.maximum(se_pair, 1e-300)]}  # fmt: skip
 
 
 def run_lar(dev, n, reps=1, with_cpu=True):
