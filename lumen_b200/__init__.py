@@ -9,9 +9,9 @@ The transport runs in the CUDA library ``lumen_b200/liblumen_b200.so`` (sm_100a)
 ``include/lumen_b200.h``; this package builds detectors, holds device buffers and mirrors lumen's Python API.
 """
 
-from lumen_b200 import autograd, detectors, geometry, optics, sources  # noqa: F401
+from lumen_b200 import autograd, detectors, geometry, optics, reference, sources  # noqa: F401
 from lumen_b200.api import Health, Light, moment_error, pe, simulate  # noqa: F401
 from lumen_b200.detector import Detector, build  # noqa: F401
 
 __all__ = ["simulate", "Light", "Health", "moment_error", "pe", "Detector", "build", "detectors", "sources",
-           "geometry", "optics", "autograd"]  # fmt: skip
+           "geometry", "optics", "autograd", "reference"]  # fmt: skip

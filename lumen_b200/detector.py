@@ -304,6 +304,8 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
                 surf = skins[cls_lv[cb].name]
             is_sensor = (not into_out) and cls_lv[cb].name in sensor_lv
             per_normal = int(is_sensor and sensor_lv[cls_lv[cb].name] in set(after_tracking))
+            if surf is not None and far_opq and O.kills_far_side(surf):  # NoRINDEX before the draw: the absorber
+                surf, is_sensor, per_normal = O.ABSORBER, False, 0
             if surf is None:
                 if into_out or from_out or opaque[cls_mat[cb]] or opaque[cls_mat[ca]]:
                     surf = O.ABSORBER  # the detector volume's boundary; Geant4's NoRINDEX
@@ -334,22 +336,33 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             if k not in col_tab:
                 col_tab[k] = pool.add(row.cols[col], None if row.name.startswith("__") else f"surfaces/{row.name}/{col}")
             row_i[r, 6 + c] = col_tab[k]
+    st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
+    cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}
+    return assemble(nav, vol_cls[:n], n_cls, cls_medium, row_of, med_i, row_i, pool, st, names, cls_names, groups,
+                    precision)  # fmt: skip
+
+
+def assemble(nav: dict, vol_cls, n_cls: int, cls_medium, row_of, med_i, row_i, pool: O.Pool, sensors: SensorTable,
+             names: list, cls_names: dict, groups: dict, precision: str = "float32") -> Detector:
+    """Return the Detector of navigator arrays ``nav`` (``geometry.navigator_arrays``, volumes of classes ``vol_cls``)
+    and the surface lookup's tables: per class its medium (``cls_medium``), per crossed class pair its surface row
+    (``row_of`` (C, C), -1 never crossed), the media's (``med_i``) and rows' (``row_i``) table indices into ``pool``;
+    then the diffusion jump's clearance grids of the media whose only channel is Rayleigh
+    (src/lumen/transport/fastpath.py:96)."""  # noqa: D205, D209
     params_index = dict(pool.names)
     tab, data = pool.arrays()
     arrays = dict(nav)
-    arrays.update(n_cls=n_cls, cls_medium=cls_medium, row_of=row_of.ravel().astype(np.int32), med_i=med_i,
-                  row_i=row_i, tab=tab)  # fmt: skip
-    # the diffusion jump's clearance grids (media whose only channel is Rayleigh; src/lumen/transport/fastpath.py:96)
+    arrays.update(n_cls=int(n_cls), cls_medium=np.asarray(cls_medium, np.int32),
+                  row_of=np.asarray(row_of).ravel().astype(np.int32), med_i=np.asarray(med_i, np.int32),
+                  row_i=np.asarray(row_i, np.int32), tab=tab)  # fmt: skip
     media = []
-    for m in range(len(med_names)):
+    for m in range(len(med_i)):
         ok = med_i[m, 0] >= 0 and med_i[m, 2] >= 0 and med_i[m, 3] < 0 and med_i[m, 7] < 0
         lam = 0.0
         if ok:
             off, k = tab[med_i[m, 2]]
             lam = float(np.min(data[off + k:off + 2 * k].astype(np.float64)))
         media.append((ok, lam))
-    jp = J.prepare(arrays, cls_medium[np.asarray(vol_cls[:n], np.int64)], media)
+    jp = J.prepare(arrays, arrays["cls_medium"][np.asarray(vol_cls, np.int64)], media)
     arrays.update(jump_f=jp["jump_f"], jump_i=jp["jump_i"], clear=jp["clear"], jump_report=jp["report"])
-    st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
-    cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}
-    return Detector(arrays, data, params_index, st, names, cls_names, groups).with_precision(precision)
+    return Detector(arrays, data, params_index, sensors, names, cls_names, groups).with_precision(precision)

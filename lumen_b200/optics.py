@@ -193,6 +193,28 @@ def edge_cover(surf: OpticalSurface, sensor: bool, support) -> int:
     return m
 
 
+FAR_SIDE = (STRAIGHT, REFRACT)  # the outcomes that end beyond the surface (src/lumen/surfaces/outcomes.py:33)
+
+
+def kills_far_side(surf: OpticalSurface) -> bool:
+    """Whether Geant4 kills a photon meeting ``surf`` into a medium without RINDEX before its draw (NoRINDEX): a
+    polished or ground dielectric_dielectric surface (src/lumen/rules/boundary.py:21-27 ``FAR_KILL``; the row is the
+    absorber). A frontpainted finish and a dielectric_metal surface with a TRANSMITTANCE transmit and are absorbed
+    where they land instead (``FAR_ABSORB``, ``surface_row``)."""  # noqa: D205, D209
+    return surf.type == "dielectric_dielectric" and surf.finish not in ("polishedfrontpainted", "groundfrontpainted")
+
+
+def _finish(row: Row, support, surf: OpticalSurface, sensor: bool, far_opaque: bool) -> Row:
+    """Return ``row`` with its far side and cover: into an opaque medium a row with far-side outcomes loses them
+    (src/lumen/surfaces/types.py:543 ``into_opaque``: the flag zeroes their shares, and they leave the outcomes the
+    cover is made of); a row without any keeps the flag off (src/lumen/rules/boundary.py:100)."""  # noqa: D205, D209
+    if far_opaque and any(o in FAR_SIDE for o in support):
+        row.far_opaque = 1
+        support = tuple(o for o in support if o not in FAR_SIDE)
+    row.cover = edge_cover(surf, sensor, support)
+    return row
+
+
 def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=None) -> Row:
     """Return the row of a Geant4 surface (types.py:445-493 types, :557 no_detection); ``entry_eff``: a sensor's
     detection on entry instead of EFFICIENCY (1 where its sensor model applies the QE after tracking,
@@ -207,8 +229,7 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
                 "p_spike": 1.0 if surf.finish == "polishedfrontpainted" else 0.0, "p_lobe": 0.0, "p_back": 0.0}  # fmt: skip
         # support: the straight share (T is read at its default), and the finish's half of the split (types.py:425)
         sup = (STRAIGHT, SPECULAR if surf.finish == "polishedfrontpainted" else DIFFUSE)
-        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-                   cover=edge_cover(surf, sensor, sup))  # fmt: skip
+        return _finish(Row(MODEL_REFLECT, normal=1, cols=cols, name=surf.name), sup, surf, sensor, far_opaque)
     if surf.type == "dielectric_metal" and (surf.rindex is not None or surf.kindex is not None):
         # PHOTOCATHODE (types.py:455): the complex index's Fresnel reflectance, specular; the rest detected with eff
         if surf.rindex is None or surf.kindex is None or surf.finish != "polished":
@@ -216,8 +237,7 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
         cols = {"nr": surf.rindex, "nk": surf.kindex, "eff": eff,
                 "T": 0.0 if surf.transmittance is None else surf.transmittance}  # fmt: skip
         sup = (SPECULAR,) + ((STRAIGHT,) if surf.transmittance is not None else ())  # types.py:455, :494
-        return Row(MODEL_COMPLEX, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-                   cover=edge_cover(surf, sensor, sup))  # fmt: skip
+        return _finish(Row(MODEL_COMPLEX, cols=cols, name=surf.name), sup, surf, sensor, far_opaque)
     if surf.type == "dielectric_dielectric":
         if surf.finish != "polished" and surf.model == "glisur" and surf.polish < 1.0:
             # GLISUR_DIELECTRIC (types.py:463): the cuts, then below R the GLISUR facet path that reflects or refracts
@@ -225,15 +245,15 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
             cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
                     "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff, "p_spike": 0.0,
                     "p_lobe": 1.0, "p_back": 0.0, "polish": float(surf.polish)}  # fmt: skip
-            return Row(MODEL_REFLECT, glisur=2, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-                       cover=edge_cover(surf, sensor, (GLOSSY, STRAIGHT)))  # fmt: skip
+            row = Row(MODEL_REFLECT, glisur=2, cols=cols, name=surf.name)
+            return _finish(row, (GLOSSY, STRAIGHT), surf, sensor, far_opaque)
         if surf.finish != "polished" and not (surf.model == "glisur" and surf.polish >= 1.0):
             raise NotImplementedError("dielectric_dielectric ground with the unified model is not built")
         cols = {"R": 1.0 if surf.reflectivity is None else surf.reflectivity,
                 "T": 0.0 if surf.transmittance is None else surf.transmittance, "eff": eff}  # fmt: skip
         # DIELECTRIC_RT (types.py:444): refract, specular, straight
-        return Row(MODEL_DIELECTRIC, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-                   cover=edge_cover(surf, sensor, (REFRACT, SPECULAR, STRAIGHT)))  # fmt: skip
+        row = Row(MODEL_DIELECTRIC, cols=cols, name=surf.name)
+        return _finish(row, (REFRACT, SPECULAR, STRAIGHT), surf, sensor, far_opaque)
     # dielectric_metal
     R = 1.0 if surf.reflectivity is None else surf.reflectivity
     cols = {"R": R, "eff": eff, "T": 0.0 if surf.transmittance is None else surf.transmittance}
@@ -241,12 +261,12 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
     if surf.model == "glisur" and surf.finish != "polished" and surf.polish < 1.0:
         # GLISUR_METAL (types.py:459): R into the GLISUR facet path of radius 1 - polish
         cols.update({"p_spike": 0.0, "p_lobe": 1.0, "p_back": 0.0, "polish": float(surf.polish)})
-        return Row(MODEL_REFLECT, glisur=1, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-                   cover=edge_cover(surf, sensor, (GLOSSY, *tr)))  # fmt: skip
+        row = Row(MODEL_REFLECT, glisur=1, cols=cols, name=surf.name)
+        return _finish(row, (GLOSSY, *tr), surf, sensor, far_opaque)
     if surf.finish == "polished" or surf.model == "glisur":
         cols["p_spike"] = 1.0  # polished, or GLISUR at polish 1: the mirror (types.py:573 SPECULAR_METAL)
-        return Row(MODEL_REFLECT, normal=1, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-                   cover=edge_cover(surf, sensor, (SPECULAR, *tr)))  # fmt: skip
+        row = Row(MODEL_REFLECT, normal=1, cols=cols, name=surf.name)
+        return _finish(row, (SPECULAR, *tr), surf, sensor, far_opaque)
     ss = 0.0 if surf.specularspike is None else surf.specularspike
     sl = 0.0 if surf.specularlobe is None else surf.specularlobe
     bs = 0.0 if surf.backscatter is None else surf.backscatter
@@ -258,8 +278,8 @@ def surface_row(surf: OpticalSurface, sensor: bool, far_opaque: bool, entry_eff=
     # UNIFIED_METAL_NORMAL (types.py:471: its support rule reads fixed constants only, and these are read values)
     # or UNIFIED_METAL (types.py:467)
     sup = (SPECULAR, BACKSCATTER, DIFFUSE) if normal else (SPECULAR, BACKSCATTER, GLOSSY, DIFFUSE)
-    return Row(MODEL_REFLECT, normal=normal, far_opaque=int(far_opaque), cols=cols, name=surf.name,
-               cover=edge_cover(surf, sensor, (*sup, *tr)))  # fmt: skip
+    row = Row(MODEL_REFLECT, normal=normal, cols=cols, name=surf.name)
+    return _finish(row, (*sup, *tr), surf, sensor, far_opaque)
 
 
 class Pool:

@@ -1,0 +1,320 @@
+"""Detectors from the reference's own host pipeline: a loaded ``lumen.Detector`` as this package's ``Detector``.
+
+    data = reference.export(ref_det)     # the reference's compiled products as plain data (JSON-able)
+    det = reference.detector(data)       # a lumen_b200.detector.Detector: simulate(det, ...) runs it
+    det = reference.from_reference(ref_det)
+
+``ref_det`` is what ``lumen.load(path)`` returns (src/lumen/api.py:310). ``export`` reads the products the reference's
+photon loop is built from, and re-derives none of them:
+
+- the navigator's scene (``Parts.nav_scene``; ``scene.instances``, src/lumen/geometry/scene.py:151): every instance
+  of a definition with a member is a navigator volume (its world pose composed by the reference's walk, its parent
+  the nearest such ancestor), each member's solid as the reference flattens it (``solids.Compiled``,
+  src/lumen/geometry/solids.py:200: the transforms baked into the leaves, one origin for the solid's quadric leaves,
+  coplanar planes made identical) with its box (``solids.node_bbox``);
+- the compiled optics (``lookup.Optics``, src/lumen/build/lookup.py:394): the class of every placed volume by its PV
+  path, the medium of every class, the surface row of every crossed class pair (``row_of``), each row's Interaction,
+  flags and outcome support (``lookup.SurfaceTable``, lookup.py:360), the sensor tags;
+- the packed parameters at the detector's own values (``pack.pack``, src/lumen/build/pack.py:84): each row's column
+  and each medium's tables, float32 as the reference's step reads them;
+- the defensive rows (``api._edge_rows``, src/lumen/api.py:797): a row the estimator covers gets its support as its
+  cover mask;
+- the parameter keys (``Parts.key_rows``): a table read directly from a key is named by the key
+  ("materials/Water/ABSLENGTH", "surfaces/Liner/REFLECTIVITY"), so ``simulate(det, src, params={key: ...})`` and its
+  ``gradients`` take the reference's names; a table with no key of its own keeps this package's name
+  ("media/Water/rayleigh": a table derived from RINDEX; "surfaces/<surface>/<column>").
+
+``detector`` then builds this package's navigator arrays (a BVH per volume over the same leaves and poses) and the C
+ABI's tables from that data: the reference's classes, media, rows and values, one table per key. The leaves and
+values are the reference's bits; the navigator's arrays are this package's layout of them.
+
+Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: meshes, split
+unions (``Definition.piece_of``), a medium channel other than Rayleigh, a vertex on the class table's diagonal (a skin
+between touching volumes of one class), a deposit to the tag before (``Optics.deposit_pre``) and born sensors
+(``Optics.born_pair``). A pass row (``types.PASS``: two classes of one medium split by a role elsewhere) becomes a
+row that carries the photon straight on: the reference steps over such a crossing, this navigator stops at it and
+continues it unchanged, so the two draw other random numbers for the same law (the same expected values).
+"""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+
+from lumen_b200 import detector as D
+from lumen_b200 import geometry as G
+from lumen_b200 import optics as O
+
+FORMAT = "lumen_b200-reference-detector/1"
+OUTSIDE_PV = "<outside>"  # the outside's PV name in the reference's class table (src/lumen/build/tree.py OUTSIDE_PV)
+MODELS = {"g4.reflect": O.MODEL_REFLECT, "g4.dielectric": O.MODEL_DIELECTRIC, "g4.complex": O.MODEL_COMPLEX}
+GLISUR_LOBES = {"glisur": 1, "glisur_dielectric": 2}  # GLISUR_METAL, GLISUR_DIELECTRIC (src/lumen/surfaces/types.py)
+OPS = {"union": 1, "inter": 2, "sub": 3}  # the postfix program's opcodes (include/lumen_b200.h)
+DIRECT = ("value", "constant", "setting", "default")  # key_rows columns read from a key as they are (build/pack.py)
+
+
+# ------------------------------------------------------------------------------------------------------ export
+def _f(x):
+    return np.asarray(x, np.float64).tolist()
+
+
+def _leaf_data(lf) -> dict:
+    if lf.kind == "q":
+        return {"kind": "q", "A": _f(lf.A), "b": _f(lf.b), "c": float(lf.c), "has_q": bool(lf.has_q), "N": _f(lf.N),
+                "H": _f(lf.H), "origin": _f(lf.origin), "qo": _f(lf.qo)}  # fmt: skip
+    if lf.kind == "torus":
+        return {"kind": "torus", "R": float(lf.R), "r": float(lf.r), "lin": _f(lf.lin), "origin": _f(lf.origin)}
+    raise NotImplementedError(f"a leaf of kind {lf.kind!r}")
+
+
+def _solid_data(node) -> dict:
+    from lumen.geometry import solids
+
+    comp = solids.Compiled(node)
+    lo, hi = solids.node_bbox(node)
+    return {"leaves": [_leaf_data(lf) for lf in comp.leaves], "expr": comp.expr, "lo": _f(lo), "hi": _f(hi)}
+
+
+def _table(t) -> list:
+    """A packed (energy, value) table, or a constant, as [energies, values] (float32 values as float64 numbers)."""
+    if isinstance(t, dict):
+        return [_f(np.asarray(t["energy"], np.float32)), _f(np.asarray(t["value"], np.float32))]
+    return float(np.float32(t))
+
+
+def export(det) -> dict:
+    """Return the products of a loaded reference detector (``lumen.load``) that its photon loop runs on, as plain
+    data (lists, numbers and strings: ``json.dumps`` keeps every float64 exactly); the module docstring says which."""  # noqa: D205, D209
+    from lumen import api
+    from lumen.build import pack
+    from lumen.geometry import scene as sc
+
+    parts = det.parts
+    scene, optics = parts.nav_scene, parts.optics
+    T = sc.instances(scene)
+    solids, volumes, vol_of_inst = {}, [], {}
+    for i, dname in enumerate(T.defn):
+        d = scene.definitions[dname]
+        if d.member is None:
+            continue
+        if isinstance(d.member.solid, sc.Mesh):
+            raise NotImplementedError(f"{dname}: a mesh (tessellated solid) is not converted")
+        if d.piece_of:
+            raise NotImplementedError(f"{dname}: a piece of a split union is not converted")
+        if dname not in solids:
+            solids[dname] = _solid_data(d.member.solid)
+        p = int(T.parent[i])
+        while p >= 0 and p not in vol_of_inst:  # an assembly places its daughters in the nearest ancestor volume
+            p = int(T.parent[p])
+        vol_of_inst[i] = len(volumes)
+        seg = sc.member_segment(d, dname)
+        volumes.append({"pv": f"{T.path[i]}/{seg}" if T.path[i] else seg, "path": T.path[i], "definition": dname,
+                        "parent": vol_of_inst[p] if p >= 0 else -1, "R": _f(T.R[i]), "t": _f(T.t[i])})  # fmt: skip
+    if optics.deposit_pre is not None and np.any(optics.deposit_pre):
+        raise NotImplementedError("a sensor depositing to the tag before (Optics.deposit_pre) is not converted")
+    if optics.born_pair is not None and np.any(np.asarray(optics.born_pair) >= 0):
+        raise NotImplementedError("a sensor counting photons born inside it (Optics.born_pair) is not converted")
+    packed = pack.pack(det, det.params())
+    keys = {}  # packed path -> the key it is read from directly
+    for path, src in parts.key_rows.items():
+        if src.key is not None and src.column in DIRECT:
+            keys["/".join(str(x) for x in path)] = src.key
+    tab = optics.table
+    edge = set(api._edge_rows(det).surfaces)
+    rows = []
+    for r, row in enumerate(optics.rows):
+        model = tab.models[int(tab.flags.model[r])].name
+        glisur = 0
+        if bool(tab.flags.glisur[r]):
+            glisur = GLISUR_LOBES[tab.lobes[int(tab.lobe_of[r])]]
+        cols, col_keys = {}, {}
+        for c in O.COLUMNS:
+            v = packed["surfaces"].get(c)
+            reads = c in tab.reads[r]
+            if v is None or (isinstance(v, dict) and not reads):
+                cols[c] = float(np.float32(tab.consts[c][r]))
+            elif isinstance(v, dict):
+                cols[c] = [_f(np.asarray(v["energy"], np.float32)[r]), _f(np.asarray(v["value"], np.float32)[r])]
+            else:
+                cols[c] = float(np.float32(np.asarray(v)[r]))
+            if reads and row.origin is not None:
+                section, _, entry = row.origin.partition(":")
+                base = f"{'surfaces' if section == 'surface' else 'sensors'}/{entry}/{tab.reads[r][c]}"
+                key = keys.get(base + "/value", keys.get(base))
+                if key is not None:
+                    col_keys[c] = key
+        rows.append({"type": row.surface_type.name, "origin": row.origin, "model": model, "reads": sorted(tab.reads[r]),
+                     "normal": bool(tab.flags.normal[r]), "glisur": glisur, "far_opaque": bool(tab.flags.far_opaque[r]),
+                     "per_normal": bool(tab.flags.per_normal[r]), "support": [bool(x) for x in tab.support[r]],
+                     "edge": r in edge, "cols": cols, "keys": col_keys})  # fmt: skip
+    media = []
+    for m, name in zip(optics.media, optics.media_names, strict=True):
+        pm = packed["media"][name]
+        entry = {"name": name, "opaque": bool(m.opaque), "tables": {}, "keys": {}}
+        for part in ("index", "absorption"):
+            if part in pm:
+                entry["tables"][part] = _table(pm[part])
+                key = keys.get(f"media/{name}/{part}/value")
+                if key is not None:
+                    entry["keys"][part] = key
+        for ch in m.channels:
+            if ch.name != "rayleigh" or ch.emission is not None:
+                raise NotImplementedError(f"medium {name}: channel {ch.name!r} is not converted (Rayleigh only)")
+            entry["tables"]["rayleigh"] = _table(pm["rayleigh"]["length"])
+            key = keys.get(f"media/{name}/rayleigh/length/value")
+            if key is not None:
+                entry["keys"]["rayleigh"] = key
+        media.append(entry)
+    row_of = np.asarray(optics.row_of, np.int64)
+    if np.any(np.diag(row_of) >= 0):
+        raise NotImplementedError("a vertex between two volumes of one class (a skin of touching siblings) is not "
+                                  "converted")  # fmt: skip
+    st = det.sensor_table()
+    return {"format": FORMAT, "name": det.name, "precision": det.precision, "solids": solids, "volumes": volumes,
+            "n_classes": int(optics.n_classes), "class_names": list(optics.class_names),
+            "class_of": {k: int(v) for k, v in optics.class_of.items()},
+            "medium_of": [int(x) for x in optics.medium_of], "media": media, "row_of": row_of.tolist(), "rows": rows,
+            "sensor_index": {k: int(v) for k, v in optics.sensor_index.items()},
+            "sensors": {"name": list(st.name), "sensor": list(st.sensor), "position": _f(st.position),
+                        "axis": _f(st.axis)}}  # fmt: skip
+
+
+def save(data: dict, path) -> None:
+    """Write exported data as JSON (every float64 round-trips exactly)."""
+    with open(path, "w") as f:
+        json.dump(data, f, separators=(",", ":"))
+
+
+def load(path) -> dict:
+    with open(path) as f:
+        data = json.load(f)
+    if data.get("format") != FORMAT:
+        raise ValueError(f"{path}: not exported reference detector data ({FORMAT})")
+    return data
+
+
+# ------------------------------------------------------------------------------------------------------ import
+class Flattened(G.Solid):
+    """A solid given as the reference flattened it: leaves in the solid's frame and its boolean expression."""
+
+    def __init__(self, data: dict):
+        self.data = data
+        self._low = None
+
+    def lower(self) -> G.Lowered:
+        if self._low is None:
+            self._low = _lowered(self.data)
+        return self._low
+
+
+def _leaf(d: dict) -> G.Leaf:
+    """This package's leaf of a reference leaf: a quadric about origin + qo in its own frame (``solids.quad_frame``),
+    the planes about origin; a torus in the canonical coordinates u = lin^-1 (x - origin)."""  # noqa: D205, D209
+    og = np.asarray(d["origin"], float)
+    if d["kind"] == "torus":
+        return G.Leaf(False, og=og, oq=og.copy(), torus=(float(d["R"]), float(d["r"])),
+                      M=np.linalg.inv(np.asarray(d["lin"], float)))  # fmt: skip
+    A, b, c = np.asarray(d["A"], float), np.asarray(d["b"], float), float(d["c"])
+    qo = np.asarray(d["qo"], float)
+    bq, cq = b + A @ qo, float(qo @ A @ qo + 2.0 * b @ qo + c)
+    N = np.asarray(d["N"], float).reshape(-1, 3)
+    return G.Leaf(bool(d["has_q"]), A, bq, cq, og + qo, og, N, np.asarray(d["H"], float).reshape(-1))
+
+
+def _program(expr) -> list:
+    if isinstance(expr, int):
+        return [(0, expr)]
+    op, a, b = expr
+    return _program(a) + _program(b) + [(OPS[op], 0)]
+
+
+def _lowered(data: dict) -> G.Lowered:
+    return G.Lowered([_leaf(d) for d in data["leaves"]], _program(data["expr"]), np.asarray(data["lo"], float),
+                     np.asarray(data["hi"], float))  # fmt: skip
+
+
+def _add(pool: O.Pool, t, name=None) -> int:
+    if isinstance(t, list):
+        return pool.add((np.asarray(t[0], np.float64), np.asarray(t[1], np.float64)), name)
+    return pool.add(float(t), name)
+
+
+def detector(data: dict, precision: str | None = None) -> D.Detector:
+    """Return this package's Detector of exported reference data (``export``, ``load``); ``precision``: the
+    navigator's (default: the reference detector's)."""  # noqa: D205, D209
+    if data.get("format") != FORMAT:
+        raise ValueError(f"not exported reference detector data ({FORMAT})")
+    solids = {k: Flattened(v) for k, v in data["solids"].items()}
+    vols = data["volumes"]
+    med_names = [m["name"] for m in data["media"]]
+    medium_of = np.asarray(data["medium_of"], np.int32)
+    class_of = data["class_of"]
+    lvs = {}
+    placed = []
+    for v in vols:
+        dn = v["definition"]
+        if dn not in lvs:
+            cls = class_of[v["pv"]]
+            lvs[dn] = G.Volume(dn, solids[dn], med_names[medium_of[cls]])
+        depth = 0 if v["parent"] < 0 else placed[v["parent"]].depth + 1
+        placed.append(G.Placed(v["pv"], lvs[dn], np.asarray(v["R"], float), np.asarray(v["t"], float),
+                               int(v["parent"]), depth))  # fmt: skip
+    vol_cls = [int(class_of[v["pv"]]) for v in vols]
+    out_cls = int(class_of[OUTSIDE_PV])
+    sensor_index = data["sensor_index"]
+    vol_sensor = np.asarray([sensor_index.get(v["pv"], -1) for v in vols], np.int32)
+    nav = G.navigator_arrays(placed, vol_cls, out_cls, vol_sensor)
+    pool = O.Pool()
+    by_key = {}  # key -> table: one table per key, shared by every row reading it
+
+    def keyed(t, key, name):
+        if key is None:
+            return _add(pool, t, name)
+        if key not in by_key:
+            by_key[key] = _add(pool, t, key)
+        else:
+            off, k = pool.tabs[by_key[key]]
+            e, y = O.table(tuple(np.asarray(x, np.float64) for x in t) if isinstance(t, list) else t)
+            have = np.asarray(pool.data[off:off + 2 * k], np.float32)
+            if len(e) != k or not np.array_equal(have, np.concatenate([np.float32(e), np.float32(y)])):
+                raise ValueError(f"key {key}: read with different values by two rows")
+        return by_key[key]
+
+    med_i = np.full((len(data["media"]), 16), -1, np.int32)
+    for m, med in enumerate(data["media"]):
+        for slot, part in ((0, "index"), (1, "absorption"), (2, "rayleigh")):
+            if part in med["tables"]:
+                med_i[m, slot] = keyed(med["tables"][part], med["keys"].get(part), f"media/{med['name']}/{part}")
+    rows = data["rows"]
+    row_i = np.zeros((len(rows), 16), np.int32)
+    for r, row in enumerate(rows):
+        cover = 0
+        if row["edge"]:
+            for o, s in enumerate(row["support"]):
+                cover |= int(s) << o
+        if row["type"] == "pass":  # straight on, unchanged (the module docstring)
+            row = dict(row, cols=dict(row["cols"], T=1.0, R=0.0))
+        row_i[r, 0:6] = [MODELS[row["model"]], int(row["normal"]), int(row["glisur"]), int(row["far_opaque"]),
+                         int(row["per_normal"]), cover]  # fmt: skip
+        section, _, entry = (row["origin"] or "").partition(":")
+        for c, col in enumerate(O.COLUMNS):
+            name = None  # a column the row reads as a parameter, with no key of its own: this package's name
+            if col in row["reads"] and row["origin"]:
+                name = f"{'surfaces' if section == 'surface' else 'sensors'}/{entry}/{col}"
+            row_i[r, 6 + c] = keyed(row["cols"][col], row["keys"].get(col), name)
+    s = data["sensors"]
+    groups = {}
+    for i, entry in enumerate(s["sensor"]):
+        groups.setdefault(entry.split(":", 1)[0], []).append(i)
+    st = D.SensorTable(list(s["name"]), [e.split(":", 1)[0] for e in s["sensor"]],
+                       np.asarray(s["position"], float).reshape(-1, 3), np.asarray(s["axis"], float).reshape(-1, 3))  # fmt: skip
+    names = [v["pv"] for v in vols]
+    cls_names = dict(enumerate(data["class_names"]))
+    return D.assemble(nav, vol_cls, int(data["n_classes"]), medium_of, np.asarray(data["row_of"]), med_i, row_i, pool,
+                      st, names, cls_names, groups, precision or data.get("precision", "float32"))  # fmt: skip
+
+
+def from_reference(det, precision: str | None = None) -> D.Detector:
+    """Return this package's Detector of a loaded reference detector (``lumen.load``): ``detector(export(det))``."""
+    return detector(export(det), precision)

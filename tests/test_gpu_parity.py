@@ -697,3 +697,32 @@ def test_engine_navigator_matches_the_reference_referee(name, built):
     bad_pts, bad_rays, n = R.compare(det, g, lambda x: eng.locate(x).cpu().numpy(), query)
     assert bad_pts <= 2 and bad_rays <= 0.002 * n, (name, bad_pts, bad_rays)
     eng.close()
+
+
+@pytest.fixture(scope="module")
+def ref_dets():
+    """The reference pipeline's own detectors (tests/golden/refdet_*.json, ``lumen_b200.reference``)."""
+    import os
+
+    from lumen_b200 import reference
+
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    return {n: reference.detector(reference.load(os.path.join(gold, f"refdet_{n}.json")))
+            for n in ("example_tank", "yaml_toy")}  # fmt: skip
+
+
+@pytest.mark.parametrize(("name", "pos", "n_photons"), [("example_tank", (0.0, 0.0, 0.1), 2e5),
+                                                        ("yaml_toy", (0.1, 0.0, 0.2), 1e5)])  # fmt: skip
+def test_reference_pipeline_detectors_match(name, pos, n_photons, ref_dets, built):
+    """The detectors the reference's own pipeline compiled: per-photon records bit-exact, then the tallies, the
+    published runs' workloads (the toy tank's arrivals are the published table: tests/test_reference_detector.py)."""  # noqa: D205, D209
+    det = ref_dets[name]
+    src = sources.Point(position=pos, n_photons=n_photons, lam=400.0)
+    bad, gi, oi, gf, of = _records_match(det, src, 1 << 15, samples=1 << 18)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+    for variant in (0, A.VARIANT_WAVEFRONT):
+        T, O = _tallies(det, src, 1 << 18, controls=A.controls(variant=variant))
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL)
+        np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
+        np.testing.assert_allclose(T.arrival_t.cpu().numpy(), O.arrival_t, rtol=RTOL)
+        assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()

@@ -1,0 +1,139 @@
+"""Detectors from the reference's own host pipeline (``lumen_b200.reference``), against the reference's published runs.
+
+``tests/golden/make_reference_detector.py`` had the reference convert and load its two shipped example detectors
+(the tutorial's toy tank from examples/data/example_tank.gdml, the YAML toy from examples/data/yaml_toy) and wrote
+what its photon loop runs on: the navigator scene's instances and flattened solids, the compiled optics (classes,
+media, the surface table's rows with their Interactions, flags and supports), the packed parameters, the defensive
+rows. Here ``reference.detector`` rebuilds them and the checker runs them:
+
+- the toy tank reproduces the reference's published tutorial run (docs/tutorial/first-hour.md:101-111) to every
+  printed digit, and is bit for bit the toy tank this package's own builder makes;
+- the YAML toy (a tube tank with a ground unified liner, sigma_alpha 0.1, and six disc PMTs) agrees with its
+  published run (docs/howto/yaml-detector.md:163, ``arrivals: [518.1 112.9 264.9 148.4 196.5 193.8]``) within the
+  run's Monte Carlo error (chi^2 against the mean of 24 seeds), and is bit for bit the same detector built from
+  its description by this package's builder. The published numbers are another sequence of draws of the same law
+  (no seed of the checker reproduces them: they came from another version of the reference's random stream), so
+  the pin is statistical.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from lumen_b200 import _abi as A
+from lumen_b200 import api, detectors, reference, sources
+from lumen_b200 import detector as D
+from lumen_b200 import geometry as G
+from lumen_b200 import optics as O
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+KEY0 = A.key_of_seed(0)
+N = 1 << 18
+RTOL = 1e-12  # FP64 sums of the same photons' deposits over the checker's threads, in another order
+PUB_TOY = [394.54, 913.75, 547.76, 501.74, 515.31, 528.14, 320.36, 340.68]  # docs/tutorial/first-hour.md:101-111
+PUB_TOY_ERR = [17.22, 26.23, 20.30, 19.43, 19.69, 19.94, 15.51, 16.03]
+PUB_YAML = [518.1, 112.9, 264.9, 148.4, 196.5, 193.8]  # docs/howto/yaml-detector.md:163
+TOY_SRC = sources.Point(position=(0.0, 0.0, 0.1), n_photons=2e5, lam=400.0)
+YAML_SRC = sources.Point(position=(0.1, 0.0, 0.2), n_photons=1e5, lam=400.0)
+
+
+def converted(name):
+    return reference.detector(reference.load(os.path.join(GOLD, f"refdet_{name}.json")))
+
+
+@pytest.fixture(scope="module")
+def toy():
+    return converted("example_tank")
+
+
+@pytest.fixture(scope="module")
+def yaml_toy():
+    return converted("yaml_toy")
+
+
+def yaml_toy_own(data):
+    """The YAML toy from its description (examples/data/yaml_toy) through this package's builder, the PMTs at the
+    poses and the tables on the knots the reference's conversion gave (RINDEX was written on wavelengths)."""  # noqa: D205, D209
+    med = {m["name"]: m for m in data["media"]}["Water"]["tables"]
+    water = O.Material("Water", rindex=tuple(med["index"]), abslength=tuple(med["absorption"]))
+    tank = G.Volume("Tank", G.Tube(rmax=0.5, dz=0.5), "Water")
+    pmt = G.Volume("PMT", G.Tube(rmax=0.04, dz=0.01), "Glass")
+    for v in data["volumes"]:
+        if v["definition"] == "PMT":
+            tank.place(pmt, v["t"], v["R"], name=v["path"].split("/")[-1])
+    liner = O.OpticalSurface("Liner", "dielectric_metal", "ground", "unified", sigma_alpha=0.1,
+                             reflectivity=([1.5, 5.0], [0.1, 0.1]))  # fmt: skip
+    cathode = O.OpticalSurface("Cathode", "dielectric_metal", "polished", reflectivity=([1.5, 5.0], [0.0, 0.0]),
+                               efficiency=([1.5, 5.0], [1.0, 1.0]))  # fmt: skip
+    borders = [("Tank", p.name, cathode) for p in tank.daughters]
+    return D.build(tank, {"Water": water, "Glass": O.Material("Glass")}, borders=borders, skins={"Tank": liner},
+                   sensors={"pmt": "PMT"}, after_tracking=("pmt",))  # fmt: skip
+
+
+def test_fixtures_hold_the_reference_products():
+    for name, n_vol, n_sensor in (("example_tank", 9, 8), ("yaml_toy", 7, 6)):
+        x = reference.load(os.path.join(GOLD, f"refdet_{name}.json"))
+        assert len(x["volumes"]) == n_vol and len(x["sensors"]["name"]) == n_sensor
+        assert x["class_of"][reference.OUTSIDE_PV] >= 0 and all(r["model"] in reference.MODELS for r in x["rows"])
+        assert any(r["edge"] for r in x["rows"])  # the defensive rows came with them
+
+
+def test_toy_tank_from_the_reference_pipeline_is_the_published_run(toy):
+    T, _ = oracle.trace(toy, KEY0, N, source=TOY_SRC, samples=N)
+    arr = T.arrival[0]
+    np.testing.assert_allclose(arr, PUB_TOY, atol=0.0051)
+    np.testing.assert_allclose(api.moment_error(T.arrival2[0], arr, N), PUB_TOY_ERR, atol=0.0051)
+    assert T.counts[A.C_DEPOSITS] == 5735  # the current rule's records (tests/test_oracle.py)
+    own, _ = oracle.trace(detectors.toy_tank(), KEY0, N, source=TOY_SRC, samples=N)
+    for a, b in ((own.arrival, T.arrival), (own.arrival2, T.arrival2), (own.arrival_t, T.arrival_t)):
+        np.testing.assert_allclose(a, b, rtol=RTOL)  # the same photons: the threads' summation order only
+    assert np.array_equal(own.counts, T.counts)
+
+
+def test_parameters_carry_the_reference_keys(toy, yaml_toy):
+    for key in ("materials/Water/RINDEX", "materials/Water/ABSLENGTH", "surfaces/CathodeSurface/REFLECTIVITY"):
+        assert key in toy.params_index
+    for key in ("surfaces/Liner/REFLECTIVITY", "surfaces/Liner/sigma_alpha", "surfaces/Cathode/REFLECTIVITY"):
+        assert key in yaml_toy.params_index
+    # a value given by its key moves the run as the same table of this package's own builder does
+    n = 1 << 14
+    a, _ = oracle.trace(toy, KEY0, n, source=TOY_SRC, samples=n,
+                        pool_live=toy.pool_with({"materials/Water/ABSLENGTH": 10.0}), pool_ref=toy.pool)  # fmt: skip
+    own = detectors.toy_tank()
+    b, _ = oracle.trace(own, KEY0, n, source=TOY_SRC, samples=n,
+                        pool_live=own.pool_with({"media/Water/absorption": 10.0}), pool_ref=own.pool)  # fmt: skip
+    np.testing.assert_allclose(a.arrival, b.arrival, rtol=RTOL)
+
+
+def test_yaml_toy_from_the_reference_pipeline_matches_its_published_run(yaml_toy):
+    runs, err = [], []
+    for seed in range(24):
+        T, _ = oracle.trace(yaml_toy, A.key_of_seed(seed), N, source=YAML_SRC, samples=N)
+        runs.append(T.arrival[0])
+        err.append(api.moment_error(T.arrival2[0], T.arrival[0], N))
+    mean, sd = np.mean(runs, 0), np.mean(err, 0)
+    chi2 = float(np.sum(((np.asarray(PUB_YAML) - mean) / sd) ** 2))  # the published run's own error dominates
+    assert chi2 / len(PUB_YAML) < 3.0, (mean, sd, chi2)
+    assert np.all(np.abs(np.asarray(PUB_YAML) - mean) < 3.5 * sd)
+
+
+def test_yaml_toy_is_the_detector_its_description_builds(yaml_toy):
+    data = reference.load(os.path.join(GOLD, "refdet_yaml_toy.json"))
+    own = yaml_toy_own(data)
+    rows_ref = yaml_toy.arrays["row_i"].reshape(-1, 16)[:, :6]
+    rows_own = own.arrays["row_i"].reshape(-1, 16)[:, :6]
+    assert set(map(tuple, rows_ref)) == set(map(tuple, rows_own[rows_own[:, 5] > 0]))  # model, flags and cover
+    n = 1 << 16
+    a, _ = oracle.trace(yaml_toy, KEY0, n, source=YAML_SRC, samples=n)
+    b, _ = oracle.trace(own, KEY0, n, source=YAML_SRC, samples=n)
+    np.testing.assert_allclose(a.arrival, b.arrival, rtol=RTOL)
+    np.testing.assert_allclose(a.arrival2, b.arrival2, rtol=RTOL)
+    assert np.array_equal(a.counts, b.counts)
+
+
+def test_refused_parts_name_themselves():
+    data = reference.load(os.path.join(GOLD, "refdet_yaml_toy.json"))
+    with pytest.raises(ValueError, match="not exported"):
+        reference.detector(dict(data, format="other"))
