@@ -319,7 +319,7 @@ def run_batched(dev, det, reps=3, with_cpu=True):
     del g
     # the reverse mode over the same photons: one adjoint replay with a cotangent per event and sensor
     cot = np.random.default_rng(10).normal(size=jac.shape[:2])
-    ca = A.controls(grad_tabs=gt)
+    ca = shape.controls(n, gt)  # the tuned shape, synchronous
     eng.adjoint(key, n, cot, source=ds, controls=ca)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()

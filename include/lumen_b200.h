@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 12
+#define LUMEN_B200_ABI_VERSION 13
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -269,8 +269,10 @@ enum { LUMEN_TR_SENSOR = 0, LUMEN_TR_TIME, LUMEN_TR_LAM, LUMEN_TR_SCALE, LUMEN_T
 enum { LUMEN_VARIANT_WAVEFRONT = 3, LUMEN_N_VARIANT = 4 };
 /* launch variants: the persistent photon loop at 0 = 256 threads x 4 blocks / SM (64 registers), 1 = 128 x 8 (64),
    2 = 256 x 3 (85 registers); 3 = the wavefront: rounds of two kernels (the query; the rest of the step and the
-   refill) over a pool of slots in HBM, launched from a host loop that reads a live-slot count back every four rounds
-   (not with LUMEN_F_ASYNC). Every variant gives the same photons the same paths. */
+   refill) over a pool of slots in HBM, then the persistent loop resuming the slots still live (its drain: one thread
+   a slot, then the photons left). A synchronous call reads a live-slot count back every four rounds and drains once
+   fewer than an eighth of the slots are live; a LUMEN_F_ASYNC call runs a fixed number of rounds (wave_rounds) and
+   drains, reading nothing back. Every variant gives the same photons the same paths. */
 typedef struct LumenControls {
   float max_distance;      /* m: a query's reach (<= 0: the scene's reach) */
   float roulette;          /* epsilon > 0 (src/lumen/rules/choices.py:112) */
@@ -283,6 +285,12 @@ typedef struct LumenControls {
   int32_t blocks_per_sm;   /* resident blocks per SM launched (<= 0: as many as fit) */
   int32_t wave_slots_log2; /* the wavefront's slots: 2^k photons in flight, k in 16 .. 23 (else 2^21), from the
                               autotuner: each slot carries n / 2^k photons in turn */
+  int32_t wave_rounds;     /* the wavefront's rounds in a LUMEN_F_ASYNC call, which reads no round back: after them
+                              the persistent loop finishes the live slots and the photons left (<= 0: the scene's
+                              rounds per photon a slot carries, measured by its last synchronous wavefront call, else
+                              3, times the photons a slot carries). A synchronous call reads the live slots back every
+                              fourth round and hands the tail (fewer than an eighth of the slots live) to the
+                              persistent loop; it ignores this field. */
 } LumenControls;
 
 /* --------------------------------------------------------------------------------------------- the tallies */

@@ -87,7 +87,8 @@ class LumenControls(ctypes.Structure):
     _fields_ = [("max_distance", ctypes.c_float), ("roulette", ctypes.c_float), ("max_vertices", ctypes.c_int32),
                 ("n_grad", ctypes.c_int32), ("grad_tab", ctypes.c_int32 * MAX_GRAD),
                 ("step_budget", ctypes.c_int64), ("flags", ctypes.c_int32), ("variant", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("wave_slots_log2", ctypes.c_int32)]  # fmt: skip
+                ("blocks_per_sm", ctypes.c_int32), ("wave_slots_log2", ctypes.c_int32),
+                ("wave_rounds", ctypes.c_int32)]  # fmt: skip
 
 
 class LumenAxis(ctypes.Structure):
@@ -125,10 +126,10 @@ def dptr(a):
 
 
 def controls(max_distance=0.0, roulette=0.01, max_vertices=1 << 22, grad_tabs=(), step_budget=0, flags=0, variant=0,
-             blocks_per_sm=0, wave_slots_log2=0):
+             blocks_per_sm=0, wave_slots_log2=0, wave_rounds=0):
     c = LumenControls()
     c.flags, c.variant, c.blocks_per_sm = int(flags), int(variant), int(blocks_per_sm)
-    c.wave_slots_log2 = int(wave_slots_log2)
+    c.wave_slots_log2, c.wave_rounds = int(wave_slots_log2), int(wave_rounds)
     c.max_distance = float(max_distance)
     c.roulette = float(roulette)
     c.max_vertices = int(max_vertices)

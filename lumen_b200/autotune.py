@@ -9,7 +9,9 @@ Tunables (``LumenControls``):
 - the wavefront's photons per slot (its slots 2^k = n / photons per slot: more slots keep more photons in flight,
   fewer leave less state in HBM and a shorter tail of half-empty rounds).
 Each candidate traces the same photon ids (the same paths: results do not depend on the shape), timed with CUDA events
-after a warm-up; the fastest is cached per (detector, source kind, gradient count, events, asynchronous). The BVH
+after a warm-up; the fastest is cached per (detector, source kind, gradient count, events, asynchronous). An
+asynchronous call reads no round back: the wavefront runs the rounds the scene's last synchronous call of that shape
+needed per photon a slot carries, and the persistent loop finishes what is left (``LumenControls.wave_rounds``). The BVH
 stack depth is the scene's (checked at scene creation against LUMEN_MAX_BVH_DEPTH), not a launch choice.
 """
 
@@ -54,12 +56,12 @@ class Shape(NamedTuple):
 
 
 def candidates(asynchronous=False):
-    """The shapes to time; the wavefront (host-driven rounds) only for synchronous calls."""
+    """The shapes to time: the persistent loop's variants at two resident-block counts, the wavefront at each photons
+    per slot (an asynchronous call runs the scene's estimated rounds, then the persistent loop drains the slots)."""  # noqa: D205, D209
     out = []
     for v in range(A.N_VARIANT):
         if v == A.VARIANT_WAVEFRONT:
-            if not asynchronous:
-                out += [Shape(v, 0, p) for p in PHOTONS_PER_SLOT]
+            out += [Shape(v, 0, p) for p in PHOTONS_PER_SLOT]
             continue
         out += [Shape(v, bps) for bps in (0, 2)]
     return out
@@ -78,6 +80,8 @@ def tune(eng, source, n_sample, grad_tabs=(), n_events=1, key=(0, 0), reps=2, as
     for sh in candidates(asynchronous):
         warm = min(n_sample, 1 << 16)
         eng.trace(key, warm, source=source, controls=sh.controls(warm, grad_tabs, fl), tallies=T)
+        if asynchronous and sh.variant == A.VARIANT_WAVEFRONT:  # the scene's rounds estimate at this shape
+            eng.trace(key, n_sample, source=source, controls=sh.controls(n_sample, grad_tabs, flags), tallies=T)
         c = sh.controls(n_sample, grad_tabs, fl)
         best = float("inf")
         for _ in range(reps):
@@ -90,5 +94,8 @@ def tune(eng, source, n_sample, grad_tabs=(), n_events=1, key=(0, 0), reps=2, as
         times[sh.label()] = best
         shapes[sh.label()] = sh
     pick = shapes[min(times, key=times.get)]
+    if asynchronous and pick.variant == A.VARIANT_WAVEFRONT:  # leave the picked shape's rounds estimate in the scene
+        eng.trace(key, n_sample, source=source, controls=pick.controls(n_sample, grad_tabs, flags), tallies=T)
+        torch.cuda.synchronize(eng.device)
     _cache[sig] = (pick, times)
     return pick, times

@@ -48,6 +48,9 @@ struct LumenScene {
   int groups;                          // frame groups (the instantiation walking them)
   int nav64;                           // LUMEN_PREC_FLOAT64: S's vol_f, node_f, leaf_f, plane_f hold float64 data
   const float* vol_f32;                // the float32 frames (the readout groups' binning reads them in either precision)
+  // the wavefront's rounds per photon a slot carries, from the last synchronous wavefront call (an estimate for the
+  // asynchronous calls' fixed rounds; concurrent calls may overwrite one another's)
+  mutable float wave_rpp = 0.0f;
 };
 
 // the position's precision of an instantiation: NAV64 = 1 the float64 navigator's (LUMEN_PREC_FLOAT64)
@@ -104,6 +107,13 @@ struct Launch {
   int budget_chunk;  // steps a thread of the persistent loop counts before it adds them to steps_used (1 .. 256)
   Tally T;
   float* truth;  // the photons' analog records (truth rows, LUMEN_F_TRUTH: the ANALOG instantiation), else null
+  // the wavefront's slots a persistent launch resumes before it takes new photons (its drain: one thread a slot), or
+  // wv_W = 0
+  const uint32_t* wv_ph;
+  const uint32_t* wv_ex;
+  const float* wv_dw;
+  const int32_t* wv_act;
+  int wv_W;
 };
 
 // what picks a launch's instantiation, host side: the scene has a torus leaf; the run keeps truth rows
@@ -215,6 +225,38 @@ __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
   else d_source_row(L.R.S, L.R.live, L.R.ref, L.src, L.key, L.first_id + i, r);
 }
 
+struct WaveExtra {  // what a slot carries besides the photon: its key, event, row weight and sensor-sum cache
+  Key pkey;
+  int ev, pad;
+  double w0;
+  PhotonTally pt;
+};
+
+struct Wave {
+  uint32_t* ph;     // W x sizeof(Photon) / 4
+  uint32_t* ex;     // W x sizeof(WaveExtra) / 4
+  uint32_t* pre;    // W x sizeof(Pre) / 4
+  uint32_t* q;      // W x sizeof(Query) / 4
+  float* dw;        // W x LUMEN_MAX_GRAD (gradient runs)
+  int32_t* act;     // W: the slot holds a live photon
+  unsigned long long* live;  // slots live after the last k_wave_step (zeroed before each)
+  int W;
+};
+
+template <class T>
+__device__ __forceinline__ void wv_ld(const uint32_t* b, int W, int i, T& v) {
+  static_assert(sizeof(T) % 4 == 0, "word-major records hold whole words");
+  uint32_t* w = reinterpret_cast<uint32_t*>(&v);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(T) / 4); ++k) w[k] = b[(size_t)k * W + i];
+}
+template <class T>
+__device__ __forceinline__ void wv_st(uint32_t* b, int W, int i, const T& v) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(&v);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(T) / 4); ++k) b[(size_t)k * W + i] = w[k];
+}
+
 // The persistent photon loop: a lane refill per step (src/lumen/run.py:81 SCHEDULE = "step").
 // Launch shapes (LumenControls.variant): 0 = 256 threads x 4 blocks per SM (64 registers, 32 warps an SM: the
 // measured best of 128 / 256 threads at 1-8 blocks on the tank: the loop is latency- and divergence-bound, so warps
@@ -244,6 +286,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
   __syncthreads();
   unsigned c_ph = 0, c_steps = 0, c_dep = 0, c_trunc = 0, c_multi = 0, c_lost = 0;
   int budget_chunk = 0;
+  if constexpr (!ANALOG && !NAV64) {
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    if (i < L.wv_W && L.wv_act[i]) {  // a wavefront slot's photon, where its last round left it
+      WaveExtra ex;
+      wv_ld(L.wv_ph, L.wv_W, i, ph);
+      wv_ld(L.wv_ex, L.wv_W, i, ex);
+      pkey = ex.pkey;
+      ev = ex.ev;
+      w0 = ex.w0;
+      pt = ex.pt;
+      if (G > 0)
+        for (int p = 0; p < L.R.P; ++p) dw[p] = L.wv_dw[(size_t)p * L.wv_W + i];
+      active = 1;
+    }
+  }
   for (;;) {
     unsigned need = __ballot_sync(FULL, !active);
     if (need) {
@@ -362,38 +419,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_trace(Launch L) {
 // step, the deposit, the photon's end and the slot's refill from the source. Each kernel is a part of the
 // megakernel's code with its own registers; the state crosses HBM between them, word-major (word k of slot i at
 // buf[k * W + i]) so that every load and store of a warp is one contiguous 128-byte access.
-struct WaveExtra {  // what a slot carries besides the photon: its key, event, row weight and sensor-sum cache
-  Key pkey;
-  int ev, pad;
-  double w0;
-  PhotonTally pt;
-};
-
-struct Wave {
-  uint32_t* ph;     // W x sizeof(Photon) / 4
-  uint32_t* ex;     // W x sizeof(WaveExtra) / 4
-  uint32_t* pre;    // W x sizeof(Pre) / 4
-  uint32_t* q;      // W x sizeof(Query) / 4
-  float* dw;        // W x LUMEN_MAX_GRAD (gradient runs)
-  int32_t* act;     // W: the slot holds a live photon
-  unsigned long long* live;  // slots live after the last k_wave_step (zeroed before each)
-  int W;
-};
-
-template <class T>
-__device__ __forceinline__ void wv_ld(const uint32_t* b, int W, int i, T& v) {
-  static_assert(sizeof(T) % 4 == 0, "word-major records hold whole words");
-  uint32_t* w = reinterpret_cast<uint32_t*>(&v);
-#pragma unroll
-  for (int k = 0; k < (int)(sizeof(T) / 4); ++k) w[k] = b[(size_t)k * W + i];
-}
-template <class T>
-__device__ __forceinline__ void wv_st(uint32_t* b, int W, int i, const T& v) {
-  const uint32_t* w = reinterpret_cast<const uint32_t*>(&v);
-#pragma unroll
-  for (int k = 0; k < (int)(sizeof(T) / 4); ++k) b[(size_t)k * W + i] = w[k];
-}
-
 template <int G, int TORUS>
 __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -602,11 +627,13 @@ inline int grid_for(const void* fn, int block, int* grid) {
   return 0;
 }
 
+// blocks > 0: that grid instead of the resident one (the wavefront's drain: one thread a slot)
 template <int G, int BLOCK, int MINB, int TORUS, int ANALOG = 0, int NAV64 = 0>
-int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
+int launch_shape(const Launch& L, int bps, cudaStream_t stream, int blocks) {
   int grid = 0, st = 0;
-  if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS, ANALOG, NAV64>, BLOCK, &grid))) return st;
-  if (bps > 0) {
+  if (blocks > 0) grid = blocks;
+  else if ((st = grid_for((const void*)k_trace<G, BLOCK, MINB, TORUS, ANALOG, NAV64>, BLOCK, &grid))) return st;
+  if (bps > 0 && blocks <= 0) {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -623,11 +650,17 @@ int launch_shape(const Launch& L, int bps, cudaStream_t stream) {
   return 0;
 }
 
-// The wavefront's rounds (LUMEN_VARIANT_WAVEFRONT): a fill, then query and step kernels until no slot is live. The
-// pool holds up to LUMEN_WAVE_POOL slots (about 350 bytes each with gradients), allocated on the call's stream.
+// The wavefront's rounds (LUMEN_VARIANT_WAVEFRONT): a fill, then query and step kernels, then the drain: the
+// persistent loop resumes every slot still live (one thread a slot) and takes the photons left. A synchronous call
+// reads the live slots back every fourth round and drains once fewer than an eighth of the slots are live (the tail,
+// where a round's launches cost more than its few steps); an asynchronous one (LUMEN_F_ASYNC) runs `rounds` rounds
+// without a readback (<= 0: *rpp rounds per photon a slot carries, the scene's estimate from its last synchronous
+// call) and drains. The pool holds up to LUMEN_WAVE_POOL slots (about 350 bytes each with gradients), allocated on the
+// call's stream.
 #define LUMEN_WAVE_POOL (1 << 21)
 template <int G>
-int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStream_t stream, int slots_log2) {
+int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStream_t stream, int slots_log2,
+             int async, int rounds, float* rpp) {
   const int64_t pool = slots_log2 >= 16 && slots_log2 <= 23 ? (int64_t)1 << slots_log2 : (int64_t)LUMEN_WAVE_POOL;
   int64_t want = L.n < pool ? L.n : pool;
   int W = (int)((want + 255) / 256 * 256);
@@ -650,8 +683,16 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
   k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);  // the fill: every slot takes a photon
   CK(cudaGetLastError());
   ++lumen_launches();
-  int st = 0;
-  for (long long r = 0;; ++r) {
+  const long long per_slot = (L.n + W - 1) / W;  // photons a slot carries in turn
+  long long cap = -1;                             // rounds of an asynchronous call
+  if (async) {
+    const float est = rpp && *rpp > 0.0f ? *rpp : 3.0f;
+    cap = rounds > 0 ? rounds : (long long)ceilf(est * (float)per_slot);
+  }
+  long long r = 0;
+  int drained = 0;
+  for (;; ++r) {
+    if (async && r >= cap) break;
     if (pk.torus) k_wave_query<G, 1><<<grid, 256, 0, stream>>>(L, V);
     else if (pk.single) k_wave_query<G, 2><<<grid, 256, 0, stream>>>(L, V);
     else k_wave_query<G, 0><<<grid, 256, 0, stream>>>(L, V);
@@ -659,15 +700,33 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
     k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaGetLastError());
     lumen_launches() += 2;
-    if ((r & 3) == 3) {
+    if (!async && (r & 3) == 3) {
       unsigned long long h = 0;
       CK(cudaMemcpyAsync(&h, V.live, sizeof(h), cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
       if (h == 0) break;
+      if (h < (unsigned long long)(W / 8)) {
+        drained = 1;
+        ++r;
+        break;
+      }
     }
   }
+  if (async || drained) {  // the persistent loop finishes the live slots and takes the photons left
+    Launch LD = L;
+    LD.wv_ph = V.ph;
+    LD.wv_ex = V.ex;
+    LD.wv_dw = V.dw;
+    LD.wv_act = V.act;
+    LD.wv_W = W;
+    int st = pk.torus ? launch_shape<G, 256, 4, 1>(LD, 0, stream, grid)
+                      : (pk.single ? launch_shape<G, 256, 4, 2>(LD, 0, stream, grid)
+                                   : launch_shape<G, 256, 4, 0>(LD, 0, stream, grid));  // fmt: skip
+    if (st) return st;
+  }
+  if (!async && rpp && per_slot > 0) *rpp = (float)r / (float)per_slot;
   CK(cudaFreeAsync(buf, stream));
-  return st;
+  return 0;
 }
 
 // the per-photon, query and locate kernels' launchers (one thread each)
@@ -713,7 +772,7 @@ int launch_locate(const DScene& S, const NF* pts, int64_t n, int32_t* vol, cudaS
 #define LUMEN_SHAPES_9(X) X(8, 256, 4, 2, 0, 1) X(8, 256, 4, 3, 0, 1) X(8, 256, 4, 1, 0, 1)
 #define LUMEN_SHAPES(X) LUMEN_SHAPES_0(X) LUMEN_SHAPES_1(X) LUMEN_SHAPES_2(X) LUMEN_SHAPES_3(X) LUMEN_SHAPES_4(X) \
   LUMEN_SHAPES_5(X) LUMEN_SHAPES_6(X) LUMEN_SHAPES_7(X) LUMEN_SHAPES_8(X) LUMEN_SHAPES_9(X)
-#define LUMEN_SHAPE_DECL(G, B, M, T, A, N) int launch_shape<G, B, M, T, A, N>(const Launch&, int, cudaStream_t);
+#define LUMEN_SHAPE_DECL(G, B, M, T, A, N) int launch_shape<G, B, M, T, A, N>(const Launch&, int, cudaStream_t, int);
 // part 10: the wavefront's rounds; part 11: the per-photon, query and locate kernels
 #define LUMEN_N_PARTS 12
 

@@ -27,8 +27,12 @@ LUMEN_SHAPES_8(LUMEN_INST_SHAPE)
 #elif LUMEN_PART == 9
 LUMEN_SHAPES_9(LUMEN_INST_SHAPE)
 #elif LUMEN_PART == 10
-template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
-template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
+// the drain's persistent loops are the other parts' instantiations
+#define LUMEN_EXTERN_SHAPE(G, B, M, T, A, N) extern template LUMEN_SHAPE_DECL(G, B, M, T, A, N)
+LUMEN_SHAPES(LUMEN_EXTERN_SHAPE)
+template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int, int, float*);
+template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int, int,
+                                      float*);
 #elif LUMEN_PART == 11
 template int launch_photons<0>(const Launch&, int32_t*, float*, cudaStream_t);
 template int launch_photons<1>(const Launch&, int32_t*, float*, cudaStream_t);

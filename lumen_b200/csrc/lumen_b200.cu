@@ -34,8 +34,9 @@ static void begin_call() {
 // the launchers instantiated in the other parts of the build
 #define LUMEN_EXTERN_SHAPE(G, B, M, T, A, N) extern template LUMEN_SHAPE_DECL(G, B, M, T, A, N)
 LUMEN_SHAPES(LUMEN_EXTERN_SHAPE)
-extern template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
-extern template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int);
+extern template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int, int, float*);
+extern template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int,
+                                             int, float*);
 extern template int launch_photons<0>(const Launch&, int32_t*, float*, cudaStream_t);
 extern template int launch_photons<1>(const Launch&, int32_t*, float*, cudaStream_t);
 extern template int launch_query<float>(const DScene&, const float*, const int32_t*, const int32_t*, float, int64_t,
@@ -360,29 +361,29 @@ template <int G>
 static int launch_trace(const Launch& L, const Pick& pk, int variant, int bps, cudaStream_t stream) {
   if (pk.nav64) {  // the float64 navigator: shape 0, extended (with frame groups or not) or single-leaf geometry
     if constexpr (G == 0)
-      if (L.truth) return pk.groups ? launch_shape<0, 256, 4, 3, 1, 1>(L, bps, stream)
-                                    : launch_shape<0, 256, 4, 1, 1, 1>(L, bps, stream);  // fmt: skip
-    if (pk.single) return launch_shape<G, 256, 4, 2, 0, 1>(L, bps, stream);
-    if (pk.groups) return launch_shape<G, 256, 4, 3, 0, 1>(L, bps, stream);
-    return launch_shape<G, 256, 4, 1, 0, 1>(L, bps, stream);
+      if (L.truth) return pk.groups ? launch_shape<0, 256, 4, 3, 1, 1>(L, bps, stream, 0)
+                                    : launch_shape<0, 256, 4, 1, 1, 1>(L, bps, stream, 0);  // fmt: skip
+    if (pk.single) return launch_shape<G, 256, 4, 2, 0, 1>(L, bps, stream, 0);
+    if (pk.groups) return launch_shape<G, 256, 4, 3, 0, 1>(L, bps, stream, 0);
+    return launch_shape<G, 256, 4, 1, 0, 1>(L, bps, stream, 0);
   }
   if constexpr (G == 0) {
     if (L.truth)  // truth rows: the analog instantiation of shape 0
-      return pk.groups ? launch_shape<0, 256, 4, 3, 1>(L, bps, stream)
-                       : (pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream)
-                                   : launch_shape<0, 256, 4, 0, 1>(L, bps, stream));  // fmt: skip
+      return pk.groups ? launch_shape<0, 256, 4, 3, 1>(L, bps, stream, 0)
+                       : (pk.torus ? launch_shape<0, 256, 4, 1, 1>(L, bps, stream, 0)
+                                   : launch_shape<0, 256, 4, 0, 1>(L, bps, stream, 0));  // fmt: skip
   }
-  if (pk.groups) return launch_shape<G, 256, 4, 3>(L, bps, stream);  // frame groups: shape 0 whatever the variant
-  if (pk.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream);  // tori: shape 0 whatever the variant
+  if (pk.groups) return launch_shape<G, 256, 4, 3>(L, bps, stream, 0);  // frame groups: shape 0 whatever the variant
+  if (pk.torus) return launch_shape<G, 256, 4, 1>(L, bps, stream, 0);  // tori: shape 0 whatever the variant
   if (pk.single) switch (variant) {  // single-leaf solids: the scan of one leaf, no postfix program
-      case 1: return launch_shape<G, 128, 8, 2>(L, bps, stream);
-      case 2: return launch_shape<G, 256, 3, 2>(L, bps, stream);
-      default: return launch_shape<G, 256, 4, 2>(L, bps, stream);
+      case 1: return launch_shape<G, 128, 8, 2>(L, bps, stream, 0);
+      case 2: return launch_shape<G, 256, 3, 2>(L, bps, stream, 0);
+      default: return launch_shape<G, 256, 4, 2>(L, bps, stream, 0);
     }
   switch (variant) {
-    case 1: return launch_shape<G, 128, 8, 0>(L, bps, stream);
-    case 2: return launch_shape<G, 256, 3, 0>(L, bps, stream);
-    default: return launch_shape<G, 256, 4, 0>(L, bps, stream);
+    case 1: return launch_shape<G, 128, 8, 0>(L, bps, stream, 0);
+    case 2: return launch_shape<G, 256, 3, 0>(L, bps, stream, 0);
+    default: return launch_shape<G, 256, 4, 0>(L, bps, stream, 0);
   }
 }
 
@@ -459,9 +460,8 @@ static int check_cells(const Tally& T) {
 }
 
 static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* cot, int n_events_cot, double* grads,
-                     cudaStream_t stream, int variant = 0, int bps = 0, int async = 0, int slots_log2 = 0) {
-  if (variant == LUMEN_VARIANT_WAVEFRONT && async)
-    return set_err(LUMEN_ERR_ARG, "the wavefront variant reads its rounds back on the host: not with LUMEN_F_ASYNC");
+                     cudaStream_t stream, int variant = 0, int bps = 0, int async = 0, int slots_log2 = 0,
+                     int rounds = 0, float* rpp = nullptr) {
   Tally& T = L.T;
   T.E = out ? (out->n_events > 0 ? out->n_events : 1) : (n_events_cot > 0 ? n_events_cot : 1);
   T.S_ = L.R.S.n_sensor > 0 ? L.R.S.n_sensor : 1;
@@ -528,11 +528,12 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
         L2.T.health = dummy;
         L2.T.counts = (unsigned long long*)(dummy + LUMEN_N_HEALTH);
       }
-      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<LUMEN_MAX_GRAD>(L2, pk, scratch + 3, stream, slots_log2)
-                                              : launch_trace<LUMEN_MAX_GRAD>(L2, pk, variant, bps, stream);
+      st = variant == LUMEN_VARIANT_WAVEFRONT
+               ? run_wave<LUMEN_MAX_GRAD>(L2, pk, scratch + 3, stream, slots_log2, async, rounds, rpp)
+               : launch_trace<LUMEN_MAX_GRAD>(L2, pk, variant, bps, stream);
       if (st) return st;
     } else {
-      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, pk, scratch + 3, stream, slots_log2)
+      st = variant == LUMEN_VARIANT_WAVEFRONT ? run_wave<0>(L, pk, scratch + 3, stream, slots_log2, async, rounds, rpp)
                                               : launch_trace<0>(L, pk, variant, bps, stream);
       if (st) return st;
     }
@@ -904,7 +905,7 @@ int32_t lumen_b200_trace(const LumenScene* sc, const LumenRows* rows, const Lume
   int st = fill_launch(sc, rows, source, key0, key1, first_id, n, c, L, pk);
   if (st) return st;
   return run_trace(L, pk, out, nullptr, 0, nullptr, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
-                   c->flags & LUMEN_F_ASYNC, c->wave_slots_log2);
+                   c->flags & LUMEN_F_ASYNC, c->wave_slots_log2, c->wave_rounds, &sc->wave_rpp);
 }
 
 int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const LumenSource* source, uint32_t key0,
@@ -919,7 +920,7 @@ int32_t lumen_b200_adjoint(const LumenScene* sc, const LumenRows* rows, const Lu
   if (st) return st;
   if (pk.analog) return set_err(LUMEN_ERR_ARG, "the adjoint replays no truth rows");
   return run_trace(L, pk, nullptr, cotangent, n_events, grads, (cudaStream_t)stream, c->variant, c->blocks_per_sm,
-                   c->flags & LUMEN_F_ASYNC, c->wave_slots_log2);
+                   c->flags & LUMEN_F_ASYNC, c->wave_slots_log2, c->wave_rounds, &sc->wave_rpp);
 }
 
 int32_t lumen_b200_trace_photons(const LumenScene* sc, const LumenRows* rows, const LumenSource* source,

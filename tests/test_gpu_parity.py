@@ -264,14 +264,34 @@ def test_cathode_reflectivity_derivative_at_zero_matches(toy, built):
         assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
 
 
-def test_wavefront_refuses_asynchronous_calls(tank, built):
+@pytest.mark.parametrize("rounds", [1, 0, 40])
+@pytest.mark.parametrize("grad", [False, True])
+def test_wavefront_asynchronous_rounds_then_drain_match(rounds, grad, tank, built):
+    """LUMEN_F_ASYNC on the wavefront: a fixed number of rounds with no readback (1: the persistent drain does nearly
+    everything; 0: the scene's estimate from the synchronous call before; 40: more rounds than the photons need, the
+    last ones empty), then the persistent loop resumes the live slots and takes the photons left: the tallies are the
+    checker's, as are those of the synchronous call (whose tail the drain takes)."""
+    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam_range=(300.0, 600.0))
+    names = ["media/Water/absorption", "surfaces/BlackSheet/R"] if grad else []
+    gt = [tank.params_index[k] for k in names]
+    n = 1 << 17
     eng = _engine(tank)
-    src = sources.Point(position=(1.0, -0.5, 2.0), n_photons=1.0, lam=400.0)
-    ds = DeviceSource(src, 1024)
-    T = DeviceTallies(tank.n_sensor, 1, 0, 0.0, 1.0, 0)
-    c = A.controls(variant=A.VARIANT_WAVEFRONT, flags=A.F_ASYNC)
-    with pytest.raises(Exception, match="LUMEN_F_ASYNC"):
-        eng.trace(KEY, 1024, source=ds, controls=c, tallies=T)
+    ds = DeviceSource(src, n)
+    O, _ = oracle.trace(tank, KEY, n, source=src, samples=n, controls=A.controls(grad_tabs=gt))
+    for flags in (0, A.F_ASYNC):  # the synchronous call first: it sets the scene's estimate
+        c = A.controls(grad_tabs=gt, variant=A.VARIANT_WAVEFRONT, flags=flags, wave_slots_log2=16,
+                       wave_rounds=rounds)  # fmt: skip
+        T = DeviceTallies(tank.n_sensor, 1, 0, 0.0, 1.0, len(gt))
+        eng.trace(KEY, n, source=ds, controls=c, tallies=T)
+        import torch
+
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL, atol=1e-15)
+        np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-7, atol=1e-6)
+        if grad:
+            np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+        assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
 
 
 @pytest.mark.parametrize("which", ["tank", "lar", "facet_lar"])
@@ -622,10 +642,12 @@ def test_wire_planes_with_frame_groups_bit_exact(built):
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
 
 
-def test_batched_events_in_a_captured_graph_match(tank, built):
+@pytest.mark.parametrize("variant", [0, A.VARIANT_WAVEFRONT])
+def test_batched_events_in_a_captured_graph_match(variant, tank, built):
     """256 uneven track events (the batched workload's shape, its counts log-uniform over 3 .. 300 photons instead of
     1e3 .. 1e6) in one LUMEN_F_ASYNC launch captured in a CUDA graph with its tallies' zeroing, replayed twice: the
-    arrivals and the Jacobian per event are the checker's, on both replays."""
+    arrivals and the Jacobian per event are the checker's, on both replays; in the persistent loop and in the
+    wavefront (its fixed rounds and the drain, no readback)."""
     import torch
 
     rng = np.random.default_rng(11)
@@ -641,7 +663,7 @@ def test_batched_events_in_a_captured_graph_match(tank, built):
     gt = [tank.params_index[k] for k in names]
     eng = _engine(tank)
     ds = DeviceSource(src, n)
-    c = A.controls(grad_tabs=gt, flags=A.F_ASYNC)
+    c = A.controls(grad_tabs=gt, flags=A.F_ASYNC, variant=variant, wave_slots_log2=16)
     T = DeviceTallies(tank.n_sensor, ds.n_events, 0, 0.0, 1.0, len(gt))
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):  # the first call on the side stream, before the capture
