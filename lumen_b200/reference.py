@@ -38,6 +38,7 @@ continues it unchanged, so the two draw other random numbers for the same law (t
 
 from __future__ import annotations
 
+import gzip
 import json
 
 import numpy as np
@@ -83,15 +84,12 @@ def _table(t) -> list:
     return float(np.float32(t))
 
 
-def export(det) -> dict:
-    """Return the products of a loaded reference detector (``lumen.load``) that its photon loop runs on, as plain
-    data (lists, numbers and strings: ``json.dumps`` keeps every float64 exactly); the module docstring says which."""  # noqa: D205, D209
-    from lumen import api
-    from lumen.build import pack
+def export_scene(scene) -> tuple:
+    """Return (solids, volumes) of a reference ``Scene``: per definition with a member its flattened solid, per
+    navigator volume (an instance of such a definition, in the reference's instance order) its PV path, definition,
+    parent volume, world pose and label (the member's (medium, sensor))."""  # noqa: D205, D209
     from lumen.geometry import scene as sc
 
-    parts = det.parts
-    scene, optics = parts.nav_scene, parts.optics
     T = sc.instances(scene)
     solids, volumes, vol_of_inst = {}, [], {}
     for i, dname in enumerate(T.defn):
@@ -109,8 +107,23 @@ def export(det) -> dict:
             p = int(T.parent[p])
         vol_of_inst[i] = len(volumes)
         seg = sc.member_segment(d, dname)
+        lab = d.member.label
         volumes.append({"pv": f"{T.path[i]}/{seg}" if T.path[i] else seg, "path": T.path[i], "definition": dname,
-                        "parent": vol_of_inst[p] if p >= 0 else -1, "R": _f(T.R[i]), "t": _f(T.t[i])})  # fmt: skip
+                        "parent": vol_of_inst[p] if p >= 0 else -1, "R": _f(T.R[i]), "t": _f(T.t[i]),
+                        "label": [int(lab.medium), int(lab.sensor)]})  # fmt: skip
+    return solids, volumes
+
+
+def export(det) -> dict:
+    """Return the products of a loaded reference detector (``lumen.load``) that its photon loop runs on, as plain
+    data (lists, numbers and strings: ``json.dumps`` keeps every float64 exactly); the module docstring says which."""  # noqa: D205, D209
+    from lumen import api
+    from lumen.build import pack
+    from lumen.geometry import scene as sc
+
+    parts = det.parts
+    optics = parts.optics
+    solids, volumes = export_scene(parts.nav_scene)
     if optics.deposit_pre is not None and np.any(optics.deposit_pre):
         raise NotImplementedError("a sensor depositing to the tag before (Optics.deposit_pre) is not converted")
     if optics.born_pair is not None and np.any(np.asarray(optics.born_pair) >= 0):
@@ -180,14 +193,24 @@ def export(det) -> dict:
                         "axis": _f(st.axis)}}  # fmt: skip
 
 
+def _open(path, mode):
+    return gzip.open(path, mode + "t") if str(path).endswith(".gz") else open(path, mode)
+
+
 def save(data: dict, path) -> None:
-    """Write exported data as JSON (every float64 round-trips exactly)."""
-    with open(path, "w") as f:
+    """Write exported data as JSON (every float64 round-trips exactly; gzip-compressed where the name ends in .gz)."""
+    with _open(path, "w") as f:
         json.dump(data, f, separators=(",", ":"))
 
 
+def load_scene(path) -> dict:
+    """Read exported scene data ({"solids", "volumes"}: ``export_scene``) written by ``save``."""
+    with _open(path, "r") as f:
+        return json.load(f)
+
+
 def load(path) -> dict:
-    with open(path) as f:
+    with _open(path, "r") as f:
         data = json.load(f)
     if data.get("format") != FORMAT:
         raise ValueError(f"{path}: not exported reference detector data ({FORMAT})")
@@ -240,26 +263,60 @@ def _add(pool: O.Pool, t, name=None) -> int:
     return pool.add(float(t), name)
 
 
+def placed_volumes(solids: dict, vols: list, material) -> list:
+    """This package's placed volumes (``geometry.Placed``) of exported solids and volumes, in their order; one
+    logical volume per definition, of ``material(volume)``."""  # noqa: D205, D209
+    flat = {k: Flattened(v) for k, v in solids.items()}
+    lvs, placed = {}, []
+    for v in vols:
+        dn = v["definition"]
+        if dn not in lvs:
+            lvs[dn] = G.Volume(dn, flat[dn], material(v))
+        depth = 0 if v["parent"] < 0 else placed[v["parent"]].depth + 1
+        placed.append(G.Placed(v["pv"], lvs[dn], np.asarray(v["R"], float), np.asarray(v["t"], float),
+                               int(v["parent"]), depth))  # fmt: skip
+    return placed
+
+
+def scene_detector(solids: dict, vols: list) -> D.Detector:
+    """The navigator of an exported scene alone (``export_scene``), for navigation checks: a class per volume
+    label (medium, sensor) and the outside, every class's medium transparent (index 1), every crossing the absorber.
+    ``Detector.names`` are the PV paths; ``arrays["vol_i"]`` holds each volume's class and sensor."""  # noqa: D205, D209
+    labels = sorted({tuple(v["label"]) for v in vols})
+    cls_of = {lab: c for c, lab in enumerate(labels)}
+    placed = placed_volumes(solids, vols, lambda v: f"m{v['label'][0]}")
+    vol_cls = [cls_of[tuple(v["label"])] for v in vols]
+    out_cls = len(labels)
+    vol_sensor = np.asarray([v["label"][1] if v["label"][1] >= 0 else -1 for v in vols], np.int32)
+    nav = G.navigator_arrays(placed, vol_cls, out_cls, vol_sensor)
+    pool = O.Pool()
+    med_i = np.full((1, 16), -1, np.int32)
+    med_i[0, 0] = pool.add(1.0)
+    row = O.surface_row(O.ABSORBER, False, True)
+    row_i = np.zeros((1, 16), np.int32)
+    row_i[0, 0:6] = [row.model, row.normal, row.glisur, row.far_opaque, row.per_normal, 0]
+    for c, col in enumerate(O.COLUMNS):
+        row_i[0, 6 + c] = pool.add(float(O.table(row.cols[col])[1][0]) if col in row.cols else O.NEUTRAL[col])
+    n_cls = out_cls + 1
+    row_of = np.zeros((n_cls, n_cls), np.int32)
+    np.fill_diagonal(row_of, -1)
+    n_sensor = int(vol_sensor.max()) + 1 if len(vol_sensor) and vol_sensor.max() >= 0 else 0
+    st = D.SensorTable([f"s{i}" for i in range(n_sensor)], ["s"] * n_sensor, np.zeros((n_sensor, 3)),
+                       np.tile([0.0, 0.0, 1.0], (n_sensor, 1)))  # fmt: skip
+    return D.assemble(nav, vol_cls, n_cls, np.zeros(n_cls, np.int32), row_of, med_i, row_i, pool, st,
+                      [v["pv"] for v in vols], {c: str(lab) for lab, c in cls_of.items()}, {})  # fmt: skip
+
+
 def detector(data: dict, precision: str | None = None) -> D.Detector:
     """Return this package's Detector of exported reference data (``export``, ``load``); ``precision``: the
     navigator's (default: the reference detector's)."""  # noqa: D205, D209
     if data.get("format") != FORMAT:
         raise ValueError(f"not exported reference detector data ({FORMAT})")
-    solids = {k: Flattened(v) for k, v in data["solids"].items()}
     vols = data["volumes"]
     med_names = [m["name"] for m in data["media"]]
     medium_of = np.asarray(data["medium_of"], np.int32)
     class_of = data["class_of"]
-    lvs = {}
-    placed = []
-    for v in vols:
-        dn = v["definition"]
-        if dn not in lvs:
-            cls = class_of[v["pv"]]
-            lvs[dn] = G.Volume(dn, solids[dn], med_names[medium_of[cls]])
-        depth = 0 if v["parent"] < 0 else placed[v["parent"]].depth + 1
-        placed.append(G.Placed(v["pv"], lvs[dn], np.asarray(v["R"], float), np.asarray(v["t"], float),
-                               int(v["parent"]), depth))  # fmt: skip
+    placed = placed_volumes(data["solids"], vols, lambda v: med_names[medium_of[class_of[v["pv"]]]])
     vol_cls = [int(class_of[v["pv"]]) for v in vols]
     out_cls = int(class_of[OUTSIDE_PV])
     sensor_index = data["sensor_index"]

@@ -12,7 +12,9 @@ the medium an index into the fixture's material names (the outside: -1), the sen
 sensor placement is a definition of its own in the Scene, so that the referee reports that index).
 
 The reference's modules are imported under the numpy-backed ``jax`` stub of ``make_golden.py``; the referee is host
-numpy in float64 and needs nothing else of JAX.
+numpy in float64 and needs nothing else of JAX. Beside each fixture, ``refscene_<detector>.json.gz`` holds the same Scene
+as the reference flattens it (``lumen_b200.reference.export_scene``): the navigator rebuilt from the reference's own
+leaves is checked against the referee too.
 """
 
 from __future__ import annotations
@@ -184,6 +186,10 @@ def dump(name, make, seed):
                         after_sen=asen, before_med=bmed, ambiguous=amb, materials=np.asarray(mats),
                         place_names=np.asarray([p[0] for p in placements]),
                         place_mats=np.asarray([p[1] for p in placements]))  # fmt: skip
+    from lumen_b200 import reference
+
+    solids, volumes = reference.export_scene(scene)  # the same Scene, flattened by the reference for lumen_b200.reference
+    reference.save({"solids": solids, "volumes": volumes}, os.path.join(HERE, f"refscene_{name}.json.gz"))
     print(f"{name}: {len(scene.definitions)} definitions, {int(hit.sum())}/{N_RAYS} rays hit, "
           f"{int((sen >= 0).sum())} points in sensors")
 

@@ -70,3 +70,36 @@ def test_fixtures_exercise_the_detectors():
         assert g["hit"].sum() > 600
         assert len(np.unique(g["med"])) >= 2
     assert (load("cylinder_tank")["after_sen"] >= 0).sum() > 20  # rays ending on PMTs
+
+
+@pytest.mark.parametrize("name", list(MAKERS))
+def test_navigator_of_the_reference_leaves_matches_the_referee(name):
+    """The same Scene as the reference flattens it (tests/golden/refscene_<detector>.json.gz: its ``solids.Compiled``
+    leaves, one origin a solid, shared planes; its instance poses), rebuilt by ``lumen_b200.reference`` into this
+    package's navigator arrays: the checker's labels and first changes against the referee's, at the same thresholds.
+    This pins the converter's reading of every solid of the catalogue the three detectors hold (boxes, tubes, spheres,
+    cones, tori, polycones, polyhedra, the convex polytopes and the booleans with placed operands)."""
+    from lumen_b200 import reference
+
+    x = reference.load_scene(os.path.join(GOLD, f"refscene_{name}.json.gz"))
+    det = reference.scene_detector(x["solids"], x["volumes"])
+    g = load(name)
+    lab = np.asarray([v["label"] for v in x["volumes"]] + [[-1, -1]], np.int64)
+
+    def labels(vol):
+        v = np.asarray(vol, np.int64)
+        return lab[v, 0], lab[v, 1]
+
+    med, sen = labels(oracle.locate(det, g["X"]))
+    bad_pts = int(np.sum((med != g["med"]) | (sen != g["sen"])))
+    vol0 = oracle.locate(det, g["O"])
+    oi, of = oracle.query(det, g["O"], g["D"], vol0, None, float(g["tmax"]))
+    hit = oi[:, 0].astype(bool)
+    t = of[:, 0].astype(np.float64)
+    amed, asen = labels(oi[:, 2])
+    ok = hit == g["hit"]
+    both = ok & hit
+    ok[both] &= np.abs(t[both] - g["t"][both]) <= 2e-5 * (1.0 + np.abs(g["t"][both]))
+    ok[both] &= (amed[both] == g["after_med"][both]) & (asen[both] == g["after_sen"][both])
+    assert bad_pts <= 2, (name, bad_pts)
+    assert int(np.sum(~ok)) <= 0.002 * len(ok), (name, int(np.sum(~ok)))
