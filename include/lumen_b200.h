@@ -93,11 +93,13 @@ enum { LUMEN_RI_MODEL = 0, LUMEN_RI_NORMAL = 1, LUMEN_RI_GLISUR = 2, LUMEN_RI_FA
    length and its lobe constants g_forward, g_backward, forward_ratio (MIEHG, MIEHG_FORWARD, MIEHG_BACKWARD,
    MIEHG_FORWARD_RATIO); the WLS (G4OpWLS) absorption length, mean photons, time constant (ns) and emission spectrum
    (WLSABSLENGTH, WLSMEANNUMBERPHOTONS, WLSTIMECONSTANT, WLSCOMPONENT: energies as the knots, intensities as the
-   values); then the WLS time profile as a plain int (0: delta, Geant4's default; 1: exponential). A channel whose
-   length table is -1 is absent. */
+   values); then the WLS time profile as a plain int (0: delta, Geant4's default; 1: exponential); then a plain int,
+   1 where the Mie lobe choice is a defensive part (its forward ratio a keyed parameter, src/lumen/api.py:797
+   _edge_rows: drawn at the ratio's cover, src/lumen/media/phase.py:173 _mie_cover, weighted live / covered,
+   src/lumen/transport/medium.py:96 channel_draw), else not. A channel whose length table is -1 is absent. */
 enum { LUMEN_MI_INDEX = 0, LUMEN_MI_ABS = 1, LUMEN_MI_RAY = 2, LUMEN_MI_MIE = 3, LUMEN_MI_MIE_GF = 4,
        LUMEN_MI_MIE_GB = 5, LUMEN_MI_MIE_R = 6, LUMEN_MI_WLS = 7, LUMEN_MI_WLS_YIELD = 8, LUMEN_MI_WLS_TAU = 9,
-       LUMEN_MI_WLS_SPEC = 10, LUMEN_MI_WLS_PROFILE = 11, LUMEN_MED_I = 16 };
+       LUMEN_MI_WLS_SPEC = 10, LUMEN_MI_WLS_PROFILE = 11, LUMEN_MI_MIE_COVER = 12, LUMEN_MED_I = 16 };
 enum { LUMEN_N_CHANNEL = 3 };  /* bulk channels: Rayleigh, Mie, WLS */
 /* Table t: tab[2t] = offset into a pool, tab[2t+1] = knots k >= 1; pool[off .. off+k) energies (eV, ascending),
    pool[off+k .. off+2k) values; linear in photon energy between knots, held beyond (G4PhysicsVector::Value) */

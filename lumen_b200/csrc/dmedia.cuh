@@ -215,10 +215,17 @@ L_DEV void d_bulk_other(const DScene& S, const float* __restrict__ live, const f
       pl[k] = d_tab(S, live, tg[k], E);
       pr[k] = shared ? pl[k] : d_tab(S, ref, tg[k], E);
     }
+    // a covered lobe choice (LUMEN_MI_MIE_COVER): at a forward ratio of 0 or 1 the lobe never drawn gets the
+    // defensive share, the pair (r, 1 - r) renormalised (phase.py:173 _mie_cover, estimator.py:101 defensive_q)
+    const float r0 = pr[2];
+    if (__ldg(m + LUMEN_MI_MIE_COVER) == 1 && !(r0 > 0.0f && 1.0f - r0 > 0.0f)) {
+      float q0 = r0 > 0.0f ? r0 : D_EDGE_SHARE, q1 = 1.0f - r0 > 0.0f ? 1.0f - r0 : D_EDGE_SHARE;
+      pr[2] = q0 / (q0 + q1);
+    }
     d_mie_sample(pr[0], pr[1], pr[2], wi, r3, r4, uniform(vkey, 5), b.d);
     float dl[3];
     float lp = d_mie_logpdf(pl[0], pl[1], pl[2], wi, b.d, dl);
-    if (!shared) b.rlw = l_exp(lp - d_mie_logpdf(pr[0], pr[1], pr[2], wi, b.d, nullptr));
+    if (!shared || pr[2] != r0) b.rlw = l_exp(lp - d_mie_logpdf(pr[0], pr[1], pr[2], wi, b.d, nullptr));
     for (int p = 0; p < P; ++p)
       for (int k = 0; k < 3; ++k)
         if (tg[k] == gt[p]) b.dlob[p] = b.dlob[p] + dl[k];

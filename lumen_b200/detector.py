@@ -267,6 +267,7 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             med_i[m, 4] = pool.add(float(mat.mie_forward), f"media/{name}/mie_g_forward")
             med_i[m, 5] = pool.add(float(mat.mie_backward), f"media/{name}/mie_g_backward")
             med_i[m, 6] = pool.add(float(mat.mie_forward_ratio), f"media/{name}/mie_forward_ratio")
+            med_i[m, 12] = 1  # the ratio is a parameter: the lobe choice is a defensive part (api.py:797 _edge_rows)
         if mat.wls is not None and mat.rindex is not None:  # G4OpWLS: the absorption length and the emission
             med_i[m, 7] = pool.add(mat.wls, f"media/{name}/wls")
             med_i[m, 8] = pool.add(float(mat.wls_mean), f"media/{name}/wls_yield")

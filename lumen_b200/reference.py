@@ -29,8 +29,9 @@ ABI's tables from that data: the reference's classes, media, rows and values, on
 values are the reference's bits; the navigator's arrays are this package's layout of them.
 
 Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: meshes, split
-unions (``Definition.piece_of``), a medium channel other than Rayleigh, a vertex on the class table's diagonal (a skin
-between touching volumes of one class), a deposit to the tag before (``Optics.deposit_pre``) and born sensors
+unions (``Definition.piece_of``), a medium channel other than Rayleigh, Mie (G4OpMieHG) and a WLS (G4OpWLS) with its
+own spectrum and a delta or exponential profile, a vertex on the class table's diagonal (a skin between touching
+volumes of one class), a deposit to the tag before (``Optics.deposit_pre``) and born sensors
 (``Optics.born_pair``). A pass row (``types.PASS``: two classes of one medium split by a role elsewhere) becomes a
 row that carries the photon straight on: the reference steps over such a crossing, this navigator stops at it and
 continues it unchanged, so the two draw other random numbers for the same law (the same expected values).
@@ -53,6 +54,9 @@ MODELS = {"g4.reflect": O.MODEL_REFLECT, "g4.dielectric": O.MODEL_DIELECTRIC, "g
 GLISUR_LOBES = {"glisur": 1, "glisur_dielectric": 2}  # GLISUR_METAL, GLISUR_DIELECTRIC (src/lumen/surfaces/types.py)
 OPS = {"union": 1, "inter": 2, "sub": 3}  # the postfix program's opcodes (include/lumen_b200.h)
 DIRECT = ("value", "constant", "setting", "default")  # key_rows columns read from a key as they are (build/pack.py)
+# the medium record's table slots in order (include/lumen_b200.h LUMEN_MI_*; this package's names of the tables)
+MEDIUM_PARTS = ("index", "absorption", "rayleigh", "mie", "mie_g_forward", "mie_g_backward", "mie_forward_ratio", "wls",
+                "wls_yield", "wls_tau", "wls_spectrum")
 
 
 # ------------------------------------------------------------------------------------------------------ export
@@ -134,7 +138,8 @@ def export(det) -> dict:
         if src.key is not None and src.column in DIRECT:
             keys["/".join(str(x) for x in path)] = src.key
     tab = optics.table
-    edge = set(api._edge_rows(det).surfaces)
+    edge_rows = api._edge_rows(det)
+    edge, lobes = set(edge_rows.surfaces), set(edge_rows.lobes)
     rows = []
     for r, row in enumerate(optics.rows):
         model = tab.models[int(tab.flags.model[r])].name
@@ -172,12 +177,30 @@ def export(det) -> dict:
                 if key is not None:
                     entry["keys"][part] = key
         for ch in m.channels:
-            if ch.name != "rayleigh" or ch.emission is not None:
-                raise NotImplementedError(f"medium {name}: channel {ch.name!r} is not converted (Rayleigh only)")
-            entry["tables"]["rayleigh"] = _table(pm["rayleigh"]["length"])
-            key = keys.get(f"media/{name}/rayleigh/length/value")
-            if key is not None:
-                entry["keys"]["rayleigh"] = key
+            pc = pm[ch.name]
+            if ch.name == "rayleigh" and ch.emission is None:
+                parts_of = {"rayleigh": ("length",)}
+            elif ch.name == "mie" and ch.emission is None:
+                parts_of = {"mie": ("length",), "mie_g_forward": ("lobe", "g_forward"),
+                            "mie_g_backward": ("lobe", "g_backward"), "mie_forward_ratio": ("lobe", "forward_ratio")}  # fmt: skip
+                entry["mie_cover"] = (name, "mie", "forward_ratio") in lobes
+            elif ch.name == "wls" and ch.emission is not None and ch.emission.spectrum is None:
+                parts_of = {"wls": ("length",), "wls_yield": ("yield",), "wls_tau": ("tau",),
+                            "wls_spectrum": ("spectrum",)}  # fmt: skip
+                comps = tuple(ch.emission.profile.components)
+                if comps not in (("delta",), ("decay",)):
+                    raise NotImplementedError(f"medium {name}: WLS time profile {comps} is not converted")
+                entry["wls_profile"] = int(comps == ("decay",))
+            else:
+                raise NotImplementedError(f"medium {name}: channel {ch.name!r} is not converted")
+            for part, path in parts_of.items():
+                leaf = pc
+                for k in path:
+                    leaf = leaf[k]
+                entry["tables"][part] = _table(leaf)
+                key = keys.get("/".join(("media", name, ch.name, *path)) + ("/value" if isinstance(leaf, dict) else ""))
+                if key is not None:
+                    entry["keys"][part] = key
         media.append(entry)
     row_of = np.asarray(optics.row_of, np.int64)
     if np.any(np.diag(row_of) >= 0):
@@ -340,9 +363,13 @@ def detector(data: dict, precision: str | None = None) -> D.Detector:
 
     med_i = np.full((len(data["media"]), 16), -1, np.int32)
     for m, med in enumerate(data["media"]):
-        for slot, part in ((0, "index"), (1, "absorption"), (2, "rayleigh")):
+        for slot, part in enumerate(MEDIUM_PARTS):
             if part in med["tables"]:
                 med_i[m, slot] = keyed(med["tables"][part], med["keys"].get(part), f"media/{med['name']}/{part}")
+        if "wls" in med["tables"]:
+            med_i[m, 11] = int(med["wls_profile"])
+        if "mie" in med["tables"]:
+            med_i[m, 12] = int(bool(med["mie_cover"]))
     rows = data["rows"]
     row_i = np.zeros((len(rows), 16), np.int32)
     for r, row in enumerate(rows):

@@ -315,10 +315,17 @@ static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
         pl[k] = o_tab(D, R->live, tg[k], Eph, 0);
         pr[k] = R->shared ? pl[k] : o_tab(D, R->ref, tg[k], Eph, 0);
       }
+      /* a covered lobe choice (medium.py:96 channel_draw): drawn at the forward ratio's defensive cover
+         (phase.py:173 _mie_cover: estimator.py:101 defensive_q over (r, 1 - r), both covered), weighted live / cover */
+      const float r0 = pr[2];
+      if (mrec[LUMEN_MI_MIE_COVER] == 1 && !(r0 > 0.0f && 1.0f - r0 > 0.0f)) {
+        float q0 = r0 > 0.0f ? r0 : O_EDGE_SHARE, q1 = 1.0f - r0 > 0.0f ? 1.0f - r0 : O_EDGE_SHARE;
+        pr[2] = q0 / (q0 + q1);
+      }
       o_mie_sample(pr[0], pr[1], pr[2], ph->d, rl3, nx_d);
       float dl[3];
       float lp = o_mie_logpdf(pl[0], pl[1], pl[2], ph->d, nx_d, dl);
-      if (!R->shared) rlw = o_exp(lp - o_mie_logpdf(pr[0], pr[1], pr[2], ph->d, nx_d, 0));
+      if (!R->shared || pr[2] != r0) rlw = o_exp(lp - o_mie_logpdf(pr[0], pr[1], pr[2], ph->d, nx_d, 0));
       for (int p = 0; p < P; ++p)
         for (int k = 0; k < 3; ++k)
           if (tg[k] == R->gt[p]) dlob[p] = dlob[p] + dl[k];

@@ -5,7 +5,9 @@
 The reference converts and loads its two shipped example detectors under the numpy-backed ``jax`` stub
 (``refstub.py``): the tutorial's toy tank (examples/data/example_tank.gdml with the recipe of
 examples/example_tank.py: detector volume TankLV, the PMT placements counted across CathodeSurface) and the YAML toy
-(examples/data/yaml_toy). ``lumen_b200.reference.export`` then writes what the reference's photon loop runs on: the
+(examples/data/yaml_toy), and the scintillator cube of ``tests/golden/yaml_scint`` (this repository's YAML, in the
+reference's format: Rayleigh, Mie and a WLS with an exponential profile in one medium, a ground unified wall).
+``lumen_b200.reference.export`` then writes what the reference's photon loop runs on: the
 navigator scene's instances and flattened solids, the compiled optics, the packed parameters, the defensive rows.
 The tests rebuild the detectors from these files with ``lumen_b200.reference.detector``.
 """
@@ -42,7 +44,8 @@ def main(ref_root):
         os.chdir(ref_root)  # the YAML toy names its sensor values relative to the reference's root
         made = {"example_tank": api.convert(os.path.join(data, "example_tank.gdml"), os.path.join(tmp, "t.lumen"),
                                             recipe=recipe),
-                "yaml_toy": api.convert(os.path.join(data, "yaml_toy"), os.path.join(tmp, "y.lumen"))}  # fmt: skip
+                "yaml_toy": api.convert(os.path.join(data, "yaml_toy"), os.path.join(tmp, "y.lumen")),
+                "yaml_scint": api.convert(os.path.join(HERE, "yaml_scint"), os.path.join(tmp, "s.lumen"))}  # fmt: skip
         for name, path in made.items():
             x = reference.export(api.load(path))
             reference.save(x, os.path.join(HERE, f"refdet_{name}.json"))

@@ -730,16 +730,18 @@ def ref_dets():
 
     gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
     return {n: reference.detector(reference.load(os.path.join(gold, f"refdet_{n}.json")))
-            for n in ("example_tank", "yaml_toy")}  # fmt: skip
+            for n in ("example_tank", "yaml_toy", "yaml_scint")}  # fmt: skip
 
 
-@pytest.mark.parametrize(("name", "pos", "n_photons"), [("example_tank", (0.0, 0.0, 0.1), 2e5),
-                                                        ("yaml_toy", (0.1, 0.0, 0.2), 1e5)])  # fmt: skip
-def test_reference_pipeline_detectors_match(name, pos, n_photons, ref_dets, built):
+@pytest.mark.parametrize(("name", "pos", "n_photons", "lam"), [("example_tank", (0.0, 0.0, 0.1), 2e5, 400.0),
+                                                               ("yaml_toy", (0.1, 0.0, 0.2), 1e5, 400.0),
+                                                               ("yaml_scint", (0.0, 0.0, 0.1), 1e4, 380.0)])  # fmt: skip
+def test_reference_pipeline_detectors_match(name, pos, n_photons, lam, ref_dets, built):
     """The detectors the reference's own pipeline compiled: per-photon records bit-exact, then the tallies, the
-    published runs' workloads (the toy tank's arrivals are the published table: tests/test_reference_detector.py)."""  # noqa: D205, D209
+    published runs' workloads (the toy tank's arrivals are the published table: tests/test_reference_detector.py)
+    and the scintillator (Rayleigh, Mie, WLS)."""  # noqa: D205, D209
     det = ref_dets[name]
-    src = sources.Point(position=pos, n_photons=n_photons, lam=400.0)
+    src = sources.Point(position=pos, n_photons=n_photons, lam=lam)
     bad, gi, oi, gf, of = _records_match(det, src, 1 << 15, samples=1 << 18)
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
     for variant in (0, A.VARIANT_WAVEFRONT):
@@ -748,3 +750,17 @@ def test_reference_pipeline_detectors_match(name, pos, n_photons, ref_dets, buil
         np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
         np.testing.assert_allclose(T.arrival_t.cpu().numpy(), O.arrival_t, rtol=RTOL)
         assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+
+
+def test_covered_mie_lobe_choice_matches(built):
+    """A reference run at a Mie forward ratio of 1 for live values at 0.9: the lobe choice drawn at its defensive
+    cover (LUMEN_MI_MIE_COVER), weighted live / covered; tallies and health are the checker's."""
+    det = detectors.scintillator_cube(mie=0.5)
+    key = "media/LAB/mie_forward_ratio"
+    src = sources.Point(position=(0.0, 0.0, 0.1), n_photons=1e4, lam=450.0)
+    pools = (det.pool_with({key: 0.9}), det.pool_with({key: 1.0}))
+    for variant in (0, A.VARIANT_WAVEFRONT):
+        T, O = _tallies(det, src, 1 << 16, controls=A.controls(variant=variant), pools=pools)
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL)
+        np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
+        np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
