@@ -288,6 +288,9 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     # surface rows per crossed class pair
     neutral = {c: pool.add(v) for c, v in O.NEUTRAL.items()}
     rows, row_key, row_of = [], {}, np.full((n_cls, n_cls), -1, np.int32)
+    # (mother class, daughter class) of every placement: a volume's and a mesh's (whose mother is a volume)
+    daughter_of = {(vol_cls[p.parent], vol_cls[i]) for i, p in enumerate(placed) if p.parent >= 0}
+    daughter_of |= {(vol_cls[new_of[flat[j].parent]], vol_cls[n + k]) for k, j in enumerate(mesh_idx)}
     border_of = {}
     for a, b, s in borders:
         border_of[(vol_cls[by_name[a]], vol_cls[by_name[b]])] = s
@@ -299,10 +302,12 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             from_out = ca == out_cls
             far_opq = into_out or opaque[cls_mat[cb]]
             surf = border_of.get((ca, cb))
-            if surf is None and not from_out and cls_lv[ca].name in skins:
-                surf = skins[cls_lv[ca].name]
-            if surf is None and not into_out and cls_lv[cb].name in skins:
-                surf = skins[cls_lv[cb].name]
+            # the skins: the entered daughter's first, then its mother's; otherwise the volume left's first
+            # (G4OpBoundaryProcess's enteredDaughter; src/lumen/rules/boundary.py:61-66)
+            sides = [(cb, into_out), (ca, from_out)] if (ca, cb) in daughter_of else [(ca, from_out), (cb, into_out)]
+            for c, out in sides:
+                if surf is None and not out and cls_lv[c].name in skins:
+                    surf = skins[cls_lv[c].name]
             is_sensor = (not into_out) and cls_lv[cb].name in sensor_lv
             per_normal = int(is_sensor and sensor_lv[cls_lv[cb].name] in set(after_tracking))
             if surf is not None and far_opq and O.kills_far_side(surf):  # NoRINDEX before the draw: the absorber

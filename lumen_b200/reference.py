@@ -11,7 +11,8 @@ photon loop is built from, and re-derives none of them:
   of a definition with a member is a navigator volume (its world pose composed by the reference's walk, its parent
   the nearest such ancestor), each member's solid as the reference flattens it (``solids.Compiled``,
   src/lumen/geometry/solids.py:200: the transforms baked into the leaves, one origin for the solid's quadric leaves,
-  coplanar planes made identical) with its box (``solids.node_bbox``);
+  coplanar planes made identical) with its box (``solids.node_bbox``); a tessellated member (``scene.Mesh``) as its
+  world triangles and mother, the navigator's opaque pseudo-volume;
 - the compiled optics (``lookup.Optics``, src/lumen/build/lookup.py:394): the class of every placed volume by its PV
   path, the medium of every class, the surface row of every crossed class pair (``row_of``), each row's Interaction,
   flags and outcome support (``lookup.SurfaceTable``, lookup.py:360), the sensor tags;
@@ -28,7 +29,7 @@ photon loop is built from, and re-derives none of them:
 ABI's tables from that data: the reference's classes, media, rows and values, one table per key. The leaves and
 values are the reference's bits; the navigator's arrays are this package's layout of them.
 
-Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: meshes, split
+Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: split
 unions (``Definition.piece_of``), a medium channel other than Rayleigh, Mie (G4OpMieHG) and a WLS (G4OpWLS) with its
 own spectrum and a delta or exponential profile, a vertex on the class table's diagonal (a skin between touching
 volumes of one class), a deposit to the tag before (``Optics.deposit_pre``) and born sensors
@@ -88,10 +89,12 @@ def _table(t) -> list:
     return float(np.float32(t))
 
 
-def export_scene(scene) -> tuple:
+def export_scene(scene, meshes=None) -> tuple:
     """Return (solids, volumes) of a reference ``Scene``: per definition with a member its flattened solid, per
     navigator volume (an instance of such a definition, in the reference's instance order) its PV path, definition,
-    parent volume, world pose and label (the member's (medium, sensor))."""  # noqa: D205, D209
+    parent volume, world pose and label (the member's (medium, sensor)). A tessellated member (``scene.Mesh``, an
+    opaque part the navigator meets as a pseudo-volume) goes to ``meshes`` (a list: its PV path, world triangles in
+    the reference's instance order, mother volume, world pose, label); without the list a mesh is refused."""  # noqa: D205, D209
     from lumen.geometry import scene as sc
 
     T = sc.instances(scene)
@@ -101,7 +104,17 @@ def export_scene(scene) -> tuple:
         if d.member is None:
             continue
         if isinstance(d.member.solid, sc.Mesh):
-            raise NotImplementedError(f"{dname}: a mesh (tessellated solid) is not converted")
+            if meshes is None:
+                raise NotImplementedError(f"{dname}: a mesh (tessellated solid) is not converted here")
+            p = int(T.parent[i])
+            while p >= 0 and p not in vol_of_inst:
+                p = int(T.parent[p])
+            seg = sc.member_segment(d, dname)
+            tris = np.einsum("ij,nkj->nki", T.R[i], np.asarray(d.member.solid.tris, float)) + T.t[i]
+            meshes.append({"pv": f"{T.path[i]}/{seg}" if T.path[i] else seg, "tris": _f(tris),
+                           "mother": vol_of_inst[p] if p >= 0 else -1, "R": _f(T.R[i]), "t": _f(T.t[i]),
+                           "label": [int(d.member.label.medium), int(d.member.label.sensor)]})  # fmt: skip
+            continue
         if d.piece_of:
             raise NotImplementedError(f"{dname}: a piece of a split union is not converted")
         if dname not in solids:
@@ -127,7 +140,8 @@ def export(det) -> dict:
 
     parts = det.parts
     optics = parts.optics
-    solids, volumes = export_scene(parts.nav_scene)
+    meshes = []
+    solids, volumes = export_scene(parts.nav_scene, meshes)
     if optics.deposit_pre is not None and np.any(optics.deposit_pre):
         raise NotImplementedError("a sensor depositing to the tag before (Optics.deposit_pre) is not converted")
     if optics.born_pair is not None and np.any(np.asarray(optics.born_pair) >= 0):
@@ -208,6 +222,7 @@ def export(det) -> dict:
                                   "converted")  # fmt: skip
     st = det.sensor_table()
     return {"format": FORMAT, "name": det.name, "precision": det.precision, "solids": solids, "volumes": volumes,
+            "meshes": meshes,
             "n_classes": int(optics.n_classes), "class_names": list(optics.class_names),
             "class_of": {k: int(v) for k, v in optics.class_of.items()},
             "medium_of": [int(x) for x in optics.medium_of], "media": media, "row_of": row_of.tolist(), "rows": rows,
@@ -344,7 +359,9 @@ def detector(data: dict, precision: str | None = None) -> D.Detector:
     out_cls = int(class_of[OUTSIDE_PV])
     sensor_index = data["sensor_index"]
     vol_sensor = np.asarray([sensor_index.get(v["pv"], -1) for v in vols], np.int32)
-    nav = G.navigator_arrays(placed, vol_cls, out_cls, vol_sensor)
+    meshes = [(np.asarray(m["tris"], float).reshape(-1, 3, 3), int(m["mother"])) for m in data.get("meshes", ())]
+    mesh_cls = [int(class_of[m["pv"]]) for m in data.get("meshes", ())]
+    nav = G.navigator_arrays(placed, vol_cls, out_cls, vol_sensor, meshes=meshes, mesh_cls=mesh_cls)
     pool = O.Pool()
     by_key = {}  # key -> table: one table per key, shared by every row reading it
 

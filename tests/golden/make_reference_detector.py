@@ -6,7 +6,8 @@ The reference converts and loads its two shipped example detectors under the num
 (``refstub.py``): the tutorial's toy tank (examples/data/example_tank.gdml with the recipe of
 examples/example_tank.py: detector volume TankLV, the PMT placements counted across CathodeSurface) and the YAML toy
 (examples/data/yaml_toy), and the scintillator cube of ``tests/golden/yaml_scint`` (this repository's YAML, in the
-reference's format: Rayleigh, Mie and a WLS with an exponential profile in one medium, a ground unified wall).
+reference's format: Rayleigh, Mie and a WLS with an exponential profile in one medium, a ground unified wall), and
+``detectors.mesh_tank`` written out in the same format by ``mesh_tank_yaml`` (tessellated parts, an orb, skins).
 ``lumen_b200.reference.export`` then writes what the reference's photon loop runs on: the
 navigator scene's instances and flattened solids, the compiled optics, the packed parameters, the defensive rows.
 The tests rebuild the detectors from these files with ``lumen_b200.reference.detector``.
@@ -23,6 +24,72 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
+
+
+def _num(x):
+    return repr(float(x))
+
+
+def mesh_tank_yaml(where):
+    """Write ``lumen_b200.detectors.mesh_tank`` (a water box holding a tessellated steel icosphere, a tessellated
+    black box, a glass orb and eight sensor discs) in the reference's YAML detector format into the directory
+    ``where``: its triangles and rotation matrices written out from this package's own geometry helpers."""  # noqa: D205, D209
+    from lumen_b200 import geometry as G
+
+    ball, block = G.icosphere(0.4, 2), G.box_mesh(0.3, 0.2, 0.25)
+    rb, rk = G.rotation("x", 20.0), G.rotation("z", 30.0) @ G.rotation("y", 15.0)
+
+    def tris(t):
+        return "[" + ", ".join("[" + ", ".join("[" + ", ".join(_num(c) for c in v) + "]" for v in tri) + "]"
+                               for tri in t) + "]"  # fmt: skip
+
+    def mat(m):
+        return "{matrix: [" + ", ".join("[" + ", ".join(_num(c) for c in row) + "]" for row in m) + "]}"
+
+    flat = "{energy: [1.5, 5.0], value: [%s, %s]}"
+    lines = ["schema: lumen-detector-yaml/3", "name: yaml_mesh", "detector_volume: Box", "solids:",
+             "  WorldBox: {type: box, params: {x: 4*m, y: 4*m, z: 4*m}}",
+             "  BoxSolid: {type: box, params: {x: 3*m, y: 3*m, z: 3*m}}",
+             "  OrbSolid: {type: orb, params: {r: 0.25*m}}",
+             "  PMTDisc: {type: tube, params: {rmax: 0.15*m, z: 0.02*m}}",
+             "  BallMesh: {type: tessellated, mesh: ball}", "  BlockMesh: {type: tessellated, mesh: block}",
+             f"meshes:\n  ball: {tris(ball)}\n  block: {tris(block)}", "volumes:",
+             "  World: {solid: WorldBox, material: Air}", "  Box: {solid: BoxSolid, material: Water}",
+             "  Ball: {solid: BallMesh, material: Steel}", "  Block: {solid: BlockMesh, material: Black}",
+             "  Orb: {solid: OrbSolid, material: Glass}", "  PMT: {solid: PMTDisc, material: Photocathode}",
+             "placements:", "  - {name: BoxPV, volume: Box, mother: World}",
+             f"  - {{name: Ball, volume: Ball, mother: Box, position: [-0.5, 0.2, 0.1], rotation: {mat(rb)}}}",
+             f"  - {{name: Block, volume: Block, mother: Box, position: [0.6, -0.3, -0.2], rotation: {mat(rk)}}}",
+             "  - {name: Orb, volume: Orb, mother: Box, position: [0.3, 0.6, 0.4]}"]  # fmt: skip
+    for i in range(4):
+        x = _num(-0.75 + 0.5 * i)
+        lines.append(f"  - {{name: PMT_{i}, volume: PMT, mother: Box, copy: {i}, position: [{x}, 0.0, -1.48]}}")
+        lines.append(f"  - {{name: PMT_{4 + i}, volume: PMT, mother: Box, copy: {4 + i}, position: [{x}, 0.0, 1.48]}}")
+    lines += ["materials:",
+              "  Water: {state: liquid, composition: {density_g_cm3: 1.0, components: [{ref: H, atoms: 2}, "
+              "{ref: O, atoms: 1}]}, properties: {RINDEX: " + flat % (1.33, 1.33) + ", ABSLENGTH: " + flat % (30.0, 30.0) +
+              ", RAYLEIGH: " + flat % (10.0, 10.0) + "}}",
+              "  Glass: {state: solid, composition: {density_g_cm3: 2.2, components: [{ref: Si, atoms: 1}, "
+              "{ref: O, atoms: 2}]}, properties: {RINDEX: " + flat % (1.5, 1.5) + ", ABSLENGTH: " + flat % (5.0, 5.0) +
+              "}}"]
+    for name in ("Air", "Steel", "Black", "Photocathode"):
+        lines.append(f"  {name}: {{state: solid, composition: {{density_g_cm3: 1.0, components: "
+                     f"[{{ref: O, fraction: 1.0}}]}}}}")
+    lines += ["surfaces:",
+              "  CathodeSurface: {type: dielectric_metal, model: unified, finish: polished, value: 0, properties: "
+              "{REFLECTIVITY: " + flat % (0.0, 0.0) + ", EFFICIENCY: " + flat % (1.0, 1.0) + "}}",
+              "  Shiny: {type: dielectric_metal, model: unified, finish: polished, value: 0, properties: "
+              "{REFLECTIVITY: " + flat % (0.8, 0.8) + "}}",
+              "  Wall: {type: dielectric_metal, model: unified, finish: ground, value: 0.2, properties: "
+              "{REFLECTIVITY: " + flat % (0.6, 0.6) + ", SPECULARLOBECONSTANT: " + flat % (0.5, 0.5) + "}}",
+              "skins:", "  - {name: WallSkin, surface: Wall, volume: Box}",
+              "  - {name: ShinySkin, surface: Shiny, volume: Ball}", "borders:"]  # fmt: skip
+    lines += [f"  - {{name: Cathode_{i}, surface: CathodeSurface, pv1: BoxPV, pv2: PMT_{i}}}" for i in range(8)]
+    lines += ["sensors:", "  - {name: pmt, rule: border_into, lv: PMT, values: examples/data/toy_pmt.json, "
+              "readout: {gate: [-10.0, 60.0]}}"]  # fmt: skip
+    os.makedirs(where, exist_ok=True)
+    with open(os.path.join(where, "detector.yaml"), "w") as f:
+        f.write("\n".join(lines) + "\n")
 
 
 def main(ref_root):
@@ -46,6 +113,8 @@ def main(ref_root):
                                             recipe=recipe),
                 "yaml_toy": api.convert(os.path.join(data, "yaml_toy"), os.path.join(tmp, "y.lumen")),
                 "yaml_scint": api.convert(os.path.join(HERE, "yaml_scint"), os.path.join(tmp, "s.lumen"))}  # fmt: skip
+        mesh_tank_yaml(os.path.join(tmp, "yaml_mesh"))
+        made["yaml_mesh"] = api.convert(os.path.join(tmp, "yaml_mesh"), os.path.join(tmp, "m.lumen"))
         for name, path in made.items():
             x = reference.export(api.load(path))
             reference.save(x, os.path.join(HERE, f"refdet_{name}.json"))

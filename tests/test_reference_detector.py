@@ -184,3 +184,41 @@ def test_covered_mie_lobe_choice():
     assert np.max(np.abs(covered.arrival / plain.arrival - 1.0)) > 1e-6  # other draws, not another summation order
     (a, ea), (b, eb) = total(covered), total(direct)
     assert abs(a - b) < 4.0 * np.hypot(ea, eb), (a, b, ea, eb)
+
+
+def test_tessellated_parts_from_the_reference_pipeline():
+    """``detectors.mesh_tank`` written in the reference's YAML format (tests/golden/make_reference_detector.py
+    ``mesh_tank_yaml``: a tessellated steel icosphere with a polished skin, a tessellated black box, a glass orb, eight
+    sensor discs, a ground wall) and read by the reference: its meshes are the navigator's opaque pseudo-volumes with
+    the reference's classes (the ball's own skin where the water enters it: Geant4's enteredDaughter order), and it
+    traces bit for bit as this builder's reading of the same description at the reference's poses (its YAML rotations
+    pass through Geant4's angles, which moves a matrix's last bits)."""
+    x = reference.load(os.path.join(GOLD, "refdet_yaml_mesh.json"))
+    assert [m["pv"].split("/")[-1] for m in x["meshes"]] == ["Ball", "Block"]
+    d = reference.detector(x)
+    pose = {v["pv"].split("/")[-2]: (v["R"], v["t"]) for v in x["volumes"] if "/" in v["pv"]}
+    pose.update({m["pv"].split("/")[-2]: (m["R"], m["t"]) for m in x["meshes"]})
+    box = G.Volume("Box", G.Box(1.5, 1.5, 1.5), "Water")
+    for name, lv in (("Ball", G.Volume("Ball", G.Mesh(G.icosphere(0.4, 2)), "Steel")),
+                     ("Block", G.Volume("Block", G.Mesh(G.box_mesh(0.3, 0.2, 0.25)), "Black")),
+                     ("Orb", G.Volume("Orb", G.Orb(0.25), "Glass"))):  # fmt: skip
+        box.place(lv, pose[name][1], pose[name][0], name=name)
+    pmt = G.Volume("PMT", G.Tube(rmax=0.15, dz=0.01), "Photocathode")
+    for i in range(8):
+        box.place(pmt, pose[f"PMT_{i}"][1], pose[f"PMT_{i}"][0], name=f"PMT_{i}", copy=i)
+    cathode = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    shiny = O.OpticalSurface("Shiny", "dielectric_metal", "polished", reflectivity=0.8)
+    wall = O.OpticalSurface("Wall", "dielectric_metal", "ground", reflectivity=0.6, sigma_alpha=0.2, specularlobe=0.5)
+    mats = {"Water": O.Material("Water", rindex=1.33, abslength=30.0, rayleigh=10.0),
+            "Glass": O.Material("Glass", rindex=1.5, abslength=5.0), "Steel": O.Material("Steel"),
+            "Black": O.Material("Black"), "Photocathode": O.Material("Photocathode")}  # fmt: skip
+    own = D.build(box, mats, borders=[("Box", f"PMT_{i}", cathode) for i in range(8)],
+                  skins={"Box": wall, "Ball": shiny}, sensors={"pmt": "PMT"}, after_tracking=("pmt",))  # fmt: skip
+    src = sources.Point(position=(0.0, 0.5, -0.6), n_photons=1.0, lam=400.0)
+    n = 1 << 16
+    a, _ = oracle.trace(d, KEY0, n, source=src, samples=n)
+    b, _ = oracle.trace(own, KEY0, n, source=src, samples=n)
+    order = [own.sensors.name.index(s.split("/")[-2]) for s in d.sensors.name]  # the reference's sensor order
+    np.testing.assert_allclose(a.arrival[0], b.arrival[0][order], rtol=RTOL)
+    np.testing.assert_allclose(a.arrival2[0], b.arrival2[0][order], rtol=RTOL)
+    assert np.array_equal(a.counts, b.counts)
