@@ -273,7 +273,7 @@ enum { LUMEN_VARIANT_WAVEFRONT = 3, LUMEN_N_VARIANT = 4 };
    2 = 256 x 3 (85 registers); 3 = the wavefront: rounds of two kernels (the query; the rest of the step and the
    refill) over a pool of slots in HBM, then the persistent loop resuming the slots still live (its drain: one thread
    a slot, then the photons left). A synchronous call reads a live-slot count back every four rounds and drains once
-   fewer than an eighth of the slots are live; a LUMEN_F_ASYNC call runs a fixed number of rounds (wave_rounds) and
+   fewer than a 64th of the slots are live; a LUMEN_F_ASYNC call runs a fixed number of rounds (wave_rounds) and
    drains, reading nothing back. Every variant gives the same photons the same paths. */
 typedef struct LumenControls {
   float max_distance;      /* m: a query's reach (<= 0: the scene's reach) */
@@ -291,7 +291,7 @@ typedef struct LumenControls {
                               the persistent loop finishes the live slots and the photons left (<= 0: the scene's
                               rounds per photon a slot carries, measured by its last synchronous wavefront call, else
                               3, times the photons a slot carries). A synchronous call reads the live slots back every
-                              fourth round and hands the tail (fewer than an eighth of the slots live) to the
+                              fourth round and hands the tail (fewer than a 64th of the slots live) to the
                               persistent loop; it ignores this field. */
 } LumenControls;
 

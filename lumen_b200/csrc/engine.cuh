@@ -652,8 +652,8 @@ int launch_shape(const Launch& L, int bps, cudaStream_t stream, int blocks) {
 
 // The wavefront's rounds (LUMEN_VARIANT_WAVEFRONT): a fill, then query and step kernels, then the drain: the
 // persistent loop resumes every slot still live (one thread a slot) and takes the photons left. A synchronous call
-// reads the live slots back every fourth round and drains once fewer than an eighth of the slots are live (the tail,
-// where a round's launches cost more than its few steps); an asynchronous one (LUMEN_F_ASYNC) runs `rounds` rounds
+// reads the live slots back every fourth round and drains once fewer than a 64th of the slots are live (the tail,
+// where a round's launches cost more than its few steps: measured against an 8th, 16th, 32nd, 256th and 1024th); an asynchronous one (LUMEN_F_ASYNC) runs `rounds` rounds
 // without a readback (<= 0: *rpp rounds per photon a slot carries, the scene's estimate from its last synchronous
 // call) and drains. The pool holds up to LUMEN_WAVE_POOL slots (about 350 bytes each with gradients), allocated on the
 // call's stream.
@@ -705,7 +705,7 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
       CK(cudaMemcpyAsync(&h, V.live, sizeof(h), cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
       if (h == 0) break;
-      if (h < (unsigned long long)(W / 8)) {
+      if (h < (unsigned long long)(W / 64)) {
         drained = 1;
         ++r;
         break;
