@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 13
+#define LUMEN_B200_ABI_VERSION 14
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -200,6 +200,13 @@ typedef struct LumenSceneDesc {
   const int32_t* group_i;    /* host, n_group * 4: the volume, first node, end node, 0 */
   const float* group_r;      /* host, n_group * 9: R row-major */
   const double* group_r64;   /* host, n_group * 9: the float64 navigator's */
+  /* sensors that count a photon born inside them (a group counting by volume, Geant4's sensitive detector:
+     src/lumen/rules/sensors.py:39 counts_born; Optics.born_pair): per class c the class b whose crossing (b, c) is
+     its entry, -1 none. A photon whose first step starts in a sensor volume of such a class deposits there what that
+     entry's row (row_of[b][c]; -1: nothing) detects, evaluated unpolarised at normal incidence with both indices 1,
+     at its emission time, and ends: its whole weight absorbed at a surface (src/lumen/transport/step.py:574 _born).
+     null: no such sensor. */
+  const int32_t* cls_born;   /* host, n_cls */
 } LumenSceneDesc;
 
 enum { LUMEN_TRI_F = 12, LUMEN_CHUNK_I = 4, LUMEN_MESH_CHUNK = 8, LUMEN_MAX_GROUPS_PER_VOLUME = 64 };

@@ -311,21 +311,30 @@ L_DEV void d_type_eval(const DScene& S, const float* __restrict__ pool, int row,
     Rc = col[LUMEN_COL_R];
   } else if (model == 1) {
     d_amplitudes(cos_i, n1, cf(n2, 0.0f), ev.amps);
-    float s_ax[3];
-    d_s_axis(wi, n, s_ax);
-    Cf es, ep;
-    d_components(er, ei, wi, s_ax, &es, &ep);
-    float F = c_abs2(ev.amps[0]) * c_abs2(es) + c_abs2(ev.amps[1]) * c_abs2(ep);
+    float F;
+    if (er) {
+      float s_ax[3];
+      d_s_axis(wi, n, s_ax);
+      Cf es, ep;
+      d_components(er, ei, wi, s_ax, &es, &ep);
+      F = c_abs2(ev.amps[0]) * c_abs2(es) + c_abs2(ev.amps[1]) * c_abs2(ep);
+    } else {  // no state (er null): the unpolarised reflectance, fractions (0.5, 0.5) (types.py:257 _real)
+      F = c_abs2(ev.amps[0]) * 0.5f + c_abs2(ev.amps[1]) * 0.5f;
+    }
     F = d_clip01(F);
     split[0] = F; split[1] = 0.0f; split[2] = 0.0f; split[3] = 0.0f; split[4] = 1.0f - F;
     Rc = col[LUMEN_COL_R];
   } else {
     d_amplitudes(cos_i, n1, cf(col[LUMEN_COL_NR], col[LUMEN_COL_NK]), ev.amps);
-    float s_ax[3];
-    d_s_axis(wi, n, s_ax);
-    Cf es, ep;
-    d_components(er, ei, wi, s_ax, &es, &ep);
-    Rc = d_clip01(c_abs2(ev.amps[0]) * c_abs2(es) + c_abs2(ev.amps[1]) * c_abs2(ep));
+    if (er) {
+      float s_ax[3];
+      d_s_axis(wi, n, s_ax);
+      Cf es, ep;
+      d_components(er, ei, wi, s_ax, &es, &ep);
+      Rc = d_clip01(c_abs2(ev.amps[0]) * c_abs2(es) + c_abs2(ev.amps[1]) * c_abs2(ep));
+    } else {  // unpolarised (fresnel.py:53 unpolarised_absorbing_reflectance)
+      Rc = d_clip01(0.5f * (c_abs2(ev.amps[0]) + c_abs2(ev.amps[1])));
+    }
     split[0] = 1.0f; split[1] = 0.0f; split[2] = 0.0f; split[3] = 0.0f; split[4] = 0.0f;
   }
   float cut[2] = {Rc, col[LUMEN_COL_T]}, zc[2] = {0.0f, 0.0f}, rta[3], drta[3];

@@ -688,9 +688,75 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
   ph.cls = nx_cls;
 }
 
+// A photon born inside a sensor that counts by volume (LumenSceneDesc.cls_born, step.py:574 _born): the entry class
+// of its sensor at its first step, else -2
+template <class NF>
+L_DEV int d_born_entry(const DScene& S, const PhotonT<NF>& ph) {
+  if (!S.cls_born || ph.vertex != 0 || !ph.alive || ph.vol < 0) return -2;
+  const int bp = __ldg(S.cls_born + ph.cls);
+  return (bp >= 0 && vI(S, ph.vol, LUMEN_VI_SENSOR) >= 0) ? bp : -2;
+}
+
+// that first step: the deposit of what the sensor's entry (row_of[bp][cls]) detects, evaluated unpolarised at normal
+// incidence with both indices 1 (step.py:589), at the emission time; the photon ends, its whole weight absorbed at a
+// surface
+template <int G, int ANALOG = 0, class NF = float>
+L_DEV void d_born(const Run& R, PhotonT<NF>& ph, float* dw, int bp, Dep& dep, float* dq, Ana& an) {
+  const DScene& S = R.S;
+  const int P = G > 0 ? R.P : 0;
+  const int row = __ldg(S.row_of + bp * S.n_cls + ph.cls);
+  const int sensor = vI(S, ph.vol, LUMEN_VI_SENSOR);
+  float nrm[3] = {-ph.d[0], -ph.d[1], -ph.d[2]};
+  float dprobs[G > 0 ? G : 1][N_OUT], ddet[G > 0 ? G : 1];
+  Eval ev;
+  d_type_eval<G>(S, R.live, row, ph.lam, ph.d, nrm, 1.0f, 1.0f, nullptr, nullptr, ev, P, R.gt, dprobs, ddet);
+  const float d = ev.detect;
+  dep.sensor = sensor;
+  dep.q = ph.w * d;
+  dep.time = ph.t;
+  if (G > 0)
+    for (int p = 0; p < P; ++p) dq[p] = dw[p] * d + ph.w * ddet[p];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) dep.fates[k] = 0.0f;
+  dep.fates[5] = ph.w;
+  dep.pushed = 0.0f;
+  float inv_an = 1.0f;
+  if (ANALOG && row >= 0 && __ldg(S.row_i + (size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL)) {
+    float a = d_normal_absorptance(S, R.live, row, ph.lam, 1.0f, nrm);
+    inv_an = a > 0.0f ? 1.0f / a : 0.0f;
+  }
+  if (R.rec) {  // the readout groups' record at the emission: the point, direction and normal -d, the volume
+    float xc[3] = {(float)ph.x[0], (float)ph.x[1], (float)ph.x[2]};
+    ph.last = d_record(R, ph.last, sensor, dep.q, ph.t, ph.lam, ph.gen, row, 1.0f, ph.vol, xc, ph.d, nrm);
+  }
+  if (ANALOG) {  // step.py:597: the analog photon absorbed with the detected share, else decided
+    if (an.x < ph.w * d) {
+      an.sensor = sensor;
+      an.time = ph.t;
+      an.lam = ph.lam;
+      an.scale = inv_an;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) an.pos[a] = (float)ph.x[a];
+      an.vol = ph.vol;
+    }
+    an.x = __int_as_float(0x7f800000);
+  }
+  ph.alive = 0;
+  ph.w = 0.0f;
+  ph.wr = 0.0f;
+  if (G > 0)
+    for (int p = 0; p < P; ++p) dw[p] = 0.0f;
+  ph.vertex += 1;
+}
+
 // one whole step: the megakernel's (k_trace)
 template <int G, int TORUS, int ANALOG = 0, class NF = float>
 L_DEV void d_step(const Run& R, PhotonT<NF>& ph, float* dw, Key pkey, Dep& dep, float* dq, Ana& an) {
+  const int bp = d_born_entry(R.S, ph);
+  if (bp != -2) {
+    d_born<G, ANALOG>(R, ph, dw, bp, dep, dq, an);
+    return;
+  }
   PreT<NF> pr;
   d_pre<(TORUS & 1)>(R, ph, pkey, pr);
   QueryT<NF> q = d_step_query<TORUS>(R, ph, pr);

@@ -427,6 +427,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   Photon ph;
   WaveExtra ex;
   wv_ld(V.ph, V.W, i, ph);
+  if (d_born_entry(L.R.S, ph) != -2) return;  // a photon born in a sensor: its step has no query (k_wave_step)
   wv_ld(V.ex, V.W, i, ex);
   Pre pr;
   d_pre<(TORUS & 1)>(L.R, ph, ex.pkey, pr);
@@ -458,14 +459,19 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
   if (act) {
     wv_ld(V.ph, V.W, i, ph);
     wv_ld(V.ex, V.W, i, ex);
-    Pre pr;
-    Query q;
-    wv_ld(V.pre, V.W, i, pr);
-    wv_ld(V.q, V.W, i, q);
     if (G > 0)
       for (int p = 0; p < L.R.P; ++p) dw[p] = V.dw[(size_t)p * V.W + i];
     Ana an;
-    d_post<G>(L.R, ph, dw, pr, q, dep, dq, an);
+    const int bp = d_born_entry(L.R.S, ph);
+    if (bp != -2) {
+      d_born<G>(L.R, ph, dw, bp, dep, dq, an);
+    } else {
+      Pre pr;
+      Query q;
+      wv_ld(V.pre, V.W, i, pr);
+      wv_ld(V.q, V.W, i, q);
+      d_post<G>(L.R, ph, dw, pr, q, dep, dq, an);
+    }
     c_steps++;
     if (dep.sensor >= 0) {
       const int m = deposit<G>(L.T, ex.ev, dep, dq, ex.w0, ex.pt);

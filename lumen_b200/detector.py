@@ -147,6 +147,8 @@ class Detector:
             d.vol_f64, d.node_f64 = dptr(keep["vol_f64"]), dptr(keep["node_f64"])
             d.leaf_f64, d.plane_f64 = dptr(keep["leaf_f64"]), dptr(keep["plane_f64"])
         d.reach = ctypes.c_float(a["reach"])
+        if a.get("cls_born") is not None:  # sensors counting the photons born inside them: each class's entry class
+            d.cls_born = iptr(keep["cls_born"])
         d.n_cls, d.n_med, d.n_row = a["n_cls"], len(keep["med_i"]), len(keep["row_i"])
         d.n_tab, d.n_pool, d.n_sensor = len(keep["tab"]), len(keep["pool"]), self.n_sensor
         d.cls_medium, d.row_of, d.med_i = iptr(keep["cls_medium"]), iptr(keep["row_of"]), iptr(keep["med_i"])
@@ -172,7 +174,7 @@ class Detector:
 
 
 def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=None, prio=None,
-          after_tracking=(), precision="float32", frame_groups=True) -> Detector:
+          after_tracking=(), precision="float32", frame_groups=True, born=()) -> Detector:
     """Return the Detector of the volume tree ``top`` (the detector volume, placed at the origin).
 
     ``materials``: {name: Material}. ``borders``: [(pv from, pv to, OpticalSurface)] (Geant4 border surfaces, ordered);
@@ -183,7 +185,9 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     absorption (eff 1) and are read per normal incidence (types.py:576 per_normal: a deposit carries 1 / A_n, by
     which a normalising readout grid divides it). ``precision``: the navigator's ("float32", or "float64":
     ``Detector.with_precision``). ``frame_groups``: daughters sharing a rotation get a BVH in its frame where that
-    pays (the navigator's speed only; the same results).
+    pays (the navigator's speed only; the same results). ``born``: sensor groups that count a photon emitted inside
+    their volumes at its emission, with what their entry from the mother volume detects (Geant4's sensitive detector
+    counting every step in the volume: src/lumen/rules/sensors.py:39 counts_born, Optics.born_pair).
     """
     skins = skins or {}
     sensors = sensors or {}
@@ -344,23 +348,38 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
             row_i[r, 6 + c] = col_tab[k]
     st = SensorTable(s_name, s_group, np.asarray(s_pos).reshape(-1, 3), np.asarray(s_axis).reshape(-1, 3))
     cls_names = {i: cls_lv[i].name for i in range(out_cls)} | {out_cls: OUTSIDE}
+    # sensors counting the photons born inside them: each such sensor class's entry, the class of its volumes'
+    # mother (the crossing whose detection the emission deposits)
+    cls_born = np.full(n_cls, -1, np.int32)
+    for g in born:
+        lv = sensors[g]
+        for c in range(out_cls):
+            if cls_lv[c].name != lv:
+                continue
+            mothers = sorted(b for b, d in daughter_of if d == c)
+            if not mothers:
+                raise ValueError(f"sensor group {g!r}: its volumes have no mother volume to enter from")
+            cls_born[c] = mothers[0]
     return assemble(nav, vol_cls[:n], n_cls, cls_medium, row_of, med_i, row_i, pool, st, names, cls_names, groups,
-                    precision)  # fmt: skip
+                    precision, cls_born)  # fmt: skip
 
 
 def assemble(nav: dict, vol_cls, n_cls: int, cls_medium, row_of, med_i, row_i, pool: O.Pool, sensors: SensorTable,
-             names: list, cls_names: dict, groups: dict, precision: str = "float32") -> Detector:
+             names: list, cls_names: dict, groups: dict, precision: str = "float32", cls_born=None) -> Detector:
     """Return the Detector of navigator arrays ``nav`` (``geometry.navigator_arrays``, volumes of classes ``vol_cls``)
     and the surface lookup's tables: per class its medium (``cls_medium``), per crossed class pair its surface row
     (``row_of`` (C, C), -1 never crossed), the media's (``med_i``) and rows' (``row_i``) table indices into ``pool``;
     then the diffusion jump's clearance grids of the media whose only channel is Rayleigh
-    (src/lumen/transport/fastpath.py:96)."""  # noqa: D205, D209
+    (src/lumen/transport/fastpath.py:96). ``cls_born``: per class the entry class of a sensor that counts the photons
+    born inside it (-1 none; None: no such sensor)."""  # noqa: D205, D209
     params_index = dict(pool.names)
     tab, data = pool.arrays()
     arrays = dict(nav)
     arrays.update(n_cls=int(n_cls), cls_medium=np.asarray(cls_medium, np.int32),
                   row_of=np.asarray(row_of).ravel().astype(np.int32), med_i=np.asarray(med_i, np.int32),
                   row_i=np.asarray(row_i, np.int32), tab=tab)  # fmt: skip
+    if cls_born is not None and np.any(np.asarray(cls_born) >= 0):
+        arrays["cls_born"] = np.asarray(cls_born, np.int32)
     media = []
     for m in range(len(med_i)):
         ok = med_i[m, 0] >= 0 and med_i[m, 2] >= 0 and med_i[m, 3] < 0 and med_i[m, 7] < 0

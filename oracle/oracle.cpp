@@ -165,12 +165,78 @@ static inline void o_dmed(const ORun* R, int mi, float lam, const OMed* m, float
    run of that version can be reproduced; every engine path runs the current rule */
 static int g_rule_020 = 0;
 
+/* the first step of a photon born inside a sensor that counts by volume (step.py:574 _born): it deposits what the
+   sensor's entry (row_of[bp][cls]) detects, evaluated unpolarised at normal incidence with both indices 1
+   (step.py:589), at its emission time, and ends: its whole weight absorbed at a surface */
+template <class NF>
+static void o_born(const ORun* R, OPhotonT<NF>* ph, ODep* dep, int bp, int sensor) {
+  const LumenSceneDesc* D = R->S.D;
+  const int P = R->P;
+  int row = D->row_of[bp * D->n_cls + ph->cls];
+  float nrm[3] = {-ph->d[0], -ph->d[1], -ph->d[2]};
+  float dcol[O_MAXG * LUMEN_N_COL], dprobs[O_MAXG * O_N_OUT], ddet[O_MAXG];
+  for (int p = 0; p < P; ++p)
+    for (int c = 0; c < LUMEN_N_COL; ++c)
+      dcol[p * LUMEN_N_COL + c] =
+          (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_COL + c] == R->gt[p]) ? 1.0f : 0.0f;
+  OEval ev;
+  o_type_eval(D, R->live, row, ph->lam, ph->d, nrm, 1.0f, 1.0f, 0, 0, &ev, P, dcol, dprobs, ddet);
+  const float d = ev.detect;
+  float inv_an = 1.0f;
+  if (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL]) {
+    float an = o_normal_absorptance(D, R->live, row, ph->lam, 1.0f, nrm);
+    inv_an = an > 0.0f ? 1.0f / an : 0.0f;
+  }
+  dep->sensor = sensor;
+  dep->q = ph->w * d;
+  dep->time = ph->t;
+  dep->lam = ph->lam;
+  for (int p = 0; p < P; ++p) dep->dq[p] = ph->dw[p] * d + ph->w * ddet[p];
+  ORec* rc = &dep->rec;
+  rc->sensor = sensor;
+  rc->q = dep->q;
+  rc->time = ph->t;
+  rc->lam = ph->lam;
+  rc->gen = ph->gen;
+  rc->vol = ph->vol;
+  for (int a = 0; a < 3; ++a) { rc->x[a] = (float)ph->x[a]; rc->d[a] = ph->d[a]; rc->n[a] = nrm[a]; }
+  rc->inv_an = inv_an;
+  for (int k = 0; k < 8; ++k) dep->fates[k] = 0.0f;
+  dep->fates[5] = ph->w;
+  dep->pushed = 0.0f;
+  if (R->analog) { /* step.py:597: the analog photon absorbed with the detected share, else decided */
+    const float share = ph->w * d;
+    if (ph->ax < share) {
+      ph->asensor = sensor;
+      ph->atime = ph->t;
+      ph->alam = ph->lam;
+      ph->ascale = inv_an;
+      for (int a = 0; a < 3; ++a) ph->apos[a] = (float)ph->x[a];
+      ph->avol = ph->vol;
+    }
+    ph->ax = INFINITY;
+  }
+  ph->alive = 0;
+  ph->w = 0.0f;
+  ph->wr = 0.0f;
+  for (int p = 0; p < P; ++p) ph->dw[p] = 0.0f;
+  ph->vertex += 1;
+}
+
 /* one step (step.py:516); NF the navigator's precision */
 template <class NF>
 static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
   const OScene* S = &R->S;
   const LumenSceneDesc* D = S->D;
   const int P = R->P;
+  if (D->cls_born && ph->vertex == 0 && ph->alive && ph->vol >= 0) {
+    const int bp = D->cls_born[ph->cls];
+    const int sensor = D->vol_i[(size_t)ph->vol * LUMEN_VOL_I + LUMEN_VI_SENSOR];
+    if (bp >= 0 && sensor >= 0) {
+      o_born(R, ph, dep, bp, sensor);
+      return;
+    }
+  }
   /* _recover: the stuck rule's push (step.py:245) */
   NF b0 = onav_band(onav_maxabs3(ph->x));
   int stuck = ph->alive && ph->nz >= O_ZSBP;

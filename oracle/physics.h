@@ -318,11 +318,16 @@ static inline void o_type_eval(const LumenSceneDesc* D, const float* pool, int r
     }
   } else if (model == 1) { /* _real: the two media's Fresnel interface */
     o_amplitudes(cos_i, n1, oc(n2, 0.0f), ev->amps);
-    float s_ax[3];
-    o_s_axis(wi, n, s_ax);
-    Oc es, ep;
-    o_components(er, ei, wi, s_ax, &es, &ep);
-    float F = oc_abs2(ev->amps[0]) * oc_abs2(es) + oc_abs2(ev->amps[1]) * oc_abs2(ep);
+    float F;
+    if (er) {
+      float s_ax[3];
+      o_s_axis(wi, n, s_ax);
+      Oc es, ep;
+      o_components(er, ei, wi, s_ax, &es, &ep);
+      F = oc_abs2(ev->amps[0]) * oc_abs2(es) + oc_abs2(ev->amps[1]) * oc_abs2(ep);
+    } else { /* no state: the unpolarised reflectance, fractions (0.5, 0.5) (types.py:257 _real) */
+      F = oc_abs2(ev->amps[0]) * 0.5f + oc_abs2(ev->amps[1]) * 0.5f;
+    }
     F = o_clip01(F);
     split[0] = F; split[1] = 0.0f; split[2] = 0.0f; split[3] = 0.0f; split[4] = 1.0f - F;
     Rc = col[LUMEN_COL_R];
@@ -332,11 +337,15 @@ static inline void o_type_eval(const LumenSceneDesc* D, const float* pool, int r
     }
   } else { /* _complex: a complex index seen from a dielectric */
     o_amplitudes(cos_i, n1, oc(col[LUMEN_COL_NR], col[LUMEN_COL_NK]), ev->amps);
-    float s_ax[3];
-    o_s_axis(wi, n, s_ax);
-    Oc es, ep;
-    o_components(er, ei, wi, s_ax, &es, &ep);
-    Rc = o_clip01(oc_abs2(ev->amps[0]) * oc_abs2(es) + oc_abs2(ev->amps[1]) * oc_abs2(ep));
+    if (er) {
+      float s_ax[3];
+      o_s_axis(wi, n, s_ax);
+      Oc es, ep;
+      o_components(er, ei, wi, s_ax, &es, &ep);
+      Rc = o_clip01(oc_abs2(ev->amps[0]) * oc_abs2(es) + oc_abs2(ev->amps[1]) * oc_abs2(ep));
+    } else { /* unpolarised (fresnel.py:53 unpolarised_absorbing_reflectance) */
+      Rc = o_clip01(0.5f * (oc_abs2(ev->amps[0]) + oc_abs2(ev->amps[1])));
+    }
     split[0] = 1.0f; split[1] = 0.0f; split[2] = 0.0f; split[3] = 0.0f; split[4] = 0.0f;
     for (int p = 0; p < grad; ++p) { for (int j = 0; j < 5; ++j) dsplit[p][j] = 0.0f; dRc[p] = 0.0f; }
   }

@@ -7,7 +7,8 @@ The reference converts and loads its two shipped example detectors under the num
 examples/example_tank.py: detector volume TankLV, the PMT placements counted across CathodeSurface) and the YAML toy
 (examples/data/yaml_toy), and the scintillator cube of ``tests/golden/yaml_scint`` (this repository's YAML, in the
 reference's format: Rayleigh, Mie and a WLS with an exponential profile in one medium, a ground unified wall), and
-``detectors.mesh_tank`` written out in the same format by ``mesh_tank_yaml`` (tessellated parts, an orb, skins).
+``detectors.mesh_tank`` written out in the same format by ``mesh_tank_yaml`` (tessellated parts, an orb, skins), and
+a water cube that is an ``any_entry`` sensor counting the photons born inside it (``born_cube_yaml``).
 ``lumen_b200.reference.export`` then writes what the reference's photon loop runs on: the
 navigator scene's instances and flattened solids, the compiled optics, the packed parameters, the defensive rows.
 The tests rebuild the detectors from these files with ``lumen_b200.reference.detector``.
@@ -92,6 +93,32 @@ def mesh_tank_yaml(where):
         f.write("\n".join(lines) + "\n")
 
 
+def born_cube_yaml(where):
+    """Write a 2 m water box holding a 0.4 m water cube that is a sensor of an ``any_entry`` group (counted on every
+    entry, and counting the photons born inside it: src/lumen/rules/sensors.py:39 counts_born), in the reference's
+    YAML detector format, into the directory ``where``."""  # noqa: D205, D209
+    flat = "{energy: [1.5, 5.0], value: [%s, %s]}"
+    text = "\n".join([
+        "schema: lumen-detector-yaml/3", "name: yaml_born", "detector_volume: Box", "solids:",
+        "  WorldBox: {type: box, params: {x: 3*m, y: 3*m, z: 3*m}}",
+        "  BoxSolid: {type: box, params: {x: 2*m, y: 2*m, z: 2*m}}",
+        "  CubeSolid: {type: box, params: {x: 0.4*m, y: 0.4*m, z: 0.4*m}}",
+        "volumes:", "  World: {solid: WorldBox, material: Air}", "  Box: {solid: BoxSolid, material: Water}",
+        "  Cube: {solid: CubeSolid, material: Water}",
+        "placements:", "  - {name: BoxPV, volume: Box, mother: World}",
+        "  - {name: CubePV, volume: Cube, mother: Box, position: [0.3, 0.0, 0.0]}",
+        "materials:",
+        "  Water: {state: liquid, composition: {density_g_cm3: 1.0, components: [{ref: H, atoms: 2}, {ref: O, "
+        "atoms: 1}]}, properties: {RINDEX: " + flat % (1.33, 1.33) + ", ABSLENGTH: " + flat % (20.0, 20.0) +
+        ", RAYLEIGH: " + flat % (5.0, 5.0) + "}}",
+        "  Air: {state: gas, composition: {density_g_cm3: 0.0012, components: [{ref: N, fraction: 1.0}]}}",
+        "sensors:", "  - {name: s, rule: any_entry, lv: Cube, values: examples/data/toy_pmt.json, "
+        "readout: {gate: [-10.0, 60.0]}}", ""])  # fmt: skip
+    os.makedirs(where, exist_ok=True)
+    with open(os.path.join(where, "detector.yaml"), "w") as f:
+        f.write(text)
+
+
 def main(ref_root):
     import refstub
 
@@ -115,6 +142,8 @@ def main(ref_root):
                 "yaml_scint": api.convert(os.path.join(HERE, "yaml_scint"), os.path.join(tmp, "s.lumen"))}  # fmt: skip
         mesh_tank_yaml(os.path.join(tmp, "yaml_mesh"))
         made["yaml_mesh"] = api.convert(os.path.join(tmp, "yaml_mesh"), os.path.join(tmp, "m.lumen"))
+        born_cube_yaml(os.path.join(tmp, "yaml_born"))
+        made["yaml_born"] = api.convert(os.path.join(tmp, "yaml_born"), os.path.join(tmp, "b.lumen"))
         for name, path in made.items():
             x = reference.export(api.load(path))
             reference.save(x, os.path.join(HERE, f"refdet_{name}.json"))

@@ -730,13 +730,14 @@ def ref_dets():
 
     gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
     return {n: reference.detector(reference.load(os.path.join(gold, f"refdet_{n}.json")))
-            for n in ("example_tank", "yaml_toy", "yaml_scint", "yaml_mesh")}  # fmt: skip
+            for n in ("example_tank", "yaml_toy", "yaml_scint", "yaml_mesh", "yaml_born")}  # fmt: skip
 
 
 @pytest.mark.parametrize(("name", "pos", "n_photons", "lam"), [("example_tank", (0.0, 0.0, 0.1), 2e5, 400.0),
                                                                ("yaml_toy", (0.1, 0.0, 0.2), 1e5, 400.0),
                                                                ("yaml_scint", (0.0, 0.0, 0.1), 1e4, 380.0),
-                                                               ("yaml_mesh", (0.0, 0.5, -0.6), 1.0, 400.0)])  # fmt: skip
+                                                               ("yaml_mesh", (0.0, 0.5, -0.6), 1.0, 400.0),
+                                                               ("yaml_born", (0.35, 0.05, -0.1), 1.0, 400.0)])  # fmt: skip
 def test_reference_pipeline_detectors_match(name, pos, n_photons, lam, ref_dets, built):
     """The detectors the reference's own pipeline compiled: per-photon records bit-exact, then the tallies, the
     published runs' workloads (the toy tank's arrivals are the published table: tests/test_reference_detector.py)
@@ -765,3 +766,49 @@ def test_covered_mie_lobe_choice_matches(built):
         np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL)
         np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
         np.testing.assert_allclose(T.health.cpu().numpy(), O.health, rtol=1e-6, atol=1e-6)
+
+
+def _born_cube():
+    from lumen_b200 import geometry as G
+    from lumen_b200 import optics as O
+    from lumen_b200.detector import build
+
+    water = O.Material("Water", rindex=1.33, abslength=20.0, rayleigh=5.0)
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "Water")
+    cube = G.Volume("Cube", G.Box(0.2, 0.2, 0.2), "Water")
+    box.place(cube, (0.3, 0.0, 0.0), name="Cube")
+    surf = O.OpticalSurface("Skin", "dielectric_metal", "polished", reflectivity=0.2, efficiency=0.7)
+    return build(box, {"Water": water}, borders=[("Box", "Cube", surf)], sensors={"s": "Cube"}, born=("s",))
+
+
+def test_photons_born_in_a_counting_sensor_match(built):
+    """A sensor that counts the photons born inside it (LumenSceneDesc.cls_born): a source whose tracks start inside
+    and outside the sensor cube; per-photon records bit-exact, tallies with a gradient in the entry efficiency in both
+    schedules, and the truth rows' analog records."""
+    det = _born_cube()
+    rng = np.random.default_rng(3)
+    e = 32
+    start = np.column_stack([rng.uniform(0.0, 0.6, e), rng.uniform(-0.3, 0.3, e), rng.uniform(-0.3, 0.3, e)])
+    u = rng.normal(size=(e, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    counts = np.full(e, 512, np.int64)
+    src = sources.Tracks(start=start, direction=u, length=rng.uniform(0.1, 0.5, e), cone_angle=np.radians(42.0),
+                         n_photons=counts.astype(float), lam_range=(300.0, 600.0), counts_=counts)  # fmt: skip
+    n = int(counts.sum())
+    bad, gi, oi, gf, of = _records_match(det, src, n)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+    gt = [det.params_index["surfaces/Skin/eff"]]
+    for variant in (0, A.VARIANT_WAVEFRONT):
+        T, O = _tallies(det, src, n, controls=A.controls(grad_tabs=gt, variant=variant))
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=RTOL)
+        np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=RTOL)
+        np.testing.assert_allclose(T.jac.cpu().numpy(), O.jac, rtol=1e-7, atol=1e-12)
+        assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
+    eng = _engine(det)
+    ds = DeviceSource(src, n)
+    c = A.controls(flags=A.F_TRUTH)
+    T = DeviceTallies(det.n_sensor, ds.n_events, 0, 0.0, 1.0, 0).attach_truth(n)
+    eng.trace(KEY, n, source=ds, controls=c, tallies=T)
+    O, _ = oracle.trace(det, KEY, n, source=src, samples=n, controls=c, truth=True, n_events=ds.n_events)
+    g = T.truth.cpu().numpy()
+    assert (g.view(np.uint32) == O.truth.view(np.uint32)).all()

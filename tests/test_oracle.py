@@ -227,3 +227,48 @@ def test_cathode_reflectivity_derivative_at_zero():
     refl = jac + lo.arrival[0]
     assert (refl > -1e-9 * lo.arrival[0]).all() and refl[0] > 0 and refl[1] > 0  # PMTs 0 and 1 face each other
     np.testing.assert_allclose(fd, jac, rtol=2e-3)
+
+
+def sensitive_cube(R=0.2, eff=0.7, born=True):
+    """A 2 m water box holding a 0.4 m water cube that is a sensor (entered through a polished metal border of
+    reflectivity R and efficiency eff) whose group counts the photons born inside it (``born``)."""
+    water = O.Material("Water", rindex=1.33, abslength=20.0, rayleigh=5.0)
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "Water")
+    cube = G.Volume("Cube", G.Box(0.2, 0.2, 0.2), "Water")
+    box.place(cube, (0.3, 0.0, 0.0), name="Cube")
+    surf = O.OpticalSurface("Skin", "dielectric_metal", "polished", reflectivity=R, efficiency=eff)
+    return build(box, {"Water": water}, borders=[("Box", "Cube", surf)], sensors={"s": "Cube"},
+                 born=("s",) if born else ())  # fmt: skip
+
+
+def test_photons_born_in_a_counting_sensor_deposit_its_entry_detection():
+    """src/lumen/transport/step.py:574 _born: a photon emitted inside a sensor that counts by volume deposits, at its
+    first step, what the sensor's entry detects at normal incidence ((1 - R) eff here), at its emission time, and ends
+    (its whole weight absorbed at a surface); emitted outside, it is counted at the entry as before."""
+    R, eff = 0.2, 0.7
+    det = sensitive_cube(R, eff)
+    assert det.arrays["cls_born"].max() >= 0
+    n = 1 << 14
+    inside = sources.Point(position=(0.35, 0.05, -0.1), n_photons=1.0, lam=400.0, time=3.0)
+    T, _ = oracle.trace(det, KEY0, n, source=inside, samples=n)
+    want = np.float32(1.0 - R) * np.float32(eff)
+    np.testing.assert_allclose(T.arrival[0, 0], want, rtol=1e-6)
+    np.testing.assert_allclose(T.arrival_t[0, 0] / T.arrival[0, 0], 3.0, rtol=1e-6)  # at the emission time
+    assert T.counts[A.C_STEPS] == n and T.counts[A.C_DEPOSITS] == n  # one step, one deposit a photon
+    h = T.health
+    np.testing.assert_allclose(h[5], 1.0, rtol=1e-6)  # every weight absorbed at a surface
+    outside = sources.Point(position=(-0.5, 0.0, 0.0), n_photons=1.0, lam=400.0)
+    a, _ = oracle.trace(det, KEY0, n, source=outside, samples=n)
+    b, _ = oracle.trace(sensitive_cube(R, eff, born=False), KEY0, n, source=outside, samples=n)
+    np.testing.assert_allclose(a.arrival, b.arrival, rtol=1e-12)  # entered from outside: unchanged
+
+
+def test_born_deposit_derivative_in_the_entry_efficiency():
+    """The born deposit's tangent: d/d eff of (1 - R) eff is 1 - R per photon."""
+    det = sensitive_cube()
+    key = "surfaces/Skin/eff"
+    c = A.controls(grad_tabs=[det.params_index[key]])
+    n = 1 << 12
+    inside = sources.Point(position=(0.35, 0.05, -0.1), n_photons=1.0, lam=400.0)
+    T, _ = oracle.trace(det, KEY0, n, source=inside, samples=n, controls=c)
+    np.testing.assert_allclose(T.jac[0, 0, 0], np.float32(1.0 - 0.2), rtol=1e-6)

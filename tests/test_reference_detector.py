@@ -222,3 +222,23 @@ def test_tessellated_parts_from_the_reference_pipeline():
     np.testing.assert_allclose(a.arrival[0], b.arrival[0][order], rtol=RTOL)
     np.testing.assert_allclose(a.arrival2[0], b.arrival2[0][order], rtol=RTOL)
     assert np.array_equal(a.counts, b.counts)
+
+
+def test_any_entry_sensor_counting_photons_born_inside():
+    """An ``any_entry`` sensor group (the reference's default count="volume": src/lumen/rules/sensors.py:39
+    counts_born) through the reference's pipeline: ``Optics.born_pair`` names the water the cube is entered from, and
+    a photon emitted inside the cube deposits at its first step what that entry's counting row detects (1: the group's
+    sensor model applies its efficiency after tracking) and ends; emitted outside, it is counted where it enters."""
+    x = reference.load(os.path.join(GOLD, "refdet_yaml_born.json"))
+    d = reference.detector(x)
+    sensor_cls = x["class_of"]["BoxPV/CubePV/Cube"]
+    assert x["born_pair"][sensor_cls] == x["class_of"]["BoxPV/Box"]
+    assert d.arrays["cls_born"][sensor_cls] == x["class_of"]["BoxPV/Box"]
+    n = 1 << 14
+    inside = sources.Point(position=(0.35, 0.05, -0.1), n_photons=1.0, lam=400.0, time=2.0)
+    T, _ = oracle.trace(d, KEY0, n, source=inside, samples=n)
+    assert T.arrival[0, 0] == 1.0 and T.counts[A.C_STEPS] == n
+    np.testing.assert_allclose(T.arrival_t[0, 0], 2.0, rtol=1e-7)
+    outside = sources.Point(position=(-0.5, 0.0, 0.0), n_photons=1.0, lam=400.0)
+    U, _ = oracle.trace(d, KEY0, n, source=outside, samples=n)
+    assert 0.0 < U.arrival[0, 0] < 1.0 and U.counts[A.C_STEPS] > n
