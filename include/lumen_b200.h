@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define LUMEN_B200_ABI_VERSION 14
+#define LUMEN_B200_ABI_VERSION 15
 
 typedef enum LumenStatus {
   LUMEN_OK = 0,
@@ -207,6 +207,11 @@ typedef struct LumenSceneDesc {
      at its emission time, and ends: its whole weight absorbed at a surface (src/lumen/transport/step.py:574 _born).
      null: no such sensor. */
   const int32_t* cls_born;   /* host, n_cls */
+  /* exit sensors (a border out of a sensor's volume whose surface has an EFFICIENCY: Geant4's boundary process
+     detects there, src/lumen/rules/boundary.py:92 "credited to pre"; Optics.deposit_pre): per (class left, class met)
+     pair 1 where the crossing's deposit goes to the sensor of the volume left (and its local fields are read in that
+     volume's frame, src/lumen/transport/step.py:615 _sensor_dep, :653 sensor_frame), else 0. null: none. */
+  const int32_t* pair_pre;   /* host, n_cls * n_cls */
 } LumenSceneDesc;
 
 enum { LUMEN_TRI_F = 12, LUMEN_CHUNK_I = 4, LUMEN_MESH_CHUNK = 8, LUMEN_MAX_GROUPS_PER_VOLUME = 64 };

@@ -68,7 +68,7 @@ class LumenSceneDesc(ctypes.Structure):
         ("n_mesh", ctypes.c_int32), ("n_chunk", ctypes.c_int32), ("n_tri", ctypes.c_int32), ("mesh_tri", c_f32p),
         ("mesh_tri64", c_f64p), ("mesh_chunk", c_i32p), ("chunk_box", c_f32p), ("chunk_box64", c_f64p),
         ("n_group", ctypes.c_int32), ("group_i", c_i32p), ("group_r", c_f32p), ("group_r64", c_f64p),
-        ("cls_born", c_i32p),
+        ("cls_born", c_i32p), ("pair_pre", c_i32p),
     ]  # fmt: skip
 
 

@@ -55,6 +55,7 @@ struct DScene {
   const int32_t* __restrict__ prog_i;
   const int32_t* __restrict__ cls_medium;
   const int32_t* __restrict__ cls_born;  // per class the entry class of a sensor counting photons born in it, or null
+  const int32_t* __restrict__ pair_pre;  // per class pair 1: the deposit goes to the volume left's sensor, or null
   const int32_t* __restrict__ row_of;
   const int32_t* __restrict__ med_i;
   const int32_t* __restrict__ row_i;

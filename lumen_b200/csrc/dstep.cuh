@@ -291,7 +291,11 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
     }
   }
   float mu_r = mr.mu_c;
-  int sensor_q = q.hit ? vI(S, q.vol_after, LUMEN_VI_SENSOR) : -1;
+  // the sensor a crossing's deposit credits: the one entered, or at an exit sensor's crossing the one left, whose
+  // frame the deposit's local fields are read in (step.py:615 _sensor_dep, :653 sensor_frame)
+  const int v_sens = (S.pair_pre && q.hit && __ldg(S.pair_pre + q.cls_before * S.n_cls + q.cls_after)) ? q.vol_before
+                                                                                                       : q.vol_after;
+  int sensor_q = (q.hit && v_sens >= 0) ? vI(S, v_sens, LUMEN_VI_SENSOR) : -1;
   float dist = q.t;
   int zero = dist <= D_ZERO_STEP_BANDS * b0;
   int cb = q.cls_before, ca = q.cls_after;
@@ -618,7 +622,7 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
       }
 #pragma unroll
       for (int a = 0; a < 3; ++a) an.pos[a] = (float)(ph.x[a] + q.t * ph.d[a]);
-      an.vol = q.vol_after;
+      an.vol = v_sens;
       an.x = inf;
     } else {
       float xr = an.x - share;
@@ -652,7 +656,7 @@ L_DEV void d_post(const Run& R, PhotonT<NF>& ph, float* dw, const PreT<NF>& pr, 
   dep.time = time;
   if (R.rec && dep.sensor >= 0) {  // the readout groups' record, at the crossing (step.py:687 _local)
     float xc[3] = {(float)(ph.x[0] + q.t * ph.d[0]), (float)(ph.x[1] + q.t * ph.d[1]), (float)(ph.x[2] + q.t * ph.d[2])};
-    ph.last = d_record(R, ph.last, dep.sensor, dep.q, time, ph.lam, ph.gen, row, ml.n, q.vol_after, xc, ph.d,
+    ph.last = d_record(R, ph.last, dep.sensor, dep.q, time, ph.lam, ph.gen, row, ml.n, v_sens, xc, ph.d,
                        q.normal);
   }
   dep.fates[0] = lost;

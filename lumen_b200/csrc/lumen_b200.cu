@@ -173,6 +173,9 @@ static int check_desc(const LumenSceneDesc* d) {
     for (int c = 0; c < d->n_cls; ++c)
       if (d->cls_born[c] < -1 || d->cls_born[c] >= d->n_cls)
         return set_err(LUMEN_ERR_ARG, "scene_create: cls_born names a class out of range");
+  if (d->pair_pre)
+    for (long long k = 0; k < (long long)d->n_cls * d->n_cls; ++k)
+      if (d->pair_pre[k] != 0 && d->pair_pre[k] != 1) return set_err(LUMEN_ERR_ARG, "scene_create: pair_pre is 0 or 1");
   for (int r = 0; r < d->n_row; ++r) {
     const int32_t* ri = d->row_i + r * LUMEN_ROW_I;
     for (int c = 0; c < LUMEN_N_COL; ++c)
@@ -790,6 +793,7 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   }
   UPLOAD(S.cls_medium, d->cls_medium, (size_t)d->n_cls);
   if (d->cls_born) UPLOAD(S.cls_born, d->cls_born, (size_t)d->n_cls);
+  if (d->pair_pre) UPLOAD(S.pair_pre, d->pair_pre, (size_t)d->n_cls * d->n_cls);
   UPLOAD(S.row_of, d->row_of, (size_t)d->n_cls * d->n_cls);
   UPLOAD(S.med_i, d->med_i, (size_t)d->n_med * LUMEN_MED_I);
   UPLOAD(S.row_i, d->row_i, (size_t)d->n_row * LUMEN_ROW_I);

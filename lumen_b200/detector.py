@@ -149,6 +149,8 @@ class Detector:
         d.reach = ctypes.c_float(a["reach"])
         if a.get("cls_born") is not None:  # sensors counting the photons born inside them: each class's entry class
             d.cls_born = iptr(keep["cls_born"])
+        if a.get("pair_pre") is not None:  # exit sensors: the class pairs whose deposit goes to the volume left
+            d.pair_pre = iptr(keep["pair_pre"])
         d.n_cls, d.n_med, d.n_row = a["n_cls"], len(keep["med_i"]), len(keep["row_i"])
         d.n_tab, d.n_pool, d.n_sensor = len(keep["tab"]), len(keep["pool"]), self.n_sensor
         d.cls_medium, d.row_of, d.med_i = iptr(keep["cls_medium"]), iptr(keep["row_of"]), iptr(keep["med_i"])
@@ -179,7 +181,8 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
 
     ``materials``: {name: Material}. ``borders``: [(pv from, pv to, OpticalSurface)] (Geant4 border surfaces, ordered);
     ``skins``: {lv name: OpticalSurface}. ``sensors``: {group: lv name}: every placement of that logical volume is a
-    sensor, counted where a crossing's surface into it deposits (the ``border_into`` rule). Light that leaves ``top``
+    sensor, counted where a crossing's surface into it deposits (the ``border_into`` rule), and where a border out of
+    it whose surface has an EFFICIENCY detects (an exit sensor, credited to the volume left). Light that leaves ``top``
     is absorbed there (the detector volume's boundary, as the reference's recipe ``detector_volume``).
     ``after_tracking``: sensor groups whose sensor model applies its QE after tracking: their rows detect every
     absorption (eff 1) and are read per normal incidence (types.py:576 per_normal: a deposit carries 1 / A_n, by
@@ -296,8 +299,16 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
     daughter_of = {(vol_cls[p.parent], vol_cls[i]) for i, p in enumerate(placed) if p.parent >= 0}
     daughter_of |= {(vol_cls[new_of[flat[j].parent]], vol_cls[n + k]) for k, j in enumerate(mesh_idx)}
     border_of = {}
+    # exit sensors: a border out of a sensor's volume whose surface has an EFFICIENCY detects there, its deposit
+    # credited to the volume left (src/lumen/rules/boundary.py:92, the surface's own EFFICIENCY)
+    exit_pairs = set()
     for a, b, s in borders:
         border_of[(vol_cls[by_name[a]], vol_cls[by_name[b]])] = s
+        if everything[by_name[a]].lv.name in sensor_lv and s.efficiency is not None:
+            exit_pairs.add((vol_cls[by_name[a]], vol_cls[by_name[b]]))
+    pair_pre = np.zeros((n_cls, n_cls), np.int32)
+    for ca, cb in exit_pairs:
+        pair_pre[ca, cb] = 1
     for ca in range(n_cls):
         for cb in range(n_cls):
             if ca == cb:
@@ -314,6 +325,8 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
                     surf = skins[cls_lv[c].name]
             is_sensor = (not into_out) and cls_lv[cb].name in sensor_lv
             per_normal = int(is_sensor and sensor_lv[cls_lv[cb].name] in set(after_tracking))
+            if (ca, cb) in exit_pairs:  # an exit sensor's crossing: the surface's EFFICIENCY, no entry rule
+                is_sensor, per_normal = True, 0
             if surf is not None and far_opq and O.kills_far_side(surf):  # NoRINDEX before the draw: the absorber
                 surf, is_sensor, per_normal = O.ABSORBER, False, 0
             if surf is None:
@@ -361,17 +374,19 @@ def build(top: G.Volume, materials: dict, *, borders=(), skins=None, sensors=Non
                 raise ValueError(f"sensor group {g!r}: its volumes have no mother volume to enter from")
             cls_born[c] = mothers[0]
     return assemble(nav, vol_cls[:n], n_cls, cls_medium, row_of, med_i, row_i, pool, st, names, cls_names, groups,
-                    precision, cls_born)  # fmt: skip
+                    precision, cls_born, pair_pre)  # fmt: skip
 
 
 def assemble(nav: dict, vol_cls, n_cls: int, cls_medium, row_of, med_i, row_i, pool: O.Pool, sensors: SensorTable,
-             names: list, cls_names: dict, groups: dict, precision: str = "float32", cls_born=None) -> Detector:
+             names: list, cls_names: dict, groups: dict, precision: str = "float32", cls_born=None,
+             pair_pre=None) -> Detector:
     """Return the Detector of navigator arrays ``nav`` (``geometry.navigator_arrays``, volumes of classes ``vol_cls``)
     and the surface lookup's tables: per class its medium (``cls_medium``), per crossed class pair its surface row
     (``row_of`` (C, C), -1 never crossed), the media's (``med_i``) and rows' (``row_i``) table indices into ``pool``;
     then the diffusion jump's clearance grids of the media whose only channel is Rayleigh
     (src/lumen/transport/fastpath.py:96). ``cls_born``: per class the entry class of a sensor that counts the photons
-    born inside it (-1 none; None: no such sensor)."""  # noqa: D205, D209
+    born inside it (-1 none; None: no such sensor); ``pair_pre`` (C, C): 1 where a crossing's deposit goes to the
+    sensor of the volume left (an exit sensor; None: none)."""  # noqa: D205, D209
     params_index = dict(pool.names)
     tab, data = pool.arrays()
     arrays = dict(nav)
@@ -380,6 +395,8 @@ def assemble(nav: dict, vol_cls, n_cls: int, cls_medium, row_of, med_i, row_i, p
                   row_i=np.asarray(row_i, np.int32), tab=tab)  # fmt: skip
     if cls_born is not None and np.any(np.asarray(cls_born) >= 0):
         arrays["cls_born"] = np.asarray(cls_born, np.int32)
+    if pair_pre is not None and np.any(np.asarray(pair_pre)):
+        arrays["pair_pre"] = np.asarray(pair_pre, np.int32).ravel()
     media = []
     for m in range(len(med_i)):
         ok = med_i[m, 0] >= 0 and med_i[m, 2] >= 0 and med_i[m, 3] < 0 and med_i[m, 7] < 0

@@ -31,9 +31,10 @@ values are the reference's bits; the navigator's arrays are this package's layou
 
 Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: split
 unions (``Definition.piece_of``), a medium channel other than Rayleigh, Mie (G4OpMieHG) and a WLS (G4OpWLS) with its
-own spectrum and a delta or exponential profile, a vertex on the class table's diagonal (a skin between touching
-volumes of one class) and a deposit to the tag before (``Optics.deposit_pre``). Sensors that count the photons
-born inside them (``Optics.born_pair``) carry their entry class per class (``LumenSceneDesc.cls_born``). A pass row
+own spectrum and a delta or exponential profile, and a vertex on the class table's diagonal (a skin between touching
+volumes of one class). Sensors that count the photons born inside them (``Optics.born_pair``) carry their entry
+class per class (``LumenSceneDesc.cls_born``), exit sensors (``Optics.deposit_pre``) the class pairs whose deposit
+goes to the volume left (``LumenSceneDesc.pair_pre``). A pass row
 (``types.PASS``: two classes of one medium split by a role elsewhere) becomes a row that carries the photon straight
 on: the reference steps over such a crossing, this navigator stops at it and continues it unchanged, so the two draw
 other random numbers for the same law (the same expected values).
@@ -143,8 +144,6 @@ def export(det) -> dict:
     optics = parts.optics
     meshes = []
     solids, volumes = export_scene(parts.nav_scene, meshes)
-    if optics.deposit_pre is not None and np.any(optics.deposit_pre):
-        raise NotImplementedError("a sensor depositing to the tag before (Optics.deposit_pre) is not converted")
     packed = pack.pack(det, det.params())
     keys = {}  # packed path -> the key it is read from directly
     for path, src in parts.key_rows.items():
@@ -227,6 +226,7 @@ def export(det) -> dict:
             "medium_of": [int(x) for x in optics.medium_of], "media": media, "row_of": row_of.tolist(), "rows": rows,
             "sensor_index": {k: int(v) for k, v in optics.sensor_index.items()},
             "born_pair": None if optics.born_pair is None else [int(x) for x in optics.born_pair],
+            "deposit_pre": None if optics.deposit_pre is None else np.asarray(optics.deposit_pre, int).tolist(),
             "sensors": {"name": list(st.name), "sensor": list(st.sensor), "position": _f(st.position),
                         "axis": _f(st.axis)}}  # fmt: skip
 
@@ -414,7 +414,7 @@ def detector(data: dict, precision: str | None = None) -> D.Detector:
     cls_names = dict(enumerate(data["class_names"]))
     return D.assemble(nav, vol_cls, int(data["n_classes"]), medium_of, np.asarray(data["row_of"]), med_i, row_i, pool,
                       st, names, cls_names, groups, precision or data.get("precision", "float32"),
-                      data.get("born_pair"))  # fmt: skip
+                      data.get("born_pair"), data.get("deposit_pre"))  # fmt: skip
 
 
 def from_reference(det, precision: str | None = None) -> D.Detector:

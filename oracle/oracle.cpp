@@ -261,7 +261,11 @@ static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
   /* _query (step.py:260; TrackedGeometry.query, tracked.py:86) */
   const NF dd[3] = {ph->d[0], ph->d[1], ph->d[2]}; /* the direction in the navigator's precision (navigate.py:682) */
   OQueryT<NF> q = onav_query(S, ph->x, dd, ph->vol, (NF)R->max_distance, ph->srf, ph->sn, (NF)s);
-  int sensor_q = q.hit ? D->vol_i[(size_t)q.vol_after * LUMEN_VOL_I + LUMEN_VI_SENSOR] : -1;
+  /* the sensor the deposit credits: the one entered, or at an exit sensor's crossing the one left, whose frame the
+     deposit's local fields are read in (step.py:615 _sensor_dep, :653 sensor_frame) */
+  const int v_sens = (D->pair_pre && q.hit && D->pair_pre[q.cls_before * D->n_cls + q.cls_after]) ? q.vol_before
+                                                                                                  : q.vol_after;
+  int sensor_q = (q.hit && v_sens >= 0) ? D->vol_i[(size_t)v_sens * LUMEN_VOL_I + LUMEN_VI_SENSOR] : -1;
   float dist = q.t;
   int zero = dist <= O_ZERO_STEP_BANDS * b0;
   /* _surface (step.py:280) */
@@ -595,7 +599,7 @@ static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
         ph->ascale = an > 0.0f ? 1.0f / an : 0.0f;
       }
       for (int a = 0; a < 3; ++a) ph->apos[a] = (float)(ph->x[a] + q.t * ph->d[a]);
-      ph->avol = q.vol_after;
+      ph->avol = v_sens;
       ph->ax = INFINITY;
     } else {
       const float left = ph->ax - share;
@@ -639,7 +643,7 @@ static void o_step(const ORun* R, OPhotonT<NF>* ph, OKey pkey, ODep* dep) {
     rc->time = time;
     rc->lam = ph->lam;
     rc->gen = ph->gen;
-    rc->vol = q.vol_after;
+    rc->vol = v_sens;
     for (int a = 0; a < 3; ++a) { rc->x[a] = (float)(ph->x[a] + q.t * ph->d[a]); rc->d[a] = ph->d[a]; rc->n[a] = q.normal[a]; }
     rc->inv_an = 1.0f;
     if (row >= 0 && D->row_i[(size_t)row * LUMEN_ROW_I + LUMEN_RI_PER_NORMAL]) {

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_entry_point(built):
 
 def test_abi_version_and_argument_errors(built):
     lib = A.engine()
-    assert lib.lumen_b200_abi_version() == 14
+    assert lib.lumen_b200_abi_version() == 15
     h = ctypes.c_void_p()
     assert lib.lumen_b200_scene_create(None, ctypes.byref(h)) == 1  # LUMEN_ERR_ARG before any device call
     assert b"null" in lib.lumen_b200_last_error()

@@ -812,3 +812,28 @@ def test_photons_born_in_a_counting_sensor_match(built):
     O, _ = oracle.trace(det, KEY, n, source=src, samples=n, controls=c, truth=True, n_events=ds.n_events)
     g = T.truth.cpu().numpy()
     assert (g.view(np.uint32) == O.truth.view(np.uint32)).all()
+
+
+def test_exit_sensor_matches(built):
+    """An exit sensor (LumenSceneDesc.pair_pre): photons emitted in a glass cube credited where they leave it through
+    a window of reflectivity 0.3; records, tallies (persistent and wavefront) and readout-free truth rows."""
+    from lumen_b200 import geometry as G
+    from lumen_b200 import optics as O
+    from lumen_b200.detector import build
+
+    water = O.Material("Water", rindex=1.33, abslength=20.0)
+    glass = O.Material("Glass", rindex=1.5, abslength=3.0)
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "Water")
+    cube = G.Volume("Cube", G.Box(0.2, 0.2, 0.2), "Glass")
+    box.place(cube, (0.3, 0.0, 0.0), name="Cube")
+    surf = O.OpticalSurface("Window", "dielectric_metal", "polished", reflectivity=0.3, efficiency=0.6)
+    det = build(box, {"Water": water, "Glass": glass}, borders=[("Cube", "Box", surf)], sensors={"s": "Cube"})
+    src = sources.Point(position=(0.32, 0.05, -0.1), n_photons=1.0, lam_range=(300.0, 600.0))
+    n = 1 << 15
+    bad, gi, oi, gf, of = _records_match(det, src, n)
+    assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}: gpu {gi[bad[:3]]} cpu {oi[bad[:3]]}"
+    for variant in (0, A.VARIANT_WAVEFRONT):
+        T, O_ = _tallies(det, src, n, controls=A.controls(variant=variant))
+        np.testing.assert_allclose(T.arrival.cpu().numpy(), O_.arrival, rtol=RTOL)
+        assert T.arrival.cpu().numpy()[0, 0] > 0.3
+        assert (T.counts.cpu().numpy()[:5] == O_.counts.astype(np.int64)[:5]).all()
