@@ -29,8 +29,9 @@ photon loop is built from, and re-derives none of them:
 ABI's tables from that data: the reference's classes, media, rows and values, one table per key. The leaves and
 values are the reference's bits; the navigator's arrays are this package's layout of them.
 
-Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: split
-unions (``Definition.piece_of``), a medium channel other than Rayleigh, Mie (G4OpMieHG) and a WLS (G4OpWLS) with its
+A split union's pieces (``Definition.piece_of``: a union of many leaves placed as its pieces) are volumes of their
+union's class. Refused (``NotImplementedError`` naming the part), where the photon loop here has no counterpart: a
+medium channel other than Rayleigh, Mie (G4OpMieHG) and a WLS (G4OpWLS) with its
 own spectrum and a delta or exponential profile, and a vertex on the class table's diagonal (a skin between touching
 volumes of one class). Sensors that count the photons born inside them (``Optics.born_pair``) carry their entry
 class per class (``LumenSceneDesc.cls_born``), exit sensors (``Optics.deposit_pre``) the class pairs whose deposit
@@ -117,19 +118,20 @@ def export_scene(scene, meshes=None) -> tuple:
                            "mother": vol_of_inst[p] if p >= 0 else -1, "R": _f(T.R[i]), "t": _f(T.t[i]),
                            "label": [int(d.member.label.medium), int(d.member.label.sensor)]})  # fmt: skip
             continue
-        if d.piece_of:
-            raise NotImplementedError(f"{dname}: a piece of a split union is not converted")
         if dname not in solids:
             solids[dname] = _solid_data(d.member.solid)
         p = int(T.parent[i])
         while p >= 0 and p not in vol_of_inst:  # an assembly places its daughters in the nearest ancestor volume
             p = int(T.parent[p])
         vol_of_inst[i] = len(volumes)
-        seg = sc.member_segment(d, dname)
+        # a piece of a split union (Definition.piece_of) takes its union's placement as its PV, the union instance
+        # being its parent (src/lumen/build/tracked.py:129 classes)
+        j = int(T.parent[i]) if d.piece_of else i
+        seg = sc.member_segment(d, d.piece_of or dname)
         lab = d.member.label
-        volumes.append({"pv": f"{T.path[i]}/{seg}" if T.path[i] else seg, "path": T.path[i], "definition": dname,
+        volumes.append({"pv": f"{T.path[j]}/{seg}" if T.path[j] else seg, "path": T.path[i], "definition": dname,
                         "parent": vol_of_inst[p] if p >= 0 else -1, "R": _f(T.R[i]), "t": _f(T.t[i]),
-                        "label": [int(lab.medium), int(lab.sensor)]})  # fmt: skip
+                        "label": [int(lab.medium), int(lab.sensor)], "piece": bool(d.piece_of)})  # fmt: skip
     return solids, volumes
 
 

@@ -8,7 +8,8 @@ examples/example_tank.py: detector volume TankLV, the PMT placements counted acr
 (examples/data/yaml_toy), and the scintillator cube of ``tests/golden/yaml_scint`` (this repository's YAML, in the
 reference's format: Rayleigh, Mie and a WLS with an exponential profile in one medium, a ground unified wall), and
 ``detectors.mesh_tank`` written out in the same format by ``mesh_tank_yaml`` (tessellated parts, an orb, skins), and
-a water cube that is an ``any_entry`` sensor counting the photons born inside it (``born_cube_yaml``).
+a water cube that is an ``any_entry`` sensor counting the photons born inside it (``born_cube_yaml``), and a comb
+of 17 bars in one union solid, which the reference places as its pieces (``comb_yaml``).
 ``lumen_b200.reference.export`` then writes what the reference's photon loop runs on: the
 navigator scene's instances and flattened solids, the compiled optics, the packed parameters, the defensive rows.
 The tests rebuild the detectors from these files with ``lumen_b200.reference.detector``.
@@ -119,6 +120,50 @@ def born_cube_yaml(where):
         f.write(text)
 
 
+COMB_BARS = 17  # a union of this many bars: past the reference's SPLIT_LEAVES (16), so it is placed as its pieces
+
+
+def comb_yaml(where):
+    """Write a 2 m water box holding a comb (a union of ``COMB_BARS`` steel bars, one solid: the reference places it
+    as its pieces) and two disc sensors, in the reference's YAML detector format, into the directory ``where``."""  # noqa: D205, D209
+    flat = "{energy: [1.5, 5.0], value: [%s, %s]}"
+    lines = ["schema: lumen-detector-yaml/3", "name: yaml_comb", "detector_volume: Box", "solids:",
+             "  WorldBox: {type: box, params: {x: 3*m, y: 3*m, z: 3*m}}",
+             "  BoxSolid: {type: box, params: {x: 2*m, y: 2*m, z: 2*m}}",
+             "  BarSolid: {type: box, params: {x: 0.04*m, y: 0.04*m, z: 1.2*m}}",
+             "  PMTDisc: {type: tube, params: {rmax: 0.15*m, z: 0.02*m}}"]  # fmt: skip
+    prev = "BarSolid"
+    for k in range(1, COMB_BARS):
+        x = -0.85 + 0.1 * k  # -0.75 .. 0.75 beside the first bar at 0: no two bars meet
+        name = "Comb" if k == COMB_BARS - 1 else f"Comb{k}"
+        lines.append(f"  {name}: {{type: union, refs: [{prev}, BarSolid], transforms: [{{}}, "
+                     f"{{position: [{x!r}, 0.0, 0.0]}}]}}")
+        prev = name
+    lines += ["volumes:", "  World: {solid: WorldBox, material: Air}", "  Box: {solid: BoxSolid, material: Water}",
+              "  Comb: {solid: Comb, material: Steel}", "  PMT: {solid: PMTDisc, material: Photocathode}",
+              "placements:", "  - {name: BoxPV, volume: Box, mother: World}",
+              "  - {name: CombPV, volume: Comb, mother: Box, position: [0.0, 0.0, 0.0]}",
+              "  - {name: PMT_0, volume: PMT, mother: Box, copy: 0, position: [0.0, 0.0, 0.95]}",
+              "  - {name: PMT_1, volume: PMT, mother: Box, copy: 1, position: [0.0, 0.0, -0.95]}",
+              "materials:",
+              "  Water: {state: liquid, composition: {density_g_cm3: 1.0, components: [{ref: H, atoms: 2}, {ref: O, "
+              "atoms: 1}]}, properties: {RINDEX: " + flat % (1.33, 1.33) + ", ABSLENGTH: " + flat % (20.0, 20.0) +
+              ", RAYLEIGH: " + flat % (5.0, 5.0) + "}}"]  # fmt: skip
+    for name in ("Air", "Steel", "Photocathode"):
+        lines.append(f"  {name}: {{state: solid, composition: {{density_g_cm3: 1.0, components: "
+                     f"[{{ref: O, fraction: 1.0}}]}}}}")
+    lines += ["surfaces:",
+              "  CathodeSurface: {type: dielectric_metal, model: unified, finish: polished, value: 0, properties: "
+              "{REFLECTIVITY: " + flat % (0.0, 0.0) + ", EFFICIENCY: " + flat % (1.0, 1.0) + "}}",
+              "borders:", "  - {name: Cathode_0, surface: CathodeSurface, pv1: BoxPV, pv2: PMT_0}",
+              "  - {name: Cathode_1, surface: CathodeSurface, pv1: BoxPV, pv2: PMT_1}",
+              "sensors:", "  - {name: pmt, rule: border_into, lv: PMT, values: examples/data/toy_pmt.json, "
+              "readout: {gate: [-10.0, 60.0]}}", ""]  # fmt: skip
+    os.makedirs(where, exist_ok=True)
+    with open(os.path.join(where, "detector.yaml"), "w") as f:
+        f.write("\n".join(lines))
+
+
 def main(ref_root):
     import refstub
 
@@ -144,6 +189,8 @@ def main(ref_root):
         made["yaml_mesh"] = api.convert(os.path.join(tmp, "yaml_mesh"), os.path.join(tmp, "m.lumen"))
         born_cube_yaml(os.path.join(tmp, "yaml_born"))
         made["yaml_born"] = api.convert(os.path.join(tmp, "yaml_born"), os.path.join(tmp, "b.lumen"))
+        comb_yaml(os.path.join(tmp, "yaml_comb"))
+        made["yaml_comb"] = api.convert(os.path.join(tmp, "yaml_comb"), os.path.join(tmp, "c.lumen"))
         for name, path in made.items():
             x = reference.export(api.load(path))
             reference.save(x, os.path.join(HERE, f"refdet_{name}.json"))

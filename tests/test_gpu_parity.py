@@ -730,14 +730,15 @@ def ref_dets():
 
     gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
     return {n: reference.detector(reference.load(os.path.join(gold, f"refdet_{n}.json")))
-            for n in ("example_tank", "yaml_toy", "yaml_scint", "yaml_mesh", "yaml_born")}  # fmt: skip
+            for n in ("example_tank", "yaml_toy", "yaml_scint", "yaml_mesh", "yaml_born", "yaml_comb")}  # fmt: skip
 
 
 @pytest.mark.parametrize(("name", "pos", "n_photons", "lam"), [("example_tank", (0.0, 0.0, 0.1), 2e5, 400.0),
                                                                ("yaml_toy", (0.1, 0.0, 0.2), 1e5, 400.0),
                                                                ("yaml_scint", (0.0, 0.0, 0.1), 1e4, 380.0),
                                                                ("yaml_mesh", (0.0, 0.5, -0.6), 1.0, 400.0),
-                                                               ("yaml_born", (0.35, 0.05, -0.1), 1.0, 400.0)])  # fmt: skip
+                                                               ("yaml_born", (0.35, 0.05, -0.1), 1.0, 400.0),
+                                                               ("yaml_comb", (0.03, 0.4, 0.2), 1.0, 400.0)])  # fmt: skip
 def test_reference_pipeline_detectors_match(name, pos, n_photons, lam, ref_dets, built):
     """The detectors the reference's own pipeline compiled: per-photon records bit-exact, then the tallies, the
     published runs' workloads (the toy tank's arrivals are the published table: tests/test_reference_detector.py)

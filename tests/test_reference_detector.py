@@ -242,3 +242,33 @@ def test_any_entry_sensor_counting_photons_born_inside():
     outside = sources.Point(position=(-0.5, 0.0, 0.0), n_photons=1.0, lam=400.0)
     U, _ = oracle.trace(d, KEY0, n, source=outside, samples=n)
     assert 0.0 < U.arrival[0, 0] < 1.0 and U.counts[A.C_STEPS] > n
+
+
+def test_split_union_pieces_are_volumes_of_their_union():
+    """A union of 17 bars (one solid, past the reference's SPLIT_LEAVES = 16: src/lumen/build/lowering.py:699
+    split_unions) is placed by the reference as its pieces, each a definition of its own (``Definition.piece_of``)
+    whose class is its union's placement's. Converted, the pieces are 17 volumes of that class, and the detector
+    traces bit for bit as this builder's 17 separate bars at the same places."""
+    x = reference.load(os.path.join(GOLD, "refdet_yaml_comb.json"))
+    pieces = [v for v in x["volumes"] if v["piece"]]
+    assert len(pieces) == 17 and len({x["class_of"][v["pv"]] for v in pieces}) == 1
+    d = reference.detector(x)
+    box = G.Volume("Box", G.Box(1.0, 1.0, 1.0), "Water")
+    bar = G.Volume("Bar", G.Box(0.02, 0.02, 0.6), "Steel")
+    for k, xk in enumerate([0.0] + [-0.85 + 0.1 * k for k in range(1, 17)]):
+        box.place(bar, (xk, 0.0, 0.0), name=f"Bar_{k}")
+    pmt = G.Volume("PMT", G.Tube(rmax=0.15, dz=0.01), "Photocathode")
+    for i, z in enumerate((0.95, -0.95)):
+        box.place(pmt, (0.0, 0.0, z), name=f"PMT_{i}", copy=i)
+    cathode = O.OpticalSurface("CathodeSurface", "dielectric_metal", "polished", reflectivity=0.0, efficiency=1.0)
+    mats = {"Water": O.Material("Water", rindex=1.33, abslength=20.0, rayleigh=5.0), "Steel": O.Material("Steel"),
+            "Photocathode": O.Material("Photocathode")}  # fmt: skip
+    own = D.build(box, mats, borders=[("Box", f"PMT_{i}", cathode) for i in range(2)], sensors={"pmt": "PMT"},
+                  after_tracking=("pmt",))  # fmt: skip
+    src = sources.Point(position=(0.03, 0.4, 0.2), n_photons=1.0, lam=400.0)
+    n = 1 << 16
+    a, _ = oracle.trace(d, KEY0, n, source=src, samples=n)
+    b, _ = oracle.trace(own, KEY0, n, source=src, samples=n)
+    np.testing.assert_allclose(a.arrival, b.arrival, rtol=RTOL)
+    np.testing.assert_allclose(a.arrival2, b.arrival2, rtol=RTOL)
+    assert np.array_equal(a.counts, b.counts)
