@@ -270,7 +270,8 @@ L_DEV void d_chained(const float* p, const float* dp, float* out, float* dout) {
 
 // the TypeEval of a surface row (types.py:352 kernel); with G > 0 gradient parameters, gt[p] the table each moves,
 // the tangents dprobs[p][o], ddet[p] (a column's value moves with its table)
-template <int G>
+// UNPOL: no polarisation state (er, ei unread): the unpolarised reflectances (a photon born in a sensor, step.py:589)
+template <int G, bool UNPOL = false>
 L_DEV void d_type_eval(const DScene& S, const float* __restrict__ pool, int row, float lam, const float* wi,
                        const float* n, float n1, float n2, const float* er, const float* ei, Eval& ev, int P,
                        const int* gt, float (*dprobs)[N_OUT], float* ddet) {
@@ -312,13 +313,13 @@ L_DEV void d_type_eval(const DScene& S, const float* __restrict__ pool, int row,
   } else if (model == 1) {
     d_amplitudes(cos_i, n1, cf(n2, 0.0f), ev.amps);
     float F;
-    if (er) {
+    if constexpr (!UNPOL) {
       float s_ax[3];
       d_s_axis(wi, n, s_ax);
       Cf es, ep;
       d_components(er, ei, wi, s_ax, &es, &ep);
       F = c_abs2(ev.amps[0]) * c_abs2(es) + c_abs2(ev.amps[1]) * c_abs2(ep);
-    } else {  // no state (er null): the unpolarised reflectance, fractions (0.5, 0.5) (types.py:257 _real)
+    } else {  // no state: the unpolarised reflectance, fractions (0.5, 0.5) (types.py:257 _real)
       F = c_abs2(ev.amps[0]) * 0.5f + c_abs2(ev.amps[1]) * 0.5f;
     }
     F = d_clip01(F);
@@ -326,7 +327,7 @@ L_DEV void d_type_eval(const DScene& S, const float* __restrict__ pool, int row,
     Rc = col[LUMEN_COL_R];
   } else {
     d_amplitudes(cos_i, n1, cf(col[LUMEN_COL_NR], col[LUMEN_COL_NK]), ev.amps);
-    if (er) {
+    if constexpr (!UNPOL) {
       float s_ax[3];
       d_s_axis(wi, n, s_ax);
       Cf es, ep;

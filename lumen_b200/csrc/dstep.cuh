@@ -713,7 +713,7 @@ L_DEV void d_born(const Run& R, PhotonT<NF>& ph, float* dw, int bp, Dep& dep, fl
   float nrm[3] = {-ph.d[0], -ph.d[1], -ph.d[2]};
   float dprobs[G > 0 ? G : 1][N_OUT], ddet[G > 0 ? G : 1];
   Eval ev;
-  d_type_eval<G>(S, R.live, row, ph.lam, ph.d, nrm, 1.0f, 1.0f, nullptr, nullptr, ev, P, R.gt, dprobs, ddet);
+  d_type_eval<G, true>(S, R.live, row, ph.lam, ph.d, nrm, 1.0f, 1.0f, nullptr, nullptr, ev, P, R.gt, dprobs, ddet);
   const float d = ev.detect;
   dep.sensor = sensor;
   dep.q = ph.w * d;

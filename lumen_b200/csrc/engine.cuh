@@ -124,6 +124,7 @@ struct Pick {
   int groups;              // frame groups: the extended instantiation with their traversal
   int analog;
   int nav64;               // the scene's navigator is float64
+  int born;                // a sensor counts the photons born inside it (the wavefront's step kernel with that branch)
   const float* vol_f32;    // the scene's float32 frames (the readout binning)
 };
 
@@ -427,7 +428,6 @@ __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   Photon ph;
   WaveExtra ex;
   wv_ld(V.ph, V.W, i, ph);
-  if (d_born_entry(L.R.S, ph) != -2) return;  // a photon born in a sensor: its step has no query (k_wave_step)
   wv_ld(V.ex, V.W, i, ex);
   Pre pr;
   d_pre<(TORUS & 1)>(L.R, ph, ex.pkey, pr);
@@ -437,7 +437,10 @@ __global__ void __launch_bounds__(256, 3) k_wave_query(Launch L, Wave V) {
   wv_st(V.q, V.W, i, q);
 }
 
-template <int G>
+// BORN: the scene has a sensor that counts the photons born inside it (the branch of their first step, which reads
+// none of the query the query kernel made for it; a scene without one runs the kernel compiled without the branch,
+// the branch costs the tank's plain forward 2 % where it is compiled in)
+template <int G, int BORN>
 __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(256, 2) k_wave_step(Launch L, Wave V) {
     if (G > 0)
       for (int p = 0; p < L.R.P; ++p) dw[p] = V.dw[(size_t)p * V.W + i];
     Ana an;
-    const int bp = d_born_entry(L.R.S, ph);
+    const int bp = BORN ? d_born_entry(L.R.S, ph) : -2;
     if (bp != -2) {
       d_born<G>(L.R, ph, dw, bp, dep, dq, an);
     } else {
@@ -686,7 +689,8 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
   V.live = live;
   const int grid = W / 256;
   CK(cudaMemsetAsync(V.act, 0, (size_t)W * 4, stream));
-  k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);  // the fill: every slot takes a photon
+  if (pk.born) k_wave_step<G, 1><<<grid, 256, 0, stream>>>(L, V);  // the fill: every slot takes a photon
+  else k_wave_step<G, 0><<<grid, 256, 0, stream>>>(L, V);
   CK(cudaGetLastError());
   ++lumen_launches();
   const long long per_slot = (L.n + W - 1) / W;  // photons a slot carries in turn
@@ -703,7 +707,8 @@ int run_wave(const Launch& L, const Pick& pk, unsigned long long* live, cudaStre
     else if (pk.single) k_wave_query<G, 2><<<grid, 256, 0, stream>>>(L, V);
     else k_wave_query<G, 0><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaMemsetAsync(V.live, 0, sizeof(unsigned long long), stream));
-    k_wave_step<G><<<grid, 256, 0, stream>>>(L, V);
+    if (pk.born) k_wave_step<G, 1><<<grid, 256, 0, stream>>>(L, V);
+    else k_wave_step<G, 0><<<grid, 256, 0, stream>>>(L, V);
     CK(cudaGetLastError());
     lumen_launches() += 2;
     if (!async && (r & 3) == 3) {

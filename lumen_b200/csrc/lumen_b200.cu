@@ -356,6 +356,7 @@ static int fill_launch(const LumenScene* sc, const LumenRows* rows, const LumenS
   pk.clip = sc->clip;
   pk.groups = sc->groups;
   pk.nav64 = sc->nav64;
+  pk.born = sc->S.cls_born != nullptr;
   pk.vol_f32 = sc->vol_f32;
   pk.analog = (c->flags & LUMEN_F_TRUTH) != 0;
   if (pk.analog && (c->n_grad > 0 || !L.R.shared))
