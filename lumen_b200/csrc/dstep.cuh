@@ -768,7 +768,9 @@ L_DEV void d_step(const Run& R, PhotonT<NF>& ph, float* dw, Key pkey, Dep& dep, 
 }
 
 // ------------------------------------------------------------------------------------------------ sources
-struct Row { float x[3], d[3], t, lam, w0, er[3], ei[3]; int event; };
+// vol: the start point's volume when the call knows it (every photon of a point-like event starts at the event's
+// point, located once: Launch.ev_vol), else -1 (located here)
+struct Row { float x[3], d[3], t, lam, w0, er[3], ei[3]; int event; int vol; };
 
 L_DEV float d_gaussian(float u) {
   float f = u - 5.9604644775390625e-8f;
@@ -985,7 +987,7 @@ L_DEV void d_start(const DScene& S, const Row& r, PhotonT<NF>& ph) {
   ph.wr = 1.0f;
   ph.alive = 1;
   ph.vertex = 0;
-  ph.vol = nav_locate<EXT>(S, ph.x);
+  ph.vol = r.vol >= 0 ? r.vol : nav_locate<EXT>(S, ph.x);
   ph.cls = d_cls(S, ph.vol);
   ph.srf = -1;
   ph.nz = 0;

@@ -114,6 +114,7 @@ struct Launch {
   const float* wv_dw;
   const int32_t* wv_act;
   int wv_W;
+  const int32_t* ev_vol;  // per event its start volume (point-like sources: k_event_locate), or null
 };
 
 // what picks a launch's instantiation, host side: the scene has a torus leaf; the run keeps truth rows
@@ -224,6 +225,18 @@ __device__ __forceinline__ int deposit(const Tally& T, int e, const Dep& dep, co
 __device__ __forceinline__ void get_row(const Launch& L, int64_t i, Row& r) {
   if (L.use_rows) d_rows_row(L.rows, i, r);
   else d_source_row(L.R.S, L.R.live, L.R.ref, L.src, L.key, L.first_id + i, r);
+  r.vol = L.ev_vol ? __ldg(L.ev_vol + r.event) : -1;
+}
+
+// every point-like event's start volume, located once per call (Launch.ev_vol: the point and time sources, whose
+// photons all start at the event's point; the same locate as each photon's would be, EXT the run's)
+template <int EXT>
+__global__ void k_event_locate(DScene S, LumenSource src, int32_t* ev_vol) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= src.n_events) return;
+  const float* f = src.ev_f + (size_t)e * LUMEN_EV_F;
+  float x[3] = {__ldg(f), __ldg(f + 1), __ldg(f + 2)};
+  ev_vol[e] = nav_locate<EXT>(S, x);
 }
 
 struct WaveExtra {  // what a slot carries besides the photon: its key, event, row weight and sensor-sum cache
@@ -765,6 +778,15 @@ template <class NF>
 int launch_locate(const DScene& S, const NF* pts, int64_t n, int32_t* vol, cudaStream_t stream) {
   const int block = 128;
   k_locate<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(S, pts, n, vol);
+  CK(cudaGetLastError());
+  ++lumen_launches();
+  return 0;
+}
+
+template <int EXT>
+int launch_event_locate(const DScene& S, const LumenSource& src, int32_t* ev_vol, cudaStream_t stream) {
+  const int block = 128;
+  k_event_locate<EXT><<<(unsigned)((src.n_events + block - 1) / block), block, 0, stream>>>(S, src, ev_vol);
   CK(cudaGetLastError());
   ++lumen_launches();
   return 0;

@@ -34,6 +34,8 @@ template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaSt
 template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int, int,
                                       float*);
 #elif LUMEN_PART == 11
+template int launch_event_locate<0>(const DScene&, const LumenSource&, int32_t*, cudaStream_t);
+template int launch_event_locate<1>(const DScene&, const LumenSource&, int32_t*, cudaStream_t);
 template int launch_photons<0>(const Launch&, int32_t*, float*, cudaStream_t);
 template int launch_photons<1>(const Launch&, int32_t*, float*, cudaStream_t);
 template int launch_query<float>(const DScene&, const float*, const int32_t*, const int32_t*, float, int64_t, int32_t*,

@@ -37,6 +37,8 @@ LUMEN_SHAPES(LUMEN_EXTERN_SHAPE)
 extern template int run_wave<0>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int, int, float*);
 extern template int run_wave<LUMEN_MAX_GRAD>(const Launch&, const Pick&, unsigned long long*, cudaStream_t, int, int,
                                              int, float*);
+extern template int launch_event_locate<0>(const DScene&, const LumenSource&, int32_t*, cudaStream_t);
+extern template int launch_event_locate<1>(const DScene&, const LumenSource&, int32_t*, cudaStream_t);
 extern template int launch_photons<0>(const Launch&, int32_t*, float*, cudaStream_t);
 extern template int launch_photons<1>(const Launch&, int32_t*, float*, cudaStream_t);
 extern template int launch_query<float>(const DScene&, const float*, const int32_t*, const int32_t*, float, int64_t,
@@ -529,6 +531,17 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
     T.mt_mask = (unsigned)(slots - 1);
   }
   int st = 0;
+  // a point-like source's events: each located once, its photons starting in that volume (the locate each would
+  // make; the float64 navigator's scenes locate per photon in float64)
+  int32_t* ev_vol = nullptr;
+  if (L.n > 0 && !L.use_rows && (L.src.kind == LUMEN_SRC_POINT || L.src.kind == LUMEN_SRC_SCINT) && !pk.nav64 &&
+      L.src.n_events > 0) {
+    CK(cudaMallocAsync((void**)&ev_vol, (size_t)L.src.n_events * sizeof(int32_t), stream));
+    st = (pk.torus || pk.groups) ? launch_event_locate<1>(L.R.S, L.src, ev_vol, stream)
+                                 : launch_event_locate<0>(L.R.S, L.src, ev_vol, stream);  // fmt: skip
+    if (st) return st;
+    L.ev_vol = ev_vol;
+  }
   if (L.n > 0) {
     if (L.R.P > 0 || cot) {
       Launch L2 = L;
@@ -546,6 +559,7 @@ static int run_trace(Launch& L, Pick pk, const LumenTallies* out, const double* 
       if (st) return st;
     }
   }
+  if (ev_vol) CK(cudaFreeAsync(ev_vol, stream));
   if (mt) {
     if ((st = launch_moment_flush(T, stream))) return st;
     CK(cudaFreeAsync(mt, stream));
