@@ -11,6 +11,7 @@ reference held, runs at nearby values share their random numbers (common random 
 
 from __future__ import annotations
 
+import hashlib
 import math
 import warnings
 from dataclasses import dataclass, field
@@ -86,6 +87,16 @@ def moment_error(x2, x, n):
     return np.sqrt(n / np.maximum(n - 1.0, 1.0) * v)
 
 
+def _check_values(det, pool, what):
+    """``Detector.check_values``, once per detector and pool values (a run repeated at the same values checks once:
+    the digests of the values found admissible are kept on the detector)."""  # noqa: D205, D209
+    key = hashlib.blake2b(np.ascontiguousarray(pool).tobytes(), digest_size=16).digest()
+    seen = det.__dict__.setdefault("_admissible", set())
+    if key not in seen:
+        det.check_values(pool, what)
+        seen.add(key)
+
+
 def _engine(det, device=None) -> Engine:
     cache = det.__dict__.setdefault("_engines", {})
     dev = torch.device(device if device is not None else "cuda", torch.cuda.current_device()) if device is None \
@@ -117,9 +128,9 @@ def simulate(det, source, params=None, *, samples=None, seed=0, reference=None, 
     """
     live = det.pool_with(params)
     ref = None if reference is None else det.pool_with({**(params or {}), **reference})
-    det.check_values(live, "simulate")  # a concrete value outside its range is refused (build/values.py:203)
+    _check_values(det, live, "simulate")  # a concrete value outside its range is refused (build/values.py:203)
     if ref is not None:
-        det.check_values(ref, "simulate: reference")
+        _check_values(det, ref, "simulate: reference")
     eng = _engine(det, device)
     eng.set_pools(live, ref)
     ctl = dict(roulette=0.01, max_distance=0.0, max_vertices=1 << 22, variant=None, jump=True) | (controls or {})
@@ -207,12 +218,28 @@ def _labels(source, dsrc, first, m, n_ev):
     return (np.searchsorted(ev_first, ids, side="right") - 1).astype(np.int32)
 
 
+def _host_tallies(T):
+    """The tallies on the host in one device-to-host copy: {name: array} of the FP64 tallies, "counts" and
+    "nonfinite" (the output cells that are not finite, counted on the device)."""  # noqa: D205, D209
+    names = [k for k in ("arrival", "arrival_t", "arrival2", "hist", "jac", "health") if getattr(T, k) is not None]
+    cells = [getattr(T, k) for k in ("arrival", "arrival_t", "arrival2", "hist", "jac") if getattr(T, k) is not None]
+    nonfinite = sum((~torch.isfinite(c)).sum() for c in cells).to(torch.float64).reshape(1)
+    flat = torch.cat([getattr(T, k).reshape(-1) for k in names] + [nonfinite, T.counts.view(torch.float64)]).cpu()
+    out, o = {}, 0
+    for k in names:
+        t = getattr(T, k)
+        out[k] = flat[o:o + t.numel()].numpy().reshape(tuple(t.shape))
+        o += t.numel()
+    out["nonfinite"] = int(flat[o].item())
+    out["counts"] = flat[o + 1:].numpy().view(np.int64)
+    return out
+
+
 def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):
-    arr = T.arrival.cpu().numpy()
-    arr_t = T.arrival_t.cpu().numpy()
-    arr2 = T.arrival2.cpu().numpy()
-    h = T.health.cpu().numpy()
-    cnt = T.counts.cpu().numpy()
+    host = _host_tallies(T)
+    arr, arr_t, arr2 = host["arrival"], host["arrival_t"], host["arrival2"]
+    h = host["health"]
+    cnt = host["counts"]
     if n_ev > 1:
         per_ev = np.diff(source.arrays(samples, det)["ev_first"]) if not isinstance(source, FromArrays) else \
             np.bincount(np.asarray(source.event), minlength=n_ev)  # fmt: skip
@@ -224,20 +251,19 @@ def _light(det, T, n_ev, samples, seed, gnames, bins, source, G=None):
     with np.errstate(invalid="ignore", divide="ignore"):
         mt = np.where(arr > 0, arr_t / np.where(arr > 0, arr, 1.0), np.nan)
     # the output cells that are not finite (the reference's exact-sum cells that are NaN, src/lumen/api.py:469)
-    cells = [arr, arr_t, arr2] + [x.cpu().numpy() for x in (T.hist, T.jac) if x is not None]
-    nonfinite = int(sum(np.count_nonzero(~np.isfinite(c)) for c in cells))
+    nonfinite = host["nonfinite"]
     health = Health(lost=h[0], abandoned=h[1], escaped=h[2], distance_cut=h[3], absorbed_bulk=h[4],
                     absorbed_surface=h[5], rouletted=h[6], reweighted=h[7], truncated=h[8], pushed=h[9],
                     start=h[10], records=int(cnt[2]), photons=int(cnt[0]), steps=int(cnt[1]),
                     nonfinite=nonfinite)  # fmt: skip
     diag = None
     if bins[0]:
-        hist = T.hist.cpu().numpy()
+        hist = host["hist"]
         diag = {"time": hist if n_ev > 1 else hist[0], "time_edges": bins[1] + bins[2] * np.arange(bins[0] + 1)}
     groups = G.histograms(nn) if G is not None else None
     grads = None
     if gnames:
-        jac = T.jac.cpu().numpy()
+        jac = host["jac"]
         grads = {k: (jac[..., i] if n_ev > 1 else jac[0, :, i]) for i, k in enumerate(gnames)}
     prov = dict(seed=seed, samples=samples, engine="lumen_b200", steps_per_photon=cnt[1] / max(cnt[0], 1),
                 moment_table_sums=int(cnt[A.C_MULTI]))  # fmt: skip
