@@ -48,6 +48,11 @@ struct DScene {
   const float* __restrict__ node_f;
   const int32_t* __restrict__ node_i;
   const int32_t* __restrict__ items;
+  // the float32 ray traversal's node records, 16 words a node: an inner node's left and right child boxes (lo, hi:
+  // words 0-5 and 6-11) and codes (12, 13), every node's own code (14); a code is an inner node's index or -2 - p for
+  // a leaf whose items are witem[p], witem[p + 1], ... up to a -1
+  const float4* __restrict__ node_w;
+  const int32_t* __restrict__ witem;
   const int32_t* __restrict__ kind_i;
   const float* __restrict__ leaf_f;
   const int32_t* __restrict__ leaf_i;

@@ -970,6 +970,7 @@ L_DEV Best d_enter_x(const DScene& S, const Ctx& c, int has_own, int vi) {
   NF tins[D_STACK];
   int sp = 0;
   int node = -1;
+  int lp = 0, lend = 0;  // the current leaf's items still to visit: S.items[lp, lend)
   int started = 0;
   int pending = has_own;
   for (;;) {
@@ -989,6 +990,10 @@ L_DEV Best d_enter_x(const DScene& S, const Ctx& c, int has_own, int vi) {
         }
       }
       while (item < 0) {
+        if (lp < lend) {
+          item = __ldg(S.items + lp++);
+          break;
+        }
         if (node < 0) {
           NF lim = d_min(b.t, c.t_bound) + c.band;
           while (sp > 0 && tins[sp - 1] > lim) sp--;
@@ -998,10 +1003,11 @@ L_DEV Best d_enter_x(const DScene& S, const Ctx& c, int has_own, int vi) {
         }
         const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
         int cnt = __ldg(ni + 1);
-        if (cnt > 0) {
-          item = __ldg(S.items + __ldg(ni + 2));
+        if (cnt > 0) {  // a leaf: its items in turn
+          lp = __ldg(ni + 2);
+          lend = lp + cnt;
           node = -1;
-          break;
+          continue;
         }
         int lc = node + 1;
         int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
@@ -1049,6 +1055,26 @@ L_DEV Best d_enter_x(const DScene& S, const Ctx& c, int has_own, int vi) {
   return b;
 }
 
+// slab test of a box held in registers (lo[3], hi[3]): d_slab's arithmetic on a node record's child box
+L_DEV void d_slab_box(const float* bx, const NF* o, const NF* inv, NF* tin, NF* tout) {
+  NF lo_t = -N_HUGE * 10.0f, hi_t = N_HUGE * 10.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    NF ta = (bx[a] - o[a]) * inv[a];
+    NF tb = (bx[3 + a] - o[a]) * inv[a];
+    lo_t = d_max(lo_t, d_min(ta, tb));
+    hi_t = d_min(hi_t, d_max(ta, tb));
+  }
+  *tin = lo_t;
+  *tout = hi_t;
+}
+
+// The candidate entries of volume c.v along the ray (navigate.py:482 enter, :465 _group, :430 _node): the volume's own
+// solid first (has_own), then its BVH depth first, the nearer child first and the farther onto the stack with its
+// entry t, the stack's entries past the best event so far dropped, each leaf's items in turn (a leaf holds one or
+// more). The float32 navigator walks the node records (S.node_w: per inner node both children's boxes and codes in
+// 64 B, four 16-byte loads a level); the float64 one the node arrays (a child's box and its right sibling's index
+// read from the node).
 template <int TORUS>
 L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   if constexpr (TORUS == 3) return d_enter_x(S, c, has_own, vi);
@@ -1064,7 +1090,13 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
   int stack[D_STACK];
   NF tins[D_STACK];
   int sp = 0;
+#if NAV_IS64
   int node = -1;       // the traversal's next node (-1: pop or done)
+  int lp = 0, lend = 0;  // the current leaf's items still to visit: S.items[lp, lend)
+#else
+  int node = -1;       // the next node's code: an inner node's index, -2 - p a leaf's item list at S.witem + p, -1 none
+  int lp = -1;         // the current leaf's next item in S.witem (-1: none)
+#endif
   int started = 0;     // the root has been tested
   int pending = has_own;
   for (;;) {
@@ -1079,29 +1111,62 @@ L_DEV Best d_enter(const DScene& S, const Ctx& c, int has_own, int vi) {
         if (n0 < n1) {
           NF tin, tout;
           d_slab(NAV_NODE(S), n0, c.od, inv, &tin, &tout);
-          node = (tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band) ? n0 : -1;
+          const int meets = tin <= tout && tout >= c.t_lo && tin <= d_min(b.t, c.t_bound) + c.band;
+#if NAV_IS64
+          node = meets ? n0 : -1;
+#else
+          node = meets ? __float_as_int(__ldg(S.node_w + (size_t)n0 * 4 + 3).z) : -1;  // the root's own code
+#endif
         }
       }
       while (item < 0) {
-        if (node < 0) {
+#if NAV_IS64
+        if (lp < lend) {
+          item = __ldg(S.items + lp++);
+          break;
+        }
+#else
+        if (lp >= 0) {
+          item = __ldg(S.witem + lp);
+          lp = __ldg(S.witem + lp + 1) >= 0 ? lp + 1 : -1;
+          break;
+        }
+#endif
+        if (node == -1) {
           NF lim = d_min(b.t, c.t_bound) + c.band;
           while (sp > 0 && tins[sp - 1] > lim) sp--;
           if (sp == 0) break;
           sp--;
           node = stack[sp];
         }
+#if NAV_IS64
         const int32_t* ni = S.node_i + (size_t)node * LUMEN_NODE_I;
         int cnt = __ldg(ni + 1);
-        if (cnt > 0) {  // a leaf: one item
-          item = __ldg(S.items + __ldg(ni + 2));
+        if (cnt > 0) {  // a leaf: its items in turn
+          lp = __ldg(ni + 2);
+          lend = lp + cnt;
           node = -1;
-          break;
+          continue;
         }
         int lc = node + 1;
         int rc = __ldg(S.node_i + (size_t)lc * LUMEN_NODE_I);
         NF tl, tlo, tr, tro;
         d_slab(NAV_NODE(S), lc, c.od, inv, &tl, &tlo);
         d_slab(NAV_NODE(S), rc, c.od, inv, &tr, &tro);
+#else
+        if (node <= -2) {  // a leaf: its items in turn
+          lp = -2 - node;
+          node = -1;
+          continue;
+        }
+        const float4* nw = S.node_w + (size_t)node * 4;
+        const float4 w0 = __ldg(nw), w1 = __ldg(nw + 1), w2 = __ldg(nw + 2), w3 = __ldg(nw + 3);
+        const float bl[6] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y}, br[6] = {w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+        const int lc = __float_as_int(w3.x), rc = __float_as_int(w3.y);
+        NF tl, tlo, tr, tro;
+        d_slab_box(bl, c.od, inv, &tl, &tlo);
+        d_slab_box(br, c.od, inv, &tr, &tro);
+#endif
         NF lim = d_min(b.t, c.t_bound) + c.band;
         int hl = tl <= tlo && tlo >= c.t_lo && tl <= lim;
         int hr = tr <= tro && tro >= c.t_lo && tr <= lim;

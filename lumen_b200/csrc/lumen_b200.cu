@@ -774,6 +774,41 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
   UPLOAD(S.node_f, d->node_f, (size_t)d->n_node * LUMEN_NODE_F);
   UPLOAD(S.node_i, d->node_i, (size_t)d->n_node * LUMEN_NODE_I);
   UPLOAD(S.items, d->items, (size_t)d->n_item);
+  {  // the float32 ray traversal's node records (DScene::node_w) and the leaves' item lists
+    const int nn = d->n_node;
+    std::vector<int32_t> code((size_t)(nn > 0 ? nn : 1), -1), witem;
+    for (int n = 0; n < nn; ++n) {
+      const int32_t* ni = d->node_i + (size_t)n * LUMEN_NODE_I;
+      if (ni[1] > 0 && (ni[2] < 0 || ni[2] + ni[1] > d->n_item)) {
+        code[n] = -1;  // outside every BVH the checks above walked: never reached
+      } else if (ni[1] > 0) {
+        code[n] = -2 - (int32_t)witem.size();
+        for (int k = 0; k < ni[1]; ++k) witem.push_back(d->items[ni[2] + k]);
+        witem.push_back(-1);
+      } else {
+        code[n] = n;
+      }
+    }
+    std::vector<float> rec((size_t)(nn > 0 ? nn : 1) * 16, 0.0f);
+    for (int n = 0; n < nn; ++n) {
+      float* r = rec.data() + (size_t)n * 16;
+      const int lc = n + 1, rc = lc < nn ? d->node_i[(size_t)lc * LUMEN_NODE_I] : -1;
+      if (d->node_i[(size_t)n * LUMEN_NODE_I + 1] == 0 && lc < nn && rc >= 0 && rc < nn) {
+        std::copy(d->node_f + (size_t)lc * LUMEN_NODE_F, d->node_f + (size_t)lc * LUMEN_NODE_F + 6, r);
+        std::copy(d->node_f + (size_t)rc * LUMEN_NODE_F, d->node_f + (size_t)rc * LUMEN_NODE_F + 6, r + 6);
+        memcpy(r + 12, &code[lc], 4);
+        memcpy(r + 13, &code[rc], 4);
+      }
+      memcpy(r + 14, &code[n], 4);
+    }
+    if (nn > 0) {
+      UPLOAD(S.node_w, reinterpret_cast<const float4*>(rec.data()), (size_t)nn * 4);
+      UPLOAD(S.witem, witem.data(), witem.size());
+    } else {
+      S.node_w = nullptr;
+      S.witem = nullptr;
+    }
+  }
   UPLOAD(S.kind_i, d->kind_i, (size_t)d->n_kind * LUMEN_KIND_I);
   if (d->n_tri > 0 || d->n_group > 0) {  // the triangles and the groups' frames after the leaves (one allocation)
     const size_t nl = (size_t)d->n_leaf * LUMEN_LEAF_F, nt = (size_t)d->n_tri * LUMEN_TRI_F;
