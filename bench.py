@@ -40,8 +40,8 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per photon-step of the tank workload, from ncu's dram__bytes_read.sum + dram__bytes_write.sum: the
 # persistent loop k_trace<0,256,4,2,0,0> on one launch of 2^20 photons (2.76 steps each; local memory almost all of
 # it), and the wavefront's k_wave_query<0,2> + k_wave_step<0> summed over every round of seven calls of 2^20 photons
-# (2.76 steps each; 2.655 GB read + 2.101 GB written per call: the slots' state and the kernels' local memory)
-TRAFFIC_PER_STEP = {0: (0.253087e9 + 1.570654e9) / (1048576 * 2.760), 3: (2.655e9 + 2.101e9) / (1048576 * 2.761)}
+# (2.76 steps each; 2.613 GB read + 2.090 GB written per call: the slots' state and the kernels' local memory)
+TRAFFIC_PER_STEP = {0: (0.253087e9 + 1.570654e9) / (1048576 * 2.760), 3: (2.613e9 + 2.090e9) / (1048576 * 2.760)}
 
 
 def workload_point(seed=12345):
