@@ -434,8 +434,7 @@ int32_t lumen_b200_adjoint(const LumenScene* scene, const LumenRows* rows, const
    refused with LUMEN_ERR_ARG. The photons' sums past their first four sensors go to a fixed moment table of
    LUMEN_STATIC_MOMENT_SLOTS slots; a sum that finds it full is squared alone and counted in
    counts[LUMEN_C_MOMENT_LOST]. Every GPU that loads the library holds both arrays until the process exits. The
-   first call on a device looks up the arrays' addresses there, with that device current, so make that first call
-   before any stream capture. All calls share the arrays and leave their contents in them; each call clears what
+   first call on a device looks up the arrays' addresses there, with that device current. All calls share the arrays and leave their contents in them; each call clears what
    must start at zero. Calls that overlap on the GPU (other streams, other host threads) race on the arrays: run
    them one after another. */
 int32_t lumen_b200_trace_static(const LumenScene* scene, const LumenRows* rows, const LumenSource* source,
