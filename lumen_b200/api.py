@@ -224,7 +224,12 @@ def _host_tallies(T):
     names = [k for k in ("arrival", "arrival_t", "arrival2", "hist", "jac", "health") if getattr(T, k) is not None]
     cells = [getattr(T, k) for k in ("arrival", "arrival_t", "arrival2", "hist", "jac") if getattr(T, k) is not None]
     nonfinite = sum((~torch.isfinite(c)).sum() for c in cells).to(torch.float64).reshape(1)
-    flat = torch.cat([getattr(T, k).reshape(-1) for k in names] + [nonfinite, T.counts.view(torch.float64)]).cpu()
+    dev = torch.cat([getattr(T, k).reshape(-1) for k in names] + [nonfinite, T.counts.view(torch.float64)])
+    if dev.is_cuda:  # into page-locked memory (torch's caching host allocator keeps it for the next call)
+        flat = torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True)
+        flat.copy_(dev)
+    else:
+        flat = dev
     out, o = {}, 0
     for k in names:
         t = getattr(T, k)
