@@ -12,6 +12,8 @@
 //
 // Numerics: compiled with -fmad=false; every fused multiply-add is an explicit fmaf, every elementary function the
 // library's own (dmath.cuh), so a photon's path is the CPU checker's bit for bit.
+#include <limits>
+
 #include "engine.cuh"
 #include "dreadout.cuh"
 
@@ -84,6 +86,8 @@ static int check_desc(const LumenSceneDesc* d) {
   if (!d || d->n_vol <= 0 || !d->vol_i || !d->vol_f || !d->kind_i || !d->leaf_f || !d->leaf_i || !d->prog_i ||
       !d->cls_medium || !d->row_of || !d->med_i || !d->tab || !d->pool || d->n_cls <= 0 || d->n_pool <= 0)
     return set_err(LUMEN_ERR_ARG, "scene_create: a required array is null or empty");
+  if (d->n_node < 0 || d->n_item < 0 || (d->n_node > 0 && (!d->node_f || !d->node_i)) || (d->n_item > 0 && !d->items))
+    return set_err(LUMEN_ERR_ARG, "scene_create: BVH nodes or items without their arrays");
   if (d->precision != LUMEN_PREC_FLOAT32 && d->precision != LUMEN_PREC_FLOAT64)
     return set_err(LUMEN_ERR_ARG, "scene_create: precision is LUMEN_PREC_FLOAT32 or LUMEN_PREC_FLOAT64");
   if (d->precision == LUMEN_PREC_FLOAT64 && (!d->vol_f64 || !d->leaf_f64 || (d->n_node > 0 && !d->node_f64) ||
@@ -149,6 +153,7 @@ static int check_desc(const LumenSceneDesc* d) {
       auto [nd, dp] = todo.back();
       todo.pop_back();
       if (nd < n0 || nd >= n1 || dp > LUMEN_MAX_BVH_DEPTH) return set_err(LUMEN_ERR_SCENE, "scene_create: a BVH is malformed or deeper than LUMEN_MAX_BVH_DEPTH");
+      if (d->node_i[(size_t)nd * LUMEN_NODE_I + 1] < 0) return set_err(LUMEN_ERR_SCENE, "scene_create: a BVH node with a negative count");
       if (d->node_i[(size_t)nd * LUMEN_NODE_I + 1] == 0) {
         todo.push_back({nd + 1, dp + 1});
         todo.push_back({d->node_i[(size_t)(nd + 1) * LUMEN_NODE_I], dp + 1});
@@ -789,9 +794,15 @@ int32_t lumen_b200_scene_create(const LumenSceneDesc* d, LumenScene** out) {
         code[n] = n;
       }
     }
-    std::vector<float> rec((size_t)(nn > 0 ? nn : 1) * 16, 0.0f);
+    // a record without children (a leaf's, or a node outside every BVH) has NaN boxes, which no slab test meets
+    // (every comparison with NaN is false), and codes -1
+    std::vector<float> rec((size_t)(nn > 0 ? nn : 1) * 16, std::numeric_limits<float>::quiet_NaN());
     for (int n = 0; n < nn; ++n) {
       float* r = rec.data() + (size_t)n * 16;
+      const int32_t none = -1, zero = 0;
+      memcpy(r + 12, &none, 4);
+      memcpy(r + 13, &none, 4);
+      memcpy(r + 15, &zero, 4);
       const int lc = n + 1, rc = lc < nn ? d->node_i[(size_t)lc * LUMEN_NODE_I] : -1;
       if (d->node_i[(size_t)n * LUMEN_NODE_I + 1] == 0 && lc < nn && rc >= 0 && rc < nn) {
         std::copy(d->node_f + (size_t)lc * LUMEN_NODE_F, d->node_f + (size_t)lc * LUMEN_NODE_F + 6, r);

@@ -6,6 +6,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 from lumen_b200 import _abi as A
@@ -90,6 +91,25 @@ def test_scene_create_refuses_a_corrupt_bvh_item(built):
 
     st, msg = _create(det, corrupt)
     assert st == 1 and "BVH item" in msg
+
+
+def test_scene_create_refuses_a_negative_leaf_count_and_missing_bvh_arrays(built):
+    """A node count below 0 is neither a leaf (count > 0) nor an inner node (count 0), and BVH nodes or items without
+    their arrays cannot be walked: both are refused on the host, before any device call."""
+    det = detectors.cylinder_tank(n_pmt=20)
+    leaf = int(np.flatnonzero(det.arrays["node_i"][:, 1] > 0)[0])
+
+    def negative(d, keep):
+        keep["node_i"][leaf, 1] = -1
+
+    st, msg = _create(det, negative)
+    assert st == 3 and "negative count" in msg  # LUMEN_ERR_SCENE
+
+    def no_nodes(d, keep):
+        d.node_i = ctypes.cast(None, A.c_i32p)
+
+    st, msg = _create(det, no_nodes)
+    assert st == 1 and "BVH nodes or items" in msg
 
 
 @pytest.mark.parametrize("bad", [float("nan"), -1.0, float("inf")])
