@@ -3,9 +3,10 @@ item of a leaf visited in turn, src/lumen/geometry/navigate.py:440-443 _node).
 
 This package's builder makes a leaf per item, so these tests rebuild a detector's BVHs with the two leaves of every
 node whose children are both leaves of consecutive items merged into one leaf of two. The winner of a query does not
-depend on the order the items are visited in, and the checker scans the candidate lists without a BVH: queries,
-locates and photons through the merged BVHs are the checker's bit for bit, in the float32 navigator (its node
-records), the float64 one (the node arrays) and the frame groups' walk.
+depend on the order the items are visited in, and the checker scans the candidate lists without a BVH. Through the
+merged BVHs: the query, locate and per-photon kernels (the extended walk over the node arrays, in float32 and float64,
+frame groups included) are the checker's bit for bit, and the engine's own trace (the wavefront and the persistent
+loop: the float32 walk over the node records) gives the checker's counts and its tallies to their summation order.
 """
 
 import copy
@@ -16,7 +17,7 @@ import pytest
 import oracle
 from lumen_b200 import _abi as A
 from lumen_b200 import detectors, sources
-from lumen_b200.engine import DeviceSource, Engine
+from lumen_b200.engine import DeviceSource, DeviceTallies, Engine
 
 pytestmark = pytest.mark.gpu
 
@@ -126,3 +127,22 @@ def test_two_item_leaves_photons_bit_exact(built):
     _, (oi, of) = oracle.trace(tank, KEY, n, source=src, samples=n, records=True, controls=c)
     bad = np.flatnonzero((gi != oi).any(1) | (gf.view(np.uint32) != of.view(np.uint32)).any(1))
     assert len(bad) == 0, f"{len(bad)} photons differ, first {bad[:5]}"
+
+
+@pytest.mark.parametrize("variant", [A.VARIANT_WAVEFRONT, 0])
+def test_two_item_leaves_traced_tallies_match(variant, built):
+    """The engine's own trace (the wavefront and the persistent loop: the float32 walk over the node records) on the
+    tank with two-item leaves, and a second event whose photons start elsewhere: the counts are the checker's and the
+    FP64 tallies agree to their summation order."""
+    tank = _two_item_leaves(detectors.cylinder_tank())
+    src = sources.Point(position=[(1.0, -0.5, 2.0), (-3.0, 2.5, -4.0)], n_photons=1.0, lam_range=(300.0, 600.0))
+    n = 1 << 15
+    c = A.controls(variant=variant)
+    eng = _engine(tank)
+    ds = DeviceSource(src, n)
+    T = DeviceTallies(eng.n_sensor, ds.n_events, 0, 0.0, 1.0, 0)
+    eng.trace(KEY, n, source=ds, controls=c, tallies=T)
+    O, _ = oracle.trace(tank, KEY, n, source=src, samples=n, controls=c, n_events=ds.n_events)
+    np.testing.assert_allclose(T.arrival.cpu().numpy(), O.arrival, rtol=1e-9, atol=1e-15)
+    np.testing.assert_allclose(T.arrival2.cpu().numpy(), O.arrival2, rtol=1e-9, atol=1e-15)
+    assert (T.counts.cpu().numpy()[:5] == O.counts.astype(np.int64)[:5]).all()
